@@ -1,0 +1,177 @@
+"""numpy restatement of the small-strain Lippmann-Schwinger solver (oracle).
+
+TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
+
+Follows mgkmc/linear_elastic_simulator.py:
+  * ``spectral_solver_2d``  -- :12-88
+  * ``spectral_solver_3d``  -- :274-376
+  * ``mixed_bc_solve_2d``   -- the macro mixed stress/strain loop of
+    ``linear_elastic_simulation_2d`` :176-197 with the compliance correction of
+    :150-152, here with an eigenstrain field (the reference driver has no
+    ``eps_plastic`` argument, so the benchmark harness restates the loop).
+and mgkmc/elasticity.py:3-105 for the Lame constants, Hooke's law and the
+isotropic Green operator.  FFTs are ortho-normalised complex fftn/ifftn with
+``.real`` taken on the inverse (mgkmc/fft.py:22-31).
+"""
+import numpy as np
+
+
+def lame_2d(E, nu, plane_mode="plane_strain"):
+    # mgkmc/elasticity.py:3-10
+    mu = E / (2 * (1 + nu))
+    if plane_mode == "plane_stress":
+        lam = E * nu / (1 - nu ** 2)
+    else:
+        lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    return lam, mu
+
+
+def lame_3d(E, nu):
+    # mgkmc/elasticity.py:55-59
+    mu = E / (2 * (1 + nu))
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    return lam, mu
+
+
+def hooke(eps, lam, mu, d):
+    # mgkmc/elasticity.py:12-18 and :62-67: sigma = 2 mu eps + lam tr(eps) I
+    tr = np.trace(eps, axis1=-2, axis2=-1)[..., None, None]
+    I = np.eye(d)
+    return 2 * np.asarray(mu)[..., None, None] * eps + np.asarray(lam)[..., None, None] * tr * I
+
+
+def wave_vectors(shape, pixel=1.0):
+    # mgkmc/fft.py:9-20
+    ks = [2 * np.pi * np.fft.fftfreq(n, d=(n * pixel) / n) for n in shape]
+    return np.meshgrid(*ks, indexing="ij")
+
+
+def green_operator(q, lam0, mu0):
+    """Gamma^0_khij(q), spatial axes first (mgkmc/elasticity.py:20-53, :70-105)."""
+    d = len(q)
+    k2 = sum(qi * qi for qi in q)
+    k2s = k2.copy()
+    k2s[(0,) * d] = 1.0
+    A = 1.0 / (4 * mu0)
+    B = (lam0 + mu0) / (mu0 * (lam0 + 2 * mu0))
+    G = np.zeros(q[0].shape + (d, d, d, d))
+    for k in range(d):
+        for h in range(d):
+            for i in range(d):
+                for j in range(d):
+                    t1 = 0.0
+                    if k == i:
+                        t1 = t1 + q[h] * q[j]
+                    if h == i:
+                        t1 = t1 + q[k] * q[j]
+                    if k == j:
+                        t1 = t1 + q[h] * q[i]
+                    if h == j:
+                        t1 = t1 + q[k] * q[i]
+                    G[..., k, h, i, j] = A * t1 / k2s - B * (q[k] * q[h] * q[i] * q[j]) / (k2s * k2s)
+    G[(0,) * d] = 0
+    return G
+
+
+def spectral_solver(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6,
+                    pixel=1.0, plane_mode="plane_strain", eps_init=None,
+                    return_info=False):
+    """LS fixed point in 2D or 3D (dimension from E.ndim).
+
+    Returns (eps, sig, eps_mean, sig_mean) like the reference, plus
+    (iterations, last diff) when ``return_info``.
+    """
+    d = E.ndim
+    axes = tuple(range(d))
+    E_avg = E.mean()
+    nu_avg = nu.mean()
+    if d == 2:
+        lam, mu = lame_2d(E, nu, plane_mode)
+        lam0, mu0 = lame_2d(E_avg, nu_avg, plane_mode)
+    else:
+        lam, mu = lame_3d(E, nu)
+        lam0, mu0 = lame_3d(E_avg, nu_avg)
+    G = green_operator(wave_vectors(E.shape, pixel), lam0, mu0)
+    # initial field (linear_elastic_simulator.py:32-41)
+    if eps_init is not None:
+        eps = eps_init.copy()
+        eps += eps_bar - eps_init.mean(axis=axes)
+    else:
+        eps = np.broadcast_to(eps_bar, E.shape + (d, d)).copy()
+    ep = eps_plastic
+    it_done = 0
+    diff = np.inf
+    sub = "xyz"[:d]
+    for it in range(max_iter):
+        sig = hooke(eps - ep if ep is not None else eps, lam, mu, d)
+        sig0 = hooke(eps, lam0, mu0, d)
+        tau = sig - sig0
+        tau_hat = np.fft.fftn(tau, axes=axes, norm="ortho")
+        et_hat = -np.einsum(f"{sub}khij,{sub}ij->{sub}kh", G, tau_hat)
+        et = np.fft.ifftn(et_hat, axes=axes, norm="ortho").real
+        et -= et.mean(axis=axes)
+        eps_new = eps_bar + et
+        diff = np.linalg.norm(eps_new - eps) / (np.linalg.norm(eps) + 1e-20)
+        eps = eps_new
+        it_done = it + 1
+        if diff < tol:
+            break
+    sig_out = hooke(eps - ep if ep is not None else eps, lam, mu, d)
+    out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
+    if return_info:
+        return out + (it_done, diff)
+    return out
+
+
+def equilibrium_residual(eps, E, nu, eps_bar, eps_plastic=None, pixel=1.0, plane_mode="plane_strain"):
+    """|| eps_bar - Gamma0 * tau(eps) - eps || / ||eps||: the fixed-point defect
+    of the LS equation, which is zero exactly at mechanical equilibrium."""
+    d = E.ndim
+    axes = tuple(range(d))
+    E_avg, nu_avg = E.mean(), nu.mean()
+    if d == 2:
+        lam, mu = lame_2d(E, nu, plane_mode)
+        lam0, mu0 = lame_2d(E_avg, nu_avg, plane_mode)
+    else:
+        lam, mu = lame_3d(E, nu)
+        lam0, mu0 = lame_3d(E_avg, nu_avg)
+    G = green_operator(wave_vectors(E.shape, pixel), lam0, mu0)
+    sub = "xyz"[:d]
+    ep = eps_plastic
+    tau = hooke(eps - ep if ep is not None else eps, lam, mu, d) - hooke(eps, lam0, mu0, d)
+    et = np.fft.ifftn(-np.einsum(f"{sub}khij,{sub}ij->{sub}kh", G,
+                                 np.fft.fftn(tau, axes=axes, norm="ortho")),
+                      axes=axes, norm="ortho").real
+    et -= et.mean(axis=axes)
+    return np.linalg.norm(eps_bar + et - eps) / (np.linalg.norm(eps) + 1e-20)
+
+
+def mixed_bc_solve_2d(E, nu, eps_plastic, strain_mask, target, tol_ls=1e-10, max_iter_ls=500,
+                      tol_macro=1e-4, max_iter_macro=20, pixel=1.0, plane_mode="plane_strain",
+                      eps_bar0=None, eps_warm=None):
+    """Mixed stress/strain macro loop (linear_elastic_simulator.py:176-197,
+    :150-152) around the warm-started LS solve, with an eigenstrain field.
+
+    strain_mask (2,2) bool: True where eps_bar is prescribed; elsewhere the mean
+    stress is driven to ``target``.  ``eps_bar0``/``eps_warm`` carry the macro
+    strain and the warm-start field of a previous load step (:170, :199).  Returns (eps, sig, eps_bar, sig_mean,
+    macro_iters, total_ls_iters)."""
+    E_avg, nu_avg = E.mean(), nu.mean()
+    stress_mask = ~strain_mask
+    eps_bar = np.zeros((2, 2)) if eps_bar0 is None else np.array(eps_bar0, dtype=np.float64)
+    total = 0
+    for it_macro in range(max_iter_macro):
+        eps_bar[strain_mask] = target[strain_mask]
+        eps, sig, epsM, sigM, its, _ = spectral_solver(
+            E, nu, eps_bar, eps_plastic, max_iter=max_iter_ls, tol=tol_ls, pixel=pixel,
+            plane_mode=plane_mode, eps_init=eps_warm, return_info=True)
+        total += its
+        eps_warm = eps
+        err = np.zeros((2, 2))
+        err[stress_mask] = target[stress_mask] - sigM[stress_mask]
+        max_err = np.max(np.abs(err[stress_mask])) if np.any(stress_mask) else 0.0
+        if max_err < tol_macro:
+            return eps, sig, eps_bar.copy(), sigM, it_macro + 1, total
+        d_eps = (err - nu_avg * np.trace(err) * np.eye(2)) / E_avg
+        eps_bar[stress_mask] += d_eps[stress_mask]
+    return eps, sig, eps_bar.copy(), sigM, max_iter_macro, total

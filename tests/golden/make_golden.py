@@ -1,0 +1,245 @@
+"""Generate golden fixtures by running the UNMODIFIED reference mgkmc code.
+
+Run in a container that has the reference checkout (default /root/reference,
+override with MGKMC_REFERENCE):
+
+    python tests/golden/make_golden.py
+
+Each fixture is an .npz of seeded inputs and the reference's outputs for one
+hot-path function.  The reference imports pyfftw/h5py/meshio/matplotlib at
+module level; ``oracle.ref_import`` maps pyfftw onto numpy.fft and stubs the
+I/O modules (none of which the hot path uses).  Numba kernels whose selection
+draws come from numba's private RNG are run through ``.py_func`` under
+``np.random.seed`` so the uniform draw is reproducible and recorded.
+
+Fixtures are small (grids up to 64^2 / 8^3) so the repository stays light; the
+GPU parity tests rerun the oracle at larger sizes.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+
+from oracle.ref_import import import_reference  # noqa: E402
+from mgkmc_b200 import workloads as W  # noqa: E402
+
+import_reference()
+from mgkmc import linear_elastic_simulator as LES  # noqa: E402
+from mgkmc import kmc_simulator_functions as KF  # noqa: E402
+from mgkmc import finite_strain_simulator as FS  # noqa: E402
+from mgkmc.stz import barriers as SB, kmc as SK, cascade as SC  # noqa: E402
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({os.path.getsize(path)/1024:.1f} KB)")
+
+
+def ls2d_fixtures():
+    # config[0]: 64^2 plane strain, 5 % pure-shear eigenstrains, eps_xx = 0.01
+    E, nu, ep, eb = W.ls2d_problem(64, 64, 0)
+    out = {"E": E, "nu": nu, "eps_plastic": ep, "eps_bar": eb}
+    for k in (1, 5):
+        eps, sig, em, sm = LES.spectral_solver_2d(E, nu, eb, ep, max_iter=k, tol=0.0)
+        out[f"eps_it{k}"] = eps
+        out[f"sig_it{k}"] = sig
+    eps, sig, em, sm = LES.spectral_solver_2d(E, nu, eb, ep, max_iter=500, tol=1e-10)
+    out.update(eps_conv=eps, sig_conv=sig, eps_mean=em, sig_mean=sm)
+    save("ls2d_cfg0_64", **out)
+
+    # non-square radix-3 grid, plane stress, asymmetric eps_bar and a warm start
+    rng = np.random.default_rng(11)
+    E, nu = W.ls2d_material(24, 16, rng)
+    ep = W.pure_shear_eigenstrain_2d(24, 16, rng, frac=0.1)
+    ep[3, 5, 0, 1] += 0.01  # one asymmetric eigenstrain entry
+    eb = np.array([[0.004, 0.003], [-0.001, -0.002]])
+    eps_init = 1e-3 * rng.standard_normal((24, 16, 2, 2))
+    out = {"E": E, "nu": nu, "eps_plastic": ep, "eps_bar": eb, "eps_init": eps_init}
+    for k in (1, 3):
+        eps, sig, _, _ = LES.spectral_solver_2d(E, nu, eb, ep, max_iter=k, tol=0.0,
+                                                plane_mode="plane_stress", eps_init=eps_init)
+        out[f"eps_it{k}"] = eps
+        out[f"sig_it{k}"] = sig
+    eps, sig, em, sm = LES.spectral_solver_2d(E, nu, eb, ep, max_iter=300, tol=1e-11,
+                                              plane_mode="plane_stress", eps_init=eps_init)
+    out.update(eps_conv=eps, sig_conv=sig, eps_mean=em, sig_mean=sm)
+    save("ls2d_24x16_pstress", **out)
+
+    # macro mixed-BC driver (no eigenstrain: the reference driver has none)
+    rng = np.random.default_rng(12)
+    E, nu = W.ls2d_material(16, 16, rng)
+    mask = np.array([[True, True], [True, False]])
+    target = np.array([[0.01, 0.0], [0.0, 0.0]])
+    epsM, sigM, eps_l, sig_l = LES.linear_elastic_simulation_2d(
+        E, nu, mask, target, n_steps=2, tol_ls=1e-10, max_iter_ls=300, tol_macro=1e3,
+        max_iter_macro=30, enable_console=False)
+    save("ls2d_macro_16", E=E, nu=nu, mask=mask, target=target, epsM=np.array(epsM),
+         sigM=np.array(sigM), eps_last=eps_l[-1], sig_last=sig_l[-1])
+
+
+def ls3d_fixtures():
+    rng = np.random.default_rng(21)
+    for shape in ((8, 8, 8), (12, 8, 6)):
+        E, nu = W.ls3d_material(*shape, rng)
+        ep = W.pure_shear_eigenstrain_3d(*shape, rng, frac=0.05)
+        eb = np.zeros((3, 3))
+        eb[0, 0] = 0.01
+        eb[1, 2] = eb[2, 1] = 0.002
+        out = {"E": E, "nu": nu, "eps_plastic": ep, "eps_bar": eb}
+        eps, sig, _, _ = LES.spectral_solver_3d(E, nu, eb, ep, max_iter=2, tol=0.0)
+        out.update(eps_it2=eps, sig_it2=sig)
+        eps, sig, em, sm = LES.spectral_solver_3d(E, nu, eb, ep, max_iter=300, tol=1e-10)
+        out.update(eps_conv=eps, sig_conv=sig, eps_mean=em, sig_mean=sm)
+        save("ls3d_%dx%dx%d" % shape, **out)
+
+
+def kmc2d_fixtures():
+    rng = np.random.default_rng(31)
+    nx, ny, M = 16, 12, 8
+    cat, Q0 = W.kmc2d_state(nx, ny, M, rng)
+    cat[2, 3, 1, 0, 1] += 0.02  # one asymmetric mode
+    sig = 1e9 * rng.standard_normal((nx, ny, 2, 2))
+    soft = np.abs(0.2 * rng.standard_normal((nx, ny, 2)))
+    soft[rng.random((nx, ny)) < 0.5, 1] = 0.0
+    t_last = np.where(rng.random((nx, ny)) < 0.3, -np.inf, rng.uniform(0, 1e-3, (nx, ny)))
+    prev = 0.05 * rng.standard_normal((nx, ny, 2, 2))
+    prev[rng.random((nx, ny)) < 0.4] = 0.0
+    out = {"catalog": cat, "Q0": Q0, "sig": sig, "soft_prop": soft, "last_event_time": t_last,
+           "prev_dir": prev}
+    cases = [  # (time, cap, scheme, tau, volume)
+        (1e-3, 0.5, 0, np.inf, 1.0),
+        (2e-3, 0.3, 1, 5e-4, 0.343),
+        (0.0, 0.0, 0, 1e-3, 1.0),
+    ]
+    for c, (t, cap, scheme, tau, vol) in enumerate(cases):
+        Q = np.zeros((nx, ny, M))
+        KF.compute_barrier_2d(Q, Q0, sig, cat, vol, soft, t_last, t, prev, cap, scheme, tau)
+        out[f"Q_case{c}"] = Q
+    out["cases"] = np.array([[t, cap, scheme, tau, vol] for (t, cap, scheme, tau, vol) in cases])
+    Q = out["Q_case1"].copy()
+    Q[0, 0, :3] = -0.1  # a few unstable modes
+    Q[5, 5, 2] = 0.0
+    out["Q_rates"] = Q
+    for T in (300.0, 0.0):
+        for cm in (False, True):
+            rates, idx, total = KF.compute_rates_2d(Q, 1.0, T, 1e13, cascade_mode=cm)
+            tag = f"T{int(T)}_c{int(cm)}"
+            out[f"rates_{tag}"] = rates
+            out[f"indices_{tag}"] = idx
+            out[f"total_{tag}"] = np.array(total)
+    rates, idx, total = KF.compute_rates_2d(Q, 1.0, 300.0, 1e13, cascade_mode=False)
+    draws, sel = [], []
+    for s in range(64):
+        np.random.seed(1000 + s)
+        k = KF.select_event_2d.py_func(rates, total)
+        np.random.seed(1000 + s)
+        u = np.random.random_sample()
+        draws.append(u)
+        sel.append(k)
+    out["sel_u"] = np.array(draws)
+    out["sel_idx"] = np.array(sel)
+    # explicit edge draws: exact partial-sum hits and the top of the range
+    S = np.cumsum(rates)
+    out["sel_total_seq"] = np.array(total)
+    assert S[-1] == total
+    # flips
+    ep = 0.01 * rng.standard_normal((nx, ny, 2, 2))
+    sp = np.abs(0.1 * rng.standard_normal((nx, ny, 2)))
+    tl = rng.uniform(0, 1, (nx, ny))
+    flips = [(3, 4, 2, 0.5, 10.0, 30.0, 2.0, 0.0), (0, 11, 7, 0.7, 10.0, 30.0, 0.3, 0.25),
+             (15, 0, 0, 0.9, 5.0, 0.0, 0.0, 0.5)]
+    out["flip_in_eps_p"], out["flip_in_soft"], out["flip_in_tlast"] = ep.copy(), sp.copy(), tl.copy()
+    for (x, y, m, t, jp, jt, gmax, jn) in flips:
+        KF.apply_flip_soa_2d.py_func(ep, sp, tl, cat, x, y, m, t, jp, jt, gmax, jn)
+    out["flips"] = np.array(flips)
+    out["flip_out_eps_p"], out["flip_out_soft"], out["flip_out_tlast"] = ep, sp, tl
+    save("kmc2d_16x12", **out)
+
+
+def kmc3d_fixtures():
+    rng = np.random.default_rng(41)
+    nx, ny, nz, M = 6, 5, 4, 6
+    cat = 0.05 * rng.standard_normal((nx, ny, nz, M, 3, 3))
+    Q0 = np.clip(rng.normal(1.0, 0.15, (nx, ny, nz, M)), 0.3, None)
+    sig = 1e9 * rng.standard_normal((nx, ny, nz, 3, 3))
+    soft = np.abs(0.2 * rng.standard_normal((nx, ny, nz, 4)))
+    t_last = np.where(rng.random((nx, ny, nz)) < 0.3, -np.inf, rng.uniform(0, 1e-3, (nx, ny, nz)))
+    prev = 0.05 * rng.standard_normal((nx, ny, nz, 3, 3))
+    out = {"catalog": cat, "Q0": Q0, "sig": sig, "soft_prop": soft, "last_event_time": t_last,
+           "prev_dir": prev}
+    Q = np.zeros((nx, ny, nz, M))
+    SB.compute_barrier(Q, Q0, sig, cat, 1.0, soft, t_last, 1e-3, prev, 0.5, 1, 5e-4)
+    out["Q"] = Q.copy()
+    Q2 = np.zeros((nx, ny, nz, M))
+    SB.compute_barrier(Q2, Q0, sig, cat, 1.0, soft, t_last, 1e-3, prev, 0.5, 0, np.inf)
+    out["Q_iso"] = Q2
+    rates, idx, total = SK.compute_rates(Q, 1.0, 300.0, 1e13, cascade_mode=False)
+    out.update(rates=rates, indices=idx, total=np.array(total))
+    draws, sel = [], []
+    for s in range(32):
+        np.random.seed(2000 + s)
+        k = SK.select_event.py_func(rates, total)
+        np.random.seed(2000 + s)
+        draws.append(np.random.random_sample())
+        sel.append(k)
+    out["sel_u"], out["sel_idx"] = np.array(draws), np.array(sel)
+    ep = 0.01 * rng.standard_normal((nx, ny, nz, 3, 3))
+    sp = np.abs(0.1 * rng.standard_normal((nx, ny, nz, 4)))
+    tl = rng.uniform(0, 1, (nx, ny, nz))
+    out["flip_in_eps_p"], out["flip_in_soft"], out["flip_in_tlast"] = ep.copy(), sp.copy(), tl.copy()
+    flips = [(1, 2, 3, 4, 0.5, 10.0, 30.0, 2.0, 0.2), (5, 0, 0, 0, 0.6, 10.0, 30.0, 0.3, 0.0)]
+    for (x, y, z, m, t, jp, jt, gmax, jn) in flips:
+        SC.apply_flip_soa.py_func(ep, None, sp, tl, cat, x, y, z, m, t, jp, jt, gmax, jn)
+    out["flips"] = np.array(flips)
+    out["flip_out_eps_p"], out["flip_out_soft"], out["flip_out_tlast"] = ep, sp, tl
+    save("kmc3d_6x5x4", **out)
+
+
+def fs3d_fixtures():
+    """One mixed-BC load step of the reference Newton-Krylov solver (SVK + F_p)."""
+    rng = np.random.default_rng(51)
+    nx = ny = nz = 6
+    E, nu, Fp = W.fs3d_material(nx, ny, nz, rng, fp_frac=0.1)
+    Ghat4 = FS.build_ghat4_3d(nx, ny, nz, nx * 1.0, ny * 1.0, nz * 1.0)
+    I2, I4, I4rt, I4s, II = FS._make_identity_tensors_3d(nx, ny, nz)
+    C4 = FS.build_C4_3d(E, nu, I4s, II)
+    F0 = np.einsum("ij,xyz->ijxyz", np.eye(3), np.ones((nx, ny, nz)))
+    out = {"E": E, "nu": nu, "Fp": Fp}
+    F_bar, F_mask, P_tgt, P_mask = FS.build_finite_strain_bc_3d(
+        (0, 0), 0.01, {(1, 1): 0.0, (2, 2): 0.0}, ndim=3)
+    F, P, Sig, K4, Fb = FS.finite_strain_solver_step_3d(
+        F0, F_bar, Ghat4, C4, I2, I4, I4rt, Fp=Fp, driving_component=(0, 0),
+        P_target=P_tgt, P_mask=P_mask, E_avg=E.mean(), nu_avg=nu.mean(),
+        tol_NW=1e-10, tol_CG=1e-10, max_NW=30, tol_macro=1e3, max_iter_macro=30,
+        enable_console=False, model_type="svk", solver="newton_cg")
+    out.update(F_bar_in=F_bar, P_mask=P_mask, F=F, P=P, Sig=Sig, F_bar_out=Fb)
+    # constitutive law alone (SVK, with F_p) at a perturbed F
+    Ft = F0 + 0.01 * rng.standard_normal(F0.shape)
+    Pc, K4c = FS.constitutive_hyperelastic_3d(Ft, C4, I2, I4, I4rt, Fp=Fp, model_type="svk")
+    dF = rng.standard_normal(F0.shape)
+    KdF = np.einsum("ijxyz->jixyz", np.einsum("ijklxyz,lkxyz->ijxyz", K4c,
+                                              np.einsum("ijxyz->jixyz", dF)))
+    GKdF = FS._project_3d(KdF, Ghat4)
+    out.update(F_trial=Ft, P_trial=Pc, dF=dF, KdF=KdF, GKdF=GKdF)
+    save("fs3d_svk_6", **out)
+
+    # 2D plane-strain Neo-Hookean law (the form restated in 3D by the oracle)
+    nx2 = ny2 = 5
+    E2, nu2 = W.ls2d_material(nx2, ny2, rng)
+    I2b, I4b, I4rtb, I4sb, IIb = FS._make_identity_tensors_2d(nx2, ny2)
+    C42 = FS.build_C4_2d(E2, nu2, I4sb, IIb)
+    F2 = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx2, ny2))) + 0.02 * rng.standard_normal((2, 2, nx2, ny2))
+    P2, K42, _ = FS.constitutive_hyperelastic_2d(F2, C42, I2b, I4b, I4rtb, model_type="neo_hookean")
+    save("fs2d_neohookean_5", E=E2, nu=nu2, F=F2, P=P2, K4=K42)
+
+
+if __name__ == "__main__":
+    ls2d_fixtures()
+    ls3d_fixtures()
+    kmc2d_fixtures()
+    kmc3d_fixtures()
+    fs3d_fixtures()

@@ -1,0 +1,138 @@
+"""The CPU oracle restatements reproduce the unmodified reference's outputs
+(golden fixtures made by tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+from oracle import kmc as OK
+from oracle import ls as OL
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("k", [1, 5])
+def test_ls2d_fixed_iterations(golden, k):
+    g = golden("ls2d_cfg0_64")
+    eps, sig, _, _ = OL.spectral_solver(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=k, tol=0.0)
+    assert rel(eps, g[f"eps_it{k}"]) < 1e-12
+    assert rel(sig, g[f"sig_it{k}"]) < 1e-12
+
+
+def test_ls2d_converged(golden):
+    g = golden("ls2d_cfg0_64")
+    eps, sig, em, sm = OL.spectral_solver(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-10)
+    assert rel(eps, g["eps_conv"]) < 1e-12
+    assert rel(sig, g["sig_conv"]) < 1e-12
+    assert rel(sm, g["sig_mean"]) < 1e-12
+
+
+def test_ls2d_plane_stress_warm_start_asymmetric(golden):
+    g = golden("ls2d_24x16_pstress")
+    for k in (1, 3):
+        eps, sig, _, _ = OL.spectral_solver(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=k,
+                                            tol=0.0, plane_mode="plane_stress", eps_init=g["eps_init"])
+        assert rel(eps, g[f"eps_it{k}"]) < 1e-12
+        assert rel(sig, g[f"sig_it{k}"]) < 1e-12
+    eps, sig, _, _ = OL.spectral_solver(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=300,
+                                        tol=1e-11, plane_mode="plane_stress", eps_init=g["eps_init"])
+    assert rel(eps, g["eps_conv"]) < 1e-12
+
+
+def test_ls2d_macro_loop(golden):
+    g = golden("ls2d_macro_16")
+    E, nu, mask, target = g["E"], g["nu"], g["mask"], g["target"]
+    # the reference driver ramps targets over n_steps=2 with warm starts
+    eps_warm, eps_bar = None, np.zeros((2, 2))
+    for s in range(3):
+        t = target * (s / 2)
+        eps, sig, eps_bar, sigM, _, _ = OL.mixed_bc_solve_2d(
+            E, nu, None, mask, t, tol_ls=1e-10, max_iter_ls=300, tol_macro=1e3, max_iter_macro=30,
+            eps_bar0=eps_bar, eps_warm=eps_warm)
+        eps_warm = eps
+        scale = np.max(np.abs(g["sigM"]))
+        assert np.max(np.abs(sigM - g["sigM"][s])) < 1e-9 * scale
+    assert rel(eps, g["eps_last"]) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["ls3d_8x8x8", "ls3d_12x8x6"])
+def test_ls3d(golden, name):
+    g = golden(name)
+    eps, sig, _, _ = OL.spectral_solver(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=2, tol=0.0)
+    assert rel(eps, g["eps_it2"]) < 1e-12
+    assert rel(sig, g["sig_it2"]) < 1e-12
+    eps, sig, _, _ = OL.spectral_solver(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=300, tol=1e-10)
+    assert rel(eps, g["eps_conv"]) < 1e-12
+    assert rel(sig, g["sig_conv"]) < 1e-12
+
+
+def test_kmc2d_barrier(golden):
+    g = golden("kmc2d_16x12")
+    for c, (t, cap, scheme, tau, vol) in enumerate(g["cases"]):
+        Q = np.zeros_like(g["Q0"])
+        OK.compute_barrier(Q, g["Q0"], g["sig"], g["catalog"], vol, g["soft_prop"], g["last_event_time"],
+                           t, g["prev_dir"], cap, int(scheme), tau)
+        np.testing.assert_allclose(Q, g[f"Q_case{c}"], rtol=0, atol=1e-14)
+
+
+def test_barrier_known_answer():
+    # tests/test_barrier_physics.py:13-47 of the reference: 1 GPa shear, gamma 0.1
+    sig = np.zeros((1, 1, 1, 3, 3)); sig[0, 0, 0, 0, 1] = sig[0, 0, 0, 1, 0] = 1e9
+    cat = np.zeros((1, 1, 1, 1, 3, 3)); cat[0, 0, 0, 0, 0, 1] = cat[0, 0, 0, 0, 1, 0] = 0.1
+    Q = np.zeros((1, 1, 1, 1))
+    OK.compute_barrier(Q, np.ones((1, 1, 1, 1)), sig, cat, 1.0, np.zeros((1, 1, 1, 4)),
+                       np.full((1, 1, 1), -np.inf), 0.0, np.zeros((1, 1, 1, 3, 3)), 2.0, 0, np.inf)
+    assert abs(Q[0, 0, 0, 0] - (1.0 - 0.6241509)) < 1e-4
+
+
+def test_kmc2d_rates_exact(golden):
+    g = golden("kmc2d_16x12")
+    Q = g["Q_rates"]
+    for T in (300.0, 0.0):
+        for cm in (False, True):
+            tag = f"T{int(T)}_c{int(cm)}"
+            r, idx, total = OK.compute_rates(Q, 1.0, T, 1e13, cascade_mode=cm)
+            np.testing.assert_array_equal(idx, g[f"indices_{tag}"])
+            np.testing.assert_allclose(r, g[f"rates_{tag}"], rtol=1e-15, atol=0)  # exp() differs by <= 1 ulp across libms
+            # total is the sequential sum of the reference's own rates: bit-exact
+            assert np.add.accumulate(g[f"rates_{tag}"])[-1] == g[f"total_{tag}"]
+
+
+def test_kmc2d_select_bit_exact(golden):
+    g = golden("kmc2d_16x12")
+    rates, total = g["rates_T300_c0"], float(g["total_T300_c0"])
+    for u, k in zip(g["sel_u"], g["sel_idx"]):
+        assert OK.select_event(rates, total, u) == k
+        assert OK.select_event_loop(rates, total, u) == k
+
+
+def test_kmc2d_flip_bit_exact(golden):
+    g = golden("kmc2d_16x12")
+    ep, sp, tl = g["flip_in_eps_p"].copy(), g["flip_in_soft"].copy(), g["flip_in_tlast"].copy()
+    for (x, y, m, t, jp, jt, gmax, jn) in g["flips"]:
+        OK.apply_flip_2d(ep, sp, tl, g["catalog"], int(x), int(y), int(m), t, jp, jt, gmax, jn)
+    np.testing.assert_array_equal(ep, g["flip_out_eps_p"])
+    np.testing.assert_array_equal(sp, g["flip_out_soft"])
+    np.testing.assert_array_equal(tl, g["flip_out_tlast"])
+
+
+def test_kmc3d(golden):
+    g = golden("kmc3d_6x5x4")
+    Q = np.zeros_like(g["Q0"])
+    OK.compute_barrier(Q, g["Q0"], g["sig"], g["catalog"], 1.0, g["soft_prop"], g["last_event_time"],
+                       1e-3, g["prev_dir"], 0.5, 1, 5e-4)
+    np.testing.assert_allclose(Q, g["Q"], rtol=0, atol=1e-14)
+    Q2 = np.zeros_like(g["Q0"])
+    OK.compute_barrier(Q2, g["Q0"], g["sig"], g["catalog"], 1.0, g["soft_prop"], g["last_event_time"],
+                       1e-3, g["prev_dir"], 0.5, 0, np.inf)
+    np.testing.assert_allclose(Q2, g["Q_iso"], rtol=0, atol=1e-14)
+    r, idx, total = OK.compute_rates(g["Q"], 1.0, 300.0, 1e13, cascade_mode=False)
+    np.testing.assert_array_equal(idx, g["indices"])
+    for u, k in zip(g["sel_u"], g["sel_idx"]):
+        assert OK.select_event(g["rates"], float(g["total"]), u) == k
+    ep, sp, tl = g["flip_in_eps_p"].copy(), g["flip_in_soft"].copy(), g["flip_in_tlast"].copy()
+    for (x, y, z, m, t, jp, jt, gmax, jn) in g["flips"]:
+        OK.apply_flip_3d(ep, sp, tl, g["catalog"], int(x), int(y), int(z), int(m), t, jp, jt, gmax, jn)
+    np.testing.assert_array_equal(ep, g["flip_out_eps_p"])
+    np.testing.assert_array_equal(sp, g["flip_out_soft"])
+    np.testing.assert_array_equal(tl, g["flip_out_tlast"])
