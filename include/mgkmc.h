@@ -1,0 +1,140 @@
+/*
+ * mgkmc B200 C-ABI: the drop-in boundary for mgkmc's mechanical-equilibrium
+ * hot path.  Plain C types only (pointers, sizes, scalars); every device
+ * pointer is a CUDA device address owned by the caller (for example a
+ * torch.Tensor's data_ptr()), every function returns an mgk_status and takes
+ * the CUDA stream the work is ordered on.  No call blocks indefinitely or
+ * traps; device-side loops are bounded by iteration caps.
+ *
+ * Array layouts are the reference's (C order, float64 unless noted):
+ *   small strain 2D   E, nu (nx,ny);  eps, sig, eps_plastic (nx,ny,2,2)
+ *   small strain 3D   E, nu (nx,ny,nz); eps, sig, eps_plastic (nx,ny,nz,3,3)
+ *   KMC 2D            Q, Q0 (nx,ny,M); catalog (nx,ny,M,2,2); soft_prop (nx,ny,2)
+ *   KMC 3D            Q, Q0 (nx,ny,nz,M); catalog (nx,ny,nz,M,3,3); soft_prop (nx,ny,nz,4)
+ *
+ * Reference interfaces each entry point replaces are cited as file:line within
+ * the mgkmc project.
+ */
+#ifndef MGKMC_B200_H
+#define MGKMC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MGK_API __attribute__((visibility("default")))
+#else
+#define MGK_API
+#endif
+
+typedef struct CUstream_st* mgk_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  MGK_OK = 0,
+  MGK_NOT_CONVERGED = 1, /* iteration cap reached (the reference returns silently) */
+  MGK_NONFINITE = 2,     /* NaN/Inf in a field or a norm */
+  MGK_BAD_ARG = 3,
+  MGK_OOM = 4,
+  MGK_TIMEOUT = 5,
+  MGK_CUDA_ERROR = 6
+} mgk_status;
+
+enum { MGK_PLANE_STRAIN = 0, MGK_PLANE_STRESS = 1 };
+enum { MGK_FP64 = 0, MGK_FP32 = 1 };
+
+/* ------------------------------------------------------------- library --- */
+MGK_API int mgk_version(void);
+MGK_API const char* mgk_status_string(int status);
+/* Text of the last error raised on the calling host thread. */
+MGK_API const char* mgk_last_error(void);
+/* 1 if n = 2^a 3^b with 4 <= n <= 4096 (grid sizes the FFT supports). */
+MGK_API int mgk_fft_supported(int n);
+
+/* ------------------------------------------- 2D small-strain LS solver --- */
+/* Replaces mgkmc/linear_elastic_simulator.py:12-88 spectral_solver_2d (and the
+ * Green operator build of mgkmc/elasticity.py:20-53, applied on the fly). */
+typedef struct mgk_ls2d_plan* mgk_ls2d_t;
+
+typedef struct {
+  int iterations;       /* LS iterations performed */
+  int status;           /* MGK_OK or MGK_NOT_CONVERGED */
+  double final_diff;    /* ||eps_new - eps|| / (||eps|| + 1e-20) of the last iteration */
+  double eps_mean[4];   /* eps.mean(axis=(0,1)) as (xx, xy, yx, yy) */
+  double sig_mean[4];   /* sig_out.mean(axis=(0,1)) */
+} mgk_ls_info;
+
+/* pixel: voxel size (only enters the wave vectors, where it cancels). */
+MGK_API int mgk_ls2d_create(int nx, int ny, int plane_mode, int precision, mgk_ls2d_t* out);
+MGK_API int mgk_ls2d_destroy(mgk_ls2d_t plan);
+/* Moduli fields E, nu (nx,ny) and the eigenstrain eps_plastic (nx,ny,2,2) or
+ * NULL (= zero).  Computes mu, lambda per voxel and the reference medium
+ * C0 = (mean E, mean nu) on the device (linear_elastic_simulator.py:22-23). */
+MGK_API int mgk_ls2d_set_material(mgk_ls2d_t plan, const double* E, const double* nu,
+                          const double* eps_plastic, mgk_stream_t stream);
+/* Update only the eigenstrain field (KMC flips). */
+MGK_API int mgk_ls2d_set_eigenstrain(mgk_ls2d_t plan, const double* eps_plastic, mgk_stream_t stream);
+/* One LS solve.  eps_bar: host (2,2).  eps_init: device (nx,ny,2,2) warm start
+ * or NULL (uniform eps_bar start, :32-41).  eps_out, sig_out: device
+ * (nx,ny,2,2).  info: host, may be NULL; when given the call synchronises the
+ * stream to fill it.  Convergence is tested on the device after every
+ * iteration; the loop runs as one CUDA graph with a device-driven while node. */
+MGK_API int mgk_ls2d_solve(mgk_ls2d_t plan, const double* eps_bar, const double* eps_init,
+                   double* eps_out, double* sig_out, int max_iter, double tol,
+                   mgk_ls_info* info, mgk_stream_t stream);
+
+/* Timing hook: runs `reps` LS iterations (tolerance 0) and returns the mean
+ * duration of the row kernel (C2R+update+tau+R2C along y) and of the column
+ * kernel (FFT+Gamma+IFFT along x), timed with CUDA events on `stream`.
+ * Leaves the plan's iterate in an unspecified state. */
+MGK_API int mgk_ls2d_profile(mgk_ls2d_t plan, const double* eps_bar, int reps, float* row_ms, float* col_ms,
+                             mgk_stream_t stream);
+
+/* ------------------------------------------------------ 2D STZ / KMC --- */
+/* mgkmc/kmc_simulator_functions.py:100-160 compute_barrier_2d (in place on Q).
+ * scheme: 0 isotropic, 1 directional.  tau: +inf for no decay. */
+MGK_API int mgk_kmc2d_barrier(int nx, int ny, int M, double* Q, const double* Q0, const double* sig,
+                      const double* catalog, double volume, const double* soft_prop,
+                      const double* last_event_time, double current_time,
+                      const double* prev_strain_dir, double softening_cap, int scheme, double tau,
+                      mgk_stream_t stream);
+
+/* mgkmc/kmc_simulator_functions.py:5-56 compute_rates_2d / _compute_rates_2d_jit.
+ * temperature: device (nx,ny) field or NULL to use temperature_scalar.
+ * Writes rates[count], indices[count] (int64) and the prefix array
+ * prefix[count] of the sequential left-to-right FP64 running sum (prefix[count-1]
+ * is the reference's total_rate, bit for bit).  count and total land in the
+ * device scalars *d_count (int64) and *d_total.  rates/indices/prefix need
+ * nx*ny*M entries.  work: device scratch of mgk_kmc_rates_work_bytes(). */
+MGK_API int64_t mgk_kmc_rates_work_bytes(int64_t n_modes);
+MGK_API int mgk_kmc2d_rates(int nx, int ny, int M, const double* Q, double volume,
+                    const double* temperature, double temperature_scalar, double nu0,
+                    int cascade_mode, double* rates, int64_t* indices, double* prefix,
+                    int64_t* d_count, double* d_total, void* work, mgk_stream_t stream);
+
+/* Sequential left-to-right running sum of n given rates into prefix[n]; the
+ * total (prefix[n-1], 0 if n == 0) lands in *d_total and n in *d_count.  This
+ * is the total_rate chain of kmc_simulator_functions.py:36-55, for callers
+ * that hold a rates array of their own (select_event_2d(rates, total)). */
+MGK_API int mgk_kmc_prefix(const double* rates, int64_t n, double* prefix, int64_t* d_count,
+                           double* d_total, mgk_stream_t stream);
+
+/* mgkmc/kmc_simulator_functions.py:58-67 select_event_2d with an explicit
+ * uniform draw u in [0,1): r = u * total, result = first i with prefix[i] >= r
+ * (count-1 if none, -1 if total <= 0).  Bit-exact with the reference given the
+ * same rates and draw.  Result in *d_index (device int64). */
+MGK_API int mgk_kmc_select(const double* prefix, const int64_t* d_count, const double* d_total, double u,
+                   int64_t* d_index, mgk_stream_t stream);
+
+/* mgkmc/kmc_simulator_functions.py:183-218 apply_flip_soa_2d (in place). */
+MGK_API int mgk_kmc2d_flip(int nx, int ny, int M, double* eps_plastic, double* soft_prop,
+                   double* last_event_time, const double* catalog, int x, int y, int m,
+                   double current_time, double jp, double jt, double g_max, double jn_frac,
+                   mgk_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGKMC_B200_H */

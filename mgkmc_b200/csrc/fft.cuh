@@ -1,0 +1,128 @@
+// Shared-memory Stockham FFT for line lengths n = 2^a 3^b (4 <= n <= 4096).
+//
+// A CTA transforms a batch of complex lines that sit in shared memory, one
+// radix-R pass at a time (R in {2, 3, 4, 8}), ping-ponging between two shared
+// buffers.  Pass p with stride Ns (product of the earlier radices) maps
+// butterfly j of a line as
+//     in  : a[j + r*n/R],            r = 0..R-1
+//     tw  : W_{Ns*R}^{r*(j mod Ns)}  (table W_n^m = exp(-2 pi i m / n))
+//     out : b[(j - j mod Ns)*R + j mod Ns + r*Ns]
+// which leaves the result in natural order (self-sorting Stockham form).
+// SIGN = -1 is the forward kernel exp(-2 pi i jk/n), SIGN = +1 the inverse
+// (unnormalised).  Twiddles are read from a per-length table in global
+// memory (L1-resident), computed once on the host in double precision.
+#pragma once
+#include "common.cuh"
+
+namespace mgk {
+
+struct FftLen {
+  int n;
+  int npass;
+  int radix[8];
+  const void* tw;  // n complex (T) entries, W_n^m
+};
+
+// host: radix schedule for n = 2^a 3^b; returns false if n is unsupported
+bool fft_schedule(int n, FftLen* f);
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft2(C* v) {
+  C a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
+  C a0 = cadd(v0, v2), a1 = csub(v0, v2);
+  C a2 = cadd(v1, v3), a3 = cmul_i<SIGN>(csub(v1, v3));
+  v0 = cadd(a0, a2);
+  v2 = csub(a0, a2);
+  v1 = cadd(a1, a3);
+  v3 = csub(a1, a3);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* v) {
+  using R = decltype(C::x);
+  const R h = R(0.70710678118654752440084436210485);
+  dft4<SIGN>(v[0], v[2], v[4], v[6]);
+  dft4<SIGN>(v[1], v[3], v[5], v[7]);
+  // odd half times W8^k, W8 = exp(SIGN * 2 pi i / 8)
+  C o1 = mk<C>(h * (v[3].x - SIGN * v[3].y), h * (v[3].y + SIGN * v[3].x));
+  C o2 = cmul_i<SIGN>(v[5]);
+  C o3 = mk<C>(-h * (v[7].x + SIGN * v[7].y), h * (SIGN * v[7].x - v[7].y));
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1];
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* v) {
+  using R = decltype(C::x);
+  const R s3 = R(0.86602540378443864676372317075294);
+  C s = cadd(v[1], v[2]);
+  C d = csub(v[1], v[2]);
+  C m = mk<C>(v[0].x - R(0.5) * s.x, v[0].y - R(0.5) * s.y);
+  C t = cmul_i<SIGN>(mk<C>(s3 * d.x, s3 * d.y));
+  v[0] = cadd(v[0], s);
+  v[1] = cadd(m, t);
+  v[2] = csub(m, t);
+}
+
+template <int R, int SIGN, typename C>
+__device__ __forceinline__ void stockham_bfly(const C* __restrict__ src, C* __restrict__ dst, int j,
+                                              int nb, int Ns, int twstride, const C* __restrict__ tw) {
+  C v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+  const int k = j % Ns;
+  if (k != 0) {
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      C w = __ldg(&tw[r * k * twstride]);
+      if (SIGN > 0) w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+  }
+  if (R == 2) dft2<SIGN>(v);
+  else if (R == 3) dft3<SIGN>(v);
+  else if (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  else dft8<SIGN>(v);
+  const int base = (j - k) * R + k;
+#pragma unroll
+  for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+}
+
+// Transform `nlines` lines of length f.n held at a[line*ld ...]; b is scratch
+// of the same shape.  All threads of the CTA must call.  Returns the buffer
+// (a or b) that holds the result.  Ends with a __syncthreads().
+template <int SIGN, typename C>
+__device__ C* fft_lines(C* a, C* b, int nlines, int ld, const FftLen& f) {
+  const C* tw = reinterpret_cast<const C*>(f.tw);
+  const int n = f.n;
+  int Ns = 1;
+  for (int p = 0; p < f.npass; ++p) {
+    const int R = f.radix[p];
+    const int nb = n / R;
+    const int total = nlines * nb;
+    const int twstride = n / (Ns * R);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int line = t / nb;
+      const int j = t - line * nb;
+      const C* s = a + line * ld;
+      C* d = b + line * ld;
+      switch (R) {
+        case 8: stockham_bfly<8, SIGN>(s, d, j, nb, Ns, twstride, tw); break;
+        case 4: stockham_bfly<4, SIGN>(s, d, j, nb, Ns, twstride, tw); break;
+        case 3: stockham_bfly<3, SIGN>(s, d, j, nb, Ns, twstride, tw); break;
+        default: stockham_bfly<2, SIGN>(s, d, j, nb, Ns, twstride, tw); break;
+      }
+    }
+    __syncthreads();
+    C* t = a; a = b; b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+}  // namespace mgk

@@ -1,0 +1,383 @@
+// Per-voxel STZ barrier / Arrhenius rate kernels and KMC event selection.
+//
+// Restates mgkmc/kmc_simulator_functions.py (2D) and mgkmc/stz/{barriers,
+// kmc,cascade}.py (3D).  Floating-point operation order follows the
+// reference where it decides bits: contractions are left-to-right sums from
+// 0.0 over (i, j) in C order, products are rounded separately (no FMA
+// contraction, mirroring the LLVM code numba emits), and the total rate is
+// the sequential left-to-right FP64 running sum in (x, y[, z], m) order.
+//
+// The sequential sum is a dependent chain by definition.  It runs in one
+// CTA: warp 0 lane 0 walks a shared-memory chunk while the other warps load
+// the next chunk and write back the previous one (3 rotating buffers), so
+// the chain sees shared-memory latency only.  The prefix array it writes is
+// monotone (rates >= 0), so selection is a two-level parallel search for the
+// first prefix >= u * total instead of the reference's linear rescan; both
+// return the same index for the same rates and draw.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace mgk {
+
+#define KB_EV 8.617e-5
+#define GPA_NM3_TO_EV 6.241509
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// softening base g (kmc_simulator_functions.py:114-128)
+__device__ __forceinline__ double soft_base(double g_p, double g_t, double t_last, double t, double cap,
+                                            double tau) {
+  double g_t_curr = 0.0;
+  if (g_t > 0) {
+    if (isinf(tau) && tau > 0) g_t_curr = g_t;
+    else if (t_last == -INFINITY) g_t_curr = 0.0;
+    else {
+      double dt = sub(t, t_last);
+      if (dt < 0) dt = 0;
+      g_t_curr = mul(g_t, exp(-__ddiv_rn(dt, tau)));
+    }
+  }
+  double g = add(g_p, g_t_curr);
+  if (cap > 0 && g > cap) g = cap;
+  return g;
+}
+
+// One thread per (voxel, mode).  D = 2 or 3 (tensor dimension); SP = soft_prop
+// stride (2 in 2D, 4 in 3D).
+template <int D, int SP>
+__global__ void barrier_kernel(long long nvox, int M, double* __restrict__ Q, const double* __restrict__ Q0,
+                               const double* __restrict__ sig, const double* __restrict__ cat, double volume,
+                               const double* __restrict__ soft, const double* __restrict__ t_last, double t,
+                               const double* __restrict__ prev, double cap, int scheme, double tau) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nvox * M) return;
+  const long long v = i / M;
+  const double g_base = soft_base(soft[SP * v], soft[SP * v + 1], t_last[v], t, cap, tau);
+  const double* c = cat + i * D * D;
+  const double* s = sig + v * D * D;
+  double modifier = 1.0;
+  if (scheme == 1) {
+    const double* p = prev + v * D * D;
+    double dot = 0.0, nm = 0.0, np = 0.0;
+#pragma unroll
+    for (int q = 0; q < D * D; ++q) {
+      const double a = c[q], b = p[q];
+      dot = add(dot, mul(a, b));
+      nm = add(nm, mul(a, a));
+      np = add(np, mul(b, b));
+    }
+    const double norm_p = sqrt(np), norm_m = sqrt(nm);
+    if (norm_p < 1e-12 || norm_m < 1e-12) modifier = 1.0;
+    else {
+      const double ct = __ddiv_rn(dot, mul(norm_m, norm_p));
+      const double o = add(1.0, ct);
+      modifier = __ddiv_rn(mul(o, o), 4.0);
+    }
+  }
+  const double g_eff = mul(modifier, g_base);
+  double w = 0.0;
+#pragma unroll
+  for (int q = 0; q < D * D; ++q) w = add(w, mul(s[q], c[q]));
+  const double w_val = mul(mul(mul(0.5, volume), __ddiv_rn(w, 1e9)), GPA_NM3_TO_EV);
+  Q[i] = sub(mul(Q0[i], exp(-g_eff)), w_val);
+}
+
+// rate of one mode (kmc_simulator_functions.py:41-48)
+__device__ __forceinline__ double mode_rate(double q, double beta, double vnu) {
+  return q <= 0 ? vnu : mul(vnu, exp(-mul(q, beta)));
+}
+
+__device__ __forceinline__ double beta_of(double T) { return T > 0.0 ? __ddiv_rn(1.0, mul(KB_EV, T)) : INFINITY; }
+
+// Non-compacting rates (KMC mode: every mode is an event).
+__global__ void rates_full_kernel(long long nvox, int M, const double* __restrict__ Q, double vnu,
+                                  const double* __restrict__ T, double Ts, double* __restrict__ rates,
+                                  long long* __restrict__ indices, long long* __restrict__ d_count) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i == 0) *d_count = nvox * M;
+  if (i >= nvox * M) return;
+  const long long v = i / M;
+  const double beta = beta_of(T ? T[v] : Ts);
+  rates[i] = mode_rate(Q[i], beta, vnu);
+  if (indices) indices[i] = i;
+}
+
+// Compacting rates (cascade mode: only q > 0), 3 passes: block counts,
+// exclusive scan of the counts, ordered scatter.
+__global__ void rates_count_kernel(long long n, const double* __restrict__ Q, int* __restrict__ bcount) {
+  __shared__ int red[32];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int f = (i < n && Q[i] > 0) ? 1 : 0;
+  int s = block_sum(f, red);
+  if (threadIdx.x == 0) bcount[blockIdx.x] = s;
+}
+
+__global__ void scan_counts_kernel(int nb, int* __restrict__ bcount, long long* __restrict__ d_count) {
+  // single CTA exclusive scan over nb block counts (in place)
+  __shared__ long long carry;
+  __shared__ int wsum[32];
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    int v = i < nb ? bcount[i] : 0;
+    // inclusive warp scan
+    int x = v;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    const int incl = x + (wid > 0 ? wsum[wid - 1] : 0);
+    if (i < nb) bcount[i] = (int)(carry + incl - v);
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *d_count = carry;
+}
+
+__global__ void rates_scatter_kernel(long long nvox, int M, const double* __restrict__ Q, double vnu,
+                                     const double* __restrict__ T, double Ts, const int* __restrict__ boff,
+                                     double* __restrict__ rates, long long* __restrict__ indices) {
+  __shared__ int wsum[32];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = nvox * M;
+  const double q = i < n ? Q[i] : 0.0;
+  const int f = (i < n && q > 0) ? 1 : 0;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = f;
+  for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  if (!f) return;
+  const long long pos = (long long)boff[blockIdx.x] + x - 1 + (wid > 0 ? wsum[wid - 1] : 0);
+  const double beta = beta_of(T ? T[i / M] : Ts);
+  rates[pos] = mode_rate(q, beta, vnu);
+  indices[pos] = i;
+}
+
+// Sequential left-to-right running sum (the reference's total_rate chain).
+#define SEQ_CHUNK 2048
+__global__ void __launch_bounds__(256) seq_prefix_kernel(const double* __restrict__ rates, long long n_fixed,
+                                                         const long long* __restrict__ d_count,
+                                                         double* __restrict__ prefix, double* __restrict__ d_total) {
+  __shared__ double buf[3][SEQ_CHUNK];
+  const long long n = d_count ? *d_count : n_fixed;
+  const long long nchunk = (n + SEQ_CHUNK - 1) / SEQ_CHUNK;
+  const int tid = threadIdx.x;
+  const int helpers = blockDim.x - 32;  // warps 1.. load and store
+  double run = 0.0;
+  // preload chunk 0
+  for (int j = tid; j < SEQ_CHUNK; j += blockDim.x) buf[0][j] = j < n ? rates[j] : 0.0;
+  __syncthreads();
+  for (long long c = 0; c <= nchunk; ++c) {
+    const int cur = (int)(c % 3), nxt = (int)((c + 1) % 3), prv = (int)((c + 2) % 3);
+    if (tid < 32) {
+      if (tid == 0 && c < nchunk) {
+        const long long base = c * SEQ_CHUNK;
+        const int len = (int)min((long long)SEQ_CHUNK, n - base);
+        double* b = buf[cur];
+        int j = 0;
+        for (; j + 8 <= len; j += 8) {
+          double v0 = b[j], v1 = b[j + 1], v2 = b[j + 2], v3 = b[j + 3];
+          double v4 = b[j + 4], v5 = b[j + 5], v6 = b[j + 6], v7 = b[j + 7];
+          run = add(run, v0); b[j] = run;
+          run = add(run, v1); b[j + 1] = run;
+          run = add(run, v2); b[j + 2] = run;
+          run = add(run, v3); b[j + 3] = run;
+          run = add(run, v4); b[j + 4] = run;
+          run = add(run, v5); b[j + 5] = run;
+          run = add(run, v6); b[j + 6] = run;
+          run = add(run, v7); b[j + 7] = run;
+        }
+        for (; j < len; ++j) { run = add(run, b[j]); b[j] = run; }
+      }
+    } else {
+      const int h = tid - 32;
+      if (c + 1 < nchunk) {
+        const long long base = (c + 1) * SEQ_CHUNK;
+        for (int j = h; j < SEQ_CHUNK; j += helpers) buf[nxt][j] = (base + j < n) ? rates[base + j] : 0.0;
+      }
+      if (c >= 1) {
+        const long long base = (c - 1) * SEQ_CHUNK;
+        for (int j = h; j < SEQ_CHUNK && base + j < n; j += helpers) prefix[base + j] = buf[prv][j];
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) *d_total = n > 0 ? run : 0.0;
+}
+
+// First i with prefix[i] >= u*total (two-level parallel search, one CTA).
+__global__ void select_kernel(const double* __restrict__ prefix, const long long* __restrict__ d_count,
+                              const double* __restrict__ d_total, double u, long long* __restrict__ d_index) {
+  __shared__ long long best;
+  const long long n = *d_count;
+  const double total = *d_total;
+  if (threadIdx.x == 0) best = LLONG_MAX;
+  __syncthreads();
+  if (!(total > 0) || n <= 0) {
+    // total <= 0 -> -1 (kmc_simulator_functions.py:61); NaN total scans to the end
+    if (threadIdx.x == 0) *d_index = (total <= 0 || n <= 0) ? -1 : n - 1;
+    return;
+  }
+  const double r = add(0.0, mul(sub(total, 0.0), u));
+  const long long T = blockDim.x;
+  const long long stride = (n + T - 1) / T;
+  // level 1: sample the last element of each stride segment
+  const long long seg_end = min(n, (threadIdx.x + 1) * stride) - 1;
+  if (threadIdx.x * stride < n && prefix[seg_end] >= r) atomicMin((unsigned long long*)&best, (unsigned long long)threadIdx.x);
+  __syncthreads();
+  const long long seg = best;
+  __syncthreads();
+  if (threadIdx.x == 0) best = LLONG_MAX;
+  __syncthreads();
+  if (seg == LLONG_MAX) {
+    if (threadIdx.x == 0) *d_index = n - 1;
+    return;
+  }
+  const long long lo = seg * stride, hi = min(n, lo + stride);
+  for (long long i = lo + threadIdx.x; i < hi; i += T)
+    if (prefix[i] >= r) atomicMin((unsigned long long*)&best, (unsigned long long)i);
+  __syncthreads();
+  if (threadIdx.x == 0) *d_index = best == LLONG_MAX ? n - 1 : best;
+}
+
+// apply_flip_soa_2d (kmc_simulator_functions.py:183-218), one thread.
+__global__ void flip2d_kernel(int nx, int ny, int M, double* ep, double* soft, double* tl, const double* cat, int x,
+                              int y, int m, double t, double jp, double jt, double gmax, double jn) {
+  const long long v = (long long)x * ny + y;
+  const double* c = cat + ((v * M) + m) * 4;
+  for (int q = 0; q < 4; ++q) ep[4 * v + q] = add(ep[4 * v + q], c[q]);
+  const double e11 = c[0], e22 = c[3], e12 = c[1];
+  const double d = sub(e11, e22);
+  const double s = add(mul(e12, e12), __ddiv_rn(add(add(mul(e22, e22), mul(e11, e11)), mul(d, d)), 6.0));
+  double gp = add(soft[2 * v], mul(jp, s));
+  if (gmax > 0 && gp > gmax) gp = gmax;
+  soft[2 * v] = gp;
+  soft[2 * v + 1] = mul(jt, s);
+  tl[v] = t;
+  if (jn > 0.0) {
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy) {
+        if (dx == 0 && dy == 0) continue;
+        const long long w = (long long)((x + dx + nx) % nx) * ny + (y + dy + ny) % ny;
+        double g = add(soft[2 * w], mul(mul(jn, jp), s));
+        if (gmax > 0 && g > gmax) g = gmax;
+        soft[2 * w] = g;
+        soft[2 * w + 1] = add(soft[2 * w + 1], mul(mul(jn, jt), s));
+      }
+  }
+}
+
+}  // namespace mgk
+
+using namespace mgk;
+
+static int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+extern "C" int mgk_kmc2d_barrier(int nx, int ny, int M, double* Q, const double* Q0, const double* sig,
+                                 const double* catalog, double volume, const double* soft_prop,
+                                 const double* last_event_time, double current_time,
+                                 const double* prev_strain_dir, double softening_cap, int scheme, double tau,
+                                 mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && M > 0, "mgk_kmc2d_barrier: bad shape");
+  MGK_REQUIRE(Q && Q0 && sig && catalog && soft_prop && last_event_time, "mgk_kmc2d_barrier: null argument");
+  MGK_REQUIRE(scheme == 0 || (scheme == 1 && prev_strain_dir), "mgk_kmc2d_barrier: bad scheme");
+  const long long nvox = (long long)nx * ny;
+  barrier_kernel<2, 2><<<blocks_for(nvox * M, 256), 256, 0, (cudaStream_t)stream>>>(
+      nvox, M, Q, Q0, sig, catalog, volume, soft_prop, last_event_time, current_time, prev_strain_dir,
+      softening_cap, scheme, tau);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int64_t mgk_kmc_rates_work_bytes(int64_t n_modes) {
+  return (int64_t)sizeof(int) * ((n_modes + 255) / 256 + 1);
+}
+
+static int kmc_rates_impl(long long nvox, int M, const double* Q, double volume, const double* T, double Ts,
+                          double nu0, int cascade_mode, double* rates, int64_t* indices, double* prefix,
+                          int64_t* d_count, double* d_total, void* work, cudaStream_t s) {
+  const long long n = nvox * M;
+  const double vnu = volume * nu0;  // host product, same rounding as (volume * nu0) in the reference
+  if (!cascade_mode) {
+    rates_full_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nvox, M, Q, vnu, T, Ts, rates, (long long*)indices,
+                                                         (long long*)d_count);
+    MGK_CUDA(cudaGetLastError());
+    seq_prefix_kernel<<<1, 256, 0, s>>>(rates, n, nullptr, prefix, d_total);
+    MGK_CUDA(cudaGetLastError());
+  } else {
+    MGK_REQUIRE(work != nullptr, "mgk_kmc2d_rates: cascade mode needs the work buffer");
+    const int nb = blocks_for(n, 256);
+    int* bcount = reinterpret_cast<int*>(work);
+    rates_count_kernel<<<nb, 256, 0, s>>>(n, Q, bcount);
+    MGK_CUDA(cudaGetLastError());
+    scan_counts_kernel<<<1, 1024, 0, s>>>(nb, bcount, (long long*)d_count);
+    MGK_CUDA(cudaGetLastError());
+    rates_scatter_kernel<<<nb, 256, 0, s>>>(nvox, M, Q, vnu, T, Ts, bcount, rates, (long long*)indices);
+    MGK_CUDA(cudaGetLastError());
+    seq_prefix_kernel<<<1, 256, 0, s>>>(rates, 0, (const long long*)d_count, prefix, d_total);
+    MGK_CUDA(cudaGetLastError());
+  }
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_rates(int nx, int ny, int M, const double* Q, double volume, const double* temperature,
+                               double temperature_scalar, double nu0, int cascade_mode, double* rates,
+                               int64_t* indices, double* prefix, int64_t* d_count, double* d_total, void* work,
+                               mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && M > 0, "mgk_kmc2d_rates: bad shape");
+  MGK_REQUIRE(Q && rates && indices && prefix && d_count && d_total, "mgk_kmc2d_rates: null argument");
+  return kmc_rates_impl((long long)nx * ny, M, Q, volume, temperature, temperature_scalar, nu0, cascade_mode, rates,
+                        indices, prefix, d_count, d_total, work, (cudaStream_t)stream);
+}
+
+__global__ void set_count_kernel(long long* d_count, long long n) { *d_count = n; }
+
+extern "C" int mgk_kmc_prefix(const double* rates, int64_t n, double* prefix, int64_t* d_count, double* d_total,
+                              mgk_stream_t stream) {
+  MGK_REQUIRE(n >= 0 && (n == 0 || (rates && prefix)) && d_count && d_total, "mgk_kmc_prefix: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  set_count_kernel<<<1, 1, 0, s>>>((long long*)d_count, (long long)n);
+  MGK_CUDA(cudaGetLastError());
+  seq_prefix_kernel<<<1, 256, 0, s>>>(rates, n, nullptr, prefix, d_total);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc_select(const double* prefix, const int64_t* d_count, const double* d_total, double u,
+                              int64_t* d_index, mgk_stream_t stream) {
+  MGK_REQUIRE(prefix && d_count && d_total && d_index, "mgk_kmc_select: null argument");
+  MGK_REQUIRE(u >= 0.0 && u < 1.0, "mgk_kmc_select: draw must be in [0, 1)");
+  select_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(prefix, (const long long*)d_count, d_total, u,
+                                                      (long long*)d_index);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_flip(int nx, int ny, int M, double* eps_plastic, double* soft_prop, double* last_event_time,
+                              const double* catalog, int x, int y, int m, double current_time, double jp, double jt,
+                              double g_max, double jn_frac, mgk_stream_t stream) {
+  MGK_REQUIRE(x >= 0 && x < nx && y >= 0 && y < ny && m >= 0 && m < M, "mgk_kmc2d_flip: index out of range");
+  MGK_REQUIRE(eps_plastic && soft_prop && last_event_time && catalog, "mgk_kmc2d_flip: null argument");
+  flip2d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, M, eps_plastic, soft_prop, last_event_time, catalog, x, y,
+                                                   m, current_time, jp, jt, g_max, jn_frac);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}

@@ -1,0 +1,98 @@
+"""GPU parity of the STZ/KMC kernels (mgk_kmc*) against the reference's golden
+outputs and the oracle.  Selection index and flip bookkeeping are compared
+bit for bit; barriers and rates to a few ulps (exp() differs by <= 1 ulp
+between CUDA and the host libm)."""
+import numpy as np
+import pytest
+
+from mgkmc_b200 import workloads as W
+from oracle import kmc as OK
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def K():
+    from mgkmc_b200 import kmc_simulator_functions as K
+    return K
+
+
+def test_barrier_golden(K, golden):
+    g = golden("kmc2d_16x12")
+    for c, (t, cap, scheme, tau, vol) in enumerate(g["cases"]):
+        Q = np.zeros_like(g["Q0"])
+        K.compute_barrier_2d(Q, g["Q0"], g["sig"], g["catalog"], vol, g["soft_prop"], g["last_event_time"], t,
+                             g["prev_dir"], cap, int(scheme), tau)
+        np.testing.assert_allclose(Q, g[f"Q_case{c}"], rtol=0, atol=1e-14)
+
+
+def test_barrier_known_answer(K):
+    sig = np.zeros((1, 1, 2, 2)); sig[0, 0, 0, 1] = sig[0, 0, 1, 0] = 1e9
+    cat = np.zeros((1, 1, 1, 2, 2)); cat[0, 0, 0, 0, 1] = cat[0, 0, 0, 1, 0] = 0.1
+    Q = np.zeros((1, 1, 1))
+    K.compute_barrier_2d(Q, np.ones((1, 1, 1)), sig, cat, 1.0, np.zeros((1, 1, 2)), np.full((1, 1), -np.inf), 0.0,
+                         np.zeros((1, 1, 2, 2)), 2.0, 0, np.inf)
+    assert abs(Q[0, 0, 0] - (1.0 - 0.6241509)) < 1e-12
+
+
+def test_rates_golden(K, golden):
+    g = golden("kmc2d_16x12")
+    for T in (300.0, 0.0):
+        for cm in (False, True):
+            tag = f"T{int(T)}_c{int(cm)}"
+            r, idx, total = K.compute_rates_2d(g["Q_rates"], 1.0, T, 1e13, cascade_mode=cm)
+            np.testing.assert_array_equal(idx, g[f"indices_{tag}"])
+            np.testing.assert_allclose(r, g[f"rates_{tag}"], rtol=1e-15, atol=0)
+            assert total == np.add.accumulate(r)[-1]  # the sequential chain, bit for bit
+
+
+def test_select_golden_bit_exact(K, golden):
+    g = golden("kmc2d_16x12")
+    rates, total = g["rates_T300_c0"], float(g["total_T300_c0"])
+    for u, k in zip(g["sel_u"], g["sel_idx"]):
+        assert K.select_event_2d_u(rates, total, u) == k
+
+
+def test_flip_golden_bit_exact(K, golden):
+    g = golden("kmc2d_16x12")
+    ep, sp, tl = g["flip_in_eps_p"].copy(), g["flip_in_soft"].copy(), g["flip_in_tlast"].copy()
+    for (x, y, m, t, jp, jt, gmax, jn) in g["flips"]:
+        K.apply_flip_soa_2d(ep, sp, tl, g["catalog"], int(x), int(y), int(m), t, jp, jt, gmax, jn)
+    np.testing.assert_array_equal(ep, g["flip_out_eps_p"])
+    np.testing.assert_array_equal(sp, g["flip_out_soft"])
+    np.testing.assert_array_equal(tl, g["flip_out_tlast"])
+
+
+def test_full_size_barrier_rates_select(K):
+    # 256^2 x 8 modes (524288 events), seeded state
+    rng = np.random.default_rng(1)
+    nx = ny = 256; M = 8
+    cat, Q0 = W.kmc2d_state(nx, ny, M, rng)
+    sig = 2e9 * rng.standard_normal((nx, ny, 2, 2))
+    soft = np.zeros((nx, ny, 2)); tl = np.full((nx, ny), -np.inf); prev = np.zeros((nx, ny, 2, 2))
+    Q = np.zeros((nx, ny, M)); Qo = np.zeros((nx, ny, M))
+    K.compute_barrier_2d(Q, Q0, sig, cat, 1.0, soft, tl, 0.0, prev, 2.0, 0, np.inf)
+    OK.compute_barrier(Qo, Q0, sig, cat, 1.0, soft, tl, 0.0, prev, 2.0, 0, np.inf)
+    np.testing.assert_allclose(Q, Qo, rtol=0, atol=1e-13)
+    r, idx, total = K.compute_rates_2d(Q, 1.0, 300.0, 1e13, cascade_mode=False)
+    ro, _, _ = OK.compute_rates(Q, 1.0, 300.0, 1e13, cascade_mode=False)
+    np.testing.assert_allclose(r, ro, rtol=1e-14, atol=0)
+    S = np.add.accumulate(r)
+    assert total == S[-1]
+    draws = list(rng.random(40)) + [0.0, np.nextafter(1.0, 0.0)]
+    # draws that land exactly on partial sums
+    for k in (0, 1, 1000, 262143, len(r) - 2):
+        draws.append(S[k] / total)
+    for u in draws:
+        if not (0.0 <= u < 1.0):
+            continue
+        assert K.select_event_2d_u(r, total, u) == OK.select_event(r, total, u)
+
+
+def test_select_edges(K):
+    assert K.select_event_2d_u(np.zeros(5), 0.0, 0.3) == -1
+    r = np.array([0.0, 0.0, 1.0, 0.0])
+    assert K.select_event_2d_u(r, 1.0, 0.0) == OK.select_event_loop(r, 1.0, 0.0) == 0
+    assert K.select_event_2d_u(r, 1.0, 0.999) == OK.select_event_loop(r, 1.0, 0.999) == 2
+    # total larger than the sum: falls off the end -> len-1
+    assert K.select_event_2d_u(r, 2.0, 0.9) == OK.select_event_loop(r, 2.0, 0.9) == 3

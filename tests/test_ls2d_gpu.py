@@ -1,0 +1,117 @@
+"""GPU parity of the 2D LS solver (mgk_ls2d_*) against the reference's golden
+outputs and the oracle.  Tolerance: 1e-9 relative (max-abs error over the
+field divided by the field's max-abs) for FP64 fields."""
+import numpy as np
+import pytest
+
+from mgkmc_b200 import workloads as W
+from oracle import ls as OL
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-9
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def les():
+    from mgkmc_b200 import linear_elastic_simulator as les
+    return les
+
+
+@pytest.mark.parametrize("k", [1, 5])
+def test_golden_cfg0_fixed_iterations(les, golden, k):
+    g = golden("ls2d_cfg0_64")
+    eps, sig, em, sm = les.spectral_solver_2d(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=k, tol=0.0)
+    assert rel(eps, g[f"eps_it{k}"]) < TOL
+    assert rel(sig, g[f"sig_it{k}"]) < TOL
+
+
+def test_golden_cfg0_converged(les, golden):
+    g = golden("ls2d_cfg0_64")
+    eps, sig, em, sm = les.spectral_solver_2d(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-10)
+    assert rel(eps, g["eps_conv"]) < TOL
+    assert rel(sig, g["sig_conv"]) < TOL
+    assert np.max(np.abs(sm - g["sig_mean"])) < TOL * np.max(np.abs(g["sig_mean"]))
+
+
+def test_golden_plane_stress_warm_asymmetric(les, golden):
+    g = golden("ls2d_24x16_pstress")
+    for k in (1, 3):
+        eps, sig, _, _ = les.spectral_solver_2d(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=k, tol=0.0,
+                                                plane_mode="plane_stress", eps_init=g["eps_init"])
+        assert rel(eps, g[f"eps_it{k}"]) < TOL, k
+        assert rel(sig, g[f"sig_it{k}"]) < TOL, k
+    eps, sig, _, _ = les.spectral_solver_2d(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=300, tol=1e-11,
+                                            plane_mode="plane_stress", eps_init=g["eps_init"])
+    assert rel(eps, g["eps_conv"]) < TOL
+    assert rel(sig, g["sig_conv"]) < TOL
+
+
+@pytest.mark.parametrize("nx,ny", [(256, 256), (96, 64), (192, 48), (12, 8), (384, 128)])
+def test_oracle_converged_sizes(les, nx, ny):
+    E, nu, ep, eb = W.ls2d_problem(nx, ny, seed=nx * 7 + ny)
+    o = OL.spectral_solver(E, nu, eb, ep, max_iter=300, tol=1e-10, return_info=True)
+    L = les.Ls2dSolver(nx, ny)
+    import torch
+    dev = torch.device("cuda")
+    eps = torch.empty((nx, ny, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    L.set_material(torch.from_numpy(E).to(dev), torch.from_numpy(nu).to(dev), torch.from_numpy(ep).to(dev))
+    info = L.solve(eb, eps, sig, max_iter=300, tol=1e-10)
+    assert info.status == 0
+    assert abs(info.iterations - o[4]) <= 1
+    assert rel(eps.cpu().numpy(), o[0]) < TOL
+    assert rel(sig.cpu().numpy(), o[1]) < TOL
+
+
+@pytest.mark.parametrize("n", [768, 1024])
+def test_oracle_large_fixed_iterations(les, n):
+    E, nu, ep, eb = W.ls2d_problem(n, n, seed=n)
+    o = OL.spectral_solver(E, nu, eb, ep, max_iter=3, tol=0.0)
+    eps, sig, _, _ = les.spectral_solver_2d(E, nu, eb, ep, max_iter=3, tol=0.0)
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
+def test_homogeneous_known_answer(les):
+    # homogeneous medium: eps = eps_bar exactly, sig = C : eps_bar
+    n = 32
+    E = np.full((n, n), 70e9)
+    nu = np.full((n, n), 0.3)
+    eb = np.array([[0.01, 0.002], [0.002, -0.005]])
+    eps, sig, em, sm = les.spectral_solver_2d(E, nu, eb, max_iter=50, tol=1e-12)
+    assert np.max(np.abs(eps - eb)) < 1e-15
+    lam, mu = OL.lame_2d(70e9, 0.3)
+    sref = 2 * mu * eb + lam * np.trace(eb) * np.eye(2)
+    assert np.max(np.abs(sm - sref)) < 1e-6 * np.max(np.abs(sref))
+
+
+def test_zero_iterations_and_info(les):
+    E, nu, ep, eb = W.ls2d_problem(16, 16, seed=3)
+    eps, sig, _, _ = les.spectral_solver_2d(E, nu, eb, ep, max_iter=0)
+    o = OL.spectral_solver(E, nu, eb, ep, max_iter=0)
+    assert rel(eps, o[0]) < TOL and rel(sig, o[1]) < TOL
+
+
+def test_deterministic_bitwise(les):
+    E, nu, ep, eb = W.ls2d_problem(128, 128, seed=5)
+    a = les.spectral_solver_2d(E, nu, eb, ep, max_iter=200, tol=1e-10)
+    b = les.spectral_solver_2d(E, nu, eb, ep, max_iter=200, tol=1e-10)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_not_converged_status(les):
+    import torch
+    E, nu, ep, eb = W.ls2d_problem(64, 64, seed=9)
+    L = les.Ls2dSolver(64, 64)
+    dev = torch.device("cuda")
+    eps = torch.empty((64, 64, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    L.set_material(torch.from_numpy(E).to(dev), torch.from_numpy(nu).to(dev), torch.from_numpy(ep).to(dev))
+    info = L.solve(eb, eps, sig, max_iter=4, tol=1e-14)
+    assert info.iterations == 4 and info.status == 1
+    o = OL.spectral_solver(E, nu, eb, ep, max_iter=4, tol=1e-14, return_info=True)
+    assert abs(info.final_diff - o[5]) < 1e-9 * o[5]
