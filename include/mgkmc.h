@@ -92,6 +92,30 @@ MGK_API int mgk_ls2d_solve(mgk_ls2d_t plan, const double* eps_bar, const double*
 MGK_API int mgk_ls2d_profile(mgk_ls2d_t plan, const double* eps_bar, int reps, float* row_ms, float* col_ms,
                              mgk_stream_t stream);
 
+/* Allocation-free 2D LS solve.  No counterpart in the reference: an addition
+ * for callers that cannot allocate device memory -- code inside a host
+ * application or framework whose caching allocator already holds the GPU's
+ * memory, serving processes with a fixed memory budget that must not allocate
+ * after start-up, and code that must avoid the device-wide synchronisation
+ * cudaFree implies.  Same arguments and results as
+ * mgk_ls2d_create + mgk_ls2d_set_material + mgk_ls2d_solve (FP64), but every
+ * buffer beyond the caller's inputs and outputs lives in one file-scope
+ * device array sized for grids up to MGK_NOALLOC_MAX_SIDE per side (about
+ * 7 MB, held by every GPU that loads the library until the process exits).
+ * Larger grids are rejected with MGK_BAD_ARG.  The call calls no cudaMalloc
+ * or cudaFree and synchronises `stream` before returning.
+ *   - The first call on a device resolves the array's device address
+ *     (cudaGetSymbolAddress, which may load the module); make that first
+ *     call before any stream capture.
+ *   - All calls on a device share the one array and each call resets what
+ *     must start at zero; calls that overlap on the GPU (other streams, other
+ *     host threads) race on it and must be serialised by the caller. */
+#define MGK_NOALLOC_MAX_SIDE 256
+MGK_API int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const double* E, const double* nu,
+                                   const double* eps_plastic, const double* eps_bar, const double* eps_init,
+                                   double* eps_out, double* sig_out, int max_iter, double tol,
+                                   mgk_ls_info* info, mgk_stream_t stream);
+
 /* ------------------------------------------------------ 2D STZ / KMC --- */
 /* mgkmc/kmc_simulator_functions.py:100-160 compute_barrier_2d (in place on Q).
  * scheme: 0 isotropic, 1 directional.  tau: +inf for no decay. */

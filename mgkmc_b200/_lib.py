@@ -45,6 +45,8 @@ _SIGS = {
     "mgk_ls2d_set_eigenstrain": (c_int, [_P, _P, _P]),
     "mgk_ls2d_solve": (c_int, [_P, POINTER(c_double), _P, _P, _P, c_int, c_double, POINTER(LsInfo), _P]),
     "mgk_ls2d_profile": (c_int, [_P, POINTER(c_double), c_int, POINTER(ctypes.c_float), POINTER(ctypes.c_float), _P]),
+    "mgk_ls2d_solve_noalloc": (c_int, [c_int, c_int, c_int, _P, _P, _P, POINTER(c_double), _P, _P, _P, c_int,
+                                       c_double, POINTER(LsInfo), _P]),
     "mgk_kmc2d_barrier": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
                                   c_double, c_int, c_double, _P]),
     "mgk_kmc_rates_work_bytes": (c_int64, [c_int64]),

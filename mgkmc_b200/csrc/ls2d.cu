@@ -865,3 +865,214 @@ extern "C" int mgk_ls2d_profile(mgk_ls2d_t p, const double* eps_bar, int reps, f
   return p->prec == MGK_FP64 ? ls2d_profile_t<double>(p, eps_bar, reps, row_ms, col_ms, s)
                              : ls2d_profile_t<float>(p, eps_bar, reps, row_ms, col_ms, s);
 }
+
+// ============================================================ no-alloc ===
+// Allocation-free 2D LS solve.  Some callers cannot call cudaMalloc: a host
+// application or framework whose caching allocator already reserves the
+// device memory, a serving process with a fixed memory budget that must not
+// allocate after start-up, or code that must avoid the device-wide
+// synchronisation cudaFree performs.  For them every buffer the solve needs
+// beyond its inputs and outputs lives in one file-scope device array, sized
+// for grids up to MGK_NOALLOC_MAX_SIDE per side; each GPU that loads this
+// library holds it (about 7 MB) until the process exits.
+namespace {
+constexpr long long kNaMaxN = (long long)MGK_NOALLOC_MAX_SIDE * MGK_NOALLOC_MAX_SIDE;
+constexpr size_t kNaPlanes = 10 * (size_t)kNaMaxN;                                          // 10 real planes
+constexpr size_t kNaSpec = 3 * (size_t)MGK_NOALLOC_MAX_SIDE * (MGK_NOALLOC_MAX_SIDE / 2 + 1) * 2;  // complex
+constexpr size_t kNaTw = 2 * (size_t)MGK_NOALLOC_MAX_SIDE * 2;                               // two tables
+constexpr size_t kNaPart = 8 * 2048;                                                         // partial sums
+constexpr size_t kNaMisc = 1024;                    // plan record, state, work maps, counters
+constexpr size_t kNaDoubles = kNaPlanes + kNaSpec + kNaTw + kNaPart + kNaMisc;
+}  // namespace
+
+// Device-side storage.  In host code this name is only a stand-in for the
+// device address, which cudaGetSymbolAddress resolves per device.
+static __device__ __align__(256) double g_ls2d_noalloc_scratch[kNaDoubles];
+
+namespace mgk {
+
+// Writes the plan record, clears the work maps, counters and state, and fills
+// the twiddle tables (sincospi) -- everything a call must start from.
+__global__ void ls2d_noalloc_setup_kernel(Ls2dRep rep, Ls2dRep* dst, Ls2dState* st, int* rowmap, int rowitems,
+                                          int* colmap, int colitems, unsigned int* counter, int* any,
+                                          double2* twx, int nx, double2* twy, int ny) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = t; i < rowitems; i += stride) rowmap[i] = 0;
+  for (int i = t; i < colitems; i += stride) colmap[i] = 0;
+  for (int m = t; m < nx; m += stride) {
+    double s, c;
+    sincospi(2.0 * m / nx, &s, &c);
+    twx[m] = make_double2(c, -s);
+  }
+  for (int m = t; m < ny; m += stride) {
+    double s, c;
+    sincospi(2.0 * m / ny, &s, &c);
+    twy[m] = make_double2(c, -s);
+  }
+  if (t == 0) {
+    *dst = rep;
+    counter[0] = 0;
+    counter[1] = 0;
+    *any = 0;
+    Ls2dState z;
+    memset(&z, 0, sizeof(z));
+    *st = z;
+  }
+}
+
+}  // namespace mgk
+
+#include <mutex>
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[128];  // resolved scratch address per device
+
+// First call on a device: resolve the device address of the scratch array
+// (this loads the module if it is not loaded yet).  Later calls reuse it.
+static int noalloc_scratch(double** out) {
+  int dev = -1;
+  MGK_CUDA(cudaGetDevice(&dev));
+  MGK_REQUIRE(dev >= 0 && dev < 128, "mgk_ls2d_solve_noalloc: device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_ls2d_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error("mgk_ls2d_solve_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
+      return MGK_CUDA_ERROR;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = reinterpret_cast<double*>(g_noalloc_addr[dev]);
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const double* E, const double* nu,
+                                      const double* eps_plastic, const double* eps_bar, const double* eps_init,
+                                      double* eps_out, double* sig_out, int max_iter, double tol,
+                                      mgk_ls_info* info, mgk_stream_t stream) {
+  MGK_REQUIRE(nx >= 4 && ny >= 4 && nx <= MGK_NOALLOC_MAX_SIDE && ny <= MGK_NOALLOC_MAX_SIDE,
+              "mgk_ls2d_solve_noalloc: grid %dx%d exceeds the maximum of %dx%d for the allocation-free entry "
+              "point (use mgk_ls2d_create/mgk_ls2d_solve)", nx, ny, MGK_NOALLOC_MAX_SIDE, MGK_NOALLOC_MAX_SIDE);
+  FftLen fx, fy;
+  MGK_REQUIRE(fft_schedule(nx, &fx) && fft_schedule(ny, &fy),
+              "mgk_ls2d_solve_noalloc: grid %dx%d unsupported (each side must be 2^a 3^b, even)", nx, ny);
+  MGK_REQUIRE(plane_mode == MGK_PLANE_STRAIN || plane_mode == MGK_PLANE_STRESS,
+              "mgk_ls2d_solve_noalloc: plane_mode must be 0 (strain) or 1 (stress)");
+  MGK_REQUIRE(E && nu && eps_bar && eps_out && sig_out, "mgk_ls2d_solve_noalloc: null argument");
+  MGK_REQUIRE(max_iter >= 0 && max_iter <= 1000000, "mgk_ls2d_solve_noalloc: max_iter out of range");
+  double* base = nullptr;
+  int st = noalloc_scratch(&base);
+  if (st != MGK_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+
+  const long long N = (long long)nx * ny;
+  const int nyh = ny / 2 + 1;
+  int tc = 8;
+  while (tc > 1 && 2 * 3 * (size_t)tc * nx * sizeof(double2) > 200 * 1024) tc >>= 1;
+  const int row_items = nx / 2, col_items = (nyh + tc - 1) / tc;
+  const size_t row_smem = 2 * 3 * (size_t)ny * sizeof(double2);
+  const size_t col_smem = 2 * 3 * (size_t)tc * nx * sizeof(double2);
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_col_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)col_smem));
+
+  // carve the scratch array (offsets in doubles, each region 256-byte aligned)
+  double* planes = base;
+  double2* spec = reinterpret_cast<double2*>(base + kNaPlanes);
+  double2* twx = reinterpret_cast<double2*>(base + kNaPlanes + kNaSpec);
+  double2* twy = twx + MGK_NOALLOC_MAX_SIDE;
+  double* part = base + kNaPlanes + kNaSpec + kNaTw;
+  char* misc = reinterpret_cast<char*>(base + kNaPlanes + kNaSpec + kNaTw + kNaPart);
+  Ls2dRep* d_rep = reinterpret_cast<Ls2dRep*>(misc);
+  Ls2dState* d_st = reinterpret_cast<Ls2dState*>(misc + 1024);
+  int* d_rowmap = reinterpret_cast<int*>(misc + 2048);
+  int* d_colmap = reinterpret_cast<int*>(misc + 2048 + 4 * 256);
+  unsigned int* d_counter = reinterpret_cast<unsigned int*>(misc + 2048 + 8 * 256);
+  int* d_any = reinterpret_cast<int*>(misc + 2048 + 8 * 256 + 64);
+  static_assert(sizeof(Ls2dRep) <= 1024 && sizeof(Ls2dState) <= 1024, "no-alloc record sizes");
+  static_assert(2048 + 8 * 256 + 128 <= kNaMisc * sizeof(double), "no-alloc misc region");
+
+  fx.tw = twx;
+  fy.tw = twy;
+  Ls2dRep R;
+  memset(&R, 0, sizeof(R));
+  R.nx = nx; R.ny = ny; R.nyh = nyh; R.ld = nyh;
+  R.row_base = 0; R.row_items = row_items; R.col_base = 0; R.col_items = col_items; R.tc = tc;
+  R.N = N; R.fx = fx; R.fy = fy;
+  R.mu = planes; R.lam = planes + N; R.eps = planes + 2 * N; R.ep = planes + 5 * N;
+  R.epa = eps_plastic ? planes + 8 * N : nullptr;
+  R.has_epa = eps_plastic ? 1 : 0;
+  R.spec = spec;
+
+  ls2d_noalloc_setup_kernel<<<4, 256, 0, s>>>(R, d_rep, d_st, d_rowmap, row_items, d_colmap, col_items, d_counter,
+                                              d_any, twx, nx, twy, ny);
+  MGK_CUDA(cudaGetLastError());
+  const int grid = grid_for(N);
+  ls2d_material_kernel<<<grid, 256, 0, s>>>(d_rep, 0, E, nu, eps_plastic, plane_mode, 1, part);
+  MGK_CUDA(cudaGetLastError());
+  ls2d_medium_kernel<<<1, 256, 0, s>>>(d_rep, d_st, 0, part, grid, plane_mode);
+  MGK_CUDA(cudaGetLastError());
+  const double* eb = eps_bar;
+  if (eps_init) {
+    aos4_partial_kernel<<<grid, 256, 0, s>>>(eps_init, N, part);
+    MGK_CUDA(cudaGetLastError());
+    finalize_sums_kernel<<<1, 256, 0, s>>>(part, grid, 4, 1.0 / (double)N,
+                                           reinterpret_cast<double*>(reinterpret_cast<char*>(d_st) +
+                                                                     offsetof(Ls2dState, means)));
+    MGK_CUDA(cudaGetLastError());
+  }
+  ls2d_begin_kernel<<<grid, 256, 0, s>>>(d_rep, d_st, 0, eb[0], eb[1], eb[2], eb[3], eps_init, tol, max_iter, part,
+                                          d_counter);
+  MGK_CUDA(cudaGetLastError());
+  if (eps_init) {
+    ls2d_begin_finalize_kernel<<<1, 256, 0, s>>>(d_st, 0, part, grid);
+    MGK_CUDA(cudaGetLastError());
+  }
+  if (max_iter > 0) {
+    ls2d_row_kernel<double, false><<<row_items, 256, row_smem, s>>>(d_rep, d_st, d_rowmap, part, d_counter, 1, 0,
+                                                                    0, d_any, 0);
+    MGK_CUDA(cudaGetLastError());
+    // host-driven loop in chunks of 4 iterations; finished iterations skip
+    // their work on the device, and the host polls the activity flag
+    int it = 0;
+    while (it < max_iter) {
+      const int chunk = max_iter - it < 4 ? max_iter - it : 4;
+      for (int c = 0; c < chunk; ++c) {
+        ls2d_col_kernel<double><<<col_items, 256, col_smem, s>>>(d_rep, d_st, d_colmap);
+        ls2d_row_kernel<double, true><<<row_items, 256, row_smem, s>>>(d_rep, d_st, d_rowmap, part, d_counter, 1,
+                                                                       0, 0, d_any, 0);
+      }
+      MGK_CUDA(cudaGetLastError());
+      it += chunk;
+      int h_any = 0;
+      MGK_CUDA(cudaMemcpyAsync(&h_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, s));
+      MGK_CUDA(cudaStreamSynchronize(s));
+      if (!h_any) break;
+    }
+  }
+  ls2d_output_kernel<<<grid, 256, 0, s>>>(d_rep, d_st, 0, eps_out, sig_out, part);
+  MGK_CUDA(cudaGetLastError());
+  finalize_sums_kernel<<<1, 256, 0, s>>>(part, grid, 8, 1.0 / (double)N,
+                                         reinterpret_cast<double*>(reinterpret_cast<char*>(d_st) +
+                                                                   offsetof(Ls2dState, out_eps_mean)));
+  MGK_CUDA(cudaGetLastError());
+  Ls2dState h;
+  MGK_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(Ls2dState), cudaMemcpyDeviceToHost, s));
+  MGK_CUDA(cudaStreamSynchronize(s));
+  if (info) {
+    info->iterations = h.iter;
+    info->status = h.status;
+    info->final_diff = h.diff;
+    for (int q = 0; q < 4; ++q) { info->eps_mean[q] = h.out_eps_mean[q]; info->sig_mean[q] = h.out_sig_mean[q]; }
+  }
+  if (h.status == MGK_NONFINITE) {
+    set_error("mgk_ls2d_solve_noalloc: non-finite residual at iteration %d", h.iter);
+    return MGK_NONFINITE;
+  }
+  return MGK_OK;
+}
