@@ -6,9 +6,11 @@ Workload (default): 2D small-strain Lippmann-Schwinger equilibrium solves on
 a 256x256 periodic plane-strain grid with the heterogeneous material of the
 KMC/AQS benchmark (mu ~ mu0 (1 + 0.1 N(0,1)) clipped, K = 100 GPa, 5 % pure
 shear eigenstrains of magnitude 0.1, eps_xx = 0.01), solved to an update norm
-of 1e-8 in FP64.  One step = one batch of ``--batch`` solves on distinct
-seeded problems; value = solves/s over all ranks (replicas only: each rank
-solves its own problems, no collective; scaling "weak").
+of 1e-8.  One step = one batch of ``--batch`` solves on distinct seeded
+problems, in three forms: plain FP64 (one solve after another), batched FP64
+(one launch per stage for the batch) and batched mixed precision (FP32 bulk,
+FP64 finish; the headline value).  value = solves/s over all ranks (replicas
+only: each rank solves its own problems, no collective; scaling "weak").
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (oracle, numpy FFT) on the host cores, one process per core, on the same
@@ -30,7 +32,7 @@ sys.path.insert(0, ROOT)
 
 NX = NY = 256
 TOL = 1e-8
-METRIC = "equilibrium solves/s (2D LS 256^2, FP64, update norm 1e-8)"
+METRIC = "equilibrium solves/s (2D LS 256^2, update norm 1e-8, field err <= 1e-6 vs FP64)"
 
 
 def parse():
@@ -99,7 +101,7 @@ def run_reference(a):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * a.batch / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, survey config)",
-            "config": {"workload": "ls2d_256_fp64", "batch": a.batch, "grid": [NX, NY], "tol": TOL},
+            "config": {"workload": f"ls2d_{NX}_batched_mixed", "batch": a.batch, "grid": [NX, NY], "tol": TOL},
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
                              "sample": f"{solves} oracle solves in {wall:.1f} s, one process per core"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -152,6 +154,19 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- GPU leg -----
+def _time_steps(step, steps, flush, stream):
+    """Device time (ms) of `steps` calls of step(), L2 flushed between them."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()  # > L2 write between timed steps, outside the events
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(e0.elapsed_time(e1) for e0, e1 in ev)
+
+
 def run_ours(a):
     import torch
     rank, world, local = _rank()
@@ -161,37 +176,60 @@ def run_ours(a):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    from mgkmc_b200 import _lib as L
     from mgkmc_b200 import linear_elastic_simulator as les
     from mgkmc_b200 import workloads as W
 
     B = a.batch
     probs = [W.ls2d_problem(NX, NY, seed=1000 * rank + b) for b in range(B)]
-    solvers, eps, sig = [], [], []
-    for (E, nu, ep, eb) in probs:
-        s = les.Ls2dSolver(NX, NY)
-        s.set_material(torch.from_numpy(E).to(dev), torch.from_numpy(nu).to(dev), torch.from_numpy(ep).to(dev))
-        solvers.append(s)
-        eps.append(torch.empty((NX, NY, 2, 2), dtype=torch.float64, device=dev))
-        sig.append(torch.empty_like(eps[-1]))
+    dE = [torch.from_numpy(p[0]).to(dev) for p in probs]
+    dnu = [torch.from_numpy(p[1]).to(dev) for p in probs]
+    dep = [torch.from_numpy(p[2]).to(dev) for p in probs]
+    ebs = [p[3] for p in probs]
+    eps = [torch.empty((NX, NY, 2, 2), dtype=torch.float64, device=dev) for _ in range(B)]
+    sig = [torch.empty_like(e) for e in eps]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
     stream = torch.cuda.current_stream()
+    reps = list(range(B))
 
-    def step():
-        for b in range(B):
-            solvers[b].solve(probs[b][3], eps[b], sig[b], max_iter=500, tol=TOL, sync=False)
-
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
-    # iterations per solve (device-decided) for the launch count and roofline
-    iters = []
+    # form 1: plain FP64, one plan per problem, one solve after another
+    plain = []
     for b in range(B):
-        info = solvers[b].solve(probs[b][3], eps[b], sig[b], max_iter=500, tol=TOL, sync=True)
-        iters.append(info.iterations)
-    # equilibrium residual of the returned field: one LS iteration from it
-    chk = solvers[0].solve(probs[0][3], torch.empty_like(eps[0]), torch.empty_like(sig[0]), eps_init=eps[0],
-                           max_iter=1, tol=0.0, sync=True)
+        s = les.Ls2dSolver(NX, NY)
+        s.set_material(dE[b], dnu[b], dep[b])
+        plain.append(s)
+
+    def step_plain():
+        for b in range(B):
+            plain[b].solve(ebs[b], eps[b], sig[b], max_iter=500, tol=TOL, sync=False)
+
+    # forms 2 and 3: one launch per stage for the whole batch
+    batches = {}
+    for prec in ("fp64", "mixed"):
+        bt = les.Ls2dBatch([(NX, NY)] * B, precision=prec)
+        for b in range(B):
+            bt.set_material(b, dE[b], dnu[b], dep[b])
+        batches[prec] = bt
+
+    def step_batch(prec):
+        batches[prec].solve(reps, ebs, eps, sig, max_iter=500, tol=TOL, sync=False)
+
+    forms = {"plain_fp64": step_plain, "batched_fp64": lambda: step_batch("fp64"),
+             "batched_mixed": lambda: step_batch("mixed")}
+    iters = {}
+    for name, fn in forms.items():
+        for _ in range(a.warmup):
+            fn()
+    torch.cuda.synchronize()
+    iters["plain_fp64"] = [plain[b].solve(ebs[b], eps[b], sig[b], max_iter=500, tol=TOL).iterations for b in range(B)]
+    ref_eps = [e.clone() for e in eps]
+    for prec in ("fp64", "mixed"):
+        inf = batches[prec].solve(reps, ebs, eps, sig, max_iter=500, tol=TOL, sync=True)
+        iters["batched_" + prec] = [i.iterations for i in inf]
+    # mixed-form field error against the FP64 result, and its equilibrium
+    # residual: one FP64 LS iteration started from the mixed field
+    err_mixed = max(float((eps[b] - ref_eps[b]).abs().max() / ref_eps[b].abs().max()) for b in range(B))
+    chk = plain[0].solve(ebs[0], torch.empty_like(eps[0]), torch.empty_like(sig[0]), eps_init=eps[0].clone(),
+                         max_iter=1, tol=0.0, sync=True)
     residual = chk.final_diff
 
     if world > 1:
@@ -199,70 +237,84 @@ def run_ours(a):
     torch.cuda.synchronize()
     clk = ClockSampler(local)
     clk.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    for k in range(a.steps):
-        flush.zero_()  # L2 flush between timed steps (outside the timed events)
-        ev[k][0].record(stream)
-        step()
-        ev[k][1].record(stream)
-    torch.cuda.synchronize()
+    ms = {name: _time_steps(fn, a.steps, flush, stream) for name, fn in forms.items()}
     clocks = clk.stop()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
+        t = torch.tensor([ms[k] for k in forms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    solves = B * a.steps * world
-    value = solves / (ms / 1e3)
+        ms = {k: float(v) for k, v in zip(forms, t.tolist())}
+    rate = {k: B * a.steps * world / (ms[k] / 1e3) for k in forms}
+    head = "batched_mixed"
 
-    # per-kernel timing of one LS iteration (row and column kernels) on solver 0
-    kt = solvers[0].profile_kernels(probs[0][3], reps=50)
+    # per-kernel timing (CUDA events on the launching stream) over the batch
+    row64, col64 = batches["fp64"].profile_kernels(reps, ebs, fp32=False, n=20)
+    row32, col32 = batches["mixed"].profile_kernels(reps, ebs, fp32=True, n=20)
 
-    # end-to-end through the reference-facing API with host numpy buffers
-    e2e_n = 0
-    h2d = d2h = 0
+    # end to end through the batch API with pinned host buffers: H2D of every
+    # problem's E, nu, eps_p, the solve, D2H of eps and sig, each step
+    hE = [torch.from_numpy(p[0]).pin_memory() for p in probs]
+    hnu = [torch.from_numpy(p[1]).pin_memory() for p in probs]
+    hep = [torch.from_numpy(p[2]).pin_memory() for p in probs]
+    heps = [torch.empty((NX, NY, 2, 2), dtype=torch.float64).pin_memory() for _ in range(B)]
+    hsig = [torch.empty_like(h).pin_memory() for h in heps]
+    bt = batches["mixed"]
+
+    def e2e_step():
+        for b in range(B):
+            dE[b].copy_(hE[b], non_blocking=True)
+            dnu[b].copy_(hnu[b], non_blocking=True)
+            dep[b].copy_(hep[b], non_blocking=True)
+            bt.set_material(b, dE[b], dnu[b], dep[b])
+        bt.solve(reps, ebs, eps, sig, max_iter=500, tol=TOL, sync=False)
+        for b in range(B):
+            heps[b].copy_(eps[b], non_blocking=True)
+            hsig[b].copy_(sig[b], non_blocking=True)
+
+    e2e_step()
     torch.cuda.synchronize()
+    n_e2e = max(2, a.steps // 2)
     t0 = time.perf_counter()
-    for k in range(max(1, a.steps // 2)):
-        for b in range(min(B, 8)):
-            E, nu, ep, eb = probs[b]
-            les.spectral_solver_2d(E, nu, eb, ep, max_iter=500, tol=TOL)
-            e2e_n += 1
+    for _ in range(n_e2e):
+        e2e_step()
+    torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    h2d = (E.nbytes + nu.nbytes + ep.nbytes)
-    d2h = 2 * ep.nbytes
-    e2e_val = e2e_n / e2e_s * world
+    h2d = B * (hE[0].nbytes + hnu[0].nbytes + hep[0].nbytes)
+    d2h = B * (heps[0].nbytes + hsig[0].nbytes)
+    e2e_val = B * n_e2e / e2e_s * world
 
-    launches_per_solve = [4 + 2 * i for i in iters]  # begin, row0, (col,row) x iters, output, finalize
-    gpu_launches = int(sum(launches_per_solve) * a.steps)
+    it_head = iters[head]
+    gpu_launches = int(a.steps * (7 + 2 * max(it_head) + 3))  # begin, row0, 2/iter, promote+phase2+row0, output, finalize
 
     if rank != 0:
         return
     N = NX * NY
-    roof = None
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
     peak_kind = "measured" if os.path.exists(peaks_path) else "fallback"
-    if kt is not None:
-        row_ms, col_ms = kt
-        row_bytes = 136.0 * N
-        achieved = row_bytes / (row_ms * 1e-3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "ls2d_row_kernel<double,true>", "peak_kind": peak_kind,
-                "row_us": row_ms * 1e3, "col_us": col_ms * 1e3}
+    row_bytes = 136.0 * N * B
+    achieved = row_bytes / (row64 * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "ls2d_row_kernel<double,double,true,true> over the batch",
+            "peak_kind": peak_kind, "bytes_per_launch": row_bytes,
+            "kernels_us": {"row_fp64": row64 * 1e3, "col_fp64": col64 * 1e3, "row_fp32": row32 * 1e3,
+                           "col_fp32": col32 * 1e3},
+            "col_fp64_frac": 48.0 * N * B / (col64 * 1e-3) / 1e9 / peak,
+            "row_fp32_frac": 68.0 * N * B / (row32 * 1e-3) / 1e9 / peak}
     cpu = None
     if world == 1 and a.cpu_seconds > 0:
         v, nsol, wall = cpu_baseline(a.cpu_seconds, 1)
         cpu = {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
                "sample": f"{nsol} oracle solves of the same {NX}^2 problem in {wall:.1f} s (numpy FFT, 1 thread)"}
-    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": rate[head], "unit": "solves/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms[head] / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, survey config)",
-            "config": {"workload": f"ls2d_{NX}_fp64_plain", "batch": B, "grid": [NX, NY], "tol": TOL,
-                       "l2": "flushed between steps (256 MB write)", "iters_mean": float(np.mean(iters)),
-                       "residual": residual, "parallelism": f"replicas x{world}"},
+            "config": {"workload": f"ls2d_{NX}_batched_mixed", "batch": B, "grid": [NX, NY], "tol": TOL,
+                       "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}",
+                       "forms_solves_per_s": rate, "speedup_vs_plain_fp64": rate[head] / rate["plain_fp64"],
+                       "iters_mean": {k: float(np.mean(v)) for k, v in iters.items()},
+                       "mixed_field_err_vs_fp64": err_mixed, "mixed_residual": residual},
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.spectral_solver_2d"},
+                    "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.Ls2dBatch"},
             "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
     print(json.dumps(line), flush=True)
     if world > 1:

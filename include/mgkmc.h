@@ -43,7 +43,10 @@ typedef enum {
 } mgk_status;
 
 enum { MGK_PLANE_STRAIN = 0, MGK_PLANE_STRESS = 1 };
-enum { MGK_FP64 = 0, MGK_FP32 = 1 };
+/* precision forms: FP64 throughout (the reference's arithmetic), or mixed:
+ * FP32 storage/FFT/Green operator until the update norm is below
+ * max(tol, 2e-6), then FP64 iterations to tol; norms are FP64 in both */
+enum { MGK_FP64 = 0, MGK_MIXED = 1 };
 
 /* ------------------------------------------------------------- library --- */
 MGK_API int mgk_version(void);
@@ -66,16 +69,25 @@ typedef struct {
   double sig_mean[4];   /* sig_out.mean(axis=(0,1)) */
 } mgk_ls_info;
 
-/* pixel: voxel size (only enters the wave vectors, where it cancels). */
+/* A plan holds nrep independent replicas ("slots"); mgk_ls2d_create makes a
+ * plan of one.  The voxel size only enters the wave vectors, where it
+ * cancels, so it is not an argument. */
 MGK_API int mgk_ls2d_create(int nx, int ny, int plane_mode, int precision, mgk_ls2d_t* out);
+/* Batched plan: replica r has grid nx[r] x ny[r] (sizes may differ). */
+MGK_API int mgk_ls2d_create_batch(int nrep, const int* nx, const int* ny, int plane_mode, int precision,
+                                  mgk_ls2d_t* out);
 MGK_API int mgk_ls2d_destroy(mgk_ls2d_t plan);
 /* Moduli fields E, nu (nx,ny) and the eigenstrain eps_plastic (nx,ny,2,2) or
  * NULL (= zero).  Computes mu, lambda per voxel and the reference medium
  * C0 = (mean E, mean nu) on the device (linear_elastic_simulator.py:22-23). */
 MGK_API int mgk_ls2d_set_material(mgk_ls2d_t plan, const double* E, const double* nu,
                           const double* eps_plastic, mgk_stream_t stream);
+MGK_API int mgk_ls2d_set_material_rep(mgk_ls2d_t plan, int rep, const double* E, const double* nu,
+                                      const double* eps_plastic, mgk_stream_t stream);
 /* Update only the eigenstrain field (KMC flips). */
 MGK_API int mgk_ls2d_set_eigenstrain(mgk_ls2d_t plan, const double* eps_plastic, mgk_stream_t stream);
+MGK_API int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t plan, int rep, const double* eps_plastic,
+                                         mgk_stream_t stream);
 /* One LS solve.  eps_bar: host (2,2).  eps_init: device (nx,ny,2,2) warm start
  * or NULL (uniform eps_bar start, :32-41).  eps_out, sig_out: device
  * (nx,ny,2,2).  info: host, may be NULL; when given the call synchronises the
@@ -84,6 +96,15 @@ MGK_API int mgk_ls2d_set_eigenstrain(mgk_ls2d_t plan, const double* eps_plastic,
 MGK_API int mgk_ls2d_solve(mgk_ls2d_t plan, const double* eps_bar, const double* eps_init,
                    double* eps_out, double* sig_out, int max_iter, double tol,
                    mgk_ls_info* info, mgk_stream_t stream);
+/* Batched solve of nsel replicas sel[0..nsel) (sel NULL = 0..nsel-1), one
+ * launch per stage for all of them, each replica converging on its own.
+ * eps_bar: host nsel x 4.  eps_init, eps_out, sig_out: host arrays of nsel
+ * device pointers (entries may be NULL; eps_init itself may be NULL).
+ * infos: host nsel entries or NULL (NULL = no synchronisation). */
+MGK_API int mgk_ls2d_solve_batch(mgk_ls2d_t plan, int nsel, const int* sel, const double* eps_bar,
+                                 const double* const* eps_init, double* const* eps_out,
+                                 double* const* sig_out, int max_iter, double tol, mgk_ls_info* infos,
+                                 mgk_stream_t stream);
 
 /* Timing hook: runs `reps` LS iterations (tolerance 0) and returns the mean
  * duration of the row kernel (C2R+update+tau+R2C along y) and of the column
@@ -91,6 +112,9 @@ MGK_API int mgk_ls2d_solve(mgk_ls2d_t plan, const double* eps_bar, const double*
  * Leaves the plan's iterate in an unspecified state. */
 MGK_API int mgk_ls2d_profile(mgk_ls2d_t plan, const double* eps_bar, int reps, float* row_ms, float* col_ms,
                              mgk_stream_t stream);
+/* Same over a batch selection; fp32 = 1 times the FP32 kernels of a mixed plan. */
+MGK_API int mgk_ls2d_profile_batch(mgk_ls2d_t plan, int nsel, const int* sel, const double* eps_bar, int fp32,
+                                   int reps, float* row_ms, float* col_ms, mgk_stream_t stream);
 
 /* Allocation-free 2D LS solve.  No counterpart in the reference: an addition
  * for callers that cannot allocate device memory -- code inside a host

@@ -15,7 +15,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "mgkmc.h")
 
 OK, NOT_CONVERGED, NONFINITE, BAD_ARG, OOM, TIMEOUT, CUDA_ERROR = range(7)
 PLANE_STRAIN, PLANE_STRESS = 0, 1
-FP64, FP32 = 0, 1
+FP64, MIXED = 0, 1
 
 
 class MgkError(RuntimeError):
@@ -43,6 +43,13 @@ _SIGS = {
     "mgk_ls2d_destroy": (c_int, [_P]),
     "mgk_ls2d_set_material": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_ls2d_set_eigenstrain": (c_int, [_P, _P, _P]),
+    "mgk_ls2d_create_batch": (c_int, [c_int, POINTER(c_int), POINTER(c_int), c_int, c_int, POINTER(c_void_p)]),
+    "mgk_ls2d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
+    "mgk_ls2d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
+    "mgk_ls2d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
+                                     POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo), _P]),
+    "mgk_ls2d_profile_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), c_int, c_int,
+                                       POINTER(ctypes.c_float), POINTER(ctypes.c_float), _P]),
     "mgk_ls2d_solve": (c_int, [_P, POINTER(c_double), _P, _P, _P, c_int, c_double, POINTER(LsInfo), _P]),
     "mgk_ls2d_profile": (c_int, [_P, POINTER(c_double), c_int, POINTER(ctypes.c_float), POINTER(ctypes.c_float), _P]),
     "mgk_ls2d_solve_noalloc": (c_int, [c_int, c_int, c_int, _P, _P, _P, POINTER(c_double), _P, _P, _P, c_int,

@@ -1,4 +1,4 @@
-// 2D small-strain Lippmann-Schwinger solver (FP64 / FP32 spectral path).
+// 2D small-strain Lippmann-Schwinger solver, batched over replicas.
 //
 // Restates mgkmc/linear_elastic_simulator.py:12-88 (spectral_solver_2d):
 //   tau = C:(eps - eps_p) - C0:eps;  eps_new = eps_bar - IFFT(Gamma0 : FFT(tau));
@@ -6,14 +6,19 @@
 // with the Green operator of mgkmc/elasticity.py:20-53 evaluated on the fly
 // from the wave vector (never materialised).
 //
-// HBM layout per replica (SoA planes of N = nx*ny doubles, C order):
+// A plan holds `nrep` independent replicas (grids of any supported size, so a
+// batch may be ragged).  A solve call selects a subset of them; every stage
+// is one launch over all selected replicas.
+//
+// HBM layout per replica (SoA planes of N = nx*ny, C order):
 //   mu, lam                 Lame fields (plane strain or plane stress lambda)
 //   eps[3]                  xx, yy, symmetric xy of the current iterate
 //   ep[3]                   xx, yy, symmetric xy of the eigenstrain
-//   epa[2] (optional)       eps_p xy and yx when eps_p is not symmetric
+//   epa[2] (optional)       eps_p xy and yx when an eigenstrain is given
 //   spec[3]                 half spectrum, nx rows of ld = ny/2+1 complex
-// The antisymmetric part of eps is uniform after the first iteration
-// (Gamma0 returns symmetric tensors), so it is carried as one scalar.
+// Mixed-precision plans also hold FP32 copies of mu, lam, eps and ep.  The
+// antisymmetric part of eps is uniform after the first iteration (Gamma0
+// returns symmetric tensors), so it is carried as one scalar.
 //
 // One iteration = two kernels:
 //   row kernel  (one CTA per pair of x-rows): C2R along y of the previous
@@ -22,10 +27,16 @@
 //               polarisation tau and the R2C along y of the next iteration;
 //   column kernel (one CTA per tile of ky columns): complex FFT along x,
 //               eps~^ = -Gamma0_sym(k) : tau^ / N, inverse FFT along x.
-// So the spectral field crosses HBM once per direction per iteration.  The
-// last CTA of each row kernel reduces the partial sums in a fixed order
-// (deterministic), decides convergence on the device and drives the CUDA
-// graph while-node that holds the loop.
+// The spectral field crosses HBM once per direction per iteration.  The last
+// CTA of each replica to finish a row kernel reduces that replica's partial
+// sums in a fixed order (deterministic), decides its convergence on the
+// device, and the last replica to decide sets the condition of the CUDA
+// graph while-node that holds the loop, so a solve needs no host round trip.
+//
+// Precision forms: FP64 (the reference's arithmetic), and mixed: FP32
+// storage, FFTs and Gamma0 until the update norm falls below max(tol, 2e-6)
+// (phase 1), then FP64 iterations from that field to the requested tol
+// (phase 2).  Norms and partial sums are FP64 in both.
 //
 // Nyquist handling: the reference takes .real of a complex ifft after
 // multiplying by Gamma(q) whose sign pattern breaks Hermitian symmetry on
@@ -39,6 +50,8 @@
 #include <stddef.h>
 #include <stdlib.h>
 
+#include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -49,17 +62,28 @@ namespace mgk {
 const void* twiddles(int n, int prec);
 
 struct Ls2dRep {
-  int nx, ny, nyh, ld;
-  int row_base, row_items, col_base, col_items, tc;
-  int has_epa;
+  int nx, ny, nyh, ld, tc;
+  int row_items, col_items;
   long long N;
-  FftLen fx, fy;
+  FftLen fx64, fy64, fx32, fy32;
   double* mu;
   double* lam;
   double* eps;   // 3 planes
   double* ep;    // 3 planes
   double* epa;   // 2 planes or null
-  void* spec;    // 3 planes of nx*ld complex
+  float* mu32;   // mixed plans only
+  float* lam32;
+  float* eps32;
+  float* ep32;
+  void* spec;    // 3 planes of nx*ld complex (double2, or float2 in FP32 phases)
+  // per call
+  const double* init;
+  double* out_eps;
+  double* out_sig;
+  double eb[4];
+  double tol;
+  int max_iter;
+  int row_first, col_first;  // first work item of this replica in the call's maps
 };
 
 struct Ls2dState {
@@ -67,10 +91,9 @@ struct Ls2dState {
   double ebar[3];
   double abar;
   double extra_d0, extra_n0;
-  double tol;
-  int max_iter;
   int iter;
-  int done;
+  int phase_iter;
+  int done;    // 0 active, 1 finished the current phase, 2 finished
   int status;
   double diff;
   double means[4];  // warm-start means (xx, xy, yx, yy)
@@ -78,9 +101,20 @@ struct Ls2dState {
   double out_sig_mean[4];
 };
 
+struct Ls2dCtl {
+  unsigned int n_active;  // replicas iterating at the start of the current body
+  unsigned int decided;
+  unsigned int still;
+  unsigned int bodies;    // loop bodies run in the current phase (guard)
+  int any;
+};
+
+constexpr double kMixedPhase1Tol = 2e-6;
+constexpr int kMixedPhase1Cap = 64;
+
 // --------------------------------------------------------------- helpers ---
 
-// eps~^ = -Gamma0(n) : tau^ * scale for symmetric tau (2D), n a unit vector.
+// eps~^ = -Gamma0(n) : tau^ for symmetric tau (2D), n a unit vector.
 template <typename C, typename T>
 __device__ __forceinline__ void gamma2d_apply(const C& txx, const C& tyy, const C& txy, T nx, T ny,
                                               T inv2mu0, T Bc, C& exx, C& eyy, C& exy) {
@@ -96,15 +130,34 @@ __device__ __forceinline__ void gamma2d_apply(const C& txx, const C& tyy, const 
 
 __device__ __forceinline__ int fftfreq(int k, int n) { return (k < (n + 1) / 2) ? k : k - n; }
 
+template <typename TS> struct Fields;
+template <> struct Fields<double> {
+  static __device__ __forceinline__ const double* mu(const Ls2dRep& R) { return R.mu; }
+  static __device__ __forceinline__ const double* lam(const Ls2dRep& R) { return R.lam; }
+  static __device__ __forceinline__ double* eps(const Ls2dRep& R) { return R.eps; }
+  static __device__ __forceinline__ const double* ep(const Ls2dRep& R) { return R.ep; }
+  static __device__ __forceinline__ const FftLen& fx(const Ls2dRep& R) { return R.fx64; }
+  static __device__ __forceinline__ const FftLen& fy(const Ls2dRep& R) { return R.fy64; }
+};
+template <> struct Fields<float> {
+  static __device__ __forceinline__ const float* mu(const Ls2dRep& R) { return R.mu32; }
+  static __device__ __forceinline__ const float* lam(const Ls2dRep& R) { return R.lam32; }
+  static __device__ __forceinline__ float* eps(const Ls2dRep& R) { return R.eps32; }
+  static __device__ __forceinline__ const float* ep(const Ls2dRep& R) { return R.ep32; }
+  static __device__ __forceinline__ const FftLen& fx(const Ls2dRep& R) { return R.fx32; }
+  static __device__ __forceinline__ const FftLen& fy(const Ls2dRep& R) { return R.fy32; }
+};
+
 // -------------------------------------------------------------- kernels ---
 
-// Per-voxel material prep: mu, lambda from (E, nu) as in elasticity.py:3-10,
-// eigenstrain planes, and per-CTA partial sums of E and nu for the means.
-__global__ void ls2d_material_kernel(Ls2dRep* reps, int rep, const double* __restrict__ E,
+// Per-voxel material prep for one replica: mu, lambda from (E, nu) as in
+// elasticity.py:3-10, eigenstrain planes (and FP32 copies for mixed plans),
+// per-CTA partial sums of E and nu for the reference medium.
+__global__ void ls2d_material_kernel(const Ls2dRep* reps, int rep, const double* __restrict__ E,
                                      const double* __restrict__ nu, const double* __restrict__ epsp,
                                      int plane_mode, int set_moduli, double* partials) {
   __shared__ double red[32];
-  Ls2dRep& R = reps[rep];
+  const Ls2dRep& R = reps[rep];
   const long long N = R.N;
   double sE = 0, sn = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
@@ -116,16 +169,20 @@ __global__ void ls2d_material_kernel(Ls2dRep* reps, int rep, const double* __res
                                                          : e * v / ((1 + v) * (1 - 2 * v));
       R.mu[i] = mu;
       R.lam[i] = lam;
+      if (R.mu32) { R.mu32[i] = (float)mu; R.lam32[i] = (float)lam; }
       sE += e;
       sn += v;
     }
     double pxx = 0, pxy = 0, pyx = 0, pyy = 0;
     if (epsp) {
-      pxx = epsp[4 * i + 0]; pxy = epsp[4 * i + 1]; pyx = epsp[4 * i + 2]; pyy = epsp[4 * i + 3];
+      const double4 p = reinterpret_cast<const double4*>(epsp)[i];
+      pxx = p.x; pxy = p.y; pyx = p.z; pyy = p.w;
     }
+    const double psym = (pxy == pyx) ? pxy : 0.5 * (pxy + pyx);
     R.ep[i] = pxx;
     R.ep[N + i] = pyy;
-    R.ep[2 * N + i] = (pxy == pyx) ? pxy : 0.5 * (pxy + pyx);
+    R.ep[2 * N + i] = psym;
+    if (R.ep32) { R.ep32[i] = (float)pxx; R.ep32[N + i] = (float)pyy; R.ep32[2 * N + i] = (float)psym; }
     if (R.epa) {
       R.epa[i] = pxy;
       R.epa[N + i] = pyx;
@@ -142,7 +199,7 @@ __global__ void ls2d_material_kernel(Ls2dRep* reps, int rep, const double* __res
 }
 
 // Reference medium from the means (linear_elastic_simulator.py:22-26).
-__global__ void ls2d_medium_kernel(Ls2dRep* reps, Ls2dState* st, int rep, const double* partials,
+__global__ void ls2d_medium_kernel(const Ls2dRep* reps, Ls2dState* st, int rep, const double* partials,
                                    int nblocks, int plane_mode) {
   __shared__ double red[32];
   double a = 0, b = 0;
@@ -162,104 +219,115 @@ __global__ void ls2d_medium_kernel(Ls2dRep* reps, Ls2dState* st, int rep, const 
   }
 }
 
-// Means of a (nx,ny,2,2) field: per-CTA partials of the 4 components.
-__global__ void aos4_partial_kernel(const double* __restrict__ f, long long N, double* partials) {
+// Warm-start means: per-CTA partials of the 4 components of each selected
+// replica's init field.  grid = (G, nsel).
+__global__ void ls2d_means_kernel(const Ls2dRep* reps, const int* sel, double* partials) {
   __shared__ double red[32];
+  const int r = sel[blockIdx.y];
+  const Ls2dRep& R = reps[r];
+  if (!R.init) return;
+  const long long N = R.N;
   double s[4] = {0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
-    const double4 v = reinterpret_cast<const double4*>(f)[i];
+    const double4 v = reinterpret_cast<const double4*>(R.init)[i];
     s[0] += v.x; s[1] += v.y; s[2] += v.z; s[3] += v.w;
   }
   for (int q = 0; q < 4; ++q) {
     double t = block_sum(s[q], red);
-    if (threadIdx.x == 0) partials[4 * blockIdx.x + q] = t;
+    if (threadIdx.x == 0) partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 8 + q] = t;
   }
 }
 
-// Sum K-wide partials of nblocks CTAs in a fixed order into out[K] (scaled).
-__global__ void finalize_sums_kernel(const double* partials, int nblocks, int K, double scale, double* out) {
+// Fixed-order sums of the per-CTA partials of replica sel[blockIdx.x]: K
+// values at byte offset `off` of its state.  need_init: 0 -> means (scaled
+// by 1/N) for every replica, 1 -> means only for replicas with a warm start,
+// 2 -> plain sums only for replicas with a warm start.
+__global__ void ls2d_finalize_kernel(const Ls2dRep* reps, Ls2dState* st, const int* sel, const double* partials,
+                                     int G, int K, int off, int need_init) {
   __shared__ double red[32];
+  const int r = sel[blockIdx.x];
+  if (need_init && !reps[r].init) return;
+  const double scale = need_init == 2 ? 1.0 : 1.0 / (double)reps[r].N;
+  double* out = reinterpret_cast<double*>(reinterpret_cast<char*>(&st[r]) + off);
   for (int q = 0; q < K; ++q) {
     double a = 0;
-    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) a += partials[K * i + q];
+    for (int i = threadIdx.x; i < G; i += blockDim.x) a += partials[((size_t)blockIdx.x * G + i) * 8 + q];
     a = block_sum(a, red);
     if (threadIdx.x == 0) out[q] = a * scale;
   }
 }
 
-// Solve start: set eps_bar, tolerances and the initial field
-// (linear_elastic_simulator.py:32-41); partial sums of the antisymmetric
-// part's contribution to the first diff and norm.
-__global__ void ls2d_begin_kernel(Ls2dRep* reps, Ls2dState* st, int rep, double e00, double e01,
-                                  double e10, double e11, const double* __restrict__ eps_init,
-                                  double tol, int max_iter, double* partials, unsigned int* counter) {
+// Solve start for each selected replica: eps_bar, caps and the initial field
+// (linear_elastic_simulator.py:32-41), and partial sums of the antisymmetric
+// part's contribution to the first diff and norm.  grid = (G, nsel).
+__global__ void ls2d_begin_kernel(const Ls2dRep* reps, Ls2dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
-  Ls2dRep& R = reps[rep];
-  Ls2dState& S = st[rep];
+  const int r = sel[blockIdx.y];
+  const Ls2dRep& R = reps[r];
+  Ls2dState& S = st[r];
   const long long N = R.N;
+  const double e00 = R.eb[0], e01 = R.eb[1], e10 = R.eb[2], e11 = R.eb[3];
   const double abar = 0.5 * (e01 - e10);
   const double sbar = (e01 == e10) ? e01 : 0.5 * (e01 + e10);
+  const double* init = R.init;
   double d2 = 0, n2 = 0;
   double m00 = 0, m01 = 0, m10 = 0, m11 = 0;
-  if (eps_init) { m00 = S.means[0]; m01 = S.means[1]; m10 = S.means[2]; m11 = S.means[3]; }
+  if (init) { m00 = S.means[0]; m01 = S.means[1]; m10 = S.means[2]; m11 = S.means[3]; }
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
-    if (eps_init) {
-      const double4 v = reinterpret_cast<const double4*>(eps_init)[i];
-      const double xx = v.x + (e00 - m00), xy = v.y + (e01 - m01);
-      const double yx = v.z + (e10 - m10), yy = v.w + (e11 - m11);
-      R.eps[i] = xx;
-      R.eps[N + i] = yy;
-      R.eps[2 * N + i] = (xy == yx) ? xy : 0.5 * (xy + yx);
+    double xx, yy, sy;
+    if (init) {
+      const double4 v = reinterpret_cast<const double4*>(init)[i];
+      xx = v.x + (e00 - m00);
+      const double xy = v.y + (e01 - m01), yx = v.z + (e10 - m10);
+      yy = v.w + (e11 - m11);
+      sy = (xy == yx) ? xy : 0.5 * (xy + yx);
       const double a0 = 0.5 * (xy - yx);
       d2 += 2 * (abar - a0) * (abar - a0);
       n2 += 2 * a0 * a0;
     } else {
-      R.eps[i] = e00;
-      R.eps[N + i] = e11;
-      R.eps[2 * N + i] = sbar;
+      xx = e00; yy = e11; sy = sbar;
     }
+    R.eps[i] = xx;
+    R.eps[N + i] = yy;
+    R.eps[2 * N + i] = sy;
+    if (R.eps32) { R.eps32[i] = (float)xx; R.eps32[N + i] = (float)yy; R.eps32[2 * N + i] = (float)sy; }
   }
-  if (eps_init) {
+  if (init) {
     d2 = block_sum(d2, red);
     n2 = block_sum(n2, red);
-    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = d2; partials[2 * blockIdx.x + 1] = n2; }
+    if (threadIdx.x == 0) {
+      partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 8 + 0] = d2;
+      partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 8 + 1] = n2;
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    counter[1] = 0;
     S.ebar[0] = e00;
     S.ebar[1] = e11;
     S.ebar[2] = sbar;
     S.abar = abar;
-    S.tol = tol;
-    S.max_iter = max_iter;
     S.iter = 0;
-    S.done = max_iter <= 0 ? 1 : 0;
+    S.phase_iter = 0;
+    S.done = R.max_iter <= 0 ? 2 : 0;
     S.status = MGK_OK;
     S.diff = 0;
-    if (!eps_init) { S.extra_d0 = 0; S.extra_n0 = 2.0 * (double)N * abar * abar; }
+    if (!init) { S.extra_d0 = 0; S.extra_n0 = 2.0 * (double)N * abar * abar; }
   }
 }
 
-__global__ void ls2d_begin_finalize_kernel(Ls2dState* st, int rep, const double* partials, int nblocks) {
-  __shared__ double red[32];
-  double a = 0, b = 0;
-  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) { a += partials[2 * i]; b += partials[2 * i + 1]; }
-  a = block_sum(a, red);
-  b = block_sum(b, red);
-  if (threadIdx.x == 0) { st[rep].extra_d0 = a; st[rep].extra_n0 = b; }
-}
-
 // Row kernel.  IN_SPEC: the previous iteration's spectrum is inverted and the
-// field updated (with diff/norm); otherwise the field is read as is.
-template <typename T, bool IN_SPEC>
+// field updated (with diff/norm and the convergence decision); otherwise the
+// field is read as is (first tau of a phase).  FINAL: this phase's decision
+// is the last one (FP64 plans, or phase 2 of mixed plans).
+template <typename TS, typename TC, bool IN_SPEC, bool FINAL>
 __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict__ reps, Ls2dState* st,
-                                                      const int* __restrict__ row_map, double* partials,
-                                                      unsigned int* counter, int nrep,
+                                                      const int* __restrict__ row_map,
+                                                      const int* __restrict__ row_local, double* partials,
+                                                      unsigned int* rep_counter, Ls2dCtl* ctl,
                                                       cudaGraphConditionalHandle cond, int use_cond,
-                                                      int* any_active, int guard_cap) {
-  using C = C_t<T>;
+                                                      int guard_cap) {
+  using C = C_t<TC>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
   __shared__ int s_last;
@@ -267,168 +335,216 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
   const int r = row_map[item];
   const Ls2dRep& R = reps[r];
   Ls2dState& S = st[r];
-  const bool active = S.done == 0;
+  if (IN_SPEC && use_cond && item == 0 && threadIdx.x == 0) {
+    // a body with no active replica has no decider: stop here; the body
+    // count bounds the loop whatever happens to the deciders
+    const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap) {
+      ctl->any = 0;
+      cudaGraphSetConditional(cond, 0u);
+    }
+  }
+  if (S.done != 0) return;
+  const int ny = R.ny, nyh = R.nyh, ld = R.ld, nx = R.nx;
+  const long long N = R.N;
+  const int x0 = 2 * row_local[item];
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 3 * ny;
+  C* spec = reinterpret_cast<C*>(R.spec);
+  const double mu0 = S.mu0, lam0 = S.lam0;
+  const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
+  TS* eps = Fields<TS>::eps(R);
+  const TS* mu = Fields<TS>::mu(R);
+  const TS* lam = Fields<TS>::lam(R);
+  const TS* ep = Fields<TS>::ep(R);
+  const FftLen& fy = Fields<TS>::fy(R);
   double d2 = 0, n2 = 0;
-  if (active) {
-    const int ny = R.ny, nyh = R.nyh, ld = R.ld, nx = R.nx;
-    const long long N = R.N;
-    const int x0 = 2 * (item - R.row_base);
-    C* bufA = reinterpret_cast<C*>(smem_raw);
-    C* bufB = bufA + 3 * ny;
-    C* spec = reinterpret_cast<C*>(R.spec);
-    const double mu0 = S.mu0, lam0 = S.lam0;
-    const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
-    C* cur;  // holds the packed real rows (x0 real, x1 imag) of eps~ or nothing
-    if (IN_SPEC) {
-      for (int e = threadIdx.x; e < 3 * ny; e += blockDim.x) {
-        const int c = e / ny, k = e - c * ny;
-        const C* ra = spec + ((size_t)c * nx + x0) * ld;
-        const C* rb = ra + ld;
+  C* cur = bufA;
+  if (IN_SPEC) {
+    const int tot = 3 * ny;
+    for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
+      C av[4], bv[4];
+      int kk[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        kk[u] = -1;
+        if (e < tot) {
+          const int c = e / ny, k = e - c * ny;
+          const int ks = (2 * k <= ny) ? k : ny - k;
+          const C* ra = spec + ((size_t)c * nx + x0) * ld;
+          av[u] = ra[ks];
+          bv[u] = ra[ld + ks];
+          kk[u] = k;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (kk[u] < 0) continue;
+        const int e = e0 + u * blockDim.x, k = kk[u];
+        C a = av[u], b = bv[u];
         C z;
         if (2 * k <= ny) {
-          C a = ra[k], b = rb[k];
           if (k == 0 || 2 * k == ny) { a.y = 0; b.y = 0; }
           z = mk<C>(a.x - b.y, a.y + b.x);
         } else {
-          const C a = ra[ny - k], b = rb[ny - k];
           z = mk<C>(a.x + b.y, b.x - a.y);
         }
-        bufA[c * ny + k] = z;
+        bufA[e] = z;  // e = c * ny + k
       }
-      __syncthreads();
-      cur = fft_lines<+1>(bufA, bufB, 3, ny, R.fy);
-    }
-    C* out = (IN_SPEC && cur == bufA) ? bufB : bufA;
-    // update + tau (packed: real = row x0, imag = row x1)
-    for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-      T tr[2][3];
-      for (int h = 0; h < 2; ++h) {
-        const long long i = (long long)(x0 + h) * ny + y;
-        double e[3];
-        for (int c = 0; c < 3; ++c) {
-          const double old = R.eps[c * N + i];
-          if (IN_SPEC) {
-            const C z = cur[c * ny + y];
-            const double et = h == 0 ? (double)z.x : (double)z.y;
-            const double nw = (c == 0 ? eb0 : (c == 1 ? eb1 : eb2)) + et;
-            const double dd = nw - old;
-            const double w = c == 2 ? 2.0 : 1.0;
-            d2 += w * dd * dd;
-            n2 += w * old * old;
-            R.eps[c * N + i] = nw;
-            e[c] = nw;
-          } else {
-            e[c] = old;
-          }
-        }
-        const double mu = R.mu[i], lam = R.lam[i];
-        const double dxx = e[0] - R.ep[i], dyy = e[1] - R.ep[N + i], dxy = e[2] - R.ep[2 * N + i];
-        const double trd = dxx + dyy, tre = e[0] + e[1];
-        tr[h][0] = (T)((2 * mu * dxx + lam * trd) - (2 * mu0 * e[0] + lam0 * tre));
-        tr[h][1] = (T)((2 * mu * dyy + lam * trd) - (2 * mu0 * e[1] + lam0 * tre));
-        tr[h][2] = (T)(2 * mu * dxy - 2 * mu0 * e[2]);
-      }
-      for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
     }
     __syncthreads();
-    C* scratch = (out == bufA) ? bufB : bufA;
-    C* Z = fft_lines<-1>(out, scratch, 3, ny, R.fy);
-    // unpack the two real rows' half spectra
-    for (int e = threadIdx.x; e < 3 * nyh; e += blockDim.x) {
-      const int c = e / nyh, k = e - c * nyh;
-      const C z = Z[c * ny + k];
-      const C w = Z[c * ny + (k == 0 ? 0 : ny - k)];
-      C* ra = spec + ((size_t)c * nx + x0) * ld;
-      ra[k] = mk<C>(T(0.5) * (z.x + w.x), T(0.5) * (z.y - w.y));
-      ra[ld + k] = mk<C>(T(0.5) * (z.y + w.y), T(-0.5) * (z.x - w.x));
+    cur = fft_lines<+1>(bufA, bufB, 3, ny, fy);
+  }
+  C* out = (IN_SPEC && cur == bufA) ? bufB : bufA;
+  for (int y = threadIdx.x; y < ny; y += blockDim.x) {
+    TC tr[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long i = (long long)(x0 + h) * ny + y;
+      double e[3];
+      const double o0 = (double)eps[i], o1 = (double)eps[N + i], o2 = (double)eps[2 * N + i];
+      const double m = (double)mu[i], l = (double)lam[i];
+      const double p0 = (double)ep[i], p1 = (double)ep[N + i], p2 = (double)ep[2 * N + i];
+      if (IN_SPEC) {
+        const C z0 = cur[y], z1 = cur[ny + y], z2 = cur[2 * ny + y];
+        e[0] = eb0 + (double)(h == 0 ? z0.x : z0.y);
+        e[1] = eb1 + (double)(h == 0 ? z1.x : z1.y);
+        e[2] = eb2 + (double)(h == 0 ? z2.x : z2.y);
+        const double q0 = e[0] - o0, q1 = e[1] - o1, q2 = e[2] - o2;
+        d2 += q0 * q0 + q1 * q1 + 2.0 * q2 * q2;
+        n2 += o0 * o0 + o1 * o1 + 2.0 * o2 * o2;
+        eps[i] = (TS)e[0];
+        eps[N + i] = (TS)e[1];
+        eps[2 * N + i] = (TS)e[2];
+      } else {
+        e[0] = o0; e[1] = o1; e[2] = o2;
+      }
+      const double dxx = e[0] - p0, dyy = e[1] - p1, dxy = e[2] - p2;
+      const double trd = dxx + dyy, tre = e[0] + e[1];
+      tr[h][0] = (TC)((2 * m * dxx + l * trd) - (2 * mu0 * e[0] + lam0 * tre));
+      tr[h][1] = (TC)((2 * m * dyy + l * trd) - (2 * mu0 * e[1] + lam0 * tre));
+      tr[h][2] = (TC)(2 * m * dxy - 2 * mu0 * e[2]);
     }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
+  }
+  __syncthreads();
+  C* scratch = (out == bufA) ? bufB : bufA;
+  C* Z = fft_lines<-1>(out, scratch, 3, ny, fy);
+  for (int e = threadIdx.x; e < 3 * nyh; e += blockDim.x) {
+    const int c = e / nyh, k = e - c * nyh;
+    const C z = Z[c * ny + k];
+    const C w = Z[c * ny + (k == 0 ? 0 : ny - k)];
+    C* ra = spec + ((size_t)c * nx + x0) * ld;
+    ra[k] = mk<C>(TC(0.5) * (z.x + w.x), TC(0.5) * (z.y - w.y));
+    ra[ld + k] = mk<C>(TC(0.5) * (z.y + w.y), TC(-0.5) * (z.x - w.x));
   }
   if (!IN_SPEC) return;
-  // partial sums -> fixed slot; the last CTA to finish reduces and decides
+  // partial sums -> fixed slot; the replica's last CTA reduces and decides
   d2 = block_sum(d2, red);
   n2 = block_sum(n2, red);
   if (threadIdx.x == 0) {
     partials[2 * item] = d2;
     partials[2 * item + 1] = n2;
     __threadfence();
-    // wraps back to 0 on the last arrival, so the counter resets itself
-    const unsigned int t = atomicInc(counter, gridDim.x - 1);
-    s_last = (t == gridDim.x - 1);
-    if (item == 0 && use_cond) {
-      // independent bound on the number of loop bodies: counter[1] is reset by
-      // the begin kernel; a loop that outlives every replica's cap is stopped
-      const unsigned int g = atomicAdd(counter + 1, 1u);
-      if (g > (unsigned int)guard_cap) cudaGraphSetConditional(cond, 0u);
-    }
+    const unsigned int t = atomicInc(&rep_counter[r], (unsigned int)R.row_items - 1);  // self-resetting
+    s_last = (t == (unsigned int)R.row_items - 1);
   }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  int any = 0;
-  for (int q = 0; q < nrep; ++q) {
-    Ls2dState& Q = st[q];
-    if (Q.done) continue;
-    const Ls2dRep& P = reps[q];
-    double a = 0, b = 0;
-    for (int i = threadIdx.x; i < P.row_items; i += blockDim.x) {
-      a += __ldcg(&partials[2 * (P.row_base + i)]);
-      b += __ldcg(&partials[2 * (P.row_base + i) + 1]);
-    }
-    a = block_sum(a, red);
-    b = block_sum(b, red);
-    if (threadIdx.x == 0) {
-      if (Q.iter == 0) { a += Q.extra_d0; b += Q.extra_n0; }
-      else { b += 2.0 * (double)P.N * Q.abar * Q.abar; }
-      const double diff = sqrt(a) / (sqrt(b) + 1e-20);
-      Q.diff = diff;
-      Q.iter += 1;
-      if (!isfinite(diff)) { Q.done = 1; Q.status = MGK_NONFINITE; }
-      else if (diff < Q.tol) { Q.done = 1; Q.status = MGK_OK; }
-      else if (Q.iter >= Q.max_iter) { Q.done = 1; Q.status = MGK_NOT_CONVERGED; }
-      else any = 1;
-    }
-    __syncthreads();
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < R.row_items; i += blockDim.x) {
+    a += __ldcg(&partials[2 * (R.row_first + i)]);
+    b += __ldcg(&partials[2 * (R.row_first + i) + 1]);
   }
-  if (threadIdx.x == 0) {
-    *any_active = any;
-    if (use_cond) {
-      const bool over = atomicAdd(counter + 1, 0u) > (unsigned int)guard_cap;
-      cudaGraphSetConditional(cond, (any && !over) ? 1u : 0u);
-    }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x != 0) return;
+  if (S.iter == 0) { a += S.extra_d0; b += S.extra_n0; }
+  else { b += 2.0 * (double)N * S.abar * S.abar; }
+  const double diff = sqrt(a) / (sqrt(b) + 1e-20);
+  S.diff = diff;
+  S.iter += 1;
+  S.phase_iter += 1;
+  int keep = 0;
+  if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
+  else if (FINAL) {
+    if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
+    else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
+    else keep = 1;
+  } else {
+    const double tol1 = R.tol > kMixedPhase1Tol ? R.tol : kMixedPhase1Tol;
+    if (S.iter >= R.max_iter) { S.done = 2; S.status = diff < R.tol ? MGK_OK : MGK_NOT_CONVERGED; }
+    else if (diff < tol1 || S.phase_iter >= kMixedPhase1Cap) S.done = 1;
+    else keep = 1;
+  }
+  const unsigned int n_act = ctl->n_active;  // stable until every active replica has decided
+  if (keep) atomicAdd(&ctl->still, 1u);
+  __threadfence();
+  const unsigned int d = atomicAdd(&ctl->decided, 1u);
+  if (d == n_act - 1) {
+    __threadfence();
+    const unsigned int still = atomicExch(&ctl->still, 0u);
+    ctl->decided = 0;
+    ctl->n_active = still;
+    const bool go = still > 0 && atomicAdd(&ctl->bodies, 0u) <= (unsigned int)guard_cap;
+    ctl->any = go ? 1 : 0;
+    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
   }
 }
 
 // Column kernel: FFT along x, Gamma0_sym, inverse FFT along x, for a tile of
 // tc consecutive ky columns and all three components.
-template <typename T>
+template <typename TS, typename TC>
 __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict__ reps,
                                                       const Ls2dState* __restrict__ st,
-                                                      const int* __restrict__ col_map) {
-  using C = C_t<T>;
+                                                      const int* __restrict__ col_map,
+                                                      const int* __restrict__ col_local) {
+  using C = C_t<TC>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int item = blockIdx.x;
   const int r = col_map[item];
   const Ls2dRep& R = reps[r];
   const Ls2dState& S = st[r];
-  if (S.done) return;
+  if (S.done != 0) return;
   const int nx = R.nx, ny = R.ny, nyh = R.nyh, ld = R.ld, tc = R.tc;
-  const int ky0 = (item - R.col_base) * tc;
+  const int ky0 = col_local[item] * tc;
   const int tcw = min(tc, nyh - ky0);
+  const FftLen& fx = Fields<TS>::fx(R);
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + 3 * tc * nx;
   C* spec = reinterpret_cast<C*>(R.spec);
   const int tot = 3 * tcw * nx;
-  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
-    const int c = e / (tcw * nx);
-    const int rem = e - c * tcw * nx;
-    const int x = rem / tcw, t = rem - x * tcw;
-    bufA[(c * tc + t) * nx + x] = spec[((size_t)c * nx + x) * ld + ky0 + t];
+  for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < tot) {
+        const int c = e / (tcw * nx);
+        const int rem = e - c * tcw * nx;
+        const int x = rem / tcw, t = rem - x * tcw;
+        v[u] = spec[((size_t)c * nx + x) * ld + ky0 + t];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < tot) {
+        const int c = e / (tcw * nx);
+        const int rem = e - c * tcw * nx;
+        const int x = rem / tcw, t = rem - x * tcw;
+        bufA[(c * tc + t) * nx + x] = v[u];
+      }
+    }
   }
   __syncthreads();
-  // lines: (c * tc + t), only t < tcw are meaningful; transform all 3*tc lines
-  C* F = fft_lines<-1>(bufA, bufB, 3 * tc, nx, R.fx);
-  const T inv2mu0 = (T)S.inv2mu0, Bc = (T)S.Bc;
-  const double scale = 1.0 / ((double)nx * (double)ny);
+  // lines (c * tc + t); only t < tcw are meaningful, all 3*tc are transformed
+  C* F = fft_lines<-1>(bufA, bufB, 3 * tc, nx, fx);
+  const TC inv2mu0 = (TC)S.inv2mu0, Bc = (TC)S.Bc;
+  const TC sc = (TC)(1.0 / ((double)nx * (double)ny));
   for (int e = threadIdx.x; e < tcw * nx; e += blockDim.x) {
     const int t = e / nx, kx = e - t * nx;
     const int ky = ky0 + t;
@@ -436,34 +552,31 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
     C* pyy = &F[(1 * tc + t) * nx + kx];
     C* pxy = &F[(2 * tc + t) * nx + kx];
     if (kx == 0 && ky == 0) {
-      *pxx = mk<C>(T(0), T(0)); *pyy = *pxx; *pxy = *pxx;
+      *pxx = mk<C>(TC(0), TC(0)); *pyy = *pxx; *pxy = *pxx;
       continue;
     }
     // fftfreq signs matter where several axes sit on their Nyquist line
     const double ux = (double)fftfreq(kx, nx) / nx, uy = (double)fftfreq(ky, ny) / ny;
     const double inv = 1.0 / sqrt(ux * ux + uy * uy);
-    const T nxv = (T)(ux * inv), nyv = (T)(uy * inv);
-    C txx = *pxx, tyy = *pyy, txy = *pxy;
+    const TC nxv = (TC)(ux * inv), nyv = (TC)(uy * inv);
+    const C txx = *pxx, tyy = *pyy, txy = *pxy;
     C exx, eyy, exy;
     gamma2d_apply(txx, tyy, txy, nxv, nyv, inv2mu0, Bc, exx, eyy, exy);
-    const bool nyq = ((nx & 1) == 0 && 2 * kx == nx) || ((ny & 1) == 0 && 2 * ky == ny);
-    if (nyq) {
-      const T sx = ((nx & 1) == 0 && 2 * kx == nx) ? -nxv : nxv;
-      const T sy = ((ny & 1) == 0 && 2 * ky == ny) ? -nyv : nyv;
+    const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqy = (ny & 1) == 0 && 2 * ky == ny;
+    if (nqx || nqy) {
       C fxx, fyy, fxy;
-      gamma2d_apply(txx, tyy, txy, sx, sy, inv2mu0, Bc, fxx, fyy, fxy);
-      exx = mk<C>(T(0.5) * (exx.x + fxx.x), T(0.5) * (exx.y + fxx.y));
-      eyy = mk<C>(T(0.5) * (eyy.x + fyy.x), T(0.5) * (eyy.y + fyy.y));
-      exy = mk<C>(T(0.5) * (exy.x + fxy.x), T(0.5) * (exy.y + fxy.y));
+      gamma2d_apply(txx, tyy, txy, nqx ? -nxv : nxv, nqy ? -nyv : nyv, inv2mu0, Bc, fxx, fyy, fxy);
+      exx = mk<C>(TC(0.5) * (exx.x + fxx.x), TC(0.5) * (exx.y + fxx.y));
+      eyy = mk<C>(TC(0.5) * (eyy.x + fyy.x), TC(0.5) * (eyy.y + fyy.y));
+      exy = mk<C>(TC(0.5) * (exy.x + fxy.x), TC(0.5) * (exy.y + fxy.y));
     }
-    const T sc = (T)scale;
     *pxx = mk<C>(exx.x * sc, exx.y * sc);
     *pyy = mk<C>(eyy.x * sc, eyy.y * sc);
     *pxy = mk<C>(exy.x * sc, exy.y * sc);
   }
   __syncthreads();
   C* G = (F == bufA) ? bufB : bufA;
-  C* Rz = fft_lines<+1>(F, G, 3 * tc, nx, R.fx);
+  C* Rz = fft_lines<+1>(F, G, 3 * tc, nx, fx);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * nx);
     const int rem = e - c * tcw * nx;
@@ -472,15 +585,44 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
   }
 }
 
+// Mixed plans, between the phases: FP64 field from the FP32 one.
+// grid = (G, nsel).
+__global__ void ls2d_promote_kernel(const Ls2dRep* reps, const int* sel) {
+  const int r = sel[blockIdx.y];
+  const Ls2dRep& R = reps[r];
+  const long long n3 = 3 * R.N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3;
+       i += (long long)gridDim.x * blockDim.x)
+    R.eps[i] = (double)R.eps32[i];
+}
+
+// Replicas that finished phase 1 re-enter for phase 2; resets the control block.
+__global__ void ls2d_phase2_kernel(Ls2dState* st, const int* sel, int nsel, Ls2dCtl* ctl) {
+  if (threadIdx.x != 0) return;
+  unsigned int n = 0;
+  for (int q = 0; q < nsel; ++q) {
+    Ls2dState& S = st[sel[q]];
+    if (S.done == 1) { S.done = 0; S.phase_iter = 0; ++n; }
+  }
+  ctl->n_active = n;
+  ctl->decided = 0;
+  ctl->still = 0;
+  ctl->bodies = 0;
+  ctl->any = n > 0;
+}
+
 // Outputs in the reference layout: eps, sig (nx,ny,2,2) and partial sums of
 // their components for the means (linear_elastic_simulator.py:83-88).
-__global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, int rep, double* eps_out,
-                                   double* sig_out, double* partials) {
+// grid = (G, nsel).
+__global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
-  const Ls2dRep& R = reps[rep];
-  const Ls2dState& S = st[rep];
+  const int r = sel[blockIdx.y];
+  const Ls2dRep& R = reps[r];
+  const Ls2dState& S = st[r];
   const long long N = R.N;
   const double abar = S.abar;
+  double* eps_out = R.out_eps;
+  double* sig_out = R.out_sig;
   double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
@@ -503,7 +645,7 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, int
   }
   for (int q = 0; q < 8; ++q) {
     double t = block_sum(s[q], red);
-    if (threadIdx.x == 0) partials[8 * blockIdx.x + q] = t;
+    if (threadIdx.x == 0) partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 8 + q] = t;
   }
 }
 
@@ -512,51 +654,82 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, int
 // ================================================================== plan ===
 using namespace mgk;
 
-struct mgk_ls2d_plan {
-  int nx, ny, nyh, ld, tc, plane_mode, prec;
-  long long N;
-  int row_items, col_items;
-  size_t row_smem, col_smem;
-  Ls2dRep h_rep;
-  Ls2dRep* d_rep = nullptr;
-  Ls2dState* d_st = nullptr;
-  int* d_rowmap = nullptr;
-  int* d_colmap = nullptr;
-  double* d_part = nullptr;
-  int n_part = 0;
-  unsigned int* d_counter = nullptr;
-  int* d_any = nullptr;
-  double* d_fields = nullptr;
-  void* d_spec = nullptr;
-  bool has_material = false;
-  bool has_epa = false;
-  // loop graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int graph_mode = -1;  // -1 untried, 1 while-node graph, 0 host loop
-  int guard_cap = 0;     // loop-body bound baked into the graph (max_iter of the build + 2)
-  Ls2dState* h_state = nullptr;  // pinned
-  int* h_any = nullptr;          // pinned
-};
+namespace {
 
-static int grid_for(long long N) {
-  long long b = (N + 255) / 256;
-  if (b > 2048) b = 2048;
+constexpr int kThreads = 256;
+constexpr int kPerVoxelBlocks = 256;  // G: CTAs per replica for per-voxel kernels
+
+int grid_blocks(long long maxN) {
+  long long b = (maxN + kThreads - 1) / kThreads;
+  if (b > kPerVoxelBlocks) b = kPerVoxelBlocks;
   if (b < 1) b = 1;
   return (int)b;
 }
 
-template <typename T>
-static int ls2d_configure(mgk_ls2d_t p) {
-  using C = C_t<T>;
-  p->row_smem = 2 * 3 * (size_t)p->ny * sizeof(C);
-  p->col_smem = 2 * 3 * (size_t)p->tc * p->nx * sizeof(C);
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)p->row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)p->row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_col_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)p->col_smem));
+// columns per CTA: largest power of two <= 8 whose double-buffered tile fits
+// `cap` bytes (keeps several CTAs resident per SM)
+int pick_tc(int nx, size_t csz, size_t cap) {
+  int tc = 8;
+  while (tc > 1 && 2 * 3 * (size_t)tc * nx * csz > cap) tc >>= 1;
+  return tc;
+}
+
+}  // namespace
+
+struct mgk_ls2d_plan {
+  int nrep = 0;
+  int plane_mode = 0, prec = 0;
+  long long maxN = 0;
+  size_t row_smem = 0, col_smem = 0;
+  std::vector<Ls2dRep> reps;      // host copy (static part)
+  std::vector<char> has_material;
+  Ls2dRep* h_reps = nullptr;      // pinned staging of the table
+  int* h_maps = nullptr;          // pinned staging: row_map, row_local, col_map, col_local, sel
+  Ls2dCtl* h_ctl = nullptr;
+  Ls2dState* h_state = nullptr;
+  cudaEvent_t staged = nullptr;   // last upload from the staging buffers
+  bool staged_pending = false;
+  Ls2dRep* d_reps = nullptr;
+  Ls2dState* d_st = nullptr;
+  Ls2dCtl* d_ctl = nullptr;
+  int* d_maps = nullptr;
+  unsigned int* d_repctr = nullptr;
+  double* d_part = nullptr;
+  double* d_mat_part = nullptr;   // partials of the material kernel
+  size_t part_doubles = 0;
+  int total_row_items = 0, total_col_items = 0;
+  std::vector<void*> allocations;
+  // loop graph for the current selection
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_mode = -1;  // -1 untried, 1 while-node graph, 0 host loop
+  int graph_cap = 0;
+  // selection of the last call
+  int nsel = 0, sel_rows = 0, sel_cols = 0;
+};
+
+static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
+  if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("mgk_ls2d: cudaMalloc of %zu bytes failed", bytes);
+    return MGK_OOM;
+  }
+  p->allocations.push_back(*ptr);
+  return MGK_OK;
+}
+
+template <typename TS, typename TC>
+static int ls2d_set_attrs(size_t row_smem, size_t col_smem) {
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(ls2d_col_kernel<TS, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)col_smem));
   return MGK_OK;
 }
 
@@ -564,247 +737,462 @@ extern "C" int mgk_ls2d_destroy(mgk_ls2d_t p) {
   if (!p) return MGK_OK;
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  cudaFree(p->d_rep);
-  cudaFree(p->d_st);
-  cudaFree(p->d_rowmap);
-  cudaFree(p->d_colmap);
-  cudaFree(p->d_part);
-  cudaFree(p->d_counter);
-  cudaFree(p->d_any);
-  cudaFree(p->d_fields);
-  cudaFree(p->d_spec);
+  if (p->staged) cudaEventDestroy(p->staged);
+  for (void* a : p->allocations) cudaFree(a);
+  if (p->h_reps) cudaFreeHost(p->h_reps);
+  if (p->h_maps) cudaFreeHost(p->h_maps);
+  if (p->h_ctl) cudaFreeHost(p->h_ctl);
   if (p->h_state) cudaFreeHost(p->h_state);
-  if (p->h_any) cudaFreeHost(p->h_any);
   delete p;
   return MGK_OK;
 }
 
-extern "C" int mgk_ls2d_create(int nx, int ny, int plane_mode, int precision, mgk_ls2d_t* out) {
-  MGK_REQUIRE(out != nullptr, "mgk_ls2d_create: null output handle");
+extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, int plane_mode, int precision,
+                                     mgk_ls2d_t* out) {
+  MGK_REQUIRE(out != nullptr, "mgk_ls2d_create_batch: null output handle");
   *out = nullptr;
+  MGK_REQUIRE(nrep >= 1 && nrep <= 65535 && nxs && nys, "mgk_ls2d_create_batch: bad replica count");
   MGK_REQUIRE(plane_mode == MGK_PLANE_STRAIN || plane_mode == MGK_PLANE_STRESS,
               "mgk_ls2d_create: plane_mode must be 0 (strain) or 1 (stress)");
-  MGK_REQUIRE(precision == MGK_FP64 || precision == MGK_FP32, "mgk_ls2d_create: bad precision");
-  FftLen fx, fy;
-  MGK_REQUIRE(fft_schedule(nx, &fx) && fft_schedule(ny, &fy),
-              "mgk_ls2d_create: grid %dx%d unsupported (each side must be 2^a 3^b, even, 4..4096)", nx, ny);
+  MGK_REQUIRE(precision == MGK_FP64 || precision == MGK_MIXED, "mgk_ls2d_create: bad precision");
+  for (int r = 0; r < nrep; ++r) {
+    FftLen f;
+    MGK_REQUIRE(fft_schedule(nxs[r], &f) && fft_schedule(nys[r], &f),
+                "mgk_ls2d_create: grid %dx%d unsupported (each side must be 2^a 3^b, even, 4..4096)", nxs[r],
+                nys[r]);
+    MGK_REQUIRE(2 * 3 * (size_t)nys[r] * sizeof(double2) <= 220 * 1024 &&
+                    2 * 3 * (size_t)pick_tc(nxs[r], sizeof(double2), 64 * 1024) * nxs[r] * sizeof(double2) <=
+                        220 * 1024,
+                "mgk_ls2d_create: grid too large for the shared-memory FFT");
+  }
   mgk_ls2d_t p = new mgk_ls2d_plan();
-  p->nx = nx; p->ny = ny; p->nyh = ny / 2 + 1; p->ld = p->nyh;
-  p->plane_mode = plane_mode; p->prec = precision;
-  p->N = (long long)nx * ny;
-  const size_t csz = precision == MGK_FP64 ? sizeof(double2) : sizeof(float2);
-  // columns per CTA: largest power of two <= 8 whose tile fits in ~200 KB
-  int tc = 8;
-  while (tc > 1 && 2 * 3 * (size_t)tc * nx * csz > 200 * 1024) tc >>= 1;
-  p->tc = tc;
-  MGK_REQUIRE(2 * 3 * (size_t)tc * nx * csz <= 220 * 1024 && 2 * 3 * (size_t)ny * csz <= 220 * 1024,
-              "mgk_ls2d_create: grid too large for the shared-memory FFT");
-  p->row_items = nx / 2;
-  p->col_items = (p->nyh + tc - 1) / tc;
-  int st = precision == MGK_FP64 ? ls2d_configure<double>(p) : ls2d_configure<float>(p);
-  if (st != MGK_OK) { delete p; return st; }
-  const long long N = p->N;
-  const size_t spec_bytes = 3 * (size_t)nx * p->ld * csz;
+  p->nrep = nrep;
+  p->plane_mode = plane_mode;
+  p->prec = precision;
+  const bool mixed = precision == MGK_MIXED;
+  const size_t c64 = sizeof(double2);
   auto fail = [&](int s) { mgk_ls2d_destroy(p); return s; };
-  if (cudaMalloc(&p->d_fields, sizeof(double) * N * 13) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_spec, spec_bytes) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_rep, sizeof(Ls2dRep)) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_st, sizeof(Ls2dState)) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_rowmap, sizeof(int) * p->row_items) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_colmap, sizeof(int) * p->col_items) != cudaSuccess) return fail(MGK_OOM);
-  p->n_part = 2048;
-  if (p->n_part < p->row_items) p->n_part = p->row_items;
-  if (cudaMalloc(&p->d_part, sizeof(double) * 8 * p->n_part) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_counter, 2 * sizeof(unsigned int)) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMalloc(&p->d_any, sizeof(int)) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMallocHost(&p->h_state, sizeof(Ls2dState)) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMemset(p->d_counter, 0, 2 * sizeof(unsigned int)) != cudaSuccess) return fail(MGK_CUDA_ERROR);
-  if (cudaMallocHost(&p->h_any, sizeof(int)) != cudaSuccess) return fail(MGK_OOM);
-  if (cudaMemset(p->d_st, 0, sizeof(Ls2dState)) != cudaSuccess) return fail(MGK_CUDA_ERROR);
-  fx.tw = twiddles(nx, precision);
-  fy.tw = twiddles(ny, precision);
-  if (!fx.tw || !fy.tw) return fail(MGK_OOM);
-  Ls2dRep& R = p->h_rep;
-  memset(&R, 0, sizeof(R));
-  R.nx = nx; R.ny = ny; R.nyh = p->nyh; R.ld = p->ld;
-  R.row_base = 0; R.row_items = p->row_items; R.col_base = 0; R.col_items = p->col_items; R.tc = tc;
-  R.N = N; R.fx = fx; R.fy = fy;
-  double* f = p->d_fields;
-  R.mu = f; R.lam = f + N; R.eps = f + 2 * N; R.ep = f + 5 * N; R.epa = nullptr;
-  R.spec = p->d_spec;
-  std::vector<int> rm(p->row_items, 0), cm(p->col_items, 0);
-  if (cudaMemcpy(p->d_rowmap, rm.data(), sizeof(int) * rm.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(p->d_colmap, cm.data(), sizeof(int) * cm.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(p->d_rep, &R, sizeof(R), cudaMemcpyHostToDevice) != cudaSuccess)
+  p->reps.resize(nrep);
+  p->has_material.assign(nrep, 0);
+  size_t row_smem = 0, col_smem = 0;
+  for (int r = 0; r < nrep; ++r) {
+    const int nx = nxs[r], ny = nys[r];
+    Ls2dRep& R = p->reps[r];
+    memset(&R, 0, sizeof(R));
+    R.nx = nx; R.ny = ny; R.nyh = ny / 2 + 1; R.ld = R.nyh;
+    R.N = (long long)nx * ny;
+    R.tc = pick_tc(nx, c64, 64 * 1024);
+    R.row_items = nx / 2;
+    R.col_items = (R.nyh + R.tc - 1) / R.tc;
+    fft_schedule(nx, &R.fx64);
+    fft_schedule(ny, &R.fy64);
+    R.fx32 = R.fx64;
+    R.fy32 = R.fy64;
+    R.fx64.tw = twiddles(nx, MGK_FP64);
+    R.fy64.tw = twiddles(ny, MGK_FP64);
+    if (!R.fx64.tw || !R.fy64.tw) return fail(MGK_OOM);
+    if (mixed) {
+      R.fx32.tw = twiddles(nx, 1 /* float table */);
+      R.fy32.tw = twiddles(ny, 1 /* float table */);
+      if (!R.fx32.tw || !R.fy32.tw) return fail(MGK_OOM);
+    }
+    row_smem = std::max(row_smem, 2 * 3 * (size_t)ny * c64);
+    col_smem = std::max(col_smem, 2 * 3 * (size_t)R.tc * nx * c64);
+    p->maxN = std::max(p->maxN, R.N);
+    p->total_row_items += R.row_items;
+    p->total_col_items += R.col_items;
+    void* f = nullptr;
+    int st = plan_alloc(p, &f, sizeof(double) * R.N * 10);
+    if (st) return fail(st);
+    double* d = reinterpret_cast<double*>(f);
+    R.mu = d; R.lam = d + R.N; R.eps = d + 2 * R.N; R.ep = d + 5 * R.N; R.epa = nullptr;
+    st = plan_alloc(p, &R.spec, 3 * (size_t)nx * R.ld * c64);
+    if (st) return fail(st);
+    if (mixed) {
+      void* g = nullptr;
+      st = plan_alloc(p, &g, sizeof(float) * R.N * 8);
+      if (st) return fail(st);
+      float* fl = reinterpret_cast<float*>(g);
+      R.mu32 = fl; R.lam32 = fl + R.N; R.eps32 = fl + 2 * R.N; R.ep32 = fl + 5 * R.N;
+    }
+  }
+  p->row_smem = row_smem;
+  p->col_smem = col_smem;
+  int st = ls2d_set_attrs<double, double>(row_smem, col_smem);
+  if (st == MGK_OK && mixed) st = ls2d_set_attrs<float, float>(row_smem / 2, col_smem / 2);
+  if (st) return fail(st);
+  const int G = grid_blocks(p->maxN);
+  p->part_doubles = std::max((size_t)2 * p->total_row_items, (size_t)nrep * G * 8);
+  void* v = nullptr;
+  if ((st = plan_alloc(p, &v, sizeof(double) * p->part_doubles))) return fail(st);
+  p->d_part = reinterpret_cast<double*>(v);
+  if ((st = plan_alloc(p, &v, sizeof(double) * 2 * kPerVoxelBlocks))) return fail(st);
+  p->d_mat_part = reinterpret_cast<double*>(v);
+  if ((st = plan_alloc(p, &v, sizeof(Ls2dRep) * nrep))) return fail(st);
+  p->d_reps = reinterpret_cast<Ls2dRep*>(v);
+  if ((st = plan_alloc(p, &v, sizeof(Ls2dState) * nrep))) return fail(st);
+  p->d_st = reinterpret_cast<Ls2dState*>(v);
+  if ((st = plan_alloc(p, &v, sizeof(Ls2dCtl)))) return fail(st);
+  p->d_ctl = reinterpret_cast<Ls2dCtl*>(v);
+  const size_t nmaps = 2 * (size_t)p->total_row_items + 2 * (size_t)p->total_col_items + nrep;
+  if ((st = plan_alloc(p, &v, sizeof(int) * nmaps))) return fail(st);
+  p->d_maps = reinterpret_cast<int*>(v);
+  if ((st = plan_alloc(p, &v, sizeof(unsigned int) * nrep))) return fail(st);
+  p->d_repctr = reinterpret_cast<unsigned int*>(v);
+  if (cudaMemset(p->d_repctr, 0, sizeof(unsigned int) * nrep) != cudaSuccess ||
+      cudaMemset(p->d_st, 0, sizeof(Ls2dState) * nrep) != cudaSuccess ||
+      cudaMemset(p->d_ctl, 0, sizeof(Ls2dCtl)) != cudaSuccess)
+    return fail(MGK_CUDA_ERROR);
+  if (cudaMallocHost(&p->h_reps, sizeof(Ls2dRep) * nrep) != cudaSuccess ||
+      cudaMallocHost(&p->h_maps, sizeof(int) * nmaps) != cudaSuccess ||
+      cudaMallocHost(&p->h_ctl, sizeof(Ls2dCtl)) != cudaSuccess ||
+      cudaMallocHost(&p->h_state, sizeof(Ls2dState) * nrep) != cudaSuccess)
+    return fail(MGK_OOM);
+  if (cudaEventCreateWithFlags(&p->staged, cudaEventDisableTiming) != cudaSuccess) return fail(MGK_CUDA_ERROR);
+  memcpy(p->h_reps, p->reps.data(), sizeof(Ls2dRep) * nrep);
+  if (cudaMemcpy(p->d_reps, p->h_reps, sizeof(Ls2dRep) * nrep, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(MGK_CUDA_ERROR);
   *out = p;
   return MGK_OK;
 }
 
-static int ls2d_upload_rep(mgk_ls2d_t p, cudaStream_t s) {
-  MGK_CUDA(cudaMemcpyAsync(p->d_rep, &p->h_rep, sizeof(Ls2dRep), cudaMemcpyHostToDevice, s));
+extern "C" int mgk_ls2d_create(int nx, int ny, int plane_mode, int precision, mgk_ls2d_t* out) {
+  return mgk_ls2d_create_batch(1, &nx, &ny, plane_mode, precision, out);
+}
+
+// wait until the previous upload from the pinned staging buffers has run
+static int staging_wait(mgk_ls2d_t p) {
+  if (p->staged_pending) {
+    MGK_CUDA(cudaEventSynchronize(p->staged));
+    p->staged_pending = false;
+  }
   return MGK_OK;
 }
 
-static int ls2d_set_fields(mgk_ls2d_t p, const double* E, const double* nu, const double* epsp,
+static int ls2d_set_fields(mgk_ls2d_t p, int rep, const double* E, const double* nu, const double* epsp,
                            int set_moduli, cudaStream_t s) {
-  // eigenstrain asymmetry must be known before the kernel: scan on the host
-  // side is impossible for device data, so keep the xy/yx planes whenever a
-  // field is given and let the kernel store both (cheap, 2 extra planes).
+  Ls2dRep& R = p->reps[rep];
   const bool want_epa = epsp != nullptr;
-  if (want_epa != (p->h_rep.epa != nullptr)) {
-    p->h_rep.epa = want_epa ? p->d_fields + 8 * p->N : nullptr;
-    p->h_rep.has_epa = want_epa;
-    int st = ls2d_upload_rep(p, s);
+  if (want_epa != (R.epa != nullptr)) {
+    R.epa = want_epa ? R.mu + 8 * R.N : nullptr;
+    int st = staging_wait(p);
     if (st) return st;
+    p->h_reps[rep] = R;
+    MGK_CUDA(cudaMemcpyAsync(&p->d_reps[rep], &p->h_reps[rep], sizeof(Ls2dRep), cudaMemcpyHostToDevice, s));
+    MGK_CUDA(cudaEventRecord(p->staged, s));
+    p->staged_pending = true;
   }
-  const int grid = grid_for(p->N);
-  ls2d_material_kernel<<<grid, 256, 0, s>>>(p->d_rep, 0, E, nu, epsp, p->plane_mode, set_moduli, p->d_part);
+  const int grid = grid_blocks(R.N);
+  ls2d_material_kernel<<<grid, kThreads, 0, s>>>(p->d_reps, rep, E, nu, epsp, p->plane_mode, set_moduli,
+                                                 p->d_mat_part);
   MGK_CUDA(cudaGetLastError());
   if (set_moduli) {
-    ls2d_medium_kernel<<<1, 256, 0, s>>>(p->d_rep, p->d_st, 0, p->d_part, grid, p->plane_mode);
+    ls2d_medium_kernel<<<1, kThreads, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, grid, p->plane_mode);
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
 }
 
-extern "C" int mgk_ls2d_set_material(mgk_ls2d_t p, const double* E, const double* nu, const double* epsp,
-                                     mgk_stream_t stream) {
+extern "C" int mgk_ls2d_set_material_rep(mgk_ls2d_t p, int rep, const double* E, const double* nu,
+                                         const double* epsp, mgk_stream_t stream) {
   MGK_REQUIRE(p && E && nu, "mgk_ls2d_set_material: null argument");
-  int st = ls2d_set_fields(p, E, nu, epsp, 1, (cudaStream_t)stream);
-  if (st == MGK_OK) p->has_material = true;
+  MGK_REQUIRE(rep >= 0 && rep < p->nrep, "mgk_ls2d_set_material: replica %d out of range", rep);
+  int st = ls2d_set_fields(p, rep, E, nu, epsp, 1, (cudaStream_t)stream);
+  if (st == MGK_OK) p->has_material[rep] = 1;
   return st;
 }
 
-extern "C" int mgk_ls2d_set_eigenstrain(mgk_ls2d_t p, const double* epsp, mgk_stream_t stream) {
-  MGK_REQUIRE(p && p->has_material, "mgk_ls2d_set_eigenstrain: plan has no material");
-  return ls2d_set_fields(p, nullptr, nullptr, epsp, 0, (cudaStream_t)stream);
+extern "C" int mgk_ls2d_set_material(mgk_ls2d_t p, const double* E, const double* nu, const double* epsp,
+                                     mgk_stream_t stream) {
+  return mgk_ls2d_set_material_rep(p, 0, E, nu, epsp, stream);
 }
 
-template <typename T>
-static int ls2d_launch_body(mgk_ls2d_t p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle h) {
-  ls2d_col_kernel<T><<<p->col_items, 256, p->col_smem, s>>>(p->d_rep, p->d_st, p->d_colmap);
+extern "C" int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t p, int rep, const double* epsp, mgk_stream_t stream) {
+  MGK_REQUIRE(p && rep >= 0 && rep < p->nrep && p->has_material[rep],
+              "mgk_ls2d_set_eigenstrain: replica has no material");
+  return ls2d_set_fields(p, rep, nullptr, nullptr, epsp, 0, (cudaStream_t)stream);
+}
+
+extern "C" int mgk_ls2d_set_eigenstrain(mgk_ls2d_t p, const double* epsp, mgk_stream_t stream) {
+  return mgk_ls2d_set_eigenstrain_rep(p, 0, epsp, stream);
+}
+
+// ------------------------------------------------------------- the loop ---
+
+struct LoopArgs {
+  const Ls2dRep* reps;
+  Ls2dState* st;
+  const int* row_map;
+  const int* row_local;
+  const int* col_map;
+  const int* col_local;
+  double* part;
+  unsigned int* repctr;
+  Ls2dCtl* ctl;
+  int rows, cols;
+  size_t row_smem, col_smem;
+};
+
+template <typename TS, bool FINAL>
+static int launch_body(const LoopArgs& a, cudaStream_t s) {
+  ls2d_col_kernel<TS, TS><<<a.cols, kThreads, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
   MGK_CUDA(cudaGetLastError());
-  ls2d_row_kernel<T, true><<<p->row_items, 256, p->row_smem, s>>>(
-      p->d_rep, p->d_st, p->d_rowmap, p->d_part, p->d_counter, 1, h, use_cond, p->d_any, p->guard_cap);
+  ls2d_row_kernel<TS, TS, true, FINAL><<<a.rows, kThreads, a.row_smem, s>>>(
+      a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }
 
-template <typename T>
-static int ls2d_build_graph(mgk_ls2d_t p) {
-  cudaGraph_t g = nullptr;
-  MGK_CUDA(cudaGraphCreate(&g, 0));
+template <typename TS, bool FINAL>
+static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* dep, int ndep, LoopArgs& a,
+                     int* guard_cap) {
   cudaGraphConditionalHandle h;
-  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  MGK_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
   // cudaGraphNodeParams has no default constructor in C++: zeroed storage
-  alignas(cudaGraphNodeParams) unsigned char cp_raw[sizeof(cudaGraphNodeParams)];
-  memset(cp_raw, 0, sizeof(cp_raw));
-  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_raw);
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
   cp.type = cudaGraphNodeTypeConditional;
   cp.conditional.handle = h;
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
-  cudaGraphNode_t wnode;
-  e = cudaGraphAddNode(&wnode, g, nullptr, 0, &cp);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  MGK_CUDA(cudaGraphAddNode(node, g, dep, ndep, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // kernel nodes of the body: column kernel -> row kernel
   cudaKernelNodeParams k1;
   memset(&k1, 0, sizeof(k1));
-  void* a1[] = {&p->d_rep, &p->d_st, &p->d_colmap};
-  k1.func = (void*)ls2d_col_kernel<T>;
-  k1.gridDim = dim3(p->col_items);
-  k1.blockDim = dim3(256);
-  k1.sharedMemBytes = (unsigned)p->col_smem;
+  void* a1[] = {&a.reps, &a.st, &a.col_map, &a.col_local};
+  k1.func = (void*)ls2d_col_kernel<TS, TS>;
+  k1.gridDim = dim3(a.cols);
+  k1.blockDim = dim3(kThreads);
+  k1.sharedMemBytes = (unsigned)a.col_smem;
   k1.kernelParams = a1;
   cudaGraphNode_t n1, n2;
-  e = cudaGraphAddKernelNode(&n1, body, nullptr, 0, &k1);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
-  int nrep = 1, use_cond = 1;
+  MGK_CUDA(cudaGraphAddKernelNode(&n1, body, nullptr, 0, &k1));
+  int use_cond = 1;
   cudaKernelNodeParams k2;
   memset(&k2, 0, sizeof(k2));
-  void* a2[] = {&p->d_rep, &p->d_st, &p->d_rowmap, &p->d_part, &p->d_counter, &nrep, &h, &use_cond, &p->d_any,
-                &p->guard_cap};
-  k2.func = (void*)ls2d_row_kernel<T, true>;
-  k2.gridDim = dim3(p->row_items);
-  k2.blockDim = dim3(256);
-  k2.sharedMemBytes = (unsigned)p->row_smem;
+  void* a2[] = {&a.reps, &a.st, &a.row_map, &a.row_local, &a.part, &a.repctr, &a.ctl, &h, &use_cond, guard_cap};
+  k2.func = (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
+  k2.gridDim = dim3(a.rows);
+  k2.blockDim = dim3(kThreads);
+  k2.sharedMemBytes = (unsigned)a.row_smem;
   k2.kernelParams = a2;
-  e = cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  MGK_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2));
+  return MGK_OK;
+}
+
+// Graph for the current selection: mixed plans run [phase-1 while, promote,
+// phase-2 setup, first FP64 row kernel] before the final while node.  It is
+// rebuilt when the selection's shape or the iteration cap changes.
+static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_sel, int nsel, int G,
+                       int guard_cap) {
+  if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
+  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  cudaGraph_t g = nullptr;
+  MGK_CUDA(cudaGraphCreate(&g, 0));
+  int cap = guard_cap;
+  int rc = MGK_OK;
+  cudaGraphNode_t last;
+  if (p->prec == MGK_MIXED) {
+    cudaGraphNode_t w1, n_prom, n_ph2, n_row0;
+    rc = add_while<float, false>(g, &w1, nullptr, 0, a32, &cap);
+    if (rc == MGK_OK) {
+      cudaKernelNodeParams k;
+      memset(&k, 0, sizeof(k));
+      void* ap[] = {&a64.reps, (void*)&d_sel};
+      k.func = (void*)ls2d_promote_kernel;
+      k.gridDim = dim3(G, nsel);
+      k.blockDim = dim3(kThreads);
+      k.kernelParams = ap;
+      rc = cudaGraphAddKernelNode(&n_prom, g, &w1, 1, &k) == cudaSuccess ? MGK_OK : MGK_CUDA_ERROR;
+    }
+    if (rc == MGK_OK) {
+      cudaKernelNodeParams k2;
+      memset(&k2, 0, sizeof(k2));
+      void* ap2[] = {&a64.st, (void*)&d_sel, &nsel, &a64.ctl};
+      k2.func = (void*)ls2d_phase2_kernel;
+      k2.gridDim = dim3(1);
+      k2.blockDim = dim3(32);
+      k2.kernelParams = ap2;
+      rc = cudaGraphAddKernelNode(&n_ph2, g, &n_prom, 1, &k2) == cudaSuccess ? MGK_OK : MGK_CUDA_ERROR;
+    }
+    if (rc == MGK_OK) {
+      cudaKernelNodeParams k3;
+      memset(&k3, 0, sizeof(k3));
+      cudaGraphConditionalHandle h0 = 0;
+      int zero = 0;
+      void* ap3[] = {&a64.reps, &a64.st, &a64.row_map, &a64.row_local, &a64.part, &a64.repctr, &a64.ctl,
+                     &h0, &zero, &zero};
+      k3.func = (void*)ls2d_row_kernel<double, double, false, true>;
+      k3.gridDim = dim3(a64.rows);
+      k3.blockDim = dim3(kThreads);
+      k3.sharedMemBytes = (unsigned)a64.row_smem;
+      k3.kernelParams = ap3;
+      rc = cudaGraphAddKernelNode(&n_row0, g, &n_ph2, 1, &k3) == cudaSuccess ? MGK_OK : MGK_CUDA_ERROR;
+    }
+    if (rc == MGK_OK) rc = add_while<double, true>(g, &last, &n_row0, 1, a64, &cap);
+  } else {
+    rc = add_while<double, true>(g, &last, nullptr, 0, a64, &cap);
+  }
   cudaGraphExec_t x = nullptr;
-  e = cudaGraphInstantiate(&x, g, 0);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  if (rc == MGK_OK && cudaGraphInstantiate(&x, g, 0) != cudaSuccess) rc = MGK_CUDA_ERROR;
+  if (rc != MGK_OK) {
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+    return rc;
+  }
   p->graph = g;
   p->exec = x;
   return MGK_OK;
 }
 
-template <typename T>
-static int ls2d_solve_t(mgk_ls2d_t p, const double* eb, const double* eps_init, double* eps_out, double* sig_out,
-                        int max_iter, double tol, mgk_ls_info* info, cudaStream_t s) {
-  const int grid = grid_for(p->N);
-  if (eps_init) {
-    aos4_partial_kernel<<<grid, 256, 0, s>>>(eps_init, p->N, p->d_part);
+extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, const double* eps_bar,
+                                    const double* const* eps_init, double* const* eps_out, double* const* sig_out,
+                                    int max_iter, double tol, mgk_ls_info* infos, mgk_stream_t stream) {
+  MGK_REQUIRE(p && eps_bar && nsel >= 1 && nsel <= p->nrep, "mgk_ls2d_solve_batch: bad argument");
+  MGK_REQUIRE(max_iter >= 0 && max_iter <= 1000000, "mgk_ls2d_solve: max_iter out of range");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<int> selv(nsel);
+  std::vector<char> seen(p->nrep, 0);
+  for (int q = 0; q < nsel; ++q) {
+    const int r = sel ? sel[q] : q;
+    MGK_REQUIRE(r >= 0 && r < p->nrep && !seen[r], "mgk_ls2d_solve_batch: bad or repeated replica index");
+    MGK_REQUIRE(p->has_material[r], "mgk_ls2d_solve: replica %d has no material (call set_material)", r);
+    seen[r] = 1;
+    selv[q] = r;
+  }
+  int rc = staging_wait(p);
+  if (rc) return rc;
+  // per-call fields and compact work maps
+  int rows = 0, cols = 0;
+  for (int q = 0; q < nsel; ++q) { rows += p->reps[selv[q]].row_items; cols += p->reps[selv[q]].col_items; }
+  const bool changed = rows != p->sel_rows || cols != p->sel_cols || nsel != p->nsel;
+  int* row_map = p->h_maps;
+  int* row_local = row_map + rows;
+  int* col_map = row_local + rows;
+  int* col_local = col_map + cols;
+  int* selp = col_local + cols;
+  int ri = 0, ci = 0;
+  for (int q = 0; q < nsel; ++q) {
+    const int r = selv[q];
+    Ls2dRep& H = p->h_reps[r];
+    H = p->reps[r];
+    H.init = eps_init ? eps_init[q] : nullptr;
+    H.out_eps = eps_out ? eps_out[q] : nullptr;
+    H.out_sig = sig_out ? sig_out[q] : nullptr;
+    for (int k = 0; k < 4; ++k) H.eb[k] = eps_bar[4 * q + k];
+    H.tol = tol;
+    H.max_iter = max_iter;
+    H.row_first = ri;
+    H.col_first = ci;
+    for (int i = 0; i < H.row_items; ++i) { row_map[ri] = r; row_local[ri] = i; ++ri; }
+    for (int i = 0; i < H.col_items; ++i) { col_map[ci] = r; col_local[ci] = i; ++ci; }
+    selp[q] = r;
+  }
+  const int n_active = max_iter > 0 ? nsel : 0;
+  p->h_ctl->n_active = (unsigned int)n_active;
+  p->h_ctl->decided = 0;
+  p->h_ctl->still = 0;
+  p->h_ctl->bodies = 0;
+  p->h_ctl->any = n_active > 0;
+  const size_t nm = 2 * (size_t)rows + 2 * (size_t)cols + nsel;
+  MGK_CUDA(cudaMemcpyAsync(p->d_maps, p->h_maps, sizeof(int) * nm, cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaMemcpyAsync(p->d_reps, p->h_reps, sizeof(Ls2dRep) * p->nrep, cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaMemcpyAsync(p->d_ctl, p->h_ctl, sizeof(Ls2dCtl), cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaEventRecord(p->staged, s));
+  p->staged_pending = true;
+  p->sel_rows = rows;
+  p->sel_cols = cols;
+  p->nsel = nsel;
+
+  const int* d_row_map = p->d_maps;
+  const int* d_row_local = d_row_map + rows;
+  const int* d_col_map = d_row_local + rows;
+  const int* d_col_local = d_col_map + cols;
+  const int* d_sel = d_col_local + cols;
+  const int G = grid_blocks(p->maxN);
+  bool any_init = false;
+  for (int q = 0; q < nsel && eps_init; ++q) any_init |= eps_init[q] != nullptr;
+  if (any_init) {
+    ls2d_means_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, d_sel, p->d_part);
     MGK_CUDA(cudaGetLastError());
-    finalize_sums_kernel<<<1, 256, 0, s>>>(p->d_part, grid, 4, 1.0 / (double)p->N,
-                                           reinterpret_cast<double*>(reinterpret_cast<char*>(p->d_st) +
-                                                                     offsetof(Ls2dState, means)));
+    ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 4,
+                                                   (int)offsetof(Ls2dState, means), 1);
     MGK_CUDA(cudaGetLastError());
   }
-  ls2d_begin_kernel<<<grid, 256, 0, s>>>(p->d_rep, p->d_st, 0, eb[0], eb[1], eb[2], eb[3], eps_init, tol,
-                                          max_iter, p->d_part, p->d_counter);
+  ls2d_begin_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());
-  if (eps_init) {
-    ls2d_begin_finalize_kernel<<<1, 256, 0, s>>>(p->d_st, 0, p->d_part, grid);
+  if (any_init) {
+    ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 2,
+                                                   (int)offsetof(Ls2dState, extra_d0), 2);
     MGK_CUDA(cudaGetLastError());
   }
-  if (max_iter > 0) {
-    ls2d_row_kernel<T, false><<<p->row_items, 256, p->row_smem, s>>>(
-        p->d_rep, p->d_st, p->d_rowmap, p->d_part, p->d_counter, 1, 0, 0, p->d_any, 0);
+  if (n_active > 0) {
+    const bool mixed = p->prec == MGK_MIXED;
+    LoopArgs a64{p->d_reps, p->d_st, d_row_map, d_row_local, d_col_map, d_col_local, p->d_part, p->d_repctr,
+                 p->d_ctl, rows, cols, p->row_smem, p->col_smem};
+    LoopArgs a32 = a64;
+    a32.row_smem = p->row_smem / 2;
+    a32.col_smem = p->col_smem / 2;
+    if (mixed)
+      ls2d_row_kernel<float, float, false, false><<<rows, kThreads, a32.row_smem, s>>>(
+          p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+    else
+      ls2d_row_kernel<double, double, false, true><<<rows, kThreads, a64.row_smem, s>>>(
+          p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
     MGK_CUDA(cudaGetLastError());
-    if (p->graph_mode == 1 && max_iter + 2 > p->guard_cap) {
-      // the loop guard is a graph kernel argument: rebuild for a larger cap
-      cudaGraphExecDestroy(p->exec); cudaGraphDestroy(p->graph);
-      p->exec = nullptr; p->graph = nullptr; p->graph_mode = -1;
-    }
+    const int guard_cap = (max_iter + 2 > 1000 ? max_iter + 2 : 1000);
+    if (p->graph_mode == 1 && (changed || guard_cap > p->graph_cap)) p->graph_mode = -1;
     if (p->graph_mode < 0) {
       const char* env = getenv("MGK_NO_GRAPH_WHILE");
-      p->guard_cap = max_iter + 2 > 1000 ? max_iter + 2 : 1000;
-      p->graph_mode = (env && env[0] == '1') ? 0 : (ls2d_build_graph<T>(p) == MGK_OK ? 1 : 0);
+      if (env && env[0] == '1') p->graph_mode = 0;
+      else {
+        p->graph_mode = build_graph(p, a64, a32, d_sel, nsel, G, guard_cap) == MGK_OK ? 1 : 0;
+        p->graph_cap = guard_cap;
+      }
     }
     if (p->graph_mode == 1) {
       MGK_CUDA(cudaGraphLaunch(p->exec, s));
     } else {
       // host-driven loop: poll the device flag after each iteration
-      int* h_any = p->h_any;
-      for (int it = 0; it < max_iter; ++it) {
-        int st = ls2d_launch_body<T>(p, s, 0, 0);
-        if (st) return st;
-        MGK_CUDA(cudaMemcpyAsync(h_any, p->d_any, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MGK_CUDA(cudaStreamSynchronize(s));
-        if (!*h_any) break;
+      for (int phase = mixed ? 1 : 2; phase <= 2; ++phase) {
+        if (phase == 2 && mixed) {
+          ls2d_promote_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, d_sel);
+          ls2d_phase2_kernel<<<1, 32, 0, s>>>(p->d_st, d_sel, nsel, p->d_ctl);
+          ls2d_row_kernel<double, double, false, true><<<rows, kThreads, a64.row_smem, s>>>(
+              p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+          MGK_CUDA(cudaGetLastError());
+        }
+        for (int it = 0; it < max_iter; ++it) {
+          rc = (phase == 1) ? launch_body<float, false>(a32, s) : launch_body<double, true>(a64, s);
+          if (rc) return rc;
+          Ls2dCtl hc;
+          MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls2dCtl), cudaMemcpyDeviceToHost, s));
+          MGK_CUDA(cudaStreamSynchronize(s));
+          if (!hc.any) break;
+        }
       }
     }
   }
-  ls2d_output_kernel<<<grid, 256, 0, s>>>(p->d_rep, p->d_st, 0, eps_out, sig_out, p->d_part);
+  ls2d_output_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());
-  finalize_sums_kernel<<<1, 256, 0, s>>>(p->d_part, grid, 8, 1.0 / (double)p->N,
-                                         reinterpret_cast<double*>(reinterpret_cast<char*>(p->d_st) +
-                                                                   offsetof(Ls2dState, out_eps_mean)));
+  ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 8,
+                                                 (int)offsetof(Ls2dState, out_eps_mean), 0);
   MGK_CUDA(cudaGetLastError());
-  if (info) {
-    MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls2dState), cudaMemcpyDeviceToHost, s));
+  if (infos) {
+    MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls2dState) * p->nrep, cudaMemcpyDeviceToHost, s));
     MGK_CUDA(cudaStreamSynchronize(s));
-    const Ls2dState& S = *p->h_state;
-    info->iterations = S.iter;
-    info->status = S.status;
-    info->final_diff = S.diff;
-    for (int q = 0; q < 4; ++q) { info->eps_mean[q] = S.out_eps_mean[q]; info->sig_mean[q] = S.out_sig_mean[q]; }
-    if (S.status == MGK_NONFINITE) {
-      set_error("mgk_ls2d_solve: non-finite residual at iteration %d", S.iter);
+    int worst = MGK_OK;
+    for (int q = 0; q < nsel; ++q) {
+      const Ls2dState& S = p->h_state[selv[q]];
+      infos[q].iterations = S.iter;
+      infos[q].status = S.status;
+      infos[q].final_diff = S.diff;
+      for (int k = 0; k < 4; ++k) { infos[q].eps_mean[k] = S.out_eps_mean[k]; infos[q].sig_mean[k] = S.out_sig_mean[k]; }
+      if (S.status == MGK_NONFINITE) worst = MGK_NONFINITE;
+    }
+    if (worst == MGK_NONFINITE) {
+      set_error("mgk_ls2d_solve: non-finite residual");
       return MGK_NONFINITE;
     }
   }
@@ -812,35 +1200,36 @@ static int ls2d_solve_t(mgk_ls2d_t p, const double* eb, const double* eps_init, 
 }
 
 extern "C" int mgk_ls2d_solve(mgk_ls2d_t p, const double* eps_bar, const double* eps_init, double* eps_out,
-                              double* sig_out, int max_iter, double tol, mgk_ls_info* info,
-                              mgk_stream_t stream) {
+                              double* sig_out, int max_iter, double tol, mgk_ls_info* info, mgk_stream_t stream) {
   MGK_REQUIRE(p && eps_bar, "mgk_ls2d_solve: null argument");
-  MGK_REQUIRE(p->has_material, "mgk_ls2d_solve: call mgk_ls2d_set_material first");
-  MGK_REQUIRE(max_iter >= 0 && max_iter <= 1000000, "mgk_ls2d_solve: max_iter out of range");
-  cudaStream_t s = (cudaStream_t)stream;
-  return p->prec == MGK_FP64 ? ls2d_solve_t<double>(p, eps_bar, eps_init, eps_out, sig_out, max_iter, tol, info, s)
-                             : ls2d_solve_t<float>(p, eps_bar, eps_init, eps_out, sig_out, max_iter, tol, info, s);
+  int r0 = 0;
+  return mgk_ls2d_solve_batch(p, 1, &r0, eps_bar, &eps_init, &eps_out, &sig_out, max_iter, tol, info, stream);
 }
 
-template <typename T>
-static int ls2d_profile_t(mgk_ls2d_t p, const double* eb, int reps, float* row_ms, float* col_ms, cudaStream_t s) {
-  const int grid = grid_for(p->N);
-  ls2d_begin_kernel<<<grid, 256, 0, s>>>(p->d_rep, p->d_st, 0, eb[0], eb[1], eb[2], eb[3], nullptr, 0.0,
-                                          1 << 30, p->d_part, p->d_counter);
-  MGK_CUDA(cudaGetLastError());
-  ls2d_row_kernel<T, false><<<p->row_items, 256, p->row_smem, s>>>(
-      p->d_rep, p->d_st, p->d_rowmap, p->d_part, p->d_counter, 1, 0, 0, p->d_any, 0);
+// ----------------------------------------------------------- profiling ---
+
+template <typename TS>
+static int profile_t(mgk_ls2d_t p, float* row_ms, float* col_ms, int reps, cudaStream_t s) {
+  const int rows = p->sel_rows, cols = p->sel_cols;
+  const int* d_row_map = p->d_maps;
+  const int* d_row_local = d_row_map + rows;
+  const int* d_col_map = d_row_local + rows;
+  const int* d_col_local = d_col_map + cols;
+  const size_t rs = sizeof(TS) == 8 ? p->row_smem : p->row_smem / 2;
+  const size_t cs = sizeof(TS) == 8 ? p->col_smem : p->col_smem / 2;
+  ls2d_row_kernel<TS, TS, false, true><<<rows, kThreads, rs, s>>>(p->d_reps, p->d_st, d_row_map, d_row_local,
+                                                                  p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
   MGK_CUDA(cudaGetLastError());
   cudaEvent_t ev[3];
   for (int i = 0; i < 3; ++i) MGK_CUDA(cudaEventCreate(&ev[i]));
   float tr = 0, tc = 0;
   int rc = MGK_OK;
-  for (int r = 0; r < reps && rc == MGK_OK; ++r) {
+  for (int r = 0; r < reps; ++r) {
     cudaEventRecord(ev[0], s);
-    ls2d_col_kernel<T><<<p->col_items, 256, p->col_smem, s>>>(p->d_rep, p->d_st, p->d_colmap);
+    ls2d_col_kernel<TS, TS><<<cols, kThreads, cs, s>>>(p->d_reps, p->d_st, d_col_map, d_col_local);
     cudaEventRecord(ev[1], s);
-    ls2d_row_kernel<T, true><<<p->row_items, 256, p->row_smem, s>>>(
-        p->d_rep, p->d_st, p->d_rowmap, p->d_part, p->d_counter, 1, 0, 0, p->d_any, 0);
+    ls2d_row_kernel<TS, TS, true, true><<<rows, kThreads, rs, s>>>(p->d_reps, p->d_st, d_row_map, d_row_local,
+                                                                   p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
     cudaEventRecord(ev[2], s);
     if (cudaEventSynchronize(ev[2]) != cudaSuccess) { rc = MGK_CUDA_ERROR; break; }
     float a = 0, b = 0;
@@ -857,13 +1246,43 @@ static int ls2d_profile_t(mgk_ls2d_t p, const double* eb, int reps, float* row_m
   return MGK_OK;
 }
 
+extern "C" int mgk_ls2d_profile_batch(mgk_ls2d_t p, int nsel, const int* sel, const double* eps_bar, int fp32,
+                                      int reps, float* row_ms, float* col_ms, mgk_stream_t stream) {
+  MGK_REQUIRE(p && eps_bar && row_ms && col_ms && reps > 0, "mgk_ls2d_profile: bad argument");
+  MGK_REQUIRE(!fp32 || p->prec == MGK_MIXED, "mgk_ls2d_profile: FP32 kernels need a mixed-precision plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  // set up the selection with a zero-iteration solve, then time iterations
+  // with tolerance 0 and an unreachable cap so every replica stays active
+  std::vector<const double*> init(nsel, nullptr);
+  std::vector<double*> outs(nsel, nullptr);
+  int rc = mgk_ls2d_solve_batch(p, nsel, sel, eps_bar, init.data(), outs.data(), outs.data(), 0, 0.0, nullptr,
+                                stream);
+  if (rc) return rc;
+  rc = staging_wait(p);
+  if (rc) return rc;
+  for (int q = 0; q < nsel; ++q) {
+    Ls2dRep& H = p->h_reps[sel ? sel[q] : q];
+    H.max_iter = 1 << 30;
+    H.tol = 0.0;
+  }
+  MGK_CUDA(cudaMemcpyAsync(p->d_reps, p->h_reps, sizeof(Ls2dRep) * p->nrep, cudaMemcpyHostToDevice, s));
+  for (int q = 0; q < nsel; ++q) {
+    const int r = sel ? sel[q] : q;
+    MGK_CUDA(cudaMemsetAsync(reinterpret_cast<char*>(&p->d_st[r]) + offsetof(Ls2dState, done), 0, sizeof(int), s));
+  }
+  p->h_ctl->n_active = nsel;
+  p->h_ctl->decided = 0;
+  p->h_ctl->still = 0;
+  p->h_ctl->bodies = 0;
+  MGK_CUDA(cudaMemcpyAsync(p->d_ctl, p->h_ctl, sizeof(Ls2dCtl), cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaStreamSynchronize(s));
+  return fp32 ? profile_t<float>(p, row_ms, col_ms, reps, s) : profile_t<double>(p, row_ms, col_ms, reps, s);
+}
+
 extern "C" int mgk_ls2d_profile(mgk_ls2d_t p, const double* eps_bar, int reps, float* row_ms, float* col_ms,
                                 mgk_stream_t stream) {
-  MGK_REQUIRE(p && eps_bar && row_ms && col_ms && reps > 0, "mgk_ls2d_profile: bad argument");
-  MGK_REQUIRE(p->has_material, "mgk_ls2d_profile: call mgk_ls2d_set_material first");
-  cudaStream_t s = (cudaStream_t)stream;
-  return p->prec == MGK_FP64 ? ls2d_profile_t<double>(p, eps_bar, reps, row_ms, col_ms, s)
-                             : ls2d_profile_t<float>(p, eps_bar, reps, row_ms, col_ms, s);
+  int r0 = 0;
+  return mgk_ls2d_profile_batch(p, 1, &r0, eps_bar, 0, reps, row_ms, col_ms, stream);
 }
 
 // ============================================================ no-alloc ===
@@ -881,8 +1300,12 @@ constexpr size_t kNaPlanes = 10 * (size_t)kNaMaxN;                              
 constexpr size_t kNaSpec = 3 * (size_t)MGK_NOALLOC_MAX_SIDE * (MGK_NOALLOC_MAX_SIDE / 2 + 1) * 2;  // complex
 constexpr size_t kNaTw = 2 * (size_t)MGK_NOALLOC_MAX_SIDE * 2;                               // two tables
 constexpr size_t kNaPart = 8 * 2048;                                                         // partial sums
-constexpr size_t kNaMisc = 1024;                    // plan record, state, work maps, counters
+constexpr size_t kNaMisc = 1024;                    // plan record, state, control, work maps
 constexpr size_t kNaDoubles = kNaPlanes + kNaSpec + kNaTw + kNaPart + kNaMisc;
+// byte offsets inside the misc region
+constexpr size_t kNaRep = 0, kNaState = 1024, kNaCtl = 2048, kNaCtr = 2112, kNaMaps = 2176;
+constexpr int kNaMapInts = 128 + 128 + 256 + 256 + 1;
+static_assert(kNaMaps + 4 * kNaMapInts <= kNaMisc * sizeof(double), "no-alloc misc region");
 }  // namespace
 
 // Device-side storage.  In host code this name is only a stand-in for the
@@ -891,15 +1314,21 @@ static __device__ __align__(256) double g_ls2d_noalloc_scratch[kNaDoubles];
 
 namespace mgk {
 
-// Writes the plan record, clears the work maps, counters and state, and fills
-// the twiddle tables (sincospi) -- everything a call must start from.
-__global__ void ls2d_noalloc_setup_kernel(Ls2dRep rep, Ls2dRep* dst, Ls2dState* st, int* rowmap, int rowitems,
-                                          int* colmap, int colitems, unsigned int* counter, int* any,
+// Writes the plan record and the work maps, clears the state, the control
+// block and the arrival counter, and fills the twiddle tables (sincospi):
+// everything a call must start from.
+__global__ void ls2d_noalloc_setup_kernel(Ls2dRep rep, Ls2dRep* dst, Ls2dState* st, Ls2dCtl* ctl,
+                                          unsigned int* repctr, int* maps, int rows, int cols, int n_active,
                                           double2* twx, int nx, double2* twy, int ny) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int stride = gridDim.x * blockDim.x;
-  for (int i = t; i < rowitems; i += stride) rowmap[i] = 0;
-  for (int i = t; i < colitems; i += stride) colmap[i] = 0;
+  int* row_map = maps;
+  int* row_local = row_map + rows;
+  int* col_map = row_local + rows;
+  int* col_local = col_map + cols;
+  int* sel = col_local + cols;
+  for (int i = t; i < rows; i += stride) { row_map[i] = 0; row_local[i] = i; }
+  for (int i = t; i < cols; i += stride) { col_map[i] = 0; col_local[i] = i; }
   for (int m = t; m < nx; m += stride) {
     double s, c;
     sincospi(2.0 * m / nx, &s, &c);
@@ -912,18 +1341,20 @@ __global__ void ls2d_noalloc_setup_kernel(Ls2dRep rep, Ls2dRep* dst, Ls2dState* 
   }
   if (t == 0) {
     *dst = rep;
-    counter[0] = 0;
-    counter[1] = 0;
-    *any = 0;
+    sel[0] = 0;
+    *repctr = 0;
     Ls2dState z;
     memset(&z, 0, sizeof(z));
     *st = z;
+    ctl->n_active = (unsigned int)n_active;
+    ctl->decided = 0;
+    ctl->still = 0;
+    ctl->bodies = 0;
+    ctl->any = n_active > 0;
   }
 }
 
 }  // namespace mgk
-
-#include <mutex>
 
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[128];  // resolved scratch address per device
@@ -969,17 +1400,12 @@ extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const doub
 
   const long long N = (long long)nx * ny;
   const int nyh = ny / 2 + 1;
-  int tc = 8;
-  while (tc > 1 && 2 * 3 * (size_t)tc * nx * sizeof(double2) > 200 * 1024) tc >>= 1;
-  const int row_items = nx / 2, col_items = (nyh + tc - 1) / tc;
+  const int tc = pick_tc(nx, sizeof(double2), 64 * 1024);
+  const int rows = nx / 2, cols = (nyh + tc - 1) / tc;
   const size_t row_smem = 2 * 3 * (size_t)ny * sizeof(double2);
   const size_t col_smem = 2 * 3 * (size_t)tc * nx * sizeof(double2);
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_col_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)col_smem));
+  st = ls2d_set_attrs<double, double>(row_smem, col_smem);
+  if (st != MGK_OK) return st;
 
   // carve the scratch array (offsets in doubles, each region 256-byte aligned)
   double* planes = base;
@@ -988,78 +1414,79 @@ extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const doub
   double2* twy = twx + MGK_NOALLOC_MAX_SIDE;
   double* part = base + kNaPlanes + kNaSpec + kNaTw;
   char* misc = reinterpret_cast<char*>(base + kNaPlanes + kNaSpec + kNaTw + kNaPart);
-  Ls2dRep* d_rep = reinterpret_cast<Ls2dRep*>(misc);
-  Ls2dState* d_st = reinterpret_cast<Ls2dState*>(misc + 1024);
-  int* d_rowmap = reinterpret_cast<int*>(misc + 2048);
-  int* d_colmap = reinterpret_cast<int*>(misc + 2048 + 4 * 256);
-  unsigned int* d_counter = reinterpret_cast<unsigned int*>(misc + 2048 + 8 * 256);
-  int* d_any = reinterpret_cast<int*>(misc + 2048 + 8 * 256 + 64);
-  static_assert(sizeof(Ls2dRep) <= 1024 && sizeof(Ls2dState) <= 1024, "no-alloc record sizes");
-  static_assert(2048 + 8 * 256 + 128 <= kNaMisc * sizeof(double), "no-alloc misc region");
+  Ls2dRep* d_rep = reinterpret_cast<Ls2dRep*>(misc + kNaRep);
+  Ls2dState* d_st = reinterpret_cast<Ls2dState*>(misc + kNaState);
+  Ls2dCtl* d_ctl = reinterpret_cast<Ls2dCtl*>(misc + kNaCtl);
+  unsigned int* d_ctr = reinterpret_cast<unsigned int*>(misc + kNaCtr);
+  int* d_maps = reinterpret_cast<int*>(misc + kNaMaps);
+  static_assert(sizeof(Ls2dRep) <= 1024 && sizeof(Ls2dState) <= 1024 && sizeof(Ls2dCtl) <= 64,
+                "no-alloc record sizes");
+  const int* d_row_map = d_maps;
+  const int* d_row_local = d_row_map + rows;
+  const int* d_col_map = d_row_local + rows;
+  const int* d_col_local = d_col_map + cols;
+  const int* d_sel = d_col_local + cols;
 
   fx.tw = twx;
   fy.tw = twy;
   Ls2dRep R;
   memset(&R, 0, sizeof(R));
-  R.nx = nx; R.ny = ny; R.nyh = nyh; R.ld = nyh;
-  R.row_base = 0; R.row_items = row_items; R.col_base = 0; R.col_items = col_items; R.tc = tc;
-  R.N = N; R.fx = fx; R.fy = fy;
+  R.nx = nx; R.ny = ny; R.nyh = nyh; R.ld = nyh; R.tc = tc;
+  R.row_items = rows; R.col_items = cols;
+  R.N = N; R.fx64 = fx; R.fy64 = fy; R.fx32 = fx; R.fy32 = fy;
   R.mu = planes; R.lam = planes + N; R.eps = planes + 2 * N; R.ep = planes + 5 * N;
   R.epa = eps_plastic ? planes + 8 * N : nullptr;
-  R.has_epa = eps_plastic ? 1 : 0;
   R.spec = spec;
+  R.init = eps_init; R.out_eps = eps_out; R.out_sig = sig_out;
+  for (int k = 0; k < 4; ++k) R.eb[k] = eps_bar[k];
+  R.tol = tol; R.max_iter = max_iter; R.row_first = 0; R.col_first = 0;
 
-  ls2d_noalloc_setup_kernel<<<4, 256, 0, s>>>(R, d_rep, d_st, d_rowmap, row_items, d_colmap, col_items, d_counter,
-                                              d_any, twx, nx, twy, ny);
+  ls2d_noalloc_setup_kernel<<<4, 256, 0, s>>>(R, d_rep, d_st, d_ctl, d_ctr, d_maps, rows, cols,
+                                              max_iter > 0 ? 1 : 0, twx, nx, twy, ny);
   MGK_CUDA(cudaGetLastError());
-  const int grid = grid_for(N);
-  ls2d_material_kernel<<<grid, 256, 0, s>>>(d_rep, 0, E, nu, eps_plastic, plane_mode, 1, part);
+  const int G = grid_blocks(N);
+  ls2d_material_kernel<<<G, kThreads, 0, s>>>(d_rep, 0, E, nu, eps_plastic, plane_mode, 1, part);
   MGK_CUDA(cudaGetLastError());
-  ls2d_medium_kernel<<<1, 256, 0, s>>>(d_rep, d_st, 0, part, grid, plane_mode);
+  ls2d_medium_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, 0, part, G, plane_mode);
   MGK_CUDA(cudaGetLastError());
-  const double* eb = eps_bar;
   if (eps_init) {
-    aos4_partial_kernel<<<grid, 256, 0, s>>>(eps_init, N, part);
-    MGK_CUDA(cudaGetLastError());
-    finalize_sums_kernel<<<1, 256, 0, s>>>(part, grid, 4, 1.0 / (double)N,
-                                           reinterpret_cast<double*>(reinterpret_cast<char*>(d_st) +
-                                                                     offsetof(Ls2dState, means)));
+    ls2d_means_kernel<<<dim3(G, 1), kThreads, 0, s>>>(d_rep, d_sel, part);
+    ls2d_finalize_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, d_sel, part, G, 4, (int)offsetof(Ls2dState, means), 1);
     MGK_CUDA(cudaGetLastError());
   }
-  ls2d_begin_kernel<<<grid, 256, 0, s>>>(d_rep, d_st, 0, eb[0], eb[1], eb[2], eb[3], eps_init, tol, max_iter, part,
-                                          d_counter);
+  ls2d_begin_kernel<<<dim3(G, 1), kThreads, 0, s>>>(d_rep, d_st, d_sel, part);
   MGK_CUDA(cudaGetLastError());
   if (eps_init) {
-    ls2d_begin_finalize_kernel<<<1, 256, 0, s>>>(d_st, 0, part, grid);
+    ls2d_finalize_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, d_sel, part, G, 2, (int)offsetof(Ls2dState, extra_d0),
+                                                1);
     MGK_CUDA(cudaGetLastError());
   }
   if (max_iter > 0) {
-    ls2d_row_kernel<double, false><<<row_items, 256, row_smem, s>>>(d_rep, d_st, d_rowmap, part, d_counter, 1, 0,
-                                                                    0, d_any, 0);
+    ls2d_row_kernel<double, double, false, true><<<rows, kThreads, row_smem, s>>>(
+        d_rep, d_st, d_row_map, d_row_local, part, d_ctr, d_ctl, 0, 0, 0);
     MGK_CUDA(cudaGetLastError());
-    // host-driven loop in chunks of 4 iterations; finished iterations skip
+    // host-driven loop in chunks of 4 iterations; finished replicas skip
     // their work on the device, and the host polls the activity flag
+    LoopArgs a{d_rep, d_st, d_row_map, d_row_local, d_col_map, d_col_local, part, d_ctr, d_ctl, rows, cols,
+               row_smem, col_smem};
     int it = 0;
     while (it < max_iter) {
       const int chunk = max_iter - it < 4 ? max_iter - it : 4;
       for (int c = 0; c < chunk; ++c) {
-        ls2d_col_kernel<double><<<col_items, 256, col_smem, s>>>(d_rep, d_st, d_colmap);
-        ls2d_row_kernel<double, true><<<row_items, 256, row_smem, s>>>(d_rep, d_st, d_rowmap, part, d_counter, 1,
-                                                                       0, 0, d_any, 0);
+        st = launch_body<double, true>(a, s);
+        if (st != MGK_OK) return st;
       }
-      MGK_CUDA(cudaGetLastError());
       it += chunk;
-      int h_any = 0;
-      MGK_CUDA(cudaMemcpyAsync(&h_any, d_any, sizeof(int), cudaMemcpyDeviceToHost, s));
+      Ls2dCtl hc;
+      MGK_CUDA(cudaMemcpyAsync(&hc, d_ctl, sizeof(Ls2dCtl), cudaMemcpyDeviceToHost, s));
       MGK_CUDA(cudaStreamSynchronize(s));
-      if (!h_any) break;
+      if (!hc.any) break;
     }
   }
-  ls2d_output_kernel<<<grid, 256, 0, s>>>(d_rep, d_st, 0, eps_out, sig_out, part);
+  ls2d_output_kernel<<<dim3(G, 1), kThreads, 0, s>>>(d_rep, d_st, d_sel, part);
   MGK_CUDA(cudaGetLastError());
-  finalize_sums_kernel<<<1, 256, 0, s>>>(part, grid, 8, 1.0 / (double)N,
-                                         reinterpret_cast<double*>(reinterpret_cast<char*>(d_st) +
-                                                                   offsetof(Ls2dState, out_eps_mean)));
+  ls2d_finalize_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, d_sel, part, G, 8, (int)offsetof(Ls2dState, out_eps_mean),
+                                              0);
   MGK_CUDA(cudaGetLastError());
   Ls2dState h;
   MGK_CUDA(cudaMemcpyAsync(&h, d_st, sizeof(Ls2dState), cudaMemcpyDeviceToHost, s));

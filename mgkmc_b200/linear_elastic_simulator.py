@@ -27,25 +27,31 @@ def _torch():
     return torch
 
 
-class Ls2dSolver:
-    """Plan-owning 2D LS solver on one device.
+class Ls2dBatch:
+    """Plan-owning batch of 2D LS replicas ("slots") on one device.
 
-    Fields are torch float64 CUDA tensors in the reference layouts:
-    E, nu (nx, ny); eps_plastic, eps, sig (nx, ny, 2, 2)."""
+    ``sizes`` lists each replica's (nx, ny); sizes may differ.  Fields are
+    torch float64 CUDA tensors in the reference layouts: E, nu (nx, ny);
+    eps_plastic, eps, sig (nx, ny, 2, 2).  ``precision`` is "fp64" (the
+    reference's arithmetic) or "mixed" (FP32 bulk iterations, FP64 finish)."""
 
-    def __init__(self, nx, ny, plane_mode="plane_strain", precision="fp64", device=None):
+    def __init__(self, sizes, plane_mode="plane_strain", precision="fp64", device=None):
         torch = _torch()
-        self.nx, self.ny = int(nx), int(ny)
+        self.sizes = [(int(a), int(b)) for a, b in sizes]
+        self.nrep = len(self.sizes)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.plane_mode = plane_mode
         self.precision = precision
+        nx = (ctypes.c_int * self.nrep)(*[a for a, _ in self.sizes])
+        ny = (ctypes.c_int * self.nrep)(*[b for _, b in self.sizes])
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            L.check(L.lib().mgk_ls2d_create(self.nx, self.ny, _PLANE[plane_mode],
-                                            L.FP64 if precision == "fp64" else L.FP32, ctypes.byref(h)),
-                    "mgk_ls2d_create")
+            L.check(L.lib().mgk_ls2d_create_batch(self.nrep, nx, ny, _PLANE[plane_mode],
+                                                  L.FP64 if precision == "fp64" else L.MIXED, ctypes.byref(h)),
+                    "mgk_ls2d_create_batch")
         self._h = h
-        self.info = L.LsInfo()
+        self._keep = {}
+        self.infos = (L.LsInfo * self.nrep)()
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -56,33 +62,71 @@ class Ls2dSolver:
                 pass
             self._h = None
 
-    def set_material(self, E, nu, eps_plastic=None, stream=None):
-        self._E, self._nu, self._ep = E, nu, eps_plastic  # keep alive until the stream consumes them
-        L.check(L.lib().mgk_ls2d_set_material(self._h, L.ptr(E), L.ptr(nu), L.ptr(eps_plastic),
-                                              L.stream_ptr(stream)), "mgk_ls2d_set_material")
+    def set_material(self, rep, E, nu, eps_plastic=None, stream=None):
+        self._keep[("m", rep)] = (E, nu, eps_plastic)  # alive until the stream has consumed them
+        L.check(L.lib().mgk_ls2d_set_material_rep(self._h, int(rep), L.ptr(E), L.ptr(nu), L.ptr(eps_plastic),
+                                                  L.stream_ptr(stream)), "mgk_ls2d_set_material")
 
-    def set_eigenstrain(self, eps_plastic, stream=None):
-        self._ep = eps_plastic
-        L.check(L.lib().mgk_ls2d_set_eigenstrain(self._h, L.ptr(eps_plastic), L.stream_ptr(stream)),
+    def set_eigenstrain(self, rep, eps_plastic, stream=None):
+        self._keep[("e", rep)] = eps_plastic
+        L.check(L.lib().mgk_ls2d_set_eigenstrain_rep(self._h, int(rep), L.ptr(eps_plastic), L.stream_ptr(stream)),
                 "mgk_ls2d_set_eigenstrain")
 
-    def solve(self, eps_bar, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True, stream=None):
-        eb = (ctypes.c_double * 4)(*[float(v) for v in np.asarray(eps_bar, dtype=np.float64).reshape(4)])
-        info = self.info if sync else None
-        st = L.lib().mgk_ls2d_solve(self._h, eb, L.ptr(eps_init), L.ptr(eps_out), L.ptr(sig_out), int(max_iter),
-                                    float(tol), ctypes.byref(info) if info is not None else None,
-                                    L.stream_ptr(stream))
-        L.check(st, "mgk_ls2d_solve", allow=(L.OK, L.NONFINITE))
-        return info
+    def solve(self, reps, eps_bars, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True,
+              stream=None):
+        """Solve replicas ``reps`` (one launch per stage for all of them).
+        eps_bars: sequence of (2,2); eps_out/sig_out/eps_init: sequences of
+        tensors (or None entries).  Returns the list of LsInfo when sync."""
+        n = len(reps)
+        sel = (ctypes.c_int * n)(*[int(r) for r in reps])
+        eb = (ctypes.c_double * (4 * n))(*np.concatenate([np.asarray(e, dtype=np.float64).reshape(4)
+                                                           for e in eps_bars]))
+        P = ctypes.c_void_p
 
+        def parr(ts):
+            if ts is None:
+                return None
+            return (P * n)(*[None if t is None else t.data_ptr() for t in ts])
+
+        infos = (L.LsInfo * n)() if sync else None
+        st = L.lib().mgk_ls2d_solve_batch(self._h, n, sel, eb, parr(eps_init), parr(eps_out), parr(sig_out),
+                                          int(max_iter), float(tol), infos, L.stream_ptr(stream))
+        L.check(st, "mgk_ls2d_solve_batch", allow=(L.OK, L.NONFINITE))
+        return list(infos) if sync else None
+
+    def profile_kernels(self, reps, eps_bars, fp32=False, n=50, stream=None):
+        """Mean (row_ms, col_ms) of the two iteration kernels over the
+        selection (CUDA events on the stream)."""
+        k = len(reps)
+        sel = (ctypes.c_int * k)(*[int(r) for r in reps])
+        eb = (ctypes.c_double * (4 * k))(*np.concatenate([np.asarray(e, dtype=np.float64).reshape(4)
+                                                           for e in eps_bars]))
+        r, c = ctypes.c_float(), ctypes.c_float()
+        L.check(L.lib().mgk_ls2d_profile_batch(self._h, k, sel, eb, 1 if fp32 else 0, int(n), ctypes.byref(r),
+                                               ctypes.byref(c), L.stream_ptr(stream)), "mgk_ls2d_profile_batch")
+        return r.value, c.value
+
+
+class Ls2dSolver(Ls2dBatch):
+    """One-replica plan with the single-solve interface."""
+
+    def __init__(self, nx, ny, plane_mode="plane_strain", precision="fp64", device=None):
+        super().__init__([(nx, ny)], plane_mode, precision, device)
+        self.nx, self.ny = int(nx), int(ny)
+
+    def set_material(self, E, nu, eps_plastic=None, stream=None):
+        super().set_material(0, E, nu, eps_plastic, stream)
+
+    def set_eigenstrain(self, eps_plastic, stream=None):
+        super().set_eigenstrain(0, eps_plastic, stream)
+
+    def solve(self, eps_bar, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True, stream=None):
+        infos = super().solve([0], [eps_bar], [eps_out], [sig_out], None if eps_init is None else [eps_init],
+                              max_iter, tol, sync, stream)
+        return infos[0] if sync else None
 
     def profile_kernels(self, eps_bar, reps=50, stream=None):
-        """Mean (row_ms, col_ms) of the two iteration kernels (CUDA events)."""
-        eb = (ctypes.c_double * 4)(*[float(v) for v in np.asarray(eps_bar, dtype=np.float64).reshape(4)])
-        r, c = ctypes.c_float(), ctypes.c_float()
-        L.check(L.lib().mgk_ls2d_profile(self._h, eb, int(reps), ctypes.byref(r), ctypes.byref(c),
-                                         L.stream_ptr(stream)), "mgk_ls2d_profile")
-        return r.value, c.value
+        return super().profile_kernels([0], [eps_bar], False, reps, stream)
 
 
 _PLANS = {}
