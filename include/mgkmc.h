@@ -53,7 +53,8 @@ MGK_API int mgk_version(void);
 MGK_API const char* mgk_status_string(int status);
 /* Text of the last error raised on the calling host thread. */
 MGK_API const char* mgk_last_error(void);
-/* 1 if n = 2^a 3^b with 4 <= n <= 4096 (grid sizes the FFT supports). */
+/* 1 if n = 2^a 3^b with 1 <= n <= 4096 (grid sides the FFT supports; the
+ * 2D solvers also need nx even, the 3D solver nx*ny even). */
 MGK_API int mgk_fft_supported(int n);
 
 /* ------------------------------------------- 2D small-strain LS solver --- */
@@ -140,6 +141,32 @@ MGK_API int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const double*
                                    double* eps_out, double* sig_out, int max_iter, double tol,
                                    mgk_ls_info* info, mgk_stream_t stream);
 
+/* ------------------------------------------- 3D small-strain LS solver --- */
+/* Replaces mgkmc/linear_elastic_simulator.py:274-376 spectral_solver_3d (and
+ * mgkmc/stz/update_fft.py:4-22 update_stress_fft_full, which wraps it), with
+ * the Green operator of mgkmc/elasticity.py:70-105 applied on the fly.  FP64.
+ * Batched plans as for 2D; eps_bar is 9 doubles per replica (3x3, C order);
+ * fields are (nx,ny,nz,3,3). */
+typedef struct mgk_ls3d_plan* mgk_ls3d_t;
+typedef struct {
+  int iterations;
+  int status;
+  double final_diff;
+  double eps_mean[9];
+  double sig_mean[9];
+} mgk_ls_info3;
+MGK_API int mgk_ls3d_create(int nx, int ny, int nz, mgk_ls3d_t* out);
+MGK_API int mgk_ls3d_create_batch(int nrep, const int* nx, const int* ny, const int* nz, mgk_ls3d_t* out);
+MGK_API int mgk_ls3d_destroy(mgk_ls3d_t plan);
+MGK_API int mgk_ls3d_set_material_rep(mgk_ls3d_t plan, int rep, const double* E, const double* nu,
+                                      const double* eps_plastic, mgk_stream_t stream);
+MGK_API int mgk_ls3d_set_eigenstrain_rep(mgk_ls3d_t plan, int rep, const double* eps_plastic,
+                                         mgk_stream_t stream);
+MGK_API int mgk_ls3d_solve_batch(mgk_ls3d_t plan, int nsel, const int* sel, const double* eps_bar,
+                                 const double* const* eps_init, double* const* eps_out,
+                                 double* const* sig_out, int max_iter, double tol, mgk_ls_info3* infos,
+                                 mgk_stream_t stream);
+
 /* ------------------------------------------------------ 2D STZ / KMC --- */
 /* mgkmc/kmc_simulator_functions.py:100-160 compute_barrier_2d (in place on Q).
  * scheme: 0 isotropic, 1 directional.  tau: +inf for no decay. */
@@ -181,6 +208,26 @@ MGK_API int mgk_kmc2d_flip(int nx, int ny, int M, double* eps_plastic, double* s
                    double* last_event_time, const double* catalog, int x, int y, int m,
                    double current_time, double jp, double jt, double g_max, double jn_frac,
                    mgk_stream_t stream);
+
+/* ------------------------------------------------------ 3D STZ / KMC --- */
+/* mgkmc/stz/barriers.py:4-100 compute_barrier (in place on Q; soft_prop has 4
+ * slots per voxel, of which 0 and 1 are used). */
+MGK_API int mgk_kmc3d_barrier(int nx, int ny, int nz, int M, double* Q, const double* Q0, const double* sig,
+                              const double* catalog, double volume, const double* soft_prop,
+                              const double* last_event_time, double current_time,
+                              const double* prev_strain_dir, double softening_cap, int scheme, double tau,
+                              mgk_stream_t stream);
+/* mgkmc/stz/kmc.py:4-74 compute_rates / _compute_rates_jit (index encoding
+ * ((x*ny + y)*nz + z)*M + m); outputs as mgk_kmc2d_rates. */
+MGK_API int mgk_kmc3d_rates(int nx, int ny, int nz, int M, const double* Q, double volume,
+                            const double* temperature, double temperature_scalar, double nu0, int cascade_mode,
+                            double* rates, int64_t* indices, double* prefix, int64_t* d_count, double* d_total,
+                            void* work, mgk_stream_t stream);
+/* mgkmc/stz/cascade.py:43-111 apply_flip_soa (in place; 26-neighbour softening). */
+MGK_API int mgk_kmc3d_flip(int nx, int ny, int nz, int M, double* eps_plastic, double* soft_prop,
+                           double* last_event_time, const double* catalog, int x, int y, int z, int m,
+                           double current_time, double jp, double jt, double g_max, double jn_frac,
+                           mgk_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -33,6 +33,11 @@ class LsInfo(Structure):
                 ("eps_mean", c_double * 4), ("sig_mean", c_double * 4)]
 
 
+class LsInfo3(Structure):
+    _fields_ = [("iterations", c_int), ("status", c_int), ("final_diff", c_double),
+                ("eps_mean", c_double * 9), ("sig_mean", c_double * 9)]
+
+
 _P = c_void_p
 _SIGS = {
     "mgk_version": (c_int, []),
@@ -54,6 +59,13 @@ _SIGS = {
     "mgk_ls2d_profile": (c_int, [_P, POINTER(c_double), c_int, POINTER(ctypes.c_float), POINTER(ctypes.c_float), _P]),
     "mgk_ls2d_solve_noalloc": (c_int, [c_int, c_int, c_int, _P, _P, _P, POINTER(c_double), _P, _P, _P, c_int,
                                        c_double, POINTER(LsInfo), _P]),
+    "mgk_ls3d_create": (c_int, [c_int, c_int, c_int, POINTER(c_void_p)]),
+    "mgk_ls3d_create_batch": (c_int, [c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_void_p)]),
+    "mgk_ls3d_destroy": (c_int, [_P]),
+    "mgk_ls3d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
+    "mgk_ls3d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
+    "mgk_ls3d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
+                                     POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo3), _P]),
     "mgk_kmc2d_barrier": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
                                   c_double, c_int, c_double, _P]),
     "mgk_kmc_rates_work_bytes": (c_int64, [c_int64]),
@@ -63,6 +75,12 @@ _SIGS = {
     "mgk_kmc_select": (c_int, [_P, _P, _P, c_double, _P, _P]),
     "mgk_kmc2d_flip": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_int, c_int, c_int, c_double, c_double,
                                c_double, c_double, c_double, _P]),
+    "mgk_kmc3d_barrier": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
+                                  c_double, c_int, c_double, _P]),
+    "mgk_kmc3d_rates": (c_int, [c_int, c_int, c_int, c_int, _P, c_double, _P, c_double, c_double, c_int, _P, _P,
+                                _P, _P, _P, _P, _P]),
+    "mgk_kmc3d_flip": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, c_int, c_int, c_int, c_int, c_double,
+                               c_double, c_double, c_double, c_double, _P]),
 }
 
 _lib = None

@@ -285,6 +285,35 @@ __global__ void flip2d_kernel(int nx, int ny, int M, double* ep, double* soft, d
   }
 }
 
+// apply_flip_soa (mgkmc/stz/cascade.py:43-111), one thread.
+__global__ void flip3d_kernel(int nx, int ny, int nz, int M, double* ep, double* soft, double* tl, const double* cat,
+                              int x, int y, int z, int m, double t, double jp, double jt, double gmax, double jn) {
+  const long long v = ((long long)x * ny + y) * nz + z;
+  const double* c = cat + ((v * M) + m) * 9;
+  for (int q = 0; q < 9; ++q) ep[9 * v + q] = add(ep[9 * v + q], c[q]);
+  const double e11 = c[0], e22 = c[4], e33 = c[8], e12 = c[1], e13 = c[2], e23 = c[5];
+  const double a = sub(e22, e33), b = sub(e33, e11), d = sub(e11, e22);
+  const double s = add(add(add(mul(e12, e12), mul(e23, e23)), mul(e13, e13)),
+                       __ddiv_rn(add(add(mul(a, a), mul(b, b)), mul(d, d)), 6.0));
+  double gp = add(soft[4 * v], mul(jp, s));
+  if (gmax > 0 && gp > gmax) gp = gmax;
+  soft[4 * v] = gp;
+  soft[4 * v + 1] = mul(jt, s);
+  tl[v] = t;
+  if (jn > 0.0) {
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dz = -1; dz <= 1; ++dz) {
+          if (dx == 0 && dy == 0 && dz == 0) continue;
+          const long long w = ((long long)((x + dx + nx) % nx) * ny + (y + dy + ny) % ny) * nz + (z + dz + nz) % nz;
+          double g = add(soft[4 * w], mul(mul(jn, jp), s));
+          if (gmax > 0 && g > gmax) g = gmax;
+          soft[4 * w] = g;
+          soft[4 * w + 1] = add(soft[4 * w + 1], mul(mul(jn, jt), s));
+        }
+  }
+}
+
 }  // namespace mgk
 
 using namespace mgk;
@@ -378,6 +407,45 @@ extern "C" int mgk_kmc2d_flip(int nx, int ny, int M, double* eps_plastic, double
   MGK_REQUIRE(eps_plastic && soft_prop && last_event_time && catalog, "mgk_kmc2d_flip: null argument");
   flip2d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, M, eps_plastic, soft_prop, last_event_time, catalog, x, y,
                                                    m, current_time, jp, jt, g_max, jn_frac);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc3d_barrier(int nx, int ny, int nz, int M, double* Q, const double* Q0, const double* sig,
+                                 const double* catalog, double volume, const double* soft_prop,
+                                 const double* last_event_time, double current_time,
+                                 const double* prev_strain_dir, double softening_cap, int scheme, double tau,
+                                 mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && nz > 0 && M > 0, "mgk_kmc3d_barrier: bad shape");
+  MGK_REQUIRE(Q && Q0 && sig && catalog && soft_prop && last_event_time, "mgk_kmc3d_barrier: null argument");
+  MGK_REQUIRE(scheme == 0 || (scheme == 1 && prev_strain_dir), "mgk_kmc3d_barrier: bad scheme");
+  const long long nvox = (long long)nx * ny * nz;
+  barrier_kernel<3, 4><<<blocks_for(nvox * M, 256), 256, 0, (cudaStream_t)stream>>>(
+      nvox, M, Q, Q0, sig, catalog, volume, soft_prop, last_event_time, current_time, prev_strain_dir,
+      softening_cap, scheme, tau);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc3d_rates(int nx, int ny, int nz, int M, const double* Q, double volume,
+                               const double* temperature, double temperature_scalar, double nu0, int cascade_mode,
+                               double* rates, int64_t* indices, double* prefix, int64_t* d_count, double* d_total,
+                               void* work, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && nz > 0 && M > 0, "mgk_kmc3d_rates: bad shape");
+  MGK_REQUIRE(Q && rates && indices && prefix && d_count && d_total, "mgk_kmc3d_rates: null argument");
+  return kmc_rates_impl((long long)nx * ny * nz, M, Q, volume, temperature, temperature_scalar, nu0, cascade_mode,
+                        rates, indices, prefix, d_count, d_total, work, (cudaStream_t)stream);
+}
+
+extern "C" int mgk_kmc3d_flip(int nx, int ny, int nz, int M, double* eps_plastic, double* soft_prop,
+                              double* last_event_time, const double* catalog, int x, int y, int z, int m,
+                              double current_time, double jp, double jt, double g_max, double jn_frac,
+                              mgk_stream_t stream) {
+  MGK_REQUIRE(x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz && m >= 0 && m < M,
+              "mgk_kmc3d_flip: index out of range");
+  MGK_REQUIRE(eps_plastic && soft_prop && last_event_time && catalog, "mgk_kmc3d_flip: null argument");
+  flip3d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, nz, M, eps_plastic, soft_prop, last_event_time, catalog,
+                                                   x, y, z, m, current_time, jp, jt, g_max, jn_frac);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

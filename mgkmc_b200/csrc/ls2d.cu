@@ -757,8 +757,8 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
   MGK_REQUIRE(precision == MGK_FP64 || precision == MGK_MIXED, "mgk_ls2d_create: bad precision");
   for (int r = 0; r < nrep; ++r) {
     FftLen f;
-    MGK_REQUIRE(fft_schedule(nxs[r], &f) && fft_schedule(nys[r], &f),
-                "mgk_ls2d_create: grid %dx%d unsupported (each side must be 2^a 3^b, even, 4..4096)", nxs[r],
+    MGK_REQUIRE(fft_schedule(nxs[r], &f) && fft_schedule(nys[r], &f) && nxs[r] % 2 == 0,
+                "mgk_ls2d_create: grid %dx%d unsupported (each side 2^a 3^b up to 4096, nx even)", nxs[r],
                 nys[r]);
     MGK_REQUIRE(2 * 3 * (size_t)nys[r] * sizeof(double2) <= 220 * 1024 &&
                     2 * 3 * (size_t)pick_tc(nxs[r], sizeof(double2), 64 * 1024) * nxs[r] * sizeof(double2) <=
@@ -1383,12 +1383,12 @@ extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const doub
                                       const double* eps_plastic, const double* eps_bar, const double* eps_init,
                                       double* eps_out, double* sig_out, int max_iter, double tol,
                                       mgk_ls_info* info, mgk_stream_t stream) {
-  MGK_REQUIRE(nx >= 4 && ny >= 4 && nx <= MGK_NOALLOC_MAX_SIDE && ny <= MGK_NOALLOC_MAX_SIDE,
+  MGK_REQUIRE(nx >= 2 && ny >= 1 && nx <= MGK_NOALLOC_MAX_SIDE && ny <= MGK_NOALLOC_MAX_SIDE,
               "mgk_ls2d_solve_noalloc: grid %dx%d exceeds the maximum of %dx%d for the allocation-free entry "
               "point (use mgk_ls2d_create/mgk_ls2d_solve)", nx, ny, MGK_NOALLOC_MAX_SIDE, MGK_NOALLOC_MAX_SIDE);
   FftLen fx, fy;
-  MGK_REQUIRE(fft_schedule(nx, &fx) && fft_schedule(ny, &fy),
-              "mgk_ls2d_solve_noalloc: grid %dx%d unsupported (each side must be 2^a 3^b, even)", nx, ny);
+  MGK_REQUIRE(fft_schedule(nx, &fx) && fft_schedule(ny, &fy) && nx % 2 == 0,
+              "mgk_ls2d_solve_noalloc: grid %dx%d unsupported (each side 2^a 3^b, nx even)", nx, ny);
   MGK_REQUIRE(plane_mode == MGK_PLANE_STRAIN || plane_mode == MGK_PLANE_STRESS,
               "mgk_ls2d_solve_noalloc: plane_mode must be 0 (strain) or 1 (stress)");
   MGK_REQUIRE(E && nu && eps_bar && eps_out && sig_out, "mgk_ls2d_solve_noalloc: null argument");

@@ -1,0 +1,920 @@
+// 3D small-strain Lippmann-Schwinger solver (FP64), batched over replicas.
+//
+// Restates mgkmc/linear_elastic_simulator.py:274-376 (spectral_solver_3d) and
+// the 3D Green operator of mgkmc/elasticity.py:70-105, applied on the fly:
+//   tau = C:(eps - eps_p) - C0:eps;  eps_new = eps_bar - IFFT(Gamma0 : FFT(tau));
+//   diff = ||eps_new - eps|| / (||eps|| + 1e-20).
+//
+// HBM layout per replica, N = nx*ny*nz (C order, z fastest):
+//   mu, lam           2 planes
+//   eps[6]            symmetric components xx, yy, zz, yz, xz, xy
+//   ep[6]             eigenstrain, symmetric components
+//   epf[9]            eigenstrain as given (only when given; output stress)
+//   spec[6]           half spectrum [c][x][y][kz], kz < nz/2+1
+// The antisymmetric part of eps is uniform after the first iteration and is
+// carried as three scalars.
+//
+// One iteration = four kernels:
+//   zline  (CTA per pair of z-lines): C2R along z of the previous spectrum,
+//          eps update, diff/norm partials (+ device convergence decision),
+//          tau, R2C along z;
+//   axis   FFT along y (forward);
+//   xgamma FFT along x, eps~^ = -Gamma0_sym : tau^ / N, IFFT along x;
+//   axis   IFFT along y.
+// Nyquist handling and the device-driven CUDA-graph loop are as in the 2D
+// solver (ls2d.cu): Gamma_sym averages Gamma over q and its mirror in the
+// Nyquist components, with numpy's fftfreq signs.
+#include <math.h>
+#include <stddef.h>
+#include <stdlib.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace mgk {
+
+const void* twiddles(int n, int prec);
+
+struct Ls3dRep {
+  int nx, ny, nz, nzh, ld, tc;
+  int zl_items;      // z-line pairs = nx*ny/2
+  int y_items;       // nx * ceil(nzh/tc)
+  int x_items;       // ny * ceil(nzh/tc)
+  long long N;
+  FftLen fx, fy, fz;
+  double* mu;
+  double* lam;
+  double* eps;   // 6 planes
+  double* ep;    // 6 planes
+  double* epf;   // 9 planes or null
+  double2* spec;
+  // per call
+  const double* init;
+  double* out_eps;
+  double* out_sig;
+  double eb[9];
+  double tol;
+  int max_iter;
+  int zl_first;
+};
+
+struct Ls3dState {
+  double mu0, lam0, Bc, inv2mu0;
+  double ebar[6];
+  double abar[3];  // (xy - yx)/2, (xz - zx)/2, (yz - zy)/2 of eps_bar
+  double extra_d0, extra_n0;
+  int iter, done, status, pad;
+  double diff;
+  double means[9];
+  double out_eps_mean[9];
+  double out_sig_mean[9];
+};
+
+struct Ls3dCtl {
+  unsigned int n_active, decided, still, bodies;
+  int any;
+};
+
+// symmetric component c -> (i, j): xx yy zz yz xz xy
+__device__ __constant__ int kSymI[6] = {0, 1, 2, 1, 0, 0};
+__device__ __constant__ int kSymJ[6] = {0, 1, 2, 2, 2, 1};
+
+__device__ __forceinline__ int fftfreq3(int k, int n) { return (k < (n + 1) / 2) ? k : k - n; }
+
+// eps~^ = -Gamma0(n) : tau^ for symmetric tau (3D), n a unit vector.
+// t[6] / e[6] in the symmetric order above.
+__device__ __forceinline__ void gamma3d_apply(const double2* t, double n0, double n1, double n2, double inv2mu0,
+                                              double Bc, double2* e) {
+  const double n[3] = {n0, n1, n2};
+  // full symmetric tau as 3x3 of complex
+  double2 T[3][3];
+  T[0][0] = t[0]; T[1][1] = t[1]; T[2][2] = t[2];
+  T[1][2] = T[2][1] = t[3];
+  T[0][2] = T[2][0] = t[4];
+  T[0][1] = T[1][0] = t[5];
+  double2 tn[3];
+  for (int i = 0; i < 3; ++i) {
+    tn[i].x = T[i][0].x * n[0] + T[i][1].x * n[1] + T[i][2].x * n[2];
+    tn[i].y = T[i][0].y * n[0] + T[i][1].y * n[1] + T[i][2].y * n[2];
+  }
+  double2 ntn;
+  ntn.x = tn[0].x * n[0] + tn[1].x * n[1] + tn[2].x * n[2];
+  ntn.y = tn[0].y * n[0] + tn[1].y * n[1] + tn[2].y * n[2];
+  for (int c = 0; c < 6; ++c) {
+    const int k = kSymI[c], h = kSymJ[c];
+    e[c].x = -(inv2mu0 * (n[h] * tn[k].x + n[k] * tn[h].x) - Bc * n[k] * n[h] * ntn.x);
+    e[c].y = -(inv2mu0 * (n[h] * tn[k].y + n[k] * tn[h].y) - Bc * n[k] * n[h] * ntn.y);
+  }
+}
+
+// -------------------------------------------------------------- kernels ---
+
+__global__ void ls3d_material_kernel(const Ls3dRep* reps, int rep, const double* __restrict__ E,
+                                     const double* __restrict__ nu, const double* __restrict__ epsp,
+                                     int set_moduli, double* partials) {
+  __shared__ double red[32];
+  const Ls3dRep& R = reps[rep];
+  const long long N = R.N;
+  double sE = 0, sn = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (set_moduli) {
+      // elasticity.py:55-59
+      const double e = E[i], v = nu[i];
+      R.mu[i] = e / (2 * (1 + v));
+      R.lam[i] = e * v / ((1 + v) * (1 - 2 * v));
+      sE += e;
+      sn += v;
+    }
+    double p[9];
+    for (int q = 0; q < 9; ++q) p[q] = epsp ? epsp[9 * i + q] : 0.0;
+    for (int c = 0; c < 6; ++c) {
+      const int a = 3 * kSymI[c] + kSymJ[c], b = 3 * kSymJ[c] + kSymI[c];
+      R.ep[c * N + i] = (p[a] == p[b]) ? p[a] : 0.5 * (p[a] + p[b]);
+    }
+    if (R.epf)
+      for (int q = 0; q < 9; ++q) R.epf[q * N + i] = p[q];
+  }
+  if (set_moduli) {
+    double a = block_sum(sE, red);
+    double b = block_sum(sn, red);
+    if (threadIdx.x == 0) { partials[2 * blockIdx.x] = a; partials[2 * blockIdx.x + 1] = b; }
+  }
+}
+
+__global__ void ls3d_medium_kernel(const Ls3dRep* reps, Ls3dState* st, int rep, const double* partials, int nb) {
+  __shared__ double red[32];
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) { a += partials[2 * i]; b += partials[2 * i + 1]; }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x == 0) {
+    const double N = (double)reps[rep].N;
+    const double E = a / N, v = b / N;
+    const double mu0 = E / (2 * (1 + v)), lam0 = E * v / ((1 + v) * (1 - 2 * v));
+    Ls3dState& S = st[rep];
+    S.mu0 = mu0;
+    S.lam0 = lam0;
+    S.Bc = (lam0 + mu0) / (mu0 * (lam0 + 2 * mu0));
+    S.inv2mu0 = 1.0 / (2 * mu0);
+  }
+}
+
+// per-CTA partials of the 9 components of the warm-start field; grid (G, nsel)
+__global__ void ls3d_means_kernel(const Ls3dRep* reps, const int* sel, double* partials) {
+  __shared__ double red[32];
+  const Ls3dRep& R = reps[sel[blockIdx.y]];
+  if (!R.init) return;
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < R.N;
+       i += (long long)gridDim.x * blockDim.x)
+    for (int q = 0; q < 9; ++q) s[q] += R.init[9 * i + q];
+  for (int q = 0; q < 9; ++q) {
+    double t = block_sum(s[q], red);
+    if (threadIdx.x == 0) partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 18 + q] = t;
+  }
+}
+
+// fixed-order sums (stride 18 per CTA slot); mode 0: means of every replica,
+// 1: means for warm-started replicas, 2: plain sums for warm-started replicas
+__global__ void ls3d_finalize_kernel(const Ls3dRep* reps, Ls3dState* st, const int* sel, const double* partials,
+                                     int G, int K, int off, int mode) {
+  __shared__ double red[32];
+  const int r = sel[blockIdx.x];
+  if (mode && !reps[r].init) return;
+  const double scale = mode == 2 ? 1.0 : 1.0 / (double)reps[r].N;
+  double* out = reinterpret_cast<double*>(reinterpret_cast<char*>(&st[r]) + off);
+  for (int q = 0; q < K; ++q) {
+    double a = 0;
+    for (int i = threadIdx.x; i < G; i += blockDim.x) a += partials[((size_t)blockIdx.x * G + i) * 18 + q];
+    a = block_sum(a, red);
+    if (threadIdx.x == 0) out[q] = a * scale;
+  }
+}
+
+// initial field (linear_elastic_simulator.py:302-313); grid (G, nsel)
+__global__ void ls3d_begin_kernel(const Ls3dRep* reps, Ls3dState* st, const int* sel, double* partials) {
+  __shared__ double red[32];
+  const int r = sel[blockIdx.y];
+  const Ls3dRep& R = reps[r];
+  Ls3dState& S = st[r];
+  const long long N = R.N;
+  const double* eb = R.eb;
+  double ab[3] = {0.5 * (eb[1] - eb[3]), 0.5 * (eb[2] - eb[6]), 0.5 * (eb[5] - eb[7])};
+  double sb[6];
+  for (int c = 0; c < 6; ++c) {
+    const int a = 3 * kSymI[c] + kSymJ[c], b = 3 * kSymJ[c] + kSymI[c];
+    sb[c] = (eb[a] == eb[b]) ? eb[a] : 0.5 * (eb[a] + eb[b]);
+  }
+  double d2 = 0, n2 = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (R.init) {
+      double v[9];
+      for (int q = 0; q < 9; ++q) v[q] = R.init[9 * i + q] + (eb[q] - S.means[q]);
+      for (int c = 0; c < 6; ++c) {
+        const int a = 3 * kSymI[c] + kSymJ[c], b = 3 * kSymJ[c] + kSymI[c];
+        R.eps[c * N + i] = (v[a] == v[b]) ? v[a] : 0.5 * (v[a] + v[b]);
+      }
+      const double a0[3] = {0.5 * (v[1] - v[3]), 0.5 * (v[2] - v[6]), 0.5 * (v[5] - v[7])};
+      for (int q = 0; q < 3; ++q) {
+        d2 += 2 * (ab[q] - a0[q]) * (ab[q] - a0[q]);
+        n2 += 2 * a0[q] * a0[q];
+      }
+    } else {
+      for (int c = 0; c < 6; ++c) R.eps[c * N + i] = sb[c];
+    }
+  }
+  if (R.init) {
+    d2 = block_sum(d2, red);
+    n2 = block_sum(n2, red);
+    if (threadIdx.x == 0) {
+      partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 18 + 0] = d2;
+      partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 18 + 1] = n2;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int c = 0; c < 6; ++c) S.ebar[c] = sb[c];
+    for (int q = 0; q < 3; ++q) S.abar[q] = ab[q];
+    S.iter = 0;
+    S.done = R.max_iter <= 0 ? 2 : 0;
+    S.status = MGK_OK;
+    S.diff = 0;
+    if (!R.init) {
+      S.extra_d0 = 0;
+      S.extra_n0 = 2.0 * (double)N * (ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
+    }
+  }
+}
+
+// z-line kernel: pairs of z-lines (flattened (x, y) index 2p, 2p+1)
+template <bool IN_SPEC>
+__global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
+                                                        const int* __restrict__ map, const int* __restrict__ loc,
+                                                        double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
+                                                        cudaGraphConditionalHandle cond, int use_cond,
+                                                        int guard_cap) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  __shared__ int s_last;
+  const int item = blockIdx.x;
+  const int r = map[item];
+  const Ls3dRep& R = reps[r];
+  Ls3dState& S = st[r];
+  if (IN_SPEC && use_cond && item == 0 && threadIdx.x == 0) {
+    const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap) {
+      ctl->any = 0;
+      cudaGraphSetConditional(cond, 0u);
+    }
+  }
+  if (S.done != 0) return;
+  const int nz = R.nz, nzh = R.nzh, ld = R.ld;
+  const long long N = R.N;
+  const long long l0 = 2LL * loc[item];  // first line (flattened x*ny + y)
+  const long long plane = (long long)R.nx * R.ny * ld;  // complex elements per component
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 6 * nz;
+  C* spec = R.spec;
+  double d2 = 0, n2 = 0;
+  C* cur = bufA;
+  if (IN_SPEC) {
+    const int tot = 6 * nz;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      const int c = e / nz, k = e - c * nz;
+      const int ks = (2 * k <= nz) ? k : nz - k;
+      const C* ra = spec + c * plane + l0 * ld;
+      C a = ra[ks], b = ra[ld + ks];
+      C z;
+      if (2 * k <= nz) {
+        if (k == 0 || 2 * k == nz) { a.y = 0; b.y = 0; }
+        z = make_double2(a.x - b.y, a.y + b.x);
+      } else {
+        z = make_double2(a.x + b.y, b.x - a.y);
+      }
+      bufA[e] = z;
+    }
+    __syncthreads();
+    cur = fft_lines<+1>(bufA, bufB, 6, nz, R.fz);
+  }
+  C* out = (IN_SPEC && cur == bufA) ? bufB : bufA;
+  const double mu0 = S.mu0, lam0 = S.lam0;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double tr[2][6];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long i = (l0 + h) * nz + z;
+      double e[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const double o = R.eps[c * N + i];
+        if (IN_SPEC) {
+          const C zz = cur[c * nz + z];
+          const double nw = S.ebar[c] + (h == 0 ? zz.x : zz.y);
+          const double dd = nw - o;
+          const double w = c < 3 ? 1.0 : 2.0;
+          d2 += w * dd * dd;
+          n2 += w * o * o;
+          R.eps[c * N + i] = nw;
+          e[c] = nw;
+        } else {
+          e[c] = o;
+        }
+      }
+      const double m = R.mu[i], l = R.lam[i];
+      double d[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) d[c] = e[c] - R.ep[c * N + i];
+      const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) tr[h][c] = (2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre);
+#pragma unroll
+      for (int c = 3; c < 6; ++c) tr[h][c] = 2 * m * d[c] - 2 * mu0 * e[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) out[c * nz + z] = make_double2(tr[0][c], tr[1][c]);
+  }
+  __syncthreads();
+  C* scratch = (out == bufA) ? bufB : bufA;
+  C* Z = fft_lines<-1>(out, scratch, 6, nz, R.fz);
+  for (int e = threadIdx.x; e < 6 * nzh; e += blockDim.x) {
+    const int c = e / nzh, k = e - c * nzh;
+    const C z = Z[c * nz + k];
+    const C w = Z[c * nz + (k == 0 ? 0 : nz - k)];
+    C* ra = spec + c * plane + l0 * ld;
+    ra[k] = make_double2(0.5 * (z.x + w.x), 0.5 * (z.y - w.y));
+    ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
+  }
+  if (!IN_SPEC) return;
+  d2 = block_sum(d2, red);
+  n2 = block_sum(n2, red);
+  if (threadIdx.x == 0) {
+    partials[2 * item] = d2;
+    partials[2 * item + 1] = n2;
+    __threadfence();
+    const unsigned int t = atomicInc(&rep_counter[r], (unsigned int)R.zl_items - 1);
+    s_last = (t == (unsigned int)R.zl_items - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < R.zl_items; i += blockDim.x) {
+    a += __ldcg(&partials[2 * (R.zl_first + i)]);
+    b += __ldcg(&partials[2 * (R.zl_first + i) + 1]);
+  }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x != 0) return;
+  if (S.iter == 0) { a += S.extra_d0; b += S.extra_n0; }
+  else b += 2.0 * (double)N * (S.abar[0] * S.abar[0] + S.abar[1] * S.abar[1] + S.abar[2] * S.abar[2]);
+  const double diff = sqrt(a) / (sqrt(b) + 1e-20);
+  S.diff = diff;
+  S.iter += 1;
+  int keep = 0;
+  if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
+  else if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
+  else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
+  else keep = 1;
+  const unsigned int n_act = ctl->n_active;
+  if (keep) atomicAdd(&ctl->still, 1u);
+  __threadfence();
+  const unsigned int dcount = atomicAdd(&ctl->decided, 1u);
+  if (dcount == n_act - 1) {
+    __threadfence();
+    const unsigned int still = atomicExch(&ctl->still, 0u);
+    ctl->decided = 0;
+    ctl->n_active = still;
+    const bool go = still > 0 && atomicAdd(&ctl->bodies, 0u) <= (unsigned int)guard_cap;
+    ctl->any = go ? 1 : 0;
+    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
+  }
+}
+
+// Strided-axis pass over tiles of tc consecutive kz columns.
+// AXIS = 1: FFT along y (SIGN given); AXIS = 0: FFT along x, Gamma0_sym,
+// IFFT along x.
+template <int AXIS, int SIGN>
+__global__ void __launch_bounds__(256) ls3d_axis_kernel(const Ls3dRep* __restrict__ reps,
+                                                       const Ls3dState* __restrict__ st,
+                                                       const int* __restrict__ map, const int* __restrict__ loc) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int item = blockIdx.x;
+  const int r = map[item];
+  const Ls3dRep& R = reps[r];
+  const Ls3dState& S = st[r];
+  if (S.done != 0) return;
+  const int nx = R.nx, ny = R.ny, nz = R.nz, nzh = R.nzh, ld = R.ld, tc = R.tc;
+  const int ntile = (nzh + tc - 1) / tc;
+  const int o = loc[item] / ntile;          // x (AXIS 1) or y (AXIS 0)
+  const int k0 = (loc[item] - o * ntile) * tc;
+  const int tcw = min(tc, nzh - k0);
+  const int n = AXIS == 1 ? ny : nx;
+  const FftLen& f = AXIS == 1 ? R.fy : R.fx;
+  const long long plane = (long long)nx * ny * ld;
+  const long long lstride = AXIS == 1 ? ld : (long long)ny * ld;
+  const long long obase = AXIS == 1 ? (long long)o * ny * ld : (long long)o * ld;
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 6 * tc * n;
+  C* spec = R.spec;
+  const int tot = 6 * tcw * n;
+  for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < tot) {
+        const int c = e / (tcw * n), rem = e - c * tcw * n, j = rem / tcw, t = rem - j * tcw;
+        v[u] = spec[c * plane + obase + j * lstride + k0 + t];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < tot) {
+        const int c = e / (tcw * n), rem = e - c * tcw * n, j = rem / tcw, t = rem - j * tcw;
+        bufA[(c * tc + t) * n + j] = v[u];
+      }
+    }
+  }
+  __syncthreads();
+  C* F;
+  if (AXIS == 1) {
+    F = fft_lines<SIGN>(bufA, bufB, 6 * tc, n, f);
+  } else {
+    C* G = fft_lines<-1>(bufA, bufB, 6 * tc, n, f);
+    const double scale = 1.0 / (double)R.N;
+    const int ky = o;
+    const double uy = (double)fftfreq3(ky, ny) / ny;
+    const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
+    for (int e = threadIdx.x; e < tcw * n; e += blockDim.x) {
+      const int t = e / n, kx = e - t * n;
+      const int kz = k0 + t;
+      C tv[6], ev[6];
+      for (int c = 0; c < 6; ++c) tv[c] = G[(c * tc + t) * n + kx];
+      if (kx == 0 && ky == 0 && kz == 0) {
+        for (int c = 0; c < 6; ++c) G[(c * tc + t) * n + kx] = make_double2(0.0, 0.0);
+        continue;
+      }
+      const double ux = (double)fftfreq3(kx, nx) / nx, uz = (double)fftfreq3(kz, nz) / nz;
+      const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
+      const double n0 = ux * inv, n1 = uy * inv, n2 = uz * inv;
+      gamma3d_apply(tv, n0, n1, n2, S.inv2mu0, S.Bc, ev);
+      const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
+      if (nqx || nqy || nqz) {
+        C fv[6];
+        gamma3d_apply(tv, nqx ? -n0 : n0, nqy ? -n1 : n1, nqz ? -n2 : n2, S.inv2mu0, S.Bc, fv);
+        for (int c = 0; c < 6; ++c) ev[c] = make_double2(0.5 * (ev[c].x + fv[c].x), 0.5 * (ev[c].y + fv[c].y));
+      }
+      for (int c = 0; c < 6; ++c) G[(c * tc + t) * n + kx] = make_double2(ev[c].x * scale, ev[c].y * scale);
+    }
+    __syncthreads();
+    C* H = (G == bufA) ? bufB : bufA;
+    F = fft_lines<+1>(G, H, 6 * tc, n, f);
+  }
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int c = e / (tcw * n), rem = e - c * tcw * n, j = rem / tcw, t = rem - j * tcw;
+    spec[c * plane + obase + j * lstride + k0 + t] = F[(c * tc + t) * n + j];
+  }
+}
+
+// outputs (nx,ny,nz,3,3) and partial sums for the means; grid (G, nsel)
+__global__ void ls3d_output_kernel(const Ls3dRep* reps, const Ls3dState* st, const int* sel, double* partials) {
+  __shared__ double red[32];
+  const int r = sel[blockIdx.y];
+  const Ls3dRep& R = reps[r];
+  const Ls3dState& S = st[r];
+  const long long N = R.N;
+  double s[18];
+  for (int q = 0; q < 18; ++q) s[q] = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    double e[9], p[9];
+    const double sxx = R.eps[i], syy = R.eps[N + i], szz = R.eps[2 * N + i];
+    const double syz = R.eps[3 * N + i], sxz = R.eps[4 * N + i], sxy = R.eps[5 * N + i];
+    e[0] = sxx; e[4] = syy; e[8] = szz;
+    e[1] = S.abar[0] == 0 ? sxy : sxy + S.abar[0];
+    e[3] = S.abar[0] == 0 ? sxy : sxy - S.abar[0];
+    e[2] = S.abar[1] == 0 ? sxz : sxz + S.abar[1];
+    e[6] = S.abar[1] == 0 ? sxz : sxz - S.abar[1];
+    e[5] = S.abar[2] == 0 ? syz : syz + S.abar[2];
+    e[7] = S.abar[2] == 0 ? syz : syz - S.abar[2];
+    if (R.epf) {
+      for (int q = 0; q < 9; ++q) p[q] = R.epf[q * N + i];
+    } else {
+      p[0] = R.ep[i]; p[4] = R.ep[N + i]; p[8] = R.ep[2 * N + i];
+      p[5] = p[7] = R.ep[3 * N + i];
+      p[2] = p[6] = R.ep[4 * N + i];
+      p[1] = p[3] = R.ep[5 * N + i];
+    }
+    const double mu = R.mu[i], lam = R.lam[i];
+    double d[9];
+    for (int q = 0; q < 9; ++q) d[q] = e[q] - p[q];
+    const double tr = d[0] + d[4] + d[8];
+    double sg[9];
+    for (int q = 0; q < 9; ++q) sg[q] = 2 * mu * d[q] + ((q % 4) == 0 ? lam * tr : 0.0);
+    for (int q = 0; q < 9; ++q) {
+      if (R.out_eps) R.out_eps[9 * i + q] = e[q];
+      if (R.out_sig) R.out_sig[9 * i + q] = sg[q];
+      s[q] += e[q];
+      s[9 + q] += sg[q];
+    }
+  }
+  for (int q = 0; q < 18; ++q) {
+    double t = block_sum(s[q], red);
+    if (threadIdx.x == 0) partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 18 + q] = t;
+  }
+}
+
+}  // namespace mgk
+
+// ================================================================== plan ===
+using namespace mgk;
+
+namespace {
+constexpr int kT3 = 256;
+constexpr int kG3 = 256;
+int g3(long long N) {
+  long long b = (N + kT3 - 1) / kT3;
+  return (int)std::max(1LL, std::min((long long)kG3, b));
+}
+int tc3(int n) {
+  int tc = 8;
+  while (tc > 1 && 2 * 6 * (size_t)tc * n * sizeof(double2) > 64 * 1024) tc >>= 1;
+  return tc;
+}
+}  // namespace
+
+struct mgk_ls3d_plan {
+  int nrep = 0;
+  long long maxN = 0;
+  size_t zl_smem = 0, ax_smem = 0;
+  std::vector<Ls3dRep> reps;
+  std::vector<char> has_material;
+  std::vector<void*> allocations;
+  Ls3dRep* h_reps = nullptr;
+  int* h_maps = nullptr;
+  Ls3dCtl* h_ctl = nullptr;
+  Ls3dState* h_state = nullptr;
+  cudaEvent_t staged = nullptr;
+  bool staged_pending = false;
+  Ls3dRep* d_reps = nullptr;
+  Ls3dState* d_st = nullptr;
+  Ls3dCtl* d_ctl = nullptr;
+  int* d_maps = nullptr;
+  unsigned int* d_repctr = nullptr;
+  double* d_part = nullptr;
+  double* d_mat_part = nullptr;
+  int tot_zl = 0, tot_y = 0, tot_x = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_mode = -1, graph_cap = 0;
+  int nsel = 0, s_zl = 0, s_y = 0, s_x = 0;
+};
+
+static int a3(mgk_ls3d_t p, void** ptr, size_t bytes) {
+  if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("mgk_ls3d: cudaMalloc of %zu bytes failed", bytes);
+    return MGK_OOM;
+  }
+  p->allocations.push_back(*ptr);
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls3d_destroy(mgk_ls3d_t p) {
+  if (!p) return MGK_OK;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->staged) cudaEventDestroy(p->staged);
+  for (void* a : p->allocations) cudaFree(a);
+  if (p->h_reps) cudaFreeHost(p->h_reps);
+  if (p->h_maps) cudaFreeHost(p->h_maps);
+  if (p->h_ctl) cudaFreeHost(p->h_ctl);
+  if (p->h_state) cudaFreeHost(p->h_state);
+  delete p;
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, const int* nzs, mgk_ls3d_t* out) {
+  MGK_REQUIRE(out, "mgk_ls3d_create: null output handle");
+  *out = nullptr;
+  MGK_REQUIRE(nrep >= 1 && nrep <= 4096 && nxs && nys && nzs, "mgk_ls3d_create: bad replica count");
+  for (int r = 0; r < nrep; ++r) {
+    FftLen f;
+    MGK_REQUIRE(fft_schedule(nxs[r], &f) && fft_schedule(nys[r], &f) && fft_schedule(nzs[r], &f),
+                "mgk_ls3d_create: grid %dx%dx%d unsupported (each side 2^a 3^b up to 4096)", nxs[r], nys[r],
+                nzs[r]);
+    MGK_REQUIRE(((long long)nxs[r] * nys[r]) % 2 == 0 /* z-lines are transformed in pairs */ && 2 * 6 * (size_t)nzs[r] * sizeof(double2) <= 220 * 1024 &&
+                    2 * 6 * (size_t)tc3(std::max(nxs[r], nys[r])) * std::max(nxs[r], nys[r]) * sizeof(double2) <=
+                        220 * 1024,
+                "mgk_ls3d_create: grid too large for the shared-memory FFT");
+  }
+  mgk_ls3d_t p = new mgk_ls3d_plan();
+  auto fail = [&](int s) { mgk_ls3d_destroy(p); return s; };
+  p->nrep = nrep;
+  p->reps.resize(nrep);
+  p->has_material.assign(nrep, 0);
+  for (int r = 0; r < nrep; ++r) {
+    Ls3dRep& R = p->reps[r];
+    memset(&R, 0, sizeof(R));
+    R.nx = nxs[r]; R.ny = nys[r]; R.nz = nzs[r];
+    R.nzh = R.nz / 2 + 1;
+    R.ld = R.nzh;
+    R.N = (long long)R.nx * R.ny * R.nz;
+    R.tc = tc3(std::max(R.nx, R.ny));
+    const int ntile = (R.nzh + R.tc - 1) / R.tc;
+    R.zl_items = R.nx * R.ny / 2;
+    R.y_items = R.nx * ntile;
+    R.x_items = R.ny * ntile;
+    fft_schedule(R.nx, &R.fx); fft_schedule(R.ny, &R.fy); fft_schedule(R.nz, &R.fz);
+    R.fx.tw = twiddles(R.nx, MGK_FP64); R.fy.tw = twiddles(R.ny, MGK_FP64); R.fz.tw = twiddles(R.nz, MGK_FP64);
+    if (!R.fx.tw || !R.fy.tw || !R.fz.tw) return fail(MGK_OOM);
+    p->zl_smem = std::max(p->zl_smem, 2 * 6 * (size_t)R.nz * sizeof(double2));
+    p->ax_smem = std::max(p->ax_smem, 2 * 6 * (size_t)R.tc * std::max(R.nx, R.ny) * sizeof(double2));
+    p->maxN = std::max(p->maxN, R.N);
+    p->tot_zl += R.zl_items; p->tot_y += R.y_items; p->tot_x += R.x_items;
+    void* f = nullptr;
+    int st = a3(p, &f, sizeof(double) * R.N * 23);
+    if (st) return fail(st);
+    double* d = reinterpret_cast<double*>(f);
+    R.mu = d; R.lam = d + R.N; R.eps = d + 2 * R.N; R.ep = d + 8 * R.N; R.epf = nullptr;
+    void* sp = nullptr;
+    st = a3(p, &sp, 6 * (size_t)R.nx * R.ny * R.ld * sizeof(double2));
+    if (st) return fail(st);
+    R.spec = reinterpret_cast<double2*>(sp);
+  }
+  int st;
+  if (cudaFuncSetAttribute(ls3d_zline_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zl_smem) ||
+      cudaFuncSetAttribute(ls3d_zline_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zl_smem) ||
+      cudaFuncSetAttribute(ls3d_axis_kernel<1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ax_smem) ||
+      cudaFuncSetAttribute(ls3d_axis_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ax_smem) ||
+      cudaFuncSetAttribute(ls3d_axis_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ax_smem)) {
+    set_error("mgk_ls3d_create: cudaFuncSetAttribute failed");
+    return fail(MGK_CUDA_ERROR);
+  }
+  const int G = g3(p->maxN);
+  const size_t part = std::max((size_t)2 * p->tot_zl, (size_t)nrep * G * 18);
+  void* v = nullptr;
+  if ((st = a3(p, &v, sizeof(double) * part))) return fail(st);
+  p->d_part = reinterpret_cast<double*>(v);
+  if ((st = a3(p, &v, sizeof(double) * 2 * kG3))) return fail(st);
+  p->d_mat_part = reinterpret_cast<double*>(v);
+  if ((st = a3(p, &v, sizeof(Ls3dRep) * nrep))) return fail(st);
+  p->d_reps = reinterpret_cast<Ls3dRep*>(v);
+  if ((st = a3(p, &v, sizeof(Ls3dState) * nrep))) return fail(st);
+  p->d_st = reinterpret_cast<Ls3dState*>(v);
+  if ((st = a3(p, &v, sizeof(Ls3dCtl)))) return fail(st);
+  p->d_ctl = reinterpret_cast<Ls3dCtl*>(v);
+  const size_t nm = 2 * (size_t)(p->tot_zl + p->tot_y + p->tot_x) + nrep;
+  if ((st = a3(p, &v, sizeof(int) * nm))) return fail(st);
+  p->d_maps = reinterpret_cast<int*>(v);
+  if ((st = a3(p, &v, sizeof(unsigned int) * nrep))) return fail(st);
+  p->d_repctr = reinterpret_cast<unsigned int*>(v);
+  if (cudaMemset(p->d_repctr, 0, sizeof(unsigned int) * nrep) || cudaMemset(p->d_st, 0, sizeof(Ls3dState) * nrep) ||
+      cudaMemset(p->d_ctl, 0, sizeof(Ls3dCtl)))
+    return fail(MGK_CUDA_ERROR);
+  if (cudaMallocHost(&p->h_reps, sizeof(Ls3dRep) * nrep) || cudaMallocHost(&p->h_maps, sizeof(int) * nm) ||
+      cudaMallocHost(&p->h_ctl, sizeof(Ls3dCtl)) || cudaMallocHost(&p->h_state, sizeof(Ls3dState) * nrep))
+    return fail(MGK_OOM);
+  if (cudaEventCreateWithFlags(&p->staged, cudaEventDisableTiming)) return fail(MGK_CUDA_ERROR);
+  memcpy(p->h_reps, p->reps.data(), sizeof(Ls3dRep) * nrep);
+  if (cudaMemcpy(p->d_reps, p->h_reps, sizeof(Ls3dRep) * nrep, cudaMemcpyHostToDevice)) return fail(MGK_CUDA_ERROR);
+  *out = p;
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls3d_create(int nx, int ny, int nz, mgk_ls3d_t* out) {
+  return mgk_ls3d_create_batch(1, &nx, &ny, &nz, out);
+}
+
+static int wait3(mgk_ls3d_t p) {
+  if (p->staged_pending) {
+    MGK_CUDA(cudaEventSynchronize(p->staged));
+    p->staged_pending = false;
+  }
+  return MGK_OK;
+}
+
+static int set3(mgk_ls3d_t p, int rep, const double* E, const double* nu, const double* epsp, int set_moduli,
+                cudaStream_t s) {
+  Ls3dRep& R = p->reps[rep];
+  const bool want = epsp != nullptr;
+  if (want != (R.epf != nullptr)) {
+    R.epf = want ? R.mu + 14 * R.N : nullptr;
+    int st = wait3(p);
+    if (st) return st;
+    p->h_reps[rep] = R;
+    MGK_CUDA(cudaMemcpyAsync(&p->d_reps[rep], &p->h_reps[rep], sizeof(Ls3dRep), cudaMemcpyHostToDevice, s));
+    MGK_CUDA(cudaEventRecord(p->staged, s));
+    p->staged_pending = true;
+  }
+  const int G = g3(R.N);
+  ls3d_material_kernel<<<G, kT3, 0, s>>>(p->d_reps, rep, E, nu, epsp, set_moduli, p->d_mat_part);
+  MGK_CUDA(cudaGetLastError());
+  if (set_moduli) {
+    ls3d_medium_kernel<<<1, kT3, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, G);
+    MGK_CUDA(cudaGetLastError());
+  }
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls3d_set_material_rep(mgk_ls3d_t p, int rep, const double* E, const double* nu,
+                                         const double* epsp, mgk_stream_t stream) {
+  MGK_REQUIRE(p && E && nu && rep >= 0 && rep < p->nrep, "mgk_ls3d_set_material: bad argument");
+  int st = set3(p, rep, E, nu, epsp, 1, (cudaStream_t)stream);
+  if (st == MGK_OK) p->has_material[rep] = 1;
+  return st;
+}
+
+extern "C" int mgk_ls3d_set_eigenstrain_rep(mgk_ls3d_t p, int rep, const double* epsp, mgk_stream_t stream) {
+  MGK_REQUIRE(p && rep >= 0 && rep < p->nrep && p->has_material[rep], "mgk_ls3d_set_eigenstrain: no material");
+  return set3(p, rep, nullptr, nullptr, epsp, 0, (cudaStream_t)stream);
+}
+
+struct Loop3 {
+  const Ls3dRep* reps;
+  Ls3dState* st;
+  const int *zm, *zl, *ym, *yl, *xm, *xl;
+  double* part;
+  unsigned int* ctr;
+  Ls3dCtl* ctl;
+  int nzl, ny, nx;
+  size_t zs, as;
+};
+
+static int body3(const Loop3& a, cudaStream_t s) {
+  ls3d_axis_kernel<1, -1><<<a.ny, kT3, a.as, s>>>(a.reps, a.st, a.ym, a.yl);
+  ls3d_axis_kernel<0, 0><<<a.nx, kT3, a.as, s>>>(a.reps, a.st, a.xm, a.xl);
+  ls3d_axis_kernel<1, 1><<<a.ny, kT3, a.as, s>>>(a.reps, a.st, a.ym, a.yl);
+  ls3d_zline_kernel<true><<<a.nzl, kT3, a.zs, s>>>(a.reps, a.st, a.zm, a.zl, a.part, a.ctr, a.ctl, 0, 0, 0);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
+  if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
+  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  cudaGraph_t g;
+  MGK_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) {
+    cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR;
+  }
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t w;
+  if (cudaGraphAddNode(&w, g, nullptr, 0, &cp)) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraphNode_t prev = nullptr, node;
+  auto add = [&](void* fn, dim3 grid, size_t smem, void** args) {
+    cudaKernelNodeParams k;
+    memset(&k, 0, sizeof(k));
+    k.func = fn; k.gridDim = grid; k.blockDim = dim3(kT3); k.sharedMemBytes = (unsigned)smem; k.kernelParams = args;
+    cudaError_t e = cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &k);
+    prev = node;
+    return e;
+  };
+  void* ay[] = {&a.reps, &a.st, &a.ym, &a.yl};
+  void* ax[] = {&a.reps, &a.st, &a.xm, &a.xl};
+  int use = 1;
+  void* az[] = {&a.reps, &a.st, &a.zm, &a.zl, &a.part, &a.ctr, &a.ctl, &h, &use, &cap};
+  cudaError_t e = add((void*)ls3d_axis_kernel<1, -1>, dim3(a.ny), a.as, ay);
+  if (!e) e = add((void*)ls3d_axis_kernel<0, 0>, dim3(a.nx), a.as, ax);
+  if (!e) e = add((void*)ls3d_axis_kernel<1, 1>, dim3(a.ny), a.as, ay);
+  if (!e) e = add((void*)ls3d_zline_kernel<true>, dim3(a.nzl), a.zs, az);
+  cudaGraphExec_t x = nullptr;
+  if (!e) e = cudaGraphInstantiate(&x, g, 0);
+  if (e) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  p->graph = g;
+  p->exec = x;
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, const double* eps_bar,
+                                    const double* const* eps_init, double* const* eps_out, double* const* sig_out,
+                                    int max_iter, double tol, mgk_ls_info3* infos, mgk_stream_t stream) {
+  MGK_REQUIRE(p && eps_bar && nsel >= 1 && nsel <= p->nrep, "mgk_ls3d_solve_batch: bad argument");
+  MGK_REQUIRE(max_iter >= 0 && max_iter <= 1000000, "mgk_ls3d_solve: max_iter out of range");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<int> selv(nsel);
+  std::vector<char> seen(p->nrep, 0);
+  for (int q = 0; q < nsel; ++q) {
+    const int r = sel ? sel[q] : q;
+    MGK_REQUIRE(r >= 0 && r < p->nrep && !seen[r], "mgk_ls3d_solve_batch: bad or repeated replica index");
+    MGK_REQUIRE(p->has_material[r], "mgk_ls3d_solve: replica %d has no material", r);
+    seen[r] = 1;
+    selv[q] = r;
+  }
+  int rc = wait3(p);
+  if (rc) return rc;
+  int nzl = 0, ny_ = 0, nx_ = 0;
+  for (int r : selv) { nzl += p->reps[r].zl_items; ny_ += p->reps[r].y_items; nx_ += p->reps[r].x_items; }
+  const bool changed = nzl != p->s_zl || ny_ != p->s_y || nx_ != p->s_x || nsel != p->nsel;
+  int* zm = p->h_maps; int* zl = zm + nzl; int* ym = zl + nzl; int* yl = ym + ny_;
+  int* xm = yl + ny_; int* xl = xm + nx_; int* sp = xl + nx_;
+  int zi = 0, yi = 0, xi = 0;
+  for (int q = 0; q < nsel; ++q) {
+    const int r = selv[q];
+    Ls3dRep& H = p->h_reps[r];
+    H = p->reps[r];
+    H.init = eps_init ? eps_init[q] : nullptr;
+    H.out_eps = eps_out ? eps_out[q] : nullptr;
+    H.out_sig = sig_out ? sig_out[q] : nullptr;
+    for (int k = 0; k < 9; ++k) H.eb[k] = eps_bar[9 * q + k];
+    H.tol = tol;
+    H.max_iter = max_iter;
+    H.zl_first = zi;
+    for (int i = 0; i < H.zl_items; ++i) { zm[zi] = r; zl[zi] = i; ++zi; }
+    for (int i = 0; i < H.y_items; ++i) { ym[yi] = r; yl[yi] = i; ++yi; }
+    for (int i = 0; i < H.x_items; ++i) { xm[xi] = r; xl[xi] = i; ++xi; }
+    sp[q] = r;
+  }
+  const int n_active = max_iter > 0 ? nsel : 0;
+  *p->h_ctl = Ls3dCtl{(unsigned int)n_active, 0u, 0u, 0u, n_active > 0};
+  const size_t nm = 2 * (size_t)(nzl + ny_ + nx_) + nsel;
+  MGK_CUDA(cudaMemcpyAsync(p->d_maps, p->h_maps, sizeof(int) * nm, cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaMemcpyAsync(p->d_reps, p->h_reps, sizeof(Ls3dRep) * p->nrep, cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaMemcpyAsync(p->d_ctl, p->h_ctl, sizeof(Ls3dCtl), cudaMemcpyHostToDevice, s));
+  MGK_CUDA(cudaEventRecord(p->staged, s));
+  p->staged_pending = true;
+  p->s_zl = nzl; p->s_y = ny_; p->s_x = nx_; p->nsel = nsel;
+  const int* d_zm = p->d_maps; const int* d_zl = d_zm + nzl; const int* d_ym = d_zl + nzl;
+  const int* d_yl = d_ym + ny_; const int* d_xm = d_yl + ny_; const int* d_xl = d_xm + nx_;
+  const int* d_sel = d_xl + nx_;
+  const int G = g3(p->maxN);
+  bool any_init = false;
+  for (int q = 0; q < nsel && eps_init; ++q) any_init |= eps_init[q] != nullptr;
+  if (any_init) {
+    ls3d_means_kernel<<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, d_sel, p->d_part);
+    ls3d_finalize_kernel<<<nsel, kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 9,
+                                              (int)offsetof(Ls3dState, means), 1);
+    MGK_CUDA(cudaGetLastError());
+  }
+  ls3d_begin_kernel<<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  MGK_CUDA(cudaGetLastError());
+  if (any_init) {
+    ls3d_finalize_kernel<<<nsel, kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 2,
+                                              (int)offsetof(Ls3dState, extra_d0), 2);
+    MGK_CUDA(cudaGetLastError());
+  }
+  if (n_active > 0) {
+    Loop3 a{p->d_reps, p->d_st, d_zm, d_zl, d_ym, d_yl, d_xm, d_xl, p->d_part, p->d_repctr, p->d_ctl,
+            nzl, ny_, nx_, p->zl_smem, p->ax_smem};
+    ls3d_zline_kernel<false><<<nzl, kT3, p->zl_smem, s>>>(p->d_reps, p->d_st, d_zm, d_zl, p->d_part, p->d_repctr,
+                                                          p->d_ctl, 0, 0, 0);
+    MGK_CUDA(cudaGetLastError());
+    const int cap = max_iter + 2 > 1000 ? max_iter + 2 : 1000;
+    if (p->graph_mode == 1 && (changed || cap > p->graph_cap)) p->graph_mode = -1;
+    if (p->graph_mode < 0) {
+      const char* env = getenv("MGK_NO_GRAPH_WHILE");
+      if (env && env[0] == '1') p->graph_mode = 0;
+      else {
+        p->graph_mode = graph3(p, a, cap) == MGK_OK ? 1 : 0;
+        p->graph_cap = cap;
+      }
+    }
+    if (p->graph_mode == 1) {
+      MGK_CUDA(cudaGraphLaunch(p->exec, s));
+    } else {
+      for (int it = 0; it < max_iter; ++it) {
+        rc = body3(a, s);
+        if (rc) return rc;
+        Ls3dCtl hc;
+        MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls3dCtl), cudaMemcpyDeviceToHost, s));
+        MGK_CUDA(cudaStreamSynchronize(s));
+        if (!hc.any) break;
+      }
+    }
+  }
+  ls3d_output_kernel<<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  MGK_CUDA(cudaGetLastError());
+  ls3d_finalize_kernel<<<nsel, kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 18,
+                                            (int)offsetof(Ls3dState, out_eps_mean), 0);
+  MGK_CUDA(cudaGetLastError());
+  if (infos) {
+    MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls3dState) * p->nrep, cudaMemcpyDeviceToHost, s));
+    MGK_CUDA(cudaStreamSynchronize(s));
+    int worst = MGK_OK;
+    for (int q = 0; q < nsel; ++q) {
+      const Ls3dState& S = p->h_state[selv[q]];
+      infos[q].iterations = S.iter;
+      infos[q].status = S.status;
+      infos[q].final_diff = S.diff;
+      for (int k = 0; k < 9; ++k) { infos[q].eps_mean[k] = S.out_eps_mean[k]; infos[q].sig_mean[k] = S.out_sig_mean[k]; }
+      if (S.status == MGK_NONFINITE) worst = MGK_NONFINITE;
+    }
+    if (worst) { set_error("mgk_ls3d_solve: non-finite residual"); return worst; }
+  }
+  return MGK_OK;
+}

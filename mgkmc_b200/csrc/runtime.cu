@@ -23,11 +23,11 @@ void set_error(const char* fmt, ...) {
 }
 
 bool fft_schedule(int n, FftLen* f) {
-  if (n < 4 || n > 4096) return false;
+  if (n < 1 || n > 4096) return false;
   int m = n, a = 0, b = 0;
   while (m % 3 == 0) { m /= 3; ++b; }
   while (m % 2 == 0) { m /= 2; ++a; }
-  if (m != 1 || a < 1) return false;
+  if (m != 1) return false;
   int np = 0;
   for (int i = 0; i < b; ++i) f->radix[np++] = 3;
   int p8 = a / 3, rem = a % 3;

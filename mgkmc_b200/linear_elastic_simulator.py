@@ -167,3 +167,92 @@ def spectral_solver_2d(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6,
     eps_np = eps.cpu().numpy()
     sig_np = sig.cpu().numpy()
     return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
+
+
+class Ls3dBatch:
+    """Plan-owning batch of 3D LS replicas (FP64).  Fields: E, nu (nx,ny,nz);
+    eps_plastic, eps, sig (nx,ny,nz,3,3) torch float64 CUDA tensors."""
+
+    def __init__(self, sizes, device=None):
+        torch = _torch()
+        self.sizes = [tuple(int(v) for v in s) for s in sizes]
+        self.nrep = len(self.sizes)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        nx = (ctypes.c_int * self.nrep)(*[s[0] for s in self.sizes])
+        ny = (ctypes.c_int * self.nrep)(*[s[1] for s in self.sizes])
+        nz = (ctypes.c_int * self.nrep)(*[s[2] for s in self.sizes])
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(L.lib().mgk_ls3d_create_batch(self.nrep, nx, ny, nz, ctypes.byref(h)), "mgk_ls3d_create_batch")
+        self._h = h
+        self._keep = {}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                L.lib().mgk_ls3d_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_material(self, rep, E, nu, eps_plastic=None, stream=None):
+        self._keep[("m", rep)] = (E, nu, eps_plastic)
+        L.check(L.lib().mgk_ls3d_set_material_rep(self._h, int(rep), L.ptr(E), L.ptr(nu), L.ptr(eps_plastic),
+                                                  L.stream_ptr(stream)), "mgk_ls3d_set_material")
+
+    def set_eigenstrain(self, rep, eps_plastic, stream=None):
+        self._keep[("e", rep)] = eps_plastic
+        L.check(L.lib().mgk_ls3d_set_eigenstrain_rep(self._h, int(rep), L.ptr(eps_plastic), L.stream_ptr(stream)),
+                "mgk_ls3d_set_eigenstrain")
+
+    def solve(self, reps, eps_bars, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True,
+              stream=None):
+        n = len(reps)
+        sel = (ctypes.c_int * n)(*[int(r) for r in reps])
+        eb = (ctypes.c_double * (9 * n))(*np.concatenate([np.asarray(e, dtype=np.float64).reshape(9)
+                                                           for e in eps_bars]))
+        P = ctypes.c_void_p
+
+        def parr(ts):
+            return None if ts is None else (P * n)(*[None if t is None else t.data_ptr() for t in ts])
+
+        infos = (L.LsInfo3 * n)() if sync else None
+        st = L.lib().mgk_ls3d_solve_batch(self._h, n, sel, eb, parr(eps_init), parr(eps_out), parr(sig_out),
+                                          int(max_iter), float(tol), infos, L.stream_ptr(stream))
+        L.check(st, "mgk_ls3d_solve_batch", allow=(L.OK, L.NONFINITE))
+        return list(infos) if sync else None
+
+
+_PLANS3 = {}
+
+
+def spectral_solver_3d(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6, verbose=False, pixel=1.0,
+                       Gamma=None, eps_init=None):
+    """3D Lippmann-Schwinger solve (linear_elastic_simulator.py:274-376);
+    numpy in/out, same returns as the reference."""
+    torch = _torch()
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    shape = E.shape
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (shape, dev.index)
+    p = _PLANS3.get(key)
+    if p is None:
+        p = _PLANS3[key] = Ls3dBatch([shape])
+    tep = None if eps_plastic is None else torch.from_numpy(np.ascontiguousarray(eps_plastic, dtype=np.float64)).to(dev)
+    tin = None if eps_init is None else torch.from_numpy(np.ascontiguousarray(eps_init, dtype=np.float64)).to(dev)
+    eps = torch.empty(shape + (3, 3), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    p.set_material(0, torch.from_numpy(E).to(dev), torch.from_numpy(nu).to(dev), tep)
+    info = p.solve([0], [eps_bar], [eps], [sig], None if tin is None else [tin], max_iter, tol)[0]
+    if verbose:
+        print(f"LS 3D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
+    e, s = eps.cpu().numpy(), sig.cpu().numpy()
+    return e, s, e.mean(axis=(0, 1, 2)), s.mean(axis=(0, 1, 2))
+
+
+def update_stress_fft_full(eps_plastic_field, eps_macro, E, nu, pixel=1.0, max_iter=200, tol=1e-6, verbose=False):
+    """mgkmc/stz/update_fft.py:4-22: the 3D solve with an eigenstrain field."""
+    return spectral_solver_3d(E, nu, eps_macro, eps_plastic=eps_plastic_field, max_iter=max_iter, tol=tol,
+                              verbose=verbose, pixel=pixel)

@@ -96,3 +96,28 @@ def test_select_edges(K):
     assert K.select_event_2d_u(r, 1.0, 0.999) == OK.select_event_loop(r, 1.0, 0.999) == 2
     # total larger than the sum: falls off the end -> len-1
     assert K.select_event_2d_u(r, 2.0, 0.9) == OK.select_event_loop(r, 2.0, 0.9) == 3
+
+
+def test_kmc3d_golden():
+    from mgkmc_b200 import stz as S
+    from tests.conftest import load_golden
+    g = load_golden("kmc3d_6x5x4")
+    Q = np.zeros_like(g["Q0"])
+    S.compute_barrier(Q, g["Q0"], g["sig"], g["catalog"], 1.0, g["soft_prop"], g["last_event_time"], 1e-3,
+                      g["prev_dir"], 0.5, 1, 5e-4)
+    np.testing.assert_allclose(Q, g["Q"], rtol=0, atol=1e-14)
+    Q2 = np.zeros_like(g["Q0"])
+    S.compute_barrier(Q2, g["Q0"], g["sig"], g["catalog"], 1.0, g["soft_prop"], g["last_event_time"], 1e-3,
+                      g["prev_dir"], 0.5, 0, np.inf)
+    np.testing.assert_allclose(Q2, g["Q_iso"], rtol=0, atol=1e-14)
+    r, idx, total = S.compute_rates(g["Q"], 1.0, 300.0, 1e13, cascade_mode=False)
+    np.testing.assert_array_equal(idx, g["indices"])
+    np.testing.assert_allclose(r, g["rates"], rtol=1e-15, atol=0)
+    for u, k in zip(g["sel_u"], g["sel_idx"]):
+        assert S.select_event_u(g["rates"], float(g["total"]), u) == k
+    ep, sp, tl = g["flip_in_eps_p"].copy(), g["flip_in_soft"].copy(), g["flip_in_tlast"].copy()
+    for (x, y, z, m, t, jp, jt, gmax, jn) in g["flips"]:
+        S.apply_flip_soa(ep, None, sp, tl, g["catalog"], int(x), int(y), int(z), int(m), t, jp, jt, gmax, jn)
+    np.testing.assert_array_equal(ep, g["flip_out_eps_p"])
+    np.testing.assert_array_equal(sp, g["flip_out_soft"])
+    np.testing.assert_array_equal(tl, g["flip_out_tlast"])

@@ -1,0 +1,77 @@
+"""GPU parity of the 3D LS solver (mgk_ls3d_*) against the reference's golden
+outputs and the oracle; tolerance 1e-9 relative (max-abs over the field)."""
+import numpy as np
+import pytest
+
+from mgkmc_b200 import workloads as W
+from oracle import ls as OL
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-9
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("name", ["ls3d_8x8x8", "ls3d_12x8x6"])
+def test_golden(golden, name):
+    from mgkmc_b200.linear_elastic_simulator import spectral_solver_3d
+    g = golden(name)
+    eps, sig, _, _ = spectral_solver_3d(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=2, tol=0.0)
+    assert rel(eps, g["eps_it2"]) < TOL
+    assert rel(sig, g["sig_it2"]) < TOL
+    eps, sig, em, sm = spectral_solver_3d(g["E"], g["nu"], g["eps_bar"], g["eps_plastic"], max_iter=300, tol=1e-10)
+    assert rel(eps, g["eps_conv"]) < TOL
+    assert rel(sig, g["sig_conv"]) < TOL
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 12), (64, 48, 32), (8, 6, 1), (6, 9, 3)])
+def test_oracle_sizes(shape):
+    from mgkmc_b200.linear_elastic_simulator import spectral_solver_3d
+    rng = np.random.default_rng(sum(shape))
+    E, nu = W.ls3d_material(*shape, rng)
+    ep = W.pure_shear_eigenstrain_3d(*shape, rng)
+    eb = np.zeros((3, 3)); eb[0, 0] = 0.01; eb[0, 1] = 0.003; eb[1, 0] = -0.001
+    o = OL.spectral_solver(E, nu, eb, ep, max_iter=200, tol=1e-10, return_info=True)
+    eps, sig, em, sm = spectral_solver_3d(E, nu, eb, ep, max_iter=200, tol=1e-10)
+    assert rel(eps, o[0]) < TOL and rel(sig, o[1]) < TOL
+
+
+def test_warm_start_and_batch():
+    import torch
+    from mgkmc_b200.linear_elastic_simulator import Ls3dBatch
+    sizes = [(16, 16, 16), (24, 24, 12)]
+    rng = np.random.default_rng(5)
+    probs = []
+    for s in sizes:
+        E, nu = W.ls3d_material(*s, rng)
+        probs.append((E, nu, W.pure_shear_eigenstrain_3d(*s, rng)))
+    B = Ls3dBatch(sizes)
+    outs, sigs = [], []
+    for r, (E, nu, ep) in enumerate(probs):
+        B.set_material(r, torch.from_numpy(E).cuda(), torch.from_numpy(nu).cuda(), torch.from_numpy(ep).cuda())
+        outs.append(torch.empty(E.shape + (3, 3), dtype=torch.float64, device="cuda"))
+        sigs.append(torch.empty_like(outs[-1]))
+    eb = np.diag([0.01, -0.002, 0.0])
+    B.solve([0, 1], [eb, eb], outs, sigs, max_iter=200, tol=1e-10)
+    for r, (E, nu, ep) in enumerate(probs):
+        o = OL.spectral_solver(E, nu, eb, ep, max_iter=200, tol=1e-10)
+        assert rel(outs[r].cpu().numpy(), o[0]) < TOL
+    init = [o.clone() for o in outs]
+    eb2 = eb + np.array([[0, 1e-3, 0], [0, 0, 0], [0, 0, 1e-3]])
+    B.solve([1], [eb2], [outs[1]], [sigs[1]], eps_init=[init[1]], max_iter=200, tol=1e-10)
+    E, nu, ep = probs[1]
+    o = OL.spectral_solver(E, nu, eb2, ep, max_iter=200, tol=1e-10, eps_init=init[1].cpu().numpy())
+    assert rel(outs[1].cpu().numpy(), o[0]) < TOL
+
+
+def test_barrier_physics_homogeneous_units():
+    # the reference's tests/test_barrier_physics.py:49-98 case: 16x16x1,
+    # homogeneous E = 70 GPa, nu = 0.3, eps_xx = 1 %: sigma_xx = (lam + 2 mu) eps
+    from mgkmc_b200.linear_elastic_simulator import spectral_solver_3d
+    E = np.full((16, 16, 1), 70e9); nu = np.full((16, 16, 1), 0.3)
+    eb = np.zeros((3, 3)); eb[0, 0] = 0.01
+    eps, sig, em, sm = spectral_solver_3d(E, nu, eb, max_iter=50, tol=1e-6)
+    lam = 70e9 * 0.3 / ((1 + 0.3) * (1 - 0.6)); mu = 70e9 / 2.6
+    assert abs(sm[0, 0] - (lam + 2 * mu) * 0.01) < 1e-6 * (lam + 2 * mu) * 0.01
