@@ -126,3 +126,90 @@ __device__ C* fft_lines(C* a, C* b, int nlines, int ld, const FftLen& f) {
 }
 
 }  // namespace mgk
+
+// ------------------------------------------------ compile-time lengths ---
+// The same Stockham passes with the radix schedule, strides and divisors
+// known at compile time (no integer division at run time), for the grid
+// sides the benchmark workloads use; other lengths take fft_lines.
+namespace mgk {
+
+struct RadixList {
+  int np;
+  int r[8];
+};
+
+// same schedule as fft_schedule(): radix-3 passes first, then radix 8, 4, 2
+constexpr RadixList make_sched(int n) {
+  RadixList s{0, {0, 0, 0, 0, 0, 0, 0, 0}};
+  int m = n, a = 0, b = 0;
+  while (m % 3 == 0) { m /= 3; ++b; }
+  while (m % 2 == 0) { m /= 2; ++a; }
+  for (int i = 0; i < b; ++i) s.r[s.np++] = 3;
+  int p8 = a / 3, rem = a % 3;
+  if (rem == 1 && p8 >= 1) { p8 -= 1; rem = 4; }
+  for (int i = 0; i < p8; ++i) s.r[s.np++] = 8;
+  if (rem == 4) { s.r[s.np++] = 4; s.r[s.np++] = 4; }
+  else if (rem == 2) s.r[s.np++] = 4;
+  else if (rem == 1) s.r[s.np++] = 2;
+  return s;
+}
+
+template <int N, int SIGN, int P, int NS, typename C>
+__device__ __forceinline__ C* stat_pass(C* a, C* b, int nlines, int ld, const C* __restrict__ tw) {
+  constexpr RadixList S = make_sched(N);
+  if constexpr (P == S.np) {
+    return a;
+  } else {
+    constexpr int R = S.r[P];
+    constexpr int nb = N / R;
+    constexpr int tws = N / (NS * R);
+    const int total = nlines * nb;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int line = t / nb;
+      const int j = t - line * nb;
+      const C* src = a + line * ld;
+      C* dst = b + line * ld;
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+      const int k = j % NS;
+      if (NS > 1 && k != 0) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = __ldg(&tw[r * k * tws]);
+          if (SIGN > 0) w.y = -w.y;
+          v[r] = cmul(v[r], w);
+        }
+      }
+      if constexpr (R == 2) dft2<SIGN>(v);
+      else if constexpr (R == 3) dft3<SIGN>(v);
+      else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+      else dft8<SIGN>(v);
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst[base + r * NS] = v[r];
+    }
+    __syncthreads();
+    return stat_pass<N, SIGN, P + 1, NS * R>(b, a, nlines, ld, tw);
+  }
+}
+
+// FFT of nlines lines: compile-time passes for the common lengths.
+template <int SIGN, typename C>
+__device__ __forceinline__ C* fft_any(C* a, C* b, int nlines, int ld, const FftLen& f) {
+  const C* tw = reinterpret_cast<const C*>(f.tw);
+  switch (f.n) {
+    case 64: return stat_pass<64, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 96: return stat_pass<96, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 128: return stat_pass<128, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 192: return stat_pass<192, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 256: return stat_pass<256, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 384: return stat_pass<384, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 512: return stat_pass<512, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 768: return stat_pass<768, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    case 1024: return stat_pass<1024, SIGN, 0, 1>(a, b, nlines, ld, tw);
+    default: return fft_lines<SIGN>(a, b, nlines, ld, f);
+  }
+}
+
+}  // namespace mgk

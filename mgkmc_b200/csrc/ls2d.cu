@@ -56,6 +56,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "tma.cuh"
 
 namespace mgk {
 
@@ -107,6 +108,7 @@ struct Ls2dCtl {
   unsigned int still;
   unsigned int bodies;    // loop bodies run in the current phase (guard)
   int any;
+  int error;              // a bounded wait gave up (MGK_TIMEOUT)
 };
 
 constexpr double kMixedPhase1Tol = 2e-6;
@@ -316,6 +318,53 @@ __global__ void ls2d_begin_kernel(const Ls2dRep* reps, Ls2dState* st, const int*
   }
 }
 
+// Convergence decision of replica r once the last of its row items has
+// written its partial sums (all threads of the CTA call; thread 0 decides).
+// The last replica to decide sets the graph while-node's condition.
+template <bool FINAL>
+__device__ void ls2d_decide(const Ls2dRep& R, Ls2dState& S, const double* partials, Ls2dCtl* ctl,
+                            cudaGraphConditionalHandle cond, int use_cond, int guard_cap, double* red) {
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < R.row_items; i += blockDim.x) {
+    a += __ldcg(&partials[2 * (R.row_first + i)]);
+    b += __ldcg(&partials[2 * (R.row_first + i) + 1]);
+  }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x != 0) return;
+  if (S.iter == 0) { a += S.extra_d0; b += S.extra_n0; }
+  else { b += 2.0 * (double)R.N * S.abar * S.abar; }
+  const double diff = sqrt(a) / (sqrt(b) + 1e-20);
+  S.diff = diff;
+  S.iter += 1;
+  S.phase_iter += 1;
+  int keep = 0;
+  if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
+  else if (FINAL) {
+    if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
+    else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
+    else keep = 1;
+  } else {
+    const double tol1 = R.tol > kMixedPhase1Tol ? R.tol : kMixedPhase1Tol;
+    if (S.iter >= R.max_iter) { S.done = 2; S.status = diff < R.tol ? MGK_OK : MGK_NOT_CONVERGED; }
+    else if (diff < tol1 || S.phase_iter >= kMixedPhase1Cap) S.done = 1;
+    else keep = 1;
+  }
+  const unsigned int n_act = ctl->n_active;  // stable until every active replica has decided
+  if (keep) atomicAdd(&ctl->still, 1u);
+  __threadfence();
+  const unsigned int d = atomicAdd(&ctl->decided, 1u);
+  if (d == n_act - 1) {
+    __threadfence();
+    const unsigned int still = atomicExch(&ctl->still, 0u);
+    ctl->decided = 0;
+    ctl->n_active = still;
+    const bool go = still > 0 && atomicAdd(&ctl->bodies, 0u) <= (unsigned int)guard_cap && *(volatile int*)&ctl->error == 0;
+    ctl->any = go ? 1 : 0;
+    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
+  }
+}
+
 // Row kernel.  IN_SPEC: the previous iteration's spectrum is inverted and the
 // field updated (with diff/norm and the convergence decision); otherwise the
 // field is read as is (first tau of a phase).  FINAL: this phase's decision
@@ -339,7 +388,7 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
     // a body with no active replica has no decider: stop here; the body
     // count bounds the loop whatever happens to the deciders
     const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
-    if (ctl->n_active == 0 || b > (unsigned int)guard_cap) {
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap || *(volatile int*)&ctl->error != 0) {
       ctl->any = 0;
       cudaGraphSetConditional(cond, 0u);
     }
@@ -394,7 +443,7 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
       }
     }
     __syncthreads();
-    cur = fft_lines<+1>(bufA, bufB, 3, ny, fy);
+    cur = fft_any<+1>(bufA, bufB, 3, ny, fy);
   }
   C* out = (IN_SPEC && cur == bufA) ? bufB : bufA;
   for (int y = threadIdx.x; y < ny; y += blockDim.x) {
@@ -431,7 +480,7 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
   }
   __syncthreads();
   C* scratch = (out == bufA) ? bufB : bufA;
-  C* Z = fft_lines<-1>(out, scratch, 3, ny, fy);
+  C* Z = fft_any<-1>(out, scratch, 3, ny, fy);
   for (int e = threadIdx.x; e < 3 * nyh; e += blockDim.x) {
     const int c = e / nyh, k = e - c * nyh;
     const C z = Z[c * ny + k];
@@ -454,44 +503,183 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  double a = 0, b = 0;
-  for (int i = threadIdx.x; i < R.row_items; i += blockDim.x) {
-    a += __ldcg(&partials[2 * (R.row_first + i)]);
-    b += __ldcg(&partials[2 * (R.row_first + i) + 1]);
+  ls2d_decide<FINAL>(R, S, partials, ctl, cond, use_cond, guard_cap, red);
+}
+
+// Persistent row kernel (IN_SPEC iterations) with double-buffered bulk
+// prefetch: each CTA walks the items blockIdx.x, +gridDim.x, ...; while it
+// transforms one row pair, the inputs of its next row pair (two spectrum rows
+// and two rows of eps, mu, lambda, eps_p, all contiguous) stream into the
+// other shared-memory stage through cp.async.bulk.  Requires ny even (16-byte
+// aligned rows).  Stage layout (bytes): spec [3][2][ld] C | eps [3][2][ny] |
+// mu [2][ny] | lam [2][ny] | ep [3][2][ny] (TS).
+template <typename TS, typename TC, bool FINAL>
+__global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __restrict__ reps, Ls2dState* st,
+                                                             const int* __restrict__ row_map,
+                                                             const int* __restrict__ row_local, double* partials,
+                                                             unsigned int* rep_counter, Ls2dCtl* ctl,
+                                                             cudaGraphConditionalHandle cond, int use_cond,
+                                                             int guard_cap, int nitems, int stage_bytes) {
+  using C = C_t<TC>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  __shared__ int s_last;
+  __shared__ __align__(8) uint64_t bars[2];
+  C* bufA = reinterpret_cast<C*>(smem_raw + 2 * (size_t)stage_bytes);
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
   }
-  a = block_sum(a, red);
-  b = block_sum(b, red);
-  if (threadIdx.x != 0) return;
-  if (S.iter == 0) { a += S.extra_d0; b += S.extra_n0; }
-  else { b += 2.0 * (double)N * S.abar * S.abar; }
-  const double diff = sqrt(a) / (sqrt(b) + 1e-20);
-  S.diff = diff;
-  S.iter += 1;
-  S.phase_iter += 1;
-  int keep = 0;
-  if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
-  else if (FINAL) {
-    if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
-    else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
-    else keep = 1;
-  } else {
-    const double tol1 = R.tol > kMixedPhase1Tol ? R.tol : kMixedPhase1Tol;
-    if (S.iter >= R.max_iter) { S.done = 2; S.status = diff < R.tol ? MGK_OK : MGK_NOT_CONVERGED; }
-    else if (diff < tol1 || S.phase_iter >= kMixedPhase1Cap) S.done = 1;
-    else keep = 1;
+  if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap || *(volatile int*)&ctl->error != 0) {
+      ctl->any = 0;
+      cudaGraphSetConditional(cond, 0u);
+    }
   }
-  const unsigned int n_act = ctl->n_active;  // stable until every active replica has decided
-  if (keep) atomicAdd(&ctl->still, 1u);
-  __threadfence();
-  const unsigned int d = atomicAdd(&ctl->decided, 1u);
-  if (d == n_act - 1) {
-    __threadfence();
-    const unsigned int still = atomicExch(&ctl->still, 0u);
-    ctl->decided = 0;
-    ctl->n_active = still;
-    const bool go = still > 0 && atomicAdd(&ctl->bodies, 0u) <= (unsigned int)guard_cap;
-    ctl->any = go ? 1 : 0;
-    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
+  __syncthreads();
+  uint32_t parity[2] = {0u, 0u};
+  // issue the bulk loads of `item` into stage s; returns whether it is active
+  auto issue = [&](int item, int s) -> bool {
+    const int r = row_map[item];
+    if (st[r].done != 0) return false;
+    if (threadIdx.x == 0) {
+      const Ls2dRep& R = reps[r];
+      const int ny = R.ny, ld = R.ld;
+      const long long N = R.N;
+      const long long x0 = 2LL * row_local[item];
+      unsigned char* sb = smem_raw + (size_t)s * stage_bytes;
+      const uint32_t spec_b = 2u * ld * sizeof(C), row_b = 2u * ny * sizeof(TS);
+      // the copy list in stage order; the barrier expects exactly its bytes
+      const void* src[11];
+      uint32_t len[11];
+      int n = 0;
+      const C* spec = reinterpret_cast<const C*>(R.spec);
+      for (int c = 0; c < 3; ++c) { src[n] = spec + ((long long)c * R.nx + x0) * ld; len[n++] = spec_b; }
+      const TS* eps = Fields<TS>::eps(R);
+      const TS* ep = Fields<TS>::ep(R);
+      for (int c = 0; c < 3; ++c) { src[n] = eps + c * N + x0 * ny; len[n++] = row_b; }
+      src[n] = Fields<TS>::mu(R) + x0 * ny; len[n++] = row_b;
+      src[n] = Fields<TS>::lam(R) + x0 * ny; len[n++] = row_b;
+      for (int c = 0; c < 3; ++c) { src[n] = ep + c * N + x0 * ny; len[n++] = row_b; }
+      uint32_t total = 0;
+      for (int q = 0; q < n; ++q) total += len[q];
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&bars[s], total);
+      unsigned char* dst = sb;
+      for (int q = 0; q < n; ++q) { bulk_g2s(dst, src[q], len[q], &bars[s]); dst += len[q]; }
+    }
+    return true;
+  };
+  int item = blockIdx.x;
+  bool act = item < nitems ? issue(item, 0) : false;
+  for (int k = 0; item < nitems; item += gridDim.x, ++k) {
+    const int s = k & 1;
+    const int next = item + gridDim.x;
+    const bool act_next = next < nitems ? issue(next, s ^ 1) : false;
+    if (act) {
+      const bool ok = __syncthreads_and(mbar_wait(&bars[s], parity[s]) ? 1 : 0);
+      parity[s] ^= 1u;
+      if (!ok) {
+        // the copy never completed: record it, wait (bounded) for the other
+        // stage's copy if one is in flight, and leave
+        if (threadIdx.x == 0) { ctl->error = 1; ctl->any = 0; }
+        if (act_next) mbar_wait(&bars[s ^ 1], parity[s ^ 1]);
+        return;
+      }
+      const int r = row_map[item];
+      const Ls2dRep& R = reps[r];
+      Ls2dState& S = st[r];
+      const int ny = R.ny, nyh = R.nyh, ld = R.ld, nx = R.nx;
+      const long long N = R.N;
+      const int x0 = 2 * row_local[item];
+      unsigned char* sb = smem_raw + (size_t)s * stage_bytes;
+      const uint32_t spec_b = 2u * ld * sizeof(C), row_b = 2u * ny * sizeof(TS);
+      const C* sspec = reinterpret_cast<const C*>(sb);
+      const TS* seps = reinterpret_cast<const TS*>(sb + 3 * spec_b);
+      const TS* smu = reinterpret_cast<const TS*>(sb + 3 * spec_b + 3 * row_b);
+      const TS* slam = smu + 2 * ny;
+      const TS* sep = slam + 2 * ny;
+      const FftLen& fy = Fields<TS>::fy(R);
+      for (int e = threadIdx.x; e < 3 * ny; e += blockDim.x) {
+        const int c = e / ny, k2 = e - c * ny;
+        const int ks = (2 * k2 <= ny) ? k2 : ny - k2;
+        C a = sspec[c * 2 * ld + ks], b = sspec[c * 2 * ld + ld + ks];
+        C z;
+        if (2 * k2 <= ny) {
+          if (k2 == 0 || 2 * k2 == ny) { a.y = 0; b.y = 0; }
+          z = mk<C>(a.x - b.y, a.y + b.x);
+        } else {
+          z = mk<C>(a.x + b.y, b.x - a.y);
+        }
+        bufA[e] = z;
+      }
+      __syncthreads();
+      C* bufB = reinterpret_cast<C*>(sb);  // the spectrum rows are consumed
+      C* cur = fft_any<+1>(bufA, bufB, 3, ny, fy);
+      C* out = (cur == bufA) ? bufB : bufA;
+      const double mu0 = S.mu0, lam0 = S.lam0;
+      const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
+      TS* eps = Fields<TS>::eps(R);
+      double d2 = 0, n2 = 0;
+      for (int y = threadIdx.x; y < ny; y += blockDim.x) {
+        TC tr[2][3];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = h * ny + y;
+          const long long i = (long long)(x0 + h) * ny + y;
+          const double o0 = (double)seps[j], o1 = (double)seps[2 * ny + j], o2 = (double)seps[4 * ny + j];
+          const double m = (double)smu[j], l = (double)slam[j];
+          const double p0 = (double)sep[j], p1 = (double)sep[2 * ny + j], p2 = (double)sep[4 * ny + j];
+          const C z0 = cur[y], z1 = cur[ny + y], z2 = cur[2 * ny + y];
+          const double e0 = eb0 + (double)(h == 0 ? z0.x : z0.y);
+          const double e1 = eb1 + (double)(h == 0 ? z1.x : z1.y);
+          const double e2 = eb2 + (double)(h == 0 ? z2.x : z2.y);
+          const double q0 = e0 - o0, q1 = e1 - o1, q2 = e2 - o2;
+          d2 += q0 * q0 + q1 * q1 + 2.0 * q2 * q2;
+          n2 += o0 * o0 + o1 * o1 + 2.0 * o2 * o2;
+          eps[i] = (TS)e0;
+          eps[N + i] = (TS)e1;
+          eps[2 * N + i] = (TS)e2;
+          const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
+          const double trd = dxx + dyy, tre = e0 + e1;
+          tr[h][0] = (TC)((2 * m * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
+          tr[h][1] = (TC)((2 * m * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
+          tr[h][2] = (TC)(2 * m * dxy - 2 * mu0 * e2);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
+      }
+      __syncthreads();
+      C* scratch = (out == bufA) ? bufB : bufA;
+      C* Z = fft_any<-1>(out, scratch, 3, ny, fy);
+      C* spec = reinterpret_cast<C*>(R.spec);
+      for (int e = threadIdx.x; e < 3 * nyh; e += blockDim.x) {
+        const int c = e / nyh, k2 = e - c * nyh;
+        const C z = Z[c * ny + k2];
+        const C w = Z[c * ny + (k2 == 0 ? 0 : ny - k2)];
+        C* ra = spec + ((size_t)c * nx + x0) * ld;
+        ra[k2] = mk<C>(TC(0.5) * (z.x + w.x), TC(0.5) * (z.y - w.y));
+        ra[ld + k2] = mk<C>(TC(0.5) * (z.y + w.y), TC(-0.5) * (z.x - w.x));
+      }
+      d2 = block_sum(d2, red);
+      n2 = block_sum(n2, red);
+      if (threadIdx.x == 0) {
+        partials[2 * item] = d2;
+        partials[2 * item + 1] = n2;
+        __threadfence();
+        const unsigned int t = atomicInc(&rep_counter[r], (unsigned int)R.row_items - 1);
+        s_last = (t == (unsigned int)R.row_items - 1);
+      }
+      __syncthreads();
+      if (s_last) {
+        __threadfence();
+        ls2d_decide<FINAL>(R, S, partials, ctl, cond, use_cond, guard_cap, red);
+      }
+    }
+    __syncthreads();  // this stage is free for the prefetch two items ahead
+    act = act_next;
   }
 }
 
@@ -542,7 +730,7 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
   }
   __syncthreads();
   // lines (c * tc + t); only t < tcw are meaningful, all 3*tc are transformed
-  C* F = fft_lines<-1>(bufA, bufB, 3 * tc, nx, fx);
+  C* F = fft_any<-1>(bufA, bufB, 3 * tc, nx, fx);
   const TC inv2mu0 = (TC)S.inv2mu0, Bc = (TC)S.Bc;
   const TC sc = (TC)(1.0 / ((double)nx * (double)ny));
   for (int e = threadIdx.x; e < tcw * nx; e += blockDim.x) {
@@ -576,7 +764,7 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
   }
   __syncthreads();
   C* G = (F == bufA) ? bufB : bufA;
-  C* Rz = fft_lines<+1>(F, G, 3 * tc, nx, fx);
+  C* Rz = fft_any<+1>(F, G, 3 * tc, nx, fx);
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * nx);
     const int rem = e - c * tcw * nx;
@@ -706,6 +894,12 @@ struct mgk_ls2d_plan {
   int graph_cap = 0;
   // selection of the last call
   int nsel = 0, sel_rows = 0, sel_cols = 0;
+  // persistent bulk-prefetch row kernels (0 when a replica has odd ny or the
+  // stages do not fit): stage bytes, dynamic smem and resident CTAs per SM
+  int tma = 0;
+  int stage64 = 0, stage32 = 0;
+  size_t tma_smem64 = 0, tma_smem32 = 0;
+  int occ64 = 0, occ32 = 0, num_sms = 0;
 };
 
 static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
@@ -821,6 +1015,43 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
   int st = ls2d_set_attrs<double, double>(row_smem, col_smem);
   if (st == MGK_OK && mixed) st = ls2d_set_attrs<float, float>(row_smem / 2, col_smem / 2);
   if (st) return fail(st);
+  {
+    // persistent bulk-prefetch row kernels: every replica needs ny even
+    bool ok = true;
+    int st64 = 0, st32 = 0, maxny = 0;
+    for (const Ls2dRep& R : p->reps) {
+      ok = ok && (R.ny % 2 == 0);
+      st64 = std::max(st64, (int)(6 * R.ld * sizeof(double2) + 16 * R.ny * sizeof(double)));
+      st32 = std::max(st32, (int)(6 * R.ld * sizeof(float2) + 16 * R.ny * sizeof(float)));
+      maxny = std::max(maxny, R.ny);
+    }
+    st64 = (st64 + 127) / 128 * 128;
+    st32 = (st32 + 127) / 128 * 128;
+    const size_t sm64 = 2 * (size_t)st64 + 3 * (size_t)maxny * sizeof(double2);
+    const size_t sm32 = 2 * (size_t)st32 + 3 * (size_t)maxny * sizeof(float2);
+    // opt-in: at 256-point lines the per-CTA FFT work, not load latency,
+    // bounds the row kernel, and the prefetching variant needs one CTA per SM
+    const char* env = getenv("MGK_TMA");
+    ok = ok && (env && env[0] == '1') && sm64 <= 220 * 1024;
+    int dev = 0;
+    if (ok && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
+      p->stage64 = st64; p->stage32 = st32; p->tma_smem64 = sm64; p->tma_smem32 = sm32;
+      bool good = cudaFuncSetAttribute(ls2d_row_tma_kernel<double, double, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64) == cudaSuccess &&
+                  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->occ64, ls2d_row_tma_kernel<double, double, true>,
+                                                                kThreads, sm64) == cudaSuccess;
+      if (good && mixed)
+        good = cudaFuncSetAttribute(ls2d_row_tma_kernel<float, float, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32) == cudaSuccess &&
+               cudaFuncSetAttribute(ls2d_row_tma_kernel<float, float, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32) == cudaSuccess &&
+               cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->occ32, ls2d_row_tma_kernel<float, float, false>,
+                                                             kThreads, sm32) == cudaSuccess;
+      p->tma = good && p->occ64 > 0 && (!mixed || p->occ32 > 0);
+    }
+    cudaGetLastError();
+  }
   const int G = grid_blocks(p->maxN);
   p->part_doubles = std::max((size_t)2 * p->total_row_items, (size_t)nrep * G * 8);
   void* v = nullptr;
@@ -931,14 +1162,22 @@ struct LoopArgs {
   Ls2dCtl* ctl;
   int rows, cols;
   size_t row_smem, col_smem;
+  int tma;            // use the persistent bulk-prefetch row kernel
+  int row_grid;       // its grid (resident CTAs), <= rows
+  int stage_bytes;
+  size_t tma_smem;
 };
 
 template <typename TS, bool FINAL>
 static int launch_body(const LoopArgs& a, cudaStream_t s) {
   ls2d_col_kernel<TS, TS><<<a.cols, kThreads, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
   MGK_CUDA(cudaGetLastError());
-  ls2d_row_kernel<TS, TS, true, FINAL><<<a.rows, kThreads, a.row_smem, s>>>(
-      a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
+  if (a.tma)
+    ls2d_row_tma_kernel<TS, TS, FINAL><<<a.row_grid, kThreads, a.tma_smem, s>>>(
+        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0, a.rows, a.stage_bytes);
+  else
+    ls2d_row_kernel<TS, TS, true, FINAL><<<a.rows, kThreads, a.row_smem, s>>>(
+        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }
@@ -972,11 +1211,20 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
   cudaKernelNodeParams k2;
   memset(&k2, 0, sizeof(k2));
   void* a2[] = {&a.reps, &a.st, &a.row_map, &a.row_local, &a.part, &a.repctr, &a.ctl, &h, &use_cond, guard_cap};
-  k2.func = (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
-  k2.gridDim = dim3(a.rows);
+  void* a2t[] = {&a.reps, &a.st, &a.row_map, &a.row_local, &a.part, &a.repctr, &a.ctl, &h, &use_cond, guard_cap,
+                 &a.rows, &a.stage_bytes};
+  if (a.tma) {
+    k2.func = (void*)ls2d_row_tma_kernel<TS, TS, FINAL>;
+    k2.gridDim = dim3(a.row_grid);
+    k2.sharedMemBytes = (unsigned)a.tma_smem;
+    k2.kernelParams = a2t;
+  } else {
+    k2.func = (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
+    k2.gridDim = dim3(a.rows);
+    k2.sharedMemBytes = (unsigned)a.row_smem;
+    k2.kernelParams = a2;
+  }
   k2.blockDim = dim3(kThreads);
-  k2.sharedMemBytes = (unsigned)a.row_smem;
-  k2.kernelParams = a2;
   MGK_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2));
   return MGK_OK;
 }
@@ -1095,6 +1343,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   p->h_ctl->still = 0;
   p->h_ctl->bodies = 0;
   p->h_ctl->any = n_active > 0;
+  p->h_ctl->error = 0;
   const size_t nm = 2 * (size_t)rows + 2 * (size_t)cols + nsel;
   MGK_CUDA(cudaMemcpyAsync(p->d_maps, p->h_maps, sizeof(int) * nm, cudaMemcpyHostToDevice, s));
   MGK_CUDA(cudaMemcpyAsync(p->d_reps, p->h_reps, sizeof(Ls2dRep) * p->nrep, cudaMemcpyHostToDevice, s));
@@ -1130,10 +1379,14 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   if (n_active > 0) {
     const bool mixed = p->prec == MGK_MIXED;
     LoopArgs a64{p->d_reps, p->d_st, d_row_map, d_row_local, d_col_map, d_col_local, p->d_part, p->d_repctr,
-                 p->d_ctl, rows, cols, p->row_smem, p->col_smem};
+                 p->d_ctl, rows, cols, p->row_smem, p->col_smem, p->tma, 0, p->stage64, p->tma_smem64};
+    a64.row_grid = std::max(1, std::min(rows, p->occ64 * p->num_sms));
     LoopArgs a32 = a64;
     a32.row_smem = p->row_smem / 2;
     a32.col_smem = p->col_smem / 2;
+    a32.stage_bytes = p->stage32;
+    a32.tma_smem = p->tma_smem32;
+    a32.row_grid = std::max(1, std::min(rows, p->occ32 * p->num_sms));
     if (mixed)
       ls2d_row_kernel<float, float, false, false><<<rows, kThreads, a32.row_smem, s>>>(
           p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
@@ -1181,7 +1434,13 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   MGK_CUDA(cudaGetLastError());
   if (infos) {
     MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls2dState) * p->nrep, cudaMemcpyDeviceToHost, s));
+    Ls2dCtl hc;
+    MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls2dCtl), cudaMemcpyDeviceToHost, s));
     MGK_CUDA(cudaStreamSynchronize(s));
+    if (hc.error) {
+      set_error("mgk_ls2d_solve: a bulk copy wait gave up (device timeout)");
+      return MGK_TIMEOUT;
+    }
     int worst = MGK_OK;
     for (int q = 0; q < nsel; ++q) {
       const Ls2dState& S = p->h_state[selv[q]];
@@ -1228,8 +1487,16 @@ static int profile_t(mgk_ls2d_t p, float* row_ms, float* col_ms, int reps, cudaS
     cudaEventRecord(ev[0], s);
     ls2d_col_kernel<TS, TS><<<cols, kThreads, cs, s>>>(p->d_reps, p->d_st, d_col_map, d_col_local);
     cudaEventRecord(ev[1], s);
-    ls2d_row_kernel<TS, TS, true, true><<<rows, kThreads, rs, s>>>(p->d_reps, p->d_st, d_row_map, d_row_local,
-                                                                   p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+    if (p->tma) {
+      const bool f64 = sizeof(TS) == 8;
+      const int grid = std::max(1, std::min(rows, (f64 ? p->occ64 : p->occ32) * p->num_sms));
+      ls2d_row_tma_kernel<TS, TS, true><<<grid, kThreads, f64 ? p->tma_smem64 : p->tma_smem32, s>>>(
+          p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0, rows,
+          f64 ? p->stage64 : p->stage32);
+    } else {
+      ls2d_row_kernel<TS, TS, true, true><<<rows, kThreads, rs, s>>>(p->d_reps, p->d_st, d_row_map, d_row_local,
+                                                                     p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+    }
     cudaEventRecord(ev[2], s);
     if (cudaEventSynchronize(ev[2]) != cudaSuccess) { rc = MGK_CUDA_ERROR; break; }
     float a = 0, b = 0;

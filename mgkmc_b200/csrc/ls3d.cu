@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
       bufA[e] = z;
     }
     __syncthreads();
-    cur = fft_lines<+1>(bufA, bufB, 6, nz, R.fz);
+    cur = fft_any<+1>(bufA, bufB, 6, nz, R.fz);
   }
   C* out = (IN_SPEC && cur == bufA) ? bufB : bufA;
   const double mu0 = S.mu0, lam0 = S.lam0;
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
   }
   __syncthreads();
   C* scratch = (out == bufA) ? bufB : bufA;
-  C* Z = fft_lines<-1>(out, scratch, 6, nz, R.fz);
+  C* Z = fft_any<-1>(out, scratch, 6, nz, R.fz);
   for (int e = threadIdx.x; e < 6 * nzh; e += blockDim.x) {
     const int c = e / nzh, k = e - c * nzh;
     const C z = Z[c * nz + k];
@@ -445,9 +445,9 @@ __global__ void __launch_bounds__(256) ls3d_axis_kernel(const Ls3dRep* __restric
   __syncthreads();
   C* F;
   if (AXIS == 1) {
-    F = fft_lines<SIGN>(bufA, bufB, 6 * tc, n, f);
+    F = fft_any<SIGN>(bufA, bufB, 6 * tc, n, f);
   } else {
-    C* G = fft_lines<-1>(bufA, bufB, 6 * tc, n, f);
+    C* G = fft_any<-1>(bufA, bufB, 6 * tc, n, f);
     const double scale = 1.0 / (double)R.N;
     const int ky = o;
     const double uy = (double)fftfreq3(ky, ny) / ny;
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(256) ls3d_axis_kernel(const Ls3dRep* __restric
     }
     __syncthreads();
     C* H = (G == bufA) ? bufB : bufA;
-    F = fft_lines<+1>(G, H, 6 * tc, n, f);
+    F = fft_any<+1>(G, H, 6 * tc, n, f);
   }
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * n), rem = e - c * tcw * n, j = rem / tcw, t = rem - j * tcw;
