@@ -167,6 +167,13 @@ MGK_API int mgk_ls3d_solve_batch(mgk_ls3d_t plan, int nsel, const int* sel, cons
                                  double* const* sig_out, int max_iter, double tol, mgk_ls_info3* infos,
                                  mgk_stream_t stream);
 
+/* After a KMC flip changed voxel (x, y) = d_xy[0..1] (device int64, e.g.
+ * from mgk_kmc2d_event) of the caller's eigenstrain field, copy that voxel
+ * into replica `rep`'s planes instead of re-reading the whole field.  The
+ * replica's material must have been set with an eigenstrain field. */
+MGK_API int mgk_ls2d_sync_voxel(mgk_ls2d_t plan, int rep, const double* eps_plastic, const int64_t* d_xy,
+                                mgk_stream_t stream);
+
 /* ------------------------------------------------------ 2D STZ / KMC --- */
 /* mgkmc/kmc_simulator_functions.py:100-160 compute_barrier_2d (in place on Q).
  * scheme: 0 isotropic, 1 directional.  tau: +inf for no decay. */
@@ -202,6 +209,34 @@ MGK_API int mgk_kmc_prefix(const double* rates, int64_t n, double* prefix, int64
  * same rates and draw.  Result in *d_index (device int64). */
 MGK_API int mgk_kmc_select(const double* prefix, const int64_t* d_count, const double* d_total, double u,
                    int64_t* d_index, mgk_stream_t stream);
+
+/* KMC-mode rates only (every mode an event; no running sum), for the fast
+ * selection mode below.  Same per-mode arithmetic as mgk_kmc2d_rates. */
+MGK_API int mgk_kmc2d_rates_only(int nx, int ny, int M, const double* Q, double volume,
+                                 const double* temperature, double temperature_scalar, double nu0,
+                                 double* rates, mgk_stream_t stream);
+
+/* Fast selection mode: parallel inclusive FP64 scan of n rates into prefix
+ * (total in *d_total, n in *d_count).  Its running sums differ from the
+ * reference's sequential chain by rounding, so the selected index can differ
+ * from the reference's only when u*total falls within that rounding of a
+ * running sum.  work: mgk_kmc_scan_work_bytes(n) bytes. */
+MGK_API int64_t mgk_kmc_scan_work_bytes(int64_t n);
+MGK_API int mgk_kmc_prefix_fast(const double* rates, int64_t n, double* prefix, int64_t* d_count,
+                                double* d_total, void* work, mgk_stream_t stream);
+
+/* One KMC event on the device: mgkmc/kmc_simulator.py:899-900 (index ->
+ * x, y, m via indices[*d_sel], decode_index_2d), :1025 apply_flip_soa_2d,
+ * :1030 prev_strain_dir[x,y] = catalog[x,y,m], and :1035-1042 the redraw of
+ * the voxel's catalog (new_catalog, M x 2 x 2) and barriers (new_q0, M),
+ * both drawn by the host (NULL: keep).  indices NULL means identity (KMC
+ * mode).  Writes (x, y, m) to d_xym (device int64[3], may be NULL); a
+ * negative *d_sel (no event) leaves everything unchanged. */
+MGK_API int mgk_kmc2d_event(int nx, int ny, int M, const int64_t* d_sel, const int64_t* indices,
+                            double* eps_plastic, double* soft_prop, double* last_event_time, double* catalog,
+                            double* Q0, double* prev_strain_dir, const double* new_catalog, const double* new_q0,
+                            double current_time, double jp, double jt, double g_max, double jn_frac,
+                            int64_t* d_xym, mgk_stream_t stream);
 
 /* mgkmc/kmc_simulator_functions.py:183-218 apply_flip_soa_2d (in place). */
 MGK_API int mgk_kmc2d_flip(int nx, int ny, int M, double* eps_plastic, double* soft_prop,

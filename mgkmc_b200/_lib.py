@@ -75,6 +75,12 @@ _SIGS = {
     "mgk_kmc_select": (c_int, [_P, _P, _P, c_double, _P, _P]),
     "mgk_kmc2d_flip": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_int, c_int, c_int, c_double, c_double,
                                c_double, c_double, c_double, _P]),
+    "mgk_ls2d_sync_voxel": (c_int, [_P, c_int, _P, _P, _P]),
+    "mgk_kmc_scan_work_bytes": (c_int64, [c_int64]),
+    "mgk_kmc2d_rates_only": (c_int, [c_int, c_int, c_int, _P, c_double, _P, c_double, c_double, _P, _P]),
+    "mgk_kmc_prefix_fast": (c_int, [_P, c_int64, _P, _P, _P, _P, _P]),
+    "mgk_kmc2d_event": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_double, c_double,
+                                c_double, c_double, c_double, _P, _P]),
     "mgk_kmc3d_barrier": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
                                   c_double, c_int, c_double, _P]),
     "mgk_kmc3d_rates": (c_int, [c_int, c_int, c_int, c_int, _P, c_double, _P, c_double, c_double, c_int, _P, _P,

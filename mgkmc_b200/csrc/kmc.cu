@@ -97,7 +97,7 @@ __global__ void rates_full_kernel(long long nvox, int M, const double* __restric
                                   const double* __restrict__ T, double Ts, double* __restrict__ rates,
                                   long long* __restrict__ indices, long long* __restrict__ d_count) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i == 0) *d_count = nvox * M;
+  if (i == 0 && d_count) *d_count = nvox * M;
   if (i >= nvox * M) return;
   const long long v = i / M;
   const double beta = beta_of(T ? T[v] : Ts);
@@ -314,6 +314,104 @@ __global__ void flip3d_kernel(int nx, int ny, int nz, int M, double* ep, double*
   }
 }
 
+// One KMC event on the device (kmc_simulator.py:899-900, :1025-1042): decode
+// the selected mode, apply the flip bookkeeping of apply_flip_soa_2d, record
+// the mode as prev_strain_dir of the voxel, and redraw the voxel's catalog and
+// barriers from values the host drew.  d_sel holds the position in the rates
+// array; `indices` maps it to the mode index (NULL: identity, KMC mode).
+__global__ void event2d_kernel(int nx, int ny, int M, const long long* d_sel, const long long* indices,
+                               double* ep, double* soft, double* tl, double* cat, double* Q0, double* prev,
+                               const double* new_cat, const double* new_q0, double t, double jp, double jt,
+                               double gmax, double jn, long long* d_xym) {
+  const long long k = *d_sel;
+  if (k < 0) {
+    if (d_xym) { d_xym[0] = -1; d_xym[1] = -1; d_xym[2] = -1; }
+    return;
+  }
+  const long long idx = indices ? indices[k] : k;
+  const int m = (int)(idx % M);
+  const long long tmp = idx / M;
+  const int y = (int)(tmp % ny);
+  const int x = (int)(tmp / ny);
+  const long long v = tmp;
+  double C[4];
+  for (int q = 0; q < 4; ++q) C[q] = cat[(v * M + m) * 4 + q];
+  for (int q = 0; q < 4; ++q) ep[4 * v + q] = add(ep[4 * v + q], C[q]);
+  const double e11 = C[0], e22 = C[3], e12 = C[1];
+  const double d = sub(e11, e22);
+  const double s = add(mul(e12, e12), __ddiv_rn(add(add(mul(e22, e22), mul(e11, e11)), mul(d, d)), 6.0));
+  double gp = add(soft[2 * v], mul(jp, s));
+  if (gmax > 0 && gp > gmax) gp = gmax;
+  soft[2 * v] = gp;
+  soft[2 * v + 1] = mul(jt, s);
+  tl[v] = t;
+  if (jn > 0.0) {
+    for (int dx = -1; dx <= 1; ++dx)
+      for (int dy = -1; dy <= 1; ++dy) {
+        if (dx == 0 && dy == 0) continue;
+        const long long w = (long long)((x + dx + nx) % nx) * ny + (y + dy + ny) % ny;
+        double g = add(soft[2 * w], mul(mul(jn, jp), s));
+        if (gmax > 0 && g > gmax) g = gmax;
+        soft[2 * w] = g;
+        soft[2 * w + 1] = add(soft[2 * w + 1], mul(mul(jn, jt), s));
+      }
+  }
+  for (int q = 0; q < 4; ++q) prev[4 * v + q] = C[q];
+  if (new_cat)
+    for (int q = 0; q < 4 * M; ++q) cat[v * M * 4 + q] = new_cat[q];
+  if (new_q0)
+    for (int q = 0; q < M; ++q) Q0[v * M + q] = new_q0[q];
+  if (d_xym) { d_xym[0] = x; d_xym[1] = y; d_xym[2] = m; }
+}
+
+// Parallel inclusive FP64 scan (fast selection mode): per-block scans of
+// 1024 rates, an exclusive scan of the block totals, and the offsets.  The
+// running sums differ from the sequential chain by rounding only.
+__global__ void scan_block_kernel(const double* __restrict__ r, long long n, double* __restrict__ prefix,
+                                  double* __restrict__ bsum) {
+  __shared__ double ws[32];
+  const long long base = (long long)blockIdx.x * 1024;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double v[4];
+  double acc = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long i = base + threadIdx.x * 4 + q;
+    acc += (i < n) ? r[i] : 0.0;
+    v[q] = acc;
+  }
+  double x = acc;
+  for (int o = 1; o < 32; o <<= 1) { double y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+  if (lane == 31) ws[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    double w = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0.0;
+    for (int o = 1; o < 32; o <<= 1) { double y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+    ws[lane] = w;
+  }
+  __syncthreads();
+  const double off = (x - acc) + (wid > 0 ? ws[wid - 1] : 0.0);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long i = base + threadIdx.x * 4 + q;
+    if (i < n) prefix[i] = off + v[q];
+  }
+  if (threadIdx.x == blockDim.x - 1) bsum[blockIdx.x] = off + acc;
+}
+
+__global__ void scan_bsum_kernel(double* bsum, int nb, long long n, double* d_total) {
+  // single-thread exclusive scan of the (few hundred) block totals
+  if (threadIdx.x != 0) return;
+  double run = 0.0;
+  for (int b = 0; b < nb; ++b) { const double t = bsum[b]; bsum[b] = run; run += t; }
+  *d_total = n > 0 ? run : 0.0;
+}
+
+__global__ void scan_add_kernel(double* prefix, long long n, const double* bsum) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) prefix[i] += bsum[i / 1024];
+}
+
 }  // namespace mgk
 
 using namespace mgk;
@@ -446,6 +544,52 @@ extern "C" int mgk_kmc3d_flip(int nx, int ny, int nz, int M, double* eps_plastic
   MGK_REQUIRE(eps_plastic && soft_prop && last_event_time && catalog, "mgk_kmc3d_flip: null argument");
   flip3d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, nz, M, eps_plastic, soft_prop, last_event_time, catalog,
                                                    x, y, z, m, current_time, jp, jt, g_max, jn_frac);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_event(int nx, int ny, int M, const int64_t* d_sel, const int64_t* indices,
+                               double* eps_plastic, double* soft_prop, double* last_event_time, double* catalog,
+                               double* Q0, double* prev_strain_dir, const double* new_catalog,
+                               const double* new_q0, double current_time, double jp, double jt, double g_max,
+                               double jn_frac, int64_t* d_xym, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && M > 0 && d_sel && eps_plastic && soft_prop && last_event_time && catalog && Q0 &&
+                  prev_strain_dir,
+              "mgk_kmc2d_event: bad argument");
+  event2d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, M, (const long long*)d_sel, (const long long*)indices,
+                                                    eps_plastic, soft_prop, last_event_time, catalog, Q0,
+                                                    prev_strain_dir, new_catalog, new_q0, current_time, jp, jt, g_max,
+                                                    jn_frac, (long long*)d_xym);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int64_t mgk_kmc_scan_work_bytes(int64_t n) { return (int64_t)sizeof(double) * ((n + 1023) / 1024 + 1); }
+
+extern "C" int mgk_kmc_prefix_fast(const double* rates, int64_t n, double* prefix, int64_t* d_count, double* d_total,
+                                   void* work, mgk_stream_t stream) {
+  MGK_REQUIRE(n >= 0 && (n == 0 || (rates && prefix)) && d_count && d_total && work, "mgk_kmc_prefix_fast: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = (int)((n + 1023) / 1024);
+  double* bsum = reinterpret_cast<double*>(work);
+  set_count_kernel<<<1, 1, 0, s>>>((long long*)d_count, (long long)n);
+  if (nb > 0) {
+    scan_block_kernel<<<nb, 256, 0, s>>>(rates, n, prefix, bsum);
+    scan_bsum_kernel<<<1, 32, 0, s>>>(bsum, nb, n, d_total);
+    scan_add_kernel<<<(int)((n + 255) / 256), 256, 0, s>>>(prefix, n, bsum);
+  } else {
+    scan_bsum_kernel<<<1, 32, 0, s>>>(bsum, 0, 0, d_total);
+  }
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_rates_only(int nx, int ny, int M, const double* Q, double volume, const double* temperature,
+                                    double temperature_scalar, double nu0, double* rates, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && M > 0 && Q && rates, "mgk_kmc2d_rates_only: bad argument");
+  const long long nvox = (long long)nx * ny, n = nvox * M;
+  rates_full_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(nvox, M, Q, volume * nu0, temperature,
+                                                                          temperature_scalar, rates, nullptr, nullptr);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

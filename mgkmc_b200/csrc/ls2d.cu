@@ -1552,6 +1552,37 @@ extern "C" int mgk_ls2d_profile(mgk_ls2d_t p, const double* eps_bar, int reps, f
   return mgk_ls2d_profile_batch(p, 1, &r0, eps_bar, 0, reps, row_ms, col_ms, stream);
 }
 
+// ------------------------------------------------- one-voxel eigenstrain ---
+
+namespace mgk {
+// Copy voxel (x, y) = d_xy[0..1] of the caller's eigenstrain field (after a
+// flip) into the plan's planes; a negative x means no event happened.
+__global__ void ls2d_sync_voxel_kernel(const Ls2dRep* reps, int rep, const double* __restrict__ epsp,
+                                       const long long* __restrict__ d_xy) {
+  const long long x = d_xy[0], y = d_xy[1];
+  const Ls2dRep& R = reps[rep];
+  if (x < 0 || y < 0 || x >= R.nx || y >= R.ny) return;
+  const long long N = R.N, i = x * R.ny + y;
+  const double4 p = reinterpret_cast<const double4*>(epsp)[i];
+  const double psym = (p.y == p.z) ? p.y : 0.5 * (p.y + p.z);
+  R.ep[i] = p.x;
+  R.ep[N + i] = p.w;
+  R.ep[2 * N + i] = psym;
+  if (R.ep32) { R.ep32[i] = (float)p.x; R.ep32[N + i] = (float)p.w; R.ep32[2 * N + i] = (float)psym; }
+  if (R.epa) { R.epa[i] = p.y; R.epa[N + i] = p.z; }
+}
+}  // namespace mgk
+
+extern "C" int mgk_ls2d_sync_voxel(mgk_ls2d_t p, int rep, const double* eps_plastic, const int64_t* d_xy,
+                                   mgk_stream_t stream) {
+  MGK_REQUIRE(p && eps_plastic && d_xy && rep >= 0 && rep < p->nrep && p->has_material[rep],
+              "mgk_ls2d_sync_voxel: bad argument");
+  MGK_REQUIRE(p->reps[rep].epa != nullptr, "mgk_ls2d_sync_voxel: set the material with an eigenstrain field first");
+  ls2d_sync_voxel_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(p->d_reps, rep, eps_plastic, (const long long*)d_xy);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
 // ============================================================ no-alloc ===
 // Allocation-free 2D LS solve.  Some callers cannot call cudaMalloc: a host
 // application or framework whose caching allocator already reserves the

@@ -1,0 +1,210 @@
+"""Device-resident 2D KMC/AQS driver.
+
+Runs the trajectory of KmcSimulation2D.run_simulation
+(mgkmc/kmc_simulator.py:796-1157) on the path the KMC benchmark exercises
+(small-strain linear elasticity, KMC mode, no cascade, no thermal
+conduction, no fast patching, redraw of directions and barriers) with every
+field resident on the GPU: barriers, rates, the running rate sum, selection,
+the flip bookkeeping and the LS re-solve never leave the device.  The host
+keeps the clock, the macro strain and the random draws (one small
+device-to-host read of the total rate per attempt, and of the mean stress
+per solve).
+
+Draw order (matches oracle/kmc_driver.py): per attempt u_wait; per event
+u_sel, then M orientations theta ~ U[0, pi) and M barriers N(q_mean, q_std)
+clipped below at q_min.
+
+Selection modes: ``exact`` reproduces the reference's sequential FP64 rate
+sum bit for bit (one dependent chain); ``fast`` uses a parallel scan whose
+running sums differ by rounding.  LS forms: ``cold`` re-solves from eps_bar
+as the reference does (kmc_simulator.py:517 passes no warm start); ``warm``
+starts from the previous field.
+"""
+import numpy as np
+
+from . import _lib as L
+from .linear_elastic_simulator import Ls2dBatch
+
+KB = 8.617e-5
+
+
+def pure_shear_modes(theta, gamma0):
+    c, s = np.cos(2 * theta), np.sin(2 * theta)
+    cat = np.empty(theta.shape + (2, 2))
+    cat[..., 0, 0] = 0.5 * gamma0 * c
+    cat[..., 1, 1] = -0.5 * gamma0 * c
+    cat[..., 0, 1] = 0.5 * gamma0 * s
+    cat[..., 1, 0] = 0.5 * gamma0 * s
+    return cat
+
+
+class Kmc2D:
+    def __init__(self, E, nu, catalog, Q0, gamma0=0.1, T=300.0, nu0=1e13, strain_rate=1e7, step_size=1e-5,
+                 q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0, stress_targets=None, mixed_tol=1e4,
+                 mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200, q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0,
+                 selection="exact", ls_start="cold", precision="fp64"):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("mgkmc_b200 needs a CUDA device (no CPU fallback)")
+        self.torch = torch
+        d = self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.nx, self.ny, self.M = Q0.shape
+        nx, ny, M = self.nx, self.ny, self.M
+        self.p = dict(gamma0=gamma0, T=T, nu0=nu0, strain_rate=strain_rate, step_size=step_size, jp=jp, jt=jt,
+                      cap=cap, jn=jn, mixed_tol=mixed_tol, mixed_max_iter=mixed_max_iter, ls_tol=ls_tol,
+                      ls_max_iter=ls_max_iter, q_mean=q_mean, q_std=q_std, q_min=q_min, volume=volume)
+        self.stress_targets = {(1, 1): 0.0} if stress_targets is None else dict(stress_targets)
+        self.selection = selection
+        self.ls_start = ls_start
+        self.tau = 1.0 / (nu0 * np.exp(-q_act_temp / (KB * T))) if T > 0 else np.inf
+        f64 = torch.float64
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(d)
+        self.E, self.nu = t(E), t(nu)
+        self.E_avg, self.nu_avg = float(np.mean(E)), float(np.mean(nu))
+        self.catalog, self.Q0 = t(catalog), t(Q0)
+        self.eps_p = torch.zeros((nx, ny, 2, 2), dtype=f64, device=d)
+        self.soft = torch.zeros((nx, ny, 2), dtype=f64, device=d)
+        self.t_last = torch.full((nx, ny), -np.inf, dtype=f64, device=d)
+        self.prev = torch.zeros((nx, ny, 2, 2), dtype=f64, device=d)
+        self.Q = torch.zeros((nx, ny, M), dtype=f64, device=d)
+        self.eps = torch.zeros((nx, ny, 2, 2), dtype=f64, device=d)
+        self.sig = torch.zeros_like(self.eps)
+        self.eps_prev = torch.zeros_like(self.eps)
+        n = nx * ny * M
+        self.rates = torch.empty(n, dtype=f64, device=d)
+        self.indices = torch.empty(n, dtype=torch.int64, device=d)
+        self.prefix = torch.empty(n, dtype=f64, device=d)
+        self.count = torch.zeros(1, dtype=torch.int64, device=d)
+        self.total = torch.zeros(1, dtype=f64, device=d)
+        self.total_h = torch.zeros(1, dtype=f64).pin_memory()
+        self.sel = torch.zeros(1, dtype=torch.int64, device=d)
+        self.xym = torch.zeros(3, dtype=torch.int64, device=d)
+        self.xym_h = torch.zeros(3, dtype=torch.int64).pin_memory()
+        self.redraw_h = torch.zeros(5 * M, dtype=f64).pin_memory()
+        self.redraw = torch.zeros(5 * M, dtype=f64, device=d)
+        self.work = torch.empty(max(int(L.lib().mgk_kmc_rates_work_bytes(n)), int(L.lib().mgk_kmc_scan_work_bytes(n))),
+                                dtype=torch.uint8, device=d)
+        self.ls = Ls2dBatch([(nx, ny)], precision=precision)
+        self.ls.set_material(0, self.E, self.nu, self.eps_p)
+        self.eps_macro = np.zeros((2, 2))
+        self.time = 0.0
+        self.events = []
+        self.n_solves = 0
+        self.stream = torch.cuda.current_stream()
+
+    # ------------------------------------------------------------ stages ---
+    def elastic_run(self):
+        """LS solve with the current eigenstrain; returns the mean stress."""
+        init = None
+        if self.ls_start == "warm" and self.n_solves > 0:
+            self.eps_prev.copy_(self.eps)
+            init = [self.eps_prev]
+        info = self.ls.solve([0], [self.eps_macro], [self.eps], [self.sig], eps_init=init,
+                             max_iter=self.p["ls_max_iter"], tol=self.p["ls_tol"])[0]
+        self.n_solves += 1
+        sigM = np.array(info.sig_mean).reshape(2, 2)
+        if not np.all(np.isfinite(sigM)) or np.max(np.abs(sigM)) / 1e9 > 20.0:
+            raise ValueError(f"Unstable stress in small-strain elastic_run: {sigM / 1e9} GPa")
+        return sigM
+
+    def barriers_and_rates(self):
+        lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
+        L.check(lib.mgk_kmc2d_barrier(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0), L.ptr(self.sig),
+                                      L.ptr(self.catalog), p["volume"], L.ptr(self.soft), L.ptr(self.t_last),
+                                      self.time, L.ptr(self.prev), p["cap"], 0, self.tau, S), "mgk_kmc2d_barrier")
+        if self.selection == "exact":
+            L.check(lib.mgk_kmc2d_rates(self.nx, self.ny, self.M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"], 0,
+                                        L.ptr(self.rates), L.ptr(self.indices), L.ptr(self.prefix), L.ptr(self.count),
+                                        L.ptr(self.total), L.ptr(self.work), S), "mgk_kmc2d_rates")
+        else:
+            # rates without the sequential chain, then the parallel scan
+            L.check(lib.mgk_kmc2d_rates_only(self.nx, self.ny, self.M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"],
+                                             L.ptr(self.rates), S), "mgk_kmc2d_rates_only")
+            n = self.nx * self.ny * self.M
+            L.check(lib.mgk_kmc_prefix_fast(L.ptr(self.rates), n, L.ptr(self.prefix), L.ptr(self.count),
+                                            L.ptr(self.total), L.ptr(self.work), S), "mgk_kmc_prefix_fast")
+        self.total_h.copy_(self.total, non_blocking=True)
+        self.stream.synchronize()
+        return float(self.total_h[0])
+
+    def event(self, u_sel, theta, q0):
+        lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
+        M = self.M
+        self.redraw_h[:4 * M] = self.torch.from_numpy(pure_shear_modes(theta, p["gamma0"]).reshape(-1))
+        self.redraw_h[4 * M:] = self.torch.from_numpy(q0)
+        self.redraw.copy_(self.redraw_h, non_blocking=True)
+        L.check(lib.mgk_kmc_select(L.ptr(self.prefix), L.ptr(self.count), L.ptr(self.total), float(u_sel),
+                                   L.ptr(self.sel), S), "mgk_kmc_select")
+        nc = L.ptr(self.redraw)
+        nq = L.c_void_p(self.redraw.data_ptr() + 4 * M * 8)
+        L.check(lib.mgk_kmc2d_event(self.nx, self.ny, M, L.ptr(self.sel), None, L.ptr(self.eps_p), L.ptr(self.soft),
+                                    L.ptr(self.t_last), L.ptr(self.catalog), L.ptr(self.Q0), L.ptr(self.prev), nc, nq,
+                                    self.time, p["jp"], p["jt"], p["cap"], p["jn"], L.ptr(self.xym), S),
+                "mgk_kmc2d_event")
+        L.check(lib.mgk_ls2d_sync_voxel(self.ls._h, 0, L.ptr(self.eps_p), L.ptr(self.xym), S), "mgk_ls2d_sync_voxel")
+        self.xym_h.copy_(self.xym, non_blocking=True)
+
+    # ---------------------------------------------------------------- run ---
+    def run(self, rng, n_steps, max_events=None):
+        p = self.p
+        self.elastic_run()
+        strain_unit = np.zeros((2, 2))
+        strain_unit[0, 0] = 1.0
+        dt_step = abs(p["step_size"]) / p["strain_rate"] if p["strain_rate"] > 0 else 1.0
+        remaining = 0.0
+        steps_done = 0
+        M = self.M
+        while steps_done < n_steps:
+            remaining += dt_step
+            while remaining > 0:
+                total = self.barriers_and_rates()
+                if total > 0:
+                    u = rng.random()
+                    t_wait = -np.log(u) / total
+                    if t_wait < remaining:
+                        self.time += t_wait
+                        self.eps_macro += strain_unit * (p["strain_rate"] * t_wait)
+                        remaining -= t_wait
+                        u_sel = rng.random()
+                        theta = rng.uniform(0.0, np.pi, M)
+                        q0 = np.clip(rng.normal(p["q_mean"], p["q_std"], M), p["q_min"], None)
+                        self.event(u_sel, theta, q0)
+                        self.elastic_run()
+                        x, y, m = (int(v) for v in self.xym_h.tolist())
+                        self.events.append((x, y, m, self.time))
+                        if max_events is not None and len(self.events) >= max_events:
+                            return self.result(steps_done)
+                        continue
+                self.eps_macro += strain_unit * (p["strain_rate"] * remaining)
+                self.time += remaining
+                remaining = 0.0
+            prev_e, prev_s = {}, {}
+            for _ in range(p["mixed_max_iter"]):
+                sigM = self.elastic_run()
+                err = np.zeros((2, 2))
+                err_max = 0.0
+                for idx, target in self.stress_targets.items():
+                    e = target - sigM[idx]
+                    err[idx] = e
+                    err_max = max(err_max, abs(e))
+                if err_max < p["mixed_tol"]:
+                    break
+                d_eps = (err - self.nu_avg * np.trace(err) * np.eye(2)) / self.E_avg
+                for idx in self.stress_targets:
+                    step = d_eps[idx]
+                    if idx in prev_e:
+                        d_e = self.eps_macro[idx] - prev_e[idx]
+                        d_s = sigM[idx] - prev_s[idx]
+                        if abs(d_e) > 1e-14 and np.isfinite(d_s):
+                            slope = d_s / d_e
+                            if np.isfinite(slope) and slope > 0.01 * self.E_avg:
+                                step = err[idx] / slope
+                    prev_e[idx] = self.eps_macro[idx]
+                    prev_s[idx] = sigM[idx]
+                    self.eps_macro[idx] += step
+            steps_done += 1
+        return self.result(steps_done)
+
+    def result(self, steps):
+        return dict(events=list(self.events), eps_macro=self.eps_macro.copy(), sig=self.sig.cpu().numpy(),
+                    eps_p=self.eps_p.cpu().numpy(), time=self.time, steps=steps, solves=self.n_solves)

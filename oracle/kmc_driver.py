@@ -1,0 +1,127 @@
+"""numpy restatement of the 2D KMC/AQS trajectory (oracle).
+
+TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
+
+Follows KmcSimulation2D.run_simulation (mgkmc/kmc_simulator.py:796-1157) on
+the path the benchmark exercises: small-strain linear elasticity, KMC mode
+(cascade off), no thermal conduction, no fast patching, redraw of both
+directions and barriers after a flip.  Per event: update_barriers (:874 ->
+compute_barrier_2d), compute_rates_2d (:891), the waiting time (:893), the
+clock/strain advance (:895-898), selection + decode (:899-900), the flip and
+its bookkeeping (:1025-1042), and a cold-started LS re-solve (:1076, which
+passes no warm start).  After each AQS step, the mixed stress-control loop
+(:1106-1143).  The NaN / |sigma| > 20 GPa guard of elastic_run (:522-524)
+raises ValueError.
+
+Draws come from an explicit numpy Generator in a fixed order instead of the
+reference's two global streams (numpy for t_wait and redraws, numba's for
+selection): per attempt u_wait; per event u_sel, then M orientations
+theta ~ U[0, pi) and M barriers N(q_mean, q_std) clipped below at q_min.  The
+GPU driver consumes the same draws in the same order.
+"""
+import numpy as np
+
+from . import kmc as OK
+from . import ls as OL
+
+
+def pure_shear_modes(theta, gamma0):
+    c, s = np.cos(2 * theta), np.sin(2 * theta)
+    cat = np.empty(theta.shape + (2, 2))
+    cat[..., 0, 0] = 0.5 * gamma0 * c
+    cat[..., 1, 1] = -0.5 * gamma0 * c
+    cat[..., 0, 1] = 0.5 * gamma0 * s
+    cat[..., 1, 0] = 0.5 * gamma0 * s
+    return cat
+
+
+def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=300.0, nu0=1e13,
+              strain_rate=1e7, step_size=1e-5, q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0,
+              stress_targets=None, mixed_tol=1e4, mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200,
+              q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0):
+    nx, ny, M = Q0.shape
+    stress_targets = {(1, 1): 0.0} if stress_targets is None else stress_targets
+    catalog = catalog.copy()
+    Q0 = Q0.copy()
+    eps_p = np.zeros((nx, ny, 2, 2))
+    soft = np.zeros((nx, ny, 2))
+    t_last = np.full((nx, ny), -np.inf)
+    prev = np.zeros((nx, ny, 2, 2))
+    Q = np.zeros((nx, ny, M))
+    eps_macro = np.zeros((2, 2))
+    time = 0.0
+    tau = 1.0 / (nu0 * np.exp(-q_act_temp / (OK.KB * T))) if T > 0 else np.inf  # kmc_simulator.py:86-92
+    E_avg, nu_avg = E.mean(), nu.mean()
+
+    def elastic_run():
+        eps, sig, _, sigM = OL.spectral_solver(E, nu, eps_macro, eps_p, max_iter=ls_max_iter, tol=ls_tol)
+        if np.any(np.isnan(sig)) or np.max(np.abs(sigM)) / 1e9 > 20.0:
+            raise ValueError(f"Unstable stress in small-strain elastic_run: {sigM / 1e9} GPa")
+        return sig, sigM
+
+    sig, sigM = elastic_run()
+    events = []
+    n_solves = 1
+    strain_unit = np.zeros((2, 2))
+    strain_unit[0, 0] = 1.0
+    dt_step = abs(step_size) / strain_rate if strain_rate > 0 else 1.0
+    remaining = 0.0
+    steps_done = 0
+    while steps_done < n_steps:
+        remaining += dt_step
+        while remaining > 0:
+            OK.compute_barrier(Q, Q0, sig, catalog, volume, soft, t_last, time, prev, cap, 0, tau)
+            rates, indices, total = OK.compute_rates(Q, 1.0, T, nu0, cascade_mode=False)
+            if total > 0:
+                u = rng.random()
+                t_wait = -np.log(u) / total
+                if t_wait < remaining:
+                    time += t_wait
+                    eps_macro += strain_unit * (strain_rate * t_wait)
+                    remaining -= t_wait
+                    k = OK.select_event(rates, total, rng.random())
+                    x, y, m = OK.decode_index_2d(int(indices[k]), ny, M)
+                    C = catalog[x, y, m].copy()
+                    OK.apply_flip_2d(eps_p, soft, t_last, catalog, x, y, m, time, jp, jt, cap, jn)
+                    prev[x, y] = C
+                    catalog[x, y] = pure_shear_modes(rng.uniform(0.0, np.pi, M), gamma0)
+                    Q0[x, y] = np.clip(rng.normal(q_mean, q_std, M), q_min, None)
+                    sig, sigM = elastic_run()
+                    n_solves += 1
+                    events.append((x, y, m, time))
+                    if max_events is not None and len(events) >= max_events:
+                        return dict(events=events, eps_macro=eps_macro, sig=sig, eps_p=eps_p, time=time,
+                                    steps=steps_done, solves=n_solves, catalog=catalog, Q0=Q0)
+                    continue
+            eps_macro += strain_unit * (strain_rate * remaining)
+            time += remaining
+            remaining = 0.0
+        # mixed stress control at the end of the AQS step (kmc_simulator.py:1106-1143)
+        prev_e, prev_s = {}, {}
+        for _ in range(mixed_max_iter):
+            sig, sigM = elastic_run()
+            n_solves += 1
+            err = np.zeros((2, 2))
+            err_max = 0.0
+            for idx, target in stress_targets.items():
+                e = target - sigM[idx]
+                err[idx] = e
+                err_max = max(err_max, abs(e))
+            if err_max < mixed_tol:
+                break
+            d_eps = (err - nu_avg * np.trace(err) * np.eye(2)) / E_avg
+            for idx in stress_targets:
+                step = d_eps[idx]
+                if idx in prev_e:
+                    d_e = eps_macro[idx] - prev_e[idx]
+                    d_s = sigM[idx] - prev_s[idx]
+                    if abs(d_e) > 1e-14 and np.isfinite(d_s):
+                        slope = d_s / d_e
+                        if np.isfinite(slope) and slope > 0.01 * E_avg:
+                            step = err[idx] / slope
+                prev_e[idx] = eps_macro[idx]
+                prev_s[idx] = sigM[idx]
+                eps_macro[idx] += step
+        steps_done += 1
+    return dict(events=events, eps_macro=eps_macro, sig=sig, eps_p=eps_p, time=time, steps=steps_done,
+                solves=n_solves, catalog=catalog, Q0=Q0)
