@@ -1,0 +1,71 @@
+"""The finite-strain oracle (oracle/fs.py) reproduces the unmodified
+reference: constitutive P, the matrix-free tangent operator, the projection,
+one mixed-BC Newton-Krylov load step (golden fixture), and the 2D
+plane-strain Neo-Hookean law the 3D Neo-Hookean is restated from."""
+import numpy as np
+
+from oracle import fs as OF
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_constitutive_tangent_projection(golden):
+    g = golden("fs3d_svk_6")
+    lam, mu = OF.lame_3d(g["E"], g["nu"])
+    F = OF.to_spatial(g["F_trial"])
+    Fpi = np.linalg.inv(OF.to_spatial(g["Fp"]))
+    P, st = OF.constitutive(F, lam, mu, Fpi, "svk")
+    assert rel(OF.to_tensor_first(P), g["P_trial"]) < 1e-13
+    KdF = OF.kdf(OF.to_spatial(g["dF"]), st)
+    assert rel(OF.to_tensor_first(KdF), g["KdF"]) < 1e-13
+    GK = OF.project(KdF)
+    assert rel(OF.to_tensor_first(GK), g["GKdF"]) < 1e-12
+
+
+def test_newton_step_matches_reference(golden):
+    g = golden("fs3d_svk_6")
+    F0 = OF.to_spatial(np.einsum("ij,xyz->ijxyz", np.eye(3), np.ones(g["E"].shape)))
+    F, P, Sig, Fb = OF.solver_step_3d(F0, g["F_bar_in"], g["E"], g["nu"], OF.to_spatial(g["Fp"]), (0, 0),
+                                      np.zeros((3, 3)), g["P_mask"], tol_NW=1e-10, tol_CG=1e-10, max_NW=30,
+                                      tol_macro=1e3, max_iter_macro=30, model="svk", krylov="bicgstab")
+    assert rel(OF.to_tensor_first(F), g["F"]) < 1e-9
+    assert rel(OF.to_tensor_first(P), g["P"]) < 1e-9
+    assert rel(OF.to_tensor_first(Sig), g["Sig"]) < 1e-9
+    assert np.max(np.abs(Fb - g["F_bar_out"])) < 1e-9
+    # CG instead of BiCGSTAB converges to the same load-step solution
+    F2, P2, _, _ = OF.solver_step_3d(F0, g["F_bar_in"], g["E"], g["nu"], OF.to_spatial(g["Fp"]), (0, 0),
+                                     np.zeros((3, 3)), g["P_mask"], tol_NW=1e-10, tol_CG=1e-10, max_NW=30,
+                                     tol_macro=1e3, max_iter_macro=30, model="svk", krylov="cg")
+    assert rel(OF.to_tensor_first(F2), g["F"]) < 1e-9
+
+
+def test_neo_hookean_2d_plane_strain(golden):
+    g = golden("fs2d_neohookean_5")
+    lam, mu = OF.lame_3d(g["E"], g["nu"])  # plane strain: the 3D Lame constants (build_C4_2d)
+    F2 = OF.to_spatial(g["F"])
+    P, st = OF.constitutive_2d_plane_strain_nh(F2, lam, mu)
+    assert rel(OF.to_tensor_first(P), g["P"]) < 1e-13
+    # in-plane tangent: the reference K4 (no F_p, mandel branch) against ours
+    rng = np.random.default_rng(0)
+    d2 = rng.standard_normal(F2.shape)
+    ref = np.einsum("ijxy->jixy", np.einsum("ijklxy,lkxy->ijxy", g["K4"], np.einsum("ijxy->jixy", OF.to_tensor_first(d2))))
+    d3 = np.zeros(d2.shape[:-2] + (3, 3)); d3[..., :2, :2] = d2
+    ours = OF.kdf(d3, st)[..., :2, :2]
+    assert rel(OF.to_tensor_first(ours), ref) < 1e-12
+
+
+def test_neo_hookean_close_to_svk_at_small_strain():
+    # the reference's tests/test_finite_strain_kmc.py:127-169 check in 2D, here in 3D
+    from mgkmc_b200 import workloads as W
+    rng = np.random.default_rng(4)
+    E, nu, Fp = W.fs3d_material(6, 6, 6, rng, fp_frac=0.0)
+    F0 = np.broadcast_to(np.eye(3), (6, 6, 6, 3, 3)).copy()
+    Fb, Fm, Pt, Pm = OF.build_bc_3d((0, 0), 1e-5, {(1, 1): 0.0, (2, 2): 0.0})
+    out = {}
+    for model in ("svk", "neo_hookean"):
+        F, P, Sig, _ = OF.solver_step_3d(F0, Fb, E, nu, None, (0, 0), Pt, Pm, tol_NW=1e-10, tol_CG=1e-10,
+                                         max_NW=30, tol_macro=1.0, max_iter_macro=30, model=model, krylov="cg")
+        out[model] = Sig.mean(axis=(0, 1, 2))
+    assert abs(out["svk"][0, 0] - out["neo_hookean"][0, 0]) < 1e-3 * abs(out["svk"][0, 0])
