@@ -174,6 +174,45 @@ MGK_API int mgk_ls3d_solve_batch(mgk_ls3d_t plan, int nsel, const int* sel, cons
 MGK_API int mgk_ls2d_sync_voxel(mgk_ls2d_t plan, int rep, const double* eps_plastic, const int64_t* d_xy,
                                 mgk_stream_t stream);
 
+/* ------------------------------------ 3D finite strain (de Geus Newton) --- */
+/* Replaces mgkmc/finite_strain_simulator.py:2967-3168
+ * finite_strain_solver_step_3d with solver="newton_cg" (the Ghat4 projection
+ * of :1121-1188 and the SVK / F_p constitutive law of :1647-1885 applied
+ * matrix-free; CG Krylov solver with FP64 inner products).  model: 0 SVK,
+ * 1 Neo-Hookean (the reference's 2D plane-strain law restated in 3D).
+ * Fields are tensor-first (3,3,nx,ny,nz) like the reference API. */
+typedef struct mgk_fs3d_plan* mgk_fs3d_t;
+typedef struct {
+  int newton_iterations;   /* summed over the macro iterations */
+  int krylov_iterations;   /* CG iterations (one matvec each) */
+  int macro_iterations;
+  int status;
+  double max_stress_error; /* Pa, last macro iteration */
+  double sig_mean[9];      /* mean Cauchy stress of the returned field */
+} mgk_fs_info;
+MGK_API int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* out);
+MGK_API int mgk_fs3d_destroy(mgk_fs3d_t plan);
+/* lam, mu: device (nx,ny,nz) Lame fields (C4[0,0,1,1], C4[0,1,0,1] of the
+ * reference's C4); Fp: device (3,3,nx,ny,nz) plastic deformation gradient or
+ * NULL (no F_p: the reference's tangent branch without F_p). */
+MGK_API int mgk_fs3d_set_material(mgk_fs3d_t plan, const double* lam, const double* mu, const double* Fp,
+                                  mgk_stream_t stream);
+/* Current deformation gradient (device, tensor-first); the plan keeps it. */
+MGK_API int mgk_fs3d_set_F(mgk_fs3d_t plan, const double* F, mgk_stream_t stream);
+/* One load step from the plan's F: F_bar_in (host 3x3), the driving
+ * component, P_target (host 3x3, Pa, may be NULL) and P_mask (host 3x3 int,
+ * may be NULL), E_avg/nu_avg for the compliance correction, the tolerances
+ * and caps of the reference.  F_bar_out (host 3x3) receives the macro
+ * deformation.  Returns MGK_NOT_CONVERGED where the reference raises
+ * ValueError (line search, Newton or macro loop). */
+MGK_API int mgk_fs3d_step(mgk_fs3d_t plan, const double* F_bar_in, int driving_i, int driving_j,
+                          const double* P_target, const int* P_mask, double E_avg, double nu_avg, double tol_NW,
+                          double tol_CG, int max_NW, double tol_macro, int max_iter_macro, double* F_bar_out,
+                          mgk_fs_info* info, mgk_stream_t stream);
+/* Copy out F and P (device, tensor-first) and compute the Cauchy stress
+ * (cauchy_from_P_3d :1892-1904); any pointer may be NULL. */
+MGK_API int mgk_fs3d_get(mgk_fs3d_t plan, double* F_out, double* P_out, double* sig_out, mgk_stream_t stream);
+
 /* ------------------------------------------------------ 2D STZ / KMC --- */
 /* mgkmc/kmc_simulator_functions.py:100-160 compute_barrier_2d (in place on Q).
  * scheme: 0 isotropic, 1 directional.  tau: +inf for no decay. */

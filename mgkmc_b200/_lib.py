@@ -38,6 +38,11 @@ class LsInfo3(Structure):
                 ("eps_mean", c_double * 9), ("sig_mean", c_double * 9)]
 
 
+class FsInfo(Structure):
+    _fields_ = [("newton_iterations", c_int), ("krylov_iterations", c_int), ("macro_iterations", c_int),
+                ("status", c_int), ("max_stress_error", c_double), ("sig_mean", c_double * 9)]
+
+
 _P = c_void_p
 _SIGS = {
     "mgk_version": (c_int, []),
@@ -66,6 +71,14 @@ _SIGS = {
     "mgk_ls3d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
     "mgk_ls3d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
                                      POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo3), _P]),
+    "mgk_fs3d_create": (c_int, [c_int, c_int, c_int, c_int, POINTER(c_void_p)]),
+    "mgk_fs3d_destroy": (c_int, [_P]),
+    "mgk_fs3d_set_material": (c_int, [_P, _P, _P, _P, _P]),
+    "mgk_fs3d_set_F": (c_int, [_P, _P, _P]),
+    "mgk_fs3d_step": (c_int, [_P, POINTER(c_double), c_int, c_int, POINTER(c_double), POINTER(c_int), c_double,
+                              c_double, c_double, c_double, c_int, c_double, c_int, POINTER(c_double),
+                              POINTER(FsInfo), _P]),
+    "mgk_fs3d_get": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_kmc2d_barrier": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
                                   c_double, c_int, c_double, _P]),
     "mgk_kmc_rates_work_bytes": (c_int64, [c_int64]),

@@ -1,0 +1,846 @@
+// 3D finite-strain de Geus Newton-Krylov solver (FP64), matrix-free.
+//
+// Restates finite_strain_solver_step_3d (mgkmc/finite_strain_simulator.py:
+// 2967-3168) with solver="newton_cg": the macro mixed-BC loop, the Newton
+// loop with the alpha-halving line search, and the Krylov solve of
+//     G : K(F) : dF = rhs,   rhs = -G:K:DbarF (first iteration) or -G:P,
+// where G is the de Geus projection (build_ghat4_3d :1121-1167, applied as
+// (G:A)_ij = (A^ xi)_i xi_j / |xi|^2, zero at DC and on Nyquist planes) and
+// K(F) is applied per voxel from F, F_p^-1 and the moduli without forming
+// the 81-component tangent:
+//   with F_p:    K:dF = S_ref dF^T + Fp^-1 Y Fe^T,  Y = C_eff : sym(Fe^T dF Fp^-1)
+//   without F_p: K:dF = dF S + Fe Y',               Y' = C_eff : sym(Fe^T dF)
+// (the two branches of the reference's tangent, :1849-1871).  Materials:
+// SVK (the reference's 3D law) and Neo-Hookean (the reference's plane-strain
+// law restated in 3D: S = mu I + (lam ln Je - mu) C^-1).  The Krylov solver
+// is CG (the operator is symmetric on the range of G); every inner product
+// and norm is FP64.
+//
+// Layout: tensor-first planes like the reference API, F[i][j] is plane
+// 3*i+j of N = nx*ny*nz doubles (C order, z fastest).
+//
+// One matvec = five kernels: zfwd (p update + K:p per voxel + R2C along z of
+// pairs of z-lines), y pass, x pass fused with G, inverse y pass, zinv (C2R
+// along z + the p.q partial sums).  The CG scalars (alpha, beta, r.r) are
+// computed on the device; the host reads r.r once per iteration.
+#include <math.h>
+#include <stddef.h>
+#include <stdlib.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace mgk {
+
+const void* twiddles(int n, int prec);
+
+struct FsScalars {
+  double rr, pq, alpha, beta, bb;
+  double xx, FF, minJe, nan, pad;
+  double sig[9];
+  double meanF[9];
+};
+
+struct FsArgs {
+  int nx, ny, nz, nzh, ld, tc;
+  long long N;
+  int has_fp, model;  // model 0 SVK, 1 Neo-Hookean
+  FftLen fx, fy, fz;
+  const double* F;
+  const double* Fpi;
+  const double* mu;
+  const double* lam;
+  const double* P;
+  double* x;
+  double* r;
+  double* p;
+  double* q;
+  double* Fout;
+  double* Pout;
+  double2* spec;
+  double* part;
+  FsScalars* sc;
+};
+
+// ------------------------------------------------------- 3x3 helpers ---
+__device__ __forceinline__ void mm(const double* A, const double* B, double* C) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+__device__ __forceinline__ void mtm(const double* A, const double* B, double* C) {  // A^T B
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) C[3 * i + j] = A[i] * B[j] + A[3 + i] * B[3 + j] + A[6 + i] * B[6 + j];
+}
+__device__ __forceinline__ void mmt(const double* A, const double* B, double* C) {  // A B^T
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      C[3 * i + j] = A[3 * i] * B[3 * j] + A[3 * i + 1] * B[3 * j + 1] + A[3 * i + 2] * B[3 * j + 2];
+}
+__device__ __forceinline__ double det3(const double* A) {
+  return A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) + A[2] * (A[3] * A[7] - A[4] * A[6]);
+}
+__device__ __forceinline__ void inv3(const double* A, double* B) {
+  const double d = det3(A);
+  const double s = 1.0 / d;
+  B[0] = (A[4] * A[8] - A[5] * A[7]) * s;
+  B[1] = -(A[1] * A[8] - A[2] * A[7]) * s;
+  B[2] = (A[1] * A[5] - A[2] * A[4]) * s;
+  B[3] = -(A[3] * A[8] - A[5] * A[6]) * s;
+  B[4] = (A[0] * A[8] - A[2] * A[6]) * s;
+  B[5] = -(A[0] * A[5] - A[2] * A[3]) * s;
+  B[6] = (A[3] * A[7] - A[4] * A[6]) * s;
+  B[7] = -(A[0] * A[7] - A[1] * A[6]) * s;
+  B[8] = (A[0] * A[4] - A[1] * A[3]) * s;
+}
+
+// Per-voxel material state at F: Fe, S_ref, and what the tangent needs.
+struct VoxelLaw {
+  double Fe[9], Fpi[9], Sref[9], S[9], Ci[9];
+  double lam, mu, c, Je;
+  int model, has_fp;
+
+  __device__ void init(const FsArgs& a, long long i, const double* F, double alpha, const double* dX) {
+    model = a.model;
+    has_fp = a.has_fp;
+    lam = a.lam[i];
+    mu = a.mu[i];
+    double Fv[9];
+    for (int q = 0; q < 9; ++q) Fv[q] = F[q] + (dX ? alpha * dX[q] : 0.0);
+    if (has_fp) {
+      for (int q = 0; q < 9; ++q) Fpi[q] = a.Fpi[q * a.N + i];
+    } else {
+      for (int q = 0; q < 9; ++q) Fpi[q] = (q % 4 == 0) ? 1.0 : 0.0;
+    }
+    mm(Fv, Fpi, Fe);
+    double C[9];
+    mtm(Fe, Fe, C);
+    Je = det3(Fe);
+    if (model == 0) {
+      double Eg[9];
+      for (int q = 0; q < 9; ++q) Eg[q] = 0.5 * (C[q] - ((q % 4 == 0) ? 1.0 : 0.0));
+      const double tr = Eg[0] + Eg[4] + Eg[8];
+      for (int q = 0; q < 9; ++q) S[q] = 2 * mu * Eg[q] + ((q % 4 == 0) ? lam * tr : 0.0);
+    } else {
+      const double lnJ = log(fmax(1e-14, Je));
+      inv3(C, Ci);
+      c = mu - lam * lnJ;
+      const double k = lam * lnJ - mu;
+      for (int q = 0; q < 9; ++q) S[q] = k * Ci[q] + ((q % 4 == 0) ? mu : 0.0);
+    }
+    double T[9];
+    mm(Fpi, S, T);
+    mmt(T, Fpi, Sref);
+  }
+
+  // P = Fe S Fp^-T
+  __device__ void stress(double* P) const {
+    double T[9];
+    mm(Fe, S, T);
+    mmt(T, Fpi, P);
+  }
+
+  // the reference's trans2(K4 : trans2(d))
+  __device__ void kdf(const double* d, double* out) const {
+    double X[9], T[9], Y[9];
+    mtm(Fe, d, T);
+    mm(T, Fpi, X);
+    if (model == 0) {
+      const double tr = X[0] + X[4] + X[8];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Y[3 * i + j] = mu * (X[3 * i + j] + X[3 * j + i]) + (i == j ? lam * tr : 0.0);
+    } else {
+      double CX[9], Xs[9], U[9];
+      mm(Ci, X, CX);
+      const double tr = CX[0] + CX[4] + CX[8];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Xs[3 * i + j] = X[3 * i + j] + X[3 * j + i];
+      mm(Ci, Xs, U);
+      mm(U, Ci, Xs);
+      for (int q = 0; q < 9; ++q) Y[q] = lam * tr * Ci[q] + c * Xs[q];
+    }
+    double A[9], B[9];
+    mmt(Sref, d, A);  // S_ref d^T
+    mm(Fpi, Y, T);
+    mmt(T, Fe, B);    // Fp^-1 Y Fe^T
+    if (has_fp) {
+      for (int q = 0; q < 9; ++q) out[q] = A[q] + B[q];
+    } else {
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[3 * i + j] = A[3 * j + i] + B[3 * j + i];
+    }
+  }
+};
+
+__device__ __forceinline__ int ffq(int k, int n) { return (k < (n + 1) / 2) ? k : k - n; }
+
+// ----------------------------------------------------------- kernels ---
+
+// z-line forward: MODE 0 CG (p = r + beta p; A = K:p), 1 uniform (A = K:dbar),
+// 2 residual (A = P).  R2C along z of pairs of z-lines, 9 components.
+template <int MODE>
+__global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __restrict__ dbar) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nz = a.nz, nzh = a.nzh, ld = a.ld;
+  const long long N = a.N;
+  const long long l0 = 2LL * blockIdx.x;
+  const long long plane = (long long)a.nx * a.ny * ld;
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 9 * nz;
+  const double beta = MODE == 0 ? a.sc->beta : 0.0;
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    double out[2][9];
+    for (int h = 0; h < 2; ++h) {
+      const long long i = (l0 + h) * nz + z;
+      if (MODE == 2) {
+        for (int q = 0; q < 9; ++q) out[h][q] = a.P[q * N + i];
+      } else {
+        double d[9];
+        if (MODE == 0) {
+          for (int q = 0; q < 9; ++q) {
+            const double pn = a.r[q * N + i] + beta * a.p[q * N + i];
+            a.p[q * N + i] = pn;
+            d[q] = pn;
+          }
+        } else {
+          for (int q = 0; q < 9; ++q) d[q] = dbar[q];
+        }
+        double F[9];
+        for (int q = 0; q < 9; ++q) F[q] = a.F[q * N + i];
+        VoxelLaw law;
+        law.init(a, i, F, 0.0, nullptr);
+        law.kdf(d, out[h]);
+      }
+    }
+    for (int q = 0; q < 9; ++q) bufA[q * nz + z] = make_double2(out[0][q], out[1][q]);
+  }
+  __syncthreads();
+  C* Z = fft_any<-1>(bufA, bufB, 9, nz, a.fz);
+  for (int e = threadIdx.x; e < 9 * nzh; e += blockDim.x) {
+    const int c = e / nzh, k = e - c * nzh;
+    const C z = Z[c * nz + k];
+    const C w = Z[c * nz + (k == 0 ? 0 : nz - k)];
+    C* ra = a.spec + c * plane + l0 * ld;
+    ra[k] = make_double2(0.5 * (z.x + w.x), 0.5 * (z.y - w.y));
+    ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
+  }
+}
+
+// z-line inverse: C2R along z.  MODE 0: q = result, partial p.q.
+// MODE 1: r = -result (right-hand side), x = p = 0, partial r.r.
+template <int MODE>
+__global__ void __launch_bounds__(256) fs_zinv_kernel(FsArgs a) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  const int nz = a.nz, ld = a.ld;
+  const long long N = a.N;
+  const long long l0 = 2LL * blockIdx.x;
+  const long long plane = (long long)a.nx * a.ny * ld;
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 9 * nz;
+  for (int e = threadIdx.x; e < 9 * nz; e += blockDim.x) {
+    const int c = e / nz, k = e - c * nz;
+    const int ks = (2 * k <= nz) ? k : nz - k;
+    const C* ra = a.spec + c * plane + l0 * ld;
+    C av = ra[ks], bv = ra[ld + ks];
+    C z;
+    if (2 * k <= nz) {
+      if (k == 0 || 2 * k == nz) { av.y = 0; bv.y = 0; }
+      z = make_double2(av.x - bv.y, av.y + bv.x);
+    } else {
+      z = make_double2(av.x + bv.y, bv.x - av.y);
+    }
+    bufA[e] = z;
+  }
+  __syncthreads();
+  C* R = fft_any<+1>(bufA, bufB, 9, nz, a.fz);
+  double acc = 0;
+  for (int e = threadIdx.x; e < 9 * nz; e += blockDim.x) {
+    const int c = e / nz, z = e - c * nz;
+    const C v = R[e];
+    for (int h = 0; h < 2; ++h) {
+      const long long i = (l0 + h) * nz + z;
+      const double val = h == 0 ? v.x : v.y;
+      if (MODE == 0) {
+        a.q[c * N + i] = val;
+        acc += a.p[c * N + i] * val;
+      } else {
+        a.r[c * N + i] = -val;
+        a.x[c * N + i] = 0.0;
+        a.p[c * N + i] = 0.0;
+        acc += val * val;
+      }
+    }
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
+}
+
+// y-axis pass over tiles of tc kz columns (9 components)
+template <int SIGN>
+__global__ void __launch_bounds__(256) fs_ypass_kernel(FsArgs a) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = a.nx, ny = a.ny, nzh = a.nzh, ld = a.ld, tc = a.tc;
+  const int ntile = (nzh + tc - 1) / tc;
+  const int o = blockIdx.x / ntile;  // x
+  const int k0 = (blockIdx.x - o * ntile) * tc;
+  const int tcw = min(tc, nzh - k0);
+  const long long plane = (long long)nx * ny * ld;
+  const long long obase = (long long)o * ny * ld;
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 9 * tc * ny;
+  const int tot = 9 * tcw * ny;
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int c = e / (tcw * ny), rem = e - c * tcw * ny, j = rem / tcw, t = rem - j * tcw;
+    bufA[(c * tc + t) * ny + j] = a.spec[c * plane + obase + (long long)j * ld + k0 + t];
+  }
+  __syncthreads();
+  C* F = fft_any<SIGN>(bufA, bufB, 9 * tc, ny, a.fy);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int c = e / (tcw * ny), rem = e - c * tcw * ny, j = rem / tcw, t = rem - j * tcw;
+    a.spec[c * plane + obase + (long long)j * ld + k0 + t] = F[(c * tc + t) * ny + j];
+  }
+}
+
+// x pass: FFT along x, G, IFFT along x (with the 1/N of the transform pair)
+__global__ void __launch_bounds__(256) fs_xg_kernel(FsArgs a) {
+  using C = double2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = a.nx, ny = a.ny, nz = a.nz, nzh = a.nzh, ld = a.ld, tc = a.tc;
+  const int ntile = (nzh + tc - 1) / tc;
+  const int o = blockIdx.x / ntile;  // y
+  const int k0 = (blockIdx.x - o * ntile) * tc;
+  const int tcw = min(tc, nzh - k0);
+  const long long plane = (long long)nx * ny * ld;
+  const long long lstride = (long long)ny * ld;
+  const long long obase = (long long)o * ld;
+  C* bufA = reinterpret_cast<C*>(smem_raw);
+  C* bufB = bufA + 9 * tc * nx;
+  const int tot = 9 * tcw * nx;
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int c = e / (tcw * nx), rem = e - c * tcw * nx, j = rem / tcw, t = rem - j * tcw;
+    bufA[(c * tc + t) * nx + j] = a.spec[c * plane + obase + j * lstride + k0 + t];
+  }
+  __syncthreads();
+  C* G = fft_any<-1>(bufA, bufB, 9 * tc, nx, a.fx);
+  const double scale = 1.0 / (double)a.N;
+  const int ky = o;
+  const double uy = (double)ffq(ky, ny) / ny;
+  const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
+  for (int e = threadIdx.x; e < tcw * nx; e += blockDim.x) {
+    const int t = e / nx, kx = e - t * nx;
+    const int kz = k0 + t;
+    const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
+    if ((kx == 0 && ky == 0 && kz == 0) || nqx || nqy || nqz) {
+      for (int c = 0; c < 9; ++c) G[(c * tc + t) * nx + kx] = make_double2(0.0, 0.0);
+      continue;
+    }
+    const double ux = (double)ffq(kx, nx) / nx, uz = (double)ffq(kz, nz) / nz;
+    const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
+    const double n[3] = {ux * inv, uy * inv, uz * inv};
+    C A[9];
+    for (int c = 0; c < 9; ++c) A[c] = G[(c * tc + t) * nx + kx];
+    for (int i = 0; i < 3; ++i) {
+      double vx = 0, vy = 0;
+      for (int l = 0; l < 3; ++l) { vx += A[3 * i + l].x * n[l]; vy += A[3 * i + l].y * n[l]; }
+      for (int j = 0; j < 3; ++j) G[((3 * i + j) * tc + t) * nx + kx] = make_double2(vx * n[j] * scale, vy * n[j] * scale);
+    }
+  }
+  __syncthreads();
+  C* H = (G == bufA) ? bufB : bufA;
+  C* Rz = fft_any<+1>(G, H, 9 * tc, nx, a.fx);
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int c = e / (tcw * nx), rem = e - c * tcw * nx, j = rem / tcw, t = rem - j * tcw;
+    a.spec[c * plane + obase + j * lstride + k0 + t] = Rz[(c * tc + t) * nx + j];
+  }
+}
+
+// CG update: x += alpha p; r -= alpha q; partial r.r
+__global__ void fs_update_kernel(FsArgs a) {
+  __shared__ double red[32];
+  const double alpha = a.sc->alpha;
+  const long long n9 = 9 * a.N;
+  double acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9; i += (long long)gridDim.x * blockDim.x) {
+    a.x[i] += alpha * a.p[i];
+    const double rn = a.r[i] - alpha * a.q[i];
+    a.r[i] = rn;
+    acc += rn * rn;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
+}
+
+// fixed-order sum of nb partials; MODE 0: pq -> alpha; 1: r.r -> beta, rr;
+// 2: right-hand side -> rr = bb, beta = 0
+template <int MODE>
+__global__ void fs_scalar_kernel(FsArgs a, int nb) {
+  __shared__ double red[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) s += a.part[i];
+  s = block_sum(s, red);
+  if (threadIdx.x != 0) return;
+  FsScalars& S = *a.sc;
+  if (MODE == 0) {
+    S.pq = s;
+    S.alpha = (s != 0.0) ? S.rr / s : 0.0;
+  } else if (MODE == 1) {
+    S.beta = (S.rr != 0.0) ? s / S.rr : 0.0;
+    S.rr = s;
+  } else {
+    S.rr = s;
+    S.bb = s;
+    S.beta = 0.0;
+  }
+}
+
+// Constitutive evaluation at F + alpha (x + dbar) (or at F when dx is 0):
+// writes Fout, Pout; per-CTA partials: min Je, NaN count, sum F^2, sum x^2,
+// and the Cauchy stress sums (cauchy_from_P_3d).  16 values per CTA.
+__global__ void fs_constitutive_kernel(FsArgs a, double alpha, const double* __restrict__ dbar, int use_x) {
+  __shared__ double red[32];
+  const long long N = a.N;
+  double mnJ = INFINITY, nan = 0, FF = 0, xx = 0;
+  double sg[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    double F[9], dX[9];
+    for (int q = 0; q < 9; ++q) {
+      F[q] = a.F[q * N + i];
+      const double xv = use_x ? a.x[q * N + i] : 0.0;
+      dX[q] = xv + (dbar ? dbar[q] : 0.0);
+      xx += xv * xv;
+    }
+    VoxelLaw law;
+    law.init(a, i, F, alpha, dX);
+    double Ft[9], P[9];
+    for (int q = 0; q < 9; ++q) Ft[q] = F[q] + alpha * dX[q];
+    law.stress(P);
+    if (!(law.Je == law.Je)) nan += 1;
+    mnJ = fmin(mnJ, law.Je);
+    double J = det3(Ft);
+    if (fabs(J) < 1e-14) J = 1e-14;
+    double PF[9];
+    mmt(P, Ft, PF);
+    for (int q = 0; q < 9; ++q) {
+      if (!(P[q] == P[q])) nan += 1;
+      a.Fout[q * N + i] = Ft[q];
+      a.Pout[q * N + i] = P[q];
+      FF += Ft[q] * Ft[q];
+      sg[q] += PF[q] / J;
+    }
+  }
+  // min via block reduction on -x with max semantics
+  double v[13] = {0};
+  v[0] = nan; v[1] = FF; v[2] = xx;
+  for (int q = 0; q < 9; ++q) v[3 + q] = sg[q];
+  for (int q = 0; q < 12; ++q) {
+    const double t = block_sum(v[q], red);
+    if (threadIdx.x == 0) a.part[(size_t)blockIdx.x * 16 + q] = t;
+  }
+  // min Je
+  __shared__ double mn[32];
+  double m = mnJ;
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) mn[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = INFINITY;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) r = fmin(r, mn[w]);
+    a.part[(size_t)blockIdx.x * 16 + 12] = r;
+  }
+}
+
+__global__ void fs_constitutive_finalize(FsArgs a, int nb) {
+  __shared__ double red[32];
+  FsScalars& S = *a.sc;
+  double v[12];
+  for (int q = 0; q < 12; ++q) {
+    double s = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) s += a.part[(size_t)i * 16 + q];
+    v[q] = block_sum(s, red);
+  }
+  __shared__ double mn;
+  if (threadIdx.x == 0) {
+    double r = INFINITY;
+    for (int i = 0; i < nb; ++i) r = fmin(r, a.part[(size_t)i * 16 + 12]);
+    mn = r;
+    S.nan = v[0];
+    S.FF = v[1];
+    S.xx = v[2];
+    for (int q = 0; q < 9; ++q) S.sig[q] = v[3 + q] / (double)a.N;
+    S.minJe = mn;
+  }
+}
+
+// means of the 9 components of F (DbarF = F_bar - mean(F)): per-CTA partials
+__global__ void fs_meanF_kernel(FsArgs a) {
+  __shared__ double red[32];
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N; i += (long long)gridDim.x * blockDim.x)
+    for (int q = 0; q < 9; ++q) s[q] += a.F[q * a.N + i];
+  for (int q = 0; q < 9; ++q) {
+    const double t = block_sum(s[q], red);
+    if (threadIdx.x == 0) a.part[(size_t)blockIdx.x * 16 + q] = t;
+  }
+}
+
+__global__ void fs_meanF_finalize(FsArgs a, int nb) {
+  __shared__ double red[32];
+  for (int q = 0; q < 9; ++q) {
+    double s = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) s += a.part[(size_t)i * 16 + q];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) a.sc->meanF[q] = s / (double)a.N;
+  }
+}
+
+// Cauchy stress field (cauchy_from_P_3d), tensor-first
+__global__ void fs_cauchy_kernel(const double* __restrict__ P, const double* __restrict__ F, long long N, double* sig) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    double Pv[9], Fv[9], PF[9];
+    for (int q = 0; q < 9; ++q) { Pv[q] = P[q * N + i]; Fv[q] = F[q * N + i]; }
+    double J = det3(Fv);
+    if (fabs(J) < 1e-14) J = 1e-14;
+    mmt(Pv, Fv, PF);
+    for (int q = 0; q < 9; ++q) sig[q * N + i] = PF[q] / J;
+  }
+}
+
+// material: lam, mu planes and Fp^-1 (plain inverse of F_p, as _invert_Fp_3d)
+__global__ void fs_material_kernel(long long N, const double* __restrict__ lam_in, const double* __restrict__ mu_in,
+                                   const double* __restrict__ Fp, double* lam, double* mu, double* Fpi) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    lam[i] = lam_in[i];
+    mu[i] = mu_in[i];
+    if (Fp) {
+      double A[9], B[9];
+      for (int q = 0; q < 9; ++q) A[q] = Fp[q * N + i];
+      double d = det3(A);
+      if (fabs(d) < 1e-14) d = 1e-14;
+      const double s = 1.0 / d;
+      B[0] = (A[4] * A[8] - A[5] * A[7]) * s;
+      B[1] = -(A[1] * A[8] - A[2] * A[7]) * s;
+      B[2] = (A[1] * A[5] - A[2] * A[4]) * s;
+      B[3] = -(A[3] * A[8] - A[5] * A[6]) * s;
+      B[4] = (A[0] * A[8] - A[2] * A[6]) * s;
+      B[5] = -(A[0] * A[5] - A[2] * A[3]) * s;
+      B[6] = (A[3] * A[7] - A[4] * A[6]) * s;
+      B[7] = -(A[0] * A[7] - A[1] * A[6]) * s;
+      B[8] = (A[0] * A[4] - A[1] * A[3]) * s;
+      for (int q = 0; q < 9; ++q) Fpi[q * N + i] = B[q];
+    }
+  }
+}
+
+}  // namespace mgk
+
+// ================================================================== plan ===
+using namespace mgk;
+
+struct mgk_fs3d_plan {
+  int nx, ny, nz, nzh, ld, tc, model;
+  long long N;
+  int has_fp = 0, has_material = 0;
+  FftLen fx, fy, fz;
+  double* fields = nullptr;  // F, Ftr, Fpi, lam, mu, P, Ptr, x, r, p, q
+  double *F, *Ftr, *Fpi, *lam, *mu, *P, *Ptr, *x, *r, *p, *q;
+  double2* spec = nullptr;
+  double* part = nullptr;
+  double* dbar = nullptr;   // device 9 doubles
+  FsScalars* sc = nullptr;
+  FsScalars* h_sc = nullptr;  // pinned
+  double* h_dbar = nullptr;   // pinned
+  size_t zsmem = 0, ysmem = 0, xsmem = 0;
+  int nblk = 0;
+  int stat_newton = 0, stat_krylov = 0, stat_macro = 0;
+};
+
+static FsArgs fs_args(mgk_fs3d_t p) {
+  FsArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nx = p->nx; a.ny = p->ny; a.nz = p->nz; a.nzh = p->nzh; a.ld = p->ld; a.tc = p->tc;
+  a.N = p->N; a.has_fp = p->has_fp; a.model = p->model;
+  a.fx = p->fx; a.fy = p->fy; a.fz = p->fz;
+  a.F = p->F; a.Fpi = p->Fpi; a.mu = p->mu; a.lam = p->lam; a.P = p->P;
+  a.x = p->x; a.r = p->r; a.p = p->p; a.q = p->q; a.Fout = p->Ftr; a.Pout = p->Ptr;
+  a.spec = p->spec; a.part = p->part; a.sc = p->sc;
+  return a;
+}
+
+extern "C" int mgk_fs3d_destroy(mgk_fs3d_t p) {
+  if (!p) return MGK_OK;
+  cudaFree(p->fields);
+  cudaFree(p->spec);
+  cudaFree(p->part);
+  cudaFree(p->dbar);
+  cudaFree(p->sc);
+  if (p->h_sc) cudaFreeHost(p->h_sc);
+  if (p->h_dbar) cudaFreeHost(p->h_dbar);
+  delete p;
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* out) {
+  MGK_REQUIRE(out, "mgk_fs3d_create: null output handle");
+  *out = nullptr;
+  MGK_REQUIRE(model == 0 || model == 1, "mgk_fs3d_create: model must be 0 (SVK) or 1 (Neo-Hookean)");
+  FftLen fx, fy, fz;
+  MGK_REQUIRE(fft_schedule(nx, &fx) && fft_schedule(ny, &fy) && fft_schedule(nz, &fz) && ((long long)nx * ny) % 2 == 0,
+              "mgk_fs3d_create: grid %dx%dx%d unsupported (sides 2^a 3^b up to 4096, nx*ny even)", nx, ny, nz);
+  mgk_fs3d_t p = new mgk_fs3d_plan();
+  auto fail = [&](int s) { mgk_fs3d_destroy(p); return s; };
+  p->nx = nx; p->ny = ny; p->nz = nz; p->nzh = nz / 2 + 1; p->ld = p->nzh; p->model = model;
+  p->N = (long long)nx * ny * nz;
+  int tc = 4;
+  while (tc > 1 && 2 * 9 * (size_t)tc * std::max(nx, ny) * sizeof(double2) > 96 * 1024) tc >>= 1;
+  p->tc = tc;
+  p->zsmem = 2 * 9 * (size_t)nz * sizeof(double2);
+  p->ysmem = 2 * 9 * (size_t)tc * ny * sizeof(double2);
+  p->xsmem = 2 * 9 * (size_t)tc * nx * sizeof(double2);
+  MGK_REQUIRE(p->zsmem <= 220 * 1024 && p->ysmem <= 220 * 1024 && p->xsmem <= 220 * 1024,
+              "mgk_fs3d_create: grid too large for the shared-memory FFT");
+  fx.tw = twiddles(nx, MGK_FP64); fy.tw = twiddles(ny, MGK_FP64); fz.tw = twiddles(nz, MGK_FP64);
+  if (!fx.tw || !fy.tw || !fz.tw) return fail(MGK_OOM);
+  p->fx = fx; p->fy = fy; p->fz = fz;
+  const long long N = p->N;
+  if (cudaMalloc(&p->fields, sizeof(double) * N * (9 * 9 + 2)) != cudaSuccess) { cudaGetLastError(); return fail(MGK_OOM); }
+  double* f = p->fields;
+  p->F = f; p->Ftr = f + 9 * N; p->Fpi = f + 18 * N; p->lam = f + 27 * N; p->mu = f + 28 * N;
+  p->P = f + 29 * N; p->Ptr = f + 38 * N; p->x = f + 47 * N; p->r = f + 56 * N; p->p = f + 65 * N; p->q = f + 74 * N;
+  if (cudaMalloc(&p->spec, 9 * (size_t)nx * ny * p->ld * sizeof(double2)) != cudaSuccess) { cudaGetLastError(); return fail(MGK_OOM); }
+  p->nblk = (int)std::max(1LL, std::min(1024LL, (N + 255) / 256));
+  const size_t npart = std::max((size_t)16 * p->nblk, (size_t)((long long)nx * ny / 2 + 16));
+  const size_t npart2 = std::max(npart, (size_t)(9 * N / 256 + 64));
+  if (cudaMalloc(&p->part, sizeof(double) * npart2) != cudaSuccess ||
+      cudaMalloc(&p->dbar, sizeof(double) * 16) != cudaSuccess || cudaMalloc(&p->sc, sizeof(FsScalars)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MGK_OOM);
+  }
+  if (cudaMallocHost(&p->h_sc, sizeof(FsScalars)) != cudaSuccess || cudaMallocHost(&p->h_dbar, sizeof(double) * 16) != cudaSuccess)
+    return fail(MGK_OOM);
+  if (cudaMemset(p->fields, 0, sizeof(double) * N * (9 * 9 + 2)) != cudaSuccess ||
+      cudaMemset(p->sc, 0, sizeof(FsScalars)) != cudaSuccess)
+    return fail(MGK_CUDA_ERROR);
+  if (cudaFuncSetAttribute(fs_zfwd_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
+      cudaFuncSetAttribute(fs_zfwd_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
+      cudaFuncSetAttribute(fs_zfwd_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
+      cudaFuncSetAttribute(fs_zinv_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
+      cudaFuncSetAttribute(fs_zinv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
+      cudaFuncSetAttribute(fs_ypass_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ysmem) ||
+      cudaFuncSetAttribute(fs_ypass_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ysmem) ||
+      cudaFuncSetAttribute(fs_xg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->xsmem)) {
+    set_error("mgk_fs3d_create: cudaFuncSetAttribute failed");
+    return fail(MGK_CUDA_ERROR);
+  }
+  *out = p;
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_set_material(mgk_fs3d_t p, const double* lam, const double* mu, const double* Fp,
+                                     mgk_stream_t stream) {
+  MGK_REQUIRE(p && lam && mu, "mgk_fs3d_set_material: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  fs_material_kernel<<<p->nblk, 256, 0, s>>>(p->N, lam, mu, Fp, p->lam, p->mu, p->Fpi);
+  MGK_CUDA(cudaGetLastError());
+  p->has_fp = Fp ? 1 : 0;
+  p->has_material = 1;
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_set_F(mgk_fs3d_t p, const double* F, mgk_stream_t stream) {
+  MGK_REQUIRE(p && F, "mgk_fs3d_set_F: null argument");
+  MGK_CUDA(cudaMemcpyAsync(p->F, F, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_get(mgk_fs3d_t p, double* F_out, double* P_out, double* sig_out, mgk_stream_t stream) {
+  MGK_REQUIRE(p, "mgk_fs3d_get: null plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (F_out) MGK_CUDA(cudaMemcpyAsync(F_out, p->F, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
+  if (P_out) MGK_CUDA(cudaMemcpyAsync(P_out, p->P, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
+  if (sig_out) {
+    fs_cauchy_kernel<<<p->nblk, 256, 0, s>>>(p->P, p->F, p->N, sig_out);
+    MGK_CUDA(cudaGetLastError());
+  }
+  return MGK_OK;
+}
+
+// one matvec / projection: zfwd<MODE> -> y -> xG -> y^-1 -> zinv<ZMODE>
+static int fs_project(mgk_fs3d_t p, int mode, int zmode, cudaStream_t s) {
+  FsArgs a = fs_args(p);
+  const int zl = (int)(p->N / p->nz / 2);
+  const int ntile = (p->nzh + p->tc - 1) / p->tc;
+  if (mode == 0) fs_zfwd_kernel<0><<<zl, 256, p->zsmem, s>>>(a, p->dbar);
+  else if (mode == 1) fs_zfwd_kernel<1><<<zl, 256, p->zsmem, s>>>(a, p->dbar);
+  else fs_zfwd_kernel<2><<<zl, 256, p->zsmem, s>>>(a, p->dbar);
+  fs_ypass_kernel<-1><<<p->nx * ntile, 256, p->ysmem, s>>>(a);
+  fs_xg_kernel<<<p->ny * ntile, 256, p->xsmem, s>>>(a);
+  fs_ypass_kernel<1><<<p->nx * ntile, 256, p->ysmem, s>>>(a);
+  if (zmode == 0) fs_zinv_kernel<0><<<zl, 256, p->zsmem, s>>>(a);
+  else fs_zinv_kernel<1><<<zl, 256, p->zsmem, s>>>(a);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+static int fs_read_scalars(mgk_fs3d_t p, cudaStream_t s) {
+  MGK_CUDA(cudaMemcpyAsync(p->h_sc, p->sc, sizeof(FsScalars), cudaMemcpyDeviceToHost, s));
+  MGK_CUDA(cudaStreamSynchronize(s));
+  return MGK_OK;
+}
+
+// constitutive at F + alpha (x + dbar); results in Ftr/Ptr and the scalars
+static int fs_trial(mgk_fs3d_t p, double alpha, bool use_dbar, bool use_x, cudaStream_t s) {
+  FsArgs a = fs_args(p);
+  fs_constitutive_kernel<<<p->nblk, 256, 0, s>>>(a, alpha, use_dbar ? p->dbar : nullptr, use_x ? 1 : 0);
+  fs_constitutive_finalize<<<1, 256, 0, s>>>(a, p->nblk);
+  MGK_CUDA(cudaGetLastError());
+  return fs_read_scalars(p, s);
+}
+
+static void fs_accept(mgk_fs3d_t p) {
+  std::swap(p->F, p->Ftr);
+  std::swap(p->P, p->Ptr);
+}
+
+// Newton branch (:3046-3119).  F holds F_start on entry, F_curr on exit.
+static int fs_newton(mgk_fs3d_t p, const double* F_bar, double tol_NW, double tol_CG, int max_NW, int max_cg,
+                     cudaStream_t s) {
+  FsArgs a = fs_args(p);
+  fs_meanF_kernel<<<p->nblk, 256, 0, s>>>(a);
+  fs_meanF_finalize<<<1, 256, 0, s>>>(a, p->nblk);
+  MGK_CUDA(cudaGetLastError());
+  int rc = fs_read_scalars(p, s);
+  if (rc) return rc;
+  for (int q = 0; q < 9; ++q) p->h_dbar[q] = F_bar[q] - p->h_sc->meanF[q];
+  MGK_CUDA(cudaMemcpyAsync(p->dbar, p->h_dbar, sizeof(double) * 9, cudaMemcpyHostToDevice, s));
+  // P, K at F_start
+  rc = fs_trial(p, 0.0, false, false, s);
+  if (rc) return rc;
+  fs_accept(p);
+  const int zl = (int)(p->N / p->nz / 2);
+  for (int it = 0; it < max_NW; ++it) {
+    // right-hand side into r (x = p = 0)
+    rc = fs_project(p, it == 0 ? 1 : 2, 1, s);
+    if (rc) return rc;
+    a = fs_args(p);
+    fs_scalar_kernel<2><<<1, 256, 0, s>>>(a, zl);
+    MGK_CUDA(cudaGetLastError());
+    rc = fs_read_scalars(p, s);
+    if (rc) return rc;
+    const double bnorm = sqrt(p->h_sc->bb);
+    for (int k = 0; k < max_cg; ++k) {
+      if (!(sqrt(p->h_sc->rr) > tol_CG * bnorm)) break;
+      rc = fs_project(p, 0, 0, s);
+      if (rc) return rc;
+      a = fs_args(p);
+      fs_scalar_kernel<0><<<1, 256, 0, s>>>(a, zl);
+      fs_update_kernel<<<p->nblk, 256, 0, s>>>(a);
+      fs_scalar_kernel<1><<<1, 256, 0, s>>>(a, p->nblk);
+      MGK_CUDA(cudaGetLastError());
+      rc = fs_read_scalars(p, s);
+      if (rc) return rc;
+      ++p->stat_krylov;
+      if (!isfinite(p->h_sc->rr)) { set_error("mgk_fs3d_step: non-finite Krylov residual"); return MGK_NONFINITE; }
+    }
+    // line search (:3088-3114)
+    double alpha = 1.0;
+    bool ok = false;
+    for (int t = 0; t < 16; ++t) {
+      rc = fs_trial(p, alpha, it == 0, true, s);
+      if (rc) return rc;
+      const FsScalars& S = *p->h_sc;
+      if (!(S.minJe > 1e-4) || S.nan != 0) { alpha *= 0.5; continue; }
+      ok = true;
+      break;
+    }
+    if (!ok) { set_error("Newton-CG line search failed to find a valid step."); return MGK_NOT_CONVERGED; }
+    fs_accept(p);
+    ++p->stat_newton;
+    const double res = sqrt(p->h_sc->xx) / (sqrt(p->h_sc->FF) + 1e-20);
+    if (res < tol_NW && it > 0) return MGK_OK;
+  }
+  set_error("Newton-CG inner solver did not converge within %d iterations.", max_NW);
+  return MGK_NOT_CONVERGED;
+}
+
+extern "C" int mgk_fs3d_step(mgk_fs3d_t p, const double* F_bar_in, int drv_i, int drv_j, const double* P_target,
+                             const int* P_mask, double E_avg, double nu_avg, double tol_NW, double tol_CG, int max_NW,
+                             double tol_macro, int max_iter_macro, double* F_bar_out, mgk_fs_info* info,
+                             mgk_stream_t stream) {
+  MGK_REQUIRE(p && p->has_material && F_bar_in && F_bar_out, "mgk_fs3d_step: bad argument (material set?)");
+  MGK_REQUIRE(max_NW >= 1 && max_iter_macro >= 1, "mgk_fs3d_step: iteration caps must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  double Fb[9], tgt[9] = {0};
+  int mask[9] = {0};
+  for (int q = 0; q < 9; ++q) {
+    Fb[q] = F_bar_in[q];
+    if (P_target) tgt[q] = P_target[q];
+    if (P_mask) mask[q] = P_mask[q] != 0;
+  }
+  bool any_mask = false;
+  for (int q = 0; q < 9; ++q) any_mask |= mask[q] != 0;
+  int upd[3] = {0, 0, 0};
+  for (int k = 0; k < 3; ++k) upd[k] = mask[4 * k] && !(k == drv_i && k == drv_j);
+  bool have_prev = false;
+  double prevF[3] = {0, 0, 0}, prevS[3] = {0, 0, 0};
+  p->stat_newton = p->stat_krylov = p->stat_macro = 0;
+  double max_err = 0.0;
+  int rc = MGK_OK;
+  for (int it = 0; it < max_iter_macro; ++it) {
+    rc = fs_newton(p, Fb, tol_NW, tol_CG, max_NW, 150, s);
+    ++p->stat_macro;
+    if (rc) break;
+    const double* Sm = p->h_sc->sig;
+    if (!any_mask) break;
+    double err[9] = {0};
+    max_err = 0.0;
+    for (int q = 0; q < 9; ++q)
+      if (mask[q]) { err[q] = tgt[q] - Sm[q]; max_err = std::max(max_err, fabs(err[q])); }
+    if (max_err < tol_macro) break;
+    const double trerr = err[0] + err[4] + err[8];
+    double dF[9];
+    for (int q = 0; q < 9; ++q)
+      dF[q] = std::min(0.01, std::max(-0.01, (err[q] - ((q % 4 == 0) ? nu_avg * trerr : 0.0)) / E_avg));
+    double d_sc[3], Fsc[3], ssc[3];
+    for (int k = 0; k < 3; ++k) { d_sc[k] = dF[4 * k]; Fsc[k] = Fb[4 * k]; ssc[k] = Sm[4 * k]; }
+    if (have_prev) {
+      for (int k = 0; k < 3; ++k) {
+        if (!upd[k]) continue;
+        const double dh = Fsc[k] - prevF[k];
+        const double slope = (ssc[k] - prevS[k]) / dh;
+        if (isfinite(slope) && fabs(dh) > 1e-14 && slope > 0.01 * E_avg)
+          d_sc[k] = std::min(0.01, std::max(-0.01, err[4 * k] / slope));
+      }
+    }
+    for (int k = 0; k < 3; ++k) { prevF[k] = Fsc[k]; prevS[k] = ssc[k]; }
+    have_prev = true;
+    for (int k = 0; k < 3; ++k)
+      if (upd[k]) Fb[4 * k] += d_sc[k];
+    if (it == max_iter_macro - 1) {
+      set_error("Outer BC loop did not converge after %d iterations. Final max stress error: %.2e Pa", max_iter_macro,
+                max_err);
+      rc = MGK_NOT_CONVERGED;
+    }
+  }
+  for (int q = 0; q < 9; ++q) F_bar_out[q] = Fb[q];
+  if (info) {
+    info->newton_iterations = p->stat_newton;
+    info->krylov_iterations = p->stat_krylov;
+    info->macro_iterations = p->stat_macro;
+    info->status = rc;
+    info->max_stress_error = max_err;
+    for (int q = 0; q < 9; ++q) info->sig_mean[q] = p->h_sc->sig[q];
+  }
+  return rc;
+}
