@@ -213,3 +213,109 @@ __device__ __forceinline__ C* fft_any(C* a, C* b, int nlines, int ld, const FftL
 }
 
 }  // namespace mgk
+
+// ------------------------------------------------------- warp-line FFTs ---
+// One warp transforms L lines of a compile-time length N that sit in shared
+// memory in a padded layout (one slot of slack per 128 bytes, so the strided
+// stores of the early Stockham passes hit distinct banks).  Each pass reads
+// all of a lane's butterfly inputs into registers, synchronises the warp,
+// then writes the outputs in place: only __syncwarp() between passes, so
+// warps of a CTA progress independently.
+namespace mgk {
+
+template <typename C> __device__ __forceinline__ int pidx(int i) {
+  return sizeof(C) == 16 ? i + (i >> 3) : i + (i >> 4);
+}
+// padded line length in elements, rounded up to 16 bytes
+template <typename C> constexpr int padded_len(int n) {
+  return sizeof(C) == 16 ? n + n / 8 + 1 : ((n + n / 16 + 1 + 1) & ~1);
+}
+
+template <int N, int SIGN, int L, int P, int NS, typename C>
+__device__ __forceinline__ void warp_pass(C* a, int stride, const C* __restrict__ tw, int lane) {
+  constexpr RadixList S = make_sched(N);
+  if constexpr (P < S.np) {
+    constexpr int R = S.r[P];
+    constexpr int nb = N / R;
+    constexpr int U = (nb + 31) / 32;
+    constexpr int tws = N / (NS * R);
+    C v[L][U][R];
+#pragma unroll
+    for (int l = 0; l < L; ++l)
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = lane + 32 * u;
+        if (nb % 32 == 0 || j < nb) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) v[l][u][r] = a[l * stride + pidx<C>(j + r * nb)];
+        }
+      }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int j = lane + 32 * u;
+      if (nb % 32 == 0 || j < nb) {
+        const int k = j % NS;
+        C w[R];
+        if constexpr (NS > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            w[r] = __ldg(&tw[r * k * tws]);
+            if (SIGN > 0) w[r].y = -w[r].y;
+          }
+        }
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+          C* x = v[l][u];
+          if constexpr (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) x[r] = cmul(x[r], w[r]);
+          }
+          if constexpr (R == 2) dft2<SIGN>(x);
+          else if constexpr (R == 3) dft3<SIGN>(x);
+          else if constexpr (R == 4) dft4<SIGN>(x[0], x[1], x[2], x[3]);
+          else dft8<SIGN>(x);
+#pragma unroll
+          for (int r = 0; r < R; ++r) a[l * stride + pidx<C>(base + r * NS)] = x[r];
+        }
+      }
+    }
+    __syncwarp();
+    warp_pass<N, SIGN, L, P + 1, NS * R>(a, stride, tw, lane);
+  }
+}
+
+// L lines at a, a + stride, ... (padded layout), transformed in place by the
+// calling warp.  tw: the W_N^m table of the line length.
+template <int N, int SIGN, int L, typename C>
+__device__ __forceinline__ void warp_fft(C* a, int stride, const C* __restrict__ tw, int lane) {
+  warp_pass<N, SIGN, L, 0, 1>(a, stride, tw, lane);
+}
+
+// line lengths with a compiled warp-line FFT
+__host__ __device__ constexpr bool warp_fft_len(int n) {
+  return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512;
+}
+
+// 16- or 8-byte asynchronous global -> shared copies (cp.async, completion
+// tracked per thread with commit/wait groups)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+template <typename C> __device__ __forceinline__ void cp_async_elem(C* dst, const C* src) {
+  if constexpr (sizeof(C) == 16) cp_async16(dst, src);
+  else cp_async8(dst, src);
+}
+
+}  // namespace mgk

@@ -773,6 +773,280 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
   }
 }
 
+// --------------------------------------------- warp-line iteration kernels ---
+// The same two stages for replicas whose sides have a compiled warp-line FFT
+// (64 .. 512).  Row kernel: one CTA of three warps per pair of x-rows; one
+// elected thread stages the pair's eps, mu, lambda and eps_p rows in shared
+// memory with bulk asynchronous copies at entry, while warp c inverts
+// component c of the spectrum; after one CTA barrier every thread updates its
+// voxels and builds tau, then warp c forward-transforms and stores component
+// c.  Column kernel: one CTA of kColTiles warps per tile of kColTiles ky
+// columns; the tile lands in shared memory through cp.async, then warp t runs
+// FFT, Gamma0_sym and inverse FFT on column t alone.
+constexpr int kRowWarps = 3;
+constexpr int kColTiles = 4;
+
+__host__ __device__ constexpr int row_fast_smem(int ny, int csz, int tsz) {
+  return ((3 * (csz == 16 ? ny + ny / 8 + 1 : ((ny + ny / 16 + 2) & ~1)) * csz + 127) / 128) * 128 + 16 * ny * tsz;
+}
+__host__ __device__ constexpr int col_fast_smem(int nx, int csz) {
+  return 3 * kColTiles * (csz == 16 ? nx + nx / 8 + 1 : ((nx + nx / 16 + 2) & ~1)) * csz;
+}
+
+template <typename T, int NY, bool IN_SPEC, bool FINAL>
+__device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, int item, int r, int x0,
+                                              double* partials,
+                                              unsigned int* rep_counter, Ls2dCtl* ctl,
+                                              cudaGraphConditionalHandle cond, int use_cond, int guard_cap,
+                                              unsigned char* smem, uint64_t* bar, double* red, int* s_last) {
+  using C = C_t<T>;
+  constexpr int PL = padded_len<C>(NY);
+  constexpr int NYH = NY / 2 + 1;
+  constexpr int NT = 32 * kRowWarps;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = R.nx, ld = R.ld;
+  const long long N = R.N;
+  C* lines = reinterpret_cast<C*>(smem);
+  T* stg = reinterpret_cast<T*>(smem + ((3 * PL * (int)sizeof(C) + 127) / 128) * 128);
+  T* eps = Fields<T>::eps(R);
+  const T* ep = Fields<T>::ep(R);
+  constexpr uint32_t rb = 2u * NY * sizeof(T);
+  if (threadIdx.x == 0) {
+    const T* src[8] = {eps, eps + N, eps + 2 * N, Fields<T>::mu(R), Fields<T>::lam(R), ep, ep + N, ep + 2 * N};
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, 8u * rb);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) bulk_g2s(stg + q * 2 * NY, src[q] + (long long)x0 * NY, rb, bar);
+  }
+  const C* tw = reinterpret_cast<const C*>(Fields<T>::fy(R).tw);
+  C* spec = reinterpret_cast<C*>(R.spec);
+  C* line = lines + warp * PL;
+  C* ra = spec + ((size_t)warp * nx + x0) * ld;
+  C* rbp = ra + ld;
+  if (IN_SPEC) {
+    constexpr int U = (NYH + 31) / 32;
+    C a[U], b[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = lane + 32 * u;
+      if (k < NYH) { a[u] = ra[k]; b[u] = rbp[k]; }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = lane + 32 * u;
+      if (k < NYH) {
+        C av = a[u], bv = b[u];
+        if (k == 0 || 2 * k == NY) { av.y = 0; bv.y = 0; }
+        line[pidx<C>(k)] = mk<C>(av.x - bv.y, av.y + bv.x);
+        if (k > 0 && 2 * k < NY) line[pidx<C>(NY - k)] = mk<C>(av.x + bv.y, bv.x - av.y);
+      }
+    }
+    __syncwarp();
+    warp_fft<NY, +1, 1>(line, PL, tw, lane);
+  }
+  const bool ok = mbar_wait(bar, 0);
+  if (!__syncthreads_and(ok ? 1 : 0)) {
+    if (threadIdx.x == 0) { ctl->error = 1; ctl->any = 0; }
+    return;
+  }
+  const double mu0 = S.mu0, lam0 = S.lam0;
+  const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
+  double d2 = 0, n2 = 0;
+  for (int y = threadIdx.x; y < NY; y += NT) {
+    T tr[2][3];
+    const int py = pidx<C>(y);
+    C z[3];
+    if (IN_SPEC) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) z[c] = lines[c * PL + py];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = h * NY + y;
+      const long long i = (long long)(x0 + h) * NY + y;
+      const double o0 = (double)stg[j], o1 = (double)stg[2 * NY + j], o2 = (double)stg[4 * NY + j];
+      const double m = (double)stg[6 * NY + j], l = (double)stg[8 * NY + j];
+      const double p0 = (double)stg[10 * NY + j], p1 = (double)stg[12 * NY + j], p2 = (double)stg[14 * NY + j];
+      double e0, e1, e2;
+      if (IN_SPEC) {
+        e0 = eb0 + (double)(h == 0 ? z[0].x : z[0].y);
+        e1 = eb1 + (double)(h == 0 ? z[1].x : z[1].y);
+        e2 = eb2 + (double)(h == 0 ? z[2].x : z[2].y);
+        const double q0 = e0 - o0, q1 = e1 - o1, q2 = e2 - o2;
+        d2 += q0 * q0 + q1 * q1 + 2.0 * q2 * q2;
+        n2 += o0 * o0 + o1 * o1 + 2.0 * o2 * o2;
+        eps[i] = (T)e0;
+        eps[N + i] = (T)e1;
+        eps[2 * N + i] = (T)e2;
+      } else {
+        e0 = o0; e1 = o1; e2 = o2;
+      }
+      const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
+      const double trd = dxx + dyy, tre = e0 + e1;
+      tr[h][0] = (T)((2 * m * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
+      tr[h][1] = (T)((2 * m * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
+      tr[h][2] = (T)(2 * m * dxy - 2 * mu0 * e2);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) lines[c * PL + py] = mk<C>(tr[0][c], tr[1][c]);
+  }
+  __syncthreads();
+  warp_fft<NY, -1, 1>(line, PL, tw, lane);
+  for (int k = lane; k < NYH; k += 32) {
+    const C zz = line[pidx<C>(k)];
+    const C w = line[pidx<C>(k == 0 ? 0 : NY - k)];
+    ra[k] = mk<C>(T(0.5) * (zz.x + w.x), T(0.5) * (zz.y - w.y));
+    rbp[k] = mk<C>(T(0.5) * (zz.y + w.y), T(-0.5) * (zz.x - w.x));
+  }
+  if (!IN_SPEC) return;
+  d2 = block_sum(d2, red);
+  n2 = block_sum(n2, red);
+  if (threadIdx.x == 0) {
+    partials[2 * item] = d2;
+    partials[2 * item + 1] = n2;
+    __threadfence();
+    const unsigned int t = atomicInc(&rep_counter[r], (unsigned int)R.row_items - 1);  // self-resetting
+    *s_last = (t == (unsigned int)R.row_items - 1);
+  }
+  __syncthreads();
+  if (!*s_last) return;
+  __threadfence();
+  ls2d_decide<FINAL>(R, S, partials, ctl, cond, use_cond, guard_cap, red);
+}
+
+template <typename T, int MAXN, bool IN_SPEC, bool FINAL>
+__global__ void __launch_bounds__(32 * kRowWarps) ls2d_row_fast_kernel(
+    const Ls2dRep* __restrict__ reps, Ls2dState* st, const int* __restrict__ row_map,
+    const int* __restrict__ row_local, double* partials, unsigned int* rep_counter, Ls2dCtl* ctl,
+    cudaGraphConditionalHandle cond, int use_cond, int guard_cap) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  __shared__ int s_last;
+  __shared__ __align__(8) uint64_t bar;
+  const int item = blockIdx.x;
+  const int r = row_map[item];
+  const Ls2dRep& R = reps[r];
+  Ls2dState& S = st[r];
+  if (IN_SPEC && use_cond && item == 0 && threadIdx.x == 0) {
+    const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap || *(volatile int*)&ctl->error != 0) {
+      ctl->any = 0;
+      cudaGraphSetConditional(cond, 0u);
+    }
+  }
+  if (S.done != 0) return;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const int x0 = 2 * row_local[item];
+#define MGK_ROW_CASE(n) \
+  case n: if constexpr (n <= MAXN) row_fast_body<T, n, IN_SPEC, FINAL>(R, S, item, r, x0, partials, rep_counter, ctl, cond, use_cond, guard_cap, \
+                                              smem_raw, &bar, red, &s_last); break;
+  switch (R.ny) {
+    MGK_ROW_CASE(64) MGK_ROW_CASE(96) MGK_ROW_CASE(128) MGK_ROW_CASE(192) MGK_ROW_CASE(256) MGK_ROW_CASE(384)
+    MGK_ROW_CASE(512)
+    default: break;
+  }
+#undef MGK_ROW_CASE
+}
+
+template <typename T, int NX>
+__device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState& S, int ky0,
+                                              unsigned char* smem) {
+  using C = C_t<T>;
+  constexpr int PL = padded_len<C>(NX);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ny = R.ny, nyh = R.nyh, ld = R.ld;
+  const int tcw = min(kColTiles, nyh - ky0);
+  C* lines = reinterpret_cast<C*>(smem);  // line (c * kColTiles + t)
+  C* spec = reinterpret_cast<C*>(R.spec);
+  constexpr int TOT = 3 * NX * kColTiles;
+  for (int e = threadIdx.x; e < TOT; e += 32 * kColTiles) {
+    const int c = e / (NX * kColTiles);
+    const int rem = e - c * NX * kColTiles;
+    const int x = rem / kColTiles, t = rem - x * kColTiles;
+    if (t < tcw) cp_async_elem(&lines[(c * kColTiles + t) * PL + pidx<C>(x)], &spec[((size_t)c * NX + x) * ld + ky0 + t]);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int t = warp;
+  if (t < tcw) {
+    const C* tw = reinterpret_cast<const C*>(Fields<T>::fx(R).tw);
+    C* l0 = lines + t * PL;
+    constexpr int LS = kColTiles * PL;  // stride between the components of a column
+    warp_fft<NX, -1, 1>(l0, LS, tw, lane);
+    warp_fft<NX, -1, 1>(l0 + LS, LS, tw, lane);
+    warp_fft<NX, -1, 1>(l0 + 2 * LS, LS, tw, lane);
+    const T inv2mu0 = (T)S.inv2mu0, Bc = (T)S.Bc;
+    const T sc = (T)(1.0 / ((double)NX * (double)ny));
+    const int ky = ky0 + t;
+    const double uy = (double)fftfreq(ky, ny) / ny;
+    const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
+    for (int kx = lane; kx < NX; kx += 32) {
+      const int pk = pidx<C>(kx);
+      C* pxx = &l0[pk];
+      C* pyy = &l0[LS + pk];
+      C* pxy = &l0[2 * LS + pk];
+      if (kx == 0 && ky == 0) {
+        *pxx = mk<C>(T(0), T(0)); *pyy = *pxx; *pxy = *pxx;
+        continue;
+      }
+      const double ux = (double)fftfreq(kx, NX) / NX;
+      const double inv = 1.0 / sqrt(ux * ux + uy * uy);
+      const T nxv = (T)(ux * inv), nyv = (T)(uy * inv);
+      const C txx = *pxx, tyy = *pyy, txy = *pxy;
+      C exx, eyy, exy;
+      gamma2d_apply(txx, tyy, txy, nxv, nyv, inv2mu0, Bc, exx, eyy, exy);
+      const bool nqx = 2 * kx == NX;
+      if (nqx || nqy) {
+        C fxx, fyy, fxy;
+        gamma2d_apply(txx, tyy, txy, nqx ? -nxv : nxv, nqy ? -nyv : nyv, inv2mu0, Bc, fxx, fyy, fxy);
+        exx = mk<C>(T(0.5) * (exx.x + fxx.x), T(0.5) * (exx.y + fxx.y));
+        eyy = mk<C>(T(0.5) * (eyy.x + fyy.x), T(0.5) * (eyy.y + fyy.y));
+        exy = mk<C>(T(0.5) * (exy.x + fxy.x), T(0.5) * (exy.y + fxy.y));
+      }
+      *pxx = mk<C>(exx.x * sc, exx.y * sc);
+      *pyy = mk<C>(eyy.x * sc, eyy.y * sc);
+      *pxy = mk<C>(exy.x * sc, exy.y * sc);
+    }
+    __syncwarp();
+    warp_fft<NX, +1, 1>(l0, LS, tw, lane);
+    warp_fft<NX, +1, 1>(l0 + LS, LS, tw, lane);
+    warp_fft<NX, +1, 1>(l0 + 2 * LS, LS, tw, lane);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < TOT; e += 32 * kColTiles) {
+    const int c = e / (NX * kColTiles);
+    const int rem = e - c * NX * kColTiles;
+    const int x = rem / kColTiles, tt = rem - x * kColTiles;
+    if (tt < tcw) spec[((size_t)c * NX + x) * ld + ky0 + tt] = lines[(c * kColTiles + tt) * PL + pidx<C>(x)];
+  }
+}
+
+template <typename T, int MAXN>
+__global__ void __launch_bounds__(32 * kColTiles) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
+                                                                       const Ls2dState* __restrict__ st,
+                                                                       const int* __restrict__ col_map,
+                                                                       const int* __restrict__ col_local) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int item = blockIdx.x;
+  const int r = col_map[item];
+  const Ls2dRep& R = reps[r];
+  const Ls2dState& S = st[r];
+  if (S.done != 0) return;
+  const int ky0 = col_local[item] * kColTiles;
+#define MGK_COL_CASE(n) \
+  case n: if constexpr (n <= MAXN) col_fast_body<T, n>(R, S, ky0, smem_raw); break;
+  switch (R.nx) {
+    MGK_COL_CASE(64) MGK_COL_CASE(96) MGK_COL_CASE(128) MGK_COL_CASE(192) MGK_COL_CASE(256) MGK_COL_CASE(384)
+    MGK_COL_CASE(512)
+    default: break;
+  }
+#undef MGK_COL_CASE
+}
+
 // Mixed plans, between the phases: FP64 field from the FP32 one.
 // grid = (G, nsel).
 __global__ void ls2d_promote_kernel(const Ls2dRep* reps, const int* sel) {
@@ -868,7 +1142,9 @@ struct mgk_ls2d_plan {
   int nrep = 0;
   int plane_mode = 0, prec = 0;
   long long maxN = 0;
-  size_t row_smem = 0, col_smem = 0;
+  size_t row_smem = 0, col_smem = 0;      // FP64 iteration kernels
+  size_t row_smem32 = 0, col_smem32 = 0;  // FP32 iteration kernels
+  int fast = 0;                           // warp-line kernels (every side has a compiled FFT)
   std::vector<Ls2dRep> reps;      // host copy (static part)
   std::vector<char> has_material;
   Ls2dRep* h_reps = nullptr;      // pinned staging of the table
@@ -909,6 +1185,26 @@ static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
     return MGK_OOM;
   }
   p->allocations.push_back(*ptr);
+  return MGK_OK;
+}
+
+// warp-line kernel variants: sides up to 256, or up to 512 (more registers)
+template <typename TS, bool IN_SPEC, bool FINAL>
+static void* row_fast_fn(int fast) {
+  return fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL>
+                    : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL>;
+}
+template <typename TS>
+static void* col_fast_fn(int fast) {
+  return fast > 256 ? (void*)ls2d_col_fast_kernel<TS, 512> : (void*)ls2d_col_fast_kernel<TS, 256>;
+}
+
+template <typename T>
+static int ls2d_set_fast_attrs(int fast, size_t row_smem, size_t col_smem) {
+  void* fns[4] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
+                  row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast)};
+  for (void* f : fns) MGK_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem));
+  MGK_CUDA(cudaFuncSetAttribute(col_fast_fn<T>(fast), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
   return MGK_OK;
 }
 
@@ -968,14 +1264,25 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
   auto fail = [&](int s) { mgk_ls2d_destroy(p); return s; };
   p->reps.resize(nrep);
   p->has_material.assign(nrep, 0);
-  size_t row_smem = 0, col_smem = 0;
+  {
+    bool fast = true;
+    int side = 0;
+    for (int r = 0; r < nrep; ++r) {
+      fast = fast && warp_fft_len(nxs[r]) && warp_fft_len(nys[r]);
+      side = std::max(side, std::max(nxs[r], nys[r]));
+    }
+    const char* env = getenv("MGK_FAST");
+    if (env && env[0] == '0') fast = false;
+    p->fast = fast ? (side > 256 ? 512 : 256) : 0;
+  }
+  size_t row_smem = 0, col_smem = 0, row_smem32 = 0, col_smem32 = 0;
   for (int r = 0; r < nrep; ++r) {
     const int nx = nxs[r], ny = nys[r];
     Ls2dRep& R = p->reps[r];
     memset(&R, 0, sizeof(R));
     R.nx = nx; R.ny = ny; R.nyh = ny / 2 + 1; R.ld = R.nyh;
     R.N = (long long)nx * ny;
-    R.tc = pick_tc(nx, c64, 64 * 1024);
+    R.tc = p->fast ? kColTiles : pick_tc(nx, c64, 64 * 1024);
     R.row_items = nx / 2;
     R.col_items = (R.nyh + R.tc - 1) / R.tc;
     fft_schedule(nx, &R.fx64);
@@ -990,8 +1297,17 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
       R.fy32.tw = twiddles(ny, 1 /* float table */);
       if (!R.fx32.tw || !R.fy32.tw) return fail(MGK_OOM);
     }
-    row_smem = std::max(row_smem, 2 * 3 * (size_t)ny * c64);
-    col_smem = std::max(col_smem, 2 * 3 * (size_t)R.tc * nx * c64);
+    if (p->fast) {
+      row_smem = std::max(row_smem, (size_t)row_fast_smem(ny, 16, 8));
+      col_smem = std::max(col_smem, (size_t)col_fast_smem(nx, 16));
+      row_smem32 = std::max(row_smem32, (size_t)row_fast_smem(ny, 8, 4));
+      col_smem32 = std::max(col_smem32, (size_t)col_fast_smem(nx, 8));
+    } else {
+      row_smem = std::max(row_smem, 2 * 3 * (size_t)ny * c64);
+      col_smem = std::max(col_smem, 2 * 3 * (size_t)R.tc * nx * c64);
+      row_smem32 = row_smem / 2;
+      col_smem32 = col_smem / 2;
+    }
     p->maxN = std::max(p->maxN, R.N);
     p->total_row_items += R.row_items;
     p->total_col_items += R.col_items;
@@ -1012,8 +1328,11 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
   }
   p->row_smem = row_smem;
   p->col_smem = col_smem;
-  int st = ls2d_set_attrs<double, double>(row_smem, col_smem);
-  if (st == MGK_OK && mixed) st = ls2d_set_attrs<float, float>(row_smem / 2, col_smem / 2);
+  p->row_smem32 = row_smem32;
+  p->col_smem32 = col_smem32;
+  int st = p->fast ? ls2d_set_fast_attrs<double>(p->fast, row_smem, col_smem) : ls2d_set_attrs<double, double>(row_smem, col_smem);
+  if (st == MGK_OK && mixed)
+    st = p->fast ? ls2d_set_fast_attrs<float>(p->fast, row_smem32, col_smem32) : ls2d_set_attrs<float, float>(row_smem32, col_smem32);
   if (st) return fail(st);
   {
     // persistent bulk-prefetch row kernels: every replica needs ny even
@@ -1032,7 +1351,7 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     // opt-in: at 256-point lines the per-CTA FFT work, not load latency,
     // bounds the row kernel, and the prefetching variant needs one CTA per SM
     const char* env = getenv("MGK_TMA");
-    ok = ok && (env && env[0] == '1') && sm64 <= 220 * 1024;
+    ok = ok && !p->fast && (env && env[0] == '1') && sm64 <= 220 * 1024;
     int dev = 0;
     if (ok && cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
@@ -1166,18 +1485,41 @@ struct LoopArgs {
   int row_grid;       // its grid (resident CTAs), <= rows
   int stage_bytes;
   size_t tma_smem;
+  int fast;           // warp-line iteration kernels
 };
+
+template <typename TS, bool IN_SPEC, bool FINAL>
+static void launch_row(const LoopArgs& a, cudaStream_t s) {
+  if (a.fast > 256)
+    ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL><<<a.rows, 32 * kRowWarps, a.row_smem, s>>>(
+        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
+  else if (a.fast)
+    ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL><<<a.rows, 32 * kRowWarps, a.row_smem, s>>>(
+        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
+  else
+    ls2d_row_kernel<TS, TS, IN_SPEC, FINAL><<<a.rows, kThreads, a.row_smem, s>>>(
+        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
+}
+
+template <typename TS>
+static void launch_col(const LoopArgs& a, cudaStream_t s) {
+  if (a.fast > 256)
+    ls2d_col_fast_kernel<TS, 512><<<a.cols, 32 * kColTiles, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
+  else if (a.fast)
+    ls2d_col_fast_kernel<TS, 256><<<a.cols, 32 * kColTiles, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
+  else
+    ls2d_col_kernel<TS, TS><<<a.cols, kThreads, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
+}
 
 template <typename TS, bool FINAL>
 static int launch_body(const LoopArgs& a, cudaStream_t s) {
-  ls2d_col_kernel<TS, TS><<<a.cols, kThreads, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
+  launch_col<TS>(a, s);
   MGK_CUDA(cudaGetLastError());
   if (a.tma)
     ls2d_row_tma_kernel<TS, TS, FINAL><<<a.row_grid, kThreads, a.tma_smem, s>>>(
         a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0, a.rows, a.stage_bytes);
   else
-    ls2d_row_kernel<TS, TS, true, FINAL><<<a.rows, kThreads, a.row_smem, s>>>(
-        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
+    launch_row<TS, true, FINAL>(a, s);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }
@@ -1200,9 +1542,9 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
   cudaKernelNodeParams k1;
   memset(&k1, 0, sizeof(k1));
   void* a1[] = {&a.reps, &a.st, &a.col_map, &a.col_local};
-  k1.func = (void*)ls2d_col_kernel<TS, TS>;
+  k1.func = a.fast ? col_fast_fn<TS>(a.fast) : (void*)ls2d_col_kernel<TS, TS>;
   k1.gridDim = dim3(a.cols);
-  k1.blockDim = dim3(kThreads);
+  k1.blockDim = dim3(a.fast ? 32 * kColTiles : kThreads);
   k1.sharedMemBytes = (unsigned)a.col_smem;
   k1.kernelParams = a1;
   cudaGraphNode_t n1, n2;
@@ -1218,13 +1560,14 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
     k2.gridDim = dim3(a.row_grid);
     k2.sharedMemBytes = (unsigned)a.tma_smem;
     k2.kernelParams = a2t;
+    k2.blockDim = dim3(kThreads);
   } else {
-    k2.func = (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
+    k2.func = a.fast ? row_fast_fn<TS, true, FINAL>(a.fast) : (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
     k2.gridDim = dim3(a.rows);
     k2.sharedMemBytes = (unsigned)a.row_smem;
     k2.kernelParams = a2;
+    k2.blockDim = dim3(a.fast ? 32 * kRowWarps : kThreads);
   }
-  k2.blockDim = dim3(kThreads);
   MGK_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2));
   return MGK_OK;
 }
@@ -1271,9 +1614,10 @@ static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_
       int zero = 0;
       void* ap3[] = {&a64.reps, &a64.st, &a64.row_map, &a64.row_local, &a64.part, &a64.repctr, &a64.ctl,
                      &h0, &zero, &zero};
-      k3.func = (void*)ls2d_row_kernel<double, double, false, true>;
+      k3.func = a64.fast ? row_fast_fn<double, false, true>(a64.fast)
+                         : (void*)ls2d_row_kernel<double, double, false, true>;
       k3.gridDim = dim3(a64.rows);
-      k3.blockDim = dim3(kThreads);
+      k3.blockDim = dim3(a64.fast ? 32 * kRowWarps : kThreads);
       k3.sharedMemBytes = (unsigned)a64.row_smem;
       k3.kernelParams = ap3;
       rc = cudaGraphAddKernelNode(&n_row0, g, &n_ph2, 1, &k3) == cudaSuccess ? MGK_OK : MGK_CUDA_ERROR;
@@ -1379,20 +1723,16 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   if (n_active > 0) {
     const bool mixed = p->prec == MGK_MIXED;
     LoopArgs a64{p->d_reps, p->d_st, d_row_map, d_row_local, d_col_map, d_col_local, p->d_part, p->d_repctr,
-                 p->d_ctl, rows, cols, p->row_smem, p->col_smem, p->tma, 0, p->stage64, p->tma_smem64};
+                 p->d_ctl, rows, cols, p->row_smem, p->col_smem, p->tma, 0, p->stage64, p->tma_smem64, p->fast};
     a64.row_grid = std::max(1, std::min(rows, p->occ64 * p->num_sms));
     LoopArgs a32 = a64;
-    a32.row_smem = p->row_smem / 2;
-    a32.col_smem = p->col_smem / 2;
+    a32.row_smem = p->row_smem32;
+    a32.col_smem = p->col_smem32;
     a32.stage_bytes = p->stage32;
     a32.tma_smem = p->tma_smem32;
     a32.row_grid = std::max(1, std::min(rows, p->occ32 * p->num_sms));
-    if (mixed)
-      ls2d_row_kernel<float, float, false, false><<<rows, kThreads, a32.row_smem, s>>>(
-          p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
-    else
-      ls2d_row_kernel<double, double, false, true><<<rows, kThreads, a64.row_smem, s>>>(
-          p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+    if (mixed) launch_row<float, false, false>(a32, s);
+    else launch_row<double, false, true>(a64, s);
     MGK_CUDA(cudaGetLastError());
     const int guard_cap = (max_iter + 2 > 1000 ? max_iter + 2 : 1000);
     if (p->graph_mode == 1 && (changed || guard_cap > p->graph_cap)) p->graph_mode = -1;
@@ -1412,8 +1752,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
         if (phase == 2 && mixed) {
           ls2d_promote_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, d_sel);
           ls2d_phase2_kernel<<<1, 32, 0, s>>>(p->d_st, d_sel, nsel, p->d_ctl);
-          ls2d_row_kernel<double, double, false, true><<<rows, kThreads, a64.row_smem, s>>>(
-              p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+          launch_row<double, false, true>(a64, s);
           MGK_CUDA(cudaGetLastError());
         }
         for (int it = 0; it < max_iter; ++it) {
@@ -1474,10 +1813,11 @@ static int profile_t(mgk_ls2d_t p, float* row_ms, float* col_ms, int reps, cudaS
   const int* d_row_local = d_row_map + rows;
   const int* d_col_map = d_row_local + rows;
   const int* d_col_local = d_col_map + cols;
-  const size_t rs = sizeof(TS) == 8 ? p->row_smem : p->row_smem / 2;
-  const size_t cs = sizeof(TS) == 8 ? p->col_smem : p->col_smem / 2;
-  ls2d_row_kernel<TS, TS, false, true><<<rows, kThreads, rs, s>>>(p->d_reps, p->d_st, d_row_map, d_row_local,
-                                                                  p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+  const size_t rs = sizeof(TS) == 8 ? p->row_smem : p->row_smem32;
+  const size_t cs = sizeof(TS) == 8 ? p->col_smem : p->col_smem32;
+  LoopArgs a{p->d_reps, p->d_st, d_row_map, d_row_local, d_col_map, d_col_local, p->d_part, p->d_repctr,
+             p->d_ctl, rows, cols, rs, cs, 0, 0, 0, 0, p->fast};
+  launch_row<TS, false, true>(a, s);
   MGK_CUDA(cudaGetLastError());
   cudaEvent_t ev[3];
   for (int i = 0; i < 3; ++i) MGK_CUDA(cudaEventCreate(&ev[i]));
@@ -1485,7 +1825,7 @@ static int profile_t(mgk_ls2d_t p, float* row_ms, float* col_ms, int reps, cudaS
   int rc = MGK_OK;
   for (int r = 0; r < reps; ++r) {
     cudaEventRecord(ev[0], s);
-    ls2d_col_kernel<TS, TS><<<cols, kThreads, cs, s>>>(p->d_reps, p->d_st, d_col_map, d_col_local);
+    launch_col<TS>(a, s);
     cudaEventRecord(ev[1], s);
     if (p->tma) {
       const bool f64 = sizeof(TS) == 8;
@@ -1494,8 +1834,7 @@ static int profile_t(mgk_ls2d_t p, float* row_ms, float* col_ms, int reps, cudaS
           p->d_reps, p->d_st, d_row_map, d_row_local, p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0, rows,
           f64 ? p->stage64 : p->stage32);
     } else {
-      ls2d_row_kernel<TS, TS, true, true><<<rows, kThreads, rs, s>>>(p->d_reps, p->d_st, d_row_map, d_row_local,
-                                                                     p->d_part, p->d_repctr, p->d_ctl, 0, 0, 0);
+      launch_row<TS, true, true>(a, s);
     }
     cudaEventRecord(ev[2], s);
     if (cudaEventSynchronize(ev[2]) != cudaSuccess) { rc = MGK_CUDA_ERROR; break; }
