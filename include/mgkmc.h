@@ -107,6 +107,13 @@ MGK_API int mgk_ls2d_solve_batch(mgk_ls2d_t plan, int nsel, const int* sel, cons
                                  double* const* sig_out, int max_iter, double tol, mgk_ls_info* infos,
                                  mgk_stream_t stream);
 
+/* Results of the last solve of replicas sel[0..nsel) (iterations, status,
+ * final diff, mean strain and stress) after a solve_batch call that passed
+ * infos = NULL: synchronises `stream` once.  Lets a scheduler launch the
+ * solves of several plans on their own streams before waiting on any.  No
+ * counterpart in the reference (its solves are synchronous). */
+MGK_API int mgk_ls2d_collect(mgk_ls2d_t plan, int nsel, const int* sel, mgk_ls_info* infos, mgk_stream_t stream);
+
 /* Timing hook: runs `reps` LS iterations (tolerance 0) and returns the mean
  * duration of the row kernel (C2R+update+tau+R2C along y) and of the column
  * kernel (FFT+Gamma+IFFT along x), timed with CUDA events on `stream`.

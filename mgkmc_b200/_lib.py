@@ -56,6 +56,7 @@ _SIGS = {
     "mgk_ls2d_create_batch": (c_int, [c_int, POINTER(c_int), POINTER(c_int), c_int, c_int, POINTER(c_void_p)]),
     "mgk_ls2d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
     "mgk_ls2d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
+    "mgk_ls2d_collect": (c_int, [_P, c_int, POINTER(c_int), POINTER(LsInfo), _P]),
     "mgk_ls2d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
                                      POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo), _P]),
     "mgk_ls2d_profile_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), c_int, c_int,

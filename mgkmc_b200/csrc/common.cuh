@@ -77,4 +77,8 @@ template <typename T> __device__ T block_sum(T v, T* red /* >= 32 entries */) {
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` (never lowers it: plans of different sizes share kernels).
+cudaError_t raise_smem(const void* fn, size_t bytes);
+
 }  // namespace mgk

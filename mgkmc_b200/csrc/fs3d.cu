@@ -632,14 +632,14 @@ extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* ou
   if (cudaMemset(p->fields, 0, sizeof(double) * N * (9 * 9 + 2)) != cudaSuccess ||
       cudaMemset(p->sc, 0, sizeof(FsScalars)) != cudaSuccess)
     return fail(MGK_CUDA_ERROR);
-  if (cudaFuncSetAttribute(fs_zfwd_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
-      cudaFuncSetAttribute(fs_zfwd_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
-      cudaFuncSetAttribute(fs_zfwd_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
-      cudaFuncSetAttribute(fs_zinv_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
-      cudaFuncSetAttribute(fs_zinv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zsmem) ||
-      cudaFuncSetAttribute(fs_ypass_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ysmem) ||
-      cudaFuncSetAttribute(fs_ypass_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ysmem) ||
-      cudaFuncSetAttribute(fs_xg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->xsmem)) {
+  if (raise_smem((const void*)fs_zfwd_kernel<0>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zfwd_kernel<1>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zfwd_kernel<2>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zinv_kernel<0>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zinv_kernel<1>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_ypass_kernel<-1>, (int)p->ysmem) ||
+      raise_smem((const void*)fs_ypass_kernel<1>, (int)p->ysmem) ||
+      raise_smem((const void*)fs_xg_kernel, (int)p->xsmem)) {
     set_error("mgk_fs3d_create: cudaFuncSetAttribute failed");
     return fail(MGK_CUDA_ERROR);
   }

@@ -784,7 +784,7 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
 // columns; the tile lands in shared memory through cp.async, then warp t runs
 // FFT, Gamma0_sym and inverse FFT on column t alone.
 constexpr int kRowWarps = 3;
-constexpr int kColTiles = 4;
+constexpr int kColTiles = 4;  // ky columns per column-kernel CTA (one warp each)
 
 __host__ __device__ constexpr int row_fast_smem(int ny, int csz, int tsz) {
   return ((3 * (csz == 16 ? ny + ny / 8 + 1 : ((ny + ny / 16 + 2) & ~1)) * csz + 127) / 128) * 128 + 16 * ny * tsz;
@@ -1026,7 +1026,7 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
 }
 
 template <typename T, int MAXN>
-__global__ void __launch_bounds__(32 * kColTiles) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
+__global__ void __launch_bounds__(32 * kColTiles, MAXN <= 256 ? 4 : 1) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
                                                                        const Ls2dState* __restrict__ st,
                                                                        const int* __restrict__ col_map,
                                                                        const int* __restrict__ col_local) {
@@ -1168,6 +1168,14 @@ struct mgk_ls2d_plan {
   cudaGraphExec_t exec = nullptr;
   int graph_mode = -1;  // -1 untried, 1 while-node graph, 0 host loop
   int graph_cap = 0;
+  // instantiated loop graphs by selection shape (a serving loop selects
+  // varying numbers of replicas; each shape is built once)
+  struct GraphEntry {
+    int rows, cols, nsel, cap;
+    cudaGraph_t g;
+    cudaGraphExec_t x;
+  };
+  std::vector<GraphEntry> gcache;
   // selection of the last call
   int nsel = 0, sel_rows = 0, sel_cols = 0;
   // persistent bulk-prefetch row kernels (0 when a replica has odd ny or the
@@ -1203,30 +1211,27 @@ template <typename T>
 static int ls2d_set_fast_attrs(int fast, size_t row_smem, size_t col_smem) {
   void* fns[4] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
                   row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast)};
-  for (void* f : fns) MGK_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(col_fast_fn<T>(fast), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col_smem));
+  for (void* f : fns) MGK_CUDA(raise_smem((const void*)f, (int)row_smem));
+  MGK_CUDA(raise_smem((const void*)col_fast_fn<T>(fast), (int)col_smem));
   return MGK_OK;
 }
 
 template <typename TS, typename TC>
 static int ls2d_set_attrs(size_t row_smem, size_t col_smem) {
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_row_kernel<TS, TC, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)row_smem));
-  MGK_CUDA(cudaFuncSetAttribute(ls2d_col_kernel<TS, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)col_smem));
+  MGK_CUDA(raise_smem((const void*)ls2d_row_kernel<TS, TC, true, true>, (int)row_smem));
+  MGK_CUDA(raise_smem((const void*)ls2d_row_kernel<TS, TC, false, true>, (int)row_smem));
+  MGK_CUDA(raise_smem((const void*)ls2d_row_kernel<TS, TC, true, false>, (int)row_smem));
+  MGK_CUDA(raise_smem((const void*)ls2d_row_kernel<TS, TC, false, false>, (int)row_smem));
+  MGK_CUDA(raise_smem((const void*)ls2d_col_kernel<TS, TC>, (int)col_smem));
   return MGK_OK;
 }
 
 extern "C" int mgk_ls2d_destroy(mgk_ls2d_t p) {
   if (!p) return MGK_OK;
-  if (p->exec) cudaGraphExecDestroy(p->exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
+  for (auto& e : p->gcache) {
+    cudaGraphExecDestroy(e.x);
+    cudaGraphDestroy(e.g);
+  }
   if (p->staged) cudaEventDestroy(p->staged);
   for (void* a : p->allocations) cudaFree(a);
   if (p->h_reps) cudaFreeHost(p->h_reps);
@@ -1356,15 +1361,12 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     if (ok && cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) {
       p->stage64 = st64; p->stage32 = st32; p->tma_smem64 = sm64; p->tma_smem32 = sm32;
-      bool good = cudaFuncSetAttribute(ls2d_row_tma_kernel<double, double, true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64) == cudaSuccess &&
+      bool good = raise_smem((const void*)ls2d_row_tma_kernel<double, double, true>, (int)sm64) == cudaSuccess &&
                   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->occ64, ls2d_row_tma_kernel<double, double, true>,
                                                                 kThreads, sm64) == cudaSuccess;
       if (good && mixed)
-        good = cudaFuncSetAttribute(ls2d_row_tma_kernel<float, float, false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32) == cudaSuccess &&
-               cudaFuncSetAttribute(ls2d_row_tma_kernel<float, float, true>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm32) == cudaSuccess &&
+        good = raise_smem((const void*)ls2d_row_tma_kernel<float, float, false>, (int)sm32) == cudaSuccess &&
+               raise_smem((const void*)ls2d_row_tma_kernel<float, float, true>, (int)sm32) == cudaSuccess &&
                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->occ32, ls2d_row_tma_kernel<float, float, false>,
                                                              kThreads, sm32) == cudaSuccess;
       p->tma = good && p->occ64 > 0 && (!mixed || p->occ32 > 0);
@@ -1577,8 +1579,6 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
 // rebuilt when the selection's shape or the iteration cap changes.
 static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_sel, int nsel, int G,
                        int guard_cap) {
-  if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
-  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
   cudaGraph_t g = nullptr;
   MGK_CUDA(cudaGraphCreate(&g, 0));
   int cap = guard_cap;
@@ -1633,9 +1633,50 @@ static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_
     cudaGetLastError();
     return rc;
   }
+  constexpr size_t kMaxGraphs = 48;
+  if (p->gcache.size() >= kMaxGraphs) {
+    cudaGraphExecDestroy(p->gcache.front().x);
+    cudaGraphDestroy(p->gcache.front().g);
+    p->gcache.erase(p->gcache.begin());
+  }
+  p->gcache.push_back({a64.rows, a64.cols, nsel, guard_cap, g, x});
   p->graph = g;
   p->exec = x;
   return MGK_OK;
+}
+
+// Copies the replicas' states to the host (one synchronisation of the
+// stream) and fills infos for the selection.
+static int ls2d_collect(mgk_ls2d_t p, int nsel, const int* selv, mgk_ls_info* infos, cudaStream_t s) {
+  MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls2dState) * p->nrep, cudaMemcpyDeviceToHost, s));
+  Ls2dCtl hc;
+  MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls2dCtl), cudaMemcpyDeviceToHost, s));
+  MGK_CUDA(cudaStreamSynchronize(s));
+  if (hc.error) {
+    set_error("mgk_ls2d_solve: a bulk copy wait gave up (device timeout)");
+    return MGK_TIMEOUT;
+  }
+  int worst = MGK_OK;
+  for (int q = 0; q < nsel; ++q) {
+    const Ls2dState& S = p->h_state[selv[q]];
+    infos[q].iterations = S.iter;
+    infos[q].status = S.status;
+    infos[q].final_diff = S.diff;
+    for (int k = 0; k < 4; ++k) { infos[q].eps_mean[k] = S.out_eps_mean[k]; infos[q].sig_mean[k] = S.out_sig_mean[k]; }
+    if (S.status == MGK_NONFINITE) worst = MGK_NONFINITE;
+  }
+  if (worst == MGK_NONFINITE) {
+    set_error("mgk_ls2d_solve: non-finite residual");
+    return MGK_NONFINITE;
+  }
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls2d_collect(mgk_ls2d_t p, int nsel, const int* sel, mgk_ls_info* infos, mgk_stream_t stream) {
+  MGK_REQUIRE(p && sel && infos && nsel >= 1 && nsel <= p->nrep, "mgk_ls2d_collect: bad argument");
+  for (int q = 0; q < nsel; ++q)
+    MGK_REQUIRE(sel[q] >= 0 && sel[q] < p->nrep, "mgk_ls2d_collect: replica %d out of range", sel[q]);
+  return ls2d_collect(p, nsel, sel, infos, (cudaStream_t)stream);
 }
 
 extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, const double* eps_bar,
@@ -1735,7 +1776,18 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     else launch_row<double, false, true>(a64, s);
     MGK_CUDA(cudaGetLastError());
     const int guard_cap = (max_iter + 2 > 1000 ? max_iter + 2 : 1000);
-    if (p->graph_mode == 1 && (changed || guard_cap > p->graph_cap)) p->graph_mode = -1;
+    if (p->graph_mode == 1 && (changed || guard_cap > p->graph_cap)) {
+      bool hit = false;
+      for (auto& e : p->gcache)
+        if (e.rows == rows && e.cols == cols && e.nsel == nsel && e.cap >= guard_cap) {
+          p->graph = e.g;
+          p->exec = e.x;
+          p->graph_cap = e.cap;
+          hit = true;
+          break;
+        }
+      if (!hit) p->graph_mode = -1;
+    }
     if (p->graph_mode < 0) {
       const char* env = getenv("MGK_NO_GRAPH_WHILE");
       if (env && env[0] == '1') p->graph_mode = 0;
@@ -1771,29 +1823,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 8,
                                                  (int)offsetof(Ls2dState, out_eps_mean), 0);
   MGK_CUDA(cudaGetLastError());
-  if (infos) {
-    MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls2dState) * p->nrep, cudaMemcpyDeviceToHost, s));
-    Ls2dCtl hc;
-    MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls2dCtl), cudaMemcpyDeviceToHost, s));
-    MGK_CUDA(cudaStreamSynchronize(s));
-    if (hc.error) {
-      set_error("mgk_ls2d_solve: a bulk copy wait gave up (device timeout)");
-      return MGK_TIMEOUT;
-    }
-    int worst = MGK_OK;
-    for (int q = 0; q < nsel; ++q) {
-      const Ls2dState& S = p->h_state[selv[q]];
-      infos[q].iterations = S.iter;
-      infos[q].status = S.status;
-      infos[q].final_diff = S.diff;
-      for (int k = 0; k < 4; ++k) { infos[q].eps_mean[k] = S.out_eps_mean[k]; infos[q].sig_mean[k] = S.out_sig_mean[k]; }
-      if (S.status == MGK_NONFINITE) worst = MGK_NONFINITE;
-    }
-    if (worst == MGK_NONFINITE) {
-      set_error("mgk_ls2d_solve: non-finite residual");
-      return MGK_NONFINITE;
-    }
-  }
+  if (infos) return ls2d_collect(p, nsel, selv.data(), infos, s);
   return MGK_OK;
 }
 

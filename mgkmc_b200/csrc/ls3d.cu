@@ -650,11 +650,11 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
     R.spec = reinterpret_cast<double2*>(sp);
   }
   int st;
-  if (cudaFuncSetAttribute(ls3d_zline_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zl_smem) ||
-      cudaFuncSetAttribute(ls3d_zline_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->zl_smem) ||
-      cudaFuncSetAttribute(ls3d_axis_kernel<1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ax_smem) ||
-      cudaFuncSetAttribute(ls3d_axis_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ax_smem) ||
-      cudaFuncSetAttribute(ls3d_axis_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->ax_smem)) {
+  if (raise_smem((const void*)ls3d_zline_kernel<true>, (int)p->zl_smem) ||
+      raise_smem((const void*)ls3d_zline_kernel<false>, (int)p->zl_smem) ||
+      raise_smem((const void*)ls3d_axis_kernel<1, -1>, (int)p->ax_smem) ||
+      raise_smem((const void*)ls3d_axis_kernel<1, 1>, (int)p->ax_smem) ||
+      raise_smem((const void*)ls3d_axis_kernel<0, 0>, (int)p->ax_smem)) {
     set_error("mgk_ls3d_create: cudaFuncSetAttribute failed");
     return fail(MGK_CUDA_ERROR);
   }

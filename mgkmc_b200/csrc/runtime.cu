@@ -22,6 +22,20 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 
+cudaError_t raise_smem(const void* fn, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<int, const void*>, size_t> set;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(m);
+  size_t& cur = set[{dev, fn}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
 bool fft_schedule(int n, FftLen* f) {
   if (n < 1 || n > 4096) return false;
   int m = n, a = 0, b = 0;

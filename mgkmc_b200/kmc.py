@@ -42,7 +42,7 @@ class Kmc2D:
     def __init__(self, E, nu, catalog, Q0, gamma0=0.1, T=300.0, nu0=1e13, strain_rate=1e7, step_size=1e-5,
                  q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0, stress_targets=None, mixed_tol=1e4,
                  mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200, q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0,
-                 selection="exact", ls_start="cold", precision="fp64"):
+                 selection="exact", ls_start="cold", precision="fp64", ls=None, rep=0, stream=None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("mgkmc_b200 needs a CUDA device (no CPU fallback)")
@@ -58,9 +58,14 @@ class Kmc2D:
         self.ls_start = ls_start
         self.tau = 1.0 / (nu0 * np.exp(-q_act_temp / (KB * T))) if T > 0 else np.inf
         f64 = torch.float64
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(d)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+
+        def t(a):
+            if isinstance(a, torch.Tensor):
+                return a.to(device=d, dtype=torch.float64).contiguous()
+            return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(d)
         self.E, self.nu = t(E), t(nu)
-        self.E_avg, self.nu_avg = float(np.mean(E)), float(np.mean(nu))
+        self.E_avg, self.nu_avg = float(self.E.mean()), float(self.nu.mean())
         self.catalog, self.Q0 = t(catalog), t(Q0)
         self.eps_p = torch.zeros((nx, ny, 2, 2), dtype=f64, device=d)
         self.soft = torch.zeros((nx, ny, 2), dtype=f64, device=d)
@@ -84,30 +89,45 @@ class Kmc2D:
         self.redraw = torch.zeros(5 * M, dtype=f64, device=d)
         self.work = torch.empty(max(int(L.lib().mgk_kmc_rates_work_bytes(n)), int(L.lib().mgk_kmc_scan_work_bytes(n))),
                                 dtype=torch.uint8, device=d)
-        self.ls = Ls2dBatch([(nx, ny)], precision=precision)
-        self.ls.set_material(0, self.E, self.nu, self.eps_p)
+        if ls is None:
+            self.ls, self.rep = Ls2dBatch([(nx, ny)], precision=precision), 0
+        else:
+            self.ls, self.rep = ls, int(rep)
+        self.ls.set_material(self.rep, self.E, self.nu, self.eps_p, stream=self.stream)
         self.eps_macro = np.zeros((2, 2))
         self.time = 0.0
         self.events = []
         self.n_solves = 0
-        self.stream = torch.cuda.current_stream()
 
     # ------------------------------------------------------------ stages ---
-    def elastic_run(self):
-        """LS solve with the current eigenstrain; returns the mean stress."""
+    def solve_args(self):
+        """(plan, replica, eps_bar, eps_out, sig_out, eps_init) of the next LS
+        solve with the current eigenstrain (the caller runs it on ``stream``)."""
         init = None
         if self.ls_start == "warm" and self.n_solves > 0:
-            self.eps_prev.copy_(self.eps)
-            init = [self.eps_prev]
-        info = self.ls.solve([0], [self.eps_macro], [self.eps], [self.sig], eps_init=init,
-                             max_iter=self.p["ls_max_iter"], tol=self.p["ls_tol"])[0]
+            with self.torch.cuda.stream(self.stream):
+                self.eps_prev.copy_(self.eps)
+            init = self.eps_prev
+        return self.ls, self.rep, self.eps_macro.copy(), self.eps, self.sig, init
+
+    def after_solve(self, info):
+        """Mean stress of a finished solve, with the reference's stability guard
+        (kmc_simulator.py:522-524)."""
         self.n_solves += 1
         sigM = np.array(info.sig_mean).reshape(2, 2)
         if not np.all(np.isfinite(sigM)) or np.max(np.abs(sigM)) / 1e9 > 20.0:
             raise ValueError(f"Unstable stress in small-strain elastic_run: {sigM / 1e9} GPa")
         return sigM
 
-    def barriers_and_rates(self):
+    def elastic_run(self):
+        """LS solve with the current eigenstrain; returns the mean stress."""
+        ls, rep, eb, eo, so, init = self.solve_args()
+        info = ls.solve([rep], [eb], [eo], [so], eps_init=None if init is None else [init],
+                        max_iter=self.p["ls_max_iter"], tol=self.p["ls_tol"], stream=self.stream)[0]
+        return self.after_solve(info)
+
+    def launch_rates(self):
+        """Enqueues barriers, rates and the copy of the total rate to the host."""
         lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
         L.check(lib.mgk_kmc2d_barrier(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0), L.ptr(self.sig),
                                       L.ptr(self.catalog), p["volume"], L.ptr(self.soft), L.ptr(self.t_last),
@@ -124,6 +144,10 @@ class Kmc2D:
             L.check(lib.mgk_kmc_prefix_fast(L.ptr(self.rates), n, L.ptr(self.prefix), L.ptr(self.count),
                                             L.ptr(self.total), L.ptr(self.work), S), "mgk_kmc_prefix_fast")
         self.total_h.copy_(self.total, non_blocking=True)
+
+    def barriers_and_rates(self):
+        """Barriers, rates and the total rate (one synchronisation)."""
+        self.launch_rates()
         self.stream.synchronize()
         return float(self.total_h[0])
 
@@ -141,13 +165,19 @@ class Kmc2D:
                                     L.ptr(self.t_last), L.ptr(self.catalog), L.ptr(self.Q0), L.ptr(self.prev), nc, nq,
                                     self.time, p["jp"], p["jt"], p["cap"], p["jn"], L.ptr(self.xym), S),
                 "mgk_kmc2d_event")
-        L.check(lib.mgk_ls2d_sync_voxel(self.ls._h, 0, L.ptr(self.eps_p), L.ptr(self.xym), S), "mgk_ls2d_sync_voxel")
+        L.check(lib.mgk_ls2d_sync_voxel(self.ls._h, self.rep, L.ptr(self.eps_p), L.ptr(self.xym), S),
+                "mgk_ls2d_sync_voxel")
         self.xym_h.copy_(self.xym, non_blocking=True)
 
     # ---------------------------------------------------------------- run ---
-    def run(self, rng, n_steps, max_events=None):
+    def trajectory(self, rng, n_steps, max_events=None):
+        """The trajectory as a generator of the host-visible results it needs:
+        it yields ("solve",) when the next LS solve (``solve_args``) must run and
+        be sent back as its LsInfo, and ("sync",) when the work enqueued on
+        ``stream`` must complete; it returns the result dict.  A scheduler can
+        advance many trajectories and batch their solves; ``run`` drives one."""
         p = self.p
-        self.elastic_run()
+        self.after_solve((yield ("solve",)))
         strain_unit = np.zeros((2, 2))
         strain_unit[0, 0] = 1.0
         dt_step = abs(p["step_size"]) / p["strain_rate"] if p["strain_rate"] > 0 else 1.0
@@ -157,7 +187,9 @@ class Kmc2D:
         while steps_done < n_steps:
             remaining += dt_step
             while remaining > 0:
-                total = self.barriers_and_rates()
+                self.launch_rates()
+                yield ("sync",)
+                total = float(self.total_h[0])
                 if total > 0:
                     u = rng.random()
                     t_wait = -np.log(u) / total
@@ -169,7 +201,7 @@ class Kmc2D:
                         theta = rng.uniform(0.0, np.pi, M)
                         q0 = np.clip(rng.normal(p["q_mean"], p["q_std"], M), p["q_min"], None)
                         self.event(u_sel, theta, q0)
-                        self.elastic_run()
+                        self.after_solve((yield ("solve",)))
                         x, y, m = (int(v) for v in self.xym_h.tolist())
                         self.events.append((x, y, m, self.time))
                         if max_events is not None and len(self.events) >= max_events:
@@ -180,7 +212,7 @@ class Kmc2D:
                 remaining = 0.0
             prev_e, prev_s = {}, {}
             for _ in range(p["mixed_max_iter"]):
-                sigM = self.elastic_run()
+                sigM = self.after_solve((yield ("solve",)))
                 err = np.zeros((2, 2))
                 err_max = 0.0
                 for idx, target in self.stress_targets.items():
@@ -204,6 +236,22 @@ class Kmc2D:
                     self.eps_macro[idx] += step
             steps_done += 1
         return self.result(steps_done)
+
+    def run(self, rng, n_steps, max_events=None):
+        gen = self.trajectory(rng, n_steps, max_events)
+        send = None
+        while True:
+            try:
+                need = gen.send(send)
+            except StopIteration as stop:
+                return stop.value
+            if need[0] == "solve":
+                ls, rep, eb, eo, so, init = self.solve_args()
+                send = ls.solve([rep], [eb], [eo], [so], eps_init=None if init is None else [init],
+                                max_iter=self.p["ls_max_iter"], tol=self.p["ls_tol"], stream=self.stream)[0]
+            else:
+                self.stream.synchronize()
+                send = None
 
     def result(self, steps):
         return dict(events=list(self.events), eps_macro=self.eps_macro.copy(), sig=self.sig.cpu().numpy(),

@@ -94,6 +94,16 @@ class Ls2dBatch:
         L.check(st, "mgk_ls2d_solve_batch", allow=(L.OK, L.NONFINITE))
         return list(infos) if sync else None
 
+    def collect(self, reps, stream=None):
+        """LsInfo of the last solve of ``reps`` after ``solve(..., sync=False)``
+        (one synchronisation of the stream)."""
+        n = len(reps)
+        sel = (ctypes.c_int * n)(*[int(r) for r in reps])
+        infos = (L.LsInfo * n)()
+        st = L.lib().mgk_ls2d_collect(self._h, n, sel, infos, L.stream_ptr(stream))
+        L.check(st, "mgk_ls2d_collect", allow=(L.OK, L.NONFINITE))
+        return list(infos)
+
     def profile_kernels(self, reps, eps_bars, fp32=False, n=50, stream=None):
         """Mean (row_ms, col_ms) of the two iteration kernels over the
         selection (CUDA events on the stream)."""

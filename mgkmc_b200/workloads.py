@@ -118,3 +118,86 @@ def fs3d_material(nx, ny, nz, rng, mu_mean=MU0, cv=0.1, K=K_BULK, fp_frac=0.02, 
     Fp[sel] += fp_amp * S
     Fp = Fp.reshape(nx, ny, nz, 3, 3)
     return E, nu, np.ascontiguousarray(np.moveaxis(Fp, (3, 4), (0, 1)))
+
+
+# ------------------------------------------------ device-side generators ---
+# The serving layer builds each request's inputs on the GPU from the
+# request's seed (torch's CUDA generator): same distributions as the numpy
+# generators above, different draws.  Host generation of a 1024^2 catalog
+# would take longer than its solves.
+
+def _gen(seed, device):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    return g
+
+
+def ls2d_problem_dev(nx, ny, seed, device, frac=0.05, gamma0=0.1, eps_xx=0.01, mu0=MU0, K=K_BULK, cv=0.1):
+    """(E, nu, eps_plastic, eps_bar) with E, nu (nx, ny) and eps_plastic
+    (nx, ny, 2, 2) float64 tensors on ``device``."""
+    import torch
+    g = _gen(seed, device)
+    f64 = torch.float64
+    mu = mu0 * (1.0 + cv * torch.randn((nx, ny), generator=g, device=device, dtype=f64))
+    mu = mu.clamp(0.7 * mu0, 1.3 * mu0)
+    E = 9.0 * K * mu / (3.0 * K + mu)
+    nu = (3.0 * K - 2.0 * mu) / (2.0 * (3.0 * K + mu))
+    N = nx * ny
+    nsel = int(round(frac * N))
+    sel = torch.randperm(N, generator=g, device=device)[:nsel]
+    theta = torch.rand(nsel, generator=g, device=device, dtype=f64) * np.pi
+    c, s = torch.cos(2 * theta), torch.sin(2 * theta)
+    ep = torch.zeros((N, 2, 2), dtype=f64, device=device)
+    ep[sel, 0, 0] = 0.5 * gamma0 * c
+    ep[sel, 1, 1] = -0.5 * gamma0 * c
+    ep[sel, 0, 1] = 0.5 * gamma0 * s
+    ep[sel, 1, 0] = 0.5 * gamma0 * s
+    eps_bar = np.zeros((2, 2))
+    eps_bar[0, 0] = eps_xx
+    return E, nu, ep.reshape(nx, ny, 2, 2), eps_bar
+
+
+def kmc2d_state_dev(nx, ny, M, seed, device, gamma0=0.1, q_mean=1.0, q_std=0.15, q_min=0.3):
+    """STZ catalog (nx, ny, M, 2, 2) and barriers Q0 (nx, ny, M) on ``device``."""
+    import torch
+    g = _gen(seed + 7919, device)
+    f64 = torch.float64
+    theta = torch.rand((nx, ny, M), generator=g, device=device, dtype=f64) * np.pi
+    c, s = torch.cos(2 * theta), torch.sin(2 * theta)
+    cat = torch.empty((nx, ny, M, 2, 2), dtype=f64, device=device)
+    cat[..., 0, 0] = 0.5 * gamma0 * c
+    cat[..., 1, 1] = -0.5 * gamma0 * c
+    cat[..., 0, 1] = 0.5 * gamma0 * s
+    cat[..., 1, 0] = 0.5 * gamma0 * s
+    Q0 = (q_mean + q_std * torch.randn((nx, ny, M), generator=g, device=device, dtype=f64)).clamp_min(q_min)
+    return cat, Q0
+
+
+def fs3d_material_dev(nx, ny, nz, seed, device, mu_mean=MU0, cv=0.1, K=K_BULK, fp_frac=0.02, fp_amp=0.05):
+    """(lam, mu) (nx, ny, nz) and tensor-first F_p (3, 3, nx, ny, nz) on ``device``."""
+    import torch
+    g = _gen(seed, device)
+    f64 = torch.float64
+    s2 = np.log(1.0 + cv * cv)
+    m = np.log(mu_mean) - 0.5 * s2
+    mu = torch.exp(m + np.sqrt(s2) * torch.randn((nx, ny, nz), generator=g, device=device, dtype=f64))
+    E = 9.0 * K * mu / (3.0 * K + mu)
+    nu = (3.0 * K - 2.0 * mu) / (2.0 * (3.0 * K + mu))
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu2 = E / (2 * (1 + nu))
+    N = nx * ny * nz
+    Fp = torch.zeros((N, 3, 3), dtype=f64, device=device)
+    Fp[:, 0, 0] = 1.0
+    Fp[:, 1, 1] = 1.0
+    Fp[:, 2, 2] = 1.0
+    nsel = int(round(fp_frac * N))
+    sel = torch.randperm(N, generator=g, device=device)[:nsel]
+    G = torch.randn((nsel, 3, 3), generator=g, device=device, dtype=f64)
+    S = 0.5 * (G + G.transpose(1, 2))
+    tr = S.diagonal(dim1=1, dim2=2).sum(-1)
+    S = S - tr[:, None, None] / 3.0 * torch.eye(3, dtype=f64, device=device)[None]
+    S = S / torch.sqrt((S * S).sum(dim=(1, 2)))[:, None, None]
+    Fp[sel] += fp_amp * S
+    Fp = Fp.reshape(nx, ny, nz, 3, 3).permute(3, 4, 0, 1, 2).contiguous()
+    return lam.contiguous(), mu2.contiguous(), Fp
