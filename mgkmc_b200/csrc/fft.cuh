@@ -219,7 +219,8 @@ __device__ __forceinline__ C* fft_any(C* a, C* b, int nlines, int ld, const FftL
 // memory in a padded layout (one slot of slack per 128 bytes, so the strided
 // stores of the early Stockham passes hit distinct banks).  Each pass reads
 // all of a lane's butterfly inputs into registers, synchronises the warp,
-// then writes the outputs in place: only __syncwarp() between passes, so
+// then writes the outputs in place: only the line's lanes synchronise between
+// passes (__syncwarp, or a named barrier for two-warp lines), so
 // warps of a CTA progress independently.
 namespace mgk {
 
@@ -231,30 +232,37 @@ template <typename C> constexpr int padded_len(int n) {
   return sizeof(C) == 16 ? n + n / 8 + 1 : ((n + n / 16 + 1 + 1) & ~1);
 }
 
-template <int N, int SIGN, int L, int P, int NS, typename C>
-__device__ __forceinline__ void warp_pass(C* a, int stride, const C* __restrict__ tw, int lane) {
+// Synchronises the G lanes that share a line: the warp (G = 32) or two
+// warps through named barrier `bid` (G = 64; ids 1.., 0 is __syncthreads).
+template <int G> __device__ __forceinline__ void grp_sync(int bid) {
+  if constexpr (G == 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(bid), "n"(G) : "memory");
+}
+
+template <int N, int SIGN, int L, int P, int NS, int G, typename C>
+__device__ __forceinline__ void warp_pass(C* a, int stride, const C* __restrict__ tw, int lane, int bid) {
   constexpr RadixList S = make_sched(N);
   if constexpr (P < S.np) {
     constexpr int R = S.r[P];
     constexpr int nb = N / R;
-    constexpr int U = (nb + 31) / 32;
+    constexpr int U = (nb + G - 1) / G;
     constexpr int tws = N / (NS * R);
     C v[L][U][R];
 #pragma unroll
     for (int l = 0; l < L; ++l)
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int j = lane + 32 * u;
-        if (nb % 32 == 0 || j < nb) {
+        const int j = lane + G * u;
+        if (nb % G == 0 || j < nb) {
 #pragma unroll
           for (int r = 0; r < R; ++r) v[l][u][r] = a[l * stride + pidx<C>(j + r * nb)];
         }
       }
-    __syncwarp();
+    grp_sync<G>(bid);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int j = lane + 32 * u;
-      if (nb % 32 == 0 || j < nb) {
+      const int j = lane + G * u;
+      if (nb % G == 0 || j < nb) {
         const int k = j % NS;
         C w[R];
         if constexpr (NS > 1) {
@@ -281,21 +289,22 @@ __device__ __forceinline__ void warp_pass(C* a, int stride, const C* __restrict_
         }
       }
     }
-    __syncwarp();
-    warp_pass<N, SIGN, L, P + 1, NS * R>(a, stride, tw, lane);
+    grp_sync<G>(bid);
+    warp_pass<N, SIGN, L, P + 1, NS * R, G>(a, stride, tw, lane, bid);
   }
 }
 
 // L lines at a, a + stride, ... (padded layout), transformed in place by the
-// calling warp.  tw: the W_N^m table of the line length.
-template <int N, int SIGN, int L, typename C>
-__device__ __forceinline__ void warp_fft(C* a, int stride, const C* __restrict__ tw, int lane) {
-  warp_pass<N, SIGN, L, 0, 1>(a, stride, tw, lane);
+// G lanes of the calling group (lane in [0, G)).  tw: the W_N^m table.
+template <int N, int SIGN, int L, int G = 32, typename C>
+__device__ __forceinline__ void warp_fft(C* a, int stride, const C* __restrict__ tw, int lane, int bid = 0) {
+  warp_pass<N, SIGN, L, 0, 1, G>(a, stride, tw, lane, bid);
 }
 
 // line lengths with a compiled warp-line FFT
 __host__ __device__ constexpr bool warp_fft_len(int n) {
-  return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512;
+  return n == 64 || n == 96 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512 || n == 768 ||
+         n == 1024;
 }
 
 // 16- or 8-byte asynchronous global -> shared copies (cp.async, completion

@@ -171,56 +171,150 @@ __global__ void rates_scatter_kernel(long long nvox, int M, const double* __rest
   indices[pos] = i;
 }
 
-// Sequential left-to-right running sum (the reference's total_rate chain).
-#define SEQ_CHUNK 2048
-__global__ void __launch_bounds__(256) seq_prefix_kernel(const double* __restrict__ rates, long long n_fixed,
-                                                         const long long* __restrict__ d_count,
-                                                         double* __restrict__ prefix, double* __restrict__ d_total) {
-  __shared__ double buf[3][SEQ_CHUNK];
+// Exact sequential running sum, computed in parallel (one CTA).
+//
+// The reference accumulates total_rate left to right in FP64
+// (kmc_simulator_functions.py:36-55), so every running sum carries the
+// rounding of all earlier additions.  Rates are >= 0, so the running sum s
+// only grows.  While s stays inside one binade [2^e, 2^(e+1)), every double
+// there is a multiple of u = 2^(e-52), and round-to-nearest of s + r is
+// s + rint(r/u)*u unless r/u sits exactly halfway between integers (a tie,
+// whose rounding depends on the parity of s).  So over a chunk of rates the
+// chain collapses to an exact int64 prefix sum of q_i = rint(r_i/u) added to
+// the mantissa integer M = s/u, valid up to the first element whose candidate
+// leaves the binade (M + Q >= 2^53) or is a tie; that element is added the
+// ordinary way (one __dadd_rn), which moves s to its new binade, and the next
+// chunk starts after it.  A zero, subnormal or non-finite s also takes single
+// ordinary adds.  The results are bit-identical to the sequential loop; the
+// number of ordinary adds is about the number of binades the sum crosses.
+constexpr int kExactThreads = 1024;
+constexpr int kExactPer = 8;  // rates per thread per chunk
+// q_i < 2^53, so sums of q are saturated at 2^61 (no int64 overflow); any
+// saturated sum is far above 2^53 - M and reads as leaving the binade
+constexpr long long kQCap = 1LL << 61;
+__device__ __forceinline__ long long qsat(long long a, long long b) { return min(a + b, kQCap); }
+
+__global__ void __launch_bounds__(kExactThreads) exact_prefix_kernel(const double* __restrict__ rates,
+                                                                    long long n_fixed,
+                                                                    const long long* __restrict__ d_count,
+                                                                    double* __restrict__ prefix,
+                                                                    double* __restrict__ d_total) {
+  constexpr int CH = kExactThreads * kExactPer;
+  __shared__ long long w_sum[32];
+  __shared__ long long w_fail[32];
+  __shared__ double s_s;
+  __shared__ long long s_p;
   const long long n = d_count ? *d_count : n_fixed;
-  const long long nchunk = (n + SEQ_CHUNK - 1) / SEQ_CHUNK;
-  const int tid = threadIdx.x;
-  const int helpers = blockDim.x - 32;  // warps 1.. load and store
-  double run = 0.0;
-  // preload chunk 0
-  for (int j = tid; j < SEQ_CHUNK; j += blockDim.x) buf[0][j] = j < n ? rates[j] : 0.0;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) { s_s = 0.0; s_p = 0; }
   __syncthreads();
-  for (long long c = 0; c <= nchunk; ++c) {
-    const int cur = (int)(c % 3), nxt = (int)((c + 1) % 3), prv = (int)((c + 2) % 3);
-    if (tid < 32) {
-      if (tid == 0 && c < nchunk) {
-        const long long base = c * SEQ_CHUNK;
-        const int len = (int)min((long long)SEQ_CHUNK, n - base);
-        double* b = buf[cur];
-        int j = 0;
-        for (; j + 8 <= len; j += 8) {
-          double v0 = b[j], v1 = b[j + 1], v2 = b[j + 2], v3 = b[j + 3];
-          double v4 = b[j + 4], v5 = b[j + 5], v6 = b[j + 6], v7 = b[j + 7];
-          run = add(run, v0); b[j] = run;
-          run = add(run, v1); b[j + 1] = run;
-          run = add(run, v2); b[j + 2] = run;
-          run = add(run, v3); b[j + 3] = run;
-          run = add(run, v4); b[j + 4] = run;
-          run = add(run, v5); b[j + 5] = run;
-          run = add(run, v6); b[j + 6] = run;
-          run = add(run, v7); b[j + 7] = run;
+  while (true) {
+    const double s = s_s;
+    const long long p = s_p;
+    if (p >= n) break;
+    if (!(s >= 2.2250738585072014e-308) || !(s < 1.0 / 0.0)) {
+      // zero, subnormal or non-finite running sum: one ordinary add
+      __syncthreads();
+      if (tid == 0) {
+        const double v = add(s, rates[p]);
+        prefix[p] = v;
+        s_s = v;
+        s_p = p + 1;
+      }
+      __syncthreads();
+      continue;
+    }
+    const long long bits = __double_as_longlong(s);
+    const int e = (int)((bits >> 52) & 0x7ff) - 1023;
+    const long long M = (bits & ((1LL << 52) - 1)) | (1LL << 52);
+    const double scale = ldexp(1.0, 52 - e);  // 1/u, exact power of two
+    const double u = ldexp(1.0, e - 52);
+    const long long base = p + (long long)tid * kExactPer;
+    long long q[kExactPer];
+    long long fail = LLONG_MAX;  // first tie or unrepresentable element of this thread
+    long long tot = 0;
+#pragma unroll
+    for (int k = 0; k < kExactPer; ++k) {
+      const long long i = base + k;
+      q[k] = 0;
+      if (i < n) {
+        const double x = rates[i] * scale;
+        if (!(x >= 0.0) || !(x < 9007199254740992.0) || x - floor(x) == 0.5) {
+          if (fail == LLONG_MAX) fail = i;
+        } else {
+          q[k] = (long long)rint(x);
         }
-        for (; j < len; ++j) { run = add(run, b[j]); b[j] = run; }
       }
-    } else {
-      const int h = tid - 32;
-      if (c + 1 < nchunk) {
-        const long long base = (c + 1) * SEQ_CHUNK;
-        for (int j = h; j < SEQ_CHUNK; j += helpers) buf[nxt][j] = (base + j < n) ? rates[base + j] : 0.0;
+      tot += q[k];
+    }
+    // exclusive block scan of the per-thread totals (int64, exact)
+    long long incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl = qsat(incl, t);
+    }
+    long long wf = fail;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wf = min(wf, __shfl_xor_sync(0xffffffffu, wf, o));
+    if (lane == 31) w_sum[wid] = incl;
+    if (lane == 0) w_fail[wid] = wf;
+    __syncthreads();
+    if (wid == 0) {
+      long long v = w_sum[lane];
+      long long f = w_fail[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = qsat(v, t);
       }
-      if (c >= 1) {
-        const long long base = (c - 1) * SEQ_CHUNK;
-        for (int j = h; j < SEQ_CHUNK && base + j < n; j += helpers) prefix[base + j] = buf[prv][j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
+      w_sum[lane] = v;  // inclusive warp totals
+      if (lane == 0) w_fail[0] = f;
+    }
+    __syncthreads();
+    // before this thread's first element (a saturated incl minus tot stays far above 2^53)
+    long long Q = qsat(wid > 0 ? w_sum[wid - 1] : 0, incl - tot);
+    long long first_bad = w_fail[0];
+    // first element whose candidate leaves the binade (Q is nondecreasing)
+    long long cross = LLONG_MAX;
+#pragma unroll
+    for (int k = 0; k < kExactPer; ++k) {
+      const long long i = base + k;
+      if (i < n && i < first_bad) {
+        Q = qsat(Q, q[k]);
+        if (M + Q >= (1LL << 53)) { cross = i; break; }
+        prefix[i] = (double)(M + Q) * u;
+      }
+    }
+    // the chunk is valid up to min(first tie, first crossing)
+    long long wc = cross;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wc = min(wc, __shfl_xor_sync(0xffffffffu, wc, o));
+    __syncthreads();  // everyone has read w_fail[0]
+    if (lane == 0) w_sum[wid] = wc;
+    __syncthreads();
+    if (tid == 0) {
+      long long stop = first_bad;
+      for (int w = 0; w < kExactThreads / 32; ++w) stop = min(stop, w_sum[w]);
+      const long long end = min(p + (long long)CH, n);
+      if (stop >= end) {
+        // whole chunk valid: the running sum is its last prefix
+        s_s = prefix[end - 1];
+        s_p = end;
+      } else {
+        // elements [p, stop) were written; stop is added the ordinary way
+        const double prev = stop > p ? prefix[stop - 1] : s;
+        const double v = add(prev, rates[stop]);
+        prefix[stop] = v;
+        s_s = v;
+        s_p = stop + 1;
       }
     }
     __syncthreads();
   }
-  if (tid == 0) *d_total = n > 0 ? run : 0.0;
+  if (tid == 0) *d_total = n > 0 ? s_s : 0.0;
 }
 
 // First i with prefix[i] >= u*total (two-level parallel search, one CTA).
@@ -447,7 +541,7 @@ static int kmc_rates_impl(long long nvox, int M, const double* Q, double volume,
     rates_full_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nvox, M, Q, vnu, T, Ts, rates, (long long*)indices,
                                                          (long long*)d_count);
     MGK_CUDA(cudaGetLastError());
-    seq_prefix_kernel<<<1, 256, 0, s>>>(rates, n, nullptr, prefix, d_total);
+    exact_prefix_kernel<<<1, kExactThreads, 0, s>>>(rates, n, nullptr, prefix, d_total);
     MGK_CUDA(cudaGetLastError());
   } else {
     MGK_REQUIRE(work != nullptr, "mgk_kmc2d_rates: cascade mode needs the work buffer");
@@ -459,7 +553,7 @@ static int kmc_rates_impl(long long nvox, int M, const double* Q, double volume,
     MGK_CUDA(cudaGetLastError());
     rates_scatter_kernel<<<nb, 256, 0, s>>>(nvox, M, Q, vnu, T, Ts, bcount, rates, (long long*)indices);
     MGK_CUDA(cudaGetLastError());
-    seq_prefix_kernel<<<1, 256, 0, s>>>(rates, 0, (const long long*)d_count, prefix, d_total);
+    exact_prefix_kernel<<<1, kExactThreads, 0, s>>>(rates, 0, (const long long*)d_count, prefix, d_total);
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
@@ -483,7 +577,7 @@ extern "C" int mgk_kmc_prefix(const double* rates, int64_t n, double* prefix, in
   cudaStream_t s = (cudaStream_t)stream;
   set_count_kernel<<<1, 1, 0, s>>>((long long*)d_count, (long long)n);
   MGK_CUDA(cudaGetLastError());
-  seq_prefix_kernel<<<1, 256, 0, s>>>(rates, n, nullptr, prefix, d_total);
+  exact_prefix_kernel<<<1, kExactThreads, 0, s>>>(rates, n, nullptr, prefix, d_total);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

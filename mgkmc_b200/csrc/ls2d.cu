@@ -785,15 +785,21 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
 // FFT, Gamma0_sym and inverse FFT on column t alone.
 constexpr int kRowWarps = 3;
 constexpr int kColTiles = 4;  // ky columns per column-kernel CTA (one warp each)
+// lanes per line and column tiles of a kernel variant (sides up to MAXN):
+// lines longer than 512 points take two warps
+__host__ __device__ constexpr int fast_group(int maxn) { return maxn > 512 ? 64 : 32; }
+__host__ __device__ constexpr int fast_col_tiles(int maxn) { return maxn > 512 ? 2 : kColTiles; }
+__host__ __device__ constexpr int row_threads(int maxn) { return 3 * fast_group(maxn); }
+__host__ __device__ constexpr int col_threads(int maxn) { return fast_col_tiles(maxn) * fast_group(maxn); }
 
 __host__ __device__ constexpr int row_fast_smem(int ny, int csz, int tsz) {
   return ((3 * (csz == 16 ? ny + ny / 8 + 1 : ((ny + ny / 16 + 2) & ~1)) * csz + 127) / 128) * 128 + 16 * ny * tsz;
 }
-__host__ __device__ constexpr int col_fast_smem(int nx, int csz) {
-  return 3 * kColTiles * (csz == 16 ? nx + nx / 8 + 1 : ((nx + nx / 16 + 2) & ~1)) * csz;
+__host__ __device__ constexpr int col_fast_smem(int nx, int csz, int tc) {
+  return 3 * tc * (csz == 16 ? nx + nx / 8 + 1 : ((nx + nx / 16 + 2) & ~1)) * csz;
 }
 
-template <typename T, int NY, bool IN_SPEC, bool FINAL>
+template <typename T, int NY, int G, bool IN_SPEC, bool FINAL>
 __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, int item, int r, int x0,
                                               double* partials,
                                               unsigned int* rep_counter, Ls2dCtl* ctl,
@@ -802,8 +808,9 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
   using C = C_t<T>;
   constexpr int PL = padded_len<C>(NY);
   constexpr int NYH = NY / 2 + 1;
-  constexpr int NT = 32 * kRowWarps;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NT = 3 * G;
+  const int warp = threadIdx.x / G, lane = threadIdx.x % G;  // line (component) and lane in it
+  const int bid = 1 + warp;
   const int nx = R.nx, ld = R.ld;
   const long long N = R.N;
   C* lines = reinterpret_cast<C*>(smem);
@@ -824,16 +831,16 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
   C* ra = spec + ((size_t)warp * nx + x0) * ld;
   C* rbp = ra + ld;
   if (IN_SPEC) {
-    constexpr int U = (NYH + 31) / 32;
+    constexpr int U = (NYH + G - 1) / G;
     C a[U], b[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int k = lane + 32 * u;
+      const int k = lane + G * u;
       if (k < NYH) { a[u] = ra[k]; b[u] = rbp[k]; }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int k = lane + 32 * u;
+      const int k = lane + G * u;
       if (k < NYH) {
         C av = a[u], bv = b[u];
         if (k == 0 || 2 * k == NY) { av.y = 0; bv.y = 0; }
@@ -841,8 +848,8 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
         if (k > 0 && 2 * k < NY) line[pidx<C>(NY - k)] = mk<C>(av.x + bv.y, bv.x - av.y);
       }
     }
-    __syncwarp();
-    warp_fft<NY, +1, 1>(line, PL, tw, lane);
+    grp_sync<G>(bid);
+    warp_fft<NY, +1, 1, G>(line, PL, tw, lane, bid);
   }
   const bool ok = mbar_wait(bar, 0);
   if (!__syncthreads_and(ok ? 1 : 0)) {
@@ -891,8 +898,8 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
     for (int c = 0; c < 3; ++c) lines[c * PL + py] = mk<C>(tr[0][c], tr[1][c]);
   }
   __syncthreads();
-  warp_fft<NY, -1, 1>(line, PL, tw, lane);
-  for (int k = lane; k < NYH; k += 32) {
+  warp_fft<NY, -1, 1, G>(line, PL, tw, lane, bid);
+  for (int k = lane; k < NYH; k += G) {
     const C zz = line[pidx<C>(k)];
     const C w = line[pidx<C>(k == 0 ? 0 : NY - k)];
     ra[k] = mk<C>(T(0.5) * (zz.x + w.x), T(0.5) * (zz.y - w.y));
@@ -915,7 +922,7 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
 }
 
 template <typename T, int MAXN, bool IN_SPEC, bool FINAL>
-__global__ void __launch_bounds__(32 * kRowWarps) ls2d_row_fast_kernel(
+__global__ void __launch_bounds__(row_threads(MAXN)) ls2d_row_fast_kernel(
     const Ls2dRep* __restrict__ reps, Ls2dState* st, const int* __restrict__ row_map,
     const int* __restrict__ row_local, double* partials, unsigned int* rep_counter, Ls2dCtl* ctl,
     cudaGraphConditionalHandle cond, int use_cond, int guard_cap) {
@@ -942,28 +949,30 @@ __global__ void __launch_bounds__(32 * kRowWarps) ls2d_row_fast_kernel(
   __syncthreads();
   const int x0 = 2 * row_local[item];
 #define MGK_ROW_CASE(n) \
-  case n: if constexpr (n <= MAXN) row_fast_body<T, n, IN_SPEC, FINAL>(R, S, item, r, x0, partials, rep_counter, ctl, cond, use_cond, guard_cap, \
+  case n: if constexpr (n <= MAXN) row_fast_body<T, n, fast_group(MAXN), IN_SPEC, FINAL>(R, S, item, r, x0, partials, rep_counter, ctl, cond, use_cond, guard_cap, \
                                               smem_raw, &bar, red, &s_last); break;
   switch (R.ny) {
     MGK_ROW_CASE(64) MGK_ROW_CASE(96) MGK_ROW_CASE(128) MGK_ROW_CASE(192) MGK_ROW_CASE(256) MGK_ROW_CASE(384)
-    MGK_ROW_CASE(512)
+    MGK_ROW_CASE(512) MGK_ROW_CASE(768) MGK_ROW_CASE(1024)
     default: break;
   }
 #undef MGK_ROW_CASE
 }
 
-template <typename T, int NX>
+template <typename T, int NX, int TC, int G>
 __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState& S, int ky0,
                                               unsigned char* smem) {
   using C = C_t<T>;
+  constexpr int kColTiles = TC;
   constexpr int PL = padded_len<C>(NX);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x / G, lane = threadIdx.x % G;  // column of the tile and lane in it
+  const int bid = 1 + warp;
   const int ny = R.ny, nyh = R.nyh, ld = R.ld;
   const int tcw = min(kColTiles, nyh - ky0);
   C* lines = reinterpret_cast<C*>(smem);  // line (c * kColTiles + t)
   C* spec = reinterpret_cast<C*>(R.spec);
   constexpr int TOT = 3 * NX * kColTiles;
-  for (int e = threadIdx.x; e < TOT; e += 32 * kColTiles) {
+  for (int e = threadIdx.x; e < TOT; e += G * kColTiles) {
     const int c = e / (NX * kColTiles);
     const int rem = e - c * NX * kColTiles;
     const int x = rem / kColTiles, t = rem - x * kColTiles;
@@ -976,15 +985,15 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
     const C* tw = reinterpret_cast<const C*>(Fields<T>::fx(R).tw);
     C* l0 = lines + t * PL;
     constexpr int LS = kColTiles * PL;  // stride between the components of a column
-    warp_fft<NX, -1, 1>(l0, LS, tw, lane);
-    warp_fft<NX, -1, 1>(l0 + LS, LS, tw, lane);
-    warp_fft<NX, -1, 1>(l0 + 2 * LS, LS, tw, lane);
+    warp_fft<NX, -1, 1, G>(l0, LS, tw, lane, bid);
+    warp_fft<NX, -1, 1, G>(l0 + LS, LS, tw, lane, bid);
+    warp_fft<NX, -1, 1, G>(l0 + 2 * LS, LS, tw, lane, bid);
     const T inv2mu0 = (T)S.inv2mu0, Bc = (T)S.Bc;
     const T sc = (T)(1.0 / ((double)NX * (double)ny));
     const int ky = ky0 + t;
     const double uy = (double)fftfreq(ky, ny) / ny;
     const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
-    for (int kx = lane; kx < NX; kx += 32) {
+    for (int kx = lane; kx < NX; kx += G) {
       const int pk = pidx<C>(kx);
       C* pxx = &l0[pk];
       C* pyy = &l0[LS + pk];
@@ -1011,13 +1020,13 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
       *pyy = mk<C>(eyy.x * sc, eyy.y * sc);
       *pxy = mk<C>(exy.x * sc, exy.y * sc);
     }
-    __syncwarp();
-    warp_fft<NX, +1, 1>(l0, LS, tw, lane);
-    warp_fft<NX, +1, 1>(l0 + LS, LS, tw, lane);
-    warp_fft<NX, +1, 1>(l0 + 2 * LS, LS, tw, lane);
+    grp_sync<G>(bid);
+    warp_fft<NX, +1, 1, G>(l0, LS, tw, lane, bid);
+    warp_fft<NX, +1, 1, G>(l0 + LS, LS, tw, lane, bid);
+    warp_fft<NX, +1, 1, G>(l0 + 2 * LS, LS, tw, lane, bid);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < TOT; e += 32 * kColTiles) {
+  for (int e = threadIdx.x; e < TOT; e += G * kColTiles) {
     const int c = e / (NX * kColTiles);
     const int rem = e - c * NX * kColTiles;
     const int x = rem / kColTiles, tt = rem - x * kColTiles;
@@ -1026,7 +1035,7 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
 }
 
 template <typename T, int MAXN>
-__global__ void __launch_bounds__(32 * kColTiles, MAXN <= 256 ? 4 : 1) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
+__global__ void __launch_bounds__(col_threads(MAXN), MAXN <= 256 ? 4 : 1) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
                                                                        const Ls2dState* __restrict__ st,
                                                                        const int* __restrict__ col_map,
                                                                        const int* __restrict__ col_local) {
@@ -1036,12 +1045,12 @@ __global__ void __launch_bounds__(32 * kColTiles, MAXN <= 256 ? 4 : 1) ls2d_col_
   const Ls2dRep& R = reps[r];
   const Ls2dState& S = st[r];
   if (S.done != 0) return;
-  const int ky0 = col_local[item] * kColTiles;
+  const int ky0 = col_local[item] * fast_col_tiles(MAXN);
 #define MGK_COL_CASE(n) \
-  case n: if constexpr (n <= MAXN) col_fast_body<T, n>(R, S, ky0, smem_raw); break;
+  case n: if constexpr (n <= MAXN) col_fast_body<T, n, fast_col_tiles(MAXN), fast_group(MAXN)>(R, S, ky0, smem_raw); break;
   switch (R.nx) {
     MGK_COL_CASE(64) MGK_COL_CASE(96) MGK_COL_CASE(128) MGK_COL_CASE(192) MGK_COL_CASE(256) MGK_COL_CASE(384)
-    MGK_COL_CASE(512)
+    MGK_COL_CASE(512) MGK_COL_CASE(768) MGK_COL_CASE(1024)
     default: break;
   }
 #undef MGK_COL_CASE
@@ -1199,12 +1208,15 @@ static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
 // warp-line kernel variants: sides up to 256, or up to 512 (more registers)
 template <typename TS, bool IN_SPEC, bool FINAL>
 static void* row_fast_fn(int fast) {
-  return fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL>
-                    : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL>;
+  return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL>
+         : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL>
+                      : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL>;
 }
 template <typename TS>
 static void* col_fast_fn(int fast) {
-  return fast > 256 ? (void*)ls2d_col_fast_kernel<TS, 512> : (void*)ls2d_col_fast_kernel<TS, 256>;
+  return fast > 512   ? (void*)ls2d_col_fast_kernel<TS, 1024>
+         : fast > 256 ? (void*)ls2d_col_fast_kernel<TS, 512>
+                      : (void*)ls2d_col_fast_kernel<TS, 256>;
 }
 
 template <typename T>
@@ -1278,7 +1290,7 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     }
     const char* env = getenv("MGK_FAST");
     if (env && env[0] == '0') fast = false;
-    p->fast = fast ? (side > 256 ? 512 : 256) : 0;
+    p->fast = fast ? (side > 512 ? 1024 : side > 256 ? 512 : 256) : 0;
   }
   size_t row_smem = 0, col_smem = 0, row_smem32 = 0, col_smem32 = 0;
   for (int r = 0; r < nrep; ++r) {
@@ -1287,7 +1299,7 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     memset(&R, 0, sizeof(R));
     R.nx = nx; R.ny = ny; R.nyh = ny / 2 + 1; R.ld = R.nyh;
     R.N = (long long)nx * ny;
-    R.tc = p->fast ? kColTiles : pick_tc(nx, c64, 64 * 1024);
+    R.tc = p->fast ? fast_col_tiles(p->fast) : pick_tc(nx, c64, 64 * 1024);
     R.row_items = nx / 2;
     R.col_items = (R.nyh + R.tc - 1) / R.tc;
     fft_schedule(nx, &R.fx64);
@@ -1304,9 +1316,9 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     }
     if (p->fast) {
       row_smem = std::max(row_smem, (size_t)row_fast_smem(ny, 16, 8));
-      col_smem = std::max(col_smem, (size_t)col_fast_smem(nx, 16));
+      col_smem = std::max(col_smem, (size_t)col_fast_smem(nx, 16, R.tc));
       row_smem32 = std::max(row_smem32, (size_t)row_fast_smem(ny, 8, 4));
-      col_smem32 = std::max(col_smem32, (size_t)col_fast_smem(nx, 8));
+      col_smem32 = std::max(col_smem32, (size_t)col_fast_smem(nx, 8, R.tc));
     } else {
       row_smem = std::max(row_smem, 2 * 3 * (size_t)ny * c64);
       col_smem = std::max(col_smem, 2 * 3 * (size_t)R.tc * nx * c64);
@@ -1492,25 +1504,28 @@ struct LoopArgs {
 
 template <typename TS, bool IN_SPEC, bool FINAL>
 static void launch_row(const LoopArgs& a, cudaStream_t s) {
-  if (a.fast > 256)
-    ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL><<<a.rows, 32 * kRowWarps, a.row_smem, s>>>(
-        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
-  else if (a.fast)
-    ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL><<<a.rows, 32 * kRowWarps, a.row_smem, s>>>(
-        a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
-  else
+  if (a.fast) {
+    void* fn = row_fast_fn<TS, IN_SPEC, FINAL>(a.fast);
+    cudaGraphConditionalHandle h = 0;
+    int zero = 0;
+    void* args[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.row_map, (void*)&a.row_local, (void*)&a.part,
+                    (void*)&a.repctr, (void*)&a.ctl, &h, &zero, &zero};
+    cudaLaunchKernel(fn, dim3(a.rows), dim3(row_threads(a.fast)), args, a.row_smem, s);
+  } else {
     ls2d_row_kernel<TS, TS, IN_SPEC, FINAL><<<a.rows, kThreads, a.row_smem, s>>>(
         a.reps, a.st, a.row_map, a.row_local, a.part, a.repctr, a.ctl, 0, 0, 0);
+  }
 }
 
 template <typename TS>
 static void launch_col(const LoopArgs& a, cudaStream_t s) {
-  if (a.fast > 256)
-    ls2d_col_fast_kernel<TS, 512><<<a.cols, 32 * kColTiles, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
-  else if (a.fast)
-    ls2d_col_fast_kernel<TS, 256><<<a.cols, 32 * kColTiles, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
-  else
+  if (a.fast) {
+    void* fn = col_fast_fn<TS>(a.fast);
+    void* args[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.col_map, (void*)&a.col_local};
+    cudaLaunchKernel(fn, dim3(a.cols), dim3(col_threads(a.fast)), args, a.col_smem, s);
+  } else {
     ls2d_col_kernel<TS, TS><<<a.cols, kThreads, a.col_smem, s>>>(a.reps, a.st, a.col_map, a.col_local);
+  }
 }
 
 template <typename TS, bool FINAL>
@@ -1546,7 +1561,7 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
   void* a1[] = {&a.reps, &a.st, &a.col_map, &a.col_local};
   k1.func = a.fast ? col_fast_fn<TS>(a.fast) : (void*)ls2d_col_kernel<TS, TS>;
   k1.gridDim = dim3(a.cols);
-  k1.blockDim = dim3(a.fast ? 32 * kColTiles : kThreads);
+  k1.blockDim = dim3(a.fast ? col_threads(a.fast) : kThreads);
   k1.sharedMemBytes = (unsigned)a.col_smem;
   k1.kernelParams = a1;
   cudaGraphNode_t n1, n2;
@@ -1568,7 +1583,7 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
     k2.gridDim = dim3(a.rows);
     k2.sharedMemBytes = (unsigned)a.row_smem;
     k2.kernelParams = a2;
-    k2.blockDim = dim3(a.fast ? 32 * kRowWarps : kThreads);
+    k2.blockDim = dim3(a.fast ? row_threads(a.fast) : kThreads);
   }
   MGK_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2));
   return MGK_OK;
@@ -1617,7 +1632,7 @@ static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_
       k3.func = a64.fast ? row_fast_fn<double, false, true>(a64.fast)
                          : (void*)ls2d_row_kernel<double, double, false, true>;
       k3.gridDim = dim3(a64.rows);
-      k3.blockDim = dim3(a64.fast ? 32 * kRowWarps : kThreads);
+      k3.blockDim = dim3(a64.fast ? row_threads(a64.fast) : kThreads);
       k3.sharedMemBytes = (unsigned)a64.row_smem;
       k3.kernelParams = ap3;
       rc = cudaGraphAddKernelNode(&n_row0, g, &n_ph2, 1, &k3) == cudaSuccess ? MGK_OK : MGK_CUDA_ERROR;

@@ -65,7 +65,11 @@ class Kmc2D:
                 return a.to(device=d, dtype=torch.float64).contiguous()
             return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(d)
         self.E, self.nu = t(E), t(nu)
-        self.E_avg, self.nu_avg = float(self.E.mean()), float(self.nu.mean())
+        # medium means for the mixed stress loop, copied without a
+        # synchronisation (first read after a solve has completed)
+        self._means_h = torch.empty(2, dtype=torch.float64).pin_memory()
+        with torch.cuda.stream(self.stream):
+            self._means_h.copy_(torch.stack([self.E.mean(), self.nu.mean()]), non_blocking=True)
         self.catalog, self.Q0 = t(catalog), t(Q0)
         self.eps_p = torch.zeros((nx, ny, 2, 2), dtype=f64, device=d)
         self.soft = torch.zeros((nx, ny, 2), dtype=f64, device=d)
@@ -98,6 +102,14 @@ class Kmc2D:
         self.time = 0.0
         self.events = []
         self.n_solves = 0
+
+    @property
+    def E_avg(self):
+        return float(self._means_h[0])
+
+    @property
+    def nu_avg(self):
+        return float(self._means_h[1])
 
     # ------------------------------------------------------------ stages ---
     def solve_args(self):

@@ -192,7 +192,11 @@ class Server:
         stress_mask = ~strain_mask
         target = np.zeros((2, 2))
         target[0, 0] = eb[0, 0]
-        E_avg, nu_avg = float(E.mean()), float(nu.mean())
+        # means for the macro update, copied without a synchronisation; read
+        # after the first solve has completed
+        means = torch.empty(2, dtype=torch.float64).pin_memory()
+        means.copy_(torch.stack([E.mean(), nu.mean()]), non_blocking=True)
+        E_avg = nu_avg = None
         eps_bar = np.zeros((2, 2))
         warm = False
         sigM = None
@@ -203,6 +207,8 @@ class Server:
             res.solves += 1
             res.ls_iterations += info.iterations
             sigM = np.array(info.sig_mean).reshape(2, 2)
+            if E_avg is None:
+                E_avg, nu_avg = float(means[0]), float(means[1])
             err = np.zeros((2, 2))
             err[stress_mask] = target[stress_mask] - sigM[stress_mask]
             if np.max(np.abs(err[stress_mask])) < self.macro_tol:
@@ -341,6 +347,25 @@ class Server:
                 self._finish(res, error=str(e))
 
     # ---------------------------------------------------------------- run ---
+    def prepare(self, requests):
+        """Creates the plans the requests will use and runs one solve on each,
+        so that plan set-up and graph instantiation happen before the first
+        arrival (a server is started before its traffic)."""
+        torch = self.torch
+        for n in sorted({r.n for r in requests if r.dim == 2}):
+            b = self._bucket(n)
+            with torch.cuda.stream(b.stream):
+                E, nu, ep, eb = W.ls2d_problem_dev(n, n, 0, self.dev)
+                eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=self.dev)
+                for k in range(min(4, len(b.free))):
+                    b.plan.set_material(k, E, nu, ep, stream=b.stream)
+                for k in range(1, min(4, len(b.free)) + 1):
+                    b.plan.solve(list(range(k)), [eb] * k, [eps] * k, [None] * k, max_iter=self.ls_max_iter,
+                                 tol=self.ls_tol, sync=True, stream=b.stream)
+        for n in sorted({r.n for r in requests if r.dim == 3}):
+            self._fs_plan(n)
+        torch.cuda.synchronize()
+
     def run(self, requests, realtime=True, keep_outputs=False):
         """Serve ``requests`` (arrival times relative to the start); returns
         the list of Results in request order."""

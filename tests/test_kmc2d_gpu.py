@@ -121,3 +121,50 @@ def test_kmc3d_golden():
     np.testing.assert_array_equal(ep, g["flip_out_eps_p"])
     np.testing.assert_array_equal(sp, g["flip_out_soft"])
     np.testing.assert_array_equal(tl, g["flip_out_tlast"])
+
+
+def _prefix_gpu(rates):
+    import torch
+    from mgkmc_b200 import _lib as L
+    n = rates.size
+    tr = torch.from_numpy(np.ascontiguousarray(rates, dtype=np.float64)).cuda()
+    prefix = torch.full((max(n, 1),), np.nan, dtype=torch.float64, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    tot = torch.zeros(1, dtype=torch.float64, device="cuda")
+    L.check(L.lib().mgk_kmc_prefix(L.ptr(tr), n, L.ptr(prefix), L.ptr(cnt), L.ptr(tot), L.stream_ptr()),
+            "mgk_kmc_prefix")
+    return prefix.cpu().numpy()[:n], float(tot.item())
+
+
+@pytest.mark.parametrize("case", ["kmc", "wild", "zeros_subnormal_huge", "ties", "all_ties", "empty", "one",
+                                  "large"])
+def test_exact_prefix_bit_for_bit(case):
+    # the parallel exact running sum against the sequential loop (np.cumsum
+    # adds left to right): every partial sum and the total, bit for bit
+    rng = np.random.default_rng(7)
+    if case == "kmc":
+        r = 1e13 * np.exp(-rng.normal(1.0, 0.15, 200_000) / 0.02585)
+    elif case == "wild":
+        r = np.exp(rng.uniform(-700, 700, 50_000))
+    elif case == "zeros_subnormal_huge":
+        r = rng.random(30_000)
+        r[::7] = 0.0
+        r[5] = 5e-324
+        r[1000] = 1e300
+    elif case == "ties":  # halfway cases whose rounding depends on the parity of the sum
+        r = np.full(40_000, 2.0 ** -53)
+        r[0] = 1.0
+        r[1::3] = 3 * 2.0 ** -53
+    elif case == "all_ties":
+        r = np.full(20_000, 1.5 * 2.0 ** -52)
+        r[0] = 1.0
+    elif case == "empty":
+        r = np.zeros(0)
+    elif case == "one":
+        r = np.array([0.37])
+    else:
+        r = 1e13 * np.exp(-rng.normal(1.0, 0.15, 8_388_608) / 0.02585)  # 1024^2 x 8 modes
+    p, tot = _prefix_gpu(r)
+    ref = np.cumsum(r)
+    assert np.array_equal(p.view(np.int64), ref.view(np.int64))
+    assert tot == (ref[-1] if r.size else 0.0)

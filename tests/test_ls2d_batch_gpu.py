@@ -32,9 +32,14 @@ def _problems(sizes, seed0=100):
     return [W.ls2d_problem(nx, ny, seed=seed0 + i) for i, (nx, ny) in enumerate(sizes)]
 
 
-def test_ragged_batch_matches_single_plans():
+@pytest.mark.parametrize("sizes", [SIZES, [(768, 64), (64, 64), (256, 128), (1024, 96)]])
+def test_ragged_batch_matches_single_plans(sizes):
+    # the second set runs every replica through the two-warp-line kernel
+    # variant (a side above 512 in the plan); single plans of the small ones
+    # use the one-warp variant: same arithmetic, same bits
     import torch
     from mgkmc_b200.linear_elastic_simulator import Ls2dBatch, Ls2dSolver
+    SIZES = sizes
     probs = _problems(SIZES)
     B = Ls2dBatch(SIZES)
     outs, sigs = [], []

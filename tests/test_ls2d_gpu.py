@@ -50,7 +50,8 @@ def test_golden_plane_stress_warm_asymmetric(les, golden):
     assert rel(sig, g["sig_conv"]) < TOL
 
 
-@pytest.mark.parametrize("nx,ny", [(256, 256), (96, 64), (192, 48), (12, 8), (384, 128), (6, 9), (2, 1), (18, 27)])
+@pytest.mark.parametrize("nx,ny", [(256, 256), (96, 64), (192, 48), (12, 8), (384, 128), (6, 9), (2, 1), (18, 27),
+                                   (1024, 768), (768, 64), (512, 1024)])
 def test_oracle_converged_sizes(les, nx, ny):
     E, nu, ep, eb = W.ls2d_problem(nx, ny, seed=nx * 7 + ny)
     o = OL.spectral_solver(E, nu, eb, ep, max_iter=300, tol=1e-10, return_info=True)
