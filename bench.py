@@ -12,6 +12,11 @@ problems, in three forms: plain FP64 (one solve after another), batched FP64
 FP64 finish; the headline value).  value = solves/s over all ranks (replicas
 only: each rank solves its own problems, no collective; scaling "weak").
 
+Serving block (N = 1, ``--serve-window`` seconds of the serving stream): the
+continuous-batching server in mixed precision against the plain FP64 form
+served one request at a time, both on this GPU with arrivals replayed in real
+time; solves/s and p50/p99 request latency of each, and their ratios.
+
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (oracle, numpy FFT) on the host cores, one process per core, on the same
 problems, and prints the same JSON line.
@@ -32,7 +37,8 @@ sys.path.insert(0, ROOT)
 
 NX = NY = 256
 TOL = 1e-8
-METRIC = "equilibrium solves/s (2D LS 256^2, update norm 1e-8, field err <= 1e-6 vs FP64)"
+METRIC = ("equilibrium solves/s (2D LS 256^2, update norm 1e-8, field err <= 1e-6 vs FP64); "
+          "serving block: served mixed precision vs plain FP64 sequential, solves/s and p50/p99 latency")
 
 
 def parse():
@@ -46,6 +52,9 @@ def parse():
     ap.add_argument("--grid", type=int, default=256, help="grid side (2^a 3^b); the headline workload is 256")
     ap.add_argument("--forms", default="plain_fp64,batched_fp64,batched_mixed",
                     help="comma list of forms to time (the headline is batched_mixed)")
+    ap.add_argument("--serve-window", type=float, default=0.1,
+                    help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
+                         "0 skips it")
     a = ap.parse_args()
     global NX, NY
     NX = NY = a.grid
@@ -153,6 +162,30 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------- serving -----
+def run_serving(window):
+    """The serving stream's first `window` seconds of arrivals, served by the
+    continuous-batching server (mixed precision) and by the plain FP64 form one
+    request at a time; arrivals replayed in real time."""
+    from mgkmc_b200.serving import Server, request_stream, summarize
+    reqs = [r for r in request_stream(rate=200.0, duration=60.0, seed=3) if r.t_arrival <= window]
+    out = {"workload": (f"serving stream (Poisson 200 req/s, seed 3; 60 % equilibrium solves, 40 % 100-event KMC "
+                        f"trajectories; 70 % 2D sides 64..1024, 30 % 3D finite-strain 64..128): the "
+                        f"{len(reqs)} arrivals of its first {window:g} s, replayed in real time"),
+           "requests": [[r.kind, r.dim, r.n] for r in reqs]}
+    for name, mode in (("served_mixed", "served"), ("plain_fp64_sequential", "sequential")):
+        srv = Server(mode=mode)
+        srv.prepare(reqs)
+        res = srv.run(reqs, realtime=True)
+        out[name] = summarize(res)
+    a, b = out["served_mixed"], out["plain_fp64_sequential"]
+    if a.get("completed") and b.get("completed"):
+        out["solves_per_s_ratio"] = a["solves_per_s"] / b["solves_per_s"]
+        out["p50_ratio"] = b["p50_s"] / a["p50_s"]
+        out["p99_ratio"] = b["p99_s"] / a["p99_s"]
+    return out
 
 
 # ------------------------------------------------------------- GPU leg -----
@@ -297,13 +330,22 @@ def run_ours(a):
     peak_kind = "measured" if os.path.exists(peaks_path) else "fallback"
     row_bytes = 136.0 * N * B
     achieved = row_bytes / (row64 * 1e-3) / 1e9
+    # DRAM read+write bytes of one launch of this kernel on this workload (32 x
+    # 256^2, FP64), from the ncu capture summarised in
+    # profiles/ls2d_warp_kernels_256x32_fp64.md; scaled by voxels for other
+    # batch sizes or grids (the traffic per voxel does not depend on them)
+    traffic = 242.4e6 * (N * B) / (32 * 256 * 256)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "ls2d_row_kernel<double,double,true,true> over the batch",
+            "traffic": traffic, "traffic_source": "ncu capture, profiles/ls2d_warp_kernels_256x32_fp64.md",
+            "kernel": "ls2d_row_fast_kernel<double,256,true,true> (C2R + update + tau + R2C along y) over the batch",
             "peak_kind": peak_kind, "bytes_per_launch": row_bytes,
             "kernels_us": {"row_fp64": row64 * 1e3, "col_fp64": col64 * 1e3, "row_fp32": row32 * 1e3,
                            "col_fp32": col32 * 1e3},
             "col_fp64_frac": 48.0 * N * B / (col64 * 1e-3) / 1e9 / peak,
             "row_fp32_frac": 68.0 * N * B / (row32 * 1e-3) / 1e9 / peak}
+    serving = None
+    if world == 1 and a.serve_window > 0:
+        serving = run_serving(a.serve_window)
     cpu = None
     if world == 1 and a.cpu_seconds > 0:
         v, nsol, wall = cpu_baseline(a.cpu_seconds, 1)
@@ -320,7 +362,8 @@ def run_ours(a):
                        "mixed_field_err_vs_fp64": err_mixed, "mixed_residual": residual},
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.Ls2dBatch"},
-            "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+            "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "serving": serving}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
