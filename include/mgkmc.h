@@ -202,6 +202,12 @@ MGK_API int mgk_fs3d_destroy(mgk_fs3d_t plan);
 /* lam, mu: device (nx,ny,nz) Lame fields (C4[0,0,1,1], C4[0,1,0,1] of the
  * reference's C4); Fp: device (3,3,nx,ny,nz) plastic deformation gradient or
  * NULL (no F_p: the reference's tangent branch without F_p). */
+/* Precision form of the Krylov matvecs: MGK_FP64 (default), or MGK_MIXED:
+ * the tangent product K:dF, the FFTs and the projection of the CG matvecs in
+ * FP32, while the Newton right-hand side (-G:P, -G:K:DbarF), the CG vectors x
+ * and r, every inner product and norm, the line search and the macro loop
+ * stay FP64.  No counterpart in the reference (FP64 only). */
+MGK_API int mgk_fs3d_set_precision(mgk_fs3d_t plan, int precision);
 MGK_API int mgk_fs3d_set_material(mgk_fs3d_t plan, const double* lam, const double* mu, const double* Fp,
                                   mgk_stream_t stream);
 /* Current deformation gradient (device, tensor-first); the plan keeps it. */

@@ -74,6 +74,7 @@ _SIGS = {
                                      POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo3), _P]),
     "mgk_fs3d_create": (c_int, [c_int, c_int, c_int, c_int, POINTER(c_void_p)]),
     "mgk_fs3d_destroy": (c_int, [_P]),
+    "mgk_fs3d_set_precision": (c_int, [_P, c_int]),
     "mgk_fs3d_set_material": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_fs3d_set_F": (c_int, [_P, _P, _P]),
     "mgk_fs3d_step": (c_int, [_P, POINTER(c_double), c_int, c_int, POINTER(c_double), POINTER(c_int), c_double,

@@ -42,6 +42,8 @@ struct FsScalars {
   double xx, FF, minJe, nan, pad;
   double sig[9];
   double meanF[9];
+  double tol2, kmax, kcount;  // device-side CG loop: (tol_CG)^2, iteration cap, iterations run
+  double pad2;
 };
 
 struct FsArgs {
@@ -63,34 +65,69 @@ struct FsArgs {
   double2* spec;
   double* part;
   FsScalars* sc;
+  // FP32 copies for the mixed form's Krylov matvecs
+  FftLen fx32, fy32, fz32;
+  const float* F32;
+  const float* Fpi32;
+  const float* mu32;
+  const float* lam32;
+  float* p32;
+  float* q32;
+};
+
+// the planes and FFT tables a matvec of precision T reads
+template <typename T> struct FsP;
+template <> struct FsP<double> {
+  static __device__ __forceinline__ const double* F(const FsArgs& a) { return a.F; }
+  static __device__ __forceinline__ const double* Fpi(const FsArgs& a) { return a.Fpi; }
+  static __device__ __forceinline__ const double* lam(const FsArgs& a) { return a.lam; }
+  static __device__ __forceinline__ const double* mu(const FsArgs& a) { return a.mu; }
+  static __device__ __forceinline__ double* p(const FsArgs& a) { return a.p; }
+  static __device__ __forceinline__ double* q(const FsArgs& a) { return a.q; }
+  static __device__ __forceinline__ double2* spec(const FsArgs& a) { return a.spec; }
+  static __device__ __forceinline__ const FftLen& fx(const FsArgs& a) { return a.fx; }
+  static __device__ __forceinline__ const FftLen& fy(const FsArgs& a) { return a.fy; }
+  static __device__ __forceinline__ const FftLen& fz(const FsArgs& a) { return a.fz; }
+};
+template <> struct FsP<float> {
+  static __device__ __forceinline__ const float* F(const FsArgs& a) { return a.F32; }
+  static __device__ __forceinline__ const float* Fpi(const FsArgs& a) { return a.Fpi32; }
+  static __device__ __forceinline__ const float* lam(const FsArgs& a) { return a.lam32; }
+  static __device__ __forceinline__ const float* mu(const FsArgs& a) { return a.mu32; }
+  static __device__ __forceinline__ float* p(const FsArgs& a) { return a.p32; }
+  static __device__ __forceinline__ float* q(const FsArgs& a) { return a.q32; }
+  static __device__ __forceinline__ float2* spec(const FsArgs& a) { return reinterpret_cast<float2*>(a.spec); }
+  static __device__ __forceinline__ const FftLen& fx(const FsArgs& a) { return a.fx32; }
+  static __device__ __forceinline__ const FftLen& fy(const FsArgs& a) { return a.fy32; }
+  static __device__ __forceinline__ const FftLen& fz(const FsArgs& a) { return a.fz32; }
 };
 
 // ------------------------------------------------------- 3x3 helpers ---
-__device__ __forceinline__ void mm(const double* A, const double* B, double* C) {
+template <typename T> __device__ __forceinline__ void mm(const T* A, const T* B, T* C) {
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
 }
-__device__ __forceinline__ void mtm(const double* A, const double* B, double* C) {  // A^T B
+template <typename T> __device__ __forceinline__ void mtm(const T* A, const T* B, T* C) {  // A^T B
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) C[3 * i + j] = A[i] * B[j] + A[3 + i] * B[3 + j] + A[6 + i] * B[6 + j];
 }
-__device__ __forceinline__ void mmt(const double* A, const double* B, double* C) {  // A B^T
+template <typename T> __device__ __forceinline__ void mmt(const T* A, const T* B, T* C) {  // A B^T
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j)
       C[3 * i + j] = A[3 * i] * B[3 * j] + A[3 * i + 1] * B[3 * j + 1] + A[3 * i + 2] * B[3 * j + 2];
 }
-__device__ __forceinline__ double det3(const double* A) {
+template <typename T> __device__ __forceinline__ T det3(const T* A) {
   return A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) + A[2] * (A[3] * A[7] - A[4] * A[6]);
 }
-__device__ __forceinline__ void inv3(const double* A, double* B) {
-  const double d = det3(A);
-  const double s = 1.0 / d;
+template <typename T> __device__ __forceinline__ void inv3(const T* A, T* B) {
+  const T d = det3(A);
+  const T s = T(1) / d;
   B[0] = (A[4] * A[8] - A[5] * A[7]) * s;
   B[1] = -(A[1] * A[8] - A[2] * A[7]) * s;
   B[2] = (A[1] * A[5] - A[2] * A[4]) * s;
@@ -102,75 +139,78 @@ __device__ __forceinline__ void inv3(const double* A, double* B) {
   B[8] = (A[0] * A[4] - A[1] * A[3]) * s;
 }
 
-// Per-voxel material state at F: Fe, S_ref, and what the tangent needs.
+// Per-voxel material state at F: Fe, S_ref, and what the tangent needs,
+// in arithmetic T (FP64, or FP32 for the mixed form's Krylov matvecs).
+template <typename T>
 struct VoxelLaw {
-  double Fe[9], Fpi[9], Sref[9], S[9], Ci[9];
-  double lam, mu, c, Je;
+  T Fe[9], Fpi[9], Sref[9], S[9], Ci[9];
+  T lam, mu, c, Je;
   int model, has_fp;
 
-  __device__ void init(const FsArgs& a, long long i, const double* F, double alpha, const double* dX) {
+  __device__ void init(const FsArgs& a, long long i, const T* F, T alpha, const T* dX) {
     model = a.model;
     has_fp = a.has_fp;
-    lam = a.lam[i];
-    mu = a.mu[i];
-    double Fv[9];
-    for (int q = 0; q < 9; ++q) Fv[q] = F[q] + (dX ? alpha * dX[q] : 0.0);
+    lam = FsP<T>::lam(a)[i];
+    mu = FsP<T>::mu(a)[i];
+    T Fv[9];
+    for (int q = 0; q < 9; ++q) Fv[q] = F[q] + (dX ? alpha * dX[q] : T(0));
     if (has_fp) {
-      for (int q = 0; q < 9; ++q) Fpi[q] = a.Fpi[q * a.N + i];
+      const T* fp = FsP<T>::Fpi(a);
+      for (int q = 0; q < 9; ++q) Fpi[q] = fp[q * a.N + i];
     } else {
-      for (int q = 0; q < 9; ++q) Fpi[q] = (q % 4 == 0) ? 1.0 : 0.0;
+      for (int q = 0; q < 9; ++q) Fpi[q] = (q % 4 == 0) ? T(1) : T(0);
     }
     mm(Fv, Fpi, Fe);
-    double C[9];
+    T C[9];
     mtm(Fe, Fe, C);
     Je = det3(Fe);
     if (model == 0) {
-      double Eg[9];
-      for (int q = 0; q < 9; ++q) Eg[q] = 0.5 * (C[q] - ((q % 4 == 0) ? 1.0 : 0.0));
-      const double tr = Eg[0] + Eg[4] + Eg[8];
-      for (int q = 0; q < 9; ++q) S[q] = 2 * mu * Eg[q] + ((q % 4 == 0) ? lam * tr : 0.0);
+      T Eg[9];
+      for (int q = 0; q < 9; ++q) Eg[q] = T(0.5) * (C[q] - ((q % 4 == 0) ? T(1) : T(0)));
+      const T tr = Eg[0] + Eg[4] + Eg[8];
+      for (int q = 0; q < 9; ++q) S[q] = 2 * mu * Eg[q] + ((q % 4 == 0) ? lam * tr : T(0));
     } else {
-      const double lnJ = log(fmax(1e-14, Je));
+      const T lnJ = log(fmax(T(1e-14), Je));
       inv3(C, Ci);
       c = mu - lam * lnJ;
-      const double k = lam * lnJ - mu;
-      for (int q = 0; q < 9; ++q) S[q] = k * Ci[q] + ((q % 4 == 0) ? mu : 0.0);
+      const T k = lam * lnJ - mu;
+      for (int q = 0; q < 9; ++q) S[q] = k * Ci[q] + ((q % 4 == 0) ? mu : T(0));
     }
-    double T[9];
-    mm(Fpi, S, T);
-    mmt(T, Fpi, Sref);
+    T Tm[9];
+    mm(Fpi, S, Tm);
+    mmt(Tm, Fpi, Sref);
   }
 
   // P = Fe S Fp^-T
-  __device__ void stress(double* P) const {
-    double T[9];
-    mm(Fe, S, T);
-    mmt(T, Fpi, P);
+  __device__ void stress(T* P) const {
+    T Tm[9];
+    mm(Fe, S, Tm);
+    mmt(Tm, Fpi, P);
   }
 
   // the reference's trans2(K4 : trans2(d))
-  __device__ void kdf(const double* d, double* out) const {
-    double X[9], T[9], Y[9];
-    mtm(Fe, d, T);
-    mm(T, Fpi, X);
+  __device__ void kdf(const T* d, T* out) const {
+    T X[9], Tm[9], Y[9];
+    mtm(Fe, d, Tm);
+    mm(Tm, Fpi, X);
     if (model == 0) {
-      const double tr = X[0] + X[4] + X[8];
+      const T tr = X[0] + X[4] + X[8];
       for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) Y[3 * i + j] = mu * (X[3 * i + j] + X[3 * j + i]) + (i == j ? lam * tr : 0.0);
+        for (int j = 0; j < 3; ++j) Y[3 * i + j] = mu * (X[3 * i + j] + X[3 * j + i]) + (i == j ? lam * tr : T(0));
     } else {
-      double CX[9], Xs[9], U[9];
+      T CX[9], Xs[9], U[9];
       mm(Ci, X, CX);
-      const double tr = CX[0] + CX[4] + CX[8];
+      const T tr = CX[0] + CX[4] + CX[8];
       for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) Xs[3 * i + j] = X[3 * i + j] + X[3 * j + i];
       mm(Ci, Xs, U);
       mm(U, Ci, Xs);
       for (int q = 0; q < 9; ++q) Y[q] = lam * tr * Ci[q] + c * Xs[q];
     }
-    double A[9], B[9];
+    T A[9], B[9];
     mmt(Sref, d, A);  // S_ref d^T
-    mm(Fpi, Y, T);
-    mmt(T, Fe, B);    // Fp^-1 Y Fe^T
+    mm(Fpi, Y, Tm);
+    mmt(Tm, Fe, B);   // Fp^-1 Y Fe^T
     if (has_fp) {
       for (int q = 0; q < 9; ++q) out[q] = A[q] + B[q];
     } else {
@@ -184,11 +224,12 @@ __device__ __forceinline__ int ffq(int k, int n) { return (k < (n + 1) / 2) ? k 
 
 // ----------------------------------------------------------- kernels ---
 
-// z-line forward: MODE 0 CG (p = r + beta p; A = K:p), 1 uniform (A = K:dbar),
-// 2 residual (A = P).  R2C along z of pairs of z-lines, 9 components.
-template <int MODE>
+// z-line forward: MODE 0 CG (p = r + beta p, or p = r when beta = 0; A = K:p),
+// 1 uniform (A = K:dbar), 2 residual (A = P).  R2C along z of pairs of
+// z-lines, 9 components, in precision T (MODEs 1 and 2 are FP64 only).
+template <int MODE, typename T>
 __global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __restrict__ dbar) {
-  using C = double2;
+  using C = C_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nz = a.nz, nzh = a.nzh, ld = a.ld;
   const long long N = a.N;
@@ -197,49 +238,53 @@ __global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + 9 * nz;
   const double beta = MODE == 0 ? a.sc->beta : 0.0;
+  T* pp = FsP<T>::p(a);
+  const T* Fp = FsP<T>::F(a);
   for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-    double out[2][9];
+    T out[2][9];
     for (int h = 0; h < 2; ++h) {
       const long long i = (l0 + h) * nz + z;
       if (MODE == 2) {
-        for (int q = 0; q < 9; ++q) out[h][q] = a.P[q * N + i];
+        for (int q = 0; q < 9; ++q) out[h][q] = (T)a.P[q * N + i];
       } else {
-        double d[9];
+        T d[9];
         if (MODE == 0) {
           for (int q = 0; q < 9; ++q) {
-            const double pn = a.r[q * N + i] + beta * a.p[q * N + i];
-            a.p[q * N + i] = pn;
+            const double rv = a.r[q * N + i];
+            const T pn = beta == 0.0 ? (T)rv : (T)(rv + beta * (double)pp[q * N + i]);
+            pp[q * N + i] = pn;
             d[q] = pn;
           }
         } else {
-          for (int q = 0; q < 9; ++q) d[q] = dbar[q];
+          for (int q = 0; q < 9; ++q) d[q] = (T)dbar[q];
         }
-        double F[9];
-        for (int q = 0; q < 9; ++q) F[q] = a.F[q * N + i];
-        VoxelLaw law;
-        law.init(a, i, F, 0.0, nullptr);
+        T F[9];
+        for (int q = 0; q < 9; ++q) F[q] = Fp[q * N + i];
+        VoxelLaw<T> law;
+        law.init(a, i, F, T(0), nullptr);
         law.kdf(d, out[h]);
       }
     }
-    for (int q = 0; q < 9; ++q) bufA[q * nz + z] = make_double2(out[0][q], out[1][q]);
+    for (int q = 0; q < 9; ++q) bufA[q * nz + z] = mk<C>(out[0][q], out[1][q]);
   }
   __syncthreads();
-  C* Z = fft_any<-1>(bufA, bufB, 9, nz, a.fz);
+  C* Z = fft_any<-1>(bufA, bufB, 9, nz, FsP<T>::fz(a));
+  C* spec = FsP<T>::spec(a);
   for (int e = threadIdx.x; e < 9 * nzh; e += blockDim.x) {
     const int c = e / nzh, k = e - c * nzh;
     const C z = Z[c * nz + k];
     const C w = Z[c * nz + (k == 0 ? 0 : nz - k)];
-    C* ra = a.spec + c * plane + l0 * ld;
-    ra[k] = make_double2(0.5 * (z.x + w.x), 0.5 * (z.y - w.y));
-    ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
+    C* ra = spec + c * plane + l0 * ld;
+    ra[k] = mk<C>(T(0.5) * (z.x + w.x), T(0.5) * (z.y - w.y));
+    ra[ld + k] = mk<C>(T(0.5) * (z.y + w.y), T(-0.5) * (z.x - w.x));
   }
 }
 
-// z-line inverse: C2R along z.  MODE 0: q = result, partial p.q.
-// MODE 1: r = -result (right-hand side), x = p = 0, partial r.r.
-template <int MODE>
+// z-line inverse: C2R along z.  MODE 0: q = result, partial p.q (FP64 sums).
+// MODE 1 (FP64): r = -result (right-hand side), x = 0, partial r.r.
+template <int MODE, typename T>
 __global__ void __launch_bounds__(256) fs_zinv_kernel(FsArgs a) {
-  using C = double2;
+  using C = C_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
   const int nz = a.nz, ld = a.ld;
@@ -248,37 +293,39 @@ __global__ void __launch_bounds__(256) fs_zinv_kernel(FsArgs a) {
   const long long plane = (long long)a.nx * a.ny * ld;
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + 9 * nz;
+  const C* spec = FsP<T>::spec(a);
   for (int e = threadIdx.x; e < 9 * nz; e += blockDim.x) {
     const int c = e / nz, k = e - c * nz;
     const int ks = (2 * k <= nz) ? k : nz - k;
-    const C* ra = a.spec + c * plane + l0 * ld;
+    const C* ra = spec + c * plane + l0 * ld;
     C av = ra[ks], bv = ra[ld + ks];
     C z;
     if (2 * k <= nz) {
       if (k == 0 || 2 * k == nz) { av.y = 0; bv.y = 0; }
-      z = make_double2(av.x - bv.y, av.y + bv.x);
+      z = mk<C>(av.x - bv.y, av.y + bv.x);
     } else {
-      z = make_double2(av.x + bv.y, bv.x - av.y);
+      z = mk<C>(av.x + bv.y, bv.x - av.y);
     }
     bufA[e] = z;
   }
   __syncthreads();
-  C* R = fft_any<+1>(bufA, bufB, 9, nz, a.fz);
+  C* R = fft_any<+1>(bufA, bufB, 9, nz, FsP<T>::fz(a));
+  T* qq = FsP<T>::q(a);
+  const T* pp = FsP<T>::p(a);
   double acc = 0;
   for (int e = threadIdx.x; e < 9 * nz; e += blockDim.x) {
     const int c = e / nz, z = e - c * nz;
     const C v = R[e];
     for (int h = 0; h < 2; ++h) {
       const long long i = (l0 + h) * nz + z;
-      const double val = h == 0 ? v.x : v.y;
+      const T val = h == 0 ? v.x : v.y;
       if (MODE == 0) {
-        a.q[c * N + i] = val;
-        acc += a.p[c * N + i] * val;
+        qq[c * N + i] = val;
+        acc += (double)pp[c * N + i] * (double)val;
       } else {
-        a.r[c * N + i] = -val;
+        a.r[c * N + i] = -(double)val;
         a.x[c * N + i] = 0.0;
-        a.p[c * N + i] = 0.0;
-        acc += val * val;
+        acc += (double)val * (double)val;
       }
     }
   }
@@ -287,9 +334,9 @@ __global__ void __launch_bounds__(256) fs_zinv_kernel(FsArgs a) {
 }
 
 // y-axis pass over tiles of tc kz columns (9 components)
-template <int SIGN>
+template <int SIGN, typename T>
 __global__ void __launch_bounds__(256) fs_ypass_kernel(FsArgs a) {
-  using C = double2;
+  using C = C_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = a.nx, ny = a.ny, nzh = a.nzh, ld = a.ld, tc = a.tc;
   const int ntile = (nzh + tc - 1) / tc;
@@ -300,22 +347,24 @@ __global__ void __launch_bounds__(256) fs_ypass_kernel(FsArgs a) {
   const long long obase = (long long)o * ny * ld;
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + 9 * tc * ny;
+  C* spec = FsP<T>::spec(a);
   const int tot = 9 * tcw * ny;
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * ny), rem = e - c * tcw * ny, j = rem / tcw, t = rem - j * tcw;
-    bufA[(c * tc + t) * ny + j] = a.spec[c * plane + obase + (long long)j * ld + k0 + t];
+    bufA[(c * tc + t) * ny + j] = spec[c * plane + obase + (long long)j * ld + k0 + t];
   }
   __syncthreads();
-  C* F = fft_any<SIGN>(bufA, bufB, 9 * tc, ny, a.fy);
+  C* F = fft_any<SIGN>(bufA, bufB, 9 * tc, ny, FsP<T>::fy(a));
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * ny), rem = e - c * tcw * ny, j = rem / tcw, t = rem - j * tcw;
-    a.spec[c * plane + obase + (long long)j * ld + k0 + t] = F[(c * tc + t) * ny + j];
+    spec[c * plane + obase + (long long)j * ld + k0 + t] = F[(c * tc + t) * ny + j];
   }
 }
 
 // x pass: FFT along x, G, IFFT along x (with the 1/N of the transform pair)
+template <typename T>
 __global__ void __launch_bounds__(256) fs_xg_kernel(FsArgs a) {
-  using C = double2;
+  using C = C_t<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = a.nx, ny = a.ny, nz = a.nz, nzh = a.nzh, ld = a.ld, tc = a.tc;
   const int ntile = (nzh + tc - 1) / tc;
@@ -327,14 +376,15 @@ __global__ void __launch_bounds__(256) fs_xg_kernel(FsArgs a) {
   const long long obase = (long long)o * ld;
   C* bufA = reinterpret_cast<C*>(smem_raw);
   C* bufB = bufA + 9 * tc * nx;
+  C* spec = FsP<T>::spec(a);
   const int tot = 9 * tcw * nx;
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * nx), rem = e - c * tcw * nx, j = rem / tcw, t = rem - j * tcw;
-    bufA[(c * tc + t) * nx + j] = a.spec[c * plane + obase + j * lstride + k0 + t];
+    bufA[(c * tc + t) * nx + j] = spec[c * plane + obase + j * lstride + k0 + t];
   }
   __syncthreads();
-  C* G = fft_any<-1>(bufA, bufB, 9 * tc, nx, a.fx);
-  const double scale = 1.0 / (double)a.N;
+  C* G = fft_any<-1>(bufA, bufB, 9 * tc, nx, FsP<T>::fx(a));
+  const T scale = (T)(1.0 / (double)a.N);
   const int ky = o;
   const double uy = (double)ffq(ky, ny) / ny;
   const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
@@ -343,38 +393,41 @@ __global__ void __launch_bounds__(256) fs_xg_kernel(FsArgs a) {
     const int kz = k0 + t;
     const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
     if ((kx == 0 && ky == 0 && kz == 0) || nqx || nqy || nqz) {
-      for (int c = 0; c < 9; ++c) G[(c * tc + t) * nx + kx] = make_double2(0.0, 0.0);
+      for (int c = 0; c < 9; ++c) G[(c * tc + t) * nx + kx] = mk<C>(T(0), T(0));
       continue;
     }
     const double ux = (double)ffq(kx, nx) / nx, uz = (double)ffq(kz, nz) / nz;
     const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
-    const double n[3] = {ux * inv, uy * inv, uz * inv};
+    const T n[3] = {(T)(ux * inv), (T)(uy * inv), (T)(uz * inv)};
     C A[9];
     for (int c = 0; c < 9; ++c) A[c] = G[(c * tc + t) * nx + kx];
     for (int i = 0; i < 3; ++i) {
-      double vx = 0, vy = 0;
+      T vx = 0, vy = 0;
       for (int l = 0; l < 3; ++l) { vx += A[3 * i + l].x * n[l]; vy += A[3 * i + l].y * n[l]; }
-      for (int j = 0; j < 3; ++j) G[((3 * i + j) * tc + t) * nx + kx] = make_double2(vx * n[j] * scale, vy * n[j] * scale);
+      for (int j = 0; j < 3; ++j) G[((3 * i + j) * tc + t) * nx + kx] = mk<C>(vx * n[j] * scale, vy * n[j] * scale);
     }
   }
   __syncthreads();
   C* H = (G == bufA) ? bufB : bufA;
-  C* Rz = fft_any<+1>(G, H, 9 * tc, nx, a.fx);
+  C* Rz = fft_any<+1>(G, H, 9 * tc, nx, FsP<T>::fx(a));
   for (int e = threadIdx.x; e < tot; e += blockDim.x) {
     const int c = e / (tcw * nx), rem = e - c * tcw * nx, j = rem / tcw, t = rem - j * tcw;
-    a.spec[c * plane + obase + j * lstride + k0 + t] = Rz[(c * tc + t) * nx + j];
+    spec[c * plane + obase + j * lstride + k0 + t] = Rz[(c * tc + t) * nx + j];
   }
 }
 
-// CG update: x += alpha p; r -= alpha q; partial r.r
+// CG update: x += alpha p; r -= alpha q (p, q in the matvec precision); partial r.r
+template <typename T>
 __global__ void fs_update_kernel(FsArgs a) {
   __shared__ double red[32];
   const double alpha = a.sc->alpha;
   const long long n9 = 9 * a.N;
+  const T* pp = FsP<T>::p(a);
+  const T* qq = FsP<T>::q(a);
   double acc = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9; i += (long long)gridDim.x * blockDim.x) {
-    a.x[i] += alpha * a.p[i];
-    const double rn = a.r[i] - alpha * a.q[i];
+    a.x[i] += alpha * (double)pp[i];
+    const double rn = a.r[i] - alpha * (double)qq[i];
     a.r[i] = rn;
     acc += rn * rn;
   }
@@ -382,10 +435,13 @@ __global__ void fs_update_kernel(FsArgs a) {
   if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
 }
 
-// fixed-order sum of nb partials; MODE 0: pq -> alpha; 1: r.r -> beta, rr;
-// 2: right-hand side -> rr = bb, beta = 0
+// fixed-order sum of nb partials; MODE 0: pq -> alpha; 1: r.r -> beta, rr,
+// one more Krylov iteration counted; 2: right-hand side -> rr = bb, beta = 0,
+// iteration count reset.  MODEs 1 and 2 decide, when use_cond, whether the
+// device-side Krylov loop runs another iteration: rr > tol^2 bb, finite, and
+// below the iteration cap.
 template <int MODE>
-__global__ void fs_scalar_kernel(FsArgs a, int nb) {
+__global__ void fs_scalar_kernel(FsArgs a, int nb, cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ double red[32];
   double s = 0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) s += a.part[i];
@@ -398,10 +454,16 @@ __global__ void fs_scalar_kernel(FsArgs a, int nb) {
   } else if (MODE == 1) {
     S.beta = (S.rr != 0.0) ? s / S.rr : 0.0;
     S.rr = s;
+    S.kcount += 1.0;
   } else {
     S.rr = s;
     S.bb = s;
     S.beta = 0.0;
+    S.kcount = 0.0;
+  }
+  if (MODE != 0 && use_cond) {
+    const bool go = isfinite(S.rr) && S.rr > S.tol2 * S.bb && S.kcount < S.kmax;
+    cudaGraphSetConditional(cond, go ? 1u : 0u);
   }
 }
 
@@ -421,7 +483,7 @@ __global__ void fs_constitutive_kernel(FsArgs a, double alpha, const double* __r
       dX[q] = xv + (dbar ? dbar[q] : 0.0);
       xx += xv * xv;
     }
-    VoxelLaw law;
+    VoxelLaw<double> law;
     law.init(a, i, F, alpha, dX);
     double Ft[9], P[9];
     for (int q = 0; q < 9; ++q) Ft[q] = F[q] + alpha * dX[q];
@@ -517,6 +579,12 @@ __global__ void fs_cauchy_kernel(const double* __restrict__ P, const double* __r
   }
 }
 
+// FP32 copies of n doubles (the mixed form's matvec inputs)
+__global__ void fs_to_f32_kernel(long long n, const double* __restrict__ src, float* __restrict__ dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
 // material: lam, mu planes and Fp^-1 (plain inverse of F_p, as _invert_Fp_3d)
 __global__ void fs_material_kernel(long long N, const double* __restrict__ lam_in, const double* __restrict__ mu_in,
                                    const double* __restrict__ Fp, double* lam, double* mu, double* Fpi) {
@@ -564,6 +632,15 @@ struct mgk_fs3d_plan {
   size_t zsmem = 0, ysmem = 0, xsmem = 0;
   int nblk = 0;
   int stat_newton = 0, stat_krylov = 0, stat_macro = 0;
+  // precision form: MGK_FP64, or MGK_MIXED (FP32 Krylov matvecs)
+  int prec = MGK_FP64;
+  float* f32 = nullptr;  // F32, Fpi32, lam32, mu32, p32, q32
+  float *F32 = nullptr, *Fpi32 = nullptr, *lam32 = nullptr, *mu32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+  FftLen fx32, fy32, fz32;
+  // device-side Krylov loop graphs, one per matvec precision (0 FP64, 1 FP32)
+  cudaGraph_t cg_graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t cg_exec[2] = {nullptr, nullptr};
+  int graph_mode = -1;  // -1 untried, 1 graphs, 0 host-driven loop
 };
 
 static FsArgs fs_args(mgk_fs3d_t p) {
@@ -575,11 +652,18 @@ static FsArgs fs_args(mgk_fs3d_t p) {
   a.F = p->F; a.Fpi = p->Fpi; a.mu = p->mu; a.lam = p->lam; a.P = p->P;
   a.x = p->x; a.r = p->r; a.p = p->p; a.q = p->q; a.Fout = p->Ftr; a.Pout = p->Ptr;
   a.spec = p->spec; a.part = p->part; a.sc = p->sc;
+  a.fx32 = p->fx32; a.fy32 = p->fy32; a.fz32 = p->fz32;
+  a.F32 = p->F32; a.Fpi32 = p->Fpi32; a.mu32 = p->mu32; a.lam32 = p->lam32; a.p32 = p->p32; a.q32 = p->q32;
   return a;
 }
 
 extern "C" int mgk_fs3d_destroy(mgk_fs3d_t p) {
   if (!p) return MGK_OK;
+  for (int k = 0; k < 2; ++k) {
+    if (p->cg_exec[k]) cudaGraphExecDestroy(p->cg_exec[k]);
+    if (p->cg_graph[k]) cudaGraphDestroy(p->cg_graph[k]);
+  }
+  cudaFree(p->f32);
   cudaFree(p->fields);
   cudaFree(p->spec);
   cudaFree(p->part);
@@ -632,18 +716,74 @@ extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* ou
   if (cudaMemset(p->fields, 0, sizeof(double) * N * (9 * 9 + 2)) != cudaSuccess ||
       cudaMemset(p->sc, 0, sizeof(FsScalars)) != cudaSuccess)
     return fail(MGK_CUDA_ERROR);
-  if (raise_smem((const void*)fs_zfwd_kernel<0>, (int)p->zsmem) ||
-      raise_smem((const void*)fs_zfwd_kernel<1>, (int)p->zsmem) ||
-      raise_smem((const void*)fs_zfwd_kernel<2>, (int)p->zsmem) ||
-      raise_smem((const void*)fs_zinv_kernel<0>, (int)p->zsmem) ||
-      raise_smem((const void*)fs_zinv_kernel<1>, (int)p->zsmem) ||
-      raise_smem((const void*)fs_ypass_kernel<-1>, (int)p->ysmem) ||
-      raise_smem((const void*)fs_ypass_kernel<1>, (int)p->ysmem) ||
-      raise_smem((const void*)fs_xg_kernel, (int)p->xsmem)) {
+  if (raise_smem((const void*)fs_zfwd_kernel<0, double>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zfwd_kernel<1, double>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zfwd_kernel<2, double>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zinv_kernel<0, double>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_zinv_kernel<1, double>, (int)p->zsmem) ||
+      raise_smem((const void*)fs_ypass_kernel<-1, double>, (int)p->ysmem) ||
+      raise_smem((const void*)fs_ypass_kernel<1, double>, (int)p->ysmem) ||
+      raise_smem((const void*)fs_xg_kernel<double>, (int)p->xsmem) ||
+      raise_smem((const void*)fs_zfwd_kernel<0, float>, (int)p->zsmem / 2) ||
+      raise_smem((const void*)fs_zinv_kernel<0, float>, (int)p->zsmem / 2) ||
+      raise_smem((const void*)fs_ypass_kernel<-1, float>, (int)p->ysmem / 2) ||
+      raise_smem((const void*)fs_ypass_kernel<1, float>, (int)p->ysmem / 2) ||
+      raise_smem((const void*)fs_xg_kernel<float>, (int)p->xsmem / 2)) {
     set_error("mgk_fs3d_create: cudaFuncSetAttribute failed");
     return fail(MGK_CUDA_ERROR);
   }
   *out = p;
+  return MGK_OK;
+}
+
+static void fs_drop_graphs(mgk_fs3d_t p) {
+  for (int k = 0; k < 2; ++k) {
+    if (p->cg_exec[k]) cudaGraphExecDestroy(p->cg_exec[k]);
+    if (p->cg_graph[k]) cudaGraphDestroy(p->cg_graph[k]);
+    p->cg_exec[k] = nullptr;
+    p->cg_graph[k] = nullptr;
+  }
+}
+
+// FP32 copies of F, F_p^-1 and the moduli for the mixed form's matvecs
+static int fs_refresh_f32(mgk_fs3d_t p, bool material, cudaStream_t s) {
+  if (p->prec != MGK_MIXED) return MGK_OK;
+  const long long N = p->N;
+  fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(9 * N, p->F, p->F32);
+  if (material) {
+    if (p->has_fp) fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(9 * N, p->Fpi, p->Fpi32);
+    fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(N, p->lam, p->lam32);
+    fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(N, p->mu, p->mu32);
+  }
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_set_precision(mgk_fs3d_t p, int precision) {
+  MGK_REQUIRE(p, "mgk_fs3d_set_precision: null plan");
+  MGK_REQUIRE(precision == MGK_FP64 || precision == MGK_MIXED, "mgk_fs3d_set_precision: bad precision");
+  if (precision == MGK_MIXED && !p->f32) {
+    const long long N = p->N;
+    if (cudaMalloc(&p->f32, sizeof(float) * N * (9 + 9 + 2 + 9 + 9)) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("mgk_fs3d_set_precision: cudaMalloc of the FP32 planes failed");
+      return MGK_OOM;
+    }
+    float* f = p->f32;
+    p->F32 = f; p->Fpi32 = f + 9 * N; p->lam32 = f + 18 * N; p->mu32 = f + 19 * N; p->p32 = f + 20 * N;
+    p->q32 = f + 29 * N;
+    p->fx32 = p->fx; p->fy32 = p->fy; p->fz32 = p->fz;
+    p->fx32.tw = twiddles(p->nx, 1); p->fy32.tw = twiddles(p->ny, 1); p->fz32.tw = twiddles(p->nz, 1);
+    if (!p->fx32.tw || !p->fy32.tw || !p->fz32.tw) return MGK_OOM;
+  }
+  if (precision != p->prec) fs_drop_graphs(p);  // the graphs capture the plane set
+  p->prec = precision;
+  if (precision == MGK_MIXED && p->has_material) {
+    MGK_CUDA(cudaDeviceSynchronize());
+    int rc = fs_refresh_f32(p, true, 0);
+    if (rc) return rc;
+    MGK_CUDA(cudaDeviceSynchronize());
+  }
   return MGK_OK;
 }
 
@@ -653,9 +793,10 @@ extern "C" int mgk_fs3d_set_material(mgk_fs3d_t p, const double* lam, const doub
   cudaStream_t s = (cudaStream_t)stream;
   fs_material_kernel<<<p->nblk, 256, 0, s>>>(p->N, lam, mu, Fp, p->lam, p->mu, p->Fpi);
   MGK_CUDA(cudaGetLastError());
+  if ((Fp ? 1 : 0) != p->has_fp) fs_drop_graphs(p);  // the graphs capture has_fp
   p->has_fp = Fp ? 1 : 0;
   p->has_material = 1;
-  return MGK_OK;
+  return fs_refresh_f32(p, true, s);
 }
 
 extern "C" int mgk_fs3d_set_F(mgk_fs3d_t p, const double* F, mgk_stream_t stream) {
@@ -676,19 +817,21 @@ extern "C" int mgk_fs3d_get(mgk_fs3d_t p, double* F_out, double* P_out, double* 
   return MGK_OK;
 }
 
-// one matvec / projection: zfwd<MODE> -> y -> xG -> y^-1 -> zinv<ZMODE>
+// one matvec / projection in precision T: zfwd<MODE> -> y -> xG -> y^-1 -> zinv<ZMODE>
+template <typename T>
 static int fs_project(mgk_fs3d_t p, int mode, int zmode, cudaStream_t s) {
   FsArgs a = fs_args(p);
   const int zl = (int)(p->N / p->nz / 2);
   const int ntile = (p->nzh + p->tc - 1) / p->tc;
-  if (mode == 0) fs_zfwd_kernel<0><<<zl, 256, p->zsmem, s>>>(a, p->dbar);
-  else if (mode == 1) fs_zfwd_kernel<1><<<zl, 256, p->zsmem, s>>>(a, p->dbar);
-  else fs_zfwd_kernel<2><<<zl, 256, p->zsmem, s>>>(a, p->dbar);
-  fs_ypass_kernel<-1><<<p->nx * ntile, 256, p->ysmem, s>>>(a);
-  fs_xg_kernel<<<p->ny * ntile, 256, p->xsmem, s>>>(a);
-  fs_ypass_kernel<1><<<p->nx * ntile, 256, p->ysmem, s>>>(a);
-  if (zmode == 0) fs_zinv_kernel<0><<<zl, 256, p->zsmem, s>>>(a);
-  else fs_zinv_kernel<1><<<zl, 256, p->zsmem, s>>>(a);
+  const size_t zs = p->zsmem * sizeof(T) / 8, ys = p->ysmem * sizeof(T) / 8, xs = p->xsmem * sizeof(T) / 8;
+  if (mode == 0) fs_zfwd_kernel<0, T><<<zl, 256, zs, s>>>(a, p->dbar);
+  else if (mode == 1) fs_zfwd_kernel<1, double><<<zl, 256, zs, s>>>(a, p->dbar);
+  else fs_zfwd_kernel<2, double><<<zl, 256, zs, s>>>(a, p->dbar);
+  fs_ypass_kernel<-1, T><<<p->nx * ntile, 256, ys, s>>>(a);
+  fs_xg_kernel<T><<<p->ny * ntile, 256, xs, s>>>(a);
+  fs_ypass_kernel<1, T><<<p->nx * ntile, 256, ys, s>>>(a);
+  if (zmode == 0) fs_zinv_kernel<0, T><<<zl, 256, zs, s>>>(a);
+  else fs_zinv_kernel<1, double><<<zl, 256, zs, s>>>(a);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }
@@ -708,9 +851,124 @@ static int fs_trial(mgk_fs3d_t p, double alpha, bool use_dbar, bool use_x, cudaS
   return fs_read_scalars(p, s);
 }
 
-static void fs_accept(mgk_fs3d_t p) {
-  std::swap(p->F, p->Ftr);
-  std::swap(p->P, p->Ptr);
+// accept the trial state: copies (the plane addresses stay fixed, so the
+// Krylov graphs stay valid), and the FP32 copy of F for mixed matvecs
+static int fs_accept(mgk_fs3d_t p, cudaStream_t s) {
+  MGK_CUDA(cudaMemcpyAsync(p->F, p->Ftr, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
+  MGK_CUDA(cudaMemcpyAsync(p->P, p->Ptr, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
+  return fs_refresh_f32(p, false, s);
+}
+
+// Krylov loop graph for matvec precision T: scalar<2> (norm of the
+// right-hand side, sets the loop condition), then while (condition) {matvec,
+// alpha, update, beta + decision}.
+template <typename T>
+static int fs_build_graph(mgk_fs3d_t p, int slot) {
+  cudaGraph_t g = nullptr;
+  MGK_CUDA(cudaGraphCreate(&g, 0));
+  int rc = MGK_OK;
+  cudaGraphConditionalHandle h;
+  FsArgs a = fs_args(p);
+  const int zl = (int)(p->N / p->nz / 2);
+  const int ntile = (p->nzh + p->tc - 1) / p->tc;
+  const size_t zs = p->zsmem * sizeof(T) / 8, ys = p->ysmem * sizeof(T) / 8, xs = p->xsmem * sizeof(T) / 8;
+  int one = 1, nb = p->nblk;
+  auto add = [&](cudaGraph_t gr, cudaGraphNode_t* node, const cudaGraphNode_t* dep, void* fn, dim3 grid,
+                 size_t smem, void** args) {
+    cudaKernelNodeParams k;
+    memset(&k, 0, sizeof(k));
+    k.func = fn;
+    k.gridDim = grid;
+    k.blockDim = dim3(256);
+    k.sharedMemBytes = (unsigned)smem;
+    k.kernelParams = args;
+    if (rc == MGK_OK && cudaGraphAddKernelNode(node, gr, dep, dep ? 1 : 0, &k) != cudaSuccess) rc = MGK_CUDA_ERROR;
+  };
+  if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) rc = MGK_CUDA_ERROR;
+  cudaGraphNode_t n0 = nullptr, wn = nullptr;
+  void* a_s2[] = {&a, (void*)&zl, &h, &one};
+  add(g, &n0, nullptr, (void*)fs_scalar_kernel<2>, dim3(1), 0, a_s2);
+  cudaGraph_t body = nullptr;
+  if (rc == MGK_OK) {
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (cudaGraphAddNode(&wn, g, &n0, 1, &cp) != cudaSuccess) rc = MGK_CUDA_ERROR;
+    else body = cp.conditional.phGraph_out[0];
+  }
+  const double* dbar = p->dbar;
+  void* a_z[] = {&a, (void*)&dbar};
+  void* a_1[] = {&a};
+  void* a_s0[] = {&a, (void*)&zl, &h, &one};
+  void* a_s1[] = {&a, &nb, &h, &one};
+  cudaGraphNode_t k1, k2, k3, k4, k5, k6, k7, k8;
+  add(body, &k1, nullptr, (void*)fs_zfwd_kernel<0, T>, dim3(zl), zs, a_z);
+  add(body, &k2, &k1, (void*)fs_ypass_kernel<-1, T>, dim3(p->nx * ntile), ys, a_1);
+  add(body, &k3, &k2, (void*)fs_xg_kernel<T>, dim3(p->ny * ntile), xs, a_1);
+  add(body, &k4, &k3, (void*)fs_ypass_kernel<1, T>, dim3(p->nx * ntile), ys, a_1);
+  add(body, &k5, &k4, (void*)fs_zinv_kernel<0, T>, dim3(zl), zs, a_1);
+  add(body, &k6, &k5, (void*)fs_scalar_kernel<0>, dim3(1), 0, a_s0);
+  add(body, &k7, &k6, (void*)fs_update_kernel<T>, dim3(p->nblk), 0, a_1);
+  add(body, &k8, &k7, (void*)fs_scalar_kernel<1>, dim3(1), 0, a_s1);
+  cudaGraphExec_t x = nullptr;
+  if (rc == MGK_OK && cudaGraphInstantiate(&x, g, 0) != cudaSuccess) rc = MGK_CUDA_ERROR;
+  if (rc != MGK_OK) {
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+    return rc;
+  }
+  p->cg_graph[slot] = g;
+  p->cg_exec[slot] = x;
+  return MGK_OK;
+}
+
+// Krylov solve of G:K:dx = r (r holds the right-hand side, x = 0): on the
+// device through the graph, or host-driven (one scalar read per iteration)
+// when conditional graphs are unavailable.
+template <typename T>
+static int fs_krylov(mgk_fs3d_t p, double tol_CG, int max_cg, cudaStream_t s) {
+  const int slot = sizeof(T) == 8 ? 0 : 1;
+  const int zl = (int)(p->N / p->nz / 2);
+  if (p->graph_mode < 0) {
+    const char* env = getenv("MGK_NO_GRAPH_WHILE");
+    p->graph_mode = (env && env[0] == '1') ? 0 : 1;
+  }
+  if (p->graph_mode == 1 && !p->cg_exec[slot] && fs_build_graph<T>(p, slot) != MGK_OK) p->graph_mode = 0;
+  if (p->graph_mode == 1) {
+    p->h_dbar[10] = tol_CG * tol_CG;
+    p->h_dbar[11] = (double)max_cg;
+    MGK_CUDA(cudaMemcpyAsync(&p->sc->tol2, &p->h_dbar[10], 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    MGK_CUDA(cudaGraphLaunch(p->cg_exec[slot], s));
+    int rc = fs_read_scalars(p, s);
+    if (rc) return rc;
+    p->stat_krylov += (int)p->h_sc->kcount;
+    if (!isfinite(p->h_sc->rr)) { set_error("mgk_fs3d_step: non-finite Krylov residual"); return MGK_NONFINITE; }
+    return MGK_OK;
+  }
+  FsArgs a = fs_args(p);
+  fs_scalar_kernel<2><<<1, 256, 0, s>>>(a, zl, 0, 0);
+  MGK_CUDA(cudaGetLastError());
+  int rc = fs_read_scalars(p, s);
+  if (rc) return rc;
+  const double bnorm = sqrt(p->h_sc->bb);
+  for (int k = 0; k < max_cg; ++k) {
+    if (!(sqrt(p->h_sc->rr) > tol_CG * bnorm)) break;
+    rc = fs_project<T>(p, 0, 0, s);
+    if (rc) return rc;
+    fs_scalar_kernel<0><<<1, 256, 0, s>>>(a, zl, 0, 0);
+    fs_update_kernel<T><<<p->nblk, 256, 0, s>>>(a);
+    fs_scalar_kernel<1><<<1, 256, 0, s>>>(a, p->nblk, 0, 0);
+    MGK_CUDA(cudaGetLastError());
+    rc = fs_read_scalars(p, s);
+    if (rc) return rc;
+    ++p->stat_krylov;
+    if (!isfinite(p->h_sc->rr)) { set_error("mgk_fs3d_step: non-finite Krylov residual"); return MGK_NONFINITE; }
+  }
+  return MGK_OK;
 }
 
 // Newton branch (:3046-3119).  F holds F_start on entry, F_curr on exit.
@@ -727,32 +985,13 @@ static int fs_newton(mgk_fs3d_t p, const double* F_bar, double tol_NW, double to
   // P, K at F_start
   rc = fs_trial(p, 0.0, false, false, s);
   if (rc) return rc;
-  fs_accept(p);
-  const int zl = (int)(p->N / p->nz / 2);
+  if ((rc = fs_accept(p, s))) return rc;
   for (int it = 0; it < max_NW; ++it) {
-    // right-hand side into r (x = p = 0)
-    rc = fs_project(p, it == 0 ? 1 : 2, 1, s);
+    // right-hand side into r (x = 0), always FP64
+    rc = fs_project<double>(p, it == 0 ? 1 : 2, 1, s);
     if (rc) return rc;
-    a = fs_args(p);
-    fs_scalar_kernel<2><<<1, 256, 0, s>>>(a, zl);
-    MGK_CUDA(cudaGetLastError());
-    rc = fs_read_scalars(p, s);
+    rc = p->prec == MGK_MIXED ? fs_krylov<float>(p, tol_CG, max_cg, s) : fs_krylov<double>(p, tol_CG, max_cg, s);
     if (rc) return rc;
-    const double bnorm = sqrt(p->h_sc->bb);
-    for (int k = 0; k < max_cg; ++k) {
-      if (!(sqrt(p->h_sc->rr) > tol_CG * bnorm)) break;
-      rc = fs_project(p, 0, 0, s);
-      if (rc) return rc;
-      a = fs_args(p);
-      fs_scalar_kernel<0><<<1, 256, 0, s>>>(a, zl);
-      fs_update_kernel<<<p->nblk, 256, 0, s>>>(a);
-      fs_scalar_kernel<1><<<1, 256, 0, s>>>(a, p->nblk);
-      MGK_CUDA(cudaGetLastError());
-      rc = fs_read_scalars(p, s);
-      if (rc) return rc;
-      ++p->stat_krylov;
-      if (!isfinite(p->h_sc->rr)) { set_error("mgk_fs3d_step: non-finite Krylov residual"); return MGK_NONFINITE; }
-    }
     // line search (:3088-3114)
     double alpha = 1.0;
     bool ok = false;
@@ -765,7 +1004,7 @@ static int fs_newton(mgk_fs3d_t p, const double* F_bar, double tol_NW, double to
       break;
     }
     if (!ok) { set_error("Newton-CG line search failed to find a valid step."); return MGK_NOT_CONVERGED; }
-    fs_accept(p);
+    if ((rc = fs_accept(p, s))) return rc;
     ++p->stat_newton;
     const double res = sqrt(p->h_sc->xx) / (sqrt(p->h_sc->FF) + 1e-20);
     if (res < tol_NW && it > 0) return MGK_OK;

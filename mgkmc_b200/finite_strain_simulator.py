@@ -54,9 +54,11 @@ def build_finite_strain_bc_3d(driving_component, eps_target_step, mixed_targets,
 
 
 class Fs3dSolver:
-    """Plan-owning 3D finite-strain solver on one device (FP64)."""
+    """Plan-owning 3D finite-strain solver on one device.  ``precision``:
+    "fp64" (the reference's arithmetic) or "mixed" (FP32 Krylov matvecs; the
+    Newton residual, CG vectors, inner products and norms stay FP64)."""
 
-    def __init__(self, nx, ny, nz, model="svk", device=None):
+    def __init__(self, nx, ny, nz, model="svk", device=None, precision="fp64"):
         torch = _torch()
         self.shape = (int(nx), int(ny), int(nz))
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -64,6 +66,9 @@ class Fs3dSolver:
         with torch.cuda.device(self.device):
             L.check(L.lib().mgk_fs3d_create(*self.shape, _MODEL[model], ctypes.byref(h)), "mgk_fs3d_create")
         self._h = h
+        self.precision = precision
+        if precision != "fp64":
+            L.check(L.lib().mgk_fs3d_set_precision(h, L.MIXED), "mgk_fs3d_set_precision")
         self._keep = {}
         self.info = L.FsInfo()
 
@@ -146,7 +151,7 @@ def finite_strain_solver_step_3d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None
 
 
 def simulate_3d(E, nu, Fp, eps_target, n_steps, driving_component=(0, 0), mixed_targets=None, model="neo_hookean",
-                tol_NW=1e-8, tol_CG=1e-6, max_NW=50, tol_macro=1e6, max_iter_macro=20, solver=None):
+                tol_NW=1e-8, tol_CG=1e-6, max_NW=50, tol_macro=1e6, max_iter_macro=20, solver=None, precision="fp64"):
     """Incremental load ramp of finite_strain_simulation_3d (:3270-3298) with
     an eigen-deformation field F_p (that driver passes Fp=None, :3282).
     Returns the list of (F_bar, info) per step; the solver keeps the field."""
@@ -157,7 +162,7 @@ def simulate_3d(E, nu, Fp, eps_target, n_steps, driving_component=(0, 0), mixed_
     mu = E / (2 * (1 + nu))
     dev = torch.device("cuda", torch.cuda.current_device())
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
-    s = solver if solver is not None else Fs3dSolver(*shape, model=model)
+    s = solver if solver is not None else Fs3dSolver(*shape, model=model, precision=precision)
     s.set_material(t(lam), t(mu), None if Fp is None else t(Fp))
     s.set_F(t(np.einsum("ij,xyz->ijxyz", np.eye(3), np.ones(shape))))
     F_bar_init = None

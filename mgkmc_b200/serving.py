@@ -304,7 +304,7 @@ class Server:
         from .finite_strain_simulator import Fs3dSolver
         s = self.fs_plans.get(n)
         if s is None:
-            s = self.fs_plans[n] = Fs3dSolver(n, n, n, model="neo_hookean")
+            s = self.fs_plans[n] = Fs3dSolver(n, n, n, model="neo_hookean", precision=self.precision)
         return s
 
     def _fs_run(self, req, stream):

@@ -67,3 +67,52 @@ def test_load_ramp_runs_and_relaxes_lateral_stress():
     assert abs(Fb[0, 0] - 1.05) < 1e-12
     sig = info["sig_mean"]
     assert abs(sig[1, 1]) < 1e6 and abs(sig[2, 2]) < 1e6 and sig[0, 0] > 1e9
+
+
+@pytest.mark.parametrize("model,with_fp", [("neo_hookean", True), ("svk", False)])
+def test_mixed_precision_matches_fp64(model, with_fp):
+    # FP32 Krylov matvecs, FP64 Newton residual: the converged fields agree
+    # with the FP64 solve within the stated field-error bound of 1e-6 (the
+    # macro loop's stress tolerance of 1e3 Pa leaves differences ~1e-8)
+    import torch
+    from mgkmc_b200.finite_strain_simulator import Fs3dSolver, build_finite_strain_bc_3d
+    n = 16
+    rng = np.random.default_rng(31)
+    E, nu, Fp = W.fs3d_material(n, n, n, rng, fp_frac=0.1)
+    lam, mu = OF.lame_3d(E, nu)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    Fb, _, Pt, Pm = build_finite_strain_bc_3d((0, 0), 0.02, {(1, 1): 0.0, (2, 2): 0.0})
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = Fs3dSolver(n, n, n, model=model, precision=prec)
+        s.set_material(t(lam), t(mu), t(Fp) if with_fp else None)
+        s.set_F(t(np.einsum("ij,xyz->ijxyz", np.eye(3), np.ones((n, n, n)))))
+        Fbo, info = s.step(Fb, (0, 0), Pt, Pm, E.mean(), nu.mean(), 1e-10, 1e-6, 40, 1e3, 40)
+        F = torch.empty((3, 3, n, n, n), dtype=torch.float64, device="cuda")
+        P = torch.empty_like(F)
+        s.get(F, P)
+        out[prec] = (F.cpu().numpy(), P.cpu().numpy(), Fbo, info.krylov_iterations)
+    assert rel(out["mixed"][0], out["fp64"][0]) < 1e-6
+    assert rel(out["mixed"][1], out["fp64"][1]) < 1e-6
+    assert np.max(np.abs(out["mixed"][2] - out["fp64"][2])) < 1e-6
+
+
+def test_host_driven_krylov_loop_matches_graph():
+    # the host-driven fallback (no conditional graphs) runs the same arithmetic
+    import subprocess, sys, os
+    code = ("import numpy as np, torch, sys; sys.path.insert(0, '.');"
+            "from mgkmc_b200 import workloads as W; from mgkmc_b200.finite_strain_simulator import simulate_3d;"
+            "E, nu, Fp = W.fs3d_material(12, 12, 12, np.random.default_rng(4));"
+            "s, st = simulate_3d(E, nu, Fp, 0.01, 2, mixed_targets={(1, 1): 0.0, (2, 2): 0.0});"
+            "F = torch.empty((3, 3, 12, 12, 12), dtype=torch.float64, device='cuda'); s.get(F);"
+            "np.save(sys.argv[1], F.cpu().numpy())")
+    import tempfile
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for flag in ("0", "1"):
+            path = os.path.join(tmp, f"F_{flag}.npy")
+            env = dict(os.environ, MGK_NO_GRAPH_WHILE=flag)
+            subprocess.run([sys.executable, "-c", code, path], cwd=root, env=env, check=True)
+            outs.append(np.load(path))
+    assert np.array_equal(outs[0], outs[1])
