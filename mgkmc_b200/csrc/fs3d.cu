@@ -73,6 +73,8 @@ struct FsArgs {
   const float* lam32;
   float* p32;
   float* q32;
+  float* r32;
+  float* x32;
 };
 
 // the planes and FFT tables a matvec of precision T reads
@@ -84,6 +86,8 @@ template <> struct FsP<double> {
   static __device__ __forceinline__ const double* mu(const FsArgs& a) { return a.mu; }
   static __device__ __forceinline__ double* p(const FsArgs& a) { return a.p; }
   static __device__ __forceinline__ double* q(const FsArgs& a) { return a.q; }
+  static __device__ __forceinline__ double* r(const FsArgs& a) { return a.r; }
+  static __device__ __forceinline__ double* x(const FsArgs& a) { return a.x; }
   static __device__ __forceinline__ double2* spec(const FsArgs& a) { return a.spec; }
   static __device__ __forceinline__ const FftLen& fx(const FsArgs& a) { return a.fx; }
   static __device__ __forceinline__ const FftLen& fy(const FsArgs& a) { return a.fy; }
@@ -96,6 +100,8 @@ template <> struct FsP<float> {
   static __device__ __forceinline__ const float* mu(const FsArgs& a) { return a.mu32; }
   static __device__ __forceinline__ float* p(const FsArgs& a) { return a.p32; }
   static __device__ __forceinline__ float* q(const FsArgs& a) { return a.q32; }
+  static __device__ __forceinline__ float* r(const FsArgs& a) { return a.r32; }
+  static __device__ __forceinline__ float* x(const FsArgs& a) { return a.x32; }
   static __device__ __forceinline__ float2* spec(const FsArgs& a) { return reinterpret_cast<float2*>(a.spec); }
   static __device__ __forceinline__ const FftLen& fx(const FsArgs& a) { return a.fx32; }
   static __device__ __forceinline__ const FftLen& fy(const FsArgs& a) { return a.fy32; }
@@ -239,6 +245,7 @@ __global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __
   C* bufB = bufA + 9 * nz;
   const double beta = MODE == 0 ? a.sc->beta : 0.0;
   T* pp = FsP<T>::p(a);
+  const T* rr = FsP<T>::r(a);
   const T* Fp = FsP<T>::F(a);
   for (int z = threadIdx.x; z < nz; z += blockDim.x) {
     T out[2][9];
@@ -250,7 +257,7 @@ __global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __
         T d[9];
         if (MODE == 0) {
           for (int q = 0; q < 9; ++q) {
-            const double rv = a.r[q * N + i];
+            const double rv = (double)rr[q * N + i];
             const T pn = beta == 0.0 ? (T)rv : (T)(rv + beta * (double)pp[q * N + i]);
             pp[q * N + i] = pn;
             d[q] = pn;
@@ -416,7 +423,8 @@ __global__ void __launch_bounds__(256) fs_xg_kernel(FsArgs a) {
   }
 }
 
-// CG update: x += alpha p; r -= alpha q (p, q in the matvec precision); partial r.r
+// CG update: x += alpha p; r -= alpha q (the Krylov vectors in the matvec
+// precision, FP64 arithmetic and sums); partial r.r
 template <typename T>
 __global__ void fs_update_kernel(FsArgs a) {
   __shared__ double red[32];
@@ -424,12 +432,14 @@ __global__ void fs_update_kernel(FsArgs a) {
   const long long n9 = 9 * a.N;
   const T* pp = FsP<T>::p(a);
   const T* qq = FsP<T>::q(a);
+  T* xx = FsP<T>::x(a);
+  T* rr = FsP<T>::r(a);
   double acc = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9; i += (long long)gridDim.x * blockDim.x) {
-    a.x[i] += alpha * (double)pp[i];
-    const double rn = a.r[i] - alpha * (double)qq[i];
-    a.r[i] = rn;
-    acc += rn * rn;
+    xx[i] = (T)((double)xx[i] + alpha * (double)pp[i]);
+    const T rn = (T)((double)rr[i] - alpha * (double)qq[i]);
+    rr[i] = rn;
+    acc += (double)rn * (double)rn;
   }
   acc = block_sum(acc, red);
   if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
@@ -525,6 +535,7 @@ __global__ void fs_constitutive_kernel(FsArgs a, double alpha, const double* __r
 
 __global__ void fs_constitutive_finalize(FsArgs a, int nb) {
   __shared__ double red[32];
+  __shared__ double mn[32];
   FsScalars& S = *a.sc;
   double v[12];
   for (int q = 0; q < 12; ++q) {
@@ -532,16 +543,19 @@ __global__ void fs_constitutive_finalize(FsArgs a, int nb) {
     for (int i = threadIdx.x; i < nb; i += blockDim.x) s += a.part[(size_t)i * 16 + q];
     v[q] = block_sum(s, red);
   }
-  __shared__ double mn;
+  double m = INFINITY;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fmin(m, a.part[(size_t)i * 16 + 12]);
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) mn[threadIdx.x >> 5] = m;
+  __syncthreads();
   if (threadIdx.x == 0) {
     double r = INFINITY;
-    for (int i = 0; i < nb; ++i) r = fmin(r, a.part[(size_t)i * 16 + 12]);
-    mn = r;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) r = fmin(r, mn[w]);
     S.nan = v[0];
     S.FF = v[1];
     S.xx = v[2];
     for (int q = 0; q < 9; ++q) S.sig[q] = v[3 + q] / (double)a.N;
-    S.minJe = mn;
+    S.minJe = r;
   }
 }
 
@@ -577,6 +591,254 @@ __global__ void fs_cauchy_kernel(const double* __restrict__ P, const double* __r
     mmt(Pv, Fv, PF);
     for (int q = 0; q < 9; ++q) sig[q * N + i] = PF[q] / J;
   }
+}
+
+// ------------------------------------------------- warp-line 3D passes ---
+// The same five matvec stages for grids whose sides are 64, 96 or 128 (the
+// served and benchmark sizes): lines sit in padded shared memory and
+// each warp transforms its own lines with warp-local passes.
+//   axis kernels: CTA of 9 warps per tile of kFsTile kz columns at one x (y
+//     pass) or one y (x pass); warp c transforms component c's lines; the x
+//     pass applies G between the forward and inverse transforms (CTA barrier).
+//   z kernels: CTA of 3 warps per pair of z-lines; the per-voxel stage (K:p or
+//     P, or q and the p.q sums) uses all threads, warp w transforms the lines
+//     of components 3w..3w+2.
+constexpr int kFsTile = 4;
+
+__host__ __device__ constexpr bool fs_fast_len(int n) { return n == 64 || n == 96 || n == 128; }
+__host__ __device__ constexpr int fs_pl(int n, int csz) {
+  return csz == 16 ? n + n / 8 + 1 : ((n + n / 16 + 2) & ~1);
+}
+
+template <int SIGN, typename T, int NL, bool XG>
+__device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, long long obase, long long jstride,
+                                             unsigned char* smem) {
+  using C = C_t<T>;
+  constexpr int PL = padded_len<C>(NL);
+  constexpr int TC = kFsTile;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nzh = a.nzh;
+  const int tcw = min(TC, nzh - k0);
+  const long long plane = (long long)a.nx * a.ny * a.ld;
+  C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t)
+  C* spec = FsP<T>::spec(a);
+  constexpr int TOT = 9 * NL * TC;
+  for (int e = threadIdx.x; e < TOT; e += 9 * 32) {
+    const int c = e / (NL * TC);
+    const int rem = e - c * NL * TC;
+    const int j = rem / TC, t = rem - j * TC;
+    if (t < tcw)
+      cp_async_elem(&lines[(c * TC + t) * PL + pidx<C>(j)], &spec[c * plane + o * obase + j * jstride + k0 + t]);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>((XG ? FsP<T>::fx(a) : FsP<T>::fy(a)).tw);
+  C* l0 = lines + warp * TC * PL;  // warp = component
+  warp_fft<NL, XG ? -1 : SIGN, 2>(l0, PL, tw, lane);
+  warp_fft<NL, XG ? -1 : SIGN, 2>(l0 + 2 * PL, PL, tw, lane);
+  if (XG) {
+    __syncthreads();
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const T scale = (T)(1.0 / (double)a.N);
+    const int ky = o;
+    const double uy = (double)ffq(ky, ny) / ny;
+    const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
+    for (int e = threadIdx.x; e < tcw * NL; e += 9 * 32) {
+      const int t = e / NL, kx = e - t * NL;
+      const int kz = k0 + t;
+      const int pk = pidx<C>(kx);
+      const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
+      if ((kx == 0 && ky == 0 && kz == 0) || nqx || nqy || nqz) {
+        for (int c = 0; c < 9; ++c) lines[(c * TC + t) * PL + pk] = mk<C>(T(0), T(0));
+        continue;
+      }
+      const double ux = (double)ffq(kx, nx) / nx, uz = (double)ffq(kz, nz) / nz;
+      const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
+      const T n[3] = {(T)(ux * inv), (T)(uy * inv), (T)(uz * inv)};
+      C A[9];
+      for (int c = 0; c < 9; ++c) A[c] = lines[(c * TC + t) * PL + pk];
+      for (int i = 0; i < 3; ++i) {
+        T vx = 0, vy = 0;
+        for (int l = 0; l < 3; ++l) { vx += A[3 * i + l].x * n[l]; vy += A[3 * i + l].y * n[l]; }
+        for (int j = 0; j < 3; ++j)
+          lines[((3 * i + j) * TC + t) * PL + pk] = mk<C>(vx * n[j] * scale, vy * n[j] * scale);
+      }
+    }
+    __syncthreads();
+    warp_fft<NL, +1, 2>(l0, PL, tw, lane);
+    warp_fft<NL, +1, 2>(l0 + 2 * PL, PL, tw, lane);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < TOT; e += 9 * 32) {
+    const int c = e / (NL * TC);
+    const int rem = e - c * NL * TC;
+    const int j = rem / TC, t = rem - j * TC;
+    if (t < tcw) spec[c * plane + o * obase + j * jstride + k0 + t] = lines[(c * TC + t) * PL + pidx<C>(j)];
+  }
+}
+
+// y pass (XG = false) or x pass with G (XG = true); grid = (nx or ny) * ntile
+template <int SIGN, typename T, bool XG>
+__global__ void __launch_bounds__(9 * 32, sizeof(T) == 8 ? 1 : 3) fs_axis_fast_kernel(FsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int ntile = (a.nzh + kFsTile - 1) / kFsTile;
+  const int o = blockIdx.x / ntile;
+  const int k0 = (blockIdx.x - o * ntile) * kFsTile;
+  const long long obase = XG ? (long long)a.ld : (long long)a.ny * a.ld;
+  const long long jstride = XG ? (long long)a.ny * a.ld : (long long)a.ld;
+  const int nl = XG ? a.nx : a.ny;
+#define MGK_AX_CASE(n) case n: fs_axis_body<SIGN, T, n, XG>(a, o, k0, obase, jstride, smem_raw); break;
+  switch (nl) {
+    MGK_AX_CASE(64) MGK_AX_CASE(96) MGK_AX_CASE(128)
+    default: break;
+  }
+#undef MGK_AX_CASE
+}
+
+// z forward: per-voxel stage (MODE 0: p = r + beta p and K:p; 1: K:dbar;
+// 2: P), R2C along z of the pair of z-lines, 9 components.
+template <int MODE, typename T, int NZ>
+__device__ __forceinline__ void fs_zfwd_body(const FsArgs& a, const double* __restrict__ dbar, unsigned char* smem) {
+  using C = C_t<T>;
+  constexpr int PL = padded_len<C>(NZ);
+  constexpr int NZH = NZ / 2 + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long N = a.N;
+  const long long l0 = 2LL * blockIdx.x;
+  const long long plane = (long long)a.nx * a.ny * a.ld;
+  const int ld = a.ld;
+  C* lines = reinterpret_cast<C*>(smem);
+  const double beta = MODE == 0 ? a.sc->beta : 0.0;
+  T* pp = FsP<T>::p(a);
+  const T* rr = FsP<T>::r(a);
+  const T* Fp = FsP<T>::F(a);
+  for (int z = threadIdx.x; z < NZ; z += 3 * 32) {
+    T out[2][9];
+    for (int h = 0; h < 2; ++h) {
+      const long long i = (l0 + h) * NZ + z;
+      if (MODE == 2) {
+        for (int q = 0; q < 9; ++q) out[h][q] = (T)a.P[q * N + i];
+      } else {
+        T d[9];
+        if (MODE == 0) {
+          for (int q = 0; q < 9; ++q) {
+            const double rv = (double)rr[q * N + i];
+            const T pn = beta == 0.0 ? (T)rv : (T)(rv + beta * (double)pp[q * N + i]);
+            pp[q * N + i] = pn;
+            d[q] = pn;
+          }
+        } else {
+          for (int q = 0; q < 9; ++q) d[q] = (T)dbar[q];
+        }
+        T F[9];
+        for (int q = 0; q < 9; ++q) F[q] = Fp[q * N + i];
+        VoxelLaw<T> law;
+        law.init(a, i, F, T(0), nullptr);
+        law.kdf(d, out[h]);
+      }
+    }
+    const int pz = pidx<C>(z);
+    for (int q = 0; q < 9; ++q) lines[q * PL + pz] = mk<C>(out[0][q], out[1][q]);
+  }
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(FsP<T>::fz(a).tw);
+  C* lw = lines + 3 * warp * PL;
+  warp_fft<NZ, -1, 3>(lw, PL, tw, lane);
+  C* spec = FsP<T>::spec(a);
+  for (int cc = 0; cc < 3; ++cc) {
+    const int c = 3 * warp + cc;
+    const C* ln = lines + c * PL;
+    C* ra = spec + c * plane + l0 * ld;
+    for (int k = lane; k < NZH; k += 32) {
+      const C zz = ln[pidx<C>(k)];
+      const C w = ln[pidx<C>(k == 0 ? 0 : NZ - k)];
+      ra[k] = mk<C>(T(0.5) * (zz.x + w.x), T(0.5) * (zz.y - w.y));
+      ra[ld + k] = mk<C>(T(0.5) * (zz.y + w.y), T(-0.5) * (zz.x - w.x));
+    }
+  }
+}
+
+template <int MODE, typename T>
+__global__ void __launch_bounds__(3 * 32) fs_zfwd_fast_kernel(FsArgs a, const double* __restrict__ dbar) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+#define MGK_ZF_CASE(n) case n: fs_zfwd_body<MODE, T, n>(a, dbar, smem_raw); break;
+  switch (a.nz) {
+    MGK_ZF_CASE(64) MGK_ZF_CASE(96) MGK_ZF_CASE(128)
+    default: break;
+  }
+#undef MGK_ZF_CASE
+}
+
+// z inverse: C2R along z of the pair of z-lines; MODE 0: q and the p.q
+// partial; MODE 1 (FP64): r = -result, x = 0, the r.r partial.
+template <int MODE, typename T, int NZ>
+__device__ __forceinline__ void fs_zinv_body(const FsArgs& a, unsigned char* smem, double* red) {
+  using C = C_t<T>;
+  constexpr int PL = padded_len<C>(NZ);
+  constexpr int NZH = NZ / 2 + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long N = a.N;
+  const long long l0 = 2LL * blockIdx.x;
+  const long long plane = (long long)a.nx * a.ny * a.ld;
+  const int ld = a.ld;
+  C* lines = reinterpret_cast<C*>(smem);
+  const C* spec = FsP<T>::spec(a);
+  for (int cc = 0; cc < 3; ++cc) {
+    const int c = 3 * warp + cc;
+    C* ln = lines + c * PL;
+    const C* ra = spec + c * plane + l0 * ld;
+    for (int k = lane; k < NZH; k += 32) {
+      C av = ra[k], bv = ra[ld + k];
+      if (k == 0 || 2 * k == NZ) { av.y = 0; bv.y = 0; }
+      ln[pidx<C>(k)] = mk<C>(av.x - bv.y, av.y + bv.x);
+      if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = mk<C>(av.x + bv.y, bv.x - av.y);
+    }
+  }
+  __syncwarp();
+  const C* tw = reinterpret_cast<const C*>(FsP<T>::fz(a).tw);
+  warp_fft<NZ, +1, 3>(lines + 3 * warp * PL, PL, tw, lane);
+  __syncthreads();
+  T* qq = FsP<T>::q(a);
+  const T* pp = FsP<T>::p(a);
+  double acc = 0;
+  for (int z = threadIdx.x; z < NZ; z += 3 * 32) {
+    const int pz = pidx<C>(z);
+    for (int c = 0; c < 9; ++c) {
+      const C v = lines[c * PL + pz];
+      for (int h = 0; h < 2; ++h) {
+        const long long i = (l0 + h) * NZ + z;
+        const T val = h == 0 ? v.x : v.y;
+        if (MODE == 0) {
+          qq[c * N + i] = val;
+          acc += (double)pp[c * N + i] * (double)val;
+        } else {
+          a.r[c * N + i] = -(double)val;
+          a.x[c * N + i] = 0.0;
+          acc += (double)val * (double)val;
+        }
+      }
+    }
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) a.part[blockIdx.x] = acc;
+}
+
+template <int MODE, typename T>
+__global__ void __launch_bounds__(3 * 32) fs_zinv_fast_kernel(FsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+#define MGK_ZI_CASE(n) case n: fs_zinv_body<MODE, T, n>(a, smem_raw, red); break;
+  switch (a.nz) {
+    MGK_ZI_CASE(64) MGK_ZI_CASE(96) MGK_ZI_CASE(128)
+    default: break;
+  }
+#undef MGK_ZI_CASE
+}
+
+// FP64 copies of n floats (the mixed form's Krylov solution back to FP64)
+__global__ void fs_to_f64_kernel(long long n, const float* __restrict__ src, double* __restrict__ dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
 }
 
 // FP32 copies of n doubles (the mixed form's matvec inputs)
@@ -636,11 +898,13 @@ struct mgk_fs3d_plan {
   int prec = MGK_FP64;
   float* f32 = nullptr;  // F32, Fpi32, lam32, mu32, p32, q32
   float *F32 = nullptr, *Fpi32 = nullptr, *lam32 = nullptr, *mu32 = nullptr, *p32 = nullptr, *q32 = nullptr;
+  float *r32 = nullptr, *x32 = nullptr;
   FftLen fx32, fy32, fz32;
   // device-side Krylov loop graphs, one per matvec precision (0 FP64, 1 FP32)
   cudaGraph_t cg_graph[2] = {nullptr, nullptr};
   cudaGraphExec_t cg_exec[2] = {nullptr, nullptr};
   int graph_mode = -1;  // -1 untried, 1 graphs, 0 host-driven loop
+  int fast = 0;         // warp-line passes (every side has a compiled FFT)
 };
 
 static FsArgs fs_args(mgk_fs3d_t p) {
@@ -654,6 +918,7 @@ static FsArgs fs_args(mgk_fs3d_t p) {
   a.spec = p->spec; a.part = p->part; a.sc = p->sc;
   a.fx32 = p->fx32; a.fy32 = p->fy32; a.fz32 = p->fz32;
   a.F32 = p->F32; a.Fpi32 = p->Fpi32; a.mu32 = p->mu32; a.lam32 = p->lam32; a.p32 = p->p32; a.q32 = p->q32;
+  a.r32 = p->r32; a.x32 = p->x32;
   return a;
 }
 
@@ -732,6 +997,31 @@ extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* ou
     set_error("mgk_fs3d_create: cudaFuncSetAttribute failed");
     return fail(MGK_CUDA_ERROR);
   }
+  {
+    const char* env = getenv("MGK_FS_FAST");
+    p->fast = fs_fast_len(nx) && fs_fast_len(ny) && fs_fast_len(nz) && !(env && env[0] == '0');
+  }
+  if (p->fast) {
+    const int zs64 = 9 * fs_pl(nz, 16) * 16, zs32 = 9 * fs_pl(nz, 8) * 8;
+    const int ys64 = 9 * kFsTile * fs_pl(ny, 16) * 16, ys32 = 9 * kFsTile * fs_pl(ny, 8) * 8;
+    const int xs64 = 9 * kFsTile * fs_pl(nx, 16) * 16, xs32 = 9 * kFsTile * fs_pl(nx, 8) * 8;
+    if (raise_smem((const void*)fs_zfwd_fast_kernel<0, double>, zs64) ||
+        raise_smem((const void*)fs_zfwd_fast_kernel<1, double>, zs64) ||
+        raise_smem((const void*)fs_zfwd_fast_kernel<2, double>, zs64) ||
+        raise_smem((const void*)fs_zfwd_fast_kernel<0, float>, zs32) ||
+        raise_smem((const void*)fs_zinv_fast_kernel<0, double>, zs64) ||
+        raise_smem((const void*)fs_zinv_fast_kernel<1, double>, zs64) ||
+        raise_smem((const void*)fs_zinv_fast_kernel<0, float>, zs32) ||
+        raise_smem((const void*)fs_axis_fast_kernel<-1, double, false>, ys64) ||
+        raise_smem((const void*)fs_axis_fast_kernel<1, double, false>, ys64) ||
+        raise_smem((const void*)fs_axis_fast_kernel<-1, double, true>, xs64) ||
+        raise_smem((const void*)fs_axis_fast_kernel<-1, float, false>, ys32) ||
+        raise_smem((const void*)fs_axis_fast_kernel<1, float, false>, ys32) ||
+        raise_smem((const void*)fs_axis_fast_kernel<-1, float, true>, xs32)) {
+      set_error("mgk_fs3d_create: cudaFuncSetAttribute failed");
+      return fail(MGK_CUDA_ERROR);
+    }
+  }
   *out = p;
   return MGK_OK;
 }
@@ -764,14 +1054,14 @@ extern "C" int mgk_fs3d_set_precision(mgk_fs3d_t p, int precision) {
   MGK_REQUIRE(precision == MGK_FP64 || precision == MGK_MIXED, "mgk_fs3d_set_precision: bad precision");
   if (precision == MGK_MIXED && !p->f32) {
     const long long N = p->N;
-    if (cudaMalloc(&p->f32, sizeof(float) * N * (9 + 9 + 2 + 9 + 9)) != cudaSuccess) {
+    if (cudaMalloc(&p->f32, sizeof(float) * N * (9 + 9 + 2 + 9 + 9 + 9 + 9)) != cudaSuccess) {
       cudaGetLastError();
       set_error("mgk_fs3d_set_precision: cudaMalloc of the FP32 planes failed");
       return MGK_OOM;
     }
     float* f = p->f32;
     p->F32 = f; p->Fpi32 = f + 9 * N; p->lam32 = f + 18 * N; p->mu32 = f + 19 * N; p->p32 = f + 20 * N;
-    p->q32 = f + 29 * N;
+    p->q32 = f + 29 * N; p->r32 = f + 38 * N; p->x32 = f + 47 * N;
     p->fx32 = p->fx; p->fy32 = p->fy; p->fz32 = p->fz;
     p->fx32.tw = twiddles(p->nx, 1); p->fy32.tw = twiddles(p->ny, 1); p->fz32.tw = twiddles(p->nz, 1);
     if (!p->fx32.tw || !p->fy32.tw || !p->fz32.tw) return MGK_OOM;
@@ -817,22 +1107,54 @@ extern "C" int mgk_fs3d_get(mgk_fs3d_t p, double* F_out, double* P_out, double* 
   return MGK_OK;
 }
 
+// The five launches of one matvec / projection (function, grid, block,
+// shared memory), for the plan's kernel family and precision T.
+struct FsLaunch {
+  void* fn;
+  dim3 grid, block;
+  size_t smem;
+};
+template <typename T>
+static void fs_stage_launches(mgk_fs3d_t p, int mode, int zmode, FsLaunch L[5]) {
+  const int zl = (int)(p->N / p->nz / 2);
+  if (p->fast) {
+    const int csz = (int)sizeof(C_t<T>);
+    const int ntile = (p->nzh + kFsTile - 1) / kFsTile;
+    const size_t zs = 9 * (size_t)fs_pl(p->nz, csz) * csz, zs64 = 9 * (size_t)fs_pl(p->nz, 16) * 16;
+    const size_t ys = 9 * (size_t)kFsTile * fs_pl(p->ny, csz) * csz;
+    const size_t xs = 9 * (size_t)kFsTile * fs_pl(p->nx, csz) * csz;
+    L[0] = {mode == 0 ? (void*)fs_zfwd_fast_kernel<0, T>
+                      : (mode == 1 ? (void*)fs_zfwd_fast_kernel<1, double> : (void*)fs_zfwd_fast_kernel<2, double>),
+            dim3(zl), dim3(96), mode == 0 ? zs : zs64};
+    L[1] = {(void*)fs_axis_fast_kernel<-1, T, false>, dim3(p->nx * ntile), dim3(288), ys};
+    L[2] = {(void*)fs_axis_fast_kernel<-1, T, true>, dim3(p->ny * ntile), dim3(288), xs};
+    L[3] = {(void*)fs_axis_fast_kernel<1, T, false>, dim3(p->nx * ntile), dim3(288), ys};
+    L[4] = {zmode == 0 ? (void*)fs_zinv_fast_kernel<0, T> : (void*)fs_zinv_fast_kernel<1, double>, dim3(zl), dim3(96),
+            zmode == 0 ? zs : zs64};
+  } else {
+    const int ntile = (p->nzh + p->tc - 1) / p->tc;
+    const size_t zs = p->zsmem * sizeof(T) / 8, ys = p->ysmem * sizeof(T) / 8, xs = p->xsmem * sizeof(T) / 8;
+    L[0] = {mode == 0 ? (void*)fs_zfwd_kernel<0, T>
+                      : (mode == 1 ? (void*)fs_zfwd_kernel<1, double> : (void*)fs_zfwd_kernel<2, double>),
+            dim3(zl), dim3(256), mode == 0 ? zs : p->zsmem};
+    L[1] = {(void*)fs_ypass_kernel<-1, T>, dim3(p->nx * ntile), dim3(256), ys};
+    L[2] = {(void*)fs_xg_kernel<T>, dim3(p->ny * ntile), dim3(256), xs};
+    L[3] = {(void*)fs_ypass_kernel<1, T>, dim3(p->nx * ntile), dim3(256), ys};
+    L[4] = {zmode == 0 ? (void*)fs_zinv_kernel<0, T> : (void*)fs_zinv_kernel<1, double>, dim3(zl), dim3(256),
+            zmode == 0 ? zs : p->zsmem};
+  }
+}
+
 // one matvec / projection in precision T: zfwd<MODE> -> y -> xG -> y^-1 -> zinv<ZMODE>
 template <typename T>
 static int fs_project(mgk_fs3d_t p, int mode, int zmode, cudaStream_t s) {
   FsArgs a = fs_args(p);
-  const int zl = (int)(p->N / p->nz / 2);
-  const int ntile = (p->nzh + p->tc - 1) / p->tc;
-  const size_t zs = p->zsmem * sizeof(T) / 8, ys = p->ysmem * sizeof(T) / 8, xs = p->xsmem * sizeof(T) / 8;
-  if (mode == 0) fs_zfwd_kernel<0, T><<<zl, 256, zs, s>>>(a, p->dbar);
-  else if (mode == 1) fs_zfwd_kernel<1, double><<<zl, 256, zs, s>>>(a, p->dbar);
-  else fs_zfwd_kernel<2, double><<<zl, 256, zs, s>>>(a, p->dbar);
-  fs_ypass_kernel<-1, T><<<p->nx * ntile, 256, ys, s>>>(a);
-  fs_xg_kernel<T><<<p->ny * ntile, 256, xs, s>>>(a);
-  fs_ypass_kernel<1, T><<<p->nx * ntile, 256, ys, s>>>(a);
-  if (zmode == 0) fs_zinv_kernel<0, T><<<zl, 256, zs, s>>>(a);
-  else fs_zinv_kernel<1, double><<<zl, 256, zs, s>>>(a);
-  MGK_CUDA(cudaGetLastError());
+  FsLaunch L[5];
+  fs_stage_launches<T>(p, mode, zmode, L);
+  const double* dbar = p->dbar;
+  void* az[] = {&a, (void*)&dbar};
+  void* a1[] = {&a};
+  for (int k = 0; k < 5; ++k) MGK_CUDA(cudaLaunchKernel(L[k].fn, L[k].grid, L[k].block, k == 0 ? az : a1, L[k].smem, s));
   return MGK_OK;
 }
 
@@ -870,16 +1192,14 @@ static int fs_build_graph(mgk_fs3d_t p, int slot) {
   cudaGraphConditionalHandle h;
   FsArgs a = fs_args(p);
   const int zl = (int)(p->N / p->nz / 2);
-  const int ntile = (p->nzh + p->tc - 1) / p->tc;
-  const size_t zs = p->zsmem * sizeof(T) / 8, ys = p->ysmem * sizeof(T) / 8, xs = p->xsmem * sizeof(T) / 8;
   int one = 1, nb = p->nblk;
-  auto add = [&](cudaGraph_t gr, cudaGraphNode_t* node, const cudaGraphNode_t* dep, void* fn, dim3 grid,
+  auto add = [&](cudaGraph_t gr, cudaGraphNode_t* node, const cudaGraphNode_t* dep, void* fn, dim3 grid, dim3 block,
                  size_t smem, void** args) {
     cudaKernelNodeParams k;
     memset(&k, 0, sizeof(k));
     k.func = fn;
     k.gridDim = grid;
-    k.blockDim = dim3(256);
+    k.blockDim = block;
     k.sharedMemBytes = (unsigned)smem;
     k.kernelParams = args;
     if (rc == MGK_OK && cudaGraphAddKernelNode(node, gr, dep, dep ? 1 : 0, &k) != cudaSuccess) rc = MGK_CUDA_ERROR;
@@ -887,7 +1207,7 @@ static int fs_build_graph(mgk_fs3d_t p, int slot) {
   if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) rc = MGK_CUDA_ERROR;
   cudaGraphNode_t n0 = nullptr, wn = nullptr;
   void* a_s2[] = {&a, (void*)&zl, &h, &one};
-  add(g, &n0, nullptr, (void*)fs_scalar_kernel<2>, dim3(1), 0, a_s2);
+  add(g, &n0, nullptr, (void*)fs_scalar_kernel<2>, dim3(1), dim3(256), 0, a_s2);
   cudaGraph_t body = nullptr;
   if (rc == MGK_OK) {
     alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
@@ -905,15 +1225,14 @@ static int fs_build_graph(mgk_fs3d_t p, int slot) {
   void* a_1[] = {&a};
   void* a_s0[] = {&a, (void*)&zl, &h, &one};
   void* a_s1[] = {&a, &nb, &h, &one};
-  cudaGraphNode_t k1, k2, k3, k4, k5, k6, k7, k8;
-  add(body, &k1, nullptr, (void*)fs_zfwd_kernel<0, T>, dim3(zl), zs, a_z);
-  add(body, &k2, &k1, (void*)fs_ypass_kernel<-1, T>, dim3(p->nx * ntile), ys, a_1);
-  add(body, &k3, &k2, (void*)fs_xg_kernel<T>, dim3(p->ny * ntile), xs, a_1);
-  add(body, &k4, &k3, (void*)fs_ypass_kernel<1, T>, dim3(p->nx * ntile), ys, a_1);
-  add(body, &k5, &k4, (void*)fs_zinv_kernel<0, T>, dim3(zl), zs, a_1);
-  add(body, &k6, &k5, (void*)fs_scalar_kernel<0>, dim3(1), 0, a_s0);
-  add(body, &k7, &k6, (void*)fs_update_kernel<T>, dim3(p->nblk), 0, a_1);
-  add(body, &k8, &k7, (void*)fs_scalar_kernel<1>, dim3(1), 0, a_s1);
+  cudaGraphNode_t kn[5], k6, k7, k8;
+  FsLaunch L[5];
+  fs_stage_launches<T>(p, 0, 0, L);
+  for (int k = 0; k < 5; ++k)
+    add(body, &kn[k], k ? &kn[k - 1] : nullptr, L[k].fn, L[k].grid, L[k].block, L[k].smem, k == 0 ? a_z : a_1);
+  add(body, &k6, &kn[4], (void*)fs_scalar_kernel<0>, dim3(1), dim3(256), 0, a_s0);
+  add(body, &k7, &k6, (void*)fs_update_kernel<T>, dim3(p->nblk), dim3(256), 0, a_1);
+  add(body, &k8, &k7, (void*)fs_scalar_kernel<1>, dim3(1), dim3(256), 0, a_s1);
   cudaGraphExec_t x = nullptr;
   if (rc == MGK_OK && cudaGraphInstantiate(&x, g, 0) != cudaSuccess) rc = MGK_CUDA_ERROR;
   if (rc != MGK_OK) {
@@ -930,9 +1249,28 @@ static int fs_build_graph(mgk_fs3d_t p, int slot) {
 // device through the graph, or host-driven (one scalar read per iteration)
 // when conditional graphs are unavailable.
 template <typename T>
+static int fs_krylov_run(mgk_fs3d_t p, double tol_CG, int max_cg, cudaStream_t s, int slot, int zl);
+
+template <typename T>
 static int fs_krylov(mgk_fs3d_t p, double tol_CG, int max_cg, cudaStream_t s) {
   const int slot = sizeof(T) == 8 ? 0 : 1;
   const int zl = (int)(p->N / p->nz / 2);
+  if (sizeof(T) == 4) {
+    // FP32 Krylov vectors: r from the FP64 right-hand side, x = 0
+    fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(9 * p->N, p->r, p->r32);
+    MGK_CUDA(cudaGetLastError());
+    MGK_CUDA(cudaMemsetAsync(p->x32, 0, sizeof(float) * 9 * p->N, s));
+  }
+  int rc2 = fs_krylov_run<T>(p, tol_CG, max_cg, s, slot, zl);
+  if (rc2 == MGK_OK && sizeof(T) == 4) {
+    fs_to_f64_kernel<<<p->nblk, 256, 0, s>>>(9 * p->N, p->x32, p->x);
+    MGK_CUDA(cudaGetLastError());
+  }
+  return rc2;
+}
+
+template <typename T>
+static int fs_krylov_run(mgk_fs3d_t p, double tol_CG, int max_cg, cudaStream_t s, int slot, int zl) {
   if (p->graph_mode < 0) {
     const char* env = getenv("MGK_NO_GRAPH_WHILE");
     p->graph_mode = (env && env[0] == '1') ? 0 : 1;
