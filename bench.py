@@ -12,6 +12,11 @@ problems, in three forms: plain FP64 (one solve after another), batched FP64
 FP64 finish; the headline value).  value = solves/s over all ranks (replicas
 only: each rank solves its own problems, no collective; scaling "weak").
 
+Finite-strain block (N = 1, ``--fs-grid``, default 128^3): the 10-step
+Neo-Hookean ramp of the finite-strain workload in the plain FP64 form and the
+mixed form (FP32 Krylov matvecs), device-timed, with the mixed form's field
+error and the per-kernel times of one Krylov iteration.
+
 Serving block (N = 1, ``--serve-window`` seconds of the serving stream): the
 continuous-batching server in mixed precision against the plain FP64 form
 served one request at a time, both on this GPU with arrivals replayed in real
@@ -52,6 +57,8 @@ def parse():
     ap.add_argument("--grid", type=int, default=256, help="grid side (2^a 3^b); the headline workload is 256")
     ap.add_argument("--forms", default="plain_fp64,batched_fp64,batched_mixed",
                     help="comma list of forms to time (the headline is batched_mixed)")
+    ap.add_argument("--fs-grid", type=int, default=128,
+                    help="side of the finite-strain block (Neo-Hookean + F_p, 10 load steps); 0 skips it")
     ap.add_argument("--serve-window", type=float, default=0.1,
                     help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
                          "0 skips it")
@@ -185,6 +192,54 @@ def run_serving(window):
         out["solves_per_s_ratio"] = a["solves_per_s"] / b["solves_per_s"]
         out["p50_ratio"] = b["p50_s"] / a["p50_s"]
         out["p99_ratio"] = b["p99_s"] / a["p99_s"]
+    return out
+
+
+# ------------------------------------------------------- finite strain -----
+def run_finite_strain(n, peak):
+    """3D finite-strain ramp (Neo-Hookean, 2 % F_p, F_xx to 1.05 in 10 load
+    steps, lateral stresses zero, Newton 1e-8, CG 1e-6) in the plain FP64 form
+    and the mixed form (FP32 Krylov matvecs), device-timed; the mixed form's
+    field error against FP64; per-kernel times of one Krylov iteration."""
+    import torch
+    from mgkmc_b200 import workloads as W
+    from mgkmc_b200.finite_strain_simulator import Fs3dSolver, simulate_3d
+    E, nu, Fp = W.fs3d_material(n, n, n, np.random.default_rng(2))
+    out = {"workload": f"finite strain {n}^3, Neo-Hookean + 2 % F_p, F_xx 1 -> 1.05 in 10 load steps, "
+                       f"lateral stresses zero, Newton tol 1e-8, CG tol 1e-6"}
+    fields = {}
+    N = n ** 3
+    for prec in ("fp64", "mixed"):
+        solver = Fs3dSolver(n, n, n, model="neo_hookean", precision=prec)
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        s, steps = simulate_3d(E, nu, Fp, 0.05, 10, mixed_targets={(1, 1): 0.0, (2, 2): 0.0}, model="neo_hookean",
+                               tol_NW=1e-8, tol_CG=1e-6, solver=solver)
+        e1.record(st)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        F = torch.empty((3, 3, n, n, n), dtype=torch.float64, device="cuda")
+        P = torch.empty_like(F)
+        s.get(F, P)
+        fields[prec] = (F, P)
+        ms = s.profile_kernels(fp32=(prec == "mixed"), reps=10)
+        w = 8.0 if prec == "fp64" else 4.0
+        it_bytes = 110.0 * w * N  # algorithmic bytes of one Krylov iteration
+        out[prec] = {"seconds": sec, "load_steps_per_s": 11 / sec,
+                     "krylov": int(sum(x[1]["krylov"] for x in steps)),
+                     "newton": int(sum(x[1]["newton"] for x in steps)),
+                     "macro": int(sum(x[1]["macro"] for x in steps)),
+                     "kernels_us": dict(zip(["z_fwd_Kp", "y", "x_G", "y_inv", "z_inv_pq", "cg_update"],
+                                            [round(1e3 * v, 1) for v in ms])),
+                     "krylov_iteration_gbs": it_bytes / (sum(ms) * 1e-3) / 1e9,
+                     "krylov_iteration_frac_of_measured_hbm": it_bytes / (sum(ms) * 1e-3) / 1e9 / peak}
+        del s, solver
+    (Fa, Pa), (Fb, Pb) = fields["mixed"], fields["fp64"]
+    out["mixed_speedup"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    out["mixed_field_err_vs_fp64"] = {"F": float((Fa - Fb).abs().max() / Fb.abs().max()),
+                                      "P": float((Pa - Pb).abs().max() / Pb.abs().max())}
     return out
 
 
@@ -343,6 +398,9 @@ def run_ours(a):
                            "col_fp32": col32 * 1e3},
             "col_fp64_frac": 48.0 * N * B / (col64 * 1e-3) / 1e9 / peak,
             "row_fp32_frac": 68.0 * N * B / (row32 * 1e-3) / 1e9 / peak}
+    finite_strain = None
+    if world == 1 and a.fs_grid > 0:
+        finite_strain = run_finite_strain(a.fs_grid, peak)
     serving = None
     if world == 1 and a.serve_window > 0:
         serving = run_serving(a.serve_window)
@@ -363,7 +421,7 @@ def run_ours(a):
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.Ls2dBatch"},
             "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "serving": serving}
+            "finite_strain": finite_strain, "serving": serving}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

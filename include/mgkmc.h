@@ -225,6 +225,12 @@ MGK_API int mgk_fs3d_step(mgk_fs3d_t plan, const double* F_bar_in, int driving_i
 /* Copy out F and P (device, tensor-first) and compute the Cauchy stress
  * (cauchy_from_P_3d :1892-1904); any pointer may be NULL. */
 MGK_API int mgk_fs3d_get(mgk_fs3d_t plan, double* F_out, double* P_out, double* sig_out, mgk_stream_t stream);
+/* Timing hook: mean duration (ms, CUDA events on `stream`) of the six kernels
+ * of one Krylov iteration (z forward with K:p, y pass, x pass with G, inverse
+ * y pass, z inverse with p.q, CG update), ms_out[6]; fp32 = 1 times the mixed
+ * form's FP32 kernels.  Leaves the Krylov vectors in an unspecified state.
+ * No counterpart in the reference. */
+MGK_API int mgk_fs3d_profile(mgk_fs3d_t plan, int fp32, int reps, float* ms_out, mgk_stream_t stream);
 
 /* ------------------------------------------------------ 2D STZ / KMC --- */
 /* mgkmc/kmc_simulator_functions.py:100-160 compute_barrier_2d (in place on Q).

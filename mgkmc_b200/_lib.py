@@ -75,6 +75,7 @@ _SIGS = {
     "mgk_fs3d_create": (c_int, [c_int, c_int, c_int, c_int, POINTER(c_void_p)]),
     "mgk_fs3d_destroy": (c_int, [_P]),
     "mgk_fs3d_set_precision": (c_int, [_P, c_int]),
+    "mgk_fs3d_profile": (c_int, [_P, c_int, c_int, POINTER(ctypes.c_float), _P]),
     "mgk_fs3d_set_material": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_fs3d_set_F": (c_int, [_P, _P, _P]),
     "mgk_fs3d_step": (c_int, [_P, POINTER(c_double), c_int, c_int, POINTER(c_double), POINTER(c_int), c_double,

@@ -75,7 +75,15 @@ struct FsArgs {
   float* q32;
   float* r32;
   float* x32;
+  // tangent state at the current F (kFsState planes), FP64 and FP32
+  double* st64;
+  float* st32;
 };
+
+// Tangent state planes: Fe (9), S_ref (6: 00 11 22 12 02 01), C^-1 (6, same
+// order; Neo-Hookean only), lambda, c (mu - lambda ln Je for Neo-Hookean, mu
+// for SVK), F_p flag (1 where F_p^-1 is not the identity).
+constexpr int kFsState = 24;
 
 // the planes and FFT tables a matvec of precision T reads
 template <typename T> struct FsP;
@@ -88,6 +96,7 @@ template <> struct FsP<double> {
   static __device__ __forceinline__ double* q(const FsArgs& a) { return a.q; }
   static __device__ __forceinline__ double* r(const FsArgs& a) { return a.r; }
   static __device__ __forceinline__ double* x(const FsArgs& a) { return a.x; }
+  static __device__ __forceinline__ double* st(const FsArgs& a) { return a.st64; }
   static __device__ __forceinline__ double2* spec(const FsArgs& a) { return a.spec; }
   static __device__ __forceinline__ const FftLen& fx(const FsArgs& a) { return a.fx; }
   static __device__ __forceinline__ const FftLen& fy(const FsArgs& a) { return a.fy; }
@@ -102,6 +111,7 @@ template <> struct FsP<float> {
   static __device__ __forceinline__ float* q(const FsArgs& a) { return a.q32; }
   static __device__ __forceinline__ float* r(const FsArgs& a) { return a.r32; }
   static __device__ __forceinline__ float* x(const FsArgs& a) { return a.x32; }
+  static __device__ __forceinline__ float* st(const FsArgs& a) { return a.st32; }
   static __device__ __forceinline__ float2* spec(const FsArgs& a) { return reinterpret_cast<float2*>(a.spec); }
   static __device__ __forceinline__ const FftLen& fx(const FsArgs& a) { return a.fx32; }
   static __device__ __forceinline__ const FftLen& fy(const FsArgs& a) { return a.fy32; }
@@ -226,6 +236,83 @@ struct VoxelLaw {
   }
 };
 
+// symmetric 3x3 from its 6 stored components (00 11 22 12 02 01)
+template <typename T> __device__ __forceinline__ void sym_load(const T* st, long long N, int off, long long i, T* M) {
+  const T a00 = st[(off + 0) * N + i], a11 = st[(off + 1) * N + i], a22 = st[(off + 2) * N + i];
+  const T a12 = st[(off + 3) * N + i], a02 = st[(off + 4) * N + i], a01 = st[(off + 5) * N + i];
+  M[0] = a00; M[1] = a01; M[2] = a02;
+  M[3] = a01; M[4] = a11; M[5] = a12;
+  M[6] = a02; M[7] = a12; M[8] = a22;
+}
+
+// Tangent state of voxel i at F (FP64 law), stored in precision T.
+template <typename T>
+__global__ void fs_tangent_kernel(FsArgs a, T* __restrict__ st) {
+  const long long N = a.N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    double F[9];
+    for (int q = 0; q < 9; ++q) F[q] = a.F[q * N + i];
+    VoxelLaw<double> law;
+    law.init(a, i, F, 0.0, nullptr);
+    for (int q = 0; q < 9; ++q) st[q * N + i] = (T)law.Fe[q];
+    const int sidx[6] = {0, 4, 8, 5, 2, 1};
+    for (int k = 0; k < 6; ++k) st[(9 + k) * N + i] = (T)law.Sref[sidx[k]];
+    if (law.model == 1)
+      for (int k = 0; k < 6; ++k) st[(15 + k) * N + i] = (T)law.Ci[sidx[k]];
+    st[21 * N + i] = (T)law.lam;
+    st[22 * N + i] = (T)(law.model == 1 ? law.c : law.mu);
+    bool ident = true;
+    for (int q = 0; q < 9; ++q) ident = ident && law.Fpi[q] == ((q % 4 == 0) ? 1.0 : 0.0);
+    st[23 * N + i] = (T)(ident ? 0 : 1);
+  }
+}
+
+// trans2(K4 : trans2(d)) from the tangent state (the kdf of VoxelLaw with
+// Fe, S_ref, C^-1 precomputed; F_p^-1 read only where the flag is set).
+template <typename T>
+__device__ __forceinline__ void kdf_state(const FsArgs& a, long long i, const T* d, T* out) {
+  const long long N = a.N;
+  const T* st = FsP<T>::st(a);
+  T Fe[9], Sref[9], X[9], Tm[9], Y[9];
+  for (int q = 0; q < 9; ++q) Fe[q] = st[q * N + i];
+  sym_load(st, N, 9, i, Sref);
+  const T lam = st[21 * N + i], c = st[22 * N + i];
+  const bool fp = a.has_fp && st[23 * N + i] != T(0);
+  T Fpi[9];
+  if (fp) {
+    const T* fpp = FsP<T>::Fpi(a);
+    for (int q = 0; q < 9; ++q) Fpi[q] = fpp[q * N + i];
+  }
+  mtm(Fe, d, Tm);
+  if (fp) mm(Tm, Fpi, X);
+  else for (int q = 0; q < 9; ++q) X[q] = Tm[q];
+  if (a.model == 0) {
+    const T tr = X[0] + X[4] + X[8];
+    for (int r = 0; r < 3; ++r)
+      for (int s2 = 0; s2 < 3; ++s2) Y[3 * r + s2] = c * (X[3 * r + s2] + X[3 * s2 + r]) + (r == s2 ? lam * tr : T(0));
+  } else {
+    T Ci[9], CX[9], Xs[9], U[9];
+    sym_load(st, N, 15, i, Ci);
+    mm(Ci, X, CX);
+    const T tr = CX[0] + CX[4] + CX[8];
+    for (int r = 0; r < 3; ++r)
+      for (int s2 = 0; s2 < 3; ++s2) Xs[3 * r + s2] = X[3 * r + s2] + X[3 * s2 + r];
+    mm(Ci, Xs, U);
+    mm(U, Ci, Xs);
+    for (int q = 0; q < 9; ++q) Y[q] = lam * tr * Ci[q] + c * Xs[q];
+  }
+  T A[9], B[9];
+  mmt(Sref, d, A);  // S_ref d^T
+  if (fp) { mm(Fpi, Y, Tm); mmt(Tm, Fe, B); }
+  else mmt(Y, Fe, B);
+  if (a.has_fp) {
+    for (int q = 0; q < 9; ++q) out[q] = A[q] + B[q];
+  } else {
+    for (int r = 0; r < 3; ++r)
+      for (int s2 = 0; s2 < 3; ++s2) out[3 * r + s2] = A[3 * s2 + r] + B[3 * s2 + r];
+  }
+}
+
 __device__ __forceinline__ int ffq(int k, int n) { return (k < (n + 1) / 2) ? k : k - n; }
 
 // ----------------------------------------------------------- kernels ---
@@ -246,7 +333,6 @@ __global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __
   const double beta = MODE == 0 ? a.sc->beta : 0.0;
   T* pp = FsP<T>::p(a);
   const T* rr = FsP<T>::r(a);
-  const T* Fp = FsP<T>::F(a);
   for (int z = threadIdx.x; z < nz; z += blockDim.x) {
     T out[2][9];
     for (int h = 0; h < 2; ++h) {
@@ -265,11 +351,7 @@ __global__ void __launch_bounds__(256) fs_zfwd_kernel(FsArgs a, const double* __
         } else {
           for (int q = 0; q < 9; ++q) d[q] = (T)dbar[q];
         }
-        T F[9];
-        for (int q = 0; q < 9; ++q) F[q] = Fp[q * N + i];
-        VoxelLaw<T> law;
-        law.init(a, i, F, T(0), nullptr);
-        law.kdf(d, out[h]);
+        kdf_state<T>(a, i, d, out[h]);
       }
     }
     for (int q = 0; q < 9; ++q) bufA[q * nz + z] = mk<C>(out[0][q], out[1][q]);
@@ -426,7 +508,7 @@ __global__ void __launch_bounds__(256) fs_xg_kernel(FsArgs a) {
 // CG update: x += alpha p; r -= alpha q (the Krylov vectors in the matvec
 // precision, FP64 arithmetic and sums); partial r.r
 template <typename T>
-__global__ void fs_update_kernel(FsArgs a) {
+__global__ void __launch_bounds__(256) fs_update_kernel(FsArgs a) {
   __shared__ double red[32];
   const double alpha = a.sc->alpha;
   const long long n9 = 9 * a.N;
@@ -435,7 +517,38 @@ __global__ void fs_update_kernel(FsArgs a) {
   T* xx = FsP<T>::x(a);
   T* rr = FsP<T>::r(a);
   double acc = 0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9; i += (long long)gridDim.x * blockDim.x) {
+  long long start = 0;
+  if constexpr (sizeof(T) == 4) {
+    // FP32 vectors: four elements per access (16-byte aligned planes)
+    const bool vec = ((reinterpret_cast<uintptr_t>(pp) | reinterpret_cast<uintptr_t>(qq) |
+                       reinterpret_cast<uintptr_t>(xx) | reinterpret_cast<uintptr_t>(rr)) & 15) == 0;
+    if (vec) {
+      const long long n4 = n9 / 4;
+      const float4* p4 = reinterpret_cast<const float4*>(pp);
+      const float4* q4 = reinterpret_cast<const float4*>(qq);
+      float4* x4 = reinterpret_cast<float4*>(xx);
+      float4* r4 = reinterpret_cast<float4*>(rr);
+      for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
+           i += (long long)gridDim.x * blockDim.x) {
+        const float4 pv = p4[i], qv = q4[i];
+        float4 xv = x4[i], rv = r4[i];
+        xv.x = (float)((double)xv.x + alpha * (double)pv.x);
+        xv.y = (float)((double)xv.y + alpha * (double)pv.y);
+        xv.z = (float)((double)xv.z + alpha * (double)pv.z);
+        xv.w = (float)((double)xv.w + alpha * (double)pv.w);
+        rv.x = (float)((double)rv.x - alpha * (double)qv.x);
+        rv.y = (float)((double)rv.y - alpha * (double)qv.y);
+        rv.z = (float)((double)rv.z - alpha * (double)qv.z);
+        rv.w = (float)((double)rv.w - alpha * (double)qv.w);
+        x4[i] = xv;
+        r4[i] = rv;
+        acc += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+      }
+      start = 4 * n4;
+    }
+  }
+  for (long long i = start + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9;
+       i += (long long)gridDim.x * blockDim.x) {
     xx[i] = (T)((double)xx[i] + alpha * (double)pp[i]);
     const T rn = (T)((double)rr[i] - alpha * (double)qq[i]);
     rr[i] = rn;
@@ -593,6 +706,30 @@ __global__ void fs_cauchy_kernel(const double* __restrict__ P, const double* __r
   }
 }
 
+// Krylov direction and tangent product, per voxel: p = r + beta p (p = r
+// when beta = 0), A = K:p from the tangent state, A written to the q planes
+// (free until the inverse z pass writes q).  Elementwise at full occupancy;
+// the z forward pass (MODE 3) then only transforms A.
+template <typename T>
+__global__ void __launch_bounds__(256) fs_kp_kernel(FsArgs a) {
+  const long long N = a.N;
+  const double beta = a.sc->beta;
+  T* pp = FsP<T>::p(a);
+  const T* rr = FsP<T>::r(a);
+  T* qq = FsP<T>::q(a);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+    T d[9], out[9];
+    for (int q = 0; q < 9; ++q) {
+      const double rv = (double)rr[q * N + i];
+      const T pn = beta == 0.0 ? (T)rv : (T)(rv + beta * (double)pp[q * N + i]);
+      pp[q * N + i] = pn;
+      d[q] = pn;
+    }
+    kdf_state<T>(a, i, d, out);
+    for (int q = 0; q < 9; ++q) qq[q * N + i] = out[q];
+  }
+}
+
 // ------------------------------------------------- warp-line 3D passes ---
 // The same five matvec stages for grids whose sides are 64, 96 or 128 (the
 // served and benchmark sizes): lines sit in padded shared memory and
@@ -696,7 +833,8 @@ __global__ void __launch_bounds__(9 * 32, sizeof(T) == 8 ? 1 : 3) fs_axis_fast_k
 }
 
 // z forward: per-voxel stage (MODE 0: p = r + beta p and K:p; 1: K:dbar;
-// 2: P), R2C along z of the pair of z-lines, 9 components.
+// 2: P; 3: A from the q planes, written by fs_kp_kernel), R2C along z of the
+// pair of z-lines, 9 components.
 template <int MODE, typename T, int NZ>
 __device__ __forceinline__ void fs_zfwd_body(const FsArgs& a, const double* __restrict__ dbar, unsigned char* smem) {
   using C = C_t<T>;
@@ -711,13 +849,15 @@ __device__ __forceinline__ void fs_zfwd_body(const FsArgs& a, const double* __re
   const double beta = MODE == 0 ? a.sc->beta : 0.0;
   T* pp = FsP<T>::p(a);
   const T* rr = FsP<T>::r(a);
-  const T* Fp = FsP<T>::F(a);
   for (int z = threadIdx.x; z < NZ; z += 3 * 32) {
     T out[2][9];
     for (int h = 0; h < 2; ++h) {
       const long long i = (l0 + h) * NZ + z;
       if (MODE == 2) {
         for (int q = 0; q < 9; ++q) out[h][q] = (T)a.P[q * N + i];
+      } else if (MODE == 3) {
+        const T* qq = FsP<T>::q(a);
+        for (int q = 0; q < 9; ++q) out[h][q] = qq[q * N + i];
       } else {
         T d[9];
         if (MODE == 0) {
@@ -730,11 +870,7 @@ __device__ __forceinline__ void fs_zfwd_body(const FsArgs& a, const double* __re
         } else {
           for (int q = 0; q < 9; ++q) d[q] = (T)dbar[q];
         }
-        T F[9];
-        for (int q = 0; q < 9; ++q) F[q] = Fp[q * N + i];
-        VoxelLaw<T> law;
-        law.init(a, i, F, T(0), nullptr);
-        law.kdf(d, out[h]);
+        kdf_state<T>(a, i, d, out[h]);
       }
     }
     const int pz = pidx<C>(z);
@@ -899,6 +1035,8 @@ struct mgk_fs3d_plan {
   float* f32 = nullptr;  // F32, Fpi32, lam32, mu32, p32, q32
   float *F32 = nullptr, *Fpi32 = nullptr, *lam32 = nullptr, *mu32 = nullptr, *p32 = nullptr, *q32 = nullptr;
   float *r32 = nullptr, *x32 = nullptr;
+  double* st64 = nullptr;  // tangent state planes (kFsState each)
+  float* st32 = nullptr;
   FftLen fx32, fy32, fz32;
   // device-side Krylov loop graphs, one per matvec precision (0 FP64, 1 FP32)
   cudaGraph_t cg_graph[2] = {nullptr, nullptr};
@@ -919,6 +1057,7 @@ static FsArgs fs_args(mgk_fs3d_t p) {
   a.fx32 = p->fx32; a.fy32 = p->fy32; a.fz32 = p->fz32;
   a.F32 = p->F32; a.Fpi32 = p->Fpi32; a.mu32 = p->mu32; a.lam32 = p->lam32; a.p32 = p->p32; a.q32 = p->q32;
   a.r32 = p->r32; a.x32 = p->x32;
+  a.st64 = p->st64; a.st32 = p->st32;
   return a;
 }
 
@@ -929,6 +1068,8 @@ extern "C" int mgk_fs3d_destroy(mgk_fs3d_t p) {
     if (p->cg_graph[k]) cudaGraphDestroy(p->cg_graph[k]);
   }
   cudaFree(p->f32);
+  cudaFree(p->st64);
+  cudaFree(p->st32);
   cudaFree(p->fields);
   cudaFree(p->spec);
   cudaFree(p->part);
@@ -968,6 +1109,7 @@ extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* ou
   p->F = f; p->Ftr = f + 9 * N; p->Fpi = f + 18 * N; p->lam = f + 27 * N; p->mu = f + 28 * N;
   p->P = f + 29 * N; p->Ptr = f + 38 * N; p->x = f + 47 * N; p->r = f + 56 * N; p->p = f + 65 * N; p->q = f + 74 * N;
   if (cudaMalloc(&p->spec, 9 * (size_t)nx * ny * p->ld * sizeof(double2)) != cudaSuccess) { cudaGetLastError(); return fail(MGK_OOM); }
+  if (cudaMalloc(&p->st64, sizeof(double) * kFsState * N) != cudaSuccess) { cudaGetLastError(); return fail(MGK_OOM); }
   p->nblk = (int)std::max(1LL, std::min(1024LL, (N + 255) / 256));
   const size_t npart = std::max((size_t)16 * p->nblk, (size_t)((long long)nx * ny / 2 + 16));
   const size_t npart2 = std::max(npart, (size_t)(9 * N / 256 + 64));
@@ -1009,6 +1151,8 @@ extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* ou
         raise_smem((const void*)fs_zfwd_fast_kernel<1, double>, zs64) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<2, double>, zs64) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<0, float>, zs32) ||
+        raise_smem((const void*)fs_zfwd_fast_kernel<3, double>, zs64) ||
+        raise_smem((const void*)fs_zfwd_fast_kernel<3, float>, zs32) ||
         raise_smem((const void*)fs_zinv_fast_kernel<0, double>, zs64) ||
         raise_smem((const void*)fs_zinv_fast_kernel<1, double>, zs64) ||
         raise_smem((const void*)fs_zinv_fast_kernel<0, float>, zs32) ||
@@ -1035,16 +1179,21 @@ static void fs_drop_graphs(mgk_fs3d_t p) {
   }
 }
 
-// FP32 copies of F, F_p^-1 and the moduli for the mixed form's matvecs
+// FP32 copy of F_p^-1 for the mixed form's matvecs (read where the tangent
+// state flags a non-identity F_p)
 static int fs_refresh_f32(mgk_fs3d_t p, bool material, cudaStream_t s) {
-  if (p->prec != MGK_MIXED) return MGK_OK;
-  const long long N = p->N;
-  fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(9 * N, p->F, p->F32);
-  if (material) {
-    if (p->has_fp) fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(9 * N, p->Fpi, p->Fpi32);
-    fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(N, p->lam, p->lam32);
-    fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(N, p->mu, p->mu32);
-  }
+  if (p->prec != MGK_MIXED || !material || !p->has_fp) return MGK_OK;
+  fs_to_f32_kernel<<<p->nblk, 256, 0, s>>>(9 * p->N, p->Fpi, p->Fpi32);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+// tangent state at the current F (once per accepted Newton iterate; every
+// Krylov matvec of the next Newton step reads it)
+static int fs_tangent(mgk_fs3d_t p, cudaStream_t s) {
+  FsArgs a = fs_args(p);
+  fs_tangent_kernel<double><<<p->nblk, 256, 0, s>>>(a, p->st64);
+  if (p->prec == MGK_MIXED) fs_tangent_kernel<float><<<p->nblk, 256, 0, s>>>(a, p->st32);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }
@@ -1062,6 +1211,11 @@ extern "C" int mgk_fs3d_set_precision(mgk_fs3d_t p, int precision) {
     float* f = p->f32;
     p->F32 = f; p->Fpi32 = f + 9 * N; p->lam32 = f + 18 * N; p->mu32 = f + 19 * N; p->p32 = f + 20 * N;
     p->q32 = f + 29 * N; p->r32 = f + 38 * N; p->x32 = f + 47 * N;
+    if (cudaMalloc(&p->st32, sizeof(float) * kFsState * N) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("mgk_fs3d_set_precision: cudaMalloc of the FP32 tangent state failed");
+      return MGK_OOM;
+    }
     p->fx32 = p->fx; p->fy32 = p->fy; p->fz32 = p->fz;
     p->fx32.tw = twiddles(p->nx, 1); p->fy32.tw = twiddles(p->ny, 1); p->fz32.tw = twiddles(p->nz, 1);
     if (!p->fx32.tw || !p->fy32.tw || !p->fz32.tw) return MGK_OOM;
@@ -1113,48 +1267,58 @@ struct FsLaunch {
   void* fn;
   dim3 grid, block;
   size_t smem;
+  int args;  // 0: (FsArgs), 1: (FsArgs, dbar)
 };
+// returns the number of launches (5, or 6 when the tangent product runs as
+// its own elementwise kernel)
 template <typename T>
-static void fs_stage_launches(mgk_fs3d_t p, int mode, int zmode, FsLaunch L[5]) {
+static int fs_stage_launches(mgk_fs3d_t p, int mode, int zmode, FsLaunch L[6]) {
   const int zl = (int)(p->N / p->nz / 2);
+  int k = 0;
   if (p->fast) {
     const int csz = (int)sizeof(C_t<T>);
     const int ntile = (p->nzh + kFsTile - 1) / kFsTile;
     const size_t zs = 9 * (size_t)fs_pl(p->nz, csz) * csz, zs64 = 9 * (size_t)fs_pl(p->nz, 16) * 16;
     const size_t ys = 9 * (size_t)kFsTile * fs_pl(p->ny, csz) * csz;
     const size_t xs = 9 * (size_t)kFsTile * fs_pl(p->nx, csz) * csz;
-    L[0] = {mode == 0 ? (void*)fs_zfwd_fast_kernel<0, T>
-                      : (mode == 1 ? (void*)fs_zfwd_fast_kernel<1, double> : (void*)fs_zfwd_fast_kernel<2, double>),
-            dim3(zl), dim3(96), mode == 0 ? zs : zs64};
-    L[1] = {(void*)fs_axis_fast_kernel<-1, T, false>, dim3(p->nx * ntile), dim3(288), ys};
-    L[2] = {(void*)fs_axis_fast_kernel<-1, T, true>, dim3(p->ny * ntile), dim3(288), xs};
-    L[3] = {(void*)fs_axis_fast_kernel<1, T, false>, dim3(p->nx * ntile), dim3(288), ys};
-    L[4] = {zmode == 0 ? (void*)fs_zinv_fast_kernel<0, T> : (void*)fs_zinv_fast_kernel<1, double>, dim3(zl), dim3(96),
-            zmode == 0 ? zs : zs64};
+    if (mode == 0) {
+      L[k++] = {(void*)fs_kp_kernel<T>, dim3(4 * p->nblk), dim3(256), 0, 0};
+      L[k++] = {(void*)fs_zfwd_fast_kernel<3, T>, dim3(zl), dim3(96), zs, 1};
+    } else {
+      L[k++] = {mode == 1 ? (void*)fs_zfwd_fast_kernel<1, double> : (void*)fs_zfwd_fast_kernel<2, double>, dim3(zl),
+                dim3(96), zs64, 1};
+    }
+    L[k++] = {(void*)fs_axis_fast_kernel<-1, T, false>, dim3(p->nx * ntile), dim3(288), ys, 0};
+    L[k++] = {(void*)fs_axis_fast_kernel<-1, T, true>, dim3(p->ny * ntile), dim3(288), xs, 0};
+    L[k++] = {(void*)fs_axis_fast_kernel<1, T, false>, dim3(p->nx * ntile), dim3(288), ys, 0};
+    L[k++] = {zmode == 0 ? (void*)fs_zinv_fast_kernel<0, T> : (void*)fs_zinv_fast_kernel<1, double>, dim3(zl),
+              dim3(96), zmode == 0 ? zs : zs64, 0};
   } else {
     const int ntile = (p->nzh + p->tc - 1) / p->tc;
     const size_t zs = p->zsmem * sizeof(T) / 8, ys = p->ysmem * sizeof(T) / 8, xs = p->xsmem * sizeof(T) / 8;
-    L[0] = {mode == 0 ? (void*)fs_zfwd_kernel<0, T>
-                      : (mode == 1 ? (void*)fs_zfwd_kernel<1, double> : (void*)fs_zfwd_kernel<2, double>),
-            dim3(zl), dim3(256), mode == 0 ? zs : p->zsmem};
-    L[1] = {(void*)fs_ypass_kernel<-1, T>, dim3(p->nx * ntile), dim3(256), ys};
-    L[2] = {(void*)fs_xg_kernel<T>, dim3(p->ny * ntile), dim3(256), xs};
-    L[3] = {(void*)fs_ypass_kernel<1, T>, dim3(p->nx * ntile), dim3(256), ys};
-    L[4] = {zmode == 0 ? (void*)fs_zinv_kernel<0, T> : (void*)fs_zinv_kernel<1, double>, dim3(zl), dim3(256),
-            zmode == 0 ? zs : p->zsmem};
+    L[k++] = {mode == 0 ? (void*)fs_zfwd_kernel<0, T>
+                        : (mode == 1 ? (void*)fs_zfwd_kernel<1, double> : (void*)fs_zfwd_kernel<2, double>),
+              dim3(zl), dim3(256), mode == 0 ? zs : p->zsmem, 1};
+    L[k++] = {(void*)fs_ypass_kernel<-1, T>, dim3(p->nx * ntile), dim3(256), ys, 0};
+    L[k++] = {(void*)fs_xg_kernel<T>, dim3(p->ny * ntile), dim3(256), xs, 0};
+    L[k++] = {(void*)fs_ypass_kernel<1, T>, dim3(p->nx * ntile), dim3(256), ys, 0};
+    L[k++] = {zmode == 0 ? (void*)fs_zinv_kernel<0, T> : (void*)fs_zinv_kernel<1, double>, dim3(zl), dim3(256),
+              zmode == 0 ? zs : p->zsmem, 0};
   }
+  return k;
 }
 
 // one matvec / projection in precision T: zfwd<MODE> -> y -> xG -> y^-1 -> zinv<ZMODE>
 template <typename T>
 static int fs_project(mgk_fs3d_t p, int mode, int zmode, cudaStream_t s) {
   FsArgs a = fs_args(p);
-  FsLaunch L[5];
-  fs_stage_launches<T>(p, mode, zmode, L);
+  FsLaunch L[6];
+  const int nl = fs_stage_launches<T>(p, mode, zmode, L);
   const double* dbar = p->dbar;
   void* az[] = {&a, (void*)&dbar};
   void* a1[] = {&a};
-  for (int k = 0; k < 5; ++k) MGK_CUDA(cudaLaunchKernel(L[k].fn, L[k].grid, L[k].block, k == 0 ? az : a1, L[k].smem, s));
+  for (int k = 0; k < nl; ++k)
+    MGK_CUDA(cudaLaunchKernel(L[k].fn, L[k].grid, L[k].block, L[k].args ? az : a1, L[k].smem, s));
   return MGK_OK;
 }
 
@@ -1174,11 +1338,11 @@ static int fs_trial(mgk_fs3d_t p, double alpha, bool use_dbar, bool use_x, cudaS
 }
 
 // accept the trial state: copies (the plane addresses stay fixed, so the
-// Krylov graphs stay valid), and the FP32 copy of F for mixed matvecs
+// Krylov graphs stay valid), and the tangent state at the new F
 static int fs_accept(mgk_fs3d_t p, cudaStream_t s) {
   MGK_CUDA(cudaMemcpyAsync(p->F, p->Ftr, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
   MGK_CUDA(cudaMemcpyAsync(p->P, p->Ptr, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
-  return fs_refresh_f32(p, false, s);
+  return fs_tangent(p, s);
 }
 
 // Krylov loop graph for matvec precision T: scalar<2> (norm of the
@@ -1225,12 +1389,12 @@ static int fs_build_graph(mgk_fs3d_t p, int slot) {
   void* a_1[] = {&a};
   void* a_s0[] = {&a, (void*)&zl, &h, &one};
   void* a_s1[] = {&a, &nb, &h, &one};
-  cudaGraphNode_t kn[5], k6, k7, k8;
-  FsLaunch L[5];
-  fs_stage_launches<T>(p, 0, 0, L);
-  for (int k = 0; k < 5; ++k)
-    add(body, &kn[k], k ? &kn[k - 1] : nullptr, L[k].fn, L[k].grid, L[k].block, L[k].smem, k == 0 ? a_z : a_1);
-  add(body, &k6, &kn[4], (void*)fs_scalar_kernel<0>, dim3(1), dim3(256), 0, a_s0);
+  cudaGraphNode_t kn[6], k6, k7, k8;
+  FsLaunch L[6];
+  const int nl = fs_stage_launches<T>(p, 0, 0, L);
+  for (int k = 0; k < nl; ++k)
+    add(body, &kn[k], k ? &kn[k - 1] : nullptr, L[k].fn, L[k].grid, L[k].block, L[k].smem, L[k].args ? a_z : a_1);
+  add(body, &k6, &kn[nl - 1], (void*)fs_scalar_kernel<0>, dim3(1), dim3(256), 0, a_s0);
   add(body, &k7, &k6, (void*)fs_update_kernel<T>, dim3(p->nblk), dim3(256), 0, a_1);
   add(body, &k8, &k7, (void*)fs_scalar_kernel<1>, dim3(1), dim3(256), 0, a_s1);
   cudaGraphExec_t x = nullptr;
@@ -1349,6 +1513,51 @@ static int fs_newton(mgk_fs3d_t p, const double* F_bar, double tol_NW, double to
   }
   set_error("Newton-CG inner solver did not converge within %d iterations.", max_NW);
   return MGK_NOT_CONVERGED;
+}
+
+// Timing hook: mean duration (ms, CUDA events on `stream`) of each kernel
+// of one Krylov iteration in the plan's kernel family: [0] z forward (p
+// update + K:p + R2C), [1] y pass, [2] x pass with G, [3] inverse y pass,
+// [4] z inverse (C2R + p.q), [5] CG update.  fp32 = 1 times the mixed form's
+// FP32 kernels.  Runs `reps` iterations on the current state and leaves the
+// Krylov vectors in an unspecified state.
+extern "C" int mgk_fs3d_profile(mgk_fs3d_t p, int fp32, int reps, float* ms_out, mgk_stream_t stream) {
+  MGK_REQUIRE(p && ms_out && reps >= 1 && p->has_material, "mgk_fs3d_profile: bad argument");
+  MGK_REQUIRE(!fp32 || p->prec == MGK_MIXED, "mgk_fs3d_profile: fp32 needs a mixed-precision plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  FsArgs a = fs_args(p);
+  FsLaunch L[6];
+  const int nl = fp32 ? fs_stage_launches<float>(p, 0, 0, L) : fs_stage_launches<double>(p, 0, 0, L);
+  // with a separate tangent-product kernel its time is folded into the z forward entry
+  const int first = nl - 5;
+  const double* dbar = p->dbar;
+  void* az[] = {&a, (void*)&dbar};
+  void* a1[] = {&a};
+  cudaEvent_t ev[7];
+  for (int i = 0; i < 7; ++i) MGK_CUDA(cudaEventCreate(&ev[i]));
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int rc = MGK_OK;
+  for (int r = 0; r < reps && rc == MGK_OK; ++r) {
+    cudaEventRecord(ev[0], s);
+    for (int k = 0; k < nl; ++k) {
+      if (cudaLaunchKernel(L[k].fn, L[k].grid, L[k].block, L[k].args ? az : a1, L[k].smem, s) != cudaSuccess)
+        rc = MGK_CUDA_ERROR;
+      if (k >= first) cudaEventRecord(ev[k - first + 1], s);
+    }
+    if (fp32) fs_update_kernel<float><<<p->nblk, 256, 0, s>>>(a);
+    else fs_update_kernel<double><<<p->nblk, 256, 0, s>>>(a);
+    cudaEventRecord(ev[6], s);
+    if (cudaEventSynchronize(ev[6]) != cudaSuccess) rc = MGK_CUDA_ERROR;
+    for (int k = 0; k < 6; ++k) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      acc[k] += ms;
+    }
+  }
+  for (int i = 0; i < 7; ++i) cudaEventDestroy(ev[i]);
+  if (rc != MGK_OK) { cudaGetLastError(); set_error("mgk_fs3d_profile: kernel failure"); return rc; }
+  for (int k = 0; k < 6; ++k) ms_out[k] = (float)(acc[k] / reps);
+  return MGK_OK;
 }
 
 extern "C" int mgk_fs3d_step(mgk_fs3d_t p, const double* F_bar_in, int drv_i, int drv_j, const double* P_target,

@@ -105,6 +105,14 @@ class Fs3dSolver:
         L.check(st, "mgk_fs3d_step")
         return np.array(out[:]).reshape(3, 3), self.info
 
+    def profile_kernels(self, fp32=False, reps=20, stream=None):
+        """Mean ms of the six kernels of one Krylov iteration (z fwd, y, x+G,
+        y inv, z inv, update); leaves the Krylov vectors unspecified."""
+        ms = (ctypes.c_float * 6)()
+        L.check(L.lib().mgk_fs3d_profile(self._h, 1 if fp32 else 0, int(reps), ms, L.stream_ptr(stream)),
+                "mgk_fs3d_profile")
+        return list(ms)
+
     def get(self, F_out=None, P_out=None, sig_out=None, stream=None):
         L.check(L.lib().mgk_fs3d_get(self._h, L.ptr(F_out), L.ptr(P_out), L.ptr(sig_out), L.stream_ptr(stream)),
                 "mgk_fs3d_get")

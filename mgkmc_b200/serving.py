@@ -447,7 +447,9 @@ class Server:
                     send = None
                     while True:
                         try:
-                            need = gen.send(send)
+                            # the request's own work (inputs, KMC kernels) on the plan's stream
+                            with torch.cuda.stream(b.stream):
+                                need = gen.send(send)
                         except StopIteration as stop:
                             out = stop.value
                             break
