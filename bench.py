@@ -17,6 +17,9 @@ Neo-Hookean ramp of the finite-strain workload in the plain FP64 form and the
 mixed form (FP32 Krylov matvecs), device-timed, with the mixed form's field
 error and the per-kernel times of one Krylov iteration.
 
+Ensemble block (``--ensemble 96``, off by default: about a minute): the
+batched KMC ensemble, events/s and replica-solves/s.
+
 Serving block (N = 1, ``--serve-window`` seconds of the serving stream): the
 continuous-batching server in mixed precision against the plain FP64 form
 served one request at a time, both on this GPU with arrivals replayed in real
@@ -59,6 +62,8 @@ def parse():
                     help="comma list of forms to time (the headline is batched_mixed)")
     ap.add_argument("--fs-grid", type=int, default=128,
                     help="side of the finite-strain block (Neo-Hookean + F_p, 10 load steps); 0 skips it")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="replicas of the batched KMC ensemble block (96 = the ensemble workload, ~1 min); 0 skips it")
     ap.add_argument("--serve-window", type=float, default=0.1,
                     help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
                          "0 skips it")
@@ -401,6 +406,13 @@ def run_ours(a):
     finite_strain = None
     if world == 1 and a.fs_grid > 0:
         finite_strain = run_finite_strain(a.fs_grid, peak)
+    ensemble = None
+    if world == 1 and a.ensemble > 0:
+        from mgkmc_b200.serving import ensemble_requests, run_ensemble
+        _, ensemble = run_ensemble(ensemble_requests(n_replicas=a.ensemble, n_events=500))
+        ensemble["workload"] = (f"{a.ensemble} 2D KMC/AQS replicas, sides uniform in {{128,192,256,384,512}}, "
+                                f"T uniform in [200, 400] K, seeds 0..{a.ensemble - 1}, 500 events each, mixed form, "
+                                f"one batched solve launch per size per round")
     serving = None
     if world == 1 and a.serve_window > 0:
         serving = run_serving(a.serve_window)
@@ -421,7 +433,7 @@ def run_ours(a):
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.Ls2dBatch"},
             "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "finite_strain": finite_strain, "serving": serving}
+            "finite_strain": finite_strain, "serving": serving, "ensemble": ensemble}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -59,6 +59,8 @@ class Request:
     dim: int          # 2 | 3
     n: int            # grid side
     seed: int
+    T: float = None   # KMC temperature (K); None: the server's
+    n_events: int = None  # events of a trajectory; None: the server's
 
 
 def request_stream(rate=200.0, duration=60.0, seed=3, p_traj=0.4, p_3d=0.3, sizes_2d=SIZES_2D,
@@ -223,11 +225,11 @@ class Server:
         n, M = req.n, self.n_modes
         E, nu, _, _ = W.ls2d_problem_dev(n, n, req.seed, self.dev)
         cat, Q0 = W.kmc2d_state_dev(n, n, M, req.seed, self.dev, q_mean=self.q_mean)
-        k = Kmc2D(E, nu, cat, Q0, T=self.kmc_T, q_mean=self.q_mean, ls_tol=self.ls_tol,
+        k = Kmc2D(E, nu, cat, Q0, T=self.kmc_T if req.T is None else req.T, q_mean=self.q_mean, ls_tol=self.ls_tol,
                   ls_max_iter=self.ls_max_iter, selection=self.selection, ls_start=self.ls_start,
                   precision=self.precision, ls=b.plan, rep=slot, stream=b.stream)
         rng = np.random.default_rng(req.seed)
-        gen = k.trajectory(rng, 10 ** 9, max_events=self.n_events)
+        gen = k.trajectory(rng, 10 ** 9, max_events=self.n_events if req.n_events is None else req.n_events)
         send = None
         while True:
             try:
@@ -463,6 +465,37 @@ class Server:
                 self._finish(res, out)
             except ValueError as e:
                 self._finish(res, error=str(e))
+
+
+def ensemble_requests(n_replicas=96, sizes=(128, 192, 256, 384, 512), T_range=(200.0, 400.0), n_events=500,
+                      seed=0):
+    """The batched KMC ensemble: replica k has seed k, a side drawn uniformly
+    from `sizes` and a temperature uniform in `T_range`, all arriving at once."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_replicas):
+        n = int(rng.choice(sizes))
+        T = float(rng.uniform(*T_range))
+        out.append(Request(k, 0.0, "trajectory", 2, n, k, T=T, n_events=n_events))
+    return out
+
+
+def run_ensemble(requests, slots=None, **server_kw):
+    """Runs an ensemble through the served form (every replica admitted at
+    once when slots allow; one batched solve launch per size per round) and
+    returns (results, summary with events/s)."""
+    from collections import Counter
+    cnt = Counter(r.n for r in requests)
+    srv = Server(mode="served", slots=slots or {n: c for n, c in cnt.items()}, **server_kw)
+    srv.prepare(requests)
+    t0 = time.perf_counter()
+    res = srv.run(requests, realtime=False, keep_outputs=False)
+    wall = time.perf_counter() - t0
+    ok = [r for r in res if not r.error]
+    events = sum(len(r.out.get("events", ())) for r in ok)
+    solves = sum(r.solves for r in ok)
+    return res, {"replicas": len(requests), "completed": len(ok), "events": events, "solves": solves,
+                 "seconds": wall, "events_per_s": events / wall, "solves_per_s": solves / wall}
 
 
 def summarize(results, window=None):

@@ -71,3 +71,17 @@ def test_summary_fields():
     reqs = [Request(i, 0.001 * i, "solve", 2, 64, i) for i in range(6)]
     s = summarize(Server(mode="served").run(reqs, realtime=True))
     assert s["completed"] == 6 and s["p99_s"] >= s["p50_s"] > 0 and s["solves_per_s"] > 0
+
+
+def test_ensemble_runs_every_replica_to_its_event_count():
+    # a small version of the batched KMC ensemble: mixed sizes and
+    # temperatures, every replica admitted at once, one batched solve per size
+    # per round; each replica reaches its event count, and a replica's
+    # trajectory is the same as when it runs alone
+    from mgkmc_b200.serving import Server, ensemble_requests, run_ensemble
+    reqs = ensemble_requests(n_replicas=5, sizes=(64, 96), T_range=(300.0, 400.0), n_events=4)
+    res, summ = run_ensemble(reqs, q_mean=0.6)
+    assert summ["completed"] == 5 and summ["events"] == 20
+    assert all(len(r.out["events"]) == 4 for r in res)
+    alone = Server(mode="served", n_events=4, q_mean=0.6, slots={64: 1, 96: 1}).run([reqs[2]], realtime=False)[0]
+    assert alone.out["events"] == res[2].out["events"]
