@@ -192,6 +192,9 @@ def run_serving(window):
         srv.prepare(reqs)
         res = srv.run(reqs, realtime=True)
         out[name] = summarize(res)
+    from mgkmc_b200 import serving as SV
+    out["autotuned_ls_families"] = {f"{k[0]}^2 x{k[1]} {k[2]}": {"family": v[0], "ms_per_iteration": v[1]}
+                                    for k, v in SV._TUNED.items()}
     a, b = out["served_mixed"], out["plain_fp64_sequential"]
     if a.get("completed") and b.get("completed"):
         out["solves_per_s_ratio"] = a["solves_per_s"] / b["solves_per_s"]

@@ -107,6 +107,21 @@ MGK_API int mgk_ls2d_solve_batch(mgk_ls2d_t plan, int nsel, const int* sel, cons
                                  double* const* sig_out, int max_iter, double tol, mgk_ls_info* infos,
                                  mgk_stream_t stream);
 
+/* Autotuner: times one iteration of every kernel family that can serve the
+ * plan (warp-line kernels for sides up to 256 / 512 / 1024 with their column
+ * tiles, and the CTA-wide passes with theirs) on the selection, `reps` times
+ * each, and keeps the fastest (FP64 plus FP32 kernels for mixed plans).
+ * *chosen: 0 CTA-wide, or 256/512/1024; *best_ms: its iteration time.  Leaves
+ * the replicas' iterates unspecified (call before solving).  No counterpart in
+ * the reference. */
+MGK_API int mgk_ls2d_autotune(mgk_ls2d_t plan, int nsel, const int* sel, const double* eps_bar, int reps,
+                              int* chosen, float* best_ms, mgk_stream_t stream);
+
+/* Sets the kernel family directly (0 CTA-wide, 256/512/1024 warp-line; at
+ * least the plan's largest side), e.g. one the autotuner chose for an equal
+ * plan.  Synchronises the device.  No counterpart in the reference. */
+MGK_API int mgk_ls2d_set_family(mgk_ls2d_t plan, int family);
+
 /* Results of the last solve of replicas sel[0..nsel) (iterations, status,
  * final diff, mean strain and stress) after a solve_batch call that passed
  * infos = NULL: synchronises `stream` once.  Lets a scheduler launch the
@@ -225,6 +240,12 @@ MGK_API int mgk_fs3d_step(mgk_fs3d_t plan, const double* F_bar_in, int driving_i
 /* Copy out F and P (device, tensor-first) and compute the Cauchy stress
  * (cauchy_from_P_3d :1892-1904); any pointer may be NULL. */
 MGK_API int mgk_fs3d_get(mgk_fs3d_t plan, double* F_out, double* P_out, double* sig_out, mgk_stream_t stream);
+/* Autotuner: times one Krylov iteration of each kernel family that can serve
+ * the plan (warp-line passes, sides 64/96/128; CTA-wide passes) on the current
+ * state and keeps the faster; *chosen 1 warp-line, 0 CTA-wide.  Call after a
+ * step (the state must be valid); leaves the Krylov vectors unspecified.  No
+ * counterpart in the reference. */
+MGK_API int mgk_fs3d_autotune(mgk_fs3d_t plan, int reps, int* chosen, float* best_ms, mgk_stream_t stream);
 /* Timing hook: mean duration (ms, CUDA events on `stream`) of the six kernels
  * of one Krylov iteration (z forward with K:p, y pass, x pass with G, inverse
  * y pass, z inverse with p.q, CG update), ms_out[6]; fp32 = 1 times the mixed

@@ -56,6 +56,9 @@ _SIGS = {
     "mgk_ls2d_create_batch": (c_int, [c_int, POINTER(c_int), POINTER(c_int), c_int, c_int, POINTER(c_void_p)]),
     "mgk_ls2d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
     "mgk_ls2d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
+    "mgk_ls2d_autotune": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), c_int, POINTER(c_int),
+                                  POINTER(ctypes.c_float), _P]),
+    "mgk_ls2d_set_family": (c_int, [_P, c_int]),
     "mgk_ls2d_collect": (c_int, [_P, c_int, POINTER(c_int), POINTER(LsInfo), _P]),
     "mgk_ls2d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
                                      POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo), _P]),
@@ -75,6 +78,7 @@ _SIGS = {
     "mgk_fs3d_create": (c_int, [c_int, c_int, c_int, c_int, POINTER(c_void_p)]),
     "mgk_fs3d_destroy": (c_int, [_P]),
     "mgk_fs3d_set_precision": (c_int, [_P, c_int]),
+    "mgk_fs3d_autotune": (c_int, [_P, c_int, POINTER(c_int), POINTER(ctypes.c_float), _P]),
     "mgk_fs3d_profile": (c_int, [_P, c_int, c_int, POINTER(ctypes.c_float), _P]),
     "mgk_fs3d_set_material": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_fs3d_set_F": (c_int, [_P, _P, _P]),

@@ -1560,6 +1560,33 @@ extern "C" int mgk_fs3d_profile(mgk_fs3d_t p, int fp32, int reps, float* ms_out,
   return MGK_OK;
 }
 
+// Autotuner: times one Krylov iteration of each kernel family that can serve
+// the plan (warp-line passes when every side is 64/96/128, the CTA-wide
+// passes always) on the current state and keeps the faster one.
+extern "C" int mgk_fs3d_autotune(mgk_fs3d_t p, int reps, int* chosen, float* best_ms, mgk_stream_t stream) {
+  MGK_REQUIRE(p && reps >= 1 && p->has_material, "mgk_fs3d_autotune: bad argument");
+  const bool can_fast = fs_fast_len(p->nx) && fs_fast_len(p->ny) && fs_fast_len(p->nz);
+  const int fp32 = p->prec == MGK_MIXED ? 1 : 0;
+  int best = p->fast;
+  float best_t = 0.0f;
+  const int cands[2] = {0, 1};
+  const int k0 = 0, k1 = can_fast ? 2 : 1;
+  for (int k = k0; k < k1; ++k) {
+    p->fast = cands[k];
+    float ms[6];
+    int st = mgk_fs3d_profile(p, fp32, reps, ms, stream);
+    if (st) return st;
+    float t = 0;
+    for (float v : ms) t += v;
+    if (k == k0 || t < best_t) { best_t = t; best = cands[k]; }
+  }
+  p->fast = best;
+  fs_drop_graphs(p);
+  if (chosen) *chosen = best;
+  if (best_ms) *best_ms = best_t;
+  return MGK_OK;
+}
+
 extern "C" int mgk_fs3d_step(mgk_fs3d_t p, const double* F_bar_in, int drv_i, int drv_j, const double* P_target,
                              const int* P_mask, double E_avg, double nu_avg, double tol_NW, double tol_CG, int max_NW,
                              double tol_macro, int max_iter_macro, double* F_bar_out, mgk_fs_info* info,

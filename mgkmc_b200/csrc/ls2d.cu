@@ -1153,7 +1153,9 @@ struct mgk_ls2d_plan {
   long long maxN = 0;
   size_t row_smem = 0, col_smem = 0;      // FP64 iteration kernels
   size_t row_smem32 = 0, col_smem32 = 0;  // FP32 iteration kernels
-  int fast = 0;                           // warp-line kernels (every side has a compiled FFT)
+  int fast = 0;                           // kernel family in use: 0 CTA-wide passes, 256/512/1024 warp-line
+  int fast_nat = 0;                       // smallest warp-line family that covers every side (0: none)
+  std::vector<int> tc_gen;                // column tiles of the CTA-wide family, per replica
   std::vector<Ls2dRep> reps;      // host copy (static part)
   std::vector<char> has_material;
   Ls2dRep* h_reps = nullptr;      // pinned staging of the table
@@ -1288,10 +1290,12 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
       fast = fast && warp_fft_len(nxs[r]) && warp_fft_len(nys[r]);
       side = std::max(side, std::max(nxs[r], nys[r]));
     }
+    p->fast_nat = fast ? (side > 512 ? 1024 : side > 256 ? 512 : 256) : 0;
     const char* env = getenv("MGK_FAST");
-    if (env && env[0] == '0') fast = false;
-    p->fast = fast ? (side > 512 ? 1024 : side > 256 ? 512 : 256) : 0;
+    p->fast = (env && env[0] == '0') ? 0 : p->fast_nat;
   }
+  p->tc_gen.resize(nrep);
+  int total_col_max = 0;
   size_t row_smem = 0, col_smem = 0, row_smem32 = 0, col_smem32 = 0;
   for (int r = 0; r < nrep; ++r) {
     const int nx = nxs[r], ny = nys[r];
@@ -1299,9 +1303,16 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     memset(&R, 0, sizeof(R));
     R.nx = nx; R.ny = ny; R.nyh = ny / 2 + 1; R.ld = R.nyh;
     R.N = (long long)nx * ny;
-    R.tc = p->fast ? fast_col_tiles(p->fast) : pick_tc(nx, c64, 64 * 1024);
+    p->tc_gen[r] = pick_tc(nx, c64, 64 * 1024);
+    R.tc = p->fast ? fast_col_tiles(p->fast) : p->tc_gen[r];
     R.row_items = nx / 2;
     R.col_items = (R.nyh + R.tc - 1) / R.tc;
+    {
+      int cmax = (R.nyh + p->tc_gen[r] - 1) / p->tc_gen[r];
+      for (int v : {256, 512, 1024})
+        if (p->fast_nat && v >= p->fast_nat) cmax = std::max(cmax, (R.nyh + fast_col_tiles(v) - 1) / fast_col_tiles(v));
+      total_col_max += cmax;
+    }
     fft_schedule(nx, &R.fx64);
     fft_schedule(ny, &R.fy64);
     R.fx32 = R.fx64;
@@ -1398,7 +1409,7 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
   p->d_st = reinterpret_cast<Ls2dState*>(v);
   if ((st = plan_alloc(p, &v, sizeof(Ls2dCtl)))) return fail(st);
   p->d_ctl = reinterpret_cast<Ls2dCtl*>(v);
-  const size_t nmaps = 2 * (size_t)p->total_row_items + 2 * (size_t)p->total_col_items + nrep;
+  const size_t nmaps = 2 * (size_t)p->total_row_items + 2 * (size_t)std::max(p->total_col_items, total_col_max) + nrep;
   if ((st = plan_alloc(p, &v, sizeof(int) * nmaps))) return fail(st);
   p->d_maps = reinterpret_cast<int*>(v);
   if ((st = plan_alloc(p, &v, sizeof(unsigned int) * nrep))) return fail(st);
@@ -1657,6 +1668,89 @@ static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_
   p->gcache.push_back({a64.rows, a64.cols, nsel, guard_cap, g, x});
   p->graph = g;
   p->exec = x;
+  return MGK_OK;
+}
+
+// Switches the plan's kernel family: 0 = CTA-wide passes, 256/512/1024 =
+// warp-line kernels for sides up to that length (at least the plan's
+// largest side).  Column tiles, shared-memory sizes and the cached loop
+// graphs follow the family.
+static int ls2d_set_variant(mgk_ls2d_t p, int v) {
+  MGK_REQUIRE(v == 0 || (p->fast_nat && v >= p->fast_nat && (v == 256 || v == 512 || v == 1024)),
+              "mgk_ls2d: kernel family %d cannot serve this plan", v);
+  const size_t c64 = sizeof(double2);
+  size_t rs = 0, cs = 0, rs32 = 0, cs32 = 0;
+  int tot_cols = 0;
+  for (int r = 0; r < p->nrep; ++r) {
+    Ls2dRep& R = p->reps[r];
+    R.tc = v ? fast_col_tiles(v) : p->tc_gen[r];
+    R.col_items = (R.nyh + R.tc - 1) / R.tc;
+    tot_cols += R.col_items;
+    if (v) {
+      rs = std::max(rs, (size_t)row_fast_smem(R.ny, 16, 8));
+      cs = std::max(cs, (size_t)col_fast_smem(R.nx, 16, R.tc));
+      rs32 = std::max(rs32, (size_t)row_fast_smem(R.ny, 8, 4));
+      cs32 = std::max(cs32, (size_t)col_fast_smem(R.nx, 8, R.tc));
+    } else {
+      rs = std::max(rs, 2 * 3 * (size_t)R.ny * c64);
+      cs = std::max(cs, 2 * 3 * (size_t)R.tc * R.nx * c64);
+      rs32 = rs / 2;
+      cs32 = cs / 2;
+    }
+  }
+  int st = v ? ls2d_set_fast_attrs<double>(v, rs, cs) : ls2d_set_attrs<double, double>(rs, cs);
+  if (st == MGK_OK && p->prec == MGK_MIXED)
+    st = v ? ls2d_set_fast_attrs<float>(v, rs32, cs32) : ls2d_set_attrs<float, float>(rs32, cs32);
+  if (st) return st;
+  p->fast = v;
+  p->total_col_items = tot_cols;
+  p->row_smem = rs; p->col_smem = cs; p->row_smem32 = rs32; p->col_smem32 = cs32;
+  for (auto& e : p->gcache) {
+    cudaGraphExecDestroy(e.x);
+    cudaGraphDestroy(e.g);
+  }
+  p->gcache.clear();
+  p->graph = nullptr;
+  p->exec = nullptr;
+  p->graph_mode = -1;
+  p->sel_rows = p->sel_cols = p->nsel = 0;
+  return MGK_OK;
+}
+
+extern "C" int mgk_ls2d_profile_batch(mgk_ls2d_t p, int nsel, const int* sel, const double* eps_bar, int fp32,
+                                      int reps, float* row_ms, float* col_ms, mgk_stream_t stream);
+
+extern "C" int mgk_ls2d_set_family(mgk_ls2d_t p, int family) {
+  MGK_REQUIRE(p, "mgk_ls2d_set_family: null plan");
+  MGK_CUDA(cudaDeviceSynchronize());  // no loop graph of this plan in flight
+  return ls2d_set_variant(p, family);
+}
+
+extern "C" int mgk_ls2d_autotune(mgk_ls2d_t p, int nsel, const int* sel, const double* eps_bar, int reps,
+                                 int* chosen, float* best_ms, mgk_stream_t stream) {
+  MGK_REQUIRE(p && eps_bar && nsel >= 1 && reps >= 1, "mgk_ls2d_autotune: bad argument");
+  int cands[4];
+  int nc = 0;
+  if (p->fast_nat)
+    for (int v : {256, 512, 1024})
+      if (v >= p->fast_nat) cands[nc++] = v;
+  cands[nc++] = 0;
+  int best = p->fast;
+  float best_t = 0.0f;
+  for (int k = 0; k < nc; ++k) {
+    int st = ls2d_set_variant(p, cands[k]);
+    if (st) return st;
+    float r64 = 0, c64 = 0, r32 = 0, c32 = 0;
+    st = mgk_ls2d_profile_batch(p, nsel, sel, eps_bar, 0, reps, &r64, &c64, stream);
+    if (st == MGK_OK && p->prec == MGK_MIXED) st = mgk_ls2d_profile_batch(p, nsel, sel, eps_bar, 1, reps, &r32, &c32, stream);
+    if (st) return st;
+    const float t = r64 + c64 + r32 + c32;
+    if (k == 0 || t < best_t) { best_t = t; best = cands[k]; }
+  }
+  int st = ls2d_set_variant(p, best);
+  if (st) return st;
+  if (chosen) *chosen = best;
+  if (best_ms) *best_ms = best_t;
   return MGK_OK;
 }
 

@@ -113,6 +113,14 @@ class Fs3dSolver:
                 "mgk_fs3d_profile")
         return list(ms)
 
+    def autotune(self, reps=5, stream=None):
+        """Keeps the faster kernel family (1 warp-line, 0 CTA-wide) for this
+        plan, timed on its current state (call after a step)."""
+        ch, ms = ctypes.c_int(), ctypes.c_float()
+        L.check(L.lib().mgk_fs3d_autotune(self._h, int(reps), ctypes.byref(ch), ctypes.byref(ms),
+                                          L.stream_ptr(stream)), "mgk_fs3d_autotune")
+        return ch.value, ms.value
+
     def get(self, F_out=None, P_out=None, sig_out=None, stream=None):
         L.check(L.lib().mgk_fs3d_get(self._h, L.ptr(F_out), L.ptr(P_out), L.ptr(sig_out), L.stream_ptr(stream)),
                 "mgk_fs3d_get")

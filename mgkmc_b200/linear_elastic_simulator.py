@@ -94,6 +94,27 @@ class Ls2dBatch:
         L.check(st, "mgk_ls2d_solve_batch", allow=(L.OK, L.NONFINITE))
         return list(infos) if sync else None
 
+    def autotune(self, reps, eps_bars, n=5, stream=None):
+        """Times every kernel family that can serve this plan on the selection
+        and keeps the fastest; returns (family, ms per iteration): 0 for the
+        CTA-wide passes, 256/512/1024 for the warp-line kernels.  Replicas must
+        have their material; their iterates are left unspecified."""
+        k = len(reps)
+        sel = (ctypes.c_int * k)(*[int(r) for r in reps])
+        eb = (ctypes.c_double * (4 * k))(*np.concatenate([np.asarray(e, dtype=np.float64).reshape(4)
+                                                           for e in eps_bars]))
+        ch, ms = ctypes.c_int(), ctypes.c_float()
+        L.check(L.lib().mgk_ls2d_autotune(self._h, k, sel, eb, int(n), ctypes.byref(ch), ctypes.byref(ms),
+                                          L.stream_ptr(stream)), "mgk_ls2d_autotune")
+        self.family = ch.value
+        return ch.value, ms.value
+
+    def set_family(self, family):
+        """Kernel family (0 CTA-wide, 256/512/1024 warp-line), e.g. one chosen
+        by ``autotune`` for an equal plan."""
+        L.check(L.lib().mgk_ls2d_set_family(self._h, int(family)), "mgk_ls2d_set_family")
+        self.family = int(family)
+
     def collect(self, reps, stream=None):
         """LsInfo of the last solve of ``reps`` after ``solve(..., sync=False)``
         (one synchronisation of the stream)."""

@@ -48,6 +48,7 @@ import numpy as np
 from . import workloads as W
 
 SIZES_2D = (64, 128, 256, 512, 768, 1024)
+_TUNED = {}  # (side, slots, precision) -> (kernel family, ms per iteration) chosen by the LS autotuner
 SIZES_3D = (64, 96, 128)
 
 
@@ -361,6 +362,14 @@ class Server:
                 eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=self.dev)
                 for k in range(min(4, len(b.free))):
                     b.plan.set_material(k, E, nu, ep, stream=b.stream)
+                k = min(4, len(b.free))
+                if self.served:
+                    # kernel family picked by measurement, once per (side, slots, precision)
+                    key = (n, len(b.free), self.precision)
+                    if key not in _TUNED:
+                        _TUNED[key] = b.plan.autotune(list(range(k)), [eb] * k, stream=b.stream)
+                    else:
+                        b.plan.set_family(_TUNED[key][0])
                 for k in range(1, min(4, len(b.free)) + 1):
                     b.plan.solve(list(range(k)), [eb] * k, [eps] * k, [None] * k, max_iter=self.ls_max_iter,
                                  tol=self.ls_tol, sync=True, stream=b.stream)

@@ -146,3 +146,32 @@ def test_warp_line_passes_match_generic(shape, model, prec):
     tol = (1e-10, 1e-9) if prec == "fp64" else (1e-6, 1e-6)
     assert rel(outs[0][0], outs[1][0]) < tol[0]
     assert rel(outs[0][1], outs[1][1]) < tol[1]
+
+
+def test_autotune_keeps_results():
+    # the finite-strain autotuner picks a kernel family by timing; the next
+    # load step gives the same fields whichever family it kept
+    import torch
+    from mgkmc_b200.finite_strain_simulator import Fs3dSolver, build_finite_strain_bc_3d
+    n = 64
+    E, nu, Fp = W.fs3d_material(n, n, n, np.random.default_rng(12))
+    lam, mu = OF.lame_3d(E, nu)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    Fs = []
+    for tune in (False, True):
+        s = Fs3dSolver(n, n, n, model="neo_hookean")
+        s.set_material(t(lam), t(mu), t(Fp))
+        F0 = t(np.einsum("ij,xyz->ijxyz", np.eye(3), np.ones((n, n, n))))
+        s.set_F(F0)
+        Fb, _, Pt, Pm = build_finite_strain_bc_3d((0, 0), 0.005, {(1, 1): 0.0, (2, 2): 0.0})
+        s.step(Fb, (0, 0), Pt, Pm, E.mean(), nu.mean(), 1e-10, 1e-9, 40, 1e3, 40)
+        if tune:
+            fam, ms = s.autotune(reps=3)
+            assert fam in (0, 1) and ms > 0
+        Fb2, _, Pt2, Pm2 = build_finite_strain_bc_3d((0, 0), 0.01, {(1, 1): 0.0, (2, 2): 0.0})
+        s.set_F(F0)
+        s.step(Fb2, (0, 0), Pt2, Pm2, E.mean(), nu.mean(), 1e-10, 1e-9, 40, 1e3, 40)
+        F = torch.empty((3, 3, n, n, n), dtype=torch.float64, device="cuda")
+        s.get(F)
+        Fs.append(F.cpu().numpy())
+    assert rel(Fs[1], Fs[0]) < 1e-10

@@ -126,3 +126,34 @@ def test_mixed_batch_many_replicas():
         o = OL.spectral_solver(E, nu, eb, ep, max_iter=500, tol=1e-13)
         assert infos[r].status == 0
         assert rel(outs[r].cpu().numpy(), o[0]) < 1e-6
+
+
+def test_autotune_and_every_family_agree():
+    # the autotuner picks among the kernel families that can serve the plan;
+    # every family computes the same solves (same radix schedules, different
+    # work decomposition; the compiler may contract FP32 operations
+    # differently per kernel, so agreement is to 1e-10, far inside tol)
+    import torch
+    from mgkmc_b200.linear_elastic_simulator import Ls2dBatch
+    sizes = [(128, 128), (96, 64), (128, 96)]
+    probs = _problems(sizes, seed0=300)
+    ref = None
+    for family in (None, 256, 512, 1024, 0):
+        B = Ls2dBatch(sizes, precision="mixed")
+        for r, (E, nu, ep, eb) in enumerate(probs):
+            B.set_material(r, _t(E), _t(nu), _t(ep))
+        if family is None:
+            fam, ms = B.autotune([0, 1, 2], [p[3] for p in probs], n=3)
+            assert fam in (0, 256, 512, 1024) and ms > 0
+            for r, (E, nu, ep, eb) in enumerate(probs):  # iterates were used for timing
+                B.set_material(r, _t(E), _t(nu), _t(ep))
+        else:
+            B.set_family(family)
+        outs = [torch.empty(p[0].shape + (2, 2), dtype=torch.float64, device="cuda") for p in probs]
+        sigs = [torch.empty_like(o) for o in outs]
+        infos = B.solve([0, 1, 2], [p[3] for p in probs], outs, sigs, max_iter=300, tol=1e-10)
+        got = [o.cpu().numpy() for o in outs]
+        if ref is None:
+            ref = got
+        for a, b in zip(got, ref):
+            assert rel(a, b) < 1e-10
