@@ -783,7 +783,14 @@ __global__ void __launch_bounds__(256) ls2d_col_kernel(const Ls2dRep* __restrict
 // c.  Column kernel: one CTA of kColTiles warps per tile of kColTiles ky
 // columns; the tile lands in shared memory through cp.async, then warp t runs
 // FFT, Gamma0_sym and inverse FFT on column t alone.
-constexpr int kRowWarps = 3;
+// resident-CTA targets for the register allocator (FP32 kernels need fewer
+// registers; more resident warps hide their latency)
+#ifndef MGK_ROW_MINB32
+#define MGK_ROW_MINB32 9
+#endif
+#ifndef MGK_COL_MINB32
+#define MGK_COL_MINB32 4
+#endif
 constexpr int kColTiles = 4;  // ky columns per column-kernel CTA (one warp each)
 // lanes per line and column tiles of a kernel variant (sides up to MAXN):
 // lines longer than 512 points take two warps
@@ -792,6 +799,9 @@ __host__ __device__ constexpr int fast_col_tiles(int maxn) { return maxn > 512 ?
 __host__ __device__ constexpr int row_threads(int maxn) { return 3 * fast_group(maxn); }
 __host__ __device__ constexpr int col_threads(int maxn) { return fast_col_tiles(maxn) * fast_group(maxn); }
 
+// Shared memory of the row kernel: 3 padded lines, then the row pair's eps
+// (3), mu, lambda and eps_p (3) planes staged by bulk copies (reading eps
+// from global memory instead serialises the loads behind the in-place stores).
 __host__ __device__ constexpr int row_fast_smem(int ny, int csz, int tsz) {
   return ((3 * (csz == 16 ? ny + ny / 8 + 1 : ((ny + ny / 16 + 2) & ~1)) * csz + 127) / 128) * 128 + 16 * ny * tsz;
 }
@@ -922,7 +932,7 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
 }
 
 template <typename T, int MAXN, bool IN_SPEC, bool FINAL>
-__global__ void __launch_bounds__(row_threads(MAXN)) ls2d_row_fast_kernel(
+__global__ void __launch_bounds__(row_threads(MAXN), sizeof(T) == 4 && MAXN <= 256 ? MGK_ROW_MINB32 : 1) ls2d_row_fast_kernel(
     const Ls2dRep* __restrict__ reps, Ls2dState* st, const int* __restrict__ row_map,
     const int* __restrict__ row_local, double* partials, unsigned int* rep_counter, Ls2dCtl* ctl,
     cudaGraphConditionalHandle cond, int use_cond, int guard_cap) {
@@ -1035,7 +1045,7 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
 }
 
 template <typename T, int MAXN>
-__global__ void __launch_bounds__(col_threads(MAXN), MAXN <= 256 ? 4 : 1) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
+__global__ void __launch_bounds__(col_threads(MAXN), MAXN <= 256 ? (sizeof(T) == 4 ? MGK_COL_MINB32 : 4) : 1) ls2d_col_fast_kernel(const Ls2dRep* __restrict__ reps,
                                                                        const Ls2dState* __restrict__ st,
                                                                        const int* __restrict__ col_map,
                                                                        const int* __restrict__ col_local) {
