@@ -227,6 +227,8 @@ namespace mgk {
 template <typename C> __device__ __forceinline__ int pidx(int i) {
   return sizeof(C) == 16 ? i + (i >> 3) : i + (i >> 4);
 }
+// elements per 128-byte padding period
+template <typename C> constexpr int kPadPeriod = sizeof(C) == 16 ? 8 : 16;
 // padded line length in elements, rounded up to 16 bytes
 template <typename C> constexpr int padded_len(int n) {
   return sizeof(C) == 16 ? n + n / 8 + 1 : ((n + n / 16 + 1 + 1) & ~1);
@@ -254,8 +256,15 @@ __device__ __forceinline__ void warp_pass(C* a, int stride, const C* __restrict_
       for (int u = 0; u < U; ++u) {
         const int j = lane + G * u;
         if (nb % G == 0 || j < nb) {
+          if constexpr (nb % kPadPeriod<C> == 0) {
+            // j + r*nb: the padding of r*nb is a constant, so one padded base
+            const int pj = l * stride + pidx<C>(j);
 #pragma unroll
-          for (int r = 0; r < R; ++r) v[l][u][r] = a[l * stride + pidx<C>(j + r * nb)];
+            for (int r = 0; r < R; ++r) v[l][u][r] = a[pj + r * (nb + nb / kPadPeriod<C>)];
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[l][u][r] = a[l * stride + pidx<C>(j + r * nb)];
+          }
         }
       }
     grp_sync<G>(bid);
@@ -284,8 +293,19 @@ __device__ __forceinline__ void warp_pass(C* a, int stride, const C* __restrict_
           else if constexpr (R == 3) dft3<SIGN>(x);
           else if constexpr (R == 4) dft4<SIGN>(x[0], x[1], x[2], x[3]);
           else dft8<SIGN>(x);
+          if constexpr (NS % kPadPeriod<C> == 0) {
+            const int pb = l * stride + pidx<C>(base);
 #pragma unroll
-          for (int r = 0; r < R; ++r) a[l * stride + pidx<C>(base + r * NS)] = x[r];
+            for (int r = 0; r < R; ++r) a[pb + r * (NS + NS / kPadPeriod<C>)] = x[r];
+          } else if constexpr (NS == 1 && kPadPeriod<C> % R == 0) {
+            // base = j*R is a multiple of R, so base..base+R-1 share one padding block
+            const int pb = l * stride + pidx<C>(base);
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[pb + r] = x[r];
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[l * stride + pidx<C>(base + r * NS)] = x[r];
+          }
         }
       }
     }
