@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "tma.cuh"
 
 namespace mgk {
 
@@ -76,6 +77,7 @@ struct Ls3dState {
 struct Ls3dCtl {
   unsigned int n_active, decided, still, bodies;
   int any;
+  int error;  // a bounded wait gave up (MGK_TIMEOUT)
 };
 
 // symmetric component c -> (i, j): xx yy zz yz xz xy
@@ -250,6 +252,59 @@ __global__ void ls3d_begin_kernel(const Ls3dRep* reps, Ls3dState* st, const int*
   }
 }
 
+// Partial sums of this z-line item, and (last item of the replica) the
+// fixed-order reduction, the convergence decision and the loop condition.
+__device__ void ls3d_decide(const Ls3dRep& R, Ls3dState& S, int r, int item, double d2, double n2,
+                            double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
+                            cudaGraphConditionalHandle cond, int use_cond, int guard_cap, double* red,
+                            int* s_last_p) {
+  int& s_last = *s_last_p;
+  const long long N = R.N;
+  d2 = block_sum(d2, red);
+  n2 = block_sum(n2, red);
+  if (threadIdx.x == 0) {
+    partials[2 * item] = d2;
+    partials[2 * item + 1] = n2;
+    __threadfence();
+    const unsigned int t = atomicInc(&rep_counter[r], (unsigned int)R.zl_items - 1);
+    s_last = (t == (unsigned int)R.zl_items - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < R.zl_items; i += blockDim.x) {
+    a += __ldcg(&partials[2 * (R.zl_first + i)]);
+    b += __ldcg(&partials[2 * (R.zl_first + i) + 1]);
+  }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x != 0) return;
+  if (S.iter == 0) { a += S.extra_d0; b += S.extra_n0; }
+  else b += 2.0 * (double)N * (S.abar[0] * S.abar[0] + S.abar[1] * S.abar[1] + S.abar[2] * S.abar[2]);
+  const double diff = sqrt(a) / (sqrt(b) + 1e-20);
+  S.diff = diff;
+  S.iter += 1;
+  int keep = 0;
+  if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
+  else if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
+  else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
+  else keep = 1;
+  const unsigned int n_act = ctl->n_active;
+  if (keep) atomicAdd(&ctl->still, 1u);
+  __threadfence();
+  const unsigned int dcount = atomicAdd(&ctl->decided, 1u);
+  if (dcount == n_act - 1) {
+    __threadfence();
+    const unsigned int still = atomicExch(&ctl->still, 0u);
+    ctl->decided = 0;
+    ctl->n_active = still;
+    const bool go = still > 0 && atomicAdd(&ctl->bodies, 0u) <= (unsigned int)guard_cap;
+    ctl->any = go ? 1 : 0;
+    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
+  }
+}
+
 // z-line kernel: pairs of z-lines (flattened (x, y) index 2p, 2p+1)
 template <bool IN_SPEC>
 __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
@@ -267,7 +322,7 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
   Ls3dState& S = st[r];
   if (IN_SPEC && use_cond && item == 0 && threadIdx.x == 0) {
     const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
-    if (ctl->n_active == 0 || b > (unsigned int)guard_cap) {
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap || *(volatile int*)&ctl->error != 0) {
       ctl->any = 0;
       cudaGraphSetConditional(cond, 0u);
     }
@@ -350,49 +405,7 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
     ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
   }
   if (!IN_SPEC) return;
-  d2 = block_sum(d2, red);
-  n2 = block_sum(n2, red);
-  if (threadIdx.x == 0) {
-    partials[2 * item] = d2;
-    partials[2 * item + 1] = n2;
-    __threadfence();
-    const unsigned int t = atomicInc(&rep_counter[r], (unsigned int)R.zl_items - 1);
-    s_last = (t == (unsigned int)R.zl_items - 1);
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  double a = 0, b = 0;
-  for (int i = threadIdx.x; i < R.zl_items; i += blockDim.x) {
-    a += __ldcg(&partials[2 * (R.zl_first + i)]);
-    b += __ldcg(&partials[2 * (R.zl_first + i) + 1]);
-  }
-  a = block_sum(a, red);
-  b = block_sum(b, red);
-  if (threadIdx.x != 0) return;
-  if (S.iter == 0) { a += S.extra_d0; b += S.extra_n0; }
-  else b += 2.0 * (double)N * (S.abar[0] * S.abar[0] + S.abar[1] * S.abar[1] + S.abar[2] * S.abar[2]);
-  const double diff = sqrt(a) / (sqrt(b) + 1e-20);
-  S.diff = diff;
-  S.iter += 1;
-  int keep = 0;
-  if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
-  else if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
-  else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
-  else keep = 1;
-  const unsigned int n_act = ctl->n_active;
-  if (keep) atomicAdd(&ctl->still, 1u);
-  __threadfence();
-  const unsigned int dcount = atomicAdd(&ctl->decided, 1u);
-  if (dcount == n_act - 1) {
-    __threadfence();
-    const unsigned int still = atomicExch(&ctl->still, 0u);
-    ctl->decided = 0;
-    ctl->n_active = still;
-    const bool go = still > 0 && atomicAdd(&ctl->bodies, 0u) <= (unsigned int)guard_cap;
-    ctl->any = go ? 1 : 0;
-    if (use_cond) cudaGraphSetConditional(cond, go ? 1u : 0u);
-  }
+  ls3d_decide(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, &s_last);
 }
 
 // Strided-axis pass over tiles of tc consecutive kz columns.
@@ -483,6 +496,255 @@ __global__ void __launch_bounds__(256) ls3d_axis_kernel(const Ls3dRep* __restric
   }
 }
 
+// --------------------------------------------- warp-line iteration kernels ---
+// The same iteration for replicas whose sides are all 64, 96 or 128:
+//   z-line kernel: CTA of 3 warps per pair of z-lines; one elected thread
+//     stages the pair's eps (6), mu, lambda and eps_p (6) lines in shared
+//     memory with bulk copies while warp w inverts components 2w, 2w+1 of the
+//     spectrum; after one CTA barrier every thread updates its voxels and
+//     builds tau; warp w transforms and stores its two components.
+//   axis kernels: CTA of 6 warps per tile of kL3Tile kz columns at one x (y
+//     pass) or one y (x pass with Gamma0_sym between the transforms); warp c
+//     owns component c's lines.
+constexpr int kL3Tile = 4;
+__host__ __device__ constexpr bool ls3_fast_len(int n) { return n == 64 || n == 96 || n == 128; }
+__host__ __device__ constexpr int ls3_pl(int n) { return n + n / 8 + 1; }
+__host__ __device__ constexpr int ls3_zl_smem(int nz) { return ((6 * ls3_pl(nz) * 16 + 127) / 128) * 128 + 14 * 2 * nz * 8; }
+__host__ __device__ constexpr int ls3_ax_smem(int n) { return 6 * kL3Tile * ls3_pl(n) * 16; }
+
+template <bool IN_SPEC, int NZ>
+__device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, int item, int r, long long l0,
+                                               double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
+                                               cudaGraphConditionalHandle cond, int use_cond, int guard_cap,
+                                               unsigned char* smem, uint64_t* bar, double* red, int* s_last) {
+  using C = double2;
+  constexpr int PL = padded_len<C>(NZ);
+  constexpr int NZH = NZ / 2 + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ld = R.ld;
+  const long long N = R.N;
+  const long long plane = (long long)R.nx * R.ny * ld;
+  C* lines = reinterpret_cast<C*>(smem);
+  double* stg = reinterpret_cast<double*>(smem + ((6 * PL * 16 + 127) / 128) * 128);
+  constexpr uint32_t rb = 2u * NZ * sizeof(double);
+  if (threadIdx.x == 0) {
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, 14u * rb);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) bulk_g2s(stg + c * 2 * NZ, R.eps + c * N + l0 * NZ, rb, bar);
+    bulk_g2s(stg + 12 * NZ, R.mu + l0 * NZ, rb, bar);
+    bulk_g2s(stg + 14 * NZ, R.lam + l0 * NZ, rb, bar);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) bulk_g2s(stg + (16 + 2 * c) * NZ, R.ep + c * N + l0 * NZ, rb, bar);
+  }
+  const C* tw = reinterpret_cast<const C*>(R.fz.tw);
+  C* lw = lines + 2 * warp * PL;
+  if (IN_SPEC) {
+    for (int cc = 0; cc < 2; ++cc) {
+      const int c = 2 * warp + cc;
+      C* ln = lines + c * PL;
+      const C* ra = R.spec + c * plane + l0 * ld;
+      for (int k = lane; k < NZH; k += 32) {
+        C av = ra[k], bv = ra[ld + k];
+        if (k == 0 || 2 * k == NZ) { av.y = 0; bv.y = 0; }
+        ln[pidx<C>(k)] = make_double2(av.x - bv.y, av.y + bv.x);
+        if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = make_double2(av.x + bv.y, bv.x - av.y);
+      }
+    }
+    __syncwarp();
+    warp_fft<NZ, +1, 2>(lw, PL, tw, lane);
+  }
+  const bool ok = mbar_wait(bar, 0);
+  if (!__syncthreads_and(ok ? 1 : 0)) {
+    if (threadIdx.x == 0) { ctl->error = 1; ctl->any = 0; }
+    return;
+  }
+  const double mu0 = S.mu0, lam0 = S.lam0;
+  double d2 = 0, n2 = 0;
+  for (int z = threadIdx.x; z < NZ; z += 96) {
+    const int pz = pidx<C>(z);
+    C zz[6];
+    if (IN_SPEC) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) zz[c] = lines[c * PL + pz];
+    }
+    double tr[2][6];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = h * NZ + z;
+      const long long i = (l0 + h) * NZ + z;
+      double e[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const double o = stg[c * 2 * NZ + j];
+        if (IN_SPEC) {
+          const double nw = S.ebar[c] + (h == 0 ? zz[c].x : zz[c].y);
+          const double dd = nw - o;
+          const double w = c < 3 ? 1.0 : 2.0;
+          d2 += w * dd * dd;
+          n2 += w * o * o;
+          R.eps[c * N + i] = nw;
+          e[c] = nw;
+        } else {
+          e[c] = o;
+        }
+      }
+      const double m = stg[12 * NZ + j], l = stg[14 * NZ + j];
+      double d[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) d[c] = e[c] - stg[(16 + 2 * c) * NZ + j];
+      const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) tr[h][c] = (2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre);
+#pragma unroll
+      for (int c = 3; c < 6; ++c) tr[h][c] = 2 * m * d[c] - 2 * mu0 * e[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) lines[c * PL + pz] = make_double2(tr[0][c], tr[1][c]);
+  }
+  __syncthreads();
+  warp_fft<NZ, -1, 2>(lw, PL, tw, lane);
+  for (int cc = 0; cc < 2; ++cc) {
+    const int c = 2 * warp + cc;
+    const C* ln = lines + c * PL;
+    C* ra = R.spec + c * plane + l0 * ld;
+    for (int k = lane; k < NZH; k += 32) {
+      const C z = ln[pidx<C>(k)];
+      const C w = ln[pidx<C>(k == 0 ? 0 : NZ - k)];
+      ra[k] = make_double2(0.5 * (z.x + w.x), 0.5 * (z.y - w.y));
+      ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
+    }
+  }
+  if (!IN_SPEC) return;
+  ls3d_decide(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, s_last);
+}
+
+template <bool IN_SPEC>
+__global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
+                                                            const int* __restrict__ map, const int* __restrict__ loc,
+                                                            double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
+                                                            cudaGraphConditionalHandle cond, int use_cond,
+                                                            int guard_cap) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[32];
+  __shared__ int s_last;
+  __shared__ __align__(8) uint64_t bar;
+  const int item = blockIdx.x;
+  const int r = map[item];
+  const Ls3dRep& R = reps[r];
+  Ls3dState& S = st[r];
+  if (IN_SPEC && use_cond && item == 0 && threadIdx.x == 0) {
+    const unsigned int b = atomicAdd(&ctl->bodies, 1u) + 1u;
+    if (ctl->n_active == 0 || b > (unsigned int)guard_cap || *(volatile int*)&ctl->error != 0) {
+      ctl->any = 0;
+      cudaGraphSetConditional(cond, 0u);
+    }
+  }
+  if (S.done != 0) return;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const long long l0 = 2LL * loc[item];
+#define MGK_Z3_CASE(n) case n: ls3_zline_body<IN_SPEC, n>(R, S, item, r, l0, partials, rep_counter, ctl, cond, use_cond, guard_cap, smem_raw, &bar, red, &s_last); break;
+  switch (R.nz) {
+    MGK_Z3_CASE(64) MGK_Z3_CASE(96) MGK_Z3_CASE(128)
+    default: break;
+  }
+#undef MGK_Z3_CASE
+}
+
+template <int AXIS, int SIGN, int NL>
+__device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState& S, int o, int k0,
+                                              unsigned char* smem) {
+  using C = double2;
+  constexpr int PL = padded_len<C>(NL);
+  constexpr int TC = kL3Tile;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = R.nx, ny = R.ny, nz = R.nz, nzh = R.nzh, ld = R.ld;
+  const int tcw = min(TC, nzh - k0);
+  const long long plane = (long long)nx * ny * ld;
+  const long long jstride = AXIS == 1 ? ld : (long long)ny * ld;
+  const long long obase = AXIS == 1 ? (long long)o * ny * ld : (long long)o * ld;
+  C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t)
+  C* spec = R.spec;
+  constexpr int TOT = 6 * NL * TC;
+  for (int e = threadIdx.x; e < TOT; e += 6 * 32) {
+    const int c = e / (NL * TC);
+    const int rem = e - c * NL * TC;
+    const int j = rem / TC, t = rem - j * TC;
+    if (t < tcw) cp_async_elem(&lines[(c * TC + t) * PL + pidx<C>(j)], &spec[c * plane + obase + j * jstride + k0 + t]);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>((AXIS == 1 ? R.fy : R.fx).tw);
+  C* l0 = lines + warp * TC * PL;
+  warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0, PL, tw, lane);
+  warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0 + 2 * PL, PL, tw, lane);
+  if (AXIS == 0) {
+    __syncthreads();
+    const double scale = 1.0 / (double)R.N;
+    const int ky = o;
+    const double uy = (double)fftfreq3(ky, ny) / ny;
+    const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
+    for (int e = threadIdx.x; e < tcw * NL; e += 6 * 32) {
+      const int t = e / NL, kx = e - t * NL;
+      const int kz = k0 + t;
+      const int pk = pidx<C>(kx);
+      C tv[6], ev[6];
+      for (int c = 0; c < 6; ++c) tv[c] = lines[(c * TC + t) * PL + pk];
+      if (kx == 0 && ky == 0 && kz == 0) {
+        for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = make_double2(0.0, 0.0);
+        continue;
+      }
+      const double ux = (double)fftfreq3(kx, nx) / nx, uz = (double)fftfreq3(kz, nz) / nz;
+      const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
+      const double n0 = ux * inv, n1 = uy * inv, n2 = uz * inv;
+      gamma3d_apply(tv, n0, n1, n2, S.inv2mu0, S.Bc, ev);
+      const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
+      if (nqx || nqy || nqz) {
+        C fv[6];
+        gamma3d_apply(tv, nqx ? -n0 : n0, nqy ? -n1 : n1, nqz ? -n2 : n2, S.inv2mu0, S.Bc, fv);
+        for (int c = 0; c < 6; ++c) ev[c] = make_double2(0.5 * (ev[c].x + fv[c].x), 0.5 * (ev[c].y + fv[c].y));
+      }
+      for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = make_double2(ev[c].x * scale, ev[c].y * scale);
+    }
+    __syncthreads();
+    warp_fft<NL, +1, 2>(l0, PL, tw, lane);
+    warp_fft<NL, +1, 2>(l0 + 2 * PL, PL, tw, lane);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < TOT; e += 6 * 32) {
+    const int c = e / (NL * TC);
+    const int rem = e - c * NL * TC;
+    const int j = rem / TC, t = rem - j * TC;
+    if (t < tcw) spec[c * plane + obase + j * jstride + k0 + t] = lines[(c * TC + t) * PL + pidx<C>(j)];
+  }
+}
+
+template <int AXIS, int SIGN>
+__global__ void __launch_bounds__(192, 2) ls3d_axis_fast_kernel(const Ls3dRep* __restrict__ reps,
+                                                             const Ls3dState* __restrict__ st,
+                                                             const int* __restrict__ map, const int* __restrict__ loc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int item = blockIdx.x;
+  const int r = map[item];
+  const Ls3dRep& R = reps[r];
+  const Ls3dState& S = st[r];
+  if (S.done != 0) return;
+  const int ntile = (R.nzh + kL3Tile - 1) / kL3Tile;
+  const int o = loc[item] / ntile;
+  const int k0 = (loc[item] - o * ntile) * kL3Tile;
+  const int nl = AXIS == 1 ? R.ny : R.nx;
+#define MGK_A3_CASE(n) case n: ls3_axis_body<AXIS, SIGN, n>(R, S, o, k0, smem_raw); break;
+  switch (nl) {
+    MGK_A3_CASE(64) MGK_A3_CASE(96) MGK_A3_CASE(128)
+    default: break;
+  }
+#undef MGK_A3_CASE
+}
+
 // outputs (nx,ny,nz,3,3) and partial sums for the means; grid (G, nsel)
 __global__ void ls3d_output_kernel(const Ls3dRep* reps, const Ls3dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
@@ -554,6 +816,7 @@ struct mgk_ls3d_plan {
   int nrep = 0;
   long long maxN = 0;
   size_t zl_smem = 0, ax_smem = 0;
+  int fast = 0;  // warp-line kernels (every side 64, 96 or 128)
   std::vector<Ls3dRep> reps;
   std::vector<char> has_material;
   std::vector<void*> allocations;
@@ -620,6 +883,12 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
   p->nrep = nrep;
   p->reps.resize(nrep);
   p->has_material.assign(nrep, 0);
+  {
+    bool fast = true;
+    for (int r = 0; r < nrep; ++r) fast = fast && ls3_fast_len(nxs[r]) && ls3_fast_len(nys[r]) && ls3_fast_len(nzs[r]);
+    const char* env = getenv("MGK_FAST");
+    p->fast = fast && !(env && env[0] == '0');
+  }
   for (int r = 0; r < nrep; ++r) {
     Ls3dRep& R = p->reps[r];
     memset(&R, 0, sizeof(R));
@@ -627,7 +896,7 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
     R.nzh = R.nz / 2 + 1;
     R.ld = R.nzh;
     R.N = (long long)R.nx * R.ny * R.nz;
-    R.tc = tc3(std::max(R.nx, R.ny));
+    R.tc = p->fast ? kL3Tile : tc3(std::max(R.nx, R.ny));
     const int ntile = (R.nzh + R.tc - 1) / R.tc;
     R.zl_items = R.nx * R.ny / 2;
     R.y_items = R.nx * ntile;
@@ -635,8 +904,13 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
     fft_schedule(R.nx, &R.fx); fft_schedule(R.ny, &R.fy); fft_schedule(R.nz, &R.fz);
     R.fx.tw = twiddles(R.nx, MGK_FP64); R.fy.tw = twiddles(R.ny, MGK_FP64); R.fz.tw = twiddles(R.nz, MGK_FP64);
     if (!R.fx.tw || !R.fy.tw || !R.fz.tw) return fail(MGK_OOM);
-    p->zl_smem = std::max(p->zl_smem, 2 * 6 * (size_t)R.nz * sizeof(double2));
-    p->ax_smem = std::max(p->ax_smem, 2 * 6 * (size_t)R.tc * std::max(R.nx, R.ny) * sizeof(double2));
+    if (p->fast) {
+      p->zl_smem = std::max(p->zl_smem, (size_t)ls3_zl_smem(R.nz));
+      p->ax_smem = std::max(p->ax_smem, (size_t)ls3_ax_smem(std::max(R.nx, R.ny)));
+    } else {
+      p->zl_smem = std::max(p->zl_smem, 2 * 6 * (size_t)R.nz * sizeof(double2));
+      p->ax_smem = std::max(p->ax_smem, 2 * 6 * (size_t)R.tc * std::max(R.nx, R.ny) * sizeof(double2));
+    }
     p->maxN = std::max(p->maxN, R.N);
     p->tot_zl += R.zl_items; p->tot_y += R.y_items; p->tot_x += R.x_items;
     void* f = nullptr;
@@ -650,11 +924,20 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
     R.spec = reinterpret_cast<double2*>(sp);
   }
   int st;
-  if (raise_smem((const void*)ls3d_zline_kernel<true>, (int)p->zl_smem) ||
+  if (p->fast &&
+      (raise_smem((const void*)ls3d_zline_fast_kernel<true>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast_kernel<false>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<1, -1>, (int)p->ax_smem) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<1, 1>, (int)p->ax_smem) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<0, 0>, (int)p->ax_smem))) {
+    set_error("mgk_ls3d_create: cudaFuncSetAttribute failed");
+    return fail(MGK_CUDA_ERROR);
+  }
+  if (!p->fast && (raise_smem((const void*)ls3d_zline_kernel<true>, (int)p->zl_smem) ||
       raise_smem((const void*)ls3d_zline_kernel<false>, (int)p->zl_smem) ||
       raise_smem((const void*)ls3d_axis_kernel<1, -1>, (int)p->ax_smem) ||
       raise_smem((const void*)ls3d_axis_kernel<1, 1>, (int)p->ax_smem) ||
-      raise_smem((const void*)ls3d_axis_kernel<0, 0>, (int)p->ax_smem)) {
+      raise_smem((const void*)ls3d_axis_kernel<0, 0>, (int)p->ax_smem))) {
     set_error("mgk_ls3d_create: cudaFuncSetAttribute failed");
     return fail(MGK_CUDA_ERROR);
   }
@@ -746,14 +1029,29 @@ struct Loop3 {
   Ls3dCtl* ctl;
   int nzl, ny, nx;
   size_t zs, as;
+  int fast;
 };
 
+static void* zline_fn(int fast, bool in_spec) {
+  if (fast) return in_spec ? (void*)ls3d_zline_fast_kernel<true> : (void*)ls3d_zline_fast_kernel<false>;
+  return in_spec ? (void*)ls3d_zline_kernel<true> : (void*)ls3d_zline_kernel<false>;
+}
+template <int AXIS, int SIGN> static void* axis_fn(int fast) {
+  return fast ? (void*)ls3d_axis_fast_kernel<AXIS, SIGN> : (void*)ls3d_axis_kernel<AXIS, SIGN>;
+}
+
 static int body3(const Loop3& a, cudaStream_t s) {
-  ls3d_axis_kernel<1, -1><<<a.ny, kT3, a.as, s>>>(a.reps, a.st, a.ym, a.yl);
-  ls3d_axis_kernel<0, 0><<<a.nx, kT3, a.as, s>>>(a.reps, a.st, a.xm, a.xl);
-  ls3d_axis_kernel<1, 1><<<a.ny, kT3, a.as, s>>>(a.reps, a.st, a.ym, a.yl);
-  ls3d_zline_kernel<true><<<a.nzl, kT3, a.zs, s>>>(a.reps, a.st, a.zm, a.zl, a.part, a.ctr, a.ctl, 0, 0, 0);
-  MGK_CUDA(cudaGetLastError());
+  const dim3 ab(a.fast ? 192 : kT3), zb(a.fast ? 96 : kT3);
+  void* ay[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.ym, (void*)&a.yl};
+  void* ax[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.xm, (void*)&a.xl};
+  cudaGraphConditionalHandle h = 0;
+  int zero = 0;
+  void* az[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.zm, (void*)&a.zl, (void*)&a.part, (void*)&a.ctr,
+                (void*)&a.ctl, &h, &zero, &zero};
+  MGK_CUDA(cudaLaunchKernel(axis_fn<1, -1>(a.fast), dim3(a.ny), ab, ay, a.as, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<0, 0>(a.fast), dim3(a.nx), ab, ax, a.as, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<1, 1>(a.fast), dim3(a.ny), ab, ay, a.as, s));
+  MGK_CUDA(cudaLaunchKernel(zline_fn(a.fast, true), dim3(a.nzl), zb, az, a.zs, s));
   return MGK_OK;
 }
 
@@ -777,10 +1075,10 @@ static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
   if (cudaGraphAddNode(&w, g, nullptr, 0, &cp)) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   cudaGraphNode_t prev = nullptr, node;
-  auto add = [&](void* fn, dim3 grid, size_t smem, void** args) {
+  auto add = [&](void* fn, dim3 grid, size_t smem, void** args, int block) {
     cudaKernelNodeParams k;
     memset(&k, 0, sizeof(k));
-    k.func = fn; k.gridDim = grid; k.blockDim = dim3(kT3); k.sharedMemBytes = (unsigned)smem; k.kernelParams = args;
+    k.func = fn; k.gridDim = grid; k.blockDim = dim3(block); k.sharedMemBytes = (unsigned)smem; k.kernelParams = args;
     cudaError_t e = cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &k);
     prev = node;
     return e;
@@ -789,10 +1087,11 @@ static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
   void* ax[] = {&a.reps, &a.st, &a.xm, &a.xl};
   int use = 1;
   void* az[] = {&a.reps, &a.st, &a.zm, &a.zl, &a.part, &a.ctr, &a.ctl, &h, &use, &cap};
-  cudaError_t e = add((void*)ls3d_axis_kernel<1, -1>, dim3(a.ny), a.as, ay);
-  if (!e) e = add((void*)ls3d_axis_kernel<0, 0>, dim3(a.nx), a.as, ax);
-  if (!e) e = add((void*)ls3d_axis_kernel<1, 1>, dim3(a.ny), a.as, ay);
-  if (!e) e = add((void*)ls3d_zline_kernel<true>, dim3(a.nzl), a.zs, az);
+  const int ab = a.fast ? 192 : kT3, zb = a.fast ? 96 : kT3;
+  cudaError_t e = add(axis_fn<1, -1>(a.fast), dim3(a.ny), a.as, ay, ab);
+  if (!e) e = add(axis_fn<0, 0>(a.fast), dim3(a.nx), a.as, ax, ab);
+  if (!e) e = add(axis_fn<1, 1>(a.fast), dim3(a.ny), a.as, ay, ab);
+  if (!e) e = add(zline_fn(a.fast, true), dim3(a.nzl), a.zs, az, zb);
   cudaGraphExec_t x = nullptr;
   if (!e) e = cudaGraphInstantiate(&x, g, 0);
   if (e) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
@@ -841,7 +1140,7 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
     sp[q] = r;
   }
   const int n_active = max_iter > 0 ? nsel : 0;
-  *p->h_ctl = Ls3dCtl{(unsigned int)n_active, 0u, 0u, 0u, n_active > 0};
+  *p->h_ctl = Ls3dCtl{(unsigned int)n_active, 0u, 0u, 0u, n_active > 0, 0};
   const size_t nm = 2 * (size_t)(nzl + ny_ + nx_) + nsel;
   MGK_CUDA(cudaMemcpyAsync(p->d_maps, p->h_maps, sizeof(int) * nm, cudaMemcpyHostToDevice, s));
   MGK_CUDA(cudaMemcpyAsync(p->d_reps, p->h_reps, sizeof(Ls3dRep) * p->nrep, cudaMemcpyHostToDevice, s));
@@ -870,10 +1169,14 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
   }
   if (n_active > 0) {
     Loop3 a{p->d_reps, p->d_st, d_zm, d_zl, d_ym, d_yl, d_xm, d_xl, p->d_part, p->d_repctr, p->d_ctl,
-            nzl, ny_, nx_, p->zl_smem, p->ax_smem};
-    ls3d_zline_kernel<false><<<nzl, kT3, p->zl_smem, s>>>(p->d_reps, p->d_st, d_zm, d_zl, p->d_part, p->d_repctr,
-                                                          p->d_ctl, 0, 0, 0);
-    MGK_CUDA(cudaGetLastError());
+            nzl, ny_, nx_, p->zl_smem, p->ax_smem, p->fast};
+    {
+      cudaGraphConditionalHandle h0 = 0;
+      int zero = 0;
+      void* az0[] = {(void*)&p->d_reps, (void*)&p->d_st, (void*)&d_zm, (void*)&d_zl, (void*)&p->d_part,
+                     (void*)&p->d_repctr, (void*)&p->d_ctl, &h0, &zero, &zero};
+      MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false), dim3(nzl), dim3(p->fast ? 96 : kT3), az0, p->zl_smem, s));
+    }
     const int cap = max_iter + 2 > 1000 ? max_iter + 2 : 1000;
     if (p->graph_mode == 1 && (changed || cap > p->graph_cap)) p->graph_mode = -1;
     if (p->graph_mode < 0) {
@@ -904,7 +1207,13 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
   MGK_CUDA(cudaGetLastError());
   if (infos) {
     MGK_CUDA(cudaMemcpyAsync(p->h_state, p->d_st, sizeof(Ls3dState) * p->nrep, cudaMemcpyDeviceToHost, s));
+    Ls3dCtl hc3;
+    MGK_CUDA(cudaMemcpyAsync(&hc3, p->d_ctl, sizeof(Ls3dCtl), cudaMemcpyDeviceToHost, s));
     MGK_CUDA(cudaStreamSynchronize(s));
+    if (hc3.error) {
+      set_error("mgk_ls3d_solve: a bulk copy wait gave up (device timeout)");
+      return MGK_TIMEOUT;
+    }
     int worst = MGK_OK;
     for (int q = 0; q < nsel; ++q) {
       const Ls3dState& S = p->h_state[selv[q]];

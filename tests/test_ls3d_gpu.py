@@ -26,7 +26,8 @@ def test_golden(golden, name):
     assert rel(sig, g["sig_conv"]) < TOL
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 12), (64, 48, 32), (8, 6, 1), (6, 9, 3)])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 16, 12), (64, 48, 32), (8, 6, 1), (6, 9, 3), (64, 64, 64),
+                                   (96, 64, 128)])
 def test_oracle_sizes(shape):
     from mgkmc_b200.linear_elastic_simulator import spectral_solver_3d
     rng = np.random.default_rng(sum(shape))
@@ -75,3 +76,30 @@ def test_barrier_physics_homogeneous_units():
     eps, sig, em, sm = spectral_solver_3d(E, nu, eb, max_iter=50, tol=1e-6)
     lam = 70e9 * 0.3 / ((1 + 0.3) * (1 - 0.6)); mu = 70e9 / 2.6
     assert abs(sm[0, 0] - (lam + 2 * mu) * 0.01) < 1e-6 * (lam + 2 * mu) * 0.01
+
+
+def test_warp_line_batch_matches_single_plans():
+    # a batch of warp-line replicas (sides 64/96/128) against one-replica plans
+    import torch
+    from mgkmc_b200.linear_elastic_simulator import Ls3dBatch
+    sizes = [(64, 64, 64), (96, 64, 128), (64, 128, 96)]
+    rng = np.random.default_rng(9)
+    probs = []
+    for sh in sizes:
+        E, nu = W.ls3d_material(*sh, rng)
+        probs.append((E, nu, W.pure_shear_eigenstrain_3d(*sh, rng)))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    eb = np.zeros((3, 3)); eb[0, 0] = 0.01
+    B = Ls3dBatch(sizes)
+    outs = []
+    for r, (E, nu, ep) in enumerate(probs):
+        B.set_material(r, t(E), t(nu), t(ep))
+        outs.append(torch.empty(E.shape + (3, 3), dtype=torch.float64, device="cuda"))
+    sigs = [torch.empty_like(o) for o in outs]
+    B.solve(list(range(3)), [eb] * 3, outs, sigs, max_iter=200, tol=1e-10)
+    for r, (E, nu, ep) in enumerate(probs):
+        S = Ls3dBatch([sizes[r]])
+        S.set_material(0, t(E), t(nu), t(ep))
+        o1 = torch.empty_like(outs[r]); s1 = torch.empty_like(outs[r])
+        S.solve([0], [eb], [o1], [s1], max_iter=200, tol=1e-10)
+        assert rel(outs[r].cpu().numpy(), o1.cpu().numpy()) < 1e-12
