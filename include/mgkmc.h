@@ -180,6 +180,12 @@ typedef struct {
 MGK_API int mgk_ls3d_create(int nx, int ny, int nz, mgk_ls3d_t* out);
 MGK_API int mgk_ls3d_create_batch(int nrep, const int* nx, const int* ny, const int* nz, mgk_ls3d_t* out);
 MGK_API int mgk_ls3d_destroy(mgk_ls3d_t plan);
+/* Precision form (plans whose sides are all 64, 96 or 128): MGK_MIXED runs
+ * FP32 iterations (fields, spectra, Gamma0) until the update norm is below
+ * max(tol, 2e-6), then FP64 iterations from that field to tol; norms and
+ * partial sums stay FP64.  Call before set_material.  No counterpart in the
+ * reference (FP64 only). */
+MGK_API int mgk_ls3d_set_precision(mgk_ls3d_t plan, int precision);
 MGK_API int mgk_ls3d_set_material_rep(mgk_ls3d_t plan, int rep, const double* E, const double* nu,
                                       const double* eps_plastic, mgk_stream_t stream);
 MGK_API int mgk_ls3d_set_eigenstrain_rep(mgk_ls3d_t plan, int rep, const double* eps_plastic,

@@ -70,6 +70,7 @@ _SIGS = {
                                        c_double, POINTER(LsInfo), _P]),
     "mgk_ls3d_create": (c_int, [c_int, c_int, c_int, POINTER(c_void_p)]),
     "mgk_ls3d_create_batch": (c_int, [c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_void_p)]),
+    "mgk_ls3d_set_precision": (c_int, [_P, c_int]),
     "mgk_ls3d_destroy": (c_int, [_P]),
     "mgk_ls3d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
     "mgk_ls3d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),

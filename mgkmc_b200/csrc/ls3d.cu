@@ -52,6 +52,13 @@ struct Ls3dRep {
   double* ep;    // 6 planes
   double* epf;   // 9 planes or null
   double2* spec;
+  // mixed-precision plans (warp-line kernels only): FP32 copies and tables;
+  // the FP32 spectrum reuses `spec`
+  float* mu32;
+  float* lam32;
+  float* eps32;  // 6 planes
+  float* ep32;   // 6 planes
+  FftLen fx32, fy32, fz32;
   // per call
   const double* init;
   double* out_eps;
@@ -67,7 +74,7 @@ struct Ls3dState {
   double ebar[6];
   double abar[3];  // (xy - yx)/2, (xz - zx)/2, (yz - zy)/2 of eps_bar
   double extra_d0, extra_n0;
-  int iter, done, status, pad;
+  int iter, done, status, phase_iter;  // done: 0 active, 1 phase 1 finished, 2 finished
   double diff;
   double means[9];
   double out_eps_mean[9];
@@ -79,6 +86,9 @@ struct Ls3dCtl {
   int any;
   int error;  // a bounded wait gave up (MGK_TIMEOUT)
 };
+
+constexpr double kL3Phase1Tol = 2e-6;  // mixed plans: FP32 iterations down to max(tol, this)
+constexpr int kL3Phase1Cap = 64;
 
 // symmetric component c -> (i, j): xx yy zz yz xz xy
 __device__ __constant__ int kSymI[6] = {0, 1, 2, 1, 0, 0};
@@ -128,6 +138,7 @@ __global__ void ls3d_material_kernel(const Ls3dRep* reps, int rep, const double*
       const double e = E[i], v = nu[i];
       R.mu[i] = e / (2 * (1 + v));
       R.lam[i] = e * v / ((1 + v) * (1 - 2 * v));
+      if (R.mu32) { R.mu32[i] = (float)R.mu[i]; R.lam32[i] = (float)R.lam[i]; }
       sE += e;
       sn += v;
     }
@@ -136,6 +147,7 @@ __global__ void ls3d_material_kernel(const Ls3dRep* reps, int rep, const double*
     for (int c = 0; c < 6; ++c) {
       const int a = 3 * kSymI[c] + kSymJ[c], b = 3 * kSymJ[c] + kSymI[c];
       R.ep[c * N + i] = (p[a] == p[b]) ? p[a] : 0.5 * (p[a] + p[b]);
+      if (R.ep32) R.ep32[c * N + i] = (float)R.ep[c * N + i];
     }
     if (R.epf)
       for (int q = 0; q < 9; ++q) R.epf[q * N + i] = p[q];
@@ -220,6 +232,7 @@ __global__ void ls3d_begin_kernel(const Ls3dRep* reps, Ls3dState* st, const int*
       for (int c = 0; c < 6; ++c) {
         const int a = 3 * kSymI[c] + kSymJ[c], b = 3 * kSymJ[c] + kSymI[c];
         R.eps[c * N + i] = (v[a] == v[b]) ? v[a] : 0.5 * (v[a] + v[b]);
+        if (R.eps32) R.eps32[c * N + i] = (float)R.eps[c * N + i];
       }
       const double a0[3] = {0.5 * (v[1] - v[3]), 0.5 * (v[2] - v[6]), 0.5 * (v[5] - v[7])};
       for (int q = 0; q < 3; ++q) {
@@ -227,7 +240,10 @@ __global__ void ls3d_begin_kernel(const Ls3dRep* reps, Ls3dState* st, const int*
         n2 += 2 * a0[q] * a0[q];
       }
     } else {
-      for (int c = 0; c < 6; ++c) R.eps[c * N + i] = sb[c];
+      for (int c = 0; c < 6; ++c) {
+        R.eps[c * N + i] = sb[c];
+        if (R.eps32) R.eps32[c * N + i] = (float)sb[c];
+      }
     }
   }
   if (R.init) {
@@ -242,6 +258,7 @@ __global__ void ls3d_begin_kernel(const Ls3dRep* reps, Ls3dState* st, const int*
     for (int c = 0; c < 6; ++c) S.ebar[c] = sb[c];
     for (int q = 0; q < 3; ++q) S.abar[q] = ab[q];
     S.iter = 0;
+    S.phase_iter = 0;
     S.done = R.max_iter <= 0 ? 2 : 0;
     S.status = MGK_OK;
     S.diff = 0;
@@ -254,6 +271,7 @@ __global__ void ls3d_begin_kernel(const Ls3dRep* reps, Ls3dState* st, const int*
 
 // Partial sums of this z-line item, and (last item of the replica) the
 // fixed-order reduction, the convergence decision and the loop condition.
+template <bool FINAL>
 __device__ void ls3d_decide(const Ls3dRep& R, Ls3dState& S, int r, int item, double d2, double n2,
                             double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
                             cudaGraphConditionalHandle cond, int use_cond, int guard_cap, double* red,
@@ -285,11 +303,19 @@ __device__ void ls3d_decide(const Ls3dRep& R, Ls3dState& S, int r, int item, dou
   const double diff = sqrt(a) / (sqrt(b) + 1e-20);
   S.diff = diff;
   S.iter += 1;
+  S.phase_iter += 1;
   int keep = 0;
   if (!isfinite(diff)) { S.done = 2; S.status = MGK_NONFINITE; }
-  else if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
-  else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
-  else keep = 1;
+  else if (FINAL) {
+    if (diff < R.tol) { S.done = 2; S.status = MGK_OK; }
+    else if (S.iter >= R.max_iter) { S.done = 2; S.status = MGK_NOT_CONVERGED; }
+    else keep = 1;
+  } else {
+    const double tol1 = R.tol > kL3Phase1Tol ? R.tol : kL3Phase1Tol;
+    if (S.iter >= R.max_iter) { S.done = 2; S.status = diff < R.tol ? MGK_OK : MGK_NOT_CONVERGED; }
+    else if (diff < tol1 || S.phase_iter >= kL3Phase1Cap) S.done = 1;
+    else keep = 1;
+  }
   const unsigned int n_act = ctl->n_active;
   if (keep) atomicAdd(&ctl->still, 1u);
   __threadfence();
@@ -405,7 +431,7 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
     ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
   }
   if (!IN_SPEC) return;
-  ls3d_decide(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, &s_last);
+  ls3d_decide<true>(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, &s_last);
 }
 
 // Strided-axis pass over tiles of tc consecutive kz columns.
@@ -507,17 +533,41 @@ __global__ void __launch_bounds__(256) ls3d_axis_kernel(const Ls3dRep* __restric
 //     pass) or one y (x pass with Gamma0_sym between the transforms); warp c
 //     owns component c's lines.
 constexpr int kL3Tile = 4;
-__host__ __device__ constexpr bool ls3_fast_len(int n) { return n == 64 || n == 96 || n == 128; }
-__host__ __device__ constexpr int ls3_pl(int n) { return n + n / 8 + 1; }
-__host__ __device__ constexpr int ls3_zl_smem(int nz) { return ((6 * ls3_pl(nz) * 16 + 127) / 128) * 128 + 14 * 2 * nz * 8; }
-__host__ __device__ constexpr int ls3_ax_smem(int n) { return 6 * kL3Tile * ls3_pl(n) * 16; }
 
-template <bool IN_SPEC, int NZ>
+template <typename T> struct L3F;
+template <> struct L3F<double> {
+  static __device__ __forceinline__ double* eps(const Ls3dRep& R) { return R.eps; }
+  static __device__ __forceinline__ const double* ep(const Ls3dRep& R) { return R.ep; }
+  static __device__ __forceinline__ const double* mu(const Ls3dRep& R) { return R.mu; }
+  static __device__ __forceinline__ const double* lam(const Ls3dRep& R) { return R.lam; }
+  static __device__ __forceinline__ double2* spec(const Ls3dRep& R) { return R.spec; }
+  static __device__ __forceinline__ const FftLen& fx(const Ls3dRep& R) { return R.fx; }
+  static __device__ __forceinline__ const FftLen& fy(const Ls3dRep& R) { return R.fy; }
+  static __device__ __forceinline__ const FftLen& fz(const Ls3dRep& R) { return R.fz; }
+};
+template <> struct L3F<float> {
+  static __device__ __forceinline__ float* eps(const Ls3dRep& R) { return R.eps32; }
+  static __device__ __forceinline__ const float* ep(const Ls3dRep& R) { return R.ep32; }
+  static __device__ __forceinline__ const float* mu(const Ls3dRep& R) { return R.mu32; }
+  static __device__ __forceinline__ const float* lam(const Ls3dRep& R) { return R.lam32; }
+  static __device__ __forceinline__ float2* spec(const Ls3dRep& R) { return reinterpret_cast<float2*>(R.spec); }
+  static __device__ __forceinline__ const FftLen& fx(const Ls3dRep& R) { return R.fx32; }
+  static __device__ __forceinline__ const FftLen& fy(const Ls3dRep& R) { return R.fy32; }
+  static __device__ __forceinline__ const FftLen& fz(const Ls3dRep& R) { return R.fz32; }
+};
+__host__ __device__ constexpr bool ls3_fast_len(int n) { return n == 64 || n == 96 || n == 128; }
+__host__ __device__ constexpr int ls3_pl(int n, int csz) { return csz == 16 ? n + n / 8 + 1 : ((n + n / 16 + 2) & ~1); }
+__host__ __device__ constexpr int ls3_zl_smem(int nz, int csz) {
+  return ((6 * ls3_pl(nz, csz) * csz + 127) / 128) * 128 + 14 * 2 * nz * (csz / 2);
+}
+__host__ __device__ constexpr int ls3_ax_smem(int n, int csz) { return 6 * kL3Tile * ls3_pl(n, csz) * csz; }
+
+template <typename T, bool IN_SPEC, bool FINAL, int NZ>
 __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, int item, int r, long long l0,
                                                double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
                                                cudaGraphConditionalHandle cond, int use_cond, int guard_cap,
                                                unsigned char* smem, uint64_t* bar, double* red, int* s_last) {
-  using C = double2;
+  using C = C_t<T>;
   constexpr int PL = padded_len<C>(NZ);
   constexpr int NZH = NZ / 2 + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -525,30 +575,33 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
   const long long N = R.N;
   const long long plane = (long long)R.nx * R.ny * ld;
   C* lines = reinterpret_cast<C*>(smem);
-  double* stg = reinterpret_cast<double*>(smem + ((6 * PL * 16 + 127) / 128) * 128);
-  constexpr uint32_t rb = 2u * NZ * sizeof(double);
+  T* stg = reinterpret_cast<T*>(smem + ((6 * PL * (int)sizeof(C) + 127) / 128) * 128);
+  T* eps = L3F<T>::eps(R);
+  const T* ep = L3F<T>::ep(R);
+  C* spec = L3F<T>::spec(R);
+  constexpr uint32_t rb = 2u * NZ * sizeof(T);
   if (threadIdx.x == 0) {
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(bar, 14u * rb);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) bulk_g2s(stg + c * 2 * NZ, R.eps + c * N + l0 * NZ, rb, bar);
-    bulk_g2s(stg + 12 * NZ, R.mu + l0 * NZ, rb, bar);
-    bulk_g2s(stg + 14 * NZ, R.lam + l0 * NZ, rb, bar);
+    for (int c = 0; c < 6; ++c) bulk_g2s(stg + c * 2 * NZ, eps + c * N + l0 * NZ, rb, bar);
+    bulk_g2s(stg + 12 * NZ, L3F<T>::mu(R) + l0 * NZ, rb, bar);
+    bulk_g2s(stg + 14 * NZ, L3F<T>::lam(R) + l0 * NZ, rb, bar);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) bulk_g2s(stg + (16 + 2 * c) * NZ, R.ep + c * N + l0 * NZ, rb, bar);
+    for (int c = 0; c < 6; ++c) bulk_g2s(stg + (16 + 2 * c) * NZ, ep + c * N + l0 * NZ, rb, bar);
   }
-  const C* tw = reinterpret_cast<const C*>(R.fz.tw);
+  const C* tw = reinterpret_cast<const C*>(L3F<T>::fz(R).tw);
   C* lw = lines + 2 * warp * PL;
   if (IN_SPEC) {
     for (int cc = 0; cc < 2; ++cc) {
       const int c = 2 * warp + cc;
       C* ln = lines + c * PL;
-      const C* ra = R.spec + c * plane + l0 * ld;
+      const C* ra = spec + c * plane + l0 * ld;
       for (int k = lane; k < NZH; k += 32) {
         C av = ra[k], bv = ra[ld + k];
         if (k == 0 || 2 * k == NZ) { av.y = 0; bv.y = 0; }
-        ln[pidx<C>(k)] = make_double2(av.x - bv.y, av.y + bv.x);
-        if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = make_double2(av.x + bv.y, bv.x - av.y);
+        ln[pidx<C>(k)] = mk<C>(av.x - bv.y, av.y + bv.x);
+        if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = mk<C>(av.x + bv.y, bv.x - av.y);
       }
     }
     __syncwarp();
@@ -568,7 +621,7 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
 #pragma unroll
       for (int c = 0; c < 6; ++c) zz[c] = lines[c * PL + pz];
     }
-    double tr[2][6];
+    T tr[2][6];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int j = h * NZ + z;
@@ -576,50 +629,50 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
       double e[6];
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        const double o = stg[c * 2 * NZ + j];
+        const double o = (double)stg[c * 2 * NZ + j];
         if (IN_SPEC) {
-          const double nw = S.ebar[c] + (h == 0 ? zz[c].x : zz[c].y);
+          const double nw = S.ebar[c] + (double)(h == 0 ? zz[c].x : zz[c].y);
           const double dd = nw - o;
           const double w = c < 3 ? 1.0 : 2.0;
           d2 += w * dd * dd;
           n2 += w * o * o;
-          R.eps[c * N + i] = nw;
+          eps[c * N + i] = (T)nw;
           e[c] = nw;
         } else {
           e[c] = o;
         }
       }
-      const double m = stg[12 * NZ + j], l = stg[14 * NZ + j];
+      const double m = (double)stg[12 * NZ + j], l = (double)stg[14 * NZ + j];
       double d[6];
 #pragma unroll
-      for (int c = 0; c < 6; ++c) d[c] = e[c] - stg[(16 + 2 * c) * NZ + j];
+      for (int c = 0; c < 6; ++c) d[c] = e[c] - (double)stg[(16 + 2 * c) * NZ + j];
       const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) tr[h][c] = (2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre);
+      for (int c = 0; c < 3; ++c) tr[h][c] = (T)((2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre));
 #pragma unroll
-      for (int c = 3; c < 6; ++c) tr[h][c] = 2 * m * d[c] - 2 * mu0 * e[c];
+      for (int c = 3; c < 6; ++c) tr[h][c] = (T)(2 * m * d[c] - 2 * mu0 * e[c]);
     }
 #pragma unroll
-    for (int c = 0; c < 6; ++c) lines[c * PL + pz] = make_double2(tr[0][c], tr[1][c]);
+    for (int c = 0; c < 6; ++c) lines[c * PL + pz] = mk<C>(tr[0][c], tr[1][c]);
   }
   __syncthreads();
   warp_fft<NZ, -1, 2>(lw, PL, tw, lane);
   for (int cc = 0; cc < 2; ++cc) {
     const int c = 2 * warp + cc;
     const C* ln = lines + c * PL;
-    C* ra = R.spec + c * plane + l0 * ld;
+    C* ra = spec + c * plane + l0 * ld;
     for (int k = lane; k < NZH; k += 32) {
       const C z = ln[pidx<C>(k)];
       const C w = ln[pidx<C>(k == 0 ? 0 : NZ - k)];
-      ra[k] = make_double2(0.5 * (z.x + w.x), 0.5 * (z.y - w.y));
-      ra[ld + k] = make_double2(0.5 * (z.y + w.y), -0.5 * (z.x - w.x));
+      ra[k] = mk<C>(T(0.5) * (z.x + w.x), T(0.5) * (z.y - w.y));
+      ra[ld + k] = mk<C>(T(0.5) * (z.y + w.y), T(-0.5) * (z.x - w.x));
     }
   }
   if (!IN_SPEC) return;
-  ls3d_decide(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, s_last);
+  ls3d_decide<FINAL>(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, s_last);
 }
 
-template <bool IN_SPEC>
+template <typename T, bool IN_SPEC, bool FINAL>
 __global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
                                                             const int* __restrict__ map, const int* __restrict__ loc,
                                                             double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
@@ -647,7 +700,7 @@ __global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __re
   }
   __syncthreads();
   const long long l0 = 2LL * loc[item];
-#define MGK_Z3_CASE(n) case n: ls3_zline_body<IN_SPEC, n>(R, S, item, r, l0, partials, rep_counter, ctl, cond, use_cond, guard_cap, smem_raw, &bar, red, &s_last); break;
+#define MGK_Z3_CASE(n) case n: ls3_zline_body<T, IN_SPEC, FINAL, n>(R, S, item, r, l0, partials, rep_counter, ctl, cond, use_cond, guard_cap, smem_raw, &bar, red, &s_last); break;
   switch (R.nz) {
     MGK_Z3_CASE(64) MGK_Z3_CASE(96) MGK_Z3_CASE(128)
     default: break;
@@ -655,10 +708,10 @@ __global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __re
 #undef MGK_Z3_CASE
 }
 
-template <int AXIS, int SIGN, int NL>
+template <typename T, int AXIS, int SIGN, int NL>
 __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState& S, int o, int k0,
                                               unsigned char* smem) {
-  using C = double2;
+  using C = C_t<T>;
   constexpr int PL = padded_len<C>(NL);
   constexpr int TC = kL3Tile;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -668,7 +721,7 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   const long long jstride = AXIS == 1 ? ld : (long long)ny * ld;
   const long long obase = AXIS == 1 ? (long long)o * ny * ld : (long long)o * ld;
   C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t)
-  C* spec = R.spec;
+  C* spec = L3F<T>::spec(R);
   constexpr int TOT = 6 * NL * TC;
   for (int e = threadIdx.x; e < TOT; e += 6 * 32) {
     const int c = e / (NL * TC);
@@ -678,7 +731,7 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   }
   cp_async_wait_all();
   __syncthreads();
-  const C* tw = reinterpret_cast<const C*>((AXIS == 1 ? R.fy : R.fx).tw);
+  const C* tw = reinterpret_cast<const C*>((AXIS == 1 ? L3F<T>::fy(R) : L3F<T>::fx(R)).tw);
   C* l0 = lines + warp * TC * PL;
   warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0, PL, tw, lane);
   warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0 + 2 * PL, PL, tw, lane);
@@ -692,10 +745,13 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
       const int t = e / NL, kx = e - t * NL;
       const int kz = k0 + t;
       const int pk = pidx<C>(kx);
-      C tv[6], ev[6];
-      for (int c = 0; c < 6; ++c) tv[c] = lines[(c * TC + t) * PL + pk];
+      double2 tv[6], ev[6];
+      for (int c = 0; c < 6; ++c) {
+        const C v = lines[(c * TC + t) * PL + pk];
+        tv[c] = make_double2((double)v.x, (double)v.y);
+      }
       if (kx == 0 && ky == 0 && kz == 0) {
-        for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = make_double2(0.0, 0.0);
+        for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = mk<C>(T(0), T(0));
         continue;
       }
       const double ux = (double)fftfreq3(kx, nx) / nx, uz = (double)fftfreq3(kz, nz) / nz;
@@ -704,11 +760,11 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
       gamma3d_apply(tv, n0, n1, n2, S.inv2mu0, S.Bc, ev);
       const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
       if (nqx || nqy || nqz) {
-        C fv[6];
+        double2 fv[6];
         gamma3d_apply(tv, nqx ? -n0 : n0, nqy ? -n1 : n1, nqz ? -n2 : n2, S.inv2mu0, S.Bc, fv);
         for (int c = 0; c < 6; ++c) ev[c] = make_double2(0.5 * (ev[c].x + fv[c].x), 0.5 * (ev[c].y + fv[c].y));
       }
-      for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = make_double2(ev[c].x * scale, ev[c].y * scale);
+      for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = mk<C>((T)(ev[c].x * scale), (T)(ev[c].y * scale));
     }
     __syncthreads();
     warp_fft<NL, +1, 2>(l0, PL, tw, lane);
@@ -723,7 +779,7 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   }
 }
 
-template <int AXIS, int SIGN>
+template <typename T, int AXIS, int SIGN>
 __global__ void __launch_bounds__(192, 2) ls3d_axis_fast_kernel(const Ls3dRep* __restrict__ reps,
                                                              const Ls3dState* __restrict__ st,
                                                              const int* __restrict__ map, const int* __restrict__ loc) {
@@ -737,12 +793,36 @@ __global__ void __launch_bounds__(192, 2) ls3d_axis_fast_kernel(const Ls3dRep* _
   const int o = loc[item] / ntile;
   const int k0 = (loc[item] - o * ntile) * kL3Tile;
   const int nl = AXIS == 1 ? R.ny : R.nx;
-#define MGK_A3_CASE(n) case n: ls3_axis_body<AXIS, SIGN, n>(R, S, o, k0, smem_raw); break;
+#define MGK_A3_CASE(n) case n: ls3_axis_body<T, AXIS, SIGN, n>(R, S, o, k0, smem_raw); break;
   switch (nl) {
     MGK_A3_CASE(64) MGK_A3_CASE(96) MGK_A3_CASE(128)
     default: break;
   }
 #undef MGK_A3_CASE
+}
+
+// Mixed plans, between the phases: FP64 field from the FP32 one; grid (G, nsel)
+__global__ void ls3d_promote_kernel(const Ls3dRep* reps, const int* sel) {
+  const int r = sel[blockIdx.y];
+  const Ls3dRep& R = reps[r];
+  const long long n6 = 6 * R.N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n6; i += (long long)gridDim.x * blockDim.x)
+    R.eps[i] = (double)R.eps32[i];
+}
+
+// replicas that finished phase 1 re-enter for phase 2; resets the control block
+__global__ void ls3d_phase2_kernel(Ls3dState* st, const int* sel, int nsel, Ls3dCtl* ctl) {
+  if (threadIdx.x != 0) return;
+  unsigned int n = 0;
+  for (int q = 0; q < nsel; ++q) {
+    Ls3dState& S = st[sel[q]];
+    if (S.done == 1) { S.done = 0; S.phase_iter = 0; ++n; }
+  }
+  ctl->n_active = n;
+  ctl->decided = 0;
+  ctl->still = 0;
+  ctl->bodies = 0;
+  ctl->any = n > 0;
 }
 
 // outputs (nx,ny,nz,3,3) and partial sums for the means; grid (G, nsel)
@@ -817,6 +897,8 @@ struct mgk_ls3d_plan {
   long long maxN = 0;
   size_t zl_smem = 0, ax_smem = 0;
   int fast = 0;  // warp-line kernels (every side 64, 96 or 128)
+  int prec = MGK_FP64;
+  size_t zl_smem32 = 0, ax_smem32 = 0;
   std::vector<Ls3dRep> reps;
   std::vector<char> has_material;
   std::vector<void*> allocations;
@@ -847,6 +929,34 @@ static int a3(mgk_ls3d_t p, void** ptr, size_t bytes) {
     return MGK_OOM;
   }
   p->allocations.push_back(*ptr);
+  return MGK_OK;
+}
+
+// Precision form (warp-line plans only): MGK_MIXED runs FP32 iterations
+// (FP32 fields, spectra and Gamma0) until the update norm is below
+// max(tol, 2e-6), then FP64 iterations from that field to tol.
+extern "C" int mgk_ls3d_set_precision(mgk_ls3d_t p, int precision) {
+  MGK_REQUIRE(p, "mgk_ls3d_set_precision: null plan");
+  MGK_REQUIRE(precision == MGK_FP64 || precision == MGK_MIXED, "mgk_ls3d_set_precision: bad precision");
+  MGK_REQUIRE(precision == MGK_FP64 || p->fast,
+              "mgk_ls3d_set_precision: the mixed form needs every side in {64, 96, 128}");
+  if (precision == MGK_MIXED && !p->reps[0].mu32) {
+    for (int r = 0; r < p->nrep; ++r) {
+      Ls3dRep& R = p->reps[r];
+      void* f = nullptr;
+      int st = a3(p, &f, sizeof(float) * R.N * 14);
+      if (st) return st;
+      float* fl = reinterpret_cast<float*>(f);
+      R.mu32 = fl; R.lam32 = fl + R.N; R.eps32 = fl + 2 * R.N; R.ep32 = fl + 8 * R.N;
+      R.fx32 = R.fx; R.fy32 = R.fy; R.fz32 = R.fz;
+      R.fx32.tw = twiddles(R.nx, 1); R.fy32.tw = twiddles(R.ny, 1); R.fz32.tw = twiddles(R.nz, 1);
+      if (!R.fx32.tw || !R.fy32.tw || !R.fz32.tw) return MGK_OOM;
+      p->has_material[r] = 0;  // the FP32 copies come with the next set_material
+    }
+    MGK_CUDA(cudaMemcpy(p->d_reps, p->reps.data(), sizeof(Ls3dRep) * p->nrep, cudaMemcpyHostToDevice));
+  }
+  if (precision != p->prec) p->graph_mode = -1;
+  p->prec = precision;
   return MGK_OK;
 }
 
@@ -905,8 +1015,10 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
     R.fx.tw = twiddles(R.nx, MGK_FP64); R.fy.tw = twiddles(R.ny, MGK_FP64); R.fz.tw = twiddles(R.nz, MGK_FP64);
     if (!R.fx.tw || !R.fy.tw || !R.fz.tw) return fail(MGK_OOM);
     if (p->fast) {
-      p->zl_smem = std::max(p->zl_smem, (size_t)ls3_zl_smem(R.nz));
-      p->ax_smem = std::max(p->ax_smem, (size_t)ls3_ax_smem(std::max(R.nx, R.ny)));
+      p->zl_smem = std::max(p->zl_smem, (size_t)ls3_zl_smem(R.nz, 16));
+      p->ax_smem = std::max(p->ax_smem, (size_t)ls3_ax_smem(std::max(R.nx, R.ny), 16));
+      p->zl_smem32 = std::max(p->zl_smem32, (size_t)ls3_zl_smem(R.nz, 8));
+      p->ax_smem32 = std::max(p->ax_smem32, (size_t)ls3_ax_smem(std::max(R.nx, R.ny), 8));
     } else {
       p->zl_smem = std::max(p->zl_smem, 2 * 6 * (size_t)R.nz * sizeof(double2));
       p->ax_smem = std::max(p->ax_smem, 2 * 6 * (size_t)R.tc * std::max(R.nx, R.ny) * sizeof(double2));
@@ -925,11 +1037,16 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
   }
   int st;
   if (p->fast &&
-      (raise_smem((const void*)ls3d_zline_fast_kernel<true>, (int)p->zl_smem) ||
-       raise_smem((const void*)ls3d_zline_fast_kernel<false>, (int)p->zl_smem) ||
-       raise_smem((const void*)ls3d_axis_fast_kernel<1, -1>, (int)p->ax_smem) ||
-       raise_smem((const void*)ls3d_axis_fast_kernel<1, 1>, (int)p->ax_smem) ||
-       raise_smem((const void*)ls3d_axis_fast_kernel<0, 0>, (int)p->ax_smem))) {
+      (raise_smem((const void*)ls3d_zline_fast_kernel<double, true, true>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast_kernel<double, false, true>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, -1>, (int)p->ax_smem) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, 1>, (int)p->ax_smem) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<double, 0, 0>, (int)p->ax_smem) ||
+       raise_smem((const void*)ls3d_zline_fast_kernel<float, true, false>, (int)p->zl_smem32) ||
+       raise_smem((const void*)ls3d_zline_fast_kernel<float, false, false>, (int)p->zl_smem32) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<float, 1, -1>, (int)p->ax_smem32) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<float, 1, 1>, (int)p->ax_smem32) ||
+       raise_smem((const void*)ls3d_axis_fast_kernel<float, 0, 0>, (int)p->ax_smem32))) {
     set_error("mgk_ls3d_create: cudaFuncSetAttribute failed");
     return fail(MGK_CUDA_ERROR);
   }
@@ -1030,40 +1147,48 @@ struct Loop3 {
   int nzl, ny, nx;
   size_t zs, as;
   int fast;
+  // mixed plans: FP32 phase shared memory, the selection and the
+  // per-voxel grid of the promote kernel
+  size_t zs32, as32;
+  const int* sel;
+  int nsel, G;
 };
 
-static void* zline_fn(int fast, bool in_spec) {
-  if (fast) return in_spec ? (void*)ls3d_zline_fast_kernel<true> : (void*)ls3d_zline_fast_kernel<false>;
+// kernels of one iteration: `f32` selects the FP32 phase of a mixed plan
+// (warp-line kernels only; its decisions end phase 1, not the solve)
+static void* zline_fn(int fast, bool in_spec, bool f32 = false) {
+  if (fast && f32)
+    return in_spec ? (void*)ls3d_zline_fast_kernel<float, true, false> : (void*)ls3d_zline_fast_kernel<float, false, false>;
+  if (fast)
+    return in_spec ? (void*)ls3d_zline_fast_kernel<double, true, true> : (void*)ls3d_zline_fast_kernel<double, false, true>;
   return in_spec ? (void*)ls3d_zline_kernel<true> : (void*)ls3d_zline_kernel<false>;
 }
-template <int AXIS, int SIGN> static void* axis_fn(int fast) {
-  return fast ? (void*)ls3d_axis_fast_kernel<AXIS, SIGN> : (void*)ls3d_axis_kernel<AXIS, SIGN>;
+template <int AXIS, int SIGN> static void* axis_fn(int fast, bool f32 = false) {
+  if (fast && f32) return (void*)ls3d_axis_fast_kernel<float, AXIS, SIGN>;
+  return fast ? (void*)ls3d_axis_fast_kernel<double, AXIS, SIGN> : (void*)ls3d_axis_kernel<AXIS, SIGN>;
 }
 
-static int body3(const Loop3& a, cudaStream_t s) {
+static int body3(const Loop3& a, cudaStream_t s, bool f32 = false) {
   const dim3 ab(a.fast ? 192 : kT3), zb(a.fast ? 96 : kT3);
+  const size_t as = f32 ? a.as32 : a.as, zs = f32 ? a.zs32 : a.zs;
   void* ay[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.ym, (void*)&a.yl};
   void* ax[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.xm, (void*)&a.xl};
   cudaGraphConditionalHandle h = 0;
   int zero = 0;
   void* az[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.zm, (void*)&a.zl, (void*)&a.part, (void*)&a.ctr,
                 (void*)&a.ctl, &h, &zero, &zero};
-  MGK_CUDA(cudaLaunchKernel(axis_fn<1, -1>(a.fast), dim3(a.ny), ab, ay, a.as, s));
-  MGK_CUDA(cudaLaunchKernel(axis_fn<0, 0>(a.fast), dim3(a.nx), ab, ax, a.as, s));
-  MGK_CUDA(cudaLaunchKernel(axis_fn<1, 1>(a.fast), dim3(a.ny), ab, ay, a.as, s));
-  MGK_CUDA(cudaLaunchKernel(zline_fn(a.fast, true), dim3(a.nzl), zb, az, a.zs, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<1, -1>(a.fast, f32), dim3(a.ny), ab, ay, as, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<0, 0>(a.fast, f32), dim3(a.nx), ab, ax, as, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<1, 1>(a.fast, f32), dim3(a.ny), ab, ay, as, s));
+  MGK_CUDA(cudaLaunchKernel(zline_fn(a.fast, true, f32), dim3(a.nzl), zb, az, zs, s));
   return MGK_OK;
 }
 
-static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
-  if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
-  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
-  cudaGraph_t g;
-  MGK_CUDA(cudaGraphCreate(&g, 0));
+// one while node running iterations of the FP32 (phase 1) or FP64 kernels
+static int add_while3(cudaGraph_t g, const cudaGraphNode_t* dep, Loop3& a, bool f32, int* cap,
+                      cudaGraphNode_t* out) {
   cudaGraphConditionalHandle h;
-  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) {
-    cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR;
-  }
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) return MGK_CUDA_ERROR;
   alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
   memset(raw, 0, sizeof(raw));
   cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
@@ -1071,8 +1196,7 @@ static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
   cp.conditional.handle = h;
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
-  cudaGraphNode_t w;
-  if (cudaGraphAddNode(&w, g, nullptr, 0, &cp)) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  if (cudaGraphAddNode(out, g, dep, dep ? 1 : 0, &cp)) return MGK_CUDA_ERROR;
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   cudaGraphNode_t prev = nullptr, node;
   auto add = [&](void* fn, dim3 grid, size_t smem, void** args, int block) {
@@ -1086,15 +1210,60 @@ static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
   void* ay[] = {&a.reps, &a.st, &a.ym, &a.yl};
   void* ax[] = {&a.reps, &a.st, &a.xm, &a.xl};
   int use = 1;
-  void* az[] = {&a.reps, &a.st, &a.zm, &a.zl, &a.part, &a.ctr, &a.ctl, &h, &use, &cap};
+  void* az[] = {&a.reps, &a.st, &a.zm, &a.zl, &a.part, &a.ctr, &a.ctl, &h, &use, cap};
   const int ab = a.fast ? 192 : kT3, zb = a.fast ? 96 : kT3;
-  cudaError_t e = add(axis_fn<1, -1>(a.fast), dim3(a.ny), a.as, ay, ab);
-  if (!e) e = add(axis_fn<0, 0>(a.fast), dim3(a.nx), a.as, ax, ab);
-  if (!e) e = add(axis_fn<1, 1>(a.fast), dim3(a.ny), a.as, ay, ab);
-  if (!e) e = add(zline_fn(a.fast, true), dim3(a.nzl), a.zs, az, zb);
+  const size_t as = f32 ? a.as32 : a.as, zs = f32 ? a.zs32 : a.zs;
+  cudaError_t e = add(axis_fn<1, -1>(a.fast, f32), dim3(a.ny), as, ay, ab);
+  if (!e) e = add(axis_fn<0, 0>(a.fast, f32), dim3(a.nx), as, ax, ab);
+  if (!e) e = add(axis_fn<1, 1>(a.fast, f32), dim3(a.ny), as, ay, ab);
+  if (!e) e = add(zline_fn(a.fast, true, f32), dim3(a.nzl), zs, az, zb);
+  return e ? MGK_CUDA_ERROR : MGK_OK;
+}
+
+// Loop graph: FP64 plans one while node; mixed plans [FP32 while, promote,
+// phase-2 set-up, first FP64 z-line pass, FP64 while].
+static int graph3(mgk_ls3d_t p, Loop3& a, int cap) {
+  if (p->exec) { cudaGraphExecDestroy(p->exec); p->exec = nullptr; }
+  if (p->graph) { cudaGraphDestroy(p->graph); p->graph = nullptr; }
+  cudaGraph_t g;
+  MGK_CUDA(cudaGraphCreate(&g, 0));
+  int capv = cap;
+  int rc = MGK_OK;
+  cudaGraphNode_t last;
+  if (p->prec == MGK_MIXED) {
+    cudaGraphNode_t w1, np, n2, nz0;
+    rc = add_while3(g, nullptr, a, true, &capv, &w1);
+    if (rc == MGK_OK) {
+      cudaKernelNodeParams k;
+      memset(&k, 0, sizeof(k));
+      void* ap[] = {&a.reps, (void*)&a.sel};
+      k.func = (void*)ls3d_promote_kernel; k.gridDim = dim3(a.G, a.nsel); k.blockDim = dim3(kT3); k.kernelParams = ap;
+      if (cudaGraphAddKernelNode(&np, g, &w1, 1, &k)) rc = MGK_CUDA_ERROR;
+    }
+    if (rc == MGK_OK) {
+      cudaKernelNodeParams k;
+      memset(&k, 0, sizeof(k));
+      void* ap[] = {&a.st, (void*)&a.sel, &a.nsel, &a.ctl};
+      k.func = (void*)ls3d_phase2_kernel; k.gridDim = dim3(1); k.blockDim = dim3(32); k.kernelParams = ap;
+      if (cudaGraphAddKernelNode(&n2, g, &np, 1, &k)) rc = MGK_CUDA_ERROR;
+    }
+    if (rc == MGK_OK) {
+      cudaKernelNodeParams k;
+      memset(&k, 0, sizeof(k));
+      cudaGraphConditionalHandle h0 = 0;
+      int zero = 0;
+      void* ap[] = {&a.reps, &a.st, &a.zm, &a.zl, &a.part, &a.ctr, &a.ctl, &h0, &zero, &zero};
+      k.func = zline_fn(a.fast, false, false); k.gridDim = dim3(a.nzl); k.blockDim = dim3(a.fast ? 96 : kT3);
+      k.sharedMemBytes = (unsigned)a.zs; k.kernelParams = ap;
+      if (cudaGraphAddKernelNode(&nz0, g, &n2, 1, &k)) rc = MGK_CUDA_ERROR;
+    }
+    if (rc == MGK_OK) rc = add_while3(g, &nz0, a, false, &capv, &last);
+  } else {
+    rc = add_while3(g, nullptr, a, false, &capv, &last);
+  }
   cudaGraphExec_t x = nullptr;
-  if (!e) e = cudaGraphInstantiate(&x, g, 0);
-  if (e) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
+  if (rc == MGK_OK && cudaGraphInstantiate(&x, g, 0)) rc = MGK_CUDA_ERROR;
+  if (rc) { cudaGraphDestroy(g); cudaGetLastError(); return MGK_CUDA_ERROR; }
   p->graph = g;
   p->exec = x;
   return MGK_OK;
@@ -1169,13 +1338,15 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
   }
   if (n_active > 0) {
     Loop3 a{p->d_reps, p->d_st, d_zm, d_zl, d_ym, d_yl, d_xm, d_xl, p->d_part, p->d_repctr, p->d_ctl,
-            nzl, ny_, nx_, p->zl_smem, p->ax_smem, p->fast};
+            nzl, ny_, nx_, p->zl_smem, p->ax_smem, p->fast, p->zl_smem32, p->ax_smem32, d_sel, nsel, G};
+    const bool mixed = p->prec == MGK_MIXED;
     {
       cudaGraphConditionalHandle h0 = 0;
       int zero = 0;
       void* az0[] = {(void*)&p->d_reps, (void*)&p->d_st, (void*)&d_zm, (void*)&d_zl, (void*)&p->d_part,
                      (void*)&p->d_repctr, (void*)&p->d_ctl, &h0, &zero, &zero};
-      MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false), dim3(nzl), dim3(p->fast ? 96 : kT3), az0, p->zl_smem, s));
+      MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false, mixed), dim3(nzl), dim3(p->fast ? 96 : kT3), az0,
+                                mixed ? p->zl_smem32 : p->zl_smem, s));
     }
     const int cap = max_iter + 2 > 1000 ? max_iter + 2 : 1000;
     if (p->graph_mode == 1 && (changed || cap > p->graph_cap)) p->graph_mode = -1;
@@ -1190,13 +1361,24 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
     if (p->graph_mode == 1) {
       MGK_CUDA(cudaGraphLaunch(p->exec, s));
     } else {
-      for (int it = 0; it < max_iter; ++it) {
-        rc = body3(a, s);
-        if (rc) return rc;
-        Ls3dCtl hc;
-        MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls3dCtl), cudaMemcpyDeviceToHost, s));
-        MGK_CUDA(cudaStreamSynchronize(s));
-        if (!hc.any) break;
+      for (int phase = mixed ? 1 : 2; phase <= 2; ++phase) {
+        if (phase == 2 && mixed) {
+          ls3d_promote_kernel<<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, d_sel);
+          ls3d_phase2_kernel<<<1, 32, 0, s>>>(p->d_st, d_sel, nsel, p->d_ctl);
+          cudaGraphConditionalHandle h0 = 0;
+          int zero = 0;
+          void* az1[] = {(void*)&p->d_reps, (void*)&p->d_st, (void*)&d_zm, (void*)&d_zl, (void*)&p->d_part,
+                         (void*)&p->d_repctr, (void*)&p->d_ctl, &h0, &zero, &zero};
+          MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false, false), dim3(nzl), dim3(96), az1, p->zl_smem, s));
+        }
+        for (int it = 0; it < max_iter; ++it) {
+          rc = body3(a, s, phase == 1);
+          if (rc) return rc;
+          Ls3dCtl hc;
+          MGK_CUDA(cudaMemcpyAsync(&hc, p->d_ctl, sizeof(Ls3dCtl), cudaMemcpyDeviceToHost, s));
+          MGK_CUDA(cudaStreamSynchronize(s));
+          if (!hc.any) break;
+        }
       }
     }
   }

@@ -201,10 +201,12 @@ def spectral_solver_2d(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6,
 
 
 class Ls3dBatch:
-    """Plan-owning batch of 3D LS replicas (FP64).  Fields: E, nu (nx,ny,nz);
-    eps_plastic, eps, sig (nx,ny,nz,3,3) torch float64 CUDA tensors."""
+    """Plan-owning batch of 3D LS replicas.  Fields: E, nu (nx,ny,nz);
+    eps_plastic, eps, sig (nx,ny,nz,3,3) torch float64 CUDA tensors.
+    ``precision``: "fp64", or "mixed" (FP32 phase then FP64; every side 64, 96
+    or 128)."""
 
-    def __init__(self, sizes, device=None):
+    def __init__(self, sizes, device=None, precision="fp64"):
         torch = _torch()
         self.sizes = [tuple(int(v) for v in s) for s in sizes]
         self.nrep = len(self.sizes)
@@ -217,6 +219,9 @@ class Ls3dBatch:
             L.check(L.lib().mgk_ls3d_create_batch(self.nrep, nx, ny, nz, ctypes.byref(h)), "mgk_ls3d_create_batch")
         self._h = h
         self._keep = {}
+        self.precision = precision
+        if precision != "fp64":
+            L.check(L.lib().mgk_ls3d_set_precision(h, L.MIXED), "mgk_ls3d_set_precision")
 
     def __del__(self):
         h = getattr(self, "_h", None)

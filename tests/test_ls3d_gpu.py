@@ -103,3 +103,31 @@ def test_warp_line_batch_matches_single_plans():
         o1 = torch.empty_like(outs[r]); s1 = torch.empty_like(outs[r])
         S.solve([0], [eb], [o1], [s1], max_iter=200, tol=1e-10)
         assert rel(outs[r].cpu().numpy(), o1.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.parametrize("sizes", [[(64, 64, 64)], [(64, 96, 128), (64, 64, 64)]])
+def test_mixed_precision_matches_fp64(sizes):
+    # FP32 phase then FP64 to the same tolerance: converged fields agree with
+    # the FP64 solve within the mixed form's bound (1e-6; ~1e-8 in practice)
+    import torch
+    from mgkmc_b200.linear_elastic_simulator import Ls3dBatch
+    rng = np.random.default_rng(21)
+    probs = []
+    for sh in sizes:
+        E, nu = W.ls3d_material(*sh, rng)
+        probs.append((E, nu, W.pure_shear_eigenstrain_3d(*sh, rng)))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    eb = np.zeros((3, 3)); eb[0, 0] = 0.01; eb[1, 2] = 0.002
+    res = {}
+    for prec in ("fp64", "mixed"):
+        B = Ls3dBatch(sizes, precision=prec)
+        outs = []
+        for r, (E, nu, ep) in enumerate(probs):
+            B.set_material(r, t(E), t(nu), t(ep))
+            outs.append(torch.empty(E.shape + (3, 3), dtype=torch.float64, device="cuda"))
+        sigs = [torch.empty_like(o) for o in outs]
+        infos = B.solve(list(range(len(sizes))), [eb] * len(sizes), outs, sigs, max_iter=300, tol=1e-8)
+        assert all(i.status == 0 for i in infos)
+        res[prec] = [(o.cpu().numpy(), g.cpu().numpy()) for o, g in zip(outs, sigs)]
+    for (e64, s64), (e32, s32) in zip(res["fp64"], res["mixed"]):
+        assert rel(e32, e64) < 1e-6 and rel(s32, s64) < 1e-6
