@@ -734,9 +734,13 @@ __global__ void __launch_bounds__(256) fs_kp_kernel(FsArgs a) {
 // The same five matvec stages for grids whose sides are 64, 96 or 128 (the
 // served and benchmark sizes): lines sit in padded shared memory and
 // each warp transforms its own lines with warp-local passes.
-//   axis kernels: CTA of 9 warps per tile of kFsTile kz columns at one x (y
-//     pass) or one y (x pass); warp c transforms component c's lines; the x
-//     pass applies G between the forward and inverse transforms (CTA barrier).
+//   axis kernels: CTA of NC warps per tile of kFsTile kz columns at one x (y
+//     pass) or one y (x pass); warp c transforms component c0 + c's lines.  The
+//     x pass applies G between the forward and inverse transforms (CTA
+//     barrier); G couples the three components of a row of the tensor only.
+//     FP64 CTAs hold 3 components (one row; three CTAs per tile: 5 resident
+//     CTAs of 3 warps per SM instead of one of 9 at the registers an FP64 line
+//     pair needs), FP32 CTAs all 9.
 //   z kernels: CTA of 3 warps per pair of z-lines; the per-voxel stage (K:p or
 //     P, or q and the p.q sums) uses all threads, warp w transforms the lines
 //     of components 3w..3w+2.
@@ -747,9 +751,9 @@ __host__ __device__ constexpr int fs_pl(int n, int csz) {
   return csz == 16 ? n + n / 8 + 1 : ((n + n / 16 + 2) & ~1);
 }
 
-template <int SIGN, typename T, int NL, bool XG>
-__device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, long long obase, long long jstride,
-                                             unsigned char* smem) {
+template <int SIGN, typename T, int NL, bool XG, int NC>
+__device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, int c0, long long obase,
+                                             long long jstride, unsigned char* smem) {
   using C = C_t<T>;
   constexpr int PL = padded_len<C>(NL);
   constexpr int TC = kFsTile;
@@ -757,10 +761,10 @@ __device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, lon
   const int nzh = a.nzh;
   const int tcw = min(TC, nzh - k0);
   const long long plane = (long long)a.nx * a.ny * a.ld;
-  C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t)
-  C* spec = FsP<T>::spec(a);
-  constexpr int TOT = 9 * NL * TC;
-  for (int e = threadIdx.x; e < TOT; e += 9 * 32) {
+  C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t), c relative to c0
+  C* spec = FsP<T>::spec(a) + c0 * plane;
+  constexpr int TOT = NC * NL * TC;
+  for (int e = threadIdx.x; e < TOT; e += NC * 32) {
     const int c = e / (NL * TC);
     const int rem = e - c * NL * TC;
     const int j = rem / TC, t = rem - j * TC;
@@ -773,28 +777,30 @@ __device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, lon
   C* l0 = lines + warp * TC * PL;  // warp = component
   warp_fft<NL, XG ? -1 : SIGN, 2>(l0, PL, tw, lane);
   warp_fft<NL, XG ? -1 : SIGN, 2>(l0 + 2 * PL, PL, tw, lane);
-  if (XG) {
+  if constexpr (XG) {
     __syncthreads();
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const T scale = (T)(1.0 / (double)a.N);
     const int ky = o;
     const double uy = (double)ffq(ky, ny) / ny;
     const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
-    for (int e = threadIdx.x; e < tcw * NL; e += 9 * 32) {
+    for (int e = threadIdx.x; e < tcw * NL; e += NC * 32) {
       const int t = e / NL, kx = e - t * NL;
       const int kz = k0 + t;
       const int pk = pidx<C>(kx);
       const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
       if ((kx == 0 && ky == 0 && kz == 0) || nqx || nqy || nqz) {
-        for (int c = 0; c < 9; ++c) lines[(c * TC + t) * PL + pk] = mk<C>(T(0), T(0));
+        for (int c = 0; c < NC; ++c) lines[(c * TC + t) * PL + pk] = mk<C>(T(0), T(0));
         continue;
       }
       const double ux = (double)ffq(kx, nx) / nx, uz = (double)ffq(kz, nz) / nz;
       const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
       const T n[3] = {(T)(ux * inv), (T)(uy * inv), (T)(uz * inv)};
-      C A[9];
-      for (int c = 0; c < 9; ++c) A[c] = lines[(c * TC + t) * PL + pk];
-      for (int i = 0; i < 3; ++i) {
+      // (G:A)_ij = (A_il n_l) n_j couples the three components of a row of A
+      // only: the CTA's NC components are NC / 3 whole rows
+      C A[NC];
+      for (int c = 0; c < NC; ++c) A[c] = lines[(c * TC + t) * PL + pk];
+      for (int i = 0; i < NC / 3; ++i) {
         T vx = 0, vy = 0;
         for (int l = 0; l < 3; ++l) { vx += A[3 * i + l].x * n[l]; vy += A[3 * i + l].y * n[l]; }
         for (int j = 0; j < 3; ++j)
@@ -806,7 +812,7 @@ __device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, lon
     warp_fft<NL, +1, 2>(l0 + 2 * PL, PL, tw, lane);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < TOT; e += 9 * 32) {
+  for (int e = threadIdx.x; e < TOT; e += NC * 32) {
     const int c = e / (NL * TC);
     const int rem = e - c * NL * TC;
     const int j = rem / TC, t = rem - j * TC;
@@ -814,17 +820,27 @@ __device__ __forceinline__ void fs_axis_body(const FsArgs& a, int o, int k0, lon
   }
 }
 
+// components per CTA of the axis kernels (FP32 keeps 9: measured faster at
+// 128^3), and resident-CTA targets for the register allocator
+__host__ __device__ constexpr int fs_axis_nc(bool, int tsz) { return tsz == 4 ? 9 : 3; }
+__host__ __device__ constexpr int fs_axis_minb(bool xg, int tsz) { return fs_axis_nc(xg, tsz) == 3 ? 5 : (tsz == 8 ? 1 : 3); }
+
 // y pass (XG = false) or x pass with G (XG = true); grid = (nx or ny) * ntile
+// * (9 / NC), the component group fastest
 template <int SIGN, typename T, bool XG>
-__global__ void __launch_bounds__(9 * 32, sizeof(T) == 8 ? 1 : 3) fs_axis_fast_kernel(FsArgs a) {
+__global__ void __launch_bounds__(fs_axis_nc(XG, sizeof(T)) * 32, fs_axis_minb(XG, sizeof(T)))
+    fs_axis_fast_kernel(FsArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NC = fs_axis_nc(XG, sizeof(T));
   const int ntile = (a.nzh + kFsTile - 1) / kFsTile;
-  const int o = blockIdx.x / ntile;
-  const int k0 = (blockIdx.x - o * ntile) * kFsTile;
+  const int cg = blockIdx.x % (9 / NC);
+  const int item = blockIdx.x / (9 / NC);
+  const int o = item / ntile;
+  const int k0 = (item - o * ntile) * kFsTile;
   const long long obase = XG ? (long long)a.ld : (long long)a.ny * a.ld;
   const long long jstride = XG ? (long long)a.ny * a.ld : (long long)a.ld;
   const int nl = XG ? a.nx : a.ny;
-#define MGK_AX_CASE(n) case n: fs_axis_body<SIGN, T, n, XG>(a, o, k0, obase, jstride, smem_raw); break;
+#define MGK_AX_CASE(n) case n: fs_axis_body<SIGN, T, n, XG, NC>(a, o, k0, cg * NC, obase, jstride, smem_raw); break;
   switch (nl) {
     MGK_AX_CASE(64) MGK_AX_CASE(96) MGK_AX_CASE(128)
     default: break;
@@ -960,7 +976,7 @@ __device__ __forceinline__ void fs_zinv_body(const FsArgs& a, unsigned char* sme
 }
 
 template <int MODE, typename T>
-__global__ void __launch_bounds__(3 * 32) fs_zinv_fast_kernel(FsArgs a) {
+__device__ __forceinline__ void fs_zinv_fast_entry(const FsArgs& a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
 #define MGK_ZI_CASE(n) case n: fs_zinv_body<MODE, T, n>(a, smem_raw, red); break;
@@ -969,6 +985,18 @@ __global__ void __launch_bounds__(3 * 32) fs_zinv_fast_kernel(FsArgs a) {
     default: break;
   }
 #undef MGK_ZI_CASE
+}
+
+// FP32 kernel (the compiler's own register target), and the FP64 kernel with
+// a register target of 5 resident CTAs per SM (measured faster than 4 at
+// 128^3 despite a few spilled registers; the forward z pass is not)
+template <int MODE, typename T>
+__global__ void __launch_bounds__(3 * 32) fs_zinv_fast_kernel(FsArgs a) { fs_zinv_fast_entry<MODE, T>(a); }
+template <int MODE>
+__global__ void __launch_bounds__(3 * 32, 5) fs_zinv_fast64_kernel(FsArgs a) { fs_zinv_fast_entry<MODE, double>(a); }
+template <int MODE, typename T> static void* fs_zinv_fast_fn() {
+  if constexpr (sizeof(T) == 8) return (void*)fs_zinv_fast64_kernel<MODE>;
+  else return (void*)fs_zinv_fast_kernel<MODE, T>;
 }
 
 // FP64 copies of n floats (the mixed form's Krylov solution back to FP64)
@@ -1145,16 +1173,18 @@ extern "C" int mgk_fs3d_create(int nx, int ny, int nz, int model, mgk_fs3d_t* ou
   }
   if (p->fast) {
     const int zs64 = 9 * fs_pl(nz, 16) * 16, zs32 = 9 * fs_pl(nz, 8) * 8;
-    const int ys64 = 9 * kFsTile * fs_pl(ny, 16) * 16, ys32 = 9 * kFsTile * fs_pl(ny, 8) * 8;
-    const int xs64 = 9 * kFsTile * fs_pl(nx, 16) * 16, xs32 = 9 * kFsTile * fs_pl(nx, 8) * 8;
+    const int ys64 = fs_axis_nc(false, 8) * kFsTile * fs_pl(ny, 16) * 16;
+    const int ys32 = fs_axis_nc(false, 4) * kFsTile * fs_pl(ny, 8) * 8;
+    const int xs64 = fs_axis_nc(true, 8) * kFsTile * fs_pl(nx, 16) * 16;
+    const int xs32 = fs_axis_nc(true, 4) * kFsTile * fs_pl(nx, 8) * 8;
     if (raise_smem((const void*)fs_zfwd_fast_kernel<0, double>, zs64) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<1, double>, zs64) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<2, double>, zs64) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<0, float>, zs32) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<3, double>, zs64) ||
         raise_smem((const void*)fs_zfwd_fast_kernel<3, float>, zs32) ||
-        raise_smem((const void*)fs_zinv_fast_kernel<0, double>, zs64) ||
-        raise_smem((const void*)fs_zinv_fast_kernel<1, double>, zs64) ||
+        raise_smem(fs_zinv_fast_fn<0, double>(), zs64) ||
+        raise_smem(fs_zinv_fast_fn<1, double>(), zs64) ||
         raise_smem((const void*)fs_zinv_fast_kernel<0, float>, zs32) ||
         raise_smem((const void*)fs_axis_fast_kernel<-1, double, false>, ys64) ||
         raise_smem((const void*)fs_axis_fast_kernel<1, double, false>, ys64) ||
@@ -1279,8 +1309,9 @@ static int fs_stage_launches(mgk_fs3d_t p, int mode, int zmode, FsLaunch L[6]) {
     const int csz = (int)sizeof(C_t<T>);
     const int ntile = (p->nzh + kFsTile - 1) / kFsTile;
     const size_t zs = 9 * (size_t)fs_pl(p->nz, csz) * csz, zs64 = 9 * (size_t)fs_pl(p->nz, 16) * 16;
-    const size_t ys = 9 * (size_t)kFsTile * fs_pl(p->ny, csz) * csz;
-    const size_t xs = 9 * (size_t)kFsTile * fs_pl(p->nx, csz) * csz;
+    constexpr int ncy = fs_axis_nc(false, sizeof(T)), ncx = fs_axis_nc(true, sizeof(T));
+    const size_t ys = ncy * (size_t)kFsTile * fs_pl(p->ny, csz) * csz;
+    const size_t xs = ncx * (size_t)kFsTile * fs_pl(p->nx, csz) * csz;
     if (mode == 0) {
       L[k++] = {(void*)fs_kp_kernel<T>, dim3(4 * p->nblk), dim3(256), 0, 0};
       L[k++] = {(void*)fs_zfwd_fast_kernel<3, T>, dim3(zl), dim3(96), zs, 1};
@@ -1288,10 +1319,10 @@ static int fs_stage_launches(mgk_fs3d_t p, int mode, int zmode, FsLaunch L[6]) {
       L[k++] = {mode == 1 ? (void*)fs_zfwd_fast_kernel<1, double> : (void*)fs_zfwd_fast_kernel<2, double>, dim3(zl),
                 dim3(96), zs64, 1};
     }
-    L[k++] = {(void*)fs_axis_fast_kernel<-1, T, false>, dim3(p->nx * ntile), dim3(288), ys, 0};
-    L[k++] = {(void*)fs_axis_fast_kernel<-1, T, true>, dim3(p->ny * ntile), dim3(288), xs, 0};
-    L[k++] = {(void*)fs_axis_fast_kernel<1, T, false>, dim3(p->nx * ntile), dim3(288), ys, 0};
-    L[k++] = {zmode == 0 ? (void*)fs_zinv_fast_kernel<0, T> : (void*)fs_zinv_fast_kernel<1, double>, dim3(zl),
+    L[k++] = {(void*)fs_axis_fast_kernel<-1, T, false>, dim3(p->nx * ntile * (9 / ncy)), dim3(32 * ncy), ys, 0};
+    L[k++] = {(void*)fs_axis_fast_kernel<-1, T, true>, dim3(p->ny * ntile * (9 / ncx)), dim3(32 * ncx), xs, 0};
+    L[k++] = {(void*)fs_axis_fast_kernel<1, T, false>, dim3(p->nx * ntile * (9 / ncy)), dim3(32 * ncy), ys, 0};
+    L[k++] = {zmode == 0 ? fs_zinv_fast_fn<0, T>() : fs_zinv_fast_fn<1, double>(), dim3(zl),
               dim3(96), zmode == 0 ? zs : zs64, 0};
   } else {
     const int ntile = (p->nzh + p->tc - 1) / p->tc;

@@ -529,9 +529,9 @@ __global__ void __launch_bounds__(256) ls3d_axis_kernel(const Ls3dRep* __restric
 //     memory with bulk copies while warp w inverts components 2w, 2w+1 of the
 //     spectrum; after one CTA barrier every thread updates its voxels and
 //     builds tau; warp w transforms and stores its two components.
-//   axis kernels: CTA of 6 warps per tile of kL3Tile kz columns at one x (y
-//     pass) or one y (x pass with Gamma0_sym between the transforms); warp c
-//     owns component c's lines.
+//   axis kernels: per tile of kL3Tile kz columns at one x (y passes) or one y
+//     (x pass with Gamma0_sym between the transforms), warp c owns component
+//     c's lines; the x pass CTA holds all 6 components, an FP64 y pass CTA 3.
 constexpr int kL3Tile = 4;
 
 template <typename T> struct L3F;
@@ -673,11 +673,10 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
 }
 
 template <typename T, bool IN_SPEC, bool FINAL>
-__global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
-                                                            const int* __restrict__ map, const int* __restrict__ loc,
-                                                            double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
-                                                            cudaGraphConditionalHandle cond, int use_cond,
-                                                            int guard_cap) {
+__device__ __forceinline__ void ls3d_zline_fast_entry(const Ls3dRep* __restrict__ reps, Ls3dState* st,
+                                                      const int* __restrict__ map, const int* __restrict__ loc,
+                                                      double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
+                                                      cudaGraphConditionalHandle cond, int use_cond, int guard_cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[32];
   __shared__ int s_last;
@@ -708,8 +707,29 @@ __global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __re
 #undef MGK_Z3_CASE
 }
 
-template <typename T, int AXIS, int SIGN, int NL>
-__device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState& S, int o, int k0,
+// FP32 phase kernel (the compiler's own register target), and the FP64
+// kernel with a register target of 5 resident CTAs per SM (measured faster
+// than 4 at 128^3 despite a few spilled registers)
+template <typename T, bool IN_SPEC, bool FINAL>
+__global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
+                                                            const int* __restrict__ map, const int* __restrict__ loc,
+                                                            double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
+                                                            cudaGraphConditionalHandle cond, int use_cond,
+                                                            int guard_cap) {
+  ls3d_zline_fast_entry<T, IN_SPEC, FINAL>(reps, st, map, loc, partials, rep_counter, ctl, cond, use_cond, guard_cap);
+}
+template <bool IN_SPEC, bool FINAL>
+__global__ void __launch_bounds__(96, 5) ls3d_zline_fast64_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
+                                                                const int* __restrict__ map, const int* __restrict__ loc,
+                                                                double* partials, unsigned int* rep_counter,
+                                                                Ls3dCtl* ctl, cudaGraphConditionalHandle cond,
+                                                                int use_cond, int guard_cap) {
+  ls3d_zline_fast_entry<double, IN_SPEC, FINAL>(reps, st, map, loc, partials, rep_counter, ctl, cond, use_cond,
+                                                guard_cap);
+}
+
+template <typename T, int AXIS, int SIGN, int NL, int NC>
+__device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState& S, int o, int k0, int c0,
                                               unsigned char* smem) {
   using C = C_t<T>;
   constexpr int PL = padded_len<C>(NL);
@@ -720,10 +740,10 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   const long long plane = (long long)nx * ny * ld;
   const long long jstride = AXIS == 1 ? ld : (long long)ny * ld;
   const long long obase = AXIS == 1 ? (long long)o * ny * ld : (long long)o * ld;
-  C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t)
-  C* spec = L3F<T>::spec(R);
-  constexpr int TOT = 6 * NL * TC;
-  for (int e = threadIdx.x; e < TOT; e += 6 * 32) {
+  C* lines = reinterpret_cast<C*>(smem);  // line (c * TC + t), c relative to c0
+  C* spec = L3F<T>::spec(R) + c0 * plane;
+  constexpr int TOT = NC * NL * TC;
+  for (int e = threadIdx.x; e < TOT; e += NC * 32) {
     const int c = e / (NL * TC);
     const int rem = e - c * NL * TC;
     const int j = rem / TC, t = rem - j * TC;
@@ -735,13 +755,13 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   C* l0 = lines + warp * TC * PL;
   warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0, PL, tw, lane);
   warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0 + 2 * PL, PL, tw, lane);
-  if (AXIS == 0) {
+  if constexpr (AXIS == 0) {
     __syncthreads();
     const double scale = 1.0 / (double)R.N;
     const int ky = o;
     const double uy = (double)fftfreq3(ky, ny) / ny;
     const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
-    for (int e = threadIdx.x; e < tcw * NL; e += 6 * 32) {
+    for (int e = threadIdx.x; e < tcw * NL; e += NC * 32) {
       const int t = e / NL, kx = e - t * NL;
       const int kz = k0 + t;
       const int pk = pidx<C>(kx);
@@ -771,7 +791,7 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
     warp_fft<NL, +1, 2>(l0 + 2 * PL, PL, tw, lane);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < TOT; e += 6 * 32) {
+  for (int e = threadIdx.x; e < TOT; e += NC * 32) {
     const int c = e / (NL * TC);
     const int rem = e - c * NL * TC;
     const int j = rem / TC, t = rem - j * TC;
@@ -779,12 +799,23 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   }
 }
 
+// components per CTA of the axis kernels: the x pass applies Gamma0 across
+// all 6 components; the FP64 y passes transform 3 components per CTA (two
+// CTAs per tile: 5 resident CTAs of 3 warps per SM instead of 2 of 6 at the
+// registers an FP64 line pair needs).  FP32 y passes keep 6 per CTA (measured
+// faster at 128^3).  Second value: resident-CTA target for the allocator.
+__host__ __device__ constexpr int ls3_axis_nc(int axis, int tsz) { return axis == 0 || tsz == 4 ? 6 : 3; }
+__host__ __device__ constexpr int ls3_axis_minb(int axis, int tsz) { return ls3_axis_nc(axis, tsz) == 3 ? 5 : 2; }
+
+// grid = items * (6 / NC), the component group fastest
 template <typename T, int AXIS, int SIGN>
-__global__ void __launch_bounds__(192, 2) ls3d_axis_fast_kernel(const Ls3dRep* __restrict__ reps,
-                                                             const Ls3dState* __restrict__ st,
-                                                             const int* __restrict__ map, const int* __restrict__ loc) {
+__global__ void __launch_bounds__(ls3_axis_nc(AXIS, sizeof(T)) * 32, ls3_axis_minb(AXIS, sizeof(T)))
+    ls3d_axis_fast_kernel(const Ls3dRep* __restrict__ reps, const Ls3dState* __restrict__ st,
+                          const int* __restrict__ map, const int* __restrict__ loc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int item = blockIdx.x;
+  constexpr int NC = ls3_axis_nc(AXIS, sizeof(T));
+  const int item = blockIdx.x / (6 / NC);
+  const int c0 = (blockIdx.x % (6 / NC)) * NC;
   const int r = map[item];
   const Ls3dRep& R = reps[r];
   const Ls3dState& S = st[r];
@@ -793,7 +824,7 @@ __global__ void __launch_bounds__(192, 2) ls3d_axis_fast_kernel(const Ls3dRep* _
   const int o = loc[item] / ntile;
   const int k0 = (loc[item] - o * ntile) * kL3Tile;
   const int nl = AXIS == 1 ? R.ny : R.nx;
-#define MGK_A3_CASE(n) case n: ls3_axis_body<T, AXIS, SIGN, n>(R, S, o, k0, smem_raw); break;
+#define MGK_A3_CASE(n) case n: ls3_axis_body<T, AXIS, SIGN, n, NC>(R, S, o, k0, c0, smem_raw); break;
   switch (nl) {
     MGK_A3_CASE(64) MGK_A3_CASE(96) MGK_A3_CASE(128)
     default: break;
@@ -1037,8 +1068,8 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
   }
   int st;
   if (p->fast &&
-      (raise_smem((const void*)ls3d_zline_fast_kernel<double, true, true>, (int)p->zl_smem) ||
-       raise_smem((const void*)ls3d_zline_fast_kernel<double, false, true>, (int)p->zl_smem) ||
+      (raise_smem((const void*)ls3d_zline_fast64_kernel<true, true>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast64_kernel<false, true>, (int)p->zl_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, -1>, (int)p->ax_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, 1>, (int)p->ax_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 0, 0>, (int)p->ax_smem) ||
@@ -1160,7 +1191,7 @@ static void* zline_fn(int fast, bool in_spec, bool f32 = false) {
   if (fast && f32)
     return in_spec ? (void*)ls3d_zline_fast_kernel<float, true, false> : (void*)ls3d_zline_fast_kernel<float, false, false>;
   if (fast)
-    return in_spec ? (void*)ls3d_zline_fast_kernel<double, true, true> : (void*)ls3d_zline_fast_kernel<double, false, true>;
+    return in_spec ? (void*)ls3d_zline_fast64_kernel<true, true> : (void*)ls3d_zline_fast64_kernel<false, true>;
   return in_spec ? (void*)ls3d_zline_kernel<true> : (void*)ls3d_zline_kernel<false>;
 }
 template <int AXIS, int SIGN> static void* axis_fn(int fast, bool f32 = false) {
@@ -1171,15 +1202,18 @@ template <int AXIS, int SIGN> static void* axis_fn(int fast, bool f32 = false) {
 static int body3(const Loop3& a, cudaStream_t s, bool f32 = false) {
   const dim3 ab(a.fast ? 192 : kT3), zb(a.fast ? 96 : kT3);
   const size_t as = f32 ? a.as32 : a.as, zs = f32 ? a.zs32 : a.zs;
+  const bool ysplit = a.fast && ls3_axis_nc(1, f32 ? 4 : 8) == 3;  // FP64 y passes: 3 components per CTA
+  const size_t asy = ysplit ? as / 2 : as;
+  const dim3 gy(ysplit ? 2 * a.ny : a.ny), aby(ysplit ? 96 : ab.x);
   void* ay[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.ym, (void*)&a.yl};
   void* ax[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.xm, (void*)&a.xl};
   cudaGraphConditionalHandle h = 0;
   int zero = 0;
   void* az[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.zm, (void*)&a.zl, (void*)&a.part, (void*)&a.ctr,
                 (void*)&a.ctl, &h, &zero, &zero};
-  MGK_CUDA(cudaLaunchKernel(axis_fn<1, -1>(a.fast, f32), dim3(a.ny), ab, ay, as, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<1, -1>(a.fast, f32), gy, aby, ay, asy, s));
   MGK_CUDA(cudaLaunchKernel(axis_fn<0, 0>(a.fast, f32), dim3(a.nx), ab, ax, as, s));
-  MGK_CUDA(cudaLaunchKernel(axis_fn<1, 1>(a.fast, f32), dim3(a.ny), ab, ay, as, s));
+  MGK_CUDA(cudaLaunchKernel(axis_fn<1, 1>(a.fast, f32), gy, aby, ay, asy, s));
   MGK_CUDA(cudaLaunchKernel(zline_fn(a.fast, true, f32), dim3(a.nzl), zb, az, zs, s));
   return MGK_OK;
 }
@@ -1213,9 +1247,13 @@ static int add_while3(cudaGraph_t g, const cudaGraphNode_t* dep, Loop3& a, bool 
   void* az[] = {&a.reps, &a.st, &a.zm, &a.zl, &a.part, &a.ctr, &a.ctl, &h, &use, cap};
   const int ab = a.fast ? 192 : kT3, zb = a.fast ? 96 : kT3;
   const size_t as = f32 ? a.as32 : a.as, zs = f32 ? a.zs32 : a.zs;
-  cudaError_t e = add(axis_fn<1, -1>(a.fast, f32), dim3(a.ny), as, ay, ab);
+  const bool ysplit = a.fast && ls3_axis_nc(1, f32 ? 4 : 8) == 3;  // FP64 y passes: 3 components per CTA
+  const size_t asy = ysplit ? as / 2 : as;
+  const dim3 gy(ysplit ? 2 * a.ny : a.ny);
+  const int aby = ysplit ? 96 : ab;
+  cudaError_t e = add(axis_fn<1, -1>(a.fast, f32), gy, asy, ay, aby);
   if (!e) e = add(axis_fn<0, 0>(a.fast, f32), dim3(a.nx), as, ax, ab);
-  if (!e) e = add(axis_fn<1, 1>(a.fast, f32), dim3(a.ny), as, ay, ab);
+  if (!e) e = add(axis_fn<1, 1>(a.fast, f32), gy, asy, ay, aby);
   if (!e) e = add(zline_fn(a.fast, true, f32), dim3(a.nzl), zs, az, zb);
   return e ? MGK_CUDA_ERROR : MGK_OK;
 }
