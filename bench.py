@@ -67,6 +67,13 @@ def parse():
     ap.add_argument("--serve-window", type=float, default=0.1,
                     help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
                          "0 skips it")
+    ap.add_argument("--profile-case", default="", choices=["", "ls3d", "fs3d", "kmc"],
+                    help="run one kernel-profiling workload instead of the benchmark (for ncu captures): ls3d = "
+                         "LS 3D solves at --profile-n^3 (tol 1e-8, three solves), fs3d = one finite-strain load "
+                         "step at --profile-n^3 (Neo-Hookean + 2 %% F_p, F_xx = 1.005), kmc = three rounds of "
+                         "barrier, exact rates/total and selection at --profile-n^2 x 8 modes")
+    ap.add_argument("--profile-n", type=int, default=128)
+    ap.add_argument("--profile-precision", default="fp64", choices=["fp64", "mixed"])
     a = ap.parse_args()
     global NX, NY
     NX = NY = a.grid
@@ -465,8 +472,59 @@ def run_ours(a):
         torch.distributed.destroy_process_group()
 
 
+def run_profile_case(a):
+    """One workload whose kernels an ncu capture looks at; prints one line."""
+    import torch
+    from mgkmc_b200 import workloads as W
+    n, prec = a.profile_n, a.profile_precision
+    dev = torch.device("cuda", 0)
+    if a.profile_case == "ls3d":
+        from mgkmc_b200.linear_elastic_simulator import Ls3dBatch
+        rng = np.random.default_rng(21)
+        E, nu = W.ls3d_material(n, n, n, rng)
+        ep = W.pure_shear_eigenstrain_3d(n, n, n, rng)
+        t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        eb = np.zeros((3, 3))
+        eb[0, 0], eb[1, 2] = 0.01, 0.002
+        B = Ls3dBatch([(n, n, n)], precision=prec)
+        B.set_material(0, t(E), t(nu), t(ep))
+        o = torch.empty((n, n, n, 3, 3), dtype=torch.float64, device=dev)
+        s = torch.empty_like(o)
+        for _ in range(3):
+            info = B.solve([0], [eb], [o], [s], max_iter=300, tol=1e-8)
+        print(f"ls3d {n}^3 {prec}: {info[0].iterations} iterations", flush=True)
+    elif a.profile_case == "fs3d":
+        from mgkmc_b200.finite_strain_simulator import Fs3dSolver
+        lam, mu, Fp = W.fs3d_material_dev(n, n, n, 2, dev)
+        S = Fs3dSolver(n, n, n, model="neo_hookean", precision=prec)
+        S.set_material(lam, mu, Fp)
+        S.set_F(torch.eye(3, dtype=torch.float64, device=dev).reshape(3, 3, 1, 1, 1).expand(3, 3, n, n, n).contiguous())
+        Fb = np.eye(3)
+        Fb[0, 0] = 1.005
+        Pm = np.zeros((3, 3), bool)
+        Pm[1, 1] = Pm[2, 2] = True
+        _, info = S.step(Fb, (0, 0), np.zeros((3, 3)), Pm, 90e9, 0.35, 1e-8, 1e-6, 50, 1e6, 20)
+        print(f"fs3d {n}^3 {prec}: {info.newton_iterations} Newton, {info.krylov_iterations} Krylov", flush=True)
+    else:
+        from mgkmc_b200 import kmc_simulator_functions as K
+        rng = np.random.default_rng(1)
+        cat, Q0 = W.kmc2d_state(n, n, 8, rng)
+        sig = 1e8 * rng.standard_normal((n, n, 2, 2))
+        Q = np.zeros((n, n, 8))
+        soft, tl, prev = np.zeros((n, n, 2)), np.full((n, n), -np.inf), np.zeros((n, n, 2, 2))
+        for _ in range(3):
+            K.compute_barrier_2d(Q, Q0, sig, cat, 1.0, soft, tl, 0.0, prev, 2.0, 0, np.inf)
+            r, idx, total = K.compute_rates_2d(Q, 1.0, 300.0, 1e13, cascade_mode=False)
+            e = K.select_event_2d_u(r, total, 0.37)
+        print(f"kmc {n}^2 x 8: total rate {total:.6e}, event {e}", flush=True)
+    torch.cuda.synchronize()
+
+
 def main():
     a = parse()
+    if a.profile_case:
+        run_profile_case(a)
+        return
     if a.impl == "reference":
         run_reference(a)
     else:

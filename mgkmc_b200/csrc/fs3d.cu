@@ -935,15 +935,28 @@ __device__ __forceinline__ void fs_zinv_body(const FsArgs& a, unsigned char* sme
   const int ld = a.ld;
   C* lines = reinterpret_cast<C*>(smem);
   const C* spec = FsP<T>::spec(a);
+  constexpr int U = (NZH + 31) / 32;
   for (int cc = 0; cc < 3; ++cc) {
     const int c = 3 * warp + cc;
     C* ln = lines + c * PL;
     const C* ra = spec + c * plane + l0 * ld;
-    for (int k = lane; k < NZH; k += 32) {
-      C av = ra[k], bv = ra[ld + k];
-      if (k == 0 || 2 * k == NZ) { av.y = 0; bv.y = 0; }
-      ln[pidx<C>(k)] = mk<C>(av.x - bv.y, av.y + bv.x);
-      if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = mk<C>(av.x + bv.y, bv.x - av.y);
+    // the component's half-spectrum rows into registers first: one memory
+    // round trip, not one per strided step behind the shared-memory stores
+    C av[U], bv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = lane + 32 * u;
+      if (k < NZH) { av[u] = ra[k]; bv[u] = ra[ld + k]; }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = lane + 32 * u;
+      if (k < NZH) {
+        C x = av[u], y = bv[u];
+        if (k == 0 || 2 * k == NZ) { x.y = 0; y.y = 0; }
+        ln[pidx<C>(k)] = mk<C>(x.x - y.y, x.y + y.x);
+        if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = mk<C>(x.x + y.y, y.x - x.y);
+      }
     }
   }
   __syncwarp();

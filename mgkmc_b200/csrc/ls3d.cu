@@ -98,28 +98,36 @@ __device__ __forceinline__ int fftfreq3(int k, int n) { return (k < (n + 1) / 2)
 
 // eps~^ = -Gamma0(n) : tau^ for symmetric tau (3D), n a unit vector.
 // t[6] / e[6] in the symmetric order above.
-__device__ __forceinline__ void gamma3d_apply(const double2* t, double n0, double n1, double n2, double inv2mu0,
-                                              double Bc, double2* e) {
-  const double n[3] = {n0, n1, n2};
+// R = double for the FP64 iterations, float for the FP32 phase of a mixed plan.
+template <typename R>
+__device__ __forceinline__ void gamma3d_apply_t(const C_t<R>* t, R n0, R n1, R n2, R inv2mu0, R Bc, C_t<R>* e) {
+  constexpr int kI[6] = {0, 1, 2, 1, 0, 0}, kJ[6] = {0, 1, 2, 2, 2, 1};
+  const R n[3] = {n0, n1, n2};
   // full symmetric tau as 3x3 of complex
-  double2 T[3][3];
+  C_t<R> T[3][3];
   T[0][0] = t[0]; T[1][1] = t[1]; T[2][2] = t[2];
   T[1][2] = T[2][1] = t[3];
   T[0][2] = T[2][0] = t[4];
   T[0][1] = T[1][0] = t[5];
-  double2 tn[3];
+  C_t<R> tn[3];
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
     tn[i].x = T[i][0].x * n[0] + T[i][1].x * n[1] + T[i][2].x * n[2];
     tn[i].y = T[i][0].y * n[0] + T[i][1].y * n[1] + T[i][2].y * n[2];
   }
-  double2 ntn;
+  C_t<R> ntn;
   ntn.x = tn[0].x * n[0] + tn[1].x * n[1] + tn[2].x * n[2];
   ntn.y = tn[0].y * n[0] + tn[1].y * n[1] + tn[2].y * n[2];
+#pragma unroll
   for (int c = 0; c < 6; ++c) {
-    const int k = kSymI[c], h = kSymJ[c];
+    const int k = kI[c], h = kJ[c];
     e[c].x = -(inv2mu0 * (n[h] * tn[k].x + n[k] * tn[h].x) - Bc * n[k] * n[h] * ntn.x);
     e[c].y = -(inv2mu0 * (n[h] * tn[k].y + n[k] * tn[h].y) - Bc * n[k] * n[h] * ntn.y);
   }
+}
+__device__ __forceinline__ void gamma3d_apply(const double2* t, double n0, double n1, double n2, double inv2mu0,
+                                              double Bc, double2* e) {
+  gamma3d_apply_t<double>(t, n0, n1, n2, inv2mu0, Bc, e);
 }
 
 // -------------------------------------------------------------- kernels ---
@@ -593,15 +601,28 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
   const C* tw = reinterpret_cast<const C*>(L3F<T>::fz(R).tw);
   C* lw = lines + 2 * warp * PL;
   if (IN_SPEC) {
+    constexpr int U = (NZH + 31) / 32;
     for (int cc = 0; cc < 2; ++cc) {
       const int c = 2 * warp + cc;
       C* ln = lines + c * PL;
       const C* ra = spec + c * plane + l0 * ld;
-      for (int k = lane; k < NZH; k += 32) {
-        C av = ra[k], bv = ra[ld + k];
-        if (k == 0 || 2 * k == NZ) { av.y = 0; bv.y = 0; }
-        ln[pidx<C>(k)] = mk<C>(av.x - bv.y, av.y + bv.x);
-        if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = mk<C>(av.x + bv.y, bv.x - av.y);
+      // the component's half-spectrum rows into registers first: one memory
+      // round trip, not one per strided step behind the shared-memory stores
+      C av[U], bv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = lane + 32 * u;
+        if (k < NZH) { av[u] = ra[k]; bv[u] = ra[ld + k]; }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = lane + 32 * u;
+        if (k < NZH) {
+          C a = av[u], b = bv[u];
+          if (k == 0 || 2 * k == NZ) { a.y = 0; b.y = 0; }
+          ln[pidx<C>(k)] = mk<C>(a.x - b.y, a.y + b.x);
+          if (k > 0 && 2 * k < NZ) ln[pidx<C>(NZ - k)] = mk<C>(a.x + b.y, b.x - a.y);
+        }
       }
     }
     __syncwarp();
@@ -756,35 +777,39 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
   warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0, PL, tw, lane);
   warp_fft<NL, AXIS == 1 ? SIGN : -1, 2>(l0 + 2 * PL, PL, tw, lane);
   if constexpr (AXIS == 0) {
+    // Gamma0 in the precision of the pass: FP64 iterations in double, the
+    // FP32 phase of a mixed plan in float (its errors are those of its FP32
+    // fields; the FP64 phase that follows removes both)
     __syncthreads();
-    const double scale = 1.0 / (double)R.N;
+    const T scale = T(1.0 / (double)R.N);
+    const T inv2mu0 = (T)S.inv2mu0, Bc = (T)S.Bc;
     const int ky = o;
-    const double uy = (double)fftfreq3(ky, ny) / ny;
+    const T uy = (T)fftfreq3(ky, ny) / (T)ny;
     const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
     for (int e = threadIdx.x; e < tcw * NL; e += NC * 32) {
       const int t = e / NL, kx = e - t * NL;
       const int kz = k0 + t;
       const int pk = pidx<C>(kx);
-      double2 tv[6], ev[6];
-      for (int c = 0; c < 6; ++c) {
-        const C v = lines[(c * TC + t) * PL + pk];
-        tv[c] = make_double2((double)v.x, (double)v.y);
-      }
+      C tv[6], ev[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) tv[c] = lines[(c * TC + t) * PL + pk];
       if (kx == 0 && ky == 0 && kz == 0) {
         for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = mk<C>(T(0), T(0));
         continue;
       }
-      const double ux = (double)fftfreq3(kx, nx) / nx, uz = (double)fftfreq3(kz, nz) / nz;
-      const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
-      const double n0 = ux * inv, n1 = uy * inv, n2 = uz * inv;
-      gamma3d_apply(tv, n0, n1, n2, S.inv2mu0, S.Bc, ev);
+      const T ux = (T)fftfreq3(kx, nx) / (T)nx, uz = (T)fftfreq3(kz, nz) / (T)nz;
+      const T inv = T(1) / sqrt(ux * ux + uy * uy + uz * uz);
+      const T n0 = ux * inv, n1 = uy * inv, n2 = uz * inv;
+      gamma3d_apply_t<T>(tv, n0, n1, n2, inv2mu0, Bc, ev);
       const bool nqx = (nx & 1) == 0 && 2 * kx == nx, nqz = (nz & 1) == 0 && 2 * kz == nz;
       if (nqx || nqy || nqz) {
-        double2 fv[6];
-        gamma3d_apply(tv, nqx ? -n0 : n0, nqy ? -n1 : n1, nqz ? -n2 : n2, S.inv2mu0, S.Bc, fv);
-        for (int c = 0; c < 6; ++c) ev[c] = make_double2(0.5 * (ev[c].x + fv[c].x), 0.5 * (ev[c].y + fv[c].y));
+        C fv[6];
+        gamma3d_apply_t<T>(tv, nqx ? -n0 : n0, nqy ? -n1 : n1, nqz ? -n2 : n2, inv2mu0, Bc, fv);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ev[c] = mk<C>(T(0.5) * (ev[c].x + fv[c].x), T(0.5) * (ev[c].y + fv[c].y));
       }
-      for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = mk<C>((T)(ev[c].x * scale), (T)(ev[c].y * scale));
+#pragma unroll
+      for (int c = 0; c < 6; ++c) lines[(c * TC + t) * PL + pk] = mk<C>(ev[c].x * scale, ev[c].y * scale);
     }
     __syncthreads();
     warp_fft<NL, +1, 2>(l0, PL, tw, lane);
