@@ -1001,7 +1001,8 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
     const T inv2mu0 = (T)S.inv2mu0, Bc = (T)S.Bc;
     const T sc = (T)(1.0 / ((double)NX * (double)ny));
     const int ky = ky0 + t;
-    const double uy = (double)fftfreq(ky, ny) / ny;
+    // the wave direction in the pass precision (FP32 phase: float)
+    const T uy = (T)fftfreq(ky, ny) / (T)ny;
     const bool nqy = (ny & 1) == 0 && 2 * ky == ny;
     for (int kx = lane; kx < NX; kx += G) {
       const int pk = pidx<C>(kx);
@@ -1012,9 +1013,9 @@ __device__ __forceinline__ void col_fast_body(const Ls2dRep& R, const Ls2dState&
         *pxx = mk<C>(T(0), T(0)); *pyy = *pxx; *pxy = *pxx;
         continue;
       }
-      const double ux = (double)fftfreq(kx, NX) / NX;
-      const double inv = 1.0 / sqrt(ux * ux + uy * uy);
-      const T nxv = (T)(ux * inv), nyv = (T)(uy * inv);
+      const T ux = (T)fftfreq(kx, NX) / (T)NX;
+      const T inv = T(1) / sqrt(ux * ux + uy * uy);
+      const T nxv = ux * inv, nyv = uy * inv;
       const C txx = *pxx, tyy = *pyy, txy = *pxy;
       C exx, eyy, exy;
       gamma2d_apply(txx, tyy, txy, nxv, nyv, inv2mu0, Bc, exx, eyy, exy);
