@@ -7,14 +7,15 @@
 // contraction, mirroring the LLVM code numba emits), and the total rate is
 // the sequential left-to-right FP64 running sum in (x, y[, z], m) order.
 //
-// The sequential sum is a dependent chain by definition.  It runs in one
-// CTA: warp 0 lane 0 walks a shared-memory chunk while the other warps load
-// the next chunk and write back the previous one (3 rotating buffers), so
-// the chain sees shared-memory latency only.  The prefix array it writes is
-// monotone (rates >= 0), so selection is a two-level parallel search for the
-// first prefix >= u * total instead of the reference's linear rescan; both
-// return the same index for the same rates and draw.
+// The sequential sum is a dependent chain by definition; it is reproduced
+// bit for bit by exact integer arithmetic inside binades (see the exact
+// running sum below), in parallel over chunks.  The prefix array it writes
+// is monotone (rates >= 0), so selection is a two-level parallel search for
+// the first prefix >= u * total instead of the reference's linear rescan;
+// both return the same index for the same rates and draw.
 #include <math.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 
@@ -171,7 +172,7 @@ __global__ void rates_scatter_kernel(long long nvox, int M, const double* __rest
   indices[pos] = i;
 }
 
-// Exact sequential running sum, computed in parallel (one CTA).
+// Exact sequential running sum, computed in parallel.
 //
 // The reference accumulates total_rate left to right in FP64
 // (kmc_simulator_functions.py:36-55), so every running sum carries the
@@ -179,53 +180,73 @@ __global__ void rates_scatter_kernel(long long nvox, int M, const double* __rest
 // only grows.  While s stays inside one binade [2^e, 2^(e+1)), every double
 // there is a multiple of u = 2^(e-52), and round-to-nearest of s + r is
 // s + rint(r/u)*u unless r/u sits exactly halfway between integers (a tie,
-// whose rounding depends on the parity of s).  So over a chunk of rates the
+// whose rounding depends on the parity of s).  So over a run of rates the
 // chain collapses to an exact int64 prefix sum of q_i = rint(r_i/u) added to
 // the mantissa integer M = s/u, valid up to the first element whose candidate
 // leaves the binade (M + Q >= 2^53) or is a tie; that element is added the
-// ordinary way (one __dadd_rn), which moves s to its new binade, and the next
-// chunk starts after it.  A zero, subnormal or non-finite s also takes single
-// ordinary adds.  The results are bit-identical to the sequential loop; the
-// number of ordinary adds is about the number of binades the sum crosses.
+// ordinary way (one __dadd_rn), which moves s to its new binade.  A zero,
+// subnormal or non-finite s also takes single ordinary adds.  The results
+// are bit-identical to the sequential loop.
+//
+// The array is cut into chunks of kExactChunk rates, processed in five
+// launches:
+//   1. chunk sums in FP64, any order (an estimate of the running sum);
+//   2. one CTA scans them: the estimated running sum at each chunk start;
+//   3. per chunk, with the binade e of that estimate: the exact int64 sum Q
+//      of q_i, and whether every element is representable and tie-free;
+//   4. one CTA walks the chunks in order with the exact running sum s: a
+//      chunk whose record holds (s in binade e, M + Q < 2^53) ends at
+//      (M + Q) u exactly and costs a few instructions; any other chunk (the
+//      first, the last short one, a binade crossing, a tie, a wrong estimate)
+//      runs the sequential-exact CTA algorithm above on its own rates;
+//   5. per chunk that the walk accepted: prefix_i = (M + Q_i) u from a block
+//      scan of its q_i.
+// A chunk's records sit in its own first four prefix entries until the walk
+// (rejected chunks) or launch 5 (accepted ones) writes its final values; the
+// walk marks accepted chunks with -0.0 in entry 3, a value no running sum
+// from +0.0 can take.  The walk's cost is about the number of binades the
+// sum crosses, times one chunk.
 constexpr int kExactThreads = 1024;
 constexpr int kExactPer = 8;  // rates per thread per chunk
+constexpr int kExactChunk = kExactThreads * kExactPer;
 // q_i < 2^53, so sums of q are saturated at 2^61 (no int64 overflow); any
 // saturated sum is far above 2^53 - M and reads as leaving the binade
 constexpr long long kQCap = 1LL << 61;
 __device__ __forceinline__ long long qsat(long long a, long long b) { return min(a + b, kQCap); }
+constexpr long long kRecOk = 1LL << 62;                      // record tag: chunk tie-free, q representable
+constexpr long long kRecMark = (long long)0x8000000000000000ULL;  // bits of -0.0: accepted by the walk
 
-__global__ void __launch_bounds__(kExactThreads) exact_prefix_kernel(const double* __restrict__ rates,
-                                                                    long long n_fixed,
-                                                                    const long long* __restrict__ d_count,
-                                                                    double* __restrict__ prefix,
-                                                                    double* __restrict__ d_total) {
-  constexpr int CH = kExactThreads * kExactPer;
-  __shared__ long long w_sum[32];
-  __shared__ long long w_fail[32];
-  __shared__ double s_s;
-  __shared__ long long s_p;
-  const long long n = d_count ? *d_count : n_fixed;
+__device__ __forceinline__ bool normal_finite(double s) { return s >= 2.2250738585072014e-308 && s < 1.0 / 0.0; }
+__device__ __forceinline__ int binade_of(double s) { return (int)((__double_as_longlong(s) >> 52) & 0x7ff) - 1023; }
+
+// The sequential-exact algorithm on rates[p0, end) from running sum s0, by
+// all kExactThreads threads of the CTA; writes prefix[p0, end) and returns
+// the running sum after element end - 1 (in every thread).
+__device__ double exact_range(const double* __restrict__ rates, long long p0, long long end, double s0,
+                              double* __restrict__ prefix, long long* w_sum, long long* w_fail, double* s_s,
+                              long long* s_p) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) { s_s = 0.0; s_p = 0; }
+  __syncthreads();
+  if (tid == 0) { *s_s = s0; *s_p = p0; }
   __syncthreads();
   while (true) {
-    const double s = s_s;
-    const long long p = s_p;
-    if (p >= n) break;
-    if (!(s >= 2.2250738585072014e-308) || !(s < 1.0 / 0.0)) {
+    const double s = *s_s;
+    const long long p = *s_p;
+    if (p >= end) break;
+    if (!normal_finite(s)) {
       // zero, subnormal or non-finite running sum: one ordinary add
       __syncthreads();
       if (tid == 0) {
         const double v = add(s, rates[p]);
         prefix[p] = v;
-        s_s = v;
-        s_p = p + 1;
+        *s_s = v;
+        *s_p = p + 1;
       }
       __syncthreads();
       continue;
     }
     const long long bits = __double_as_longlong(s);
-    const int e = (int)((bits >> 52) & 0x7ff) - 1023;
+    const int e = binade_of(s);
     const long long M = (bits & ((1LL << 52) - 1)) | (1LL << 52);
     const double scale = ldexp(1.0, 52 - e);  // 1/u, exact power of two
     const double u = ldexp(1.0, e - 52);
@@ -237,7 +258,7 @@ __global__ void __launch_bounds__(kExactThreads) exact_prefix_kernel(const doubl
     for (int k = 0; k < kExactPer; ++k) {
       const long long i = base + k;
       q[k] = 0;
-      if (i < n) {
+      if (i < end) {
         const double x = rates[i] * scale;
         if (!(x >= 0.0) || !(x < 9007199254740992.0) || x - floor(x) == 0.5) {
           if (fail == LLONG_MAX) fail = i;
@@ -282,13 +303,13 @@ __global__ void __launch_bounds__(kExactThreads) exact_prefix_kernel(const doubl
 #pragma unroll
     for (int k = 0; k < kExactPer; ++k) {
       const long long i = base + k;
-      if (i < n && i < first_bad) {
+      if (i < end && i < first_bad) {
         Q = qsat(Q, q[k]);
         if (M + Q >= (1LL << 53)) { cross = i; break; }
         prefix[i] = (double)(M + Q) * u;
       }
     }
-    // the chunk is valid up to min(first tie, first crossing)
+    // the step is valid up to min(first tie, first crossing)
     long long wc = cross;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) wc = min(wc, __shfl_xor_sync(0xffffffffu, wc, o));
@@ -298,23 +319,285 @@ __global__ void __launch_bounds__(kExactThreads) exact_prefix_kernel(const doubl
     if (tid == 0) {
       long long stop = first_bad;
       for (int w = 0; w < kExactThreads / 32; ++w) stop = min(stop, w_sum[w]);
-      const long long end = min(p + (long long)CH, n);
-      if (stop >= end) {
-        // whole chunk valid: the running sum is its last prefix
-        s_s = prefix[end - 1];
-        s_p = end;
+      const long long stp_end = min(p + (long long)kExactChunk, end);
+      if (stop >= stp_end) {
+        // whole step valid: the running sum is its last prefix
+        *s_s = prefix[stp_end - 1];
+        *s_p = stp_end;
       } else {
         // elements [p, stop) were written; stop is added the ordinary way
         const double prev = stop > p ? prefix[stop - 1] : s;
         const double v = add(prev, rates[stop]);
         prefix[stop] = v;
-        s_s = v;
-        s_p = stop + 1;
+        *s_s = v;
+        *s_p = stop + 1;
       }
     }
     __syncthreads();
   }
-  if (tid == 0) *d_total = n > 0 ? s_s : 0.0;
+  return *s_s;
+}
+
+__device__ __forceinline__ long long exact_count(long long n_fixed, const long long* d_count) {
+  return d_count ? *d_count : n_fixed;
+}
+// chunks that carry records: not the first, at least 4 rates long
+__device__ __forceinline__ bool has_record(long long c0, long long n) { return c0 > 0 && n - c0 >= 4; }
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x + 31) / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  return t;  // valid in thread 0
+}
+
+// 1. FP64 sum of each chunk (an estimate) into the chunk's entry 0; grid = chunks
+__global__ void __launch_bounds__(256) exact_chunk_sum_kernel(const double* __restrict__ rates, long long n_fixed,
+                                                              const long long* __restrict__ d_count,
+                                                              double* __restrict__ prefix) {
+  __shared__ double red[32];
+  const long long n = exact_count(n_fixed, d_count);
+  const long long c0 = (long long)blockIdx.x * kExactChunk;
+  if (c0 >= n || n - c0 < 4) return;  // the last short chunk needs no estimate
+  const long long c1 = min(c0 + (long long)kExactChunk, n);
+  double v = 0;
+  for (long long i = c0 + threadIdx.x; i < c1; i += blockDim.x) v += rates[i];
+  v = block_sum_d(v, red);
+  if (threadIdx.x == 0) prefix[c0] = v;
+}
+
+// 2. one CTA: estimated running sum at each chunk start into entry 1
+__global__ void __launch_bounds__(1024) exact_chunk_scan_kernel(long long n_fixed, const long long* __restrict__ d_count,
+                                                                double* __restrict__ prefix) {
+  __shared__ double wtot[32];
+  __shared__ double carry;
+  const long long n = exact_count(n_fixed, d_count);
+  const long long K = (n + kExactChunk - 1) / kExactChunk;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0.0;
+  __syncthreads();
+  for (long long kb = 0; kb < K; kb += 1024) {
+    const long long k = kb + threadIdx.x;
+    const long long c0 = k * kExactChunk;
+    const double v = (k < K && n - c0 >= 4) ? prefix[c0] : 0.0;
+    double incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const double t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wtot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      double w = wtot[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      wtot[lane] = w;
+    }
+    __syncthreads();
+    const double excl = carry + (wid > 0 ? wtot[wid - 1] : 0.0) + (incl - v);
+    if (k < K && has_record(c0, n)) prefix[c0 + 1] = excl;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += wtot[31];
+    __syncthreads();
+  }
+}
+
+// q_i = rint(r_i * scale) of rate i, or -1 when it is a tie or not
+// representable (then the chunk is left to the sequential algorithm)
+__device__ __forceinline__ long long exact_q(double r, double scale) {
+  const double x = r * scale;
+  if (!(x >= 0.0) || !(x < 9007199254740992.0) || x - floor(x) == 0.5) return -1;
+  return (long long)rint(x);
+}
+
+// 3. per chunk with a record: Q = sum of q_i at the binade of its estimated
+// start (entry 2), and the tag with that binade (entry 3); grid = chunks
+__global__ void __launch_bounds__(kExactThreads) exact_chunk_q_kernel(const double* __restrict__ rates,
+                                                                      long long n_fixed,
+                                                                      const long long* __restrict__ d_count,
+                                                                      double* __restrict__ prefix) {
+  __shared__ long long w_q[32];
+  __shared__ int w_bad[32];
+  __shared__ double s_est;
+  const long long n = exact_count(n_fixed, d_count);
+  const long long c0 = (long long)blockIdx.x * kExactChunk;
+  if (c0 >= n || !has_record(c0, n)) return;
+  const long long c1 = min(c0 + (long long)kExactChunk, n);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) s_est = prefix[c0 + 1];
+  __syncthreads();
+  const double est = s_est;
+  const bool est_ok = normal_finite(est);
+  const int e = est_ok ? binade_of(est) : 0;
+  const double scale = ldexp(1.0, 52 - e);
+  long long tot = 0;
+  int bad = est_ok ? 0 : 1;
+  const long long base = c0 + (long long)tid * kExactPer;
+#pragma unroll
+  for (int k = 0; k < kExactPer; ++k) {
+    const long long i = base + k;
+    if (i < c1 && !bad) {
+      const long long q = exact_q(rates[i], scale);
+      if (q < 0) bad = 1;
+      else tot = qsat(tot, q);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    tot = qsat(tot, __shfl_xor_sync(0xffffffffu, tot, o));
+    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if (lane == 0) { w_q[wid] = tot; w_bad[wid] = bad; }
+  __syncthreads();  // every thread has read entry 1 (s_est) before entry 2/3 change
+  if (tid == 0) {
+    long long Q = 0;
+    int b = 0;
+    for (int w = 0; w < kExactThreads / 32; ++w) { Q = qsat(Q, w_q[w]); b |= w_bad[w]; }
+    prefix[c0 + 2] = __longlong_as_double(Q);
+    prefix[c0 + 3] = __longlong_as_double(b ? 0LL : (kRecOk | (long long)(e + 2048)));
+  }
+}
+
+// 4. one CTA walks the chunks in order with the exact running sum; writes the
+// total.  Accepted chunks get (M, e, mark) in entries 0, 1, 3.
+__global__ void __launch_bounds__(kExactThreads) exact_walk_kernel(const double* __restrict__ rates, long long n_fixed,
+                                                                   const long long* __restrict__ d_count,
+                                                                   double* __restrict__ prefix,
+                                                                   double* __restrict__ d_total) {
+  __shared__ long long w_sum[32];
+  __shared__ long long w_fail[32];
+  __shared__ double s_s;
+  __shared__ long long s_p;
+  __shared__ long long rec_q[kExactThreads];
+  __shared__ long long rec_t[kExactThreads];
+  __shared__ double w_s;
+  __shared__ long long w_k;
+  const long long n = exact_count(n_fixed, d_count);
+  const long long K = (n + kExactChunk - 1) / kExactChunk;
+  double s = 0.0;
+  for (long long kb = 0; kb < K; kb += kExactThreads) {
+    const long long kend = min(kb + (long long)kExactThreads, K);
+    {
+      const long long k = kb + threadIdx.x;
+      const long long c0 = k * kExactChunk;
+      const bool rec = k < kend && has_record(c0, n);
+      rec_q[threadIdx.x] = rec ? __double_as_longlong(prefix[c0 + 2]) : 0;
+      rec_t[threadIdx.x] = rec ? __double_as_longlong(prefix[c0 + 3]) : 0;
+    }
+    __syncthreads();
+    long long k = kb;
+    while (k < kend) {
+      if (threadIdx.x == 0) {
+        // accept chunks while their records hold at the exact running sum
+        while (k < kend) {
+          const long long c0 = k * kExactChunk;
+          const long long t = rec_t[k - kb];
+          if (!has_record(c0, n) || !(t & kRecOk) || !normal_finite(s)) break;
+          const int e = (int)(t & 0xffff) - 2048;
+          if (binade_of(s) != e) break;
+          const long long M = (__double_as_longlong(s) & ((1LL << 52) - 1)) | (1LL << 52);
+          const long long Q = rec_q[k - kb];
+          if (M + Q >= (1LL << 53)) break;
+          prefix[c0] = __longlong_as_double(M);
+          prefix[c0 + 1] = __longlong_as_double((long long)e);
+          prefix[c0 + 3] = __longlong_as_double(kRecMark);
+          s = (double)(M + Q) * ldexp(1.0, e - 52);
+          ++k;
+        }
+        w_s = s;
+        w_k = k;
+      }
+      __syncthreads();
+      s = w_s;
+      k = w_k;
+      if (k < kend) {
+        // chunk k by the sequential-exact algorithm
+        const long long c0 = k * kExactChunk;
+        s = exact_range(rates, c0, min(c0 + (long long)kExactChunk, n), s, prefix, w_sum, w_fail, &s_s, &s_p);
+        ++k;
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) *d_total = n > 0 ? s : 0.0;
+}
+
+// 5. per accepted chunk: prefix_i = (M + Q_i) u, Q_i the inclusive sum of q
+// up to i; grid = chunks
+__global__ void __launch_bounds__(kExactThreads) exact_write_kernel(const double* __restrict__ rates, long long n_fixed,
+                                                                    const long long* __restrict__ d_count,
+                                                                    double* __restrict__ prefix) {
+  __shared__ long long w_sum[32];
+  __shared__ long long s_rec[3];
+  const long long n = exact_count(n_fixed, d_count);
+  const long long c0 = (long long)blockIdx.x * kExactChunk;
+  if (c0 >= n || !has_record(c0, n)) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid < 3) s_rec[tid] = __double_as_longlong(prefix[c0 + (tid == 2 ? 3 : tid)]);
+  __syncthreads();
+  if (s_rec[2] != kRecMark) return;  // the walk wrote this chunk
+  const long long M = s_rec[0];
+  const int e = (int)s_rec[1];
+  const long long c1 = min(c0 + (long long)kExactChunk, n);
+  const double scale = ldexp(1.0, 52 - e), u = ldexp(1.0, e - 52);
+  const long long base = c0 + (long long)tid * kExactPer;
+  long long q[kExactPer];
+  long long tot = 0;
+#pragma unroll
+  for (int k = 0; k < kExactPer; ++k) {
+    const long long i = base + k;
+    q[k] = i < c1 ? exact_q(rates[i], scale) : 0;  // >= 0: the chunk's record said so
+    tot += q[k];
+  }
+  long long incl = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) w_sum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    long long v = w_sum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    w_sum[lane] = v;
+  }
+  __syncthreads();
+  long long Q = (wid > 0 ? w_sum[wid - 1] : 0) + (incl - tot);
+#pragma unroll
+  for (int k = 0; k < kExactPer; ++k) {
+    const long long i = base + k;
+    if (i < c1) {
+      Q += q[k];
+      prefix[i] = (double)(M + Q) * u;
+    }
+  }
+}
+
+// the five launches for up to n_max rates (the count is *d_count when given)
+static int launch_exact_prefix(const double* rates, long long n_max, const long long* d_count, double* prefix,
+                               double* d_total, cudaStream_t s) {
+  const long long nfix = d_count ? 0 : n_max;
+  const unsigned int K = (unsigned int)std::max(1LL, (n_max + kExactChunk - 1) / kExactChunk);
+  exact_chunk_sum_kernel<<<K, 256, 0, s>>>(rates, nfix, d_count, prefix);
+  exact_chunk_scan_kernel<<<1, 1024, 0, s>>>(nfix, d_count, prefix);
+  exact_chunk_q_kernel<<<K, kExactThreads, 0, s>>>(rates, nfix, d_count, prefix);
+  exact_walk_kernel<<<1, kExactThreads, 0, s>>>(rates, nfix, d_count, prefix, d_total);
+  exact_write_kernel<<<K, kExactThreads, 0, s>>>(rates, nfix, d_count, prefix);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
 }
 
 // First i with prefix[i] >= u*total (two-level parallel search, one CTA).
@@ -541,8 +824,8 @@ static int kmc_rates_impl(long long nvox, int M, const double* Q, double volume,
     rates_full_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nvox, M, Q, vnu, T, Ts, rates, (long long*)indices,
                                                          (long long*)d_count);
     MGK_CUDA(cudaGetLastError());
-    exact_prefix_kernel<<<1, kExactThreads, 0, s>>>(rates, n, nullptr, prefix, d_total);
-    MGK_CUDA(cudaGetLastError());
+    int rc = launch_exact_prefix(rates, n, nullptr, prefix, d_total, s);
+    if (rc) return rc;
   } else {
     MGK_REQUIRE(work != nullptr, "mgk_kmc2d_rates: cascade mode needs the work buffer");
     const int nb = blocks_for(n, 256);
@@ -553,8 +836,8 @@ static int kmc_rates_impl(long long nvox, int M, const double* Q, double volume,
     MGK_CUDA(cudaGetLastError());
     rates_scatter_kernel<<<nb, 256, 0, s>>>(nvox, M, Q, vnu, T, Ts, bcount, rates, (long long*)indices);
     MGK_CUDA(cudaGetLastError());
-    exact_prefix_kernel<<<1, kExactThreads, 0, s>>>(rates, 0, (const long long*)d_count, prefix, d_total);
-    MGK_CUDA(cudaGetLastError());
+    int rc = launch_exact_prefix(rates, n, (const long long*)d_count, prefix, d_total, s);
+    if (rc) return rc;
   }
   return MGK_OK;
 }
@@ -577,9 +860,7 @@ extern "C" int mgk_kmc_prefix(const double* rates, int64_t n, double* prefix, in
   cudaStream_t s = (cudaStream_t)stream;
   set_count_kernel<<<1, 1, 0, s>>>((long long*)d_count, (long long)n);
   MGK_CUDA(cudaGetLastError());
-  exact_prefix_kernel<<<1, kExactThreads, 0, s>>>(rates, n, nullptr, prefix, d_total);
-  MGK_CUDA(cudaGetLastError());
-  return MGK_OK;
+  return launch_exact_prefix(rates, n, nullptr, prefix, d_total, s);
 }
 
 extern "C" int mgk_kmc_select(const double* prefix, const int64_t* d_count, const double* d_total, double u,

@@ -136,8 +136,15 @@ def _prefix_gpu(rates):
     return prefix.cpu().numpy()[:n], float(tot.item())
 
 
+def _tie_at(r, j, k=3):
+    # make r[j] land exactly halfway between two doubles of the running sum
+    # before it (a tie: its rounding depends on the parity of that sum)
+    s = np.cumsum(r[:j])[-1]
+    r[j] = (k + 0.5) * np.spacing(s)
+
+
 @pytest.mark.parametrize("case", ["kmc", "wild", "zeros_subnormal_huge", "ties", "all_ties", "empty", "one",
-                                  "large"])
+                                  "large", "late_ties", "jump", "n8192", "n8193", "n8195", "n8196", "n16387"])
 def test_exact_prefix_bit_for_bit(case):
     # the parallel exact running sum against the sequential loop (np.cumsum
     # adds left to right): every partial sum and the total, bit for bit
@@ -162,6 +169,16 @@ def test_exact_prefix_bit_for_bit(case):
         r = np.zeros(0)
     elif case == "one":
         r = np.array([0.37])
+    elif case == "late_ties":  # ties deep inside later chunks of an otherwise regular array
+        r = 1e13 * np.exp(-rng.normal(1.0, 0.15, 200_000) / 0.02585)
+        for j in (9_000, 100_000, 150_007, 199_999):
+            _tie_at(r, j)
+    elif case == "jump":  # a rate that moves the sum up many binades in the middle of a chunk
+        r = rng.random(100_000)
+        r[50_000] = 1e6
+        r[70_003] = 1e12
+    elif case.startswith("n"):  # chunk boundaries: last chunk of 0, 1, 3, 4 and 3 rates
+        r = 1e13 * np.exp(-rng.normal(1.0, 0.15, int(case[1:])) / 0.02585)
     else:
         r = 1e13 * np.exp(-rng.normal(1.0, 0.15, 8_388_608) / 0.02585)  # 1024^2 x 8 modes
     p, tot = _prefix_gpu(r)
