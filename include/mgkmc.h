@@ -295,6 +295,23 @@ MGK_API int mgk_kmc_prefix(const double* rates, int64_t n, double* prefix, int64
 MGK_API int mgk_kmc_select(const double* prefix, const int64_t* d_count, const double* d_total, double u,
                    int64_t* d_index, mgk_stream_t stream);
 
+/* Fast selection mode, the rate step of a KMC/AQS step in one pass:
+ * mgk_kmc2d_barrier (Q written as there; volume is the barrier's), then each
+ * mode's KMC-mode rate from its new barrier (same per-mode arithmetic as
+ * mgk_kmc2d_rates, rate_volume * nu0 as its prefactor) and the FP64 sum of
+ * all rates into *d_total, summed per CTA in a fixed order (it can differ
+ * from the reference's sequential total in the last bits).  No rate array is
+ * written: a caller computes rates and running sums only when an event is
+ * drawn.  No counterpart in the reference (its compute_barrier_2d and
+ * compute_rates_2d are two passes).  work: mgk_kmc_scan_work_bytes(nx*ny*M). */
+MGK_API int mgk_kmc2d_barrier_total(int nx, int ny, int M, double* Q, const double* Q0, const double* sig,
+                                    const double* catalog, double volume, const double* soft_prop,
+                                    const double* last_event_time, double current_time,
+                                    const double* prev_strain_dir, double softening_cap, int scheme,
+                                    double tau, double rate_volume, const double* temperature,
+                                    double temperature_scalar, double nu0, double* d_total, void* work,
+                                    mgk_stream_t stream);
+
 /* KMC-mode rates only (every mode an event; no running sum), for the fast
  * selection mode below.  Same per-mode arithmetic as mgk_kmc2d_rates. */
 MGK_API int mgk_kmc2d_rates_only(int nx, int ny, int M, const double* Q, double volume,

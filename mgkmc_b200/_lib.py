@@ -89,6 +89,8 @@ _SIGS = {
     "mgk_fs3d_get": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_kmc2d_barrier": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
                                   c_double, c_int, c_double, _P]),
+    "mgk_kmc2d_barrier_total": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
+                                        c_double, c_int, c_double, c_double, _P, c_double, c_double, _P, _P, _P]),
     "mgk_kmc_rates_work_bytes": (c_int64, [c_int64]),
     "mgk_kmc2d_rates": (c_int, [c_int, c_int, c_int, _P, c_double, _P, c_double, c_double, c_int, _P, _P, _P,
                                 _P, _P, _P, _P]),

@@ -49,12 +49,12 @@ __device__ __forceinline__ double soft_base(double g_p, double g_t, double t_las
 // One thread per (voxel, mode).  D = 2 or 3 (tensor dimension); SP = soft_prop
 // stride (2 in 2D, 4 in 3D).
 template <int D, int SP>
-__global__ void barrier_kernel(long long nvox, int M, double* __restrict__ Q, const double* __restrict__ Q0,
-                               const double* __restrict__ sig, const double* __restrict__ cat, double volume,
-                               const double* __restrict__ soft, const double* __restrict__ t_last, double t,
-                               const double* __restrict__ prev, double cap, int scheme, double tau) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= nvox * M) return;
+__device__ __forceinline__ double barrier_mode(long long i, int M, double* __restrict__ Q,
+                                               const double* __restrict__ Q0, const double* __restrict__ sig,
+                                               const double* __restrict__ cat, double volume,
+                                               const double* __restrict__ soft, const double* __restrict__ t_last,
+                                               double t, const double* __restrict__ prev, double cap, int scheme,
+                                               double tau) {
   const long long v = i / M;
   const double g_base = soft_base(soft[SP * v], soft[SP * v + 1], t_last[v], t, cap, tau);
   const double* c = cat + i * D * D;
@@ -83,7 +83,19 @@ __global__ void barrier_kernel(long long nvox, int M, double* __restrict__ Q, co
 #pragma unroll
   for (int q = 0; q < D * D; ++q) w = add(w, mul(s[q], c[q]));
   const double w_val = mul(mul(mul(0.5, volume), __ddiv_rn(w, 1e9)), GPA_NM3_TO_EV);
-  Q[i] = sub(mul(Q0[i], exp(-g_eff)), w_val);
+  const double q = sub(mul(Q0[i], exp(-g_eff)), w_val);
+  Q[i] = q;
+  return q;
+}
+
+template <int D, int SP>
+__global__ void barrier_kernel(long long nvox, int M, double* __restrict__ Q, const double* __restrict__ Q0,
+                               const double* __restrict__ sig, const double* __restrict__ cat, double volume,
+                               const double* __restrict__ soft, const double* __restrict__ t_last, double t,
+                               const double* __restrict__ prev, double cap, int scheme, double tau) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nvox * M) return;
+  barrier_mode<D, SP>(i, M, Q, Q0, sig, cat, volume, soft, t_last, t, prev, cap, scheme, tau);
 }
 
 // rate of one mode (kmc_simulator_functions.py:41-48)
@@ -92,6 +104,42 @@ __device__ __forceinline__ double mode_rate(double q, double beta, double vnu) {
 }
 
 __device__ __forceinline__ double beta_of(double T) { return T > 0.0 ? __ddiv_rn(1.0, mul(KB_EV, T)) : INFINITY; }
+
+// Fused barrier, rate and block-sum pass (fast selection mode): the barriers
+// as barrier_kernel, each mode's KMC-mode rate from its new barrier, and the
+// FP64 sum of the rates per CTA (grid-stride, fixed grid: a deterministic
+// order); no rate array is written.
+template <int D, int SP>
+__global__ void __launch_bounds__(256) barrier_total_kernel(long long nvox, int M, double* __restrict__ Q,
+                                                            const double* __restrict__ Q0,
+                                                            const double* __restrict__ sig,
+                                                            const double* __restrict__ cat, double volume,
+                                                            const double* __restrict__ soft,
+                                                            const double* __restrict__ t_last, double t,
+                                                            const double* __restrict__ prev, double cap, int scheme,
+                                                            double tau, const double* __restrict__ T, double Ts,
+                                                            double vnu, double* __restrict__ partials) {
+  __shared__ double red[32];
+  const double beta_s = beta_of(Ts);
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvox * M;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double q = barrier_mode<D, SP>(i, M, Q, Q0, sig, cat, volume, soft, t_last, t, prev, cap, scheme, tau);
+    acc += mode_rate(q, T ? beta_of(T[i / M]) : beta_s, vnu);
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// sum of nb partials in a fixed order (one CTA)
+__global__ void __launch_bounds__(256) partials_total_kernel(const double* __restrict__ partials, int nb,
+                                                             double* __restrict__ d_total) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += partials[k];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) *d_total = acc;
+}
 
 // Non-compacting rates (KMC mode: every mode is an event).
 __global__ void rates_full_kernel(long long nvox, int M, const double* __restrict__ Q, double vnu,
@@ -807,6 +855,30 @@ extern "C" int mgk_kmc2d_barrier(int nx, int ny, int M, double* Q, const double*
   barrier_kernel<2, 2><<<blocks_for(nvox * M, 256), 256, 0, (cudaStream_t)stream>>>(
       nvox, M, Q, Q0, sig, catalog, volume, soft_prop, last_event_time, current_time, prev_strain_dir,
       softening_cap, scheme, tau);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_barrier_total(int nx, int ny, int M, double* Q, const double* Q0, const double* sig,
+                                       const double* catalog, double volume, const double* soft_prop,
+                                       const double* last_event_time, double current_time,
+                                       const double* prev_strain_dir, double softening_cap, int scheme, double tau,
+                                       double rate_volume, const double* temperature, double temperature_scalar,
+                                       double nu0, double* d_total, void* work, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && M > 0, "mgk_kmc2d_barrier_total: bad shape");
+  MGK_REQUIRE(Q && Q0 && sig && catalog && soft_prop && last_event_time && d_total && work,
+              "mgk_kmc2d_barrier_total: null argument");
+  MGK_REQUIRE(scheme == 0 || (scheme == 1 && prev_strain_dir), "mgk_kmc2d_barrier_total: bad scheme");
+  const long long nvox = (long long)nx * ny, n = nvox * M;
+  // partials fit the scan work buffer: at most n / 1024 + 1 CTAs
+  const int nb = (int)std::max(1LL, std::min(1184LL, n / 1024));
+  const double vnu = rate_volume * nu0;  // host product, as in mgk_kmc2d_rates
+  cudaStream_t s = (cudaStream_t)stream;
+  double* partials = reinterpret_cast<double*>(work);
+  barrier_total_kernel<2, 2><<<nb, 256, 0, s>>>(nvox, M, Q, Q0, sig, catalog, volume, soft_prop, last_event_time,
+                                                current_time, prev_strain_dir, softening_cap, scheme, tau,
+                                                temperature, temperature_scalar, vnu, partials);
+  partials_total_kernel<<<1, 256, 0, s>>>(partials, nb, d_total);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

@@ -86,6 +86,7 @@ class Kmc2D:
         self.count = torch.zeros(1, dtype=torch.int64, device=d)
         self.total = torch.zeros(1, dtype=f64, device=d)
         self.total_h = torch.zeros(1, dtype=f64).pin_memory()
+        self.total_fast = torch.zeros(1, dtype=f64, device=d)  # fast mode: total of the fused rate pass
         self.sel = torch.zeros(1, dtype=torch.int64, device=d)
         self.xym = torch.zeros(3, dtype=torch.int64, device=d)
         self.xym_h = torch.zeros(3, dtype=torch.int64).pin_memory()
@@ -139,23 +140,26 @@ class Kmc2D:
         return self.after_solve(info)
 
     def launch_rates(self):
-        """Enqueues barriers, rates and the copy of the total rate to the host."""
+        """Enqueues barriers, rates and the copy of the total rate to the host.
+        Exact selection: barriers, then rates with the reference's sequential
+        running sum.  Fast selection: one fused pass for barriers and the total
+        (rates and running sums are built in ``event`` when a draw needs them)."""
         lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
-        L.check(lib.mgk_kmc2d_barrier(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0), L.ptr(self.sig),
-                                      L.ptr(self.catalog), p["volume"], L.ptr(self.soft), L.ptr(self.t_last),
-                                      self.time, L.ptr(self.prev), p["cap"], 0, self.tau, S), "mgk_kmc2d_barrier")
         if self.selection == "exact":
+            L.check(lib.mgk_kmc2d_barrier(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0), L.ptr(self.sig),
+                                          L.ptr(self.catalog), p["volume"], L.ptr(self.soft), L.ptr(self.t_last),
+                                          self.time, L.ptr(self.prev), p["cap"], 0, self.tau, S), "mgk_kmc2d_barrier")
             L.check(lib.mgk_kmc2d_rates(self.nx, self.ny, self.M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"], 0,
                                         L.ptr(self.rates), L.ptr(self.indices), L.ptr(self.prefix), L.ptr(self.count),
                                         L.ptr(self.total), L.ptr(self.work), S), "mgk_kmc2d_rates")
+            self.total_h.copy_(self.total, non_blocking=True)
         else:
-            # rates without the sequential chain, then the parallel scan
-            L.check(lib.mgk_kmc2d_rates_only(self.nx, self.ny, self.M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"],
-                                             L.ptr(self.rates), S), "mgk_kmc2d_rates_only")
-            n = self.nx * self.ny * self.M
-            L.check(lib.mgk_kmc_prefix_fast(L.ptr(self.rates), n, L.ptr(self.prefix), L.ptr(self.count),
-                                            L.ptr(self.total), L.ptr(self.work), S), "mgk_kmc_prefix_fast")
-        self.total_h.copy_(self.total, non_blocking=True)
+            L.check(lib.mgk_kmc2d_barrier_total(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0),
+                                                L.ptr(self.sig), L.ptr(self.catalog), p["volume"], L.ptr(self.soft),
+                                                L.ptr(self.t_last), self.time, L.ptr(self.prev), p["cap"], 0,
+                                                self.tau, 1.0, None, p["T"], p["nu0"], L.ptr(self.total_fast),
+                                                L.ptr(self.work), S), "mgk_kmc2d_barrier_total")
+            self.total_h.copy_(self.total_fast, non_blocking=True)
 
     def barriers_and_rates(self):
         """Barriers, rates and the total rate (one synchronisation)."""
@@ -169,7 +173,17 @@ class Kmc2D:
         self.redraw_h[:4 * M] = self.torch.from_numpy(pure_shear_modes(theta, p["gamma0"]).reshape(-1))
         self.redraw_h[4 * M:] = self.torch.from_numpy(q0)
         self.redraw.copy_(self.redraw_h, non_blocking=True)
-        L.check(lib.mgk_kmc_select(L.ptr(self.prefix), L.ptr(self.count), L.ptr(self.total), float(u_sel),
+        total = self.total
+        if self.selection != "exact":
+            # rates of the drawn step and their parallel running sums; the draw
+            # scales the total the waiting time used (the fused pass's)
+            L.check(lib.mgk_kmc2d_rates_only(self.nx, self.ny, M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"],
+                                             L.ptr(self.rates), S), "mgk_kmc2d_rates_only")
+            L.check(lib.mgk_kmc_prefix_fast(L.ptr(self.rates), self.nx * self.ny * M, L.ptr(self.prefix),
+                                            L.ptr(self.count), L.ptr(self.total), L.ptr(self.work), S),
+                    "mgk_kmc_prefix_fast")
+            total = self.total_fast
+        L.check(lib.mgk_kmc_select(L.ptr(self.prefix), L.ptr(self.count), L.ptr(total), float(u_sel),
                                    L.ptr(self.sel), S), "mgk_kmc_select")
         nc = L.ptr(self.redraw)
         nq = L.c_void_p(self.redraw.data_ptr() + 4 * M * 8)

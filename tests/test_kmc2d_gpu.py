@@ -185,3 +185,35 @@ def test_exact_prefix_bit_for_bit(case):
     ref = np.cumsum(r)
     assert np.array_equal(p.view(np.int64), ref.view(np.int64))
     assert tot == (ref[-1] if r.size else 0.0)
+
+
+@pytest.mark.parametrize("n,T", [(64, 300.0), (256, 300.0), (96, 0.0)])
+def test_fused_barrier_total(n, T):
+    # the fused barrier + rate + block-sum pass of the fast selection mode:
+    # barriers bit-equal to the barrier kernel's, the total equal to the sum
+    # of the two-pass rates up to FP64 summation order
+    import torch
+    from mgkmc_b200 import _lib as L
+    rng = np.random.default_rng(3)
+    cat, Q0 = W.kmc2d_state(n, n, 8, rng)
+    sig = 1e8 * rng.standard_normal((n, n, 2, 2))
+    soft = np.abs(0.1 * rng.standard_normal((n, n, 2)))
+    tl = rng.uniform(-1e-9, 0.0, (n, n))
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+    tQ0, tsig, tcat, tsoft, ttl = d(Q0), d(sig), d(cat), d(soft), d(tl)
+    Qa, Qb = torch.zeros_like(tQ0), torch.zeros_like(tQ0)
+    lib, S = L.lib(), L.stream_ptr()
+    tau = 1e-10
+    L.check(lib.mgk_kmc2d_barrier(n, n, 8, L.ptr(Qa), L.ptr(tQ0), L.ptr(tsig), L.ptr(tcat), 1.0, L.ptr(tsoft),
+                                  L.ptr(ttl), 0.0, None, 2.0, 0, tau, S), "barrier")
+    nm = n * n * 8
+    work = torch.empty(int(lib.mgk_kmc_scan_work_bytes(nm)), dtype=torch.uint8, device="cuda")
+    tot = torch.zeros(1, dtype=torch.float64, device="cuda")
+    L.check(lib.mgk_kmc2d_barrier_total(n, n, 8, L.ptr(Qb), L.ptr(tQ0), L.ptr(tsig), L.ptr(tcat), 1.0, L.ptr(tsoft),
+                                        L.ptr(ttl), 0.0, None, 2.0, 0, tau, 1.0, None, T, 1e13, L.ptr(tot),
+                                        L.ptr(work), S), "barrier_total")
+    assert torch.equal(Qa, Qb)
+    rates = torch.empty(nm, dtype=torch.float64, device="cuda")
+    L.check(lib.mgk_kmc2d_rates_only(n, n, 8, L.ptr(Qa), 1.0, None, T, 1e13, L.ptr(rates), S), "rates_only")
+    r = rates.cpu().numpy()
+    assert abs(float(tot.item()) - np.sum(r)) <= 1e-13 * np.sum(r)
