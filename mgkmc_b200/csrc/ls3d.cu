@@ -728,11 +728,11 @@ __device__ __forceinline__ void ls3d_zline_fast_entry(const Ls3dRep* __restrict_
 #undef MGK_Z3_CASE
 }
 
-// FP32 phase kernel (the compiler's own register target), and the FP64
-// kernel with a register target of 5 resident CTAs per SM (measured faster
-// than 4 at 128^3 despite a few spilled registers)
+// FP32 phase kernel with a register target of 8 resident CTAs per SM, and
+// the FP64 kernel with one of 5 (both measured faster at 128^3 than the
+// compiler's own choice, despite some spilled registers)
 template <typename T, bool IN_SPEC, bool FINAL>
-__global__ void __launch_bounds__(96) ls3d_zline_fast_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
+__global__ void __launch_bounds__(96, 8) ls3d_zline_fast_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
                                                             const int* __restrict__ map, const int* __restrict__ loc,
                                                             double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
                                                             cudaGraphConditionalHandle cond, int use_cond,
@@ -828,9 +828,12 @@ __device__ __forceinline__ void ls3_axis_body(const Ls3dRep& R, const Ls3dState&
 // all 6 components; the FP64 y passes transform 3 components per CTA (two
 // CTAs per tile: 5 resident CTAs of 3 warps per SM instead of 2 of 6 at the
 // registers an FP64 line pair needs).  FP32 y passes keep 6 per CTA (measured
-// faster at 128^3).  Second value: resident-CTA target for the allocator.
+// faster at 128^3).  Second value: resident-CTA target for the allocator
+// (the FP32 x pass: 3, at most 96 registers).
 __host__ __device__ constexpr int ls3_axis_nc(int axis, int tsz) { return axis == 0 || tsz == 4 ? 6 : 3; }
-__host__ __device__ constexpr int ls3_axis_minb(int axis, int tsz) { return ls3_axis_nc(axis, tsz) == 3 ? 5 : 2; }
+__host__ __device__ constexpr int ls3_axis_minb(int axis, int tsz) {
+  return ls3_axis_nc(axis, tsz) == 3 ? 5 : (axis == 0 && tsz == 4 ? 3 : 2);
+}
 
 // grid = items * (6 / NC), the component group fastest
 template <typename T, int AXIS, int SIGN>
