@@ -85,6 +85,18 @@ MGK_API int mgk_ls2d_set_material(mgk_ls2d_t plan, const double* E, const double
                           const double* eps_plastic, mgk_stream_t stream);
 MGK_API int mgk_ls2d_set_material_rep(mgk_ls2d_t plan, int rep, const double* E, const double* nu,
                                       const double* eps_plastic, mgk_stream_t stream);
+/* Lame fields lam, mu (nx,ny) given directly, as spectral_solver_secant_2d
+ * takes them (mgkmc/linear_elastic_simulator.py:614-619), with the reference
+ * medium C0 = (mean lam, mean mu) (:679-681). */
+MGK_API int mgk_ls2d_set_lame_rep(mgk_ls2d_t plan, int rep, const double* lam, const double* mu,
+                                  const double* eps_plastic, mgk_stream_t stream);
+/* Constitutive law of every replica: d = 0 linear elastic; otherwise the
+ * secant degradation law of spectral_solver_secant_2d
+ * (linear_elastic_simulator.py:614-765; elasticity.py:112-150, :189-260):
+ * sigma = lam tr(e) I + 2 mu (1 - d (1 - exp(-k eq(e)))) e, e = eps - eps_p,
+ * eq the plane-strain von Mises equivalent strain.  0 <= d <= 1, k >= 0;
+ * FP64 plans only.  Takes effect at the next solve. */
+MGK_API int mgk_ls2d_set_secant(mgk_ls2d_t plan, double d, double k);
 /* Update only the eigenstrain field (KMC flips). */
 MGK_API int mgk_ls2d_set_eigenstrain(mgk_ls2d_t plan, const double* eps_plastic, mgk_stream_t stream);
 MGK_API int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t plan, int rep, const double* eps_plastic,

@@ -66,6 +66,9 @@ struct Ls2dRep {
   int nx, ny, nyh, ld, tc;
   int row_items, col_items;
   long long N;
+  // constitutive law: sec_d == 0 linear (elasticity.py:12-18); otherwise the
+  // secant degradation law with magnitude sec_d and rate sec_k
+  double sec_d, sec_k;
   FftLen fx64, fy64, fx32, fy32;
   double* mu;
   double* lam;
@@ -152,9 +155,22 @@ template <> struct Fields<float> {
 
 // -------------------------------------------------------------- kernels ---
 
+// Secant shear modulus mu (1 - d (1 - exp(-k eps_eq))) (elasticity.py:189-214)
+// at the von Mises equivalent strain of the elastic strain (dxx, dyy, sym
+// dxy): sqrt(2/3 eps':eps') with the plane-strain eps'_33 = -(dxx + dyy)/3
+// (elasticity.py:112-150; the two shear entries sum to 2 dxy).
+__device__ __forceinline__ double secant_mu(double m, double dxx, double dyy, double dxy, double d, double k) {
+  const double tr3 = (dxx + dyy) / 3.0;
+  const double a = dxx - tr3, b = dyy - tr3, c = -(dxx + dyy) / 3.0, sh = 2.0 * dxy;
+  const double eq = sqrt((2.0 / 3.0) * (a * a + b * b + c * c + 0.5 * sh * sh));
+  return m * (1.0 - d * (1.0 - exp(-k * eq)));
+}
+
 // Per-voxel material prep for one replica: mu, lambda from (E, nu) as in
-// elasticity.py:3-10, eigenstrain planes (and FP32 copies for mixed plans),
-// per-CTA partial sums of E and nu for the reference medium.
+// elasticity.py:3-10 (set_moduli 1), or given directly (set_moduli 2: E holds
+// lambda, nu holds mu, as the secant solver takes them), eigenstrain planes
+// (and FP32 copies for mixed plans), per-CTA partial sums of the two inputs
+// for the reference medium.
 __global__ void ls2d_material_kernel(const Ls2dRep* reps, int rep, const double* __restrict__ E,
                                      const double* __restrict__ nu, const double* __restrict__ epsp,
                                      int plane_mode, int set_moduli, double* partials) {
@@ -166,9 +182,10 @@ __global__ void ls2d_material_kernel(const Ls2dRep* reps, int rep, const double*
        i += (long long)gridDim.x * blockDim.x) {
     if (set_moduli) {
       const double e = E[i], v = nu[i];
-      const double mu = e / (2 * (1 + v));
-      const double lam = plane_mode == MGK_PLANE_STRESS ? e * v / (1 - v * v)
-                                                         : e * v / ((1 + v) * (1 - 2 * v));
+      const double mu = set_moduli == 2 ? v : e / (2 * (1 + v));
+      const double lam = set_moduli == 2 ? e
+                         : plane_mode == MGK_PLANE_STRESS ? e * v / (1 - v * v)
+                                                          : e * v / ((1 + v) * (1 - 2 * v));
       R.mu[i] = mu;
       R.lam[i] = lam;
       if (R.mu32) { R.mu32[i] = (float)mu; R.lam32[i] = (float)lam; }
@@ -200,9 +217,10 @@ __global__ void ls2d_material_kernel(const Ls2dRep* reps, int rep, const double*
   }
 }
 
-// Reference medium from the means (linear_elastic_simulator.py:22-26).
+// Reference medium from the means: of E and nu (linear_elastic_simulator.py:
+// 22-26), or of lambda and mu (lame_in; the secant solver, :679-681).
 __global__ void ls2d_medium_kernel(const Ls2dRep* reps, Ls2dState* st, int rep, const double* partials,
-                                   int nblocks, int plane_mode) {
+                                   int nblocks, int plane_mode, int lame_in) {
   __shared__ double red[32];
   double a = 0, b = 0;
   for (int i = threadIdx.x; i < nblocks; i += blockDim.x) { a += partials[2 * i]; b += partials[2 * i + 1]; }
@@ -211,8 +229,9 @@ __global__ void ls2d_medium_kernel(const Ls2dRep* reps, Ls2dState* st, int rep, 
   if (threadIdx.x == 0) {
     const double N = (double)reps[rep].N;
     const double E = a / N, v = b / N;
-    const double mu0 = E / (2 * (1 + v));
-    const double lam0 = plane_mode == MGK_PLANE_STRESS ? E * v / (1 - v * v) : E * v / ((1 + v) * (1 - 2 * v));
+    const double mu0 = lame_in ? v : E / (2 * (1 + v));
+    const double lam0 = lame_in ? E
+                        : plane_mode == MGK_PLANE_STRESS ? E * v / (1 - v * v) : E * v / ((1 + v) * (1 - 2 * v));
     Ls2dState& S = st[rep];
     S.mu0 = mu0;
     S.lam0 = lam0;
@@ -401,6 +420,7 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
   C* bufB = bufA + 3 * ny;
   C* spec = reinterpret_cast<C*>(R.spec);
   const double mu0 = S.mu0, lam0 = S.lam0;
+  const double sec_d = R.sec_d, sec_k = R.sec_k;
   const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
   TS* eps = Fields<TS>::eps(R);
   const TS* mu = Fields<TS>::mu(R);
@@ -471,9 +491,13 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
       }
       const double dxx = e[0] - p0, dyy = e[1] - p1, dxy = e[2] - p2;
       const double trd = dxx + dyy, tre = e[0] + e[1];
-      tr[h][0] = (TC)((2 * m * dxx + l * trd) - (2 * mu0 * e[0] + lam0 * tre));
-      tr[h][1] = (TC)((2 * m * dyy + l * trd) - (2 * mu0 * e[1] + lam0 * tre));
-      tr[h][2] = (TC)(2 * m * dxy - 2 * mu0 * e[2]);
+      double ms = m;  // FP64 kernels only: plans with the secant law are FP64
+      if constexpr (sizeof(TS) == 8) {
+        if (sec_d != 0.0) ms = secant_mu(m, dxx, dyy, dxy, sec_d, sec_k);
+      }
+      tr[h][0] = (TC)((2 * ms * dxx + l * trd) - (2 * mu0 * e[0] + lam0 * tre));
+      tr[h][1] = (TC)((2 * ms * dyy + l * trd) - (2 * mu0 * e[1] + lam0 * tre));
+      tr[h][2] = (TC)(2 * ms * dxy - 2 * mu0 * e[2]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
@@ -620,6 +644,7 @@ __global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __r
       C* cur = fft_any<+1>(bufA, bufB, 3, ny, fy);
       C* out = (cur == bufA) ? bufB : bufA;
       const double mu0 = S.mu0, lam0 = S.lam0;
+      const double sec_d = R.sec_d, sec_k = R.sec_k;
       const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
       TS* eps = Fields<TS>::eps(R);
       double d2 = 0, n2 = 0;
@@ -644,9 +669,13 @@ __global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __r
           eps[2 * N + i] = (TS)e2;
           const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
           const double trd = dxx + dyy, tre = e0 + e1;
-          tr[h][0] = (TC)((2 * m * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
-          tr[h][1] = (TC)((2 * m * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
-          tr[h][2] = (TC)(2 * m * dxy - 2 * mu0 * e2);
+          double ms = m;  // FP64 kernels only: plans with the secant law are FP64
+          if constexpr (sizeof(TS) == 8) {
+            if (sec_d != 0.0) ms = secant_mu(m, dxx, dyy, dxy, sec_d, sec_k);
+          }
+          tr[h][0] = (TC)((2 * ms * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
+          tr[h][1] = (TC)((2 * ms * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
+          tr[h][2] = (TC)(2 * ms * dxy - 2 * mu0 * e2);
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
@@ -809,7 +838,7 @@ __host__ __device__ constexpr int col_fast_smem(int nx, int csz, int tc) {
   return 3 * tc * (csz == 16 ? nx + nx / 8 + 1 : ((nx + nx / 16 + 2) & ~1)) * csz;
 }
 
-template <typename T, int NY, int G, bool IN_SPEC, bool FINAL>
+template <typename T, int NY, int G, bool IN_SPEC, bool FINAL, int LAW>
 __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, int item, int r, int x0,
                                               double* partials,
                                               unsigned int* rep_counter, Ls2dCtl* ctl,
@@ -867,6 +896,7 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
     return;
   }
   const double mu0 = S.mu0, lam0 = S.lam0;
+  const double sec_d = R.sec_d, sec_k = R.sec_k;
   const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
   double d2 = 0, n2 = 0;
   for (int y = threadIdx.x; y < NY; y += NT) {
@@ -900,9 +930,11 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
       }
       const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
       const double trd = dxx + dyy, tre = e0 + e1;
-      tr[h][0] = (T)((2 * m * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
-      tr[h][1] = (T)((2 * m * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
-      tr[h][2] = (T)(2 * m * dxy - 2 * mu0 * e2);
+      double ms = m;  // LAW 1: the secant law (FP64 plans; LAW 0 is the linear law)
+      if constexpr (LAW == 1) ms = secant_mu(m, dxx, dyy, dxy, sec_d, sec_k);
+      tr[h][0] = (T)((2 * ms * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
+      tr[h][1] = (T)((2 * ms * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
+      tr[h][2] = (T)(2 * ms * dxy - 2 * mu0 * e2);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) lines[c * PL + py] = mk<C>(tr[0][c], tr[1][c]);
@@ -931,7 +963,7 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
   ls2d_decide<FINAL>(R, S, partials, ctl, cond, use_cond, guard_cap, red);
 }
 
-template <typename T, int MAXN, bool IN_SPEC, bool FINAL>
+template <typename T, int MAXN, bool IN_SPEC, bool FINAL, int LAW = 0>
 __global__ void __launch_bounds__(row_threads(MAXN), sizeof(T) == 4 && MAXN <= 256 ? MGK_ROW_MINB32 : 1) ls2d_row_fast_kernel(
     const Ls2dRep* __restrict__ reps, Ls2dState* st, const int* __restrict__ row_map,
     const int* __restrict__ row_local, double* partials, unsigned int* rep_counter, Ls2dCtl* ctl,
@@ -959,7 +991,7 @@ __global__ void __launch_bounds__(row_threads(MAXN), sizeof(T) == 4 && MAXN <= 2
   __syncthreads();
   const int x0 = 2 * row_local[item];
 #define MGK_ROW_CASE(n) \
-  case n: if constexpr (n <= MAXN) row_fast_body<T, n, fast_group(MAXN), IN_SPEC, FINAL>(R, S, item, r, x0, partials, rep_counter, ctl, cond, use_cond, guard_cap, \
+  case n: if constexpr (n <= MAXN) row_fast_body<T, n, fast_group(MAXN), IN_SPEC, FINAL, LAW>(R, S, item, r, x0, partials, rep_counter, ctl, cond, use_cond, guard_cap, \
                                               smem_raw, &bar, red, &s_last); break;
   switch (R.ny) {
     MGK_ROW_CASE(64) MGK_ROW_CASE(96) MGK_ROW_CASE(128) MGK_ROW_CASE(192) MGK_ROW_CASE(256) MGK_ROW_CASE(384)
@@ -1096,6 +1128,7 @@ __global__ void ls2d_phase2_kernel(Ls2dState* st, const int* sel, int nsel, Ls2d
 // Outputs in the reference layout: eps, sig (nx,ny,2,2) and partial sums of
 // their components for the means (linear_elastic_simulator.py:83-88).
 // grid = (G, nsel).
+template <int LAW = 0>  // 1: the secant law
 __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
   const int r = sel[blockIdx.y];
@@ -1105,6 +1138,7 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
   const double abar = S.abar;
   double* eps_out = R.out_eps;
   double* sig_out = R.out_sig;
+  const double sec_d = R.sec_d, sec_k = R.sec_k;
   double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
@@ -1115,8 +1149,10 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
     double pxx = R.ep[i], pyy = R.ep[N + i], pxy, pyx;
     if (R.epa) { pxy = R.epa[i]; pyx = R.epa[N + i]; }
     else { pxy = R.ep[2 * N + i]; pyx = pxy; }
-    const double mu = R.mu[i], lam = R.lam[i];
+    const double lam = R.lam[i];
     const double dxx = exx - pxx, dxy = exy - pxy, dyx = eyx - pyx, dyy = eyy - pyy;
+    double mu = R.mu[i];
+    if constexpr (LAW == 1) mu = secant_mu(mu, dxx, dyy, 0.5 * (dxy + dyx), sec_d, sec_k);
     const double tr = dxx + dyy;
     const double sxx = 2 * mu * dxx + lam * tr, syy = 2 * mu * dyy + lam * tr;
     const double sxy2 = 2 * mu * dxy, syx2 = 2 * mu * dyx;
@@ -1166,6 +1202,7 @@ struct mgk_ls2d_plan {
   size_t row_smem32 = 0, col_smem32 = 0;  // FP32 iteration kernels
   int fast = 0;                           // kernel family in use: 0 CTA-wide passes, 256/512/1024 warp-line
   int fast_nat = 0;                       // smallest warp-line family that covers every side (0: none)
+  int law = 0;                            // 1: secant degradation law (mgk_ls2d_set_secant)
   std::vector<int> tc_gen;                // column tiles of the CTA-wide family, per replica
   std::vector<Ls2dRep> reps;      // host copy (static part)
   std::vector<char> has_material;
@@ -1220,7 +1257,13 @@ static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
 
 // warp-line kernel variants: sides up to 256, or up to 512 (more registers)
 template <typename TS, bool IN_SPEC, bool FINAL>
-static void* row_fast_fn(int fast) {
+static void* row_fast_fn(int fast, int law = 0) {
+  if constexpr (sizeof(TS) == 8) {
+    if (law)  // the secant law (FP64 plans only)
+      return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL, 1>
+             : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL, 1>
+                          : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL, 1>;
+  }
   return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL>
          : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL>
                       : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL>;
@@ -1234,8 +1277,10 @@ static void* col_fast_fn(int fast) {
 
 template <typename T>
 static int ls2d_set_fast_attrs(int fast, size_t row_smem, size_t col_smem) {
-  void* fns[4] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
-                  row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast)};
+  void* fns[8] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
+                  row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast),
+                  row_fast_fn<T, true, true>(fast, 1), row_fast_fn<T, false, true>(fast, 1),
+                  row_fast_fn<T, true, false>(fast, 1), row_fast_fn<T, false, false>(fast, 1)};
   for (void* f : fns) MGK_CUDA(raise_smem((const void*)f, (int)row_smem));
   MGK_CUDA(raise_smem((const void*)col_fast_fn<T>(fast), (int)col_smem));
   return MGK_OK;
@@ -1473,7 +1518,8 @@ static int ls2d_set_fields(mgk_ls2d_t p, int rep, const double* E, const double*
                                                  p->d_mat_part);
   MGK_CUDA(cudaGetLastError());
   if (set_moduli) {
-    ls2d_medium_kernel<<<1, kThreads, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, grid, p->plane_mode);
+    ls2d_medium_kernel<<<1, kThreads, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, grid, p->plane_mode,
+                                              set_moduli == 2 ? 1 : 0);
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
@@ -1491,6 +1537,37 @@ extern "C" int mgk_ls2d_set_material_rep(mgk_ls2d_t p, int rep, const double* E,
 extern "C" int mgk_ls2d_set_material(mgk_ls2d_t p, const double* E, const double* nu, const double* epsp,
                                      mgk_stream_t stream) {
   return mgk_ls2d_set_material_rep(p, 0, E, nu, epsp, stream);
+}
+
+extern "C" int mgk_ls2d_set_lame_rep(mgk_ls2d_t p, int rep, const double* lam, const double* mu,
+                                     const double* epsp, mgk_stream_t stream) {
+  MGK_REQUIRE(p && lam && mu, "mgk_ls2d_set_lame: null argument");
+  MGK_REQUIRE(rep >= 0 && rep < p->nrep, "mgk_ls2d_set_lame: replica %d out of range", rep);
+  int st = ls2d_set_fields(p, rep, lam, mu, epsp, 2, (cudaStream_t)stream);
+  if (st == MGK_OK) p->has_material[rep] = 1;
+  return st;
+}
+
+extern "C" int mgk_ls2d_set_secant(mgk_ls2d_t p, double d, double k) {
+  MGK_REQUIRE(p, "mgk_ls2d_set_secant: null plan");
+  MGK_REQUIRE(d >= 0.0 && d <= 1.0 && k >= 0.0 && isfinite(k), "mgk_ls2d_set_secant: need 0 <= d <= 1, k >= 0");
+  MGK_REQUIRE(d == 0.0 || p->prec == MGK_FP64, "mgk_ls2d_set_secant: the secant law runs in FP64 plans only");
+  for (auto& R : p->reps) { R.sec_d = d; R.sec_k = k; }
+  const int law = d != 0.0 ? 1 : 0;
+  if (law != p->law) {
+    // cached loop graphs hold the other law's row kernel
+    for (auto& e : p->gcache) {
+      cudaGraphExecDestroy(e.x);
+      cudaGraphDestroy(e.g);
+    }
+    p->gcache.clear();
+    p->graph = nullptr;
+    p->exec = nullptr;
+    p->sel_rows = p->sel_cols = p->nsel = 0;  // the next solve builds its graph again
+    if (p->graph_mode == 1) p->graph_mode = -1;
+    p->law = law;
+  }
+  return MGK_OK;
 }
 
 extern "C" int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t p, int rep, const double* epsp, mgk_stream_t stream) {
@@ -1522,12 +1599,13 @@ struct LoopArgs {
   int stage_bytes;
   size_t tma_smem;
   int fast;           // warp-line iteration kernels
+  int law = 0;        // constitutive law of the warp-line row kernel (1: secant)
 };
 
 template <typename TS, bool IN_SPEC, bool FINAL>
 static void launch_row(const LoopArgs& a, cudaStream_t s) {
   if (a.fast) {
-    void* fn = row_fast_fn<TS, IN_SPEC, FINAL>(a.fast);
+    void* fn = row_fast_fn<TS, IN_SPEC, FINAL>(a.fast, a.law);
     cudaGraphConditionalHandle h = 0;
     int zero = 0;
     void* args[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.row_map, (void*)&a.row_local, (void*)&a.part,
@@ -1601,7 +1679,7 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
     k2.kernelParams = a2t;
     k2.blockDim = dim3(kThreads);
   } else {
-    k2.func = a.fast ? row_fast_fn<TS, true, FINAL>(a.fast) : (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
+    k2.func = a.fast ? row_fast_fn<TS, true, FINAL>(a.fast, a.law) : (void*)ls2d_row_kernel<TS, TS, true, FINAL>;
     k2.gridDim = dim3(a.rows);
     k2.sharedMemBytes = (unsigned)a.row_smem;
     k2.kernelParams = a2;
@@ -1651,7 +1729,7 @@ static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_
       int zero = 0;
       void* ap3[] = {&a64.reps, &a64.st, &a64.row_map, &a64.row_local, &a64.part, &a64.repctr, &a64.ctl,
                      &h0, &zero, &zero};
-      k3.func = a64.fast ? row_fast_fn<double, false, true>(a64.fast)
+      k3.func = a64.fast ? row_fast_fn<double, false, true>(a64.fast, a64.law)
                          : (void*)ls2d_row_kernel<double, double, false, true>;
       k3.gridDim = dim3(a64.rows);
       k3.blockDim = dim3(a64.fast ? row_threads(a64.fast) : kThreads);
@@ -1886,7 +1964,9 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     LoopArgs a64{p->d_reps, p->d_st, d_row_map, d_row_local, d_col_map, d_col_local, p->d_part, p->d_repctr,
                  p->d_ctl, rows, cols, p->row_smem, p->col_smem, p->tma, 0, p->stage64, p->tma_smem64, p->fast};
     a64.row_grid = std::max(1, std::min(rows, p->occ64 * p->num_sms));
+    a64.law = p->law;
     LoopArgs a32 = a64;
+    a32.law = 0;
     a32.row_smem = p->row_smem32;
     a32.col_smem = p->col_smem32;
     a32.stage_bytes = p->stage32;
@@ -1938,7 +2018,8 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
       }
     }
   }
-  ls2d_output_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  if (p->law) ls2d_output_kernel<1><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  else ls2d_output_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());
   ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 8,
                                                  (int)offsetof(Ls2dState, out_eps_mean), 0);
@@ -1967,6 +2048,7 @@ static int profile_t(mgk_ls2d_t p, float* row_ms, float* col_ms, int reps, cudaS
   const size_t cs = sizeof(TS) == 8 ? p->col_smem : p->col_smem32;
   LoopArgs a{p->d_reps, p->d_st, d_row_map, d_row_local, d_col_map, d_col_local, p->d_part, p->d_repctr,
              p->d_ctl, rows, cols, rs, cs, 0, 0, 0, 0, p->fast};
+  a.law = sizeof(TS) == 8 ? p->law : 0;
   launch_row<TS, false, true>(a, s);
   MGK_CUDA(cudaGetLastError());
   cudaEvent_t ev[3];
@@ -2234,7 +2316,7 @@ extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const doub
   const int G = grid_blocks(N);
   ls2d_material_kernel<<<G, kThreads, 0, s>>>(d_rep, 0, E, nu, eps_plastic, plane_mode, 1, part);
   MGK_CUDA(cudaGetLastError());
-  ls2d_medium_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, 0, part, G, plane_mode);
+  ls2d_medium_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, 0, part, G, plane_mode, 0);
   MGK_CUDA(cudaGetLastError());
   if (eps_init) {
     ls2d_means_kernel<<<dim3(G, 1), kThreads, 0, s>>>(d_rep, d_sel, part);

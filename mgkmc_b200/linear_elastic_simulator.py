@@ -72,6 +72,17 @@ class Ls2dBatch:
         L.check(L.lib().mgk_ls2d_set_eigenstrain_rep(self._h, int(rep), L.ptr(eps_plastic), L.stream_ptr(stream)),
                 "mgk_ls2d_set_eigenstrain")
 
+    def set_lame(self, rep, lam, mu, eps_plastic=None, stream=None):
+        """Lame fields given directly (the secant solver's inputs); reference
+        medium (mean lam, mean mu)."""
+        self._keep[("m", rep)] = (lam, mu, eps_plastic)
+        L.check(L.lib().mgk_ls2d_set_lame_rep(self._h, int(rep), L.ptr(lam), L.ptr(mu), L.ptr(eps_plastic),
+                                              L.stream_ptr(stream)), "mgk_ls2d_set_lame")
+
+    def set_secant(self, d, k):
+        """Secant degradation law for every replica (d = 0: linear); FP64 plans."""
+        L.check(L.lib().mgk_ls2d_set_secant(self._h, float(d), float(k)), "mgk_ls2d_set_secant")
+
     def solve(self, reps, eps_bars, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True,
               stream=None):
         """Solve replicas ``reps`` (one launch per stage for all of them).
@@ -195,6 +206,40 @@ def spectral_solver_2d(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6,
     info = p.solve(eps_bar, eps, sig, eps_init=tin, max_iter=max_iter, tol=tol, sync=True)
     if verbose:
         print(f"LS 2D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
+    eps_np = eps.cpu().numpy()
+    sig_np = sig.cpu().numpy()
+    return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
+
+
+_PLANS_SECANT = {}
+
+
+def spectral_solver_secant_2d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, verbose=False,
+                              pixel=1.0, plane_mode="plane_strain", Gamma=None, eps_init=None):
+    """Nonlinear 2D Lippmann-Schwinger solve with the secant degradation law
+    (linear_elastic_simulator.py:614-765): sigma = lam tr(e) I + 2 mu_sec e,
+    e = eps - eps_plastic, mu_sec = mu (1 - d (1 - exp(-k eps_eq(e)))), the
+    reference medium (mean lam, mean mu) held fixed.  ``lam`` is the caller's
+    (effective, for plane stress) lambda field, as in the reference.  Returns
+    (eps, sig, eps.mean(axis=(0,1)), sig.mean(axis=(0,1)))."""
+    torch = _torch()
+    lam = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
+    mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
+    nx, ny = lam.shape
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (nx, ny, dev.index)
+    p = _PLANS_SECANT.get(key)
+    if p is None:
+        p = _PLANS_SECANT[key] = Ls2dBatch([(nx, ny)])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    eps = torch.empty((nx, ny, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
+    p.set_secant(d, k)
+    info = p.solve([0], [eps_bar], [eps], [sig], eps_init=None if eps_init is None else [t(eps_init)],
+                   max_iter=max_iter, tol=tol)[0]
+    if verbose:
+        print(f"secant LS 2D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
     eps_np = eps.cpu().numpy()
     sig_np = sig.cpu().numpy()
     return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))

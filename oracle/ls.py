@@ -5,6 +5,8 @@ TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 Follows mgkmc/linear_elastic_simulator.py:
   * ``spectral_solver_2d``  -- :12-88
   * ``spectral_solver_3d``  -- :274-376
+  * ``spectral_solver_secant_2d`` -- :614-765 (secant degradation law,
+    elasticity.py:112-150, :189-260)
   * ``mixed_bc_solve_2d``   -- the macro mixed stress/strain loop of
     ``linear_elastic_simulation_2d`` :176-197 with the compliance correction of
     :150-152, here with an eigenstrain field (the reference driver has no
@@ -121,6 +123,56 @@ def spectral_solver(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6,
     if return_info:
         return out + (it_done, diff)
     return out
+
+
+def von_mises_strain_2d(e):
+    """sqrt(2/3 e':e'), plane strain (e'_33 = -(e11 + e22)/3)
+    (mgkmc/elasticity.py:112-150)."""
+    e11, e22, e12, e21 = e[..., 0, 0], e[..., 1, 1], e[..., 0, 1], e[..., 1, 0]
+    tr3 = (e11 + e22) / 3.0
+    return np.sqrt((2.0 / 3.0) * ((e11 - tr3) ** 2 + (e22 - tr3) ** 2 + (-(e11 + e22) / 3.0) ** 2
+                                  + 0.5 * (e12 + e21) ** 2))
+
+
+def secant_stress_2d(e, lam, mu, d, k):
+    """lam tr(e) I + 2 mu (1 - d (1 - exp(-k eq(e)))) e
+    (mgkmc/elasticity.py:189-260)."""
+    mu_sec = mu * (1.0 - d * (1.0 - np.exp(-k * von_mises_strain_2d(e))))
+    return hooke(e, lam, mu_sec, 2)
+
+
+def spectral_solver_secant_2d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
+                              eps_init=None, return_info=False):
+    """Secant-degradation LS fixed point (mgkmc/linear_elastic_simulator.py:
+    614-765): reference medium (mean lam, mean mu) fixed; tau = sigma_sec(eps
+    - eps_p) - C0:eps; same Green step, update and stopping rule as the linear
+    solver."""
+    lam0, mu0 = float(np.mean(lam)), float(np.mean(mu))
+    shape = np.shape(lam)
+    axes = (0, 1)
+    G = green_operator(wave_vectors(shape, pixel), lam0, mu0)
+    if eps_init is not None:
+        eps = eps_init.copy()
+        eps += eps_bar - eps_init.mean(axis=axes)
+    else:
+        eps = np.broadcast_to(eps_bar, shape + (2, 2)).copy()
+    ep = eps_plastic
+    it_done, diff = 0, np.inf
+    for it in range(max_iter):
+        sig = secant_stress_2d(eps - ep if ep is not None else eps, lam, mu, d, k)
+        tau = sig - hooke(eps, lam0, mu0, 2)
+        tau_hat = np.fft.fftn(tau, axes=axes, norm="ortho")
+        et = np.fft.ifftn(-np.einsum("xykhij,xyij->xykh", G, tau_hat), axes=axes, norm="ortho").real
+        et -= et.mean(axis=axes)
+        eps_new = eps_bar + et
+        diff = np.linalg.norm(eps_new - eps) / (np.linalg.norm(eps) + 1e-20)
+        eps = eps_new
+        it_done = it + 1
+        if diff < tol:
+            break
+    sig_out = secant_stress_2d(eps - ep if ep is not None else eps, lam, mu, d, k)
+    out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
+    return out + (it_done, diff) if return_info else out
 
 
 def equilibrium_residual(eps, E, nu, eps_bar, eps_plastic=None, pixel=1.0, plane_mode="plane_strain"):

@@ -237,9 +237,31 @@ def fs3d_fixtures():
     save("fs2d_neohookean_5", E=E2, nu=nu2, F=F2, P=P2, K4=K42)
 
 
+def ls2d_secant_fixtures():
+    """The reference's secant-degradation LS solver (spectral_solver_secant_2d)
+    on a heterogeneous medium with eigenstrains, warm and cold starts."""
+    rng = np.random.default_rng(61)
+    nx, ny = 24, 16
+    E, nu = W.ls2d_material(nx, ny, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    ep = W.pure_shear_eigenstrain_2d(nx, ny, rng, frac=0.1)
+    eb = np.array([[0.02, 0.0], [0.0, -0.005]])
+    out = dict(lam=lam, mu=mu, eps_plastic=ep, eps_bar=eb)
+    for tag, d, k in (("a", 0.3, 50.0), ("b", 0.8, 200.0)):
+        e, s, em, sm = LES.spectral_solver_secant_2d(lam, mu, d, k, eb, eps_plastic=ep, max_iter=500, tol=1e-12)
+        out.update({f"eps_{tag}": e, f"sig_{tag}": s, f"d_{tag}": d, f"k_{tag}": k})
+    init = out["eps_a"] + 1e-4 * rng.standard_normal(out["eps_a"].shape)
+    e, s, _, _ = LES.spectral_solver_secant_2d(lam, mu, 0.3, 50.0, eb * 1.1, eps_plastic=ep, max_iter=500, tol=1e-12,
+                                               eps_init=init)
+    out.update(eps_init=init, eps_warm=e, sig_warm=s)
+    save("ls2d_secant_24x16", **out)
+
+
 if __name__ == "__main__":
     ls2d_fixtures()
     ls3d_fixtures()
     kmc2d_fixtures()
     kmc3d_fixtures()
     fs3d_fixtures()
+    ls2d_secant_fixtures()

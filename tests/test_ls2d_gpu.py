@@ -116,3 +116,51 @@ def test_not_converged_status(les):
     assert info.iterations == 4 and info.status == 1
     o = OL.spectral_solver(E, nu, eb, ep, max_iter=4, tol=1e-14, return_info=True)
     assert abs(info.final_diff - o[5]) < 1e-9 * o[5]
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_golden_secant(les, golden, tag):
+    # secant-degradation law (CTA-wide kernels at 24 x 16) against the reference
+    g = golden("ls2d_secant_24x16")
+    eps, sig, em, sm = les.spectral_solver_secant_2d(g["lam"], g["mu"], float(g[f"d_{tag}"]), float(g[f"k_{tag}"]),
+                                                     g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-12)
+    assert rel(eps, g[f"eps_{tag}"]) < TOL
+    assert rel(sig, g[f"sig_{tag}"]) < TOL
+    assert np.allclose(sm, g[f"sig_{tag}"].mean(axis=(0, 1)), rtol=1e-9, atol=0)
+
+
+def test_golden_secant_warm(les, golden):
+    g = golden("ls2d_secant_24x16")
+    eps, sig, _, _ = les.spectral_solver_secant_2d(g["lam"], g["mu"], 0.3, 50.0, g["eps_bar"] * 1.1, g["eps_plastic"],
+                                                   max_iter=500, tol=1e-12, eps_init=g["eps_init"])
+    assert rel(eps, g["eps_warm"]) < TOL
+    assert rel(sig, g["sig_warm"]) < TOL
+
+
+@pytest.mark.parametrize("nx,ny,d,k", [(64, 64, 0.5, 100.0), (256, 128, 0.3, 50.0), (96, 192, 0.9, 300.0)])
+def test_secant_against_oracle(les, nx, ny, d, k):
+    # warp-line kernels (sides 64..256) and the secant law, against the oracle
+    E, nu, ep, eb = W.ls2d_problem(nx, ny, seed=11)
+    eb = np.array([[0.03, 0.0], [0.0, -0.01]])
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eps, sig, _, _ = les.spectral_solver_secant_2d(lam, mu, d, k, eb, ep, max_iter=500, tol=1e-11)
+    o = OL.spectral_solver_secant_2d(lam, mu, d, k, eb, ep, max_iter=500, tol=1e-11)
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
+def test_secant_d0_is_linear_and_mixed_refused(les):
+    # d = 0 reduces to Hooke's law with the (mean lam, mean mu) medium; the
+    # secant law is refused on mixed-precision plans
+    import torch
+    from mgkmc_b200 import _lib as L
+    E, nu, ep, eb = W.ls2d_problem(64, 64, seed=5)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eps, sig, _, _ = les.spectral_solver_secant_2d(lam, mu, 0.0, 10.0, eb, ep, max_iter=500, tol=1e-11)
+    o = OL.spectral_solver_secant_2d(lam, mu, 0.0, 10.0, eb, ep, max_iter=500, tol=1e-11)
+    assert rel(eps, o[0]) < TOL and rel(sig, o[1]) < TOL
+    b = les.Ls2dBatch([(64, 64)], precision="mixed")
+    with pytest.raises(L.MgkError):
+        b.set_secant(0.5, 10.0)

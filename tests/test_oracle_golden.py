@@ -39,6 +39,24 @@ def test_ls2d_plane_stress_warm_start_asymmetric(golden):
     assert rel(eps, g["eps_conv"]) < 1e-12
 
 
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_ls2d_secant(golden, tag):
+    # the secant-degradation LS restatement against the reference's solver
+    g = golden("ls2d_secant_24x16")
+    eps, sig, _, _ = OL.spectral_solver_secant_2d(g["lam"], g["mu"], float(g[f"d_{tag}"]), float(g[f"k_{tag}"]),
+                                                  g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-12)
+    assert rel(eps, g[f"eps_{tag}"]) < 1e-12
+    assert rel(sig, g[f"sig_{tag}"]) < 1e-12
+
+
+def test_ls2d_secant_warm(golden):
+    g = golden("ls2d_secant_24x16")
+    eps, sig, _, _ = OL.spectral_solver_secant_2d(g["lam"], g["mu"], 0.3, 50.0, g["eps_bar"] * 1.1, g["eps_plastic"],
+                                                  max_iter=500, tol=1e-12, eps_init=g["eps_init"])
+    assert rel(eps, g["eps_warm"]) < 1e-12
+    assert rel(sig, g["sig_warm"]) < 1e-12
+
+
 def test_ls2d_macro_loop(golden):
     g = golden("ls2d_macro_16")
     E, nu, mask, target = g["E"], g["nu"], g["mask"], g["target"]
