@@ -223,8 +223,8 @@ def spectral_solver_secant_2d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
     (effective, for plane stress) lambda field, as in the reference.  Returns
     (eps, sig, eps.mean(axis=(0,1)), sig.mean(axis=(0,1)))."""
     torch = _torch()
-    lam = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
-    mu = np.ascontiguousarray(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
+    lam = np.array(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
+    mu = np.array(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
     nx, ny = lam.shape
     dev = torch.device("cuda", torch.cuda.current_device())
     key = (nx, ny, dev.index)
