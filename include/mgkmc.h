@@ -97,6 +97,14 @@ MGK_API int mgk_ls2d_set_lame_rep(mgk_ls2d_t plan, int rep, const double* lam, c
  * eq the plane-strain von Mises equivalent strain.  0 <= d <= 1, k >= 0;
  * FP64 plans only.  Takes effect at the next solve. */
 MGK_API int mgk_ls2d_set_secant(mgk_ls2d_t plan, double d, double k);
+/* The Rose secant-modulus law of spectral_solver_rose_2d
+ * (linear_elastic_simulator.py:852-950; elasticity.py:868-944) for every
+ * replica: G = max(mu exp(-eta eq), floor_fraction mu), bulk modulus kept,
+ * sigma_yx copied from sigma_xy; plane_stress != 0 solves eps_zz per voxel by
+ * the reference's five fixed-point steps.  Reference medium (mean lam,
+ * (mean mu + floor_fraction mean mu) / 2): call before mgk_ls2d_set_lame_rep.
+ * Macro strain, eigenstrain and warm start must be symmetric; FP64 plans. */
+MGK_API int mgk_ls2d_set_rose(mgk_ls2d_t plan, double eta, double floor_fraction, int plane_stress);
 /* Update only the eigenstrain field (KMC flips). */
 MGK_API int mgk_ls2d_set_eigenstrain(mgk_ls2d_t plan, const double* eps_plastic, mgk_stream_t stream);
 MGK_API int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t plan, int rep, const double* eps_plastic,

@@ -66,9 +66,11 @@ struct Ls2dRep {
   int nx, ny, nyh, ld, tc;
   int row_items, col_items;
   long long N;
-  // constitutive law: sec_d == 0 linear (elasticity.py:12-18); otherwise the
-  // secant degradation law with magnitude sec_d and rate sec_k
-  double sec_d, sec_k;
+  // constitutive law: 0 linear (elasticity.py:12-18); 1 secant degradation
+  // (law_a = d, law_b = k); 2 Rose (law_a = eta, law_b = floor fraction,
+  // law_ps = 1 for plane stress)
+  int law, law_ps;
+  double law_a, law_b;
   FftLen fx64, fy64, fx32, fy32;
   double* mu;
   double* lam;
@@ -166,6 +168,53 @@ __device__ __forceinline__ double secant_mu(double m, double dxx, double dyy, do
   return m * (1.0 - d * (1.0 - exp(-k * eq)));
 }
 
+// Rose secant model (elasticity.py:868-944) at the elastic strain (dxx, dyy,
+// dxy = its [0,1] entry): G = max(mu exp(-eta eq), floor mu), bulk modulus
+// K = lam + 2 mu / 3 kept, lam_eff = K - 2 G / 3; plane stress solves
+// eps_zz by the reference's five fixed-point steps.  Returns the trace
+// (eps_zz included) and sets G and lam_eff.
+__device__ __forceinline__ double rose_moduli(double l, double m, double dxx, double dyy, double dxy, double eta,
+                                              double floor_f, int pstress, double& G, double& lam_eff) {
+  const double K = l + (2.0 / 3.0) * m;
+  double ezz = 0.0;
+  auto eq_of = [&](double zz) {
+    const double tr3 = (dxx + dyy + zz) / 3.0;
+    const double a = dxx - tr3, b = dyy - tr3, c = zz - tr3;
+    return sqrt((2.0 / 3.0) * (a * a + b * b + c * c + 2.0 * dxy * dxy));
+  };
+  auto g_of = [&](double eq) { return fmax(m * exp(-eta * eq), floor_f * m); };
+  if (pstress) {
+    ezz = -l / (l + 2.0 * m) * (dxx + dyy);
+    for (int it = 0; it < 5; ++it) {
+      const double g = g_of(eq_of(ezz));
+      ezz = -((3.0 * K - 2.0 * g) / (3.0 * K + 4.0 * g)) * (dxx + dyy);
+    }
+  }
+  G = g_of(eq_of(ezz));
+  lam_eff = K - (2.0 / 3.0) * G;
+  return dxx + dyy + ezz;
+}
+
+// stress of the elastic strain (dxx, dyy, dxy) under law LAW; m, l the voxel's
+// mu, lambda; LAW 0 is Hooke's law with the reference's operation order
+template <int LAW>
+__device__ __forceinline__ void law_sigma(double m, double l, double dxx, double dyy, double dxy, double a, double b,
+                                          int ps, double& sxx, double& syy, double& sxy) {
+  if constexpr (LAW == 2) {
+    double G, le;
+    const double tr = rose_moduli(l, m, dxx, dyy, dxy, a, b, ps, G, le);
+    sxx = le * tr + 2.0 * G * dxx;
+    syy = le * tr + 2.0 * G * dyy;
+    sxy = 2.0 * G * dxy;
+  } else {
+    const double ms = LAW == 1 ? secant_mu(m, dxx, dyy, dxy, a, b) : m;
+    const double trd = dxx + dyy;
+    sxx = 2 * ms * dxx + l * trd;
+    syy = 2 * ms * dyy + l * trd;
+    sxy = 2 * ms * dxy;
+  }
+}
+
 // Per-voxel material prep for one replica: mu, lambda from (E, nu) as in
 // elasticity.py:3-10 (set_moduli 1), or given directly (set_moduli 2: E holds
 // lambda, nu holds mu, as the secant solver takes them), eigenstrain planes
@@ -218,9 +267,11 @@ __global__ void ls2d_material_kernel(const Ls2dRep* reps, int rep, const double*
 }
 
 // Reference medium from the means: of E and nu (linear_elastic_simulator.py:
-// 22-26), or of lambda and mu (lame_in; the secant solver, :679-681).
+// 22-26), or of lambda and mu (lame_in 1: the secant solver, :679-681;
+// lame_in 2: the Rose solver's (mean lambda, (mean mu + floor mean mu) / 2),
+// :866-869).
 __global__ void ls2d_medium_kernel(const Ls2dRep* reps, Ls2dState* st, int rep, const double* partials,
-                                   int nblocks, int plane_mode, int lame_in) {
+                                   int nblocks, int plane_mode, int lame_in, double floor_f) {
   __shared__ double red[32];
   double a = 0, b = 0;
   for (int i = threadIdx.x; i < nblocks; i += blockDim.x) { a += partials[2 * i]; b += partials[2 * i + 1]; }
@@ -229,7 +280,7 @@ __global__ void ls2d_medium_kernel(const Ls2dRep* reps, Ls2dState* st, int rep, 
   if (threadIdx.x == 0) {
     const double N = (double)reps[rep].N;
     const double E = a / N, v = b / N;
-    const double mu0 = lame_in ? v : E / (2 * (1 + v));
+    const double mu0 = lame_in == 2 ? 0.5 * (v + floor_f * v) : lame_in ? v : E / (2 * (1 + v));
     const double lam0 = lame_in ? E
                         : plane_mode == MGK_PLANE_STRESS ? E * v / (1 - v * v) : E * v / ((1 + v) * (1 - 2 * v));
     Ls2dState& S = st[rep];
@@ -420,7 +471,8 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
   C* bufB = bufA + 3 * ny;
   C* spec = reinterpret_cast<C*>(R.spec);
   const double mu0 = S.mu0, lam0 = S.lam0;
-  const double sec_d = R.sec_d, sec_k = R.sec_k;
+  const int law = R.law, law_ps = R.law_ps;
+  const double law_a = R.law_a, law_b = R.law_b;
   const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
   TS* eps = Fields<TS>::eps(R);
   const TS* mu = Fields<TS>::mu(R);
@@ -490,14 +542,14 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
         e[0] = o0; e[1] = o1; e[2] = o2;
       }
       const double dxx = e[0] - p0, dyy = e[1] - p1, dxy = e[2] - p2;
-      const double trd = dxx + dyy, tre = e[0] + e[1];
-      double ms = m;  // FP64 kernels only: plans with the secant law are FP64
-      if constexpr (sizeof(TS) == 8) {
-        if (sec_d != 0.0) ms = secant_mu(m, dxx, dyy, dxy, sec_d, sec_k);
-      }
-      tr[h][0] = (TC)((2 * ms * dxx + l * trd) - (2 * mu0 * e[0] + lam0 * tre));
-      tr[h][1] = (TC)((2 * ms * dyy + l * trd) - (2 * mu0 * e[1] + lam0 * tre));
-      tr[h][2] = (TC)(2 * ms * dxy - 2 * mu0 * e[2]);
+      const double tre = e[0] + e[1];
+      double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
+      if (sizeof(TS) == 8 && law == 1) law_sigma<1>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+      else if (sizeof(TS) == 8 && law == 2) law_sigma<2>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+      else law_sigma<0>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2);
+      tr[h][0] = (TC)(s0 - (2 * mu0 * e[0] + lam0 * tre));
+      tr[h][1] = (TC)(s1 - (2 * mu0 * e[1] + lam0 * tre));
+      tr[h][2] = (TC)(s2 - 2 * mu0 * e[2]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
@@ -644,7 +696,8 @@ __global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __r
       C* cur = fft_any<+1>(bufA, bufB, 3, ny, fy);
       C* out = (cur == bufA) ? bufB : bufA;
       const double mu0 = S.mu0, lam0 = S.lam0;
-      const double sec_d = R.sec_d, sec_k = R.sec_k;
+      const int law = R.law, law_ps = R.law_ps;
+  const double law_a = R.law_a, law_b = R.law_b;
       const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
       TS* eps = Fields<TS>::eps(R);
       double d2 = 0, n2 = 0;
@@ -668,14 +721,14 @@ __global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __r
           eps[N + i] = (TS)e1;
           eps[2 * N + i] = (TS)e2;
           const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
-          const double trd = dxx + dyy, tre = e0 + e1;
-          double ms = m;  // FP64 kernels only: plans with the secant law are FP64
-          if constexpr (sizeof(TS) == 8) {
-            if (sec_d != 0.0) ms = secant_mu(m, dxx, dyy, dxy, sec_d, sec_k);
-          }
-          tr[h][0] = (TC)((2 * ms * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
-          tr[h][1] = (TC)((2 * ms * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
-          tr[h][2] = (TC)(2 * ms * dxy - 2 * mu0 * e2);
+          const double tre = e0 + e1;
+          double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
+          if (sizeof(TS) == 8 && law == 1) law_sigma<1>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+          else if (sizeof(TS) == 8 && law == 2) law_sigma<2>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+          else law_sigma<0>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2);
+          tr[h][0] = (TC)(s0 - (2 * mu0 * e0 + lam0 * tre));
+          tr[h][1] = (TC)(s1 - (2 * mu0 * e1 + lam0 * tre));
+          tr[h][2] = (TC)(s2 - 2 * mu0 * e2);
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
@@ -896,7 +949,8 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
     return;
   }
   const double mu0 = S.mu0, lam0 = S.lam0;
-  const double sec_d = R.sec_d, sec_k = R.sec_k;
+  const int law = R.law, law_ps = R.law_ps;
+  const double law_a = R.law_a, law_b = R.law_b;
   const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
   double d2 = 0, n2 = 0;
   for (int y = threadIdx.x; y < NY; y += NT) {
@@ -929,12 +983,12 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
         e0 = o0; e1 = o1; e2 = o2;
       }
       const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
-      const double trd = dxx + dyy, tre = e0 + e1;
-      double ms = m;  // LAW 1: the secant law (FP64 plans; LAW 0 is the linear law)
-      if constexpr (LAW == 1) ms = secant_mu(m, dxx, dyy, dxy, sec_d, sec_k);
-      tr[h][0] = (T)((2 * ms * dxx + l * trd) - (2 * mu0 * e0 + lam0 * tre));
-      tr[h][1] = (T)((2 * ms * dyy + l * trd) - (2 * mu0 * e1 + lam0 * tre));
-      tr[h][2] = (T)(2 * ms * dxy - 2 * mu0 * e2);
+      const double tre = e0 + e1;
+      double s0, s1, s2;  // LAW 0 linear; 1 secant, 2 Rose (FP64 plans)
+      law_sigma<LAW>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+      tr[h][0] = (T)(s0 - (2 * mu0 * e0 + lam0 * tre));
+      tr[h][1] = (T)(s1 - (2 * mu0 * e1 + lam0 * tre));
+      tr[h][2] = (T)(s2 - 2 * mu0 * e2);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) lines[c * PL + py] = mk<C>(tr[0][c], tr[1][c]);
@@ -1128,7 +1182,7 @@ __global__ void ls2d_phase2_kernel(Ls2dState* st, const int* sel, int nsel, Ls2d
 // Outputs in the reference layout: eps, sig (nx,ny,2,2) and partial sums of
 // their components for the means (linear_elastic_simulator.py:83-88).
 // grid = (G, nsel).
-template <int LAW = 0>  // 1: the secant law
+template <int LAW = 0>  // 1: the secant law, 2: the Rose law
 __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
   const int r = sel[blockIdx.y];
@@ -1138,7 +1192,8 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
   const double abar = S.abar;
   double* eps_out = R.out_eps;
   double* sig_out = R.out_sig;
-  const double sec_d = R.sec_d, sec_k = R.sec_k;
+  const int law_ps = R.law_ps;
+  const double law_a = R.law_a, law_b = R.law_b;
   double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
@@ -1152,10 +1207,19 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
     const double lam = R.lam[i];
     const double dxx = exx - pxx, dxy = exy - pxy, dyx = eyx - pyx, dyy = eyy - pyy;
     double mu = R.mu[i];
-    if constexpr (LAW == 1) mu = secant_mu(mu, dxx, dyy, 0.5 * (dxy + dyx), sec_d, sec_k);
-    const double tr = dxx + dyy;
-    const double sxx = 2 * mu * dxx + lam * tr, syy = 2 * mu * dyy + lam * tr;
-    const double sxy2 = 2 * mu * dxy, syx2 = 2 * mu * dyx;
+    double sxx, syy, sxy2, syx2;
+    if constexpr (LAW == 2) {
+      // Rose: sigma_yx is a copy of sigma_xy, from the [0,1] strain entry
+      law_sigma<2>(mu, lam, dxx, dyy, dxy, law_a, law_b, law_ps, sxx, syy, sxy2);
+      syx2 = sxy2;
+    } else {
+      if constexpr (LAW == 1) mu = secant_mu(mu, dxx, dyy, 0.5 * (dxy + dyx), law_a, law_b);
+      const double tr = dxx + dyy;
+      sxx = 2 * mu * dxx + lam * tr;
+      syy = 2 * mu * dyy + lam * tr;
+      sxy2 = 2 * mu * dxy;
+      syx2 = 2 * mu * dyx;
+    }
     if (eps_out) reinterpret_cast<double4*>(eps_out)[i] = make_double4(exx, exy, eyx, eyy);
     if (sig_out) reinterpret_cast<double4*>(sig_out)[i] = make_double4(sxx, sxy2, syx2, syy);
     s[0] += exx; s[1] += exy; s[2] += eyx; s[3] += eyy;
@@ -1202,7 +1266,9 @@ struct mgk_ls2d_plan {
   size_t row_smem32 = 0, col_smem32 = 0;  // FP32 iteration kernels
   int fast = 0;                           // kernel family in use: 0 CTA-wide passes, 256/512/1024 warp-line
   int fast_nat = 0;                       // smallest warp-line family that covers every side (0: none)
-  int law = 0;                            // 1: secant degradation law (mgk_ls2d_set_secant)
+  int law = 0;                            // 1: secant degradation law, 2: Rose law
+  double law_a = 0, law_b = 0;            // the law's parameters (set_secant, set_rose)
+  int law_ps = 0;
   std::vector<int> tc_gen;                // column tiles of the CTA-wide family, per replica
   std::vector<Ls2dRep> reps;      // host copy (static part)
   std::vector<char> has_material;
@@ -1259,10 +1325,14 @@ static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
 template <typename TS, bool IN_SPEC, bool FINAL>
 static void* row_fast_fn(int fast, int law = 0) {
   if constexpr (sizeof(TS) == 8) {
-    if (law)  // the secant law (FP64 plans only)
+    if (law == 1)  // the secant law (FP64 plans only)
       return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL, 1>
              : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL, 1>
                           : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL, 1>;
+    if (law == 2)  // the Rose law (FP64 plans only)
+      return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL, 2>
+             : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL, 2>
+                          : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL, 2>;
   }
   return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL>
          : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL>
@@ -1277,10 +1347,12 @@ static void* col_fast_fn(int fast) {
 
 template <typename T>
 static int ls2d_set_fast_attrs(int fast, size_t row_smem, size_t col_smem) {
-  void* fns[8] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
-                  row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast),
-                  row_fast_fn<T, true, true>(fast, 1), row_fast_fn<T, false, true>(fast, 1),
-                  row_fast_fn<T, true, false>(fast, 1), row_fast_fn<T, false, false>(fast, 1)};
+  void* fns[12] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
+                   row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast),
+                   row_fast_fn<T, true, true>(fast, 1), row_fast_fn<T, false, true>(fast, 1),
+                   row_fast_fn<T, true, false>(fast, 1), row_fast_fn<T, false, false>(fast, 1),
+                   row_fast_fn<T, true, true>(fast, 2), row_fast_fn<T, false, true>(fast, 2),
+                   row_fast_fn<T, true, false>(fast, 2), row_fast_fn<T, false, false>(fast, 2)};
   for (void* f : fns) MGK_CUDA(raise_smem((const void*)f, (int)row_smem));
   MGK_CUDA(raise_smem((const void*)col_fast_fn<T>(fast), (int)col_smem));
   return MGK_OK;
@@ -1519,7 +1591,7 @@ static int ls2d_set_fields(mgk_ls2d_t p, int rep, const double* E, const double*
   MGK_CUDA(cudaGetLastError());
   if (set_moduli) {
     ls2d_medium_kernel<<<1, kThreads, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, grid, p->plane_mode,
-                                              set_moduli == 2 ? 1 : 0);
+                                              set_moduli == 2 ? (p->law == 2 ? 2 : 1) : 0, p->law_b);
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
@@ -1548,14 +1620,12 @@ extern "C" int mgk_ls2d_set_lame_rep(mgk_ls2d_t p, int rep, const double* lam, c
   return st;
 }
 
-extern "C" int mgk_ls2d_set_secant(mgk_ls2d_t p, double d, double k) {
-  MGK_REQUIRE(p, "mgk_ls2d_set_secant: null plan");
-  MGK_REQUIRE(d >= 0.0 && d <= 1.0 && k >= 0.0 && isfinite(k), "mgk_ls2d_set_secant: need 0 <= d <= 1, k >= 0");
-  MGK_REQUIRE(d == 0.0 || p->prec == MGK_FP64, "mgk_ls2d_set_secant: the secant law runs in FP64 plans only");
-  for (auto& R : p->reps) { R.sec_d = d; R.sec_k = k; }
-  const int law = d != 0.0 ? 1 : 0;
+// switches every replica of the plan to law (a, b, ps); cached loop graphs
+// hold the previous law's row kernel and are dropped
+static int ls2d_set_law(mgk_ls2d_t p, int law, double a, double b, int ps) {
+  for (auto& R : p->reps) { R.law = law; R.law_a = a; R.law_b = b; R.law_ps = ps; }
+  p->law_a = a; p->law_b = b; p->law_ps = ps;
   if (law != p->law) {
-    // cached loop graphs hold the other law's row kernel
     for (auto& e : p->gcache) {
       cudaGraphExecDestroy(e.x);
       cudaGraphDestroy(e.g);
@@ -1568,6 +1638,21 @@ extern "C" int mgk_ls2d_set_secant(mgk_ls2d_t p, double d, double k) {
     p->law = law;
   }
   return MGK_OK;
+}
+
+extern "C" int mgk_ls2d_set_secant(mgk_ls2d_t p, double d, double k) {
+  MGK_REQUIRE(p, "mgk_ls2d_set_secant: null plan");
+  MGK_REQUIRE(d >= 0.0 && d <= 1.0 && k >= 0.0 && isfinite(k), "mgk_ls2d_set_secant: need 0 <= d <= 1, k >= 0");
+  MGK_REQUIRE(d == 0.0 || p->prec == MGK_FP64, "mgk_ls2d_set_secant: the secant law runs in FP64 plans only");
+  return ls2d_set_law(p, d != 0.0 ? 1 : 0, d, k, 0);
+}
+
+extern "C" int mgk_ls2d_set_rose(mgk_ls2d_t p, double eta, double floor_fraction, int plane_stress) {
+  MGK_REQUIRE(p, "mgk_ls2d_set_rose: null plan");
+  MGK_REQUIRE(eta >= 0.0 && isfinite(eta) && floor_fraction >= 0.0 && floor_fraction <= 1.0,
+              "mgk_ls2d_set_rose: need eta >= 0, 0 <= floor_fraction <= 1");
+  MGK_REQUIRE(p->prec == MGK_FP64, "mgk_ls2d_set_rose: the Rose law runs in FP64 plans only");
+  return ls2d_set_law(p, 2, eta, floor_fraction, plane_stress ? 1 : 0);
 }
 
 extern "C" int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t p, int rep, const double* epsp, mgk_stream_t stream) {
@@ -1599,7 +1684,7 @@ struct LoopArgs {
   int stage_bytes;
   size_t tma_smem;
   int fast;           // warp-line iteration kernels
-  int law = 0;        // constitutive law of the warp-line row kernel (1: secant)
+  int law = 0;        // constitutive law of the warp-line row kernel (1: secant, 2: Rose)
 };
 
 template <typename TS, bool IN_SPEC, bool FINAL>
@@ -1889,6 +1974,11 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     const int r = sel ? sel[q] : q;
     MGK_REQUIRE(r >= 0 && r < p->nrep && !seen[r], "mgk_ls2d_solve_batch: bad or repeated replica index");
     MGK_REQUIRE(p->has_material[r], "mgk_ls2d_solve: replica %d has no material (call set_material)", r);
+    // the Rose law reads the [0,1] strain entry; the symmetric storage carries it
+    // when macro strain and eigenstrain are symmetric (the eigenstrain is the
+    // caller's to keep symmetric)
+    MGK_REQUIRE(p->law != 2 || eps_bar[4 * q + 1] == eps_bar[4 * q + 2],
+                "mgk_ls2d_solve: the Rose law needs a symmetric macro strain");
     seen[r] = 1;
     selv[q] = r;
   }
@@ -2018,7 +2108,8 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
       }
     }
   }
-  if (p->law) ls2d_output_kernel<1><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  if (p->law == 1) ls2d_output_kernel<1><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  else if (p->law == 2) ls2d_output_kernel<2><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   else ls2d_output_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());
   ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 8,
@@ -2316,7 +2407,7 @@ extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const doub
   const int G = grid_blocks(N);
   ls2d_material_kernel<<<G, kThreads, 0, s>>>(d_rep, 0, E, nu, eps_plastic, plane_mode, 1, part);
   MGK_CUDA(cudaGetLastError());
-  ls2d_medium_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, 0, part, G, plane_mode, 0);
+  ls2d_medium_kernel<<<1, kThreads, 0, s>>>(d_rep, d_st, 0, part, G, plane_mode, 0, 0.0);
   MGK_CUDA(cudaGetLastError());
   if (eps_init) {
     ls2d_means_kernel<<<dim3(G, 1), kThreads, 0, s>>>(d_rep, d_sel, part);

@@ -83,6 +83,12 @@ class Ls2dBatch:
         """Secant degradation law for every replica (d = 0: linear); FP64 plans."""
         L.check(L.lib().mgk_ls2d_set_secant(self._h, float(d), float(k)), "mgk_ls2d_set_secant")
 
+    def set_rose(self, eta, mu_floor_fraction=0.1, plane_mode="plane_strain"):
+        """Rose secant-modulus law for every replica; call before set_lame (the
+        reference medium depends on the floor); FP64 plans."""
+        L.check(L.lib().mgk_ls2d_set_rose(self._h, float(eta), float(mu_floor_fraction),
+                                          1 if plane_mode == "plane_stress" else 0), "mgk_ls2d_set_rose")
+
     def solve(self, reps, eps_bars, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True,
               stream=None):
         """Solve replicas ``reps`` (one launch per stage for all of them).
@@ -240,6 +246,47 @@ def spectral_solver_secant_2d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
                    max_iter=max_iter, tol=tol)[0]
     if verbose:
         print(f"secant LS 2D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
+    eps_np = eps.cpu().numpy()
+    sig_np = sig.cpu().numpy()
+    return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
+
+
+_PLANS_ROSE = {}
+
+
+def spectral_solver_rose_2d(lam, mu, eta, mu_floor_fraction=0.1, eps_bar=None, eps_plastic=None, max_iter=400,
+                            tol=1e-6, verbose=False, pixel=1.0, plane_mode="plane_strain", Gamma=None,
+                            eps_init=None):
+    """Nonlinear 2D Lippmann-Schwinger solve with the Rose secant-modulus law
+    (linear_elastic_simulator.py:852-950): G = max(mu exp(-eta eps_eq),
+    floor mu) at constant bulk modulus, reference medium (mean lam,
+    (mean mu + floor mean mu) / 2).  ``lam`` is the 3D Lame lambda (plane
+    stress is reduced per voxel, as in the reference).  Macro strain,
+    eigenstrain and warm start must be symmetric (the strain's [0,1] entry
+    drives the law).  Returns (eps, sig, eps.mean(axis=(0,1)),
+    sig.mean(axis=(0,1)))."""
+    torch = _torch()
+    lam = np.array(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
+    mu = np.array(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
+    eps_bar = np.asarray(eps_bar, dtype=np.float64)
+    for a in (eps_bar, eps_plastic, eps_init):
+        if a is not None and not np.array_equal(np.asarray(a)[..., 0, 1], np.asarray(a)[..., 1, 0]):
+            raise NotImplementedError("spectral_solver_rose_2d: asymmetric strain tensors are not supported")
+    nx, ny = lam.shape
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (nx, ny, dev.index)
+    p = _PLANS_ROSE.get(key)
+    if p is None:
+        p = _PLANS_ROSE[key] = Ls2dBatch([(nx, ny)])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    eps = torch.empty((nx, ny, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    p.set_rose(eta, mu_floor_fraction, plane_mode)
+    p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
+    info = p.solve([0], [eps_bar], [eps], [sig], eps_init=None if eps_init is None else [t(eps_init)],
+                   max_iter=max_iter, tol=tol)[0]
+    if verbose:
+        print(f"Rose LS 2D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
     eps_np = eps.cpu().numpy()
     sig_np = sig.cpu().numpy()
     return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))

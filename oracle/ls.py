@@ -7,6 +7,7 @@ Follows mgkmc/linear_elastic_simulator.py:
   * ``spectral_solver_3d``  -- :274-376
   * ``spectral_solver_secant_2d`` -- :614-765 (secant degradation law,
     elasticity.py:112-150, :189-260)
+  * ``spectral_solver_rose_2d`` -- :852-950 (Rose law, elasticity.py:868-944)
   * ``mixed_bc_solve_2d``   -- the macro mixed stress/strain loop of
     ``linear_elastic_simulation_2d`` :176-197 with the compliance correction of
     :150-152, here with an eigenstrain field (the reference driver has no
@@ -171,6 +172,71 @@ def spectral_solver_secant_2d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
         if diff < tol:
             break
     sig_out = secant_stress_2d(eps - ep if ep is not None else eps, lam, mu, d, k)
+    out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
+    return out + (it_done, diff) if return_info else out
+
+
+def rose_stress_2d(e, lam, mu, eta, floor_f=0.1, plane_mode="plane_strain"):
+    """Rose secant-modulus stress (mgkmc/elasticity.py:868-944): G = max(mu
+    exp(-eta eq), floor mu), K = lam + 2 mu / 3 kept; plane stress: eps_zz by
+    five fixed-point steps; sigma_yx copied from sigma_xy."""
+    exx, eyy, exy = e[..., 0, 0], e[..., 1, 1], e[..., 0, 1]
+    K = lam + (2.0 / 3.0) * mu
+
+    def eq_of(ezz):
+        tr3 = (exx + eyy + ezz) / 3.0
+        return np.sqrt((2.0 / 3.0) * ((exx - tr3) ** 2 + (eyy - tr3) ** 2 + (ezz - tr3) ** 2 + 2.0 * exy ** 2))
+
+    def g_of(eq):
+        return np.maximum(mu * np.exp(-eta * eq), floor_f * mu)
+
+    ezz = np.zeros_like(exx)
+    if plane_mode == "plane_stress":
+        ezz = -lam / (lam + 2.0 * mu) * (exx + eyy)
+        for _ in range(5):
+            g = g_of(eq_of(ezz))
+            ezz = -((3.0 * K - 2.0 * g) / (3.0 * K + 4.0 * g)) * (exx + eyy)
+    G = g_of(eq_of(ezz))
+    tr = exx + eyy + ezz
+    le = K - (2.0 / 3.0) * G
+    sig = np.zeros_like(e)
+    sig[..., 0, 0] = le * tr + 2.0 * G * exx
+    sig[..., 1, 1] = le * tr + 2.0 * G * eyy
+    sig[..., 0, 1] = 2.0 * G * exy
+    sig[..., 1, 0] = sig[..., 0, 1]
+    return sig
+
+
+def spectral_solver_rose_2d(lam, mu, eta, floor_f, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
+                            plane_mode="plane_strain", eps_init=None, return_info=False):
+    """Rose-law LS fixed point (mgkmc/linear_elastic_simulator.py:852-950):
+    reference medium (mean lam, (mean mu + floor mean mu) / 2)."""
+    lam0 = float(np.mean(lam))
+    mu_avg = float(np.mean(mu))
+    mu0 = 0.5 * (mu_avg + floor_f * mu_avg)
+    shape = np.shape(lam)
+    axes = (0, 1)
+    G = green_operator(wave_vectors(shape, pixel), lam0, mu0)
+    if eps_init is not None:
+        eps = eps_init.copy()
+        eps += eps_bar - eps_init.mean(axis=axes)
+    else:
+        eps = np.broadcast_to(eps_bar, shape + (2, 2)).copy()
+    ep = eps_plastic
+    it_done, diff = 0, np.inf
+    for it in range(max_iter):
+        sig = rose_stress_2d(eps - ep if ep is not None else eps, lam, mu, eta, floor_f, plane_mode)
+        tau = sig - hooke(eps, lam0, mu0, 2)
+        tau_hat = np.fft.fftn(tau, axes=axes, norm="ortho")
+        et = np.fft.ifftn(-np.einsum("xykhij,xyij->xykh", G, tau_hat), axes=axes, norm="ortho").real
+        et -= et.mean(axis=axes)
+        eps_new = eps_bar + et
+        diff = np.linalg.norm(eps_new - eps) / (np.linalg.norm(eps) + 1e-20)
+        eps = eps_new
+        it_done = it + 1
+        if diff < tol:
+            break
+    sig_out = rose_stress_2d(eps - ep if ep is not None else eps, lam, mu, eta, floor_f, plane_mode)
     out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
     return out + (it_done, diff) if return_info else out
 

@@ -258,6 +258,24 @@ def ls2d_secant_fixtures():
     save("ls2d_secant_24x16", **out)
 
 
+def ls2d_rose_fixtures():
+    """The reference's Rose-law LS solver (spectral_solver_rose_2d), plane
+    strain and plane stress, with the 3D Lame lambda as its KMC driver passes."""
+    rng = np.random.default_rng(62)
+    nx, ny = 16, 24
+    E, nu = W.ls2d_material(nx, ny, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    ep = W.pure_shear_eigenstrain_2d(nx, ny, rng, frac=0.1)
+    eb = np.array([[0.02, 0.003], [0.003, -0.004]])
+    out = dict(lam=lam, mu=mu, eps_plastic=ep, eps_bar=eb)
+    for tag, eta, fl, pm in (("ps", 30.0, 0.1, "plane_strain"), ("pst", 60.0, 0.2, "plane_stress")):
+        e, s, em, sm = LES.spectral_solver_rose_2d(lam, mu, eta, fl, eps_bar=eb, eps_plastic=ep, max_iter=500,
+                                                   tol=1e-12, plane_mode=pm)
+        out.update({f"eps_{tag}": e, f"sig_{tag}": s, f"eta_{tag}": eta, f"floor_{tag}": fl})
+    save("ls2d_rose_16x24", **out)
+
+
 if __name__ == "__main__":
     ls2d_fixtures()
     ls3d_fixtures()
@@ -265,3 +283,4 @@ if __name__ == "__main__":
     kmc3d_fixtures()
     fs3d_fixtures()
     ls2d_secant_fixtures()
+    ls2d_rose_fixtures()

@@ -164,3 +164,36 @@ def test_secant_d0_is_linear_and_mixed_refused(les):
     b = les.Ls2dBatch([(64, 64)], precision="mixed")
     with pytest.raises(L.MgkError):
         b.set_secant(0.5, 10.0)
+
+
+@pytest.mark.parametrize("tag,pm", [("ps", "plane_strain"), ("pst", "plane_stress")])
+def test_golden_rose(les, golden, tag, pm):
+    # Rose law (CTA-wide kernels at 16 x 24) against the reference
+    g = golden("ls2d_rose_16x24")
+    eps, sig, _, _ = les.spectral_solver_rose_2d(g["lam"], g["mu"], float(g[f"eta_{tag}"]), float(g[f"floor_{tag}"]),
+                                                 g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-12,
+                                                 plane_mode=pm)
+    assert rel(eps, g[f"eps_{tag}"]) < TOL
+    assert rel(sig, g[f"sig_{tag}"]) < TOL
+
+
+@pytest.mark.parametrize("nx,ny,eta,fl,pm", [(64, 64, 30.0, 0.1, "plane_strain"), (256, 128, 60.0, 0.2, "plane_stress"),
+                                             (96, 192, 100.0, 0.3, "plane_strain")])
+def test_rose_against_oracle(les, nx, ny, eta, fl, pm):
+    # warp-line kernels with the Rose law, against the oracle
+    E, nu, ep, _ = W.ls2d_problem(nx, ny, seed=13)
+    eb = np.array([[0.025, 0.002], [0.002, -0.008]])
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eps, sig, _, _ = les.spectral_solver_rose_2d(lam, mu, eta, fl, eb, ep, max_iter=500, tol=1e-11, plane_mode=pm)
+    o = OL.spectral_solver_rose_2d(lam, mu, eta, fl, eb, ep, max_iter=500, tol=1e-11, plane_mode=pm)
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
+def test_rose_refuses_asymmetric_strain(les):
+    E, nu, ep, _ = W.ls2d_problem(64, 64, seed=13)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_rose_2d(lam, mu, 30.0, 0.1, np.array([[0.01, 0.002], [0.0, 0.0]]), ep)

@@ -57,6 +57,17 @@ def test_ls2d_secant_warm(golden):
     assert rel(sig, g["sig_warm"]) < 1e-12
 
 
+@pytest.mark.parametrize("tag,pm", [("ps", "plane_strain"), ("pst", "plane_stress")])
+def test_ls2d_rose(golden, tag, pm):
+    # the Rose-law LS restatement against the reference's solver
+    g = golden("ls2d_rose_16x24")
+    eps, sig, _, _ = OL.spectral_solver_rose_2d(g["lam"], g["mu"], float(g[f"eta_{tag}"]), float(g[f"floor_{tag}"]),
+                                                g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-12,
+                                                plane_mode=pm)
+    assert rel(eps, g[f"eps_{tag}"]) < 1e-12
+    assert rel(sig, g[f"sig_{tag}"]) < 1e-12
+
+
 def test_ls2d_macro_loop(golden):
     g = golden("ls2d_macro_16")
     E, nu, mask, target = g["E"], g["nu"], g["mask"], g["target"]
