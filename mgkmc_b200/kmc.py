@@ -42,7 +42,8 @@ class Kmc2D:
     def __init__(self, E, nu, catalog, Q0, gamma0=0.1, T=300.0, nu0=1e13, strain_rate=1e7, step_size=1e-5,
                  q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0, stress_targets=None, mixed_tol=1e4,
                  mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200, q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0,
-                 selection="exact", ls_start="cold", precision="fp64", ls=None, rep=0, stream=None):
+                 selection="exact", ls_start="cold", precision="fp64", ls=None, rep=0, stream=None,
+                 cascade_mode=False, stability_threshold=0.0, max_cascade_steps_pct=0.3):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("mgkmc_b200 needs a CUDA device (no CPU fallback)")
@@ -55,6 +56,15 @@ class Kmc2D:
                       ls_max_iter=ls_max_iter, q_mean=q_mean, q_std=q_std, q_min=q_min, volume=volume)
         self.stress_targets = {(1, 1): 0.0} if stress_targets is None else dict(stress_targets)
         self.selection = selection
+        # cascade mode (kmc_simulator.py:876-889, _run_cascade :577-794): flips of
+        # unstable modes in batches; its rates keep only q > 0 modes, which the
+        # exact (compacting) rate path provides
+        if cascade_mode and selection != "exact":
+            raise ValueError("cascade mode uses the exact selection (compacted rates)")
+        self.cascade_mode = bool(cascade_mode)
+        self.stability_threshold = float(stability_threshold)
+        self.max_cascade_limit = int(max_cascade_steps_pct * self.nx * self.ny)
+        self.cascade_flips = []
         self.ls_start = ls_start
         self.tau = 1.0 / (nu0 * np.exp(-q_act_temp / (KB * T))) if T > 0 else np.inf
         f64 = torch.float64
@@ -149,9 +159,10 @@ class Kmc2D:
             L.check(lib.mgk_kmc2d_barrier(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0), L.ptr(self.sig),
                                           L.ptr(self.catalog), p["volume"], L.ptr(self.soft), L.ptr(self.t_last),
                                           self.time, L.ptr(self.prev), p["cap"], 0, self.tau, S), "mgk_kmc2d_barrier")
-            L.check(lib.mgk_kmc2d_rates(self.nx, self.ny, self.M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"], 0,
-                                        L.ptr(self.rates), L.ptr(self.indices), L.ptr(self.prefix), L.ptr(self.count),
-                                        L.ptr(self.total), L.ptr(self.work), S), "mgk_kmc2d_rates")
+            L.check(lib.mgk_kmc2d_rates(self.nx, self.ny, self.M, L.ptr(self.Q), 1.0, None, p["T"], p["nu0"],
+                                        1 if self.cascade_mode else 0, L.ptr(self.rates), L.ptr(self.indices),
+                                        L.ptr(self.prefix), L.ptr(self.count), L.ptr(self.total), L.ptr(self.work),
+                                        S), "mgk_kmc2d_rates")
             self.total_h.copy_(self.total, non_blocking=True)
         else:
             L.check(lib.mgk_kmc2d_barrier_total(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0),
@@ -187,13 +198,70 @@ class Kmc2D:
                                    L.ptr(self.sel), S), "mgk_kmc_select")
         nc = L.ptr(self.redraw)
         nq = L.c_void_p(self.redraw.data_ptr() + 4 * M * 8)
-        L.check(lib.mgk_kmc2d_event(self.nx, self.ny, M, L.ptr(self.sel), None, L.ptr(self.eps_p), L.ptr(self.soft),
+        # compacted rates (cascade mode) map the selected position to its mode
+        ind = L.ptr(self.indices) if self.cascade_mode else None
+        L.check(lib.mgk_kmc2d_event(self.nx, self.ny, M, L.ptr(self.sel), ind, L.ptr(self.eps_p), L.ptr(self.soft),
                                     L.ptr(self.t_last), L.ptr(self.catalog), L.ptr(self.Q0), L.ptr(self.prev), nc, nq,
                                     self.time, p["jp"], p["jt"], p["cap"], p["jn"], L.ptr(self.xym), S),
                 "mgk_kmc2d_event")
         L.check(lib.mgk_ls2d_sync_voxel(self.ls._h, self.rep, L.ptr(self.eps_p), L.ptr(self.xym), S),
                 "mgk_ls2d_sync_voxel")
         self.xym_h.copy_(self.xym, non_blocking=True)
+
+    # ------------------------------------------------------------ cascade ---
+    def launch_barriers(self):
+        lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
+        L.check(lib.mgk_kmc2d_barrier(self.nx, self.ny, self.M, L.ptr(self.Q), L.ptr(self.Q0), L.ptr(self.sig),
+                                      L.ptr(self.catalog), p["volume"], L.ptr(self.soft), L.ptr(self.t_last),
+                                      self.time, L.ptr(self.prev), p["cap"], 0, self.tau, S), "mgk_kmc2d_barrier")
+
+    def unstable_batch(self):
+        """The modes of one cascade batch (kmc_simulator.py:578-600,
+        find_unstable_2d :162-181): modes with Q < threshold in (x, y, m)
+        order, sorted by Q ascending, the first of each voxel.  Reads the
+        barriers (call after the stream has completed them)."""
+        with self.torch.cuda.stream(self.stream):
+            Qf = self.Q.reshape(-1)
+            flat = self.torch.nonzero(Qf < self.stability_threshold).flatten()
+            q = Qf[flat].cpu().numpy()
+            flat = flat.cpu().numpy()
+        if flat.size == 0:
+            return []
+        order = flat[np.argsort(q)]
+        seen, batch = set(), []
+        for f in order:
+            v = int(f) // self.M
+            if v not in seen:
+                seen.add(v)
+                batch.append(int(f))
+        return batch
+
+    def cascade_flips_batch(self, batch, rng):
+        """Flips the batch's modes in order, each with the bookkeeping and
+        redraws of a KMC event (kmc_simulator.py:728-760)."""
+        lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
+        M, k = self.M, len(batch)
+        torch = self.torch
+        sel_h = torch.tensor(batch, dtype=torch.int64).pin_memory()
+        red_h = torch.empty((k, 5 * M), dtype=torch.float64).pin_memory()
+        for i in range(k):
+            theta = rng.uniform(0.0, np.pi, M)
+            q0 = np.clip(rng.normal(p["q_mean"], p["q_std"], M), p["q_min"], None)
+            red_h[i, :4 * M] = torch.from_numpy(pure_shear_modes(theta, p["gamma0"]).reshape(-1))
+            red_h[i, 4 * M:] = torch.from_numpy(q0)
+        with torch.cuda.stream(self.stream):
+            sel_d = sel_h.to(self.dev, non_blocking=True)
+            red_d = red_h.to(self.dev, non_blocking=True)
+        self._keep_batch = (sel_h, red_h, sel_d, red_d)  # alive until the stream has used them
+        for i in range(k):
+            nc = L.c_void_p(red_d.data_ptr() + i * 5 * M * 8)
+            nq = L.c_void_p(red_d.data_ptr() + (i * 5 * M + 4 * M) * 8)
+            L.check(lib.mgk_kmc2d_event(self.nx, self.ny, M, L.c_void_p(sel_d.data_ptr() + 8 * i), None,
+                                        L.ptr(self.eps_p), L.ptr(self.soft), L.ptr(self.t_last),
+                                        L.ptr(self.catalog), L.ptr(self.Q0), L.ptr(self.prev), nc, nq, self.time,
+                                        p["jp"], p["jt"], p["cap"], p["jn"], L.ptr(self.xym), S), "mgk_kmc2d_event")
+            L.check(lib.mgk_ls2d_sync_voxel(self.ls._h, self.rep, L.ptr(self.eps_p), L.ptr(self.xym), S),
+                    "mgk_ls2d_sync_voxel")
 
     # ---------------------------------------------------------------- run ---
     def trajectory(self, rng, n_steps, max_events=None):
@@ -210,9 +278,38 @@ class Kmc2D:
         remaining = 0.0
         steps_done = 0
         M = self.M
+        cascade_count = 0
+        n_batches = 0
         while steps_done < n_steps:
             remaining += dt_step
             while remaining > 0:
+                if self.cascade_mode:
+                    self.launch_barriers()
+                    yield ("sync",)
+                    batch = self.unstable_batch()
+                    if batch:
+                        # _run_cascade: batches until no mode is unstable
+                        local_step = flips = 0
+                        while batch:
+                            self.cascade_flips_batch(batch, rng)
+                            for f in batch:
+                                x, y, m = f // (self.ny * M), (f // M) % self.ny, f % M
+                                self.cascade_flips.append((x, y, m, self.time, n_batches))
+                            self.after_solve((yield ("solve",)))
+                            n_batches += 1
+                            flips += len(batch)
+                            local_step += 1
+                            if local_step > self.nx * self.ny:
+                                break
+                            self.launch_barriers()
+                            yield ("sync",)
+                            batch = self.unstable_batch()
+                        if flips > 0:
+                            cascade_count += 1
+                        if cascade_count > self.max_cascade_limit:
+                            return self.result(steps_done)
+                        continue
+                    cascade_count = 0
                 self.launch_rates()
                 yield ("sync",)
                 total = float(self.total_h[0])
@@ -281,4 +378,5 @@ class Kmc2D:
 
     def result(self, steps):
         return dict(events=list(self.events), eps_macro=self.eps_macro.copy(), sig=self.sig.cpu().numpy(),
-                    eps_p=self.eps_p.cpu().numpy(), time=self.time, steps=steps, solves=self.n_solves)
+                    eps_p=self.eps_p.cpu().numpy(), time=self.time, steps=steps, solves=self.n_solves,
+                    cascade_flips=list(self.cascade_flips))

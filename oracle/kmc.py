@@ -180,3 +180,11 @@ def apply_flip_3d(eps_p, soft, t_last, catalog, x, y, z, m, t, jp, jt, gmax, jn)
                         g = gmax
                     soft[a, b, cc, 0] = g
                     soft[a, b, cc, 1] = soft[a, b, cc, 1] + jn * jt * s
+
+
+def find_unstable_2d(Q, threshold=0.0):
+    """(x, y, m) rows of the modes with Q < threshold, in (x, y, m) order
+    (mgkmc/kmc_simulator_functions.py:162-181)."""
+    nx, ny, M = Q.shape
+    flat = np.flatnonzero(Q.reshape(-1) < threshold)
+    return np.stack([flat // (ny * M), (flat // M) % ny, flat % M], axis=1).astype(np.int64)

@@ -4,8 +4,14 @@ TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 
 Follows KmcSimulation2D.run_simulation (mgkmc/kmc_simulator.py:796-1157) on
 the path the benchmark exercises: small-strain linear elasticity, KMC mode
-(cascade off), no thermal conduction, no fast patching, redraw of both
-directions and barriers after a flip.  Per event: update_barriers (:874 ->
+(cascade off, or on: ``cascade_mode``), no thermal conduction, no fast
+patching, redraw of both directions and barriers after a flip.  Cascade mode
+(:876-889, _run_cascade :577-794, linear small-strain branch :728-784):
+after each barrier update, while modes with Q < stability_threshold exist,
+flip in one batch the most unstable mode of each voxel that has one (modes
+sorted by Q ascending, first per voxel), each with the flip bookkeeping and
+redraws of a KMC event, then one LS re-solve; rates then use only modes with
+q > 0 (compute_rates_2d cascade_mode=True).  Per event: update_barriers (:874 ->
 compute_barrier_2d), compute_rates_2d (:891), the waiting time (:893), the
 clock/strain advance (:895-898), selection + decode (:899-900), the flip and
 its bookkeeping (:1025-1042), and a cold-started LS re-solve (:1076, which
@@ -16,8 +22,9 @@ raises ValueError.
 Draws come from an explicit numpy Generator in a fixed order instead of the
 reference's two global streams (numpy for t_wait and redraws, numba's for
 selection): per attempt u_wait; per event u_sel, then M orientations
-theta ~ U[0, pi) and M barriers N(q_mean, q_std) clipped below at q_min.  The
-GPU driver consumes the same draws in the same order.
+theta ~ U[0, pi) and M barriers N(q_mean, q_std) clipped below at q_min; per
+cascade flip (in batch order) the same M + M redraws.  The GPU driver
+consumes the same draws in the same order.
 """
 import numpy as np
 
@@ -38,7 +45,8 @@ def pure_shear_modes(theta, gamma0):
 def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=300.0, nu0=1e13,
               strain_rate=1e7, step_size=1e-5, q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0,
               stress_targets=None, mixed_tol=1e4, mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200,
-              q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0):
+              q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0, cascade_mode=False, stability_threshold=0.0,
+              max_cascade_steps_pct=0.3):
     nx, ny, M = Q0.shape
     stress_targets = {(1, 1): 0.0} if stress_targets is None else stress_targets
     catalog = catalog.copy()
@@ -61,7 +69,22 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
 
     sig, sigM = elastic_run()
     events = []
+    cascade_flips = []  # (x, y, m, time, batch)
     n_solves = 1
+    max_cascade_limit = int(max_cascade_steps_pct * nx * ny)  # kmc_simulator.py:815
+    cascade_count = 0
+    n_batches = 0
+
+    def result():
+        return dict(events=events, eps_macro=eps_macro, sig=sig, eps_p=eps_p, time=time, steps=steps_done,
+                    solves=n_solves, catalog=catalog, Q0=Q0, cascade_flips=cascade_flips)
+
+    def flip(x, y, m):
+        C = catalog[x, y, m].copy()
+        OK.apply_flip_2d(eps_p, soft, t_last, catalog, x, y, m, time, jp, jt, cap, jn)
+        prev[x, y] = C
+        catalog[x, y] = pure_shear_modes(rng.uniform(0.0, np.pi, M), gamma0)
+        Q0[x, y] = np.clip(rng.normal(q_mean, q_std, M), q_min, None)
     strain_unit = np.zeros((2, 2))
     strain_unit[0, 0] = 1.0
     dt_step = abs(step_size) / strain_rate if strain_rate > 0 else 1.0
@@ -71,7 +94,39 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
         remaining += dt_step
         while remaining > 0:
             OK.compute_barrier(Q, Q0, sig, catalog, volume, soft, t_last, time, prev, cap, 0, tau)
-            rates, indices, total = OK.compute_rates(Q, 1.0, T, nu0, cascade_mode=False)
+            if cascade_mode and np.any(Q < stability_threshold):
+                # _run_cascade: batches until no mode is unstable
+                local_step, flips = 0, 0
+                while True:
+                    OK.compute_barrier(Q, Q0, sig, catalog, volume, soft, t_last, time, prev, cap, 0, tau)
+                    uns = OK.find_unstable_2d(Q, stability_threshold)  # (x, y, m) order
+                    if len(uns) == 0:
+                        break
+                    flat = (uns[:, 0] * ny + uns[:, 1]) * M + uns[:, 2]
+                    order = flat[np.argsort(Q.reshape(-1)[flat])]
+                    seen, batch = set(), []
+                    for f in order:
+                        v = int(f) // M
+                        if v not in seen:
+                            seen.add(v)
+                            batch.append(OK.decode_index_2d(int(f), ny, M))
+                    for (x, y, m) in batch:
+                        flip(x, y, m)
+                        cascade_flips.append((x, y, m, time, n_batches))
+                    sig, sigM = elastic_run()
+                    n_solves += 1
+                    n_batches += 1
+                    flips += len(batch)
+                    local_step += 1
+                    if local_step > nx * ny:
+                        break
+                if flips > 0:
+                    cascade_count += 1
+                if cascade_count > max_cascade_limit:
+                    return result()
+                continue
+            cascade_count = 0
+            rates, indices, total = OK.compute_rates(Q, 1.0, T, nu0, cascade_mode=cascade_mode)
             if total > 0:
                 u = rng.random()
                 t_wait = -np.log(u) / total
@@ -81,17 +136,12 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
                     remaining -= t_wait
                     k = OK.select_event(rates, total, rng.random())
                     x, y, m = OK.decode_index_2d(int(indices[k]), ny, M)
-                    C = catalog[x, y, m].copy()
-                    OK.apply_flip_2d(eps_p, soft, t_last, catalog, x, y, m, time, jp, jt, cap, jn)
-                    prev[x, y] = C
-                    catalog[x, y] = pure_shear_modes(rng.uniform(0.0, np.pi, M), gamma0)
-                    Q0[x, y] = np.clip(rng.normal(q_mean, q_std, M), q_min, None)
+                    flip(x, y, m)
                     sig, sigM = elastic_run()
                     n_solves += 1
                     events.append((x, y, m, time))
                     if max_events is not None and len(events) >= max_events:
-                        return dict(events=events, eps_macro=eps_macro, sig=sig, eps_p=eps_p, time=time,
-                                    steps=steps_done, solves=n_solves, catalog=catalog, Q0=Q0)
+                        return result()
                     continue
             eps_macro += strain_unit * (strain_rate * remaining)
             time += remaining
@@ -123,5 +173,4 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
                 prev_s[idx] = sigM[idx]
                 eps_macro[idx] += step
         steps_done += 1
-    return dict(events=events, eps_macro=eps_macro, sig=sig, eps_p=eps_p, time=time, steps=steps_done,
-                solves=n_solves, catalog=catalog, Q0=Q0)
+    return result()

@@ -276,6 +276,17 @@ def ls2d_rose_fixtures():
     save("ls2d_rose_16x24", **out)
 
 
+def kmc2d_cascade_fixtures():
+    """The reference's find_unstable_2d on a barrier field with unstable modes."""
+    rng = np.random.default_rng(63)
+    Q = rng.normal(0.3, 0.25, (12, 10, 4))
+    out = dict(Q=Q)
+    for tag, thr in (("t0", 0.0), ("t1", 0.1)):
+        out[f"unstable_{tag}"] = KF.find_unstable_2d(Q, thr)
+        out[f"thr_{tag}"] = thr
+    save("kmc2d_cascade_12x10", **out)
+
+
 if __name__ == "__main__":
     ls2d_fixtures()
     ls3d_fixtures()
@@ -284,3 +295,4 @@ if __name__ == "__main__":
     fs3d_fixtures()
     ls2d_secant_fixtures()
     ls2d_rose_fixtures()
+    kmc2d_cascade_fixtures()

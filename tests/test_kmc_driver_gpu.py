@@ -55,3 +55,22 @@ def test_fast_modes_follow_the_trajectory():
     g = Kmc2D(E, nu, cat, Q0, selection="fast", ls_start="warm", **kw).run(
         np.random.default_rng(7), n_steps=200, max_events=20)
     assert [e[:3] for e in g["events"]] == [e[:3] for e in o["events"]]
+
+
+@pytest.mark.parametrize("n,M,seed", [(24, 4, 3), (32, 8, 4)])
+def test_cascade_trajectory_matches_oracle(n, M, seed):
+    # cascade mode (kmc_simulator.py:876-889, _run_cascade :577-794): low
+    # barriers (mean 0.35 eV, floor 0.05 eV) make modes unstable, so the
+    # trajectory holds cascade batches (most unstable mode per voxel, one LS
+    # re-solve per batch) between KMC events on compacted (q > 0) rates
+    from mgkmc_b200.kmc import Kmc2D
+    rng = np.random.default_rng(seed)
+    E, nu = W.ls2d_material(n, n, rng)
+    cat, Q0 = W.kmc2d_state(n, n, M, rng, q_mean=0.35, q_min=0.05)
+    kw = dict(step_size=1e-4, strain_rate=1e7, q_mean=0.35, q_min=0.05, ls_tol=1e-10, cascade_mode=True)
+    o = OD.run_kmc2d(E, nu, cat, Q0, np.random.default_rng(200 + seed), n_steps=60, max_events=12, **kw)
+    g = Kmc2D(E, nu, cat, Q0, **kw).run(np.random.default_rng(200 + seed), n_steps=60, max_events=12)
+    assert len(o["cascade_flips"]) > 0
+    assert [f[:3] for f in g["cascade_flips"]] == [f[:3] for f in o["cascade_flips"]]
+    assert [f[4] for f in g["cascade_flips"]] == [f[4] for f in o["cascade_flips"]]
+    _cmp(g, o, len(o["events"]))

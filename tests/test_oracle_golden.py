@@ -68,6 +68,13 @@ def test_ls2d_rose(golden, tag, pm):
     assert rel(sig, g[f"sig_{tag}"]) < 1e-12
 
 
+@pytest.mark.parametrize("tag", ["t0", "t1"])
+def test_find_unstable(golden, tag):
+    # the cascade's unstable-mode list against the reference's find_unstable_2d
+    g = golden("kmc2d_cascade_12x10")
+    np.testing.assert_array_equal(OK.find_unstable_2d(g["Q"], float(g[f"thr_{tag}"])), g[f"unstable_{tag}"])
+
+
 def test_ls2d_macro_loop(golden):
     g = golden("ls2d_macro_16")
     E, nu, mask, target = g["E"], g["nu"], g["mask"], g["target"]
