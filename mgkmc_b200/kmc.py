@@ -2,7 +2,7 @@
 
 Runs the trajectory of KmcSimulation2D.run_simulation
 (mgkmc/kmc_simulator.py:796-1157) on the path the KMC benchmark exercises
-(small-strain linear elasticity, KMC mode, no cascade, no thermal
+(small-strain linear elasticity, KMC mode, optional cascade mode, no thermal
 conduction, no fast patching, redraw of directions and barriers) with every
 field resident on the GPU: barriers, rates, the running rate sum, selection,
 the flip bookkeeping and the LS re-solve never leave the device.  The host
