@@ -360,6 +360,31 @@ MGK_API int mgk_kmc2d_event(int nx, int ny, int M, const int64_t* d_sel, const i
                             double current_time, double jp, double jt, double g_max, double jn_frac,
                             int64_t* d_xym, mgk_stream_t stream);
 
+/* Fast-patching stress patches: replaces KmcSimulation2D._precompute_patch_kernels
+ * (mgkmc/kmc_simulator.py:229-261) after its two LS solves.  r0, r1 (nx,ny,2,2)
+ * are the stress responses to the unit eigenstrains [[1,0],[0,-1]] and
+ * [[0,1],[1,0]] at voxel (nx/2, ny/2) under zero macro strain.  Writes
+ * kernels (2, 2R+1, 2R+1, 2, 2): each response in the window centred on that
+ * voxel (periodic), and missing_mean (2, 2, 2): mean(r_b) - sum(window_b) /
+ * (nx*ny).  0 <= R <= 4096. */
+MGK_API int mgk_kmc2d_patch_setup(int nx, int ny, int R, const double* r0, const double* r1, double* kernels,
+                                  double* missing_mean, mgk_stream_t stream);
+
+/* One fast-patching stress update of sig (nx,ny,2,2) in place: replaces
+ * mgkmc/kmc_simulator.py:1052-1069 (KMC event) and :764-774 (cascade flip).
+ * The mode is the device selection d_sel (through `indices` when non-null,
+ * as in mgk_kmc2d_event); gxx, gxy are its catalog entries (0,0) and (0,1)
+ * when the call runs: enqueue it before mgk_kmc2d_event for the pre-flip
+ * direction (KMC events), after it for the redrawn one (cascade flips).
+ * sig += sig_unit * unit_scale when sig_unit is non-null, then
+ * gxx*K0 + gxy*K1 added in the window around the mode's voxel, then
+ * gxx*m0 + gxy*m1 added to every voxel.  A negative selection leaves the
+ * patch out; a null d_sel applies only the sig_unit term (the macro-strain
+ * increment of :1094-1096).  sig and sig_unit 16-byte aligned. */
+MGK_API int mgk_kmc2d_patch(int nx, int ny, int M, double* sig, const double* sig_unit, double unit_scale,
+                            const double* kernels, const double* missing_mean, int R, const double* catalog,
+                            const int64_t* d_sel, const int64_t* indices, mgk_stream_t stream);
+
 /* mgkmc/kmc_simulator_functions.py:183-218 apply_flip_soa_2d (in place). */
 MGK_API int mgk_kmc2d_flip(int nx, int ny, int M, double* eps_plastic, double* soft_prop,
                    double* last_event_time, const double* catalog, int x, int y, int m,

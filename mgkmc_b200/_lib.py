@@ -107,6 +107,8 @@ _SIGS = {
     "mgk_kmc_prefix_fast": (c_int, [_P, c_int64, _P, _P, _P, _P, _P]),
     "mgk_kmc2d_event": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_double, c_double,
                                 c_double, c_double, c_double, _P, _P]),
+    "mgk_kmc2d_patch_setup": (c_int, [c_int, c_int, c_int, _P, _P, _P, _P, _P]),
+    "mgk_kmc2d_patch": (c_int, [c_int, c_int, c_int, _P, _P, c_double, _P, _P, c_int, _P, _P, _P, _P]),
     "mgk_kmc3d_barrier": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, c_double, _P, _P, c_double, _P,
                                   c_double, c_int, c_double, _P]),
     "mgk_kmc3d_rates": (c_int, [c_int, c_int, c_int, c_int, _P, c_double, _P, c_double, c_double, c_int, _P, _P,

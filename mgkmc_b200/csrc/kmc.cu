@@ -789,6 +789,100 @@ __global__ void event2d_kernel(int nx, int ny, int M, const long long* d_sel, co
   if (d_xym) { d_xym[0] = x; d_xym[1] = y; d_xym[2] = m; }
 }
 
+// Fast-patching stress update (mgkmc/kmc_simulator.py:1052-1069; cascade
+// branch :764-774), one thread per voxel.  The flipped mode comes from the
+// device selection (through the compacted index list when one is given), so
+// the host never waits for it; a negative selection changes nothing, and a
+// null selection applies only the macro-strain term.  Per component, in the
+// reference's order: s + unit*scale, then every window entry gxx*K0 + gxy*K1
+// that lands on this voxel in (dx, dy) order (periodic wrap: a window wider
+// than the grid adds more than once), then + (gxx*m0 + gxy*m1).  Each product
+// and sum is rounded on its own, as numpy evaluates the expressions.
+__global__ void patch2d_kernel(int nx, int ny, int M, double* __restrict__ sig, const double* __restrict__ unit,
+                               double scale, const double* __restrict__ kern, const double* __restrict__ miss,
+                               int R, const double* __restrict__ cat, const long long* __restrict__ d_sel,
+                               const long long* __restrict__ indices) {
+  const long long nv = (long long)nx * ny;
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  long long idx = -1;
+  if (d_sel) {
+    const long long k = *d_sel;
+    if (k < 0) return;
+    idx = indices ? indices[k] : k;
+    if (idx < 0 || idx >= nv * M) return;
+  }
+  double2* s2 = reinterpret_cast<double2*>(sig + 4 * v);
+  const double2 a = s2[0], b = s2[1];
+  double s[4] = {a.x, a.y, b.x, b.y};
+  if (unit) {
+    const double2* u2 = reinterpret_cast<const double2*>(unit + 4 * v);
+    const double2 ua = u2[0], ub = u2[1];
+    s[0] = add(s[0], mul(ua.x, scale));
+    s[1] = add(s[1], mul(ua.y, scale));
+    s[2] = add(s[2], mul(ub.x, scale));
+    s[3] = add(s[3], mul(ub.y, scale));
+  }
+  if (idx >= 0) {
+    const long long fv = idx / M;
+    const int x = (int)(fv / ny), y = (int)(fv % ny);
+    const double gxx = cat[idx * 4 + 0], gxy = cat[idx * 4 + 1];
+    const int i = (int)(v / ny), j = (int)(v % ny);
+    const int W = 2 * R + 1;
+    const int di = ((i - x) % nx + nx) % nx, dj = ((j - y) % ny + ny) % ny;
+    for (int dx = di - nx * ((di + R) / nx); dx <= R; dx += nx)
+      for (int dy = dj - ny * ((dj + R) / ny); dy <= R; dy += ny) {
+        const double* k0 = kern + ((long long)(dx + R) * W + (dy + R)) * 4;
+        const double* k1 = k0 + (long long)W * W * 4;
+        for (int c = 0; c < 4; ++c) s[c] = add(s[c], add(mul(gxx, k0[c]), mul(gxy, k1[c])));
+      }
+    for (int c = 0; c < 4; ++c) s[c] = add(s[c], add(mul(gxx, miss[c]), mul(gxy, miss[4 + c])));
+  }
+  s2[0] = make_double2(s[0], s[1]);
+  s2[1] = make_double2(s[2], s[3]);
+}
+
+// Stress patches from the two basis responses (kmc_simulator.py:229-261).
+// Block b crops response b to the (2R+1)^2 window centred on (nx/2, ny/2) and
+// writes mean(r_b) - sum(window_b) / (nx*ny) per component.  Runs once per
+// simulation; 256 threads.
+__global__ void patch2d_setup_kernel(int nx, int ny, int R, const double* __restrict__ r0,
+                                     const double* __restrict__ r1, double* __restrict__ kern,
+                                     double* __restrict__ miss) {
+  __shared__ double red[4][256];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const double* r = b ? r1 : r0;
+  const long long W = 2 * R + 1, nv = (long long)nx * ny;
+  double* kb = kern + b * W * W * 4;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0}, wacc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long e = t; e < W * W; e += blockDim.x) {
+    const int dx = (int)(e / W) - R, dy = (int)(e % W) - R;
+    const long long px = ((dx + nx / 2) % nx + nx) % nx, py = ((dy + ny / 2) % ny + ny) % ny;
+    for (int c = 0; c < 4; ++c) {
+      const double val = r[(px * ny + py) * 4 + c];
+      kb[e * 4 + c] = val;
+      wacc[c] += val;
+    }
+  }
+  for (long long v = t; v < nv; v += blockDim.x)
+    for (int c = 0; c < 4; ++c) acc[c] += r[v * 4 + c];
+  for (int pass = 0; pass < 2; ++pass) {
+    double* src = pass ? wacc : acc;
+    for (int c = 0; c < 4; ++c) red[c][t] = src[c];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+      if (t < h)
+        for (int c = 0; c < 4; ++c) red[c][t] += red[c][t + h];
+      __syncthreads();
+    }
+    if (t == 0)
+      for (int c = 0; c < 4; ++c) src[c] = red[c][0];
+    __syncthreads();
+  }
+  if (t == 0)
+    for (int c = 0; c < 4; ++c) miss[b * 4 + c] = acc[c] / (double)nv - wacc[c] / (double)nv;
+}
+
 // Parallel inclusive FP64 scan (fast selection mode): per-block scans of
 // 1024 rates, an exclusive scan of the block totals, and the offsets.  The
 // running sums differ from the sequential chain by rounding only.
@@ -1007,6 +1101,31 @@ extern "C" int mgk_kmc2d_event(int nx, int ny, int M, const int64_t* d_sel, cons
                                                     eps_plastic, soft_prop, last_event_time, catalog, Q0,
                                                     prev_strain_dir, new_catalog, new_q0, current_time, jp, jt, g_max,
                                                     jn_frac, (long long*)d_xym);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_patch_setup(int nx, int ny, int R, const double* r0, const double* r1, double* kernels,
+                                     double* missing_mean, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && R >= 0 && R <= 4096 && r0 && r1 && kernels && missing_mean,
+              "mgk_kmc2d_patch_setup: bad argument");
+  patch2d_setup_kernel<<<2, 256, 0, (cudaStream_t)stream>>>(nx, ny, R, r0, r1, kernels, missing_mean);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc2d_patch(int nx, int ny, int M, double* sig, const double* sig_unit, double unit_scale,
+                               const double* kernels, const double* missing_mean, int R, const double* catalog,
+                               const int64_t* d_sel, const int64_t* indices, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && M > 0 && sig && R >= 0 && R <= 4096 &&
+                  (!d_sel || (kernels && missing_mean && catalog)),
+              "mgk_kmc2d_patch: bad argument");
+  MGK_REQUIRE(((uintptr_t)sig & 15) == 0 && ((uintptr_t)sig_unit & 15) == 0,
+              "mgk_kmc2d_patch: sig and sig_unit must be 16-byte aligned");
+  const long long nv = (long long)nx * ny;
+  patch2d_kernel<<<blocks_for(nv, 256), 256, 0, (cudaStream_t)stream>>>(
+      nx, ny, M, sig, sig_unit, unit_scale, kernels, missing_mean, R, catalog, (const long long*)d_sel,
+      (const long long*)indices);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

@@ -2,8 +2,8 @@
 
 Runs the trajectory of KmcSimulation2D.run_simulation
 (mgkmc/kmc_simulator.py:796-1157) on the path the KMC benchmark exercises
-(small-strain linear elasticity, KMC mode, optional cascade mode, no thermal
-conduction, no fast patching, redraw of directions and barriers) with every
+(small-strain linear elasticity, KMC mode, optional cascade mode and fast
+patching, no thermal conduction, redraw of directions and barriers) with every
 field resident on the GPU: barriers, rates, the running rate sum, selection,
 the flip bookkeeping and the LS re-solve never leave the device.  The host
 keeps the clock, the macro strain and the random draws (one small
@@ -43,7 +43,7 @@ class Kmc2D:
                  q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0, stress_targets=None, mixed_tol=1e4,
                  mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200, q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0,
                  selection="exact", ls_start="cold", precision="fp64", ls=None, rep=0, stream=None,
-                 cascade_mode=False, stability_threshold=0.0, max_cascade_steps_pct=0.3):
+                 cascade_mode=False, stability_threshold=0.0, max_cascade_steps_pct=0.3, fast_patching=None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("mgkmc_b200 needs a CUDA device (no CPU fallback)")
@@ -109,10 +109,61 @@ class Kmc2D:
         else:
             self.ls, self.rep = ls, int(rep)
         self.ls.set_material(self.rep, self.E, self.nu, self.eps_p, stream=self.stream)
+        # fast patching (kmc_simulator.py:76-80, :170-171, :229-261): stress
+        # patches and the unit macro-strain response, solved once
+        self.fast = bool(fast_patching and fast_patching.get("enabled", False))
+        if self.fast:
+            self.R = int(fast_patching.get("patch_radius", 5))
+            self.sync_interval = int(fast_patching.get("sync_interval", 100))
+            self._setup_patches(getattr(self.ls, "precision", precision))
+        self.flips_since_sync = 0
+        self.unit_ready = False  # the reference computes the unit response at the first KMC flip
         self.eps_macro = np.zeros((2, 2))
         self.time = 0.0
         self.events = []
         self.n_solves = 0
+
+    def _setup_patches(self, precision):
+        """LS responses to unit eigenstrains [[1,0],[0,-1]] and [[0,1],[1,0]] at
+        (nx//2, ny//2) under zero macro strain, and to the unit macro strain
+        e_00 without eigenstrain (one batched solve of three replicas), then
+        the windows and missing means on the device."""
+        torch, d, f64 = self.torch, self.dev, self.torch.float64
+        nx, ny = self.nx, self.ny
+        with torch.cuda.stream(self.stream):
+            ep = torch.zeros((3, nx, ny, 2, 2), dtype=f64, device=d)
+            ep[0, nx // 2, ny // 2, 0, 0], ep[0, nx // 2, ny // 2, 1, 1] = 1.0, -1.0
+            ep[1, nx // 2, ny // 2, 0, 1], ep[1, nx // 2, ny // 2, 1, 0] = 1.0, 1.0
+        tmp = Ls2dBatch([(nx, ny)] * 3, precision=precision)
+        for r in range(3):
+            tmp.set_material(r, self.E, self.nu, ep[r], stream=self.stream)
+        resp = torch.empty((3, nx, ny, 2, 2), dtype=f64, device=d)
+        eps = torch.empty_like(resp)
+        unit = np.zeros((2, 2))
+        unit[0, 0] = 1.0
+        infos = tmp.solve([0, 1, 2], [np.zeros((2, 2)), np.zeros((2, 2)), unit], list(eps), list(resp),
+                          max_iter=self.p["ls_max_iter"], tol=self.p["ls_tol"], stream=self.stream)
+        for info in infos:
+            if not np.all(np.isfinite(np.array(info.sig_mean))):
+                raise ValueError("fast patching: non-finite patch response")
+        W = 2 * self.R + 1
+        self.kern = torch.empty((2, W, W, 2, 2), dtype=f64, device=d)
+        self.miss = torch.empty((2, 2, 2), dtype=f64, device=d)
+        L.check(L.lib().mgk_kmc2d_patch_setup(nx, ny, self.R, L.ptr(resp[0]), L.ptr(resp[1]), L.ptr(self.kern),
+                                              L.ptr(self.miss), L.stream_ptr(self.stream)), "mgk_kmc2d_patch_setup")
+        with torch.cuda.stream(self.stream):
+            self.sig_unit = resp[2].clone()
+        self.stream.synchronize()  # the temporary plan and responses are released after this
+        del tmp
+
+    def launch_patch(self, sel, indices=None, unit_scale=None):
+        """One fast-patching stress update (``mgk_kmc2d_patch``); ``sel`` a
+        device pointer to the selection (None: only the macro-strain term)."""
+        unit = L.ptr(self.sig_unit) if unit_scale is not None else None
+        L.check(L.lib().mgk_kmc2d_patch(self.nx, self.ny, self.M, L.ptr(self.sig), unit,
+                                        0.0 if unit_scale is None else float(unit_scale), L.ptr(self.kern),
+                                        L.ptr(self.miss), self.R, L.ptr(self.catalog), sel, indices,
+                                        L.stream_ptr(self.stream)), "mgk_kmc2d_patch")
 
     @property
     def E_avg(self):
@@ -178,7 +229,7 @@ class Kmc2D:
         self.stream.synchronize()
         return float(self.total_h[0])
 
-    def event(self, u_sel, theta, q0):
+    def event(self, u_sel, theta, q0, t_wait=0.0):
         lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
         M = self.M
         self.redraw_h[:4 * M] = self.torch.from_numpy(pure_shear_modes(theta, p["gamma0"]).reshape(-1))
@@ -200,6 +251,10 @@ class Kmc2D:
         nq = L.c_void_p(self.redraw.data_ptr() + 4 * M * 8)
         # compacted rates (cascade mode) map the selected position to its mode
         ind = L.ptr(self.indices) if self.cascade_mode else None
+        if self.fast:
+            # the stress patch of the pre-flip direction (kmc_simulator.py:1044-1069)
+            self.unit_ready = True
+            self.launch_patch(L.ptr(self.sel), ind, p["strain_rate"] * t_wait if t_wait > 0 else None)
         L.check(lib.mgk_kmc2d_event(self.nx, self.ny, M, L.ptr(self.sel), ind, L.ptr(self.eps_p), L.ptr(self.soft),
                                     L.ptr(self.t_last), L.ptr(self.catalog), L.ptr(self.Q0), L.ptr(self.prev), nc, nq,
                                     self.time, p["jp"], p["jt"], p["cap"], p["jn"], L.ptr(self.xym), S),
@@ -262,6 +317,9 @@ class Kmc2D:
                                         p["jp"], p["jt"], p["cap"], p["jn"], L.ptr(self.xym), S), "mgk_kmc2d_event")
             L.check(lib.mgk_ls2d_sync_voxel(self.ls._h, self.rep, L.ptr(self.eps_p), L.ptr(self.xym), S),
                     "mgk_ls2d_sync_voxel")
+            if self.fast:
+                # the patch of the redrawn direction (kmc_simulator.py:764-774)
+                self.launch_patch(L.c_void_p(sel_d.data_ptr() + 8 * i))
 
     # ---------------------------------------------------------------- run ---
     def trajectory(self, rng, n_steps, max_events=None):
@@ -295,7 +353,8 @@ class Kmc2D:
                             for f in batch:
                                 x, y, m = f // (self.ny * M), (f // M) % self.ny, f % M
                                 self.cascade_flips.append((x, y, m, self.time, n_batches))
-                            self.after_solve((yield ("solve",)))
+                            if not self.fast:
+                                self.after_solve((yield ("solve",)))
                             n_batches += 1
                             flips += len(batch)
                             local_step += 1
@@ -304,6 +363,9 @@ class Kmc2D:
                             self.launch_barriers()
                             yield ("sync",)
                             batch = self.unstable_batch()
+                        if self.fast and flips > 0:
+                            # corrector: the final sync (kmc_simulator.py:790-792)
+                            self.after_solve((yield ("solve",)))
                         if flips > 0:
                             cascade_count += 1
                         if cascade_count > self.max_cascade_limit:
@@ -323,13 +385,24 @@ class Kmc2D:
                         u_sel = rng.random()
                         theta = rng.uniform(0.0, np.pi, M)
                         q0 = np.clip(rng.normal(p["q_mean"], p["q_std"], M), p["q_min"], None)
-                        self.event(u_sel, theta, q0)
-                        self.after_solve((yield ("solve",)))
+                        self.event(u_sel, theta, q0, t_wait)
+                        if not self.fast:
+                            self.after_solve((yield ("solve",)))
+                        else:
+                            # a full re-solve every sync_interval KMC flips (:1071-1074)
+                            self.flips_since_sync += 1
+                            if self.flips_since_sync >= self.sync_interval:
+                                self.after_solve((yield ("solve",)))
+                                self.flips_since_sync = 0
+                            else:
+                                yield ("sync",)
                         x, y, m = (int(v) for v in self.xym_h.tolist())
                         self.events.append((x, y, m, self.time))
                         if max_events is not None and len(self.events) >= max_events:
                             return self.result(steps_done)
                         continue
+                if self.fast and self.unit_ready:
+                    self.launch_patch(None, None, p["strain_rate"] * remaining)  # :1094-1096
                 self.eps_macro += strain_unit * (p["strain_rate"] * remaining)
                 self.time += remaining
                 remaining = 0.0

@@ -4,8 +4,12 @@ TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 
 Follows KmcSimulation2D.run_simulation (mgkmc/kmc_simulator.py:796-1157) on
 the path the benchmark exercises: small-strain linear elasticity, KMC mode
-(cascade off, or on: ``cascade_mode``), no thermal conduction, no fast
-patching, redraw of both directions and barriers after a flip.  Cascade mode
+(cascade off, or on: ``cascade_mode``), no thermal conduction, fast
+patching off or on (``fast_patching``), redraw of both directions and
+barriers after a flip.  Fast patching (:229-261, :1044-1074, :764-792,
+:1094-1096) replaces the LS re-solve after a flip by a local stress patch
+and a uniform shift, with a full re-solve every ``sync_interval`` KMC flips
+and after each cascade.  Cascade mode
 (:876-889, _run_cascade :577-794, linear small-strain branch :728-784):
 after each barrier update, while modes with Q < stability_threshold exist,
 flip in one batch the most unstable mode of each voxel that has one (modes
@@ -42,11 +46,55 @@ def pure_shear_modes(theta, gamma0):
     return cat
 
 
+def patch_kernels_2d(E, nu, R, max_iter=200, tol=1e-6, pixel=1.0, plane_mode="plane_strain"):
+    """Stress patches of the fast-patching mode (kmc_simulator.py:229-261).
+
+    For each deviatoric basis P0 = [[1, 0], [0, -1]] and P1 = [[0, 1], [1, 0]]:
+    the LS stress response to a unit eigenstrain P at the voxel
+    (nx//2, ny//2) under zero macro strain, read in the (2R+1)^2 window centred
+    on that voxel (periodic), and the part of its mean that the window
+    misses: mean(sigma) - sum(window) / (nx*ny).  Returns
+    (kernels (2, 2R+1, 2R+1, 2, 2), missing_mean (2, 2, 2))."""
+    nx, ny = E.shape
+    bases = (np.array([[1.0, 0.0], [0.0, -1.0]]), np.array([[0.0, 1.0], [1.0, 0.0]]))
+    ix = (np.arange(-R, R + 1) + nx // 2) % nx
+    iy = (np.arange(-R, R + 1) + ny // 2) % ny
+    kernels = np.zeros((2, 2 * R + 1, 2 * R + 1, 2, 2))
+    missing = np.zeros((2, 2, 2))
+    for b, P in enumerate(bases):
+        ep = np.zeros((nx, ny, 2, 2))
+        ep[nx // 2, ny // 2] = P
+        _, sig, _, _ = OL.spectral_solver(E, nu, np.zeros((2, 2)), ep, max_iter=max_iter, tol=tol,
+                                          pixel=pixel, plane_mode=plane_mode)
+        kernels[b] = sig[ix[:, None], iy[None, :]]
+        missing[b] = np.mean(sig, axis=(0, 1)) - np.sum(kernels[b], axis=(0, 1)) / (nx * ny)
+    return kernels, missing
+
+
+def apply_patch_2d(sig, x, y, gxx, gxy, kernels, missing, unit=None, scale=0.0):
+    """One fast-patching stress update in place (kmc_simulator.py:1052-1069,
+    cascade branch :764-774): sig += unit * scale (when ``unit`` is given), then
+    the window gxx*K0 + gxy*K1 added around (x, y) with periodic wrap in (dx, dy)
+    order, then the missing mean gxx*m0 + gxy*m1 added everywhere."""
+    nx, ny = sig.shape[:2]
+    R = (kernels.shape[1] - 1) // 2
+    if unit is not None:
+        sig += unit * scale
+    patch = gxx * kernels[0] + gxy * kernels[1]
+    shift = gxx * missing[0] + gxy * missing[1]
+    px = (x + np.arange(-R, R + 1)) % nx
+    py = (y + np.arange(-R, R + 1)) % ny
+    # unbuffered adds in (dx, dy) order: repeated voxels (window wider than the
+    # grid) accumulate in the reference's loop order
+    np.add.at(sig, (px[:, None], py[None, :]), patch)
+    sig += shift
+
+
 def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=300.0, nu0=1e13,
               strain_rate=1e7, step_size=1e-5, q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0,
               stress_targets=None, mixed_tol=1e4, mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200,
               q_mean=1.0, q_std=0.15, q_min=0.3, volume=1.0, cascade_mode=False, stability_threshold=0.0,
-              max_cascade_steps_pct=0.3):
+              max_cascade_steps_pct=0.3, fast_patching=None):
     nx, ny, M = Q0.shape
     stress_targets = {(1, 1): 0.0} if stress_targets is None else stress_targets
     catalog = catalog.copy()
@@ -66,6 +114,17 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
         if np.any(np.isnan(sig)) or np.max(np.abs(sigM)) / 1e9 > 20.0:
             raise ValueError(f"Unstable stress in small-strain elastic_run: {sigM / 1e9} GPa")
         return sig, sigM
+
+    # fast patching (kmc_simulator.py:76-80, :170-171): patches computed once
+    # from the initial moduli; the unit macro-strain response is computed at
+    # the first KMC flip (:1045-1050)
+    fast = bool(fast_patching and fast_patching.get("enabled", False))
+    if fast:
+        R = int(fast_patching.get("patch_radius", 5))
+        sync_interval = int(fast_patching.get("sync_interval", 100))
+        kernels, missing = patch_kernels_2d(E, nu, R, max_iter=ls_max_iter, tol=ls_tol)
+    sig_unit = None
+    flips_since_sync = 0
 
     sig, sigM = elastic_run()
     events = []
@@ -113,13 +172,22 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
                     for (x, y, m) in batch:
                         flip(x, y, m)
                         cascade_flips.append((x, y, m, time, n_batches))
-                    sig, sigM = elastic_run()
-                    n_solves += 1
+                        if fast:
+                            # the patch uses the redrawn mode (:764-774)
+                            apply_patch_2d(sig, x, y, catalog[x, y, m, 0, 0], catalog[x, y, m, 0, 1],
+                                           kernels, missing)
+                    if not fast:
+                        sig, sigM = elastic_run()
+                        n_solves += 1
                     n_batches += 1
                     flips += len(batch)
                     local_step += 1
                     if local_step > nx * ny:
                         break
+                if fast and flips > 0:
+                    # corrector: the final sync (:790-792)
+                    sig, sigM = elastic_run()
+                    n_solves += 1
                 if flips > 0:
                     cascade_count += 1
                 if cascade_count > max_cascade_limit:
@@ -136,13 +204,28 @@ def run_kmc2d(E, nu, catalog, Q0, rng, n_steps, max_events=None, gamma0=0.1, T=3
                     remaining -= t_wait
                     k = OK.select_event(rates, total, rng.random())
                     x, y, m = OK.decode_index_2d(int(indices[k]), ny, M)
+                    C = catalog[x, y, m].copy()
                     flip(x, y, m)
-                    sig, sigM = elastic_run()
-                    n_solves += 1
+                    if fast:
+                        if sig_unit is None:
+                            _, sig_unit, _, _ = OL.spectral_solver(E, nu, strain_unit, np.zeros_like(eps_p),
+                                                                   max_iter=ls_max_iter, tol=ls_tol)
+                        apply_patch_2d(sig, x, y, C[0, 0], C[0, 1], kernels, missing,
+                                       unit=sig_unit if t_wait > 0 else None, scale=strain_rate * t_wait)
+                        flips_since_sync += 1
+                        if flips_since_sync >= sync_interval:
+                            sig, sigM = elastic_run()
+                            n_solves += 1
+                            flips_since_sync = 0
+                    else:
+                        sig, sigM = elastic_run()
+                        n_solves += 1
                     events.append((x, y, m, time))
                     if max_events is not None and len(events) >= max_events:
                         return result()
                     continue
+            if fast and sig_unit is not None:
+                sig += sig_unit * (strain_rate * remaining)
             eps_macro += strain_unit * (strain_rate * remaining)
             time += remaining
             remaining = 0.0

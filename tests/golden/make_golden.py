@@ -287,6 +287,23 @@ def kmc2d_cascade_fixtures():
     save("kmc2d_cascade_12x10", **out)
 
 
+def kmc2d_patch_fixtures():
+    """The reference's fast-patching stress patches
+    (KmcSimulation2D._precompute_patch_kernels) for the benchmark material on a
+    16 x 12 grid, radius 3 and a radius whose window wraps the grid (9)."""
+    import types
+    from mgkmc import kmc_simulator as KS
+    E, nu, _, _ = W.ls2d_problem(16, 12, seed=71)
+    out = dict(E=E, nu=nu)
+    for R in (3, 9):
+        host = types.SimpleNamespace(patch_radius=R, nx=16, ny=12, nu_field=nu, pixel=1.0,
+                                     plane_mode="plane_strain", solver_args={})
+        KS.KmcSimulation2D._precompute_patch_kernels(host, E)
+        out[f"kernels_r{R}"] = np.stack(host.patch_kernels)
+        out[f"missing_r{R}"] = np.stack(host.patch_missing_mean)
+    save("kmc2d_patch_16x12", **out)
+
+
 if __name__ == "__main__":
     ls2d_fixtures()
     ls3d_fixtures()
@@ -296,3 +313,4 @@ if __name__ == "__main__":
     ls2d_secant_fixtures()
     ls2d_rose_fixtures()
     kmc2d_cascade_fixtures()
+    kmc2d_patch_fixtures()

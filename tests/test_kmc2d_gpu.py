@@ -217,3 +217,64 @@ def test_fused_barrier_total(n, T):
     L.check(lib.mgk_kmc2d_rates_only(n, n, 8, L.ptr(Qa), 1.0, None, T, 1e13, L.ptr(rates), S), "rates_only")
     r = rates.cpu().numpy()
     assert abs(float(tot.item()) - np.sum(r)) <= 1e-13 * np.sum(r)
+
+
+@pytest.mark.parametrize("nx,ny,M,R,x,y,m", [(24, 20, 4, 3, 1, 18, 2), (5, 4, 3, 3, 4, 1, 1), (16, 16, 8, 0, 7, 0, 5)])
+def test_patch_bit_exact(nx, ny, M, R, x, y, m):
+    # fast-patching stress update (kmc_simulator.py:1052-1069) against the
+    # oracle's numpy form, bit for bit: with the unit macro-strain term, through
+    # the compacted index list, a window that wraps (5 x 4 grid, R = 3), R = 0
+    import torch
+    from mgkmc_b200 import _lib as L
+    from oracle import kmc_driver as OD
+    rng = np.random.default_rng(nx * 100 + R)
+    W_ = 2 * R + 1
+    sig0 = rng.normal(0, 1e8, (nx, ny, 2, 2))
+    unit = rng.normal(0, 5e10, (nx, ny, 2, 2))
+    kern = rng.normal(0, 1e10, (2, W_, W_, 2, 2))
+    miss = rng.normal(0, 1e6, (2, 2, 2))
+    cat = rng.normal(0, 0.05, (nx, ny, M, 2, 2))
+    scale = 3.7e-7
+    flat = (x * ny + y) * M + m
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    tsig, tunit, tkern, tmiss, tcat = t(sig0), t(unit), t(kern), t(miss), t(cat)
+    indices = t(np.array([5, flat, 2], dtype=np.int64))
+    sel = t(np.array([1], dtype=np.int64))
+    lib, S = L.lib(), L.stream_ptr()
+    L.check(lib.mgk_kmc2d_patch(nx, ny, M, L.ptr(tsig), L.ptr(tunit), scale, L.ptr(tkern), L.ptr(tmiss), R,
+                                L.ptr(tcat), L.ptr(sel), L.ptr(indices), S), "patch")
+    ref = sig0.copy()
+    OD.apply_patch_2d(ref, x, y, cat[x, y, m, 0, 0], cat[x, y, m, 0, 1], kern, miss, unit=unit, scale=scale)
+    np.testing.assert_array_equal(tsig.cpu().numpy(), ref)
+    # a negative selection leaves the patch out; no selection: only the unit term
+    neg = t(np.array([-1], dtype=np.int64))
+    tsig2 = t(sig0)
+    L.check(lib.mgk_kmc2d_patch(nx, ny, M, L.ptr(tsig2), None, 0.0, L.ptr(tkern), L.ptr(tmiss), R, L.ptr(tcat),
+                                L.ptr(neg), None, S), "patch")
+    np.testing.assert_array_equal(tsig2.cpu().numpy(), sig0)
+    L.check(lib.mgk_kmc2d_patch(nx, ny, M, L.ptr(tsig2), L.ptr(tunit), scale, None, None, R, None, None, None, S),
+            "patch")
+    np.testing.assert_array_equal(tsig2.cpu().numpy(), sig0 + unit * scale)
+
+
+@pytest.mark.parametrize("nx,ny,R", [(24, 20, 3), (14, 12, 7)])
+def test_patch_setup(nx, ny, R):
+    # windows and missing means of kmc_simulator.py:229-261 from given responses
+    import torch
+    from mgkmc_b200 import _lib as L
+    rng = np.random.default_rng(R)
+    r = rng.normal(0, 1e9, (2, nx, ny, 2, 2))
+    dev = torch.device("cuda")
+    tr = torch.from_numpy(r).to(dev)
+    kern = torch.empty((2, 2 * R + 1, 2 * R + 1, 2, 2), dtype=torch.float64, device=dev)
+    miss = torch.empty((2, 2, 2), dtype=torch.float64, device=dev)
+    L.check(L.lib().mgk_kmc2d_patch_setup(nx, ny, R, L.ptr(tr[0]), L.ptr(tr[1]), L.ptr(kern), L.ptr(miss),
+                                          L.stream_ptr()), "patch_setup")
+    ix = (np.arange(-R, R + 1) + nx // 2) % nx
+    iy = (np.arange(-R, R + 1) + ny // 2) % ny
+    for b in range(2):
+        crop = r[b][ix[:, None], iy[None, :]]
+        np.testing.assert_array_equal(kern[b].cpu().numpy(), crop)
+        want = np.mean(r[b], axis=(0, 1)) - np.sum(crop, axis=(0, 1)) / (nx * ny)
+        np.testing.assert_allclose(miss[b].cpu().numpy(), want, rtol=0, atol=1e-12 * np.max(np.abs(r)))

@@ -74,3 +74,52 @@ def test_cascade_trajectory_matches_oracle(n, M, seed):
     assert [f[:3] for f in g["cascade_flips"]] == [f[:3] for f in o["cascade_flips"]]
     assert [f[4] for f in g["cascade_flips"]] == [f[4] for f in o["cascade_flips"]]
     _cmp(g, o, len(o["events"]))
+
+
+def test_patch_kernels_golden(golden):
+    # the driver's stress patches against the reference's _precompute_patch_kernels
+    # (LS tolerance 1e-6 and 200 iterations, the reference's solver defaults)
+    from mgkmc_b200.kmc import Kmc2D
+    g = golden("kmc2d_patch_16x12")
+    rng = np.random.default_rng(1)
+    cat, Q0 = W.kmc2d_state(16, 12, 4, rng)
+    for R in (3, 9):
+        k = Kmc2D(g["E"], g["nu"], cat, Q0, ls_tol=1e-6, fast_patching=dict(enabled=True, patch_radius=R))
+        kern = g[f"kernels_r{R}"]
+        assert np.max(np.abs(k.kern.cpu().numpy() - kern)) / np.max(np.abs(kern)) < 1e-9
+        np.testing.assert_allclose(k.miss.cpu().numpy(), g[f"missing_r{R}"], rtol=0, atol=1e-9 * np.max(np.abs(kern)))
+
+
+@pytest.mark.parametrize("n,M,seed,R,sync", [(32, 8, 1, 3, 5), (12, 4, 2, 7, 3)])
+def test_fast_patching_trajectory_matches_oracle(n, M, seed, R, sync):
+    # fast patching (kmc_simulator.py:1044-1074, :1094-1096): stress patches
+    # instead of the LS re-solve after each flip, a full re-solve every `sync`
+    # flips and in the mixed stress loop; R = 7 on a 12 x 12 grid wraps
+    from mgkmc_b200.kmc import Kmc2D
+    E, nu, cat, Q0 = _setup(n, M, seed)
+    kw = dict(step_size=1e-4, strain_rate=1e7, q_mean=Q_MEAN, ls_tol=1e-10,
+              fast_patching=dict(enabled=True, patch_radius=R, sync_interval=sync))
+    o = OD.run_kmc2d(E, nu, cat, Q0, np.random.default_rng(100 + seed), n_steps=200, max_events=25, **kw)
+    g = Kmc2D(E, nu, cat, Q0, **kw).run(np.random.default_rng(100 + seed), n_steps=200, max_events=25)
+    assert o["steps"] > 0 and o["solves"] < 25 + o["steps"] * 50
+    assert g["steps"] == o["steps"] and g["solves"] == o["solves"]
+    _cmp(g, o, 25)
+
+
+def test_fast_patching_cascade_matches_oracle():
+    # cascade batches with fast patching (kmc_simulator.py:764-792): patches of
+    # the redrawn directions, no re-solve per batch, one after each cascade
+    from mgkmc_b200.kmc import Kmc2D
+    n, M, seed = 24, 4, 6
+    rng = np.random.default_rng(seed)
+    E, nu = W.ls2d_material(n, n, rng)
+    cat, Q0 = W.kmc2d_state(n, n, M, rng, q_mean=0.45, q_min=0.15)
+    kw = dict(step_size=1e-4, strain_rate=1e7, q_mean=0.45, q_min=0.15, ls_tol=1e-10, cascade_mode=True,
+              max_cascade_steps_pct=0.02, fast_patching=dict(enabled=True, patch_radius=3, sync_interval=4))
+    o = OD.run_kmc2d(E, nu, cat, Q0, np.random.default_rng(200 + seed), n_steps=60, max_events=12, **kw)
+    g = Kmc2D(E, nu, cat, Q0, **kw).run(np.random.default_rng(200 + seed), n_steps=60, max_events=12)
+    assert len(o["cascade_flips"]) > 10
+    assert [f[:3] for f in g["cascade_flips"]] == [f[:3] for f in o["cascade_flips"]]
+    assert [f[4] for f in g["cascade_flips"]] == [f[4] for f in o["cascade_flips"]]
+    assert g["solves"] == o["solves"]
+    _cmp(g, o, len(o["events"]))

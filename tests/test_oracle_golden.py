@@ -75,6 +75,39 @@ def test_find_unstable(golden, tag):
     np.testing.assert_array_equal(OK.find_unstable_2d(g["Q"], float(g[f"thr_{tag}"])), g[f"unstable_{tag}"])
 
 
+@pytest.mark.parametrize("R", [3, 9])
+def test_patch_kernels(golden, R):
+    # fast-patching stress patches against the reference's _precompute_patch_kernels
+    # (R = 9: the 19 x 19 window wraps the 16 x 12 grid)
+    from oracle import kmc_driver as OD
+    g = golden("kmc2d_patch_16x12")
+    kern, miss = OD.patch_kernels_2d(g["E"], g["nu"], R)
+    assert rel(kern, g[f"kernels_r{R}"]) < 1e-12
+    np.testing.assert_allclose(miss, g[f"missing_r{R}"], rtol=0, atol=1e-12 * np.max(np.abs(kern)))
+
+
+def test_apply_patch_wrap_order():
+    # the vectorised window add equals the reference's (dx, dy) loop, also when
+    # the window is wider than the grid and voxels receive several adds
+    from oracle import kmc_driver as OD
+    rng = np.random.default_rng(5)
+    nx, ny, R = 5, 4, 3
+    kern = rng.normal(size=(2, 2 * R + 1, 2 * R + 1, 2, 2))
+    miss = rng.normal(size=(2, 2, 2))
+    sig0 = rng.normal(size=(nx, ny, 2, 2))
+    unit = rng.normal(size=(nx, ny, 2, 2))
+    gxx, gxy, x, y, scale = 0.031, -0.017, 4, 1, 0.37
+    sig = sig0.copy()
+    OD.apply_patch_2d(sig, x, y, gxx, gxy, kern, miss, unit=unit, scale=scale)
+    ref = sig0 + unit * scale
+    patch = gxx * kern[0] + gxy * kern[1]
+    for dx in range(-R, R + 1):
+        for dy in range(-R, R + 1):
+            ref[(x + dx) % nx, (y + dy) % ny] += patch[dx + R, dy + R]
+    ref += gxx * miss[0] + gxy * miss[1]
+    np.testing.assert_array_equal(sig, ref)
+
+
 def test_ls2d_macro_loop(golden):
     g = golden("ls2d_macro_16")
     E, nu, mask, target = g["E"], g["nu"], g["mask"], g["target"]
