@@ -210,6 +210,18 @@ MGK_API int mgk_ls3d_set_material_rep(mgk_ls3d_t plan, int rep, const double* E,
                                       const double* eps_plastic, mgk_stream_t stream);
 MGK_API int mgk_ls3d_set_eigenstrain_rep(mgk_ls3d_t plan, int rep, const double* eps_plastic,
                                          mgk_stream_t stream);
+/* Lame fields lam, mu (nx,ny,nz) given directly, as spectral_solver_secant_3d
+ * takes them (mgkmc/linear_elastic_simulator.py:768-771), with the reference
+ * medium C0 = (mean lam, mean mu) (:783-784). */
+MGK_API int mgk_ls3d_set_lame_rep(mgk_ls3d_t plan, int rep, const double* lam, const double* mu,
+                                  const double* eps_plastic, mgk_stream_t stream);
+/* Constitutive law of every replica: d = 0 linear elastic; otherwise the
+ * secant degradation law of spectral_solver_secant_3d
+ * (linear_elastic_simulator.py:768-850; elasticity.py:261-295, :665-728):
+ * sigma = lam tr(e) I + 2 mu (1 - d (1 - exp(-k eq(e)))) e, e = eps - eps_p,
+ * eq the von Mises equivalent strain.  0 <= d <= 1, k >= 0; FP64 plans
+ * only.  Takes effect at the next solve. */
+MGK_API int mgk_ls3d_set_secant(mgk_ls3d_t plan, double d, double k);
 MGK_API int mgk_ls3d_solve_batch(mgk_ls3d_t plan, int nsel, const int* sel, const double* eps_bar,
                                  const double* const* eps_init, double* const* eps_out,
                                  double* const* sig_out, int max_iter, double tol, mgk_ls_info3* infos,

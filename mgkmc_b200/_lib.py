@@ -77,6 +77,8 @@ _SIGS = {
     "mgk_ls3d_destroy": (c_int, [_P]),
     "mgk_ls3d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
     "mgk_ls3d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
+    "mgk_ls3d_set_lame_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
+    "mgk_ls3d_set_secant": (c_int, [_P, c_double, c_double]),
     "mgk_ls3d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
                                      POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo3), _P]),
     "mgk_fs3d_create": (c_int, [c_int, c_int, c_int, c_int, POINTER(c_void_p)]),

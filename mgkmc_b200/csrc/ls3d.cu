@@ -67,6 +67,10 @@ struct Ls3dRep {
   double tol;
   int max_iter;
   int zl_first;
+  // constitutive law: 0 linear (elasticity.py:62-67); 1 the secant
+  // degradation law with magnitude law_a and rate law_b (FP64 plans)
+  int law;
+  double law_a, law_b;
 };
 
 struct Ls3dState {
@@ -132,6 +136,19 @@ __device__ __forceinline__ void gamma3d_apply(const double2* t, double n0, doubl
 
 // -------------------------------------------------------------- kernels ---
 
+// Secant shear modulus mu (1 - d (1 - exp(-k eq))) (elasticity.py:703-728) at
+// the von Mises equivalent strain sqrt(2/3 e':e') of the elastic strain
+// (elasticity.py:665-700) given by its symmetric components; each pair of
+// shear entries sums to twice the symmetric one.
+__device__ __forceinline__ double secant_mu3(double m, double xx, double yy, double zz, double yz, double xz,
+                                             double xy, double d, double k) {
+  const double tr3 = (xx + yy + zz) / 3.0;
+  const double a = xx - tr3, b = yy - tr3, c = zz - tr3;
+  const double s1 = 2.0 * xy, s2 = 2.0 * xz, s3 = 2.0 * yz;
+  const double eq = sqrt((2.0 / 3.0) * (a * a + b * b + c * c + 0.5 * (s1 * s1 + s2 * s2 + s3 * s3)));
+  return m * (1.0 - d * (1.0 - exp(-k * eq)));
+}
+
 __global__ void ls3d_material_kernel(const Ls3dRep* reps, int rep, const double* __restrict__ E,
                                      const double* __restrict__ nu, const double* __restrict__ epsp,
                                      int set_moduli, double* partials) {
@@ -142,10 +159,11 @@ __global__ void ls3d_material_kernel(const Ls3dRep* reps, int rep, const double*
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
     if (set_moduli) {
-      // elasticity.py:55-59
+      // elasticity.py:55-59 (set_moduli 1); set_moduli 2: E holds lambda and
+      // nu holds mu, as the secant solver takes them
       const double e = E[i], v = nu[i];
-      R.mu[i] = e / (2 * (1 + v));
-      R.lam[i] = e * v / ((1 + v) * (1 - 2 * v));
+      R.mu[i] = set_moduli == 2 ? v : e / (2 * (1 + v));
+      R.lam[i] = set_moduli == 2 ? e : e * v / ((1 + v) * (1 - 2 * v));
       if (R.mu32) { R.mu32[i] = (float)R.mu[i]; R.lam32[i] = (float)R.lam[i]; }
       sE += e;
       sn += v;
@@ -167,7 +185,10 @@ __global__ void ls3d_material_kernel(const Ls3dRep* reps, int rep, const double*
   }
 }
 
-__global__ void ls3d_medium_kernel(const Ls3dRep* reps, Ls3dState* st, int rep, const double* partials, int nb) {
+// reference medium from the means of E and nu (linear_elastic_simulator.py:
+// 284-289), or of lambda and mu (lame_in; the secant solver, :783-784)
+__global__ void ls3d_medium_kernel(const Ls3dRep* reps, Ls3dState* st, int rep, const double* partials, int nb,
+                                   int lame_in) {
   __shared__ double red[32];
   double a = 0, b = 0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) { a += partials[2 * i]; b += partials[2 * i + 1]; }
@@ -176,7 +197,8 @@ __global__ void ls3d_medium_kernel(const Ls3dRep* reps, Ls3dState* st, int rep, 
   if (threadIdx.x == 0) {
     const double N = (double)reps[rep].N;
     const double E = a / N, v = b / N;
-    const double mu0 = E / (2 * (1 + v)), lam0 = E * v / ((1 + v) * (1 - 2 * v));
+    const double mu0 = lame_in ? v : E / (2 * (1 + v));
+    const double lam0 = lame_in ? E : E * v / ((1 + v) * (1 - 2 * v));
     Ls3dState& S = st[rep];
     S.mu0 = mu0;
     S.lam0 = lam0;
@@ -414,10 +436,12 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
           e[c] = o;
         }
       }
-      const double m = R.mu[i], l = R.lam[i];
+      double m = R.mu[i];
+      const double l = R.lam[i];
       double d[6];
 #pragma unroll
       for (int c = 0; c < 6; ++c) d[c] = e[c] - R.ep[c * N + i];
+      if (R.law == 1) m = secant_mu3(m, d[0], d[1], d[2], d[3], d[4], d[5], R.law_a, R.law_b);
       const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
 #pragma unroll
       for (int c = 0; c < 3; ++c) tr[h][c] = (2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre);
@@ -570,7 +594,7 @@ __host__ __device__ constexpr int ls3_zl_smem(int nz, int csz) {
 }
 __host__ __device__ constexpr int ls3_ax_smem(int n, int csz) { return 6 * kL3Tile * ls3_pl(n, csz) * csz; }
 
-template <typename T, bool IN_SPEC, bool FINAL, int NZ>
+template <typename T, bool IN_SPEC, bool FINAL, int NZ, int LAW>
 __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, int item, int r, long long l0,
                                                double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
                                                cudaGraphConditionalHandle cond, int use_cond, int guard_cap,
@@ -663,10 +687,12 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
           e[c] = o;
         }
       }
-      const double m = (double)stg[12 * NZ + j], l = (double)stg[14 * NZ + j];
+      double m = (double)stg[12 * NZ + j];
+      const double l = (double)stg[14 * NZ + j];
       double d[6];
 #pragma unroll
       for (int c = 0; c < 6; ++c) d[c] = e[c] - (double)stg[(16 + 2 * c) * NZ + j];
+      if constexpr (LAW == 1) m = secant_mu3(m, d[0], d[1], d[2], d[3], d[4], d[5], R.law_a, R.law_b);
       const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
 #pragma unroll
       for (int c = 0; c < 3; ++c) tr[h][c] = (T)((2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre));
@@ -693,7 +719,7 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
   ls3d_decide<FINAL>(R, S, r, item, d2, n2, partials, rep_counter, ctl, cond, use_cond, guard_cap, red, s_last);
 }
 
-template <typename T, bool IN_SPEC, bool FINAL>
+template <typename T, bool IN_SPEC, bool FINAL, int LAW = 0>
 __device__ __forceinline__ void ls3d_zline_fast_entry(const Ls3dRep* __restrict__ reps, Ls3dState* st,
                                                       const int* __restrict__ map, const int* __restrict__ loc,
                                                       double* partials, unsigned int* rep_counter, Ls3dCtl* ctl,
@@ -720,7 +746,7 @@ __device__ __forceinline__ void ls3d_zline_fast_entry(const Ls3dRep* __restrict_
   }
   __syncthreads();
   const long long l0 = 2LL * loc[item];
-#define MGK_Z3_CASE(n) case n: ls3_zline_body<T, IN_SPEC, FINAL, n>(R, S, item, r, l0, partials, rep_counter, ctl, cond, use_cond, guard_cap, smem_raw, &bar, red, &s_last); break;
+#define MGK_Z3_CASE(n) case n: ls3_zline_body<T, IN_SPEC, FINAL, n, LAW>(R, S, item, r, l0, partials, rep_counter, ctl, cond, use_cond, guard_cap, smem_raw, &bar, red, &s_last); break;
   switch (R.nz) {
     MGK_Z3_CASE(64) MGK_Z3_CASE(96) MGK_Z3_CASE(128)
     default: break;
@@ -739,14 +765,14 @@ __global__ void __launch_bounds__(96, 8) ls3d_zline_fast_kernel(const Ls3dRep* _
                                                             int guard_cap) {
   ls3d_zline_fast_entry<T, IN_SPEC, FINAL>(reps, st, map, loc, partials, rep_counter, ctl, cond, use_cond, guard_cap);
 }
-template <bool IN_SPEC, bool FINAL>
+template <bool IN_SPEC, bool FINAL, int LAW = 0>  // LAW 1: the secant law
 __global__ void __launch_bounds__(96, 5) ls3d_zline_fast64_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
                                                                 const int* __restrict__ map, const int* __restrict__ loc,
                                                                 double* partials, unsigned int* rep_counter,
                                                                 Ls3dCtl* ctl, cudaGraphConditionalHandle cond,
                                                                 int use_cond, int guard_cap) {
-  ls3d_zline_fast_entry<double, IN_SPEC, FINAL>(reps, st, map, loc, partials, rep_counter, ctl, cond, use_cond,
-                                                guard_cap);
+  ls3d_zline_fast_entry<double, IN_SPEC, FINAL, LAW>(reps, st, map, loc, partials, rep_counter, ctl, cond,
+                                                     use_cond, guard_cap);
 }
 
 template <typename T, int AXIS, int SIGN, int NL, int NC>
@@ -885,6 +911,7 @@ __global__ void ls3d_phase2_kernel(Ls3dState* st, const int* sel, int nsel, Ls3d
 }
 
 // outputs (nx,ny,nz,3,3) and partial sums for the means; grid (G, nsel)
+template <int LAW = 0>  // 1: the secant law
 __global__ void ls3d_output_kernel(const Ls3dRep* reps, const Ls3dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
   const int r = sel[blockIdx.y];
@@ -913,9 +940,13 @@ __global__ void ls3d_output_kernel(const Ls3dRep* reps, const Ls3dState* st, con
       p[2] = p[6] = R.ep[4 * N + i];
       p[1] = p[3] = R.ep[5 * N + i];
     }
-    const double mu = R.mu[i], lam = R.lam[i];
+    double mu = R.mu[i];
+    const double lam = R.lam[i];
     double d[9];
     for (int q = 0; q < 9; ++q) d[q] = e[q] - p[q];
+    if constexpr (LAW == 1)
+      mu = secant_mu3(mu, d[0], d[4], d[8], 0.5 * (d[5] + d[7]), 0.5 * (d[2] + d[6]), 0.5 * (d[1] + d[3]),
+                      R.law_a, R.law_b);
     const double tr = d[0] + d[4] + d[8];
     double sg[9];
     for (int q = 0; q < 9; ++q) sg[q] = 2 * mu * d[q] + ((q % 4) == 0 ? lam * tr : 0.0);
@@ -979,6 +1010,7 @@ struct mgk_ls3d_plan {
   cudaGraphExec_t exec = nullptr;
   int graph_mode = -1, graph_cap = 0;
   int nsel = 0, s_zl = 0, s_y = 0, s_x = 0;
+  int law = 0;  // 1: secant degradation law (mgk_ls3d_set_secant)
 };
 
 static int a3(mgk_ls3d_t p, void** ptr, size_t bytes) {
@@ -1098,6 +1130,8 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
   if (p->fast &&
       (raise_smem((const void*)ls3d_zline_fast64_kernel<true, true>, (int)p->zl_smem) ||
        raise_smem((const void*)ls3d_zline_fast64_kernel<false, true>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast64_kernel<true, true, 1>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast64_kernel<false, true, 1>, (int)p->zl_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, -1>, (int)p->ax_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, 1>, (int)p->ax_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 0, 0>, (int)p->ax_smem) ||
@@ -1177,7 +1211,7 @@ static int set3(mgk_ls3d_t p, int rep, const double* E, const double* nu, const 
   ls3d_material_kernel<<<G, kT3, 0, s>>>(p->d_reps, rep, E, nu, epsp, set_moduli, p->d_mat_part);
   MGK_CUDA(cudaGetLastError());
   if (set_moduli) {
-    ls3d_medium_kernel<<<1, kT3, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, G);
+    ls3d_medium_kernel<<<1, kT3, 0, s>>>(p->d_reps, p->d_st, rep, p->d_mat_part, G, set_moduli == 2);
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
@@ -1189,6 +1223,29 @@ extern "C" int mgk_ls3d_set_material_rep(mgk_ls3d_t p, int rep, const double* E,
   int st = set3(p, rep, E, nu, epsp, 1, (cudaStream_t)stream);
   if (st == MGK_OK) p->has_material[rep] = 1;
   return st;
+}
+
+extern "C" int mgk_ls3d_set_lame_rep(mgk_ls3d_t p, int rep, const double* lam, const double* mu,
+                                     const double* epsp, mgk_stream_t stream) {
+  MGK_REQUIRE(p && lam && mu && rep >= 0 && rep < p->nrep, "mgk_ls3d_set_lame: bad argument");
+  int st = set3(p, rep, lam, mu, epsp, 2, (cudaStream_t)stream);
+  if (st == MGK_OK) p->has_material[rep] = 1;
+  return st;
+}
+
+// every replica to the secant law (d > 0) or back to the linear law; cached
+// loop graphs hold the previous law's z-line kernel and are dropped
+extern "C" int mgk_ls3d_set_secant(mgk_ls3d_t p, double d, double k) {
+  MGK_REQUIRE(p, "mgk_ls3d_set_secant: null plan");
+  MGK_REQUIRE(d >= 0.0 && d <= 1.0 && k >= 0.0 && isfinite(k), "mgk_ls3d_set_secant: need 0 <= d <= 1, k >= 0");
+  MGK_REQUIRE(d == 0.0 || p->prec == MGK_FP64, "mgk_ls3d_set_secant: the secant law runs in FP64 plans only");
+  const int law = d != 0.0 ? 1 : 0;
+  for (auto& R : p->reps) { R.law = law; R.law_a = d; R.law_b = k; }
+  if (law != p->law) {
+    if (p->graph_mode == 1) p->graph_mode = -1;
+    p->law = law;
+  }
+  return MGK_OK;
 }
 
 extern "C" int mgk_ls3d_set_eigenstrain_rep(mgk_ls3d_t p, int rep, const double* epsp, mgk_stream_t stream) {
@@ -1211,11 +1268,14 @@ struct Loop3 {
   size_t zs32, as32;
   const int* sel;
   int nsel, G;
+  int law;
 };
 
 // kernels of one iteration: `f32` selects the FP32 phase of a mixed plan
 // (warp-line kernels only; its decisions end phase 1, not the solve)
-static void* zline_fn(int fast, bool in_spec, bool f32 = false) {
+static void* zline_fn(int fast, bool in_spec, bool f32 = false, int law = 0) {
+  if (fast && !f32 && law == 1)
+    return in_spec ? (void*)ls3d_zline_fast64_kernel<true, true, 1> : (void*)ls3d_zline_fast64_kernel<false, true, 1>;
   if (fast && f32)
     return in_spec ? (void*)ls3d_zline_fast_kernel<float, true, false> : (void*)ls3d_zline_fast_kernel<float, false, false>;
   if (fast)
@@ -1242,7 +1302,7 @@ static int body3(const Loop3& a, cudaStream_t s, bool f32 = false) {
   MGK_CUDA(cudaLaunchKernel(axis_fn<1, -1>(a.fast, f32), gy, aby, ay, asy, s));
   MGK_CUDA(cudaLaunchKernel(axis_fn<0, 0>(a.fast, f32), dim3(a.nx), ab, ax, as, s));
   MGK_CUDA(cudaLaunchKernel(axis_fn<1, 1>(a.fast, f32), gy, aby, ay, asy, s));
-  MGK_CUDA(cudaLaunchKernel(zline_fn(a.fast, true, f32), dim3(a.nzl), zb, az, zs, s));
+  MGK_CUDA(cudaLaunchKernel(zline_fn(a.fast, true, f32, a.law), dim3(a.nzl), zb, az, zs, s));
   return MGK_OK;
 }
 
@@ -1282,7 +1342,7 @@ static int add_while3(cudaGraph_t g, const cudaGraphNode_t* dep, Loop3& a, bool 
   cudaError_t e = add(axis_fn<1, -1>(a.fast, f32), gy, asy, ay, aby);
   if (!e) e = add(axis_fn<0, 0>(a.fast, f32), dim3(a.nx), as, ax, ab);
   if (!e) e = add(axis_fn<1, 1>(a.fast, f32), gy, asy, ay, aby);
-  if (!e) e = add(zline_fn(a.fast, true, f32), dim3(a.nzl), zs, az, zb);
+  if (!e) e = add(zline_fn(a.fast, true, f32, a.law), dim3(a.nzl), zs, az, zb);
   return e ? MGK_CUDA_ERROR : MGK_OK;
 }
 
@@ -1404,14 +1464,14 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
   }
   if (n_active > 0) {
     Loop3 a{p->d_reps, p->d_st, d_zm, d_zl, d_ym, d_yl, d_xm, d_xl, p->d_part, p->d_repctr, p->d_ctl,
-            nzl, ny_, nx_, p->zl_smem, p->ax_smem, p->fast, p->zl_smem32, p->ax_smem32, d_sel, nsel, G};
+            nzl, ny_, nx_, p->zl_smem, p->ax_smem, p->fast, p->zl_smem32, p->ax_smem32, d_sel, nsel, G, p->law};
     const bool mixed = p->prec == MGK_MIXED;
     {
       cudaGraphConditionalHandle h0 = 0;
       int zero = 0;
       void* az0[] = {(void*)&p->d_reps, (void*)&p->d_st, (void*)&d_zm, (void*)&d_zl, (void*)&p->d_part,
                      (void*)&p->d_repctr, (void*)&p->d_ctl, &h0, &zero, &zero};
-      MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false, mixed), dim3(nzl), dim3(p->fast ? 96 : kT3), az0,
+      MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false, mixed, p->law), dim3(nzl), dim3(p->fast ? 96 : kT3), az0,
                                 mixed ? p->zl_smem32 : p->zl_smem, s));
     }
     const int cap = max_iter + 2 > 1000 ? max_iter + 2 : 1000;
@@ -1435,7 +1495,7 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
           int zero = 0;
           void* az1[] = {(void*)&p->d_reps, (void*)&p->d_st, (void*)&d_zm, (void*)&d_zl, (void*)&p->d_part,
                          (void*)&p->d_repctr, (void*)&p->d_ctl, &h0, &zero, &zero};
-          MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false, false), dim3(nzl), dim3(96), az1, p->zl_smem, s));
+          MGK_CUDA(cudaLaunchKernel(zline_fn(p->fast, false, false, p->law), dim3(nzl), dim3(96), az1, p->zl_smem, s));
         }
         for (int it = 0; it < max_iter; ++it) {
           rc = body3(a, s, phase == 1);
@@ -1448,7 +1508,10 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
       }
     }
   }
-  ls3d_output_kernel<<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  if (p->law == 1)
+    ls3d_output_kernel<1><<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  else
+    ls3d_output_kernel<0><<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());
   ls3d_finalize_kernel<<<nsel, kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 18,
                                             (int)offsetof(Ls3dState, out_eps_mean), 0);

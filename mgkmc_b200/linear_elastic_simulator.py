@@ -329,6 +329,17 @@ class Ls3dBatch:
         L.check(L.lib().mgk_ls3d_set_material_rep(self._h, int(rep), L.ptr(E), L.ptr(nu), L.ptr(eps_plastic),
                                                   L.stream_ptr(stream)), "mgk_ls3d_set_material")
 
+    def set_lame(self, rep, lam, mu, eps_plastic=None, stream=None):
+        """Lame fields given directly, medium (mean lam, mean mu): the secant
+        solver's inputs (linear_elastic_simulator.py:768-784)."""
+        self._keep[("m", rep)] = (lam, mu, eps_plastic)
+        L.check(L.lib().mgk_ls3d_set_lame_rep(self._h, int(rep), L.ptr(lam), L.ptr(mu), L.ptr(eps_plastic),
+                                              L.stream_ptr(stream)), "mgk_ls3d_set_lame")
+
+    def set_secant(self, d, k):
+        """Secant degradation law for every replica (0 < d <= 1; d = 0 linear)."""
+        L.check(L.lib().mgk_ls3d_set_secant(self._h, float(d), float(k)), "mgk_ls3d_set_secant")
+
     def set_eigenstrain(self, rep, eps_plastic, stream=None):
         self._keep[("e", rep)] = eps_plastic
         L.check(L.lib().mgk_ls3d_set_eigenstrain_rep(self._h, int(rep), L.ptr(eps_plastic), L.stream_ptr(stream)),
@@ -378,6 +389,37 @@ def spectral_solver_3d(E, nu, eps_bar, eps_plastic=None, max_iter=200, tol=1e-6,
         print(f"LS 3D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
     e, s = eps.cpu().numpy(), sig.cpu().numpy()
     return e, s, e.mean(axis=(0, 1, 2)), s.mean(axis=(0, 1, 2))
+
+
+_PLANS3_SECANT = {}
+
+
+def spectral_solver_secant_3d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, verbose=False,
+                              pixel=1.0, Gamma=None, eps_init=None):
+    """Nonlinear 3D Lippmann-Schwinger solve with the secant degradation law
+    (linear_elastic_simulator.py:768-850): sigma = lam tr(e) I + 2 mu_sec e,
+    e = eps - eps_plastic, mu_sec = mu (1 - d (1 - exp(-k eps_eq(e)))), the
+    reference medium (mean lam, mean mu) held fixed.  Returns
+    (eps, sig, eps.mean(axis=(0,1,2)), sig.mean(axis=(0,1,2)))."""
+    torch = _torch()
+    lam = np.array(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
+    mu = np.array(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
+    shape = lam.shape
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (shape, dev.index)
+    p = _PLANS3_SECANT.get(key)
+    if p is None:
+        p = _PLANS3_SECANT[key] = Ls3dBatch([shape])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    eps = torch.empty(shape + (3, 3), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
+    p.set_secant(d, k)
+    info = p.solve([0], [eps_bar], [eps], [sig], None if eps_init is None else [t(eps_init)], max_iter, tol)[0]
+    if verbose:
+        print(f"secant LS 3D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
+    e, s_ = eps.cpu().numpy(), sig.cpu().numpy()
+    return e, s_, e.mean(axis=(0, 1, 2)), s_.mean(axis=(0, 1, 2))
 
 
 def update_stress_fft_full(eps_plastic_field, eps_macro, E, nu, pixel=1.0, max_iter=200, tol=1e-6, verbose=False):

@@ -176,6 +176,56 @@ def spectral_solver_secant_2d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
     return out + (it_done, diff) if return_info else out
 
 
+def von_mises_strain_3d(e):
+    """sqrt(2/3 e':e') (mgkmc/elasticity.py:665-700)."""
+    tr3 = (e[..., 0, 0] + e[..., 1, 1] + e[..., 2, 2]) / 3.0
+    return np.sqrt((2.0 / 3.0) * ((e[..., 0, 0] - tr3) ** 2 + (e[..., 1, 1] - tr3) ** 2
+                                  + (e[..., 2, 2] - tr3) ** 2
+                                  + 0.5 * ((e[..., 0, 1] + e[..., 1, 0]) ** 2 + (e[..., 0, 2] + e[..., 2, 0]) ** 2
+                                           + (e[..., 1, 2] + e[..., 2, 1]) ** 2)))
+
+
+def secant_stress_3d(e, lam, mu, d, k):
+    """lam tr(e) I + 2 mu (1 - d (1 - exp(-k eq(e)))) e
+    (mgkmc/elasticity.py:261-295, :703-728)."""
+    mu_sec = mu * (1.0 - d * (1.0 - np.exp(-k * von_mises_strain_3d(e))))
+    return hooke(e, lam, mu_sec, 3)
+
+
+def spectral_solver_secant_3d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
+                              eps_init=None, return_info=False):
+    """Secant-degradation LS fixed point in 3D (mgkmc/linear_elastic_simulator.py:
+    768-850): reference medium (mean lam, mean mu) fixed; tau = sigma_sec(eps
+    - eps_p) - C0:eps; the linear solver's Green step, update and stopping
+    rule."""
+    lam0, mu0 = float(np.mean(lam)), float(np.mean(mu))
+    shape = np.shape(lam)
+    axes = (0, 1, 2)
+    G = green_operator(wave_vectors(shape, pixel), lam0, mu0)
+    if eps_init is not None:
+        eps = eps_init.copy()
+        eps += eps_bar - eps_init.mean(axis=axes)
+    else:
+        eps = np.broadcast_to(eps_bar, shape + (3, 3)).copy()
+    ep = eps_plastic
+    it_done, diff = 0, np.inf
+    for it in range(max_iter):
+        sig = secant_stress_3d(eps - ep if ep is not None else eps, lam, mu, d, k)
+        tau = sig - hooke(eps, lam0, mu0, 3)
+        tau_hat = np.fft.fftn(tau, axes=axes, norm="ortho")
+        et = np.fft.ifftn(-np.einsum("xyzkhij,xyzij->xyzkh", G, tau_hat), axes=axes, norm="ortho").real
+        et -= et.mean(axis=axes)
+        eps_new = eps_bar + et
+        diff = np.linalg.norm(eps_new - eps) / (np.linalg.norm(eps) + 1e-20)
+        eps = eps_new
+        it_done = it + 1
+        if diff < tol:
+            break
+    sig_out = secant_stress_3d(eps - ep if ep is not None else eps, lam, mu, d, k)
+    out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
+    return out + (it_done, diff) if return_info else out
+
+
 def rose_stress_2d(e, lam, mu, eta, floor_f=0.1, plane_mode="plane_strain"):
     """Rose secant-modulus stress (mgkmc/elasticity.py:868-944): G = max(mu
     exp(-eta eq), floor mu), K = lam + 2 mu / 3 kept; plane stress: eps_zz by

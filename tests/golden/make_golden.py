@@ -258,6 +258,29 @@ def ls2d_secant_fixtures():
     save("ls2d_secant_24x16", **out)
 
 
+def ls3d_secant_fixtures():
+    """The reference's 3D secant-degradation LS solver (spectral_solver_secant_3d)
+    on a heterogeneous medium with eigenstrains, cold and warm starts."""
+    rng = np.random.default_rng(67)
+    shape = (12, 8, 6)
+    E, nu = W.ls3d_material(*shape, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    ep = W.pure_shear_eigenstrain_3d(*shape, rng, frac=0.1)
+    eb = np.zeros((3, 3))
+    eb[0, 0], eb[1, 1] = 0.015, -0.004
+    eb[0, 2] = eb[2, 0] = 0.003
+    out = dict(lam=lam, mu=mu, eps_plastic=ep, eps_bar=eb)
+    for tag, d, k in (("a", 0.3, 50.0), ("b", 0.8, 200.0)):
+        e, s, _, _ = LES.spectral_solver_secant_3d(lam, mu, d, k, eb, eps_plastic=ep, max_iter=500, tol=1e-12)
+        out.update({f"eps_{tag}": e, f"sig_{tag}": s, f"d_{tag}": d, f"k_{tag}": k})
+    init = out["eps_a"] + 1e-4 * rng.standard_normal(out["eps_a"].shape)
+    e, s, _, _ = LES.spectral_solver_secant_3d(lam, mu, 0.3, 50.0, eb * 1.1, eps_plastic=ep, max_iter=500,
+                                               tol=1e-12, eps_init=init)
+    out.update(eps_init=init, eps_warm=e, sig_warm=s)
+    save("ls3d_secant_12x8x6", **out)
+
+
 def ls2d_rose_fixtures():
     """The reference's Rose-law LS solver (spectral_solver_rose_2d), plane
     strain and plane stress, with the 3D Lame lambda as its KMC driver passes."""
@@ -314,3 +337,4 @@ if __name__ == "__main__":
     ls2d_rose_fixtures()
     kmc2d_cascade_fixtures()
     kmc2d_patch_fixtures()
+    ls3d_secant_fixtures()

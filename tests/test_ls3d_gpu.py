@@ -131,3 +131,45 @@ def test_mixed_precision_matches_fp64(sizes):
         res[prec] = [(o.cpu().numpy(), g.cpu().numpy()) for o, g in zip(outs, sigs)]
     for (e64, s64), (e32, s32) in zip(res["fp64"], res["mixed"]):
         assert rel(e32, e64) < 1e-6 and rel(s32, s64) < 1e-6
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "warm"])
+def test_golden_secant(golden, tag):
+    # 3D secant-degradation law (CTA-wide passes at 12 x 8 x 6) against the reference
+    from mgkmc_b200.linear_elastic_simulator import spectral_solver_secant_3d
+    g = golden("ls3d_secant_12x8x6")
+    if tag == "warm":
+        eps, sig, _, sm = spectral_solver_secant_3d(g["lam"], g["mu"], 0.3, 50.0, g["eps_bar"] * 1.1,
+                                                    g["eps_plastic"], max_iter=500, tol=1e-12,
+                                                    eps_init=g["eps_init"])
+    else:
+        eps, sig, _, sm = spectral_solver_secant_3d(g["lam"], g["mu"], float(g[f"d_{tag}"]), float(g[f"k_{tag}"]),
+                                                    g["eps_bar"], g["eps_plastic"], max_iter=500, tol=1e-12)
+    assert rel(eps, g[f"eps_{tag}"]) < TOL
+    assert rel(sig, g[f"sig_{tag}"]) < TOL
+    assert np.allclose(sm, g[f"sig_{tag}"].mean(axis=(0, 1, 2)), rtol=1e-9, atol=1e-3)
+
+
+@pytest.mark.parametrize("shape,d,k", [((64, 64, 64), 0.5, 100.0), ((32, 24, 16), 0.8, 200.0),
+                                       ((32, 24, 16), 0.0, 10.0)])
+def test_secant_against_oracle(shape, d, k):
+    # warp-line FP64 kernels (64^3) and the CTA-wide passes with the secant law,
+    # against the oracle; d = 0 is Hooke's law with the (mean lam, mean mu) medium
+    from mgkmc_b200.linear_elastic_simulator import spectral_solver_secant_3d
+    rng = np.random.default_rng(sum(shape) + int(k))
+    E, nu = W.ls3d_material(*shape, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    ep = W.pure_shear_eigenstrain_3d(*shape, rng, frac=0.1)
+    eb = np.zeros((3, 3)); eb[0, 0] = 0.02; eb[1, 1] = -0.005; eb[0, 1] = 0.004; eb[1, 0] = 0.001
+    o = OL.spectral_solver_secant_3d(lam, mu, d, k, eb, ep, max_iter=500, tol=1e-10)
+    eps, sig, _, _ = spectral_solver_secant_3d(lam, mu, d, k, eb, ep, max_iter=500, tol=1e-10)
+    assert rel(eps, o[0]) < TOL and rel(sig, o[1]) < TOL
+
+
+def test_secant_refused_on_mixed_plans():
+    from mgkmc_b200 import _lib as L
+    from mgkmc_b200.linear_elastic_simulator import Ls3dBatch
+    b = Ls3dBatch([(64, 64, 64)], precision="mixed")
+    with pytest.raises(L.MgkError):
+        b.set_secant(0.5, 100.0)

@@ -57,6 +57,22 @@ def test_ls2d_secant_warm(golden):
     assert rel(sig, g["sig_warm"]) < 1e-12
 
 
+@pytest.mark.parametrize("tag", ["a", "b", "warm"])
+def test_ls3d_secant(golden, tag):
+    # the 3D secant-degradation LS restatement against the reference's solver
+    g = golden("ls3d_secant_12x8x6")
+    if tag == "warm":
+        eps, sig, _, _ = OL.spectral_solver_secant_3d(g["lam"], g["mu"], 0.3, 50.0, g["eps_bar"] * 1.1,
+                                                      g["eps_plastic"], max_iter=500, tol=1e-12,
+                                                      eps_init=g["eps_init"])
+    else:
+        eps, sig, _, _ = OL.spectral_solver_secant_3d(g["lam"], g["mu"], float(g[f"d_{tag}"]),
+                                                      float(g[f"k_{tag}"]), g["eps_bar"], g["eps_plastic"],
+                                                      max_iter=500, tol=1e-12)
+    assert rel(eps, g[f"eps_{tag}"]) < 1e-12
+    assert rel(sig, g[f"sig_{tag}"]) < 1e-12
+
+
 @pytest.mark.parametrize("tag,pm", [("ps", "plane_strain"), ("pst", "plane_stress")])
 def test_ls2d_rose(golden, tag, pm):
     # the Rose-law LS restatement against the reference's solver
