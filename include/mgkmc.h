@@ -105,6 +105,30 @@ MGK_API int mgk_ls2d_set_secant(mgk_ls2d_t plan, double d, double k);
  * (mean mu + floor_fraction mean mu) / 2): call before mgk_ls2d_set_lame_rep.
  * Macro strain, eigenstrain and warm start must be symmetric; FP64 plans. */
 MGK_API int mgk_ls2d_set_rose(mgk_ls2d_t plan, double eta, double floor_fraction, int plane_stress);
+/* The Landau small-strain law of spectral_solver_landau_2d, plane strain
+ * (linear_elastic_simulator.py:952-1228; elasticity.py:487-639 with e33 = 0)
+ * for every replica: v = (v1, v2, v3, g1, g2, g3, g4); capping 0 none,
+ * 1 piecewise, 2 smooth (tanh of power smooth_power) at the equivalent
+ * strain e_cap with tangent 2 tangent_ratio mu.  Medium (mean lam, mean mu):
+ * give the material with mgk_ls2d_set_lame_rep.  Symmetric strains; FP64
+ * plans only.  A solve runs the basic scheme; Anderson mixing of its iterates
+ * is mgk_aa_update / mgk_aa_mix between one-iteration solves. */
+MGK_API int mgk_ls2d_set_landau(mgk_ls2d_t plan, const double* v, int capping, double e_cap, double tangent_ratio,
+                                double smooth_power);
+/* Type-II Anderson mixing (linear_elastic_simulator.py:1185-1209) of
+ * fixed-point iterates x -> g = G(x), fields of n doubles, history depth
+ * 1 <= m <= 8.  hist: (2m + 2) n doubles (dF columns, dG columns, f_prev,
+ * g_prev).  mgk_aa_update forms f = g - x; with have_prev, column `slot`
+ * becomes dF = f - f_prev, dG = g - g_prev; f, g become the previous pair;
+ * dots (16 doubles, device) receive <dF_j, dF_slot> at j and <dF_j, f> at
+ * 8 + j for j < ncols.  The caller solves the ncols x ncols least-squares
+ * system; mgk_aa_mix writes x = g - sum_j gamma_j dG_j (gamma on the host).
+ * work: mgk_aa_work_bytes bytes of device memory. */
+MGK_API int64_t mgk_aa_work_bytes(int64_t n);
+MGK_API int mgk_aa_update(int64_t n, const double* x, const double* g, double* hist, int m, int slot, int have_prev,
+                          int ncols, double* dots, void* work, mgk_stream_t stream);
+MGK_API int mgk_aa_mix(int64_t n, const double* g, const double* hist, int m, int ncols, const double* gamma,
+                       double* x, mgk_stream_t stream);
 /* Update only the eigenstrain field (KMC flips). */
 MGK_API int mgk_ls2d_set_eigenstrain(mgk_ls2d_t plan, const double* eps_plastic, mgk_stream_t stream);
 MGK_API int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t plan, int rep, const double* eps_plastic,

@@ -68,9 +68,12 @@ struct Ls2dRep {
   long long N;
   // constitutive law: 0 linear (elasticity.py:12-18); 1 secant degradation
   // (law_a = d, law_b = k); 2 Rose (law_a = eta, law_b = floor fraction,
-  // law_ps = 1 for plane stress)
+  // law_ps = 1 for plane stress); 3 Landau, plane strain (lp: v1, v2, v3,
+  // g1, g2, g3, g4, capping 0 none / 1 piecewise / 2 smooth, E_cap, tangent
+  // ratio, smooth power)
   int law, law_ps;
   double law_a, law_b;
+  double lp[11];
   FftLen fx64, fy64, fx32, fy32;
   double* mu;
   double* lam;
@@ -195,12 +198,70 @@ __device__ __forceinline__ double rose_moduli(double l, double m, double dxx, do
   return dxx + dyy + ezz;
 }
 
+// Landau small-strain stress, plane strain (elasticity.py:487-639 with
+// e33 = 0), parameters lp as in Ls2dRep; a12, a21 the two shear entries of
+// the elastic strain.  With capping on, every voxel's strain goes through the
+// capped form f (a - m) + m, as in the reference.
+__device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, double a22, double a12, double a21,
+                                             const double* __restrict__ lp, double& s11, double& s22, double& s12,
+                                             double& s21) {
+  const double v1 = lp[0], v2 = lp[1], v3 = lp[2], g1 = lp[3], g2 = lp[4], g3 = lp[5], g4 = lp[6];
+  const int cap = (int)lp[7];
+  double c11 = a11, c22 = a22, c12 = a12, c21 = a21, c33 = 0.0, w = 0.0;
+  if (cap) {
+    const double m3 = (a11 + a22 + 0.0) / 3.0;
+    const double d11 = a11 - m3, d22 = a22 - m3, d33 = 0.0 - m3;
+    const double Ecap = lp[8];
+    const double Eeq = sqrt(fmax(0.0, (2.0 / 3.0) * (d11 * d11 + d22 * d22 + d33 * d33 + 2.0 * a12 * a21)));
+    double f = 1.0;
+    if (cap == 2) {
+      const double pw = lp[10];
+      if (Eeq > 1e-12) f = (Ecap / Eeq) * pow(tanh(fmin(100.0, pow(Eeq / Ecap, pw))), 1.0 / pw);
+      const double t = tanh(fmin(100.0, pow(Eeq / Ecap, pw)));
+      w = t * t;
+    } else if (Eeq > Ecap) {
+      f = Ecap / Eeq;
+      w = 1.0;
+    }
+    c11 = f * d11 + m3;
+    c22 = f * d22 + m3;
+    c12 = f * a12;
+    c21 = f * a21;
+    c33 = f * d33 + m3;
+  }
+  const double I1 = c11 + c22 + c33;
+  const double cross = c12 * c21;
+  const double tr2 = c11 * c11 + c22 * c22 + 2.0 * cross;
+  const double I2 = tr2 + c33 * c33;
+  const double t_ip = c11 + c22;
+  const double I3 = t_ip * (tr2 - (c11 * c22 - cross)) + c33 * c33 * c33;
+  const double cI = lam * I1 + 0.5 * v1 * (I1 * I1) + v2 * I2 + (1.0 / 6.0) * g1 * (I1 * I1 * I1) + g2 * I1 * I2 +
+                    (4.0 / 3.0) * g3 * I3;
+  const double ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * (I1 * I1) + g4 * I2);
+  const double ce2 = 4.0 * (v3 + g3 * I1);
+  s11 = cI + ce * c11 + ce2 * (c11 * c11 + cross);
+  s22 = cI + ce * c22 + ce2 * (c22 * c22 + cross);
+  s12 = ce * c12 + ce2 * (c12 * t_ip);
+  s21 = ce * c21 + ce2 * (c21 * t_ip);
+  if (cap) {
+    const double r = 2.0 * (lp[9] * mu) * w;
+    s11 += r * (a11 - c11);
+    s22 += r * (a22 - c22);
+    s12 += r * (a12 - c12);
+    s21 += r * (a21 - c21);
+  }
+}
+
 // stress of the elastic strain (dxx, dyy, dxy) under law LAW; m, l the voxel's
 // mu, lambda; LAW 0 is Hooke's law with the reference's operation order
 template <int LAW>
 __device__ __forceinline__ void law_sigma(double m, double l, double dxx, double dyy, double dxy, double a, double b,
-                                          int ps, double& sxx, double& syy, double& sxy) {
-  if constexpr (LAW == 2) {
+                                          int ps, double& sxx, double& syy, double& sxy,
+                                          const double* __restrict__ lp = nullptr) {
+  if constexpr (LAW == 3) {
+    double syx;
+    landau_sigma(m, l, dxx, dyy, dxy, dxy, lp, sxx, syy, sxy, syx);
+  } else if constexpr (LAW == 2) {
     double G, le;
     const double tr = rose_moduli(l, m, dxx, dyy, dxy, a, b, ps, G, le);
     sxx = le * tr + 2.0 * G * dxx;
@@ -546,6 +607,7 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
       double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
       if (sizeof(TS) == 8 && law == 1) law_sigma<1>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
       else if (sizeof(TS) == 8 && law == 2) law_sigma<2>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+      else if (sizeof(TS) == 8 && law == 3) law_sigma<3>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2, R.lp);
       else law_sigma<0>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2);
       tr[h][0] = (TC)(s0 - (2 * mu0 * e[0] + lam0 * tre));
       tr[h][1] = (TC)(s1 - (2 * mu0 * e[1] + lam0 * tre));
@@ -725,6 +787,7 @@ __global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __r
           double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
           if (sizeof(TS) == 8 && law == 1) law_sigma<1>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
           else if (sizeof(TS) == 8 && law == 2) law_sigma<2>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+          else if (sizeof(TS) == 8 && law == 3) law_sigma<3>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2, R.lp);
           else law_sigma<0>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2);
           tr[h][0] = (TC)(s0 - (2 * mu0 * e0 + lam0 * tre));
           tr[h][1] = (TC)(s1 - (2 * mu0 * e1 + lam0 * tre));
@@ -984,8 +1047,8 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
       }
       const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
       const double tre = e0 + e1;
-      double s0, s1, s2;  // LAW 0 linear; 1 secant, 2 Rose (FP64 plans)
-      law_sigma<LAW>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
+      double s0, s1, s2;  // LAW 0 linear; 1 secant, 2 Rose, 3 Landau (FP64 plans)
+      law_sigma<LAW>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2, R.lp);
       tr[h][0] = (T)(s0 - (2 * mu0 * e0 + lam0 * tre));
       tr[h][1] = (T)(s1 - (2 * mu0 * e1 + lam0 * tre));
       tr[h][2] = (T)(s2 - 2 * mu0 * e2);
@@ -1182,7 +1245,7 @@ __global__ void ls2d_phase2_kernel(Ls2dState* st, const int* sel, int nsel, Ls2d
 // Outputs in the reference layout: eps, sig (nx,ny,2,2) and partial sums of
 // their components for the means (linear_elastic_simulator.py:83-88).
 // grid = (G, nsel).
-template <int LAW = 0>  // 1: the secant law, 2: the Rose law
+template <int LAW = 0>  // 1: the secant law, 2: the Rose law, 3: the Landau law
 __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
   const int r = sel[blockIdx.y];
@@ -1208,7 +1271,9 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
     const double dxx = exx - pxx, dxy = exy - pxy, dyx = eyx - pyx, dyy = eyy - pyy;
     double mu = R.mu[i];
     double sxx, syy, sxy2, syx2;
-    if constexpr (LAW == 2) {
+    if constexpr (LAW == 3) {
+      landau_sigma(mu, lam, dxx, dyy, dxy, dyx, R.lp, sxx, syy, sxy2, syx2);
+    } else if constexpr (LAW == 2) {
       // Rose: sigma_yx is a copy of sigma_xy, from the [0,1] strain entry
       law_sigma<2>(mu, lam, dxx, dyy, dxy, law_a, law_b, law_ps, sxx, syy, sxy2);
       syx2 = sxy2;
@@ -1228,6 +1293,84 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
   for (int q = 0; q < 8; ++q) {
     double t = block_sum(s[q], red);
     if (threadIdx.x == 0) partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 8 + q] = t;
+  }
+}
+
+// Anderson mixing over fields of n doubles (linear_elastic_simulator.py:
+// 1185-1209), kept as differences: hist holds 2 m + 2 vectors of n doubles,
+// dF columns 0..m-1, dG columns 0..m-1, then f_prev and g_prev.  One pass
+// forms f = g - x, writes column `slot` (dF = f - f_prev, dG = g - g_prev)
+// when a previous pair exists, stores f and g as the previous pair, and
+// accumulates <dF_j, dF_slot> and <dF_j, f> for the ncols valid columns.
+constexpr int kAaMax = 8;
+constexpr int kAaBlocks = 296;
+
+__global__ void __launch_bounds__(256) aa_update_kernel(long long n, const double* __restrict__ x,
+                                                        const double* __restrict__ g, double* __restrict__ hist,
+                                                        int m, int slot, int have_prev, int ncols,
+                                                        double* __restrict__ partials) {
+  __shared__ double red[32];
+  double* dF = hist;
+  double* dG = hist + (size_t)m * n;
+  double* fp = hist + 2 * (size_t)m * n;
+  double* gp = fp + n;
+  double an[kAaMax], ar[kAaMax];
+#pragma unroll
+  for (int j = 0; j < kAaMax; ++j) { an[j] = 0.0; ar[j] = 0.0; }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double gi = g[i], fi = gi - x[i];
+    double df = 0.0;
+    if (have_prev) {
+      df = fi - fp[i];
+      dF[(size_t)slot * n + i] = df;
+      dG[(size_t)slot * n + i] = gi - gp[i];
+    }
+    fp[i] = fi;
+    gp[i] = gi;
+#pragma unroll
+    for (int j = 0; j < kAaMax; ++j)
+      if (j < ncols) {
+        const double c = (j == slot && have_prev) ? df : dF[(size_t)j * n + i];
+        an[j] += c * df;
+        ar[j] += c * fi;
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < kAaMax; ++j)
+    if (j < ncols) {
+      const double a = block_sum(an[j], red);
+      const double b = block_sum(ar[j], red);
+      if (threadIdx.x == 0) {
+        partials[(size_t)blockIdx.x * 2 * kAaMax + j] = a;
+        partials[(size_t)blockIdx.x * 2 * kAaMax + kAaMax + j] = b;
+      }
+    }
+}
+
+// sums the per-block partials: out[j] = <dF_j, dF_slot>, out[kAaMax + j] = <dF_j, f>
+__global__ void aa_sum_kernel(const double* __restrict__ partials, int nb, int ncols, double* __restrict__ out) {
+  __shared__ double red[32];
+  for (int q = 0; q < 2 * kAaMax; ++q) {
+    if ((q % kAaMax) >= ncols) continue;
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) a += partials[(size_t)b * 2 * kAaMax + q];
+    a = block_sum(a, red);
+    if (threadIdx.x == 0) out[q] = a;
+  }
+}
+
+struct AaCoef { double v[kAaMax]; };
+
+// x = g - sum_j gamma_j dG_j
+__global__ void aa_mix_kernel(long long n, const double* __restrict__ g, const double* __restrict__ hist, int m,
+                              int ncols, AaCoef gam, double* __restrict__ x) {
+  const double* dG = hist + (size_t)m * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < kAaMax; ++j)
+      if (j < ncols) s += gam.v[j] * dG[(size_t)j * n + i];
+    x[i] = g[i] - s;
   }
 }
 
@@ -1333,6 +1476,10 @@ static void* row_fast_fn(int fast, int law = 0) {
       return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL, 2>
              : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL, 2>
                           : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL, 2>;
+    if (law == 3)  // the Landau law (FP64 plans only)
+      return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL, 3>
+             : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL, 3>
+                          : (void*)ls2d_row_fast_kernel<TS, 256, IN_SPEC, FINAL, 3>;
   }
   return fast > 512   ? (void*)ls2d_row_fast_kernel<TS, 1024, IN_SPEC, FINAL>
          : fast > 256 ? (void*)ls2d_row_fast_kernel<TS, 512, IN_SPEC, FINAL>
@@ -1347,12 +1494,14 @@ static void* col_fast_fn(int fast) {
 
 template <typename T>
 static int ls2d_set_fast_attrs(int fast, size_t row_smem, size_t col_smem) {
-  void* fns[12] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
+  void* fns[16] = {row_fast_fn<T, true, true>(fast), row_fast_fn<T, false, true>(fast),
                    row_fast_fn<T, true, false>(fast), row_fast_fn<T, false, false>(fast),
                    row_fast_fn<T, true, true>(fast, 1), row_fast_fn<T, false, true>(fast, 1),
                    row_fast_fn<T, true, false>(fast, 1), row_fast_fn<T, false, false>(fast, 1),
                    row_fast_fn<T, true, true>(fast, 2), row_fast_fn<T, false, true>(fast, 2),
-                   row_fast_fn<T, true, false>(fast, 2), row_fast_fn<T, false, false>(fast, 2)};
+                   row_fast_fn<T, true, false>(fast, 2), row_fast_fn<T, false, false>(fast, 2),
+                   row_fast_fn<T, true, true>(fast, 3), row_fast_fn<T, false, true>(fast, 3),
+                   row_fast_fn<T, true, false>(fast, 3), row_fast_fn<T, false, false>(fast, 3)};
   for (void* f : fns) MGK_CUDA(raise_smem((const void*)f, (int)row_smem));
   MGK_CUDA(raise_smem((const void*)col_fast_fn<T>(fast), (int)col_smem));
   return MGK_OK;
@@ -1622,8 +1771,11 @@ extern "C" int mgk_ls2d_set_lame_rep(mgk_ls2d_t p, int rep, const double* lam, c
 
 // switches every replica of the plan to law (a, b, ps); cached loop graphs
 // hold the previous law's row kernel and are dropped
-static int ls2d_set_law(mgk_ls2d_t p, int law, double a, double b, int ps) {
-  for (auto& R : p->reps) { R.law = law; R.law_a = a; R.law_b = b; R.law_ps = ps; }
+static int ls2d_set_law(mgk_ls2d_t p, int law, double a, double b, int ps, const double* lp = nullptr) {
+  for (auto& R : p->reps) {
+    R.law = law; R.law_a = a; R.law_b = b; R.law_ps = ps;
+    for (int q = 0; q < 11; ++q) R.lp[q] = lp ? lp[q] : 0.0;
+  }
   p->law_a = a; p->law_b = b; p->law_ps = ps;
   if (law != p->law) {
     for (auto& e : p->gcache) {
@@ -1653,6 +1805,23 @@ extern "C" int mgk_ls2d_set_rose(mgk_ls2d_t p, double eta, double floor_fraction
               "mgk_ls2d_set_rose: need eta >= 0, 0 <= floor_fraction <= 1");
   MGK_REQUIRE(p->prec == MGK_FP64, "mgk_ls2d_set_rose: the Rose law runs in FP64 plans only");
   return ls2d_set_law(p, 2, eta, floor_fraction, plane_stress ? 1 : 0);
+}
+
+extern "C" int mgk_ls2d_set_landau(mgk_ls2d_t p, const double* v, int capping, double e_cap, double tangent_ratio,
+                                   double smooth_power) {
+  MGK_REQUIRE(p && v, "mgk_ls2d_set_landau: null argument");
+  MGK_REQUIRE(p->prec == MGK_FP64, "mgk_ls2d_set_landau: the Landau law runs in FP64 plans only");
+  MGK_REQUIRE(capping >= 0 && capping <= 2, "mgk_ls2d_set_landau: capping must be 0, 1 or 2");
+  MGK_REQUIRE(!capping || (e_cap > 0.0 && isfinite(e_cap) && isfinite(tangent_ratio) &&
+                           (capping != 2 || (smooth_power > 0.0 && isfinite(smooth_power)))),
+              "mgk_ls2d_set_landau: need e_cap > 0 (and smooth_power > 0 for smooth capping)");
+  double lp[11];
+  for (int q = 0; q < 7; ++q) {
+    MGK_REQUIRE(isfinite(v[q]), "mgk_ls2d_set_landau: non-finite coefficient");
+    lp[q] = v[q];
+  }
+  lp[7] = capping; lp[8] = e_cap; lp[9] = tangent_ratio; lp[10] = smooth_power;
+  return ls2d_set_law(p, 3, 0.0, 0.0, 0, lp);
 }
 
 extern "C" int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t p, int rep, const double* epsp, mgk_stream_t stream) {
@@ -1977,8 +2146,8 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     // the Rose law reads the [0,1] strain entry; the symmetric storage carries it
     // when macro strain and eigenstrain are symmetric (the eigenstrain is the
     // caller's to keep symmetric)
-    MGK_REQUIRE(p->law != 2 || eps_bar[4 * q + 1] == eps_bar[4 * q + 2],
-                "mgk_ls2d_solve: the Rose law needs a symmetric macro strain");
+    MGK_REQUIRE(p->law < 2 || eps_bar[4 * q + 1] == eps_bar[4 * q + 2],
+                "mgk_ls2d_solve: the Rose and Landau laws need a symmetric macro strain");
     seen[r] = 1;
     selv[q] = r;
   }
@@ -2110,6 +2279,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   }
   if (p->law == 1) ls2d_output_kernel<1><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   else if (p->law == 2) ls2d_output_kernel<2><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  else if (p->law == 3) ls2d_output_kernel<3><<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   else ls2d_output_kernel<<<dim3(G, nsel), kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());
   ls2d_finalize_kernel<<<nsel, kThreads, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part, G, 8,
@@ -2461,5 +2631,45 @@ extern "C" int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const doub
     set_error("mgk_ls2d_solve_noalloc: non-finite residual at iteration %d", h.iter);
     return MGK_NONFINITE;
   }
+  return MGK_OK;
+}
+
+extern "C" int64_t mgk_aa_work_bytes(int64_t n) {
+  (void)n;
+  return (int64_t)sizeof(double) * kAaBlocks * 2 * kAaMax;
+}
+
+extern "C" int mgk_aa_update(int64_t n, const double* x, const double* g, double* hist, int m, int slot,
+                             int have_prev, int ncols, double* dots, void* work, mgk_stream_t stream) {
+  MGK_REQUIRE(n > 0 && x && g && hist && work && dots, "mgk_aa_update: bad argument");
+  MGK_REQUIRE(m >= 1 && m <= kAaMax && ncols >= 0 && ncols <= m && slot >= 0 && slot < m &&
+                  (!have_prev || slot < ncols),
+              "mgk_aa_update: need 1 <= m <= %d, 0 <= ncols <= m, slot < m (and < ncols with a previous pair)",
+              kAaMax);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = (int)std::min<long long>(kAaBlocks, (n + 255) / 256);
+  double* part = reinterpret_cast<double*>(work);
+  aa_update_kernel<<<nb, 256, 0, s>>>(n, x, g, hist, m, slot, have_prev, ncols, part);
+  MGK_CUDA(cudaGetLastError());
+  if (ncols > 0) {
+    aa_sum_kernel<<<1, 256, 0, s>>>(part, nb, ncols, dots);
+    MGK_CUDA(cudaGetLastError());
+  }
+  return MGK_OK;
+}
+
+extern "C" int mgk_aa_mix(int64_t n, const double* g, const double* hist, int m, int ncols, const double* gamma,
+                          double* x, mgk_stream_t stream) {
+  MGK_REQUIRE(n > 0 && g && hist && x && (ncols == 0 || gamma), "mgk_aa_mix: bad argument");
+  MGK_REQUIRE(m >= 1 && m <= kAaMax && ncols >= 0 && ncols <= m, "mgk_aa_mix: need 1 <= m <= %d, ncols <= m",
+              kAaMax);
+  AaCoef c;
+  for (int j = 0; j < kAaMax; ++j) {
+    c.v[j] = j < ncols ? gamma[j] : 0.0;
+    MGK_REQUIRE(isfinite(c.v[j]), "mgk_aa_mix: non-finite coefficient");
+  }
+  const int nb = (int)std::min<long long>(4 * kAaBlocks, (n + 255) / 256);
+  aa_mix_kernel<<<nb, 256, 0, (cudaStream_t)stream>>>(n, g, hist, m, ncols, c, x);
+  MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

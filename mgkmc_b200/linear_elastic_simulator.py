@@ -89,6 +89,13 @@ class Ls2dBatch:
         L.check(L.lib().mgk_ls2d_set_rose(self._h, float(eta), float(mu_floor_fraction),
                                           1 if plane_mode == "plane_stress" else 0), "mgk_ls2d_set_rose")
 
+    def set_landau(self, v, capping=0, e_cap=0.0, tangent_ratio=0.1, smooth_power=1.0):
+        """Landau law (plane strain) for every replica: v = (v1, v2, v3, g1, g2,
+        g3, g4); capping 0 none, 1 piecewise, 2 smooth at e_cap; FP64 plans."""
+        arr = (ctypes.c_double * 7)(*[float(a) for a in v])
+        L.check(L.lib().mgk_ls2d_set_landau(self._h, ctypes.cast(arr, ctypes.c_void_p), int(capping), float(e_cap),
+                                            float(tangent_ratio), float(smooth_power)), "mgk_ls2d_set_landau")
+
     def solve(self, reps, eps_bars, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True,
               stream=None):
         """Solve replicas ``reps`` (one launch per stage for all of them).
@@ -289,6 +296,112 @@ def spectral_solver_rose_2d(lam, mu, eta, mu_floor_fraction=0.1, eps_bar=None, e
         print(f"Rose LS 2D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
     eps_np = eps.cpu().numpy()
     sig_np = sig.cpu().numpy()
+    return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
+
+
+_PLANS_LANDAU = {}
+
+
+def spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6,
+                              verbose=False, pixel=1.0, plane_mode="plane_strain", Gamma=None, eps_init=None,
+                              strain_capping_enabled=False, strain_capping_limit=None,
+                              strain_capping_tangent_ratio=0.1, strain_capping_type="piecewise",
+                              strain_capping_smooth_power=1.0, solver="dbfft", e33_state=None, anderson_m=5):
+    """Nonlinear 2D Lippmann-Schwinger solve with the Landau small-strain law
+    (linear_elastic_simulator.py:952-1228, solver "dbfft"), plane strain: the
+    basic scheme with the (mean lam, mean mu) medium, each iteration one
+    device solve step, and type-II Anderson mixing of the last anderson_m
+    iterates on the device (the small least-squares problem on the host).
+    Returns (eps, sig, eps.mean(axis=(0,1)), sig.mean(axis=(0,1))); a
+    non-finite update raises FloatingPointError as the reference does.
+    Plane stress, the Newton-CG branch and asymmetric strains are not built
+    (NotImplementedError); anderson_m is limited to 8."""
+    if plane_mode != "plane_strain":
+        raise NotImplementedError("spectral_solver_landau_2d: plane stress is not built (plane strain only)")
+    if solver != "dbfft":
+        raise NotImplementedError("spectral_solver_landau_2d: only the basic scheme (solver='dbfft') is built")
+    m = int(anderson_m)
+    if m < 0 or m > 8:
+        raise NotImplementedError("spectral_solver_landau_2d: anderson_m must be 0..8")
+    torch = _torch()
+    lam = np.array(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
+    mu = np.array(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
+    eps_bar = np.asarray(eps_bar, dtype=np.float64)
+    for a in (eps_bar, eps_plastic, eps_init):
+        if a is not None and not np.array_equal(np.asarray(a)[..., 0, 1], np.asarray(a)[..., 1, 0]):
+            raise NotImplementedError("spectral_solver_landau_2d: asymmetric strain tensors are not supported")
+    cap, e_cap = 0, 0.0
+    if strain_capping_enabled:
+        cap = 2 if strain_capping_type == "smooth" else 1
+        if strain_capping_limit is None or strain_capping_limit <= 0:
+            e_cap = float(np.sqrt(0.2 * mu.mean() / abs(g4))) if g4 < 0 else 999.0
+        else:
+            e_cap = float(strain_capping_limit)
+    nx, ny = lam.shape
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (nx, ny, dev.index)
+    p = _PLANS_LANDAU.get(key)
+    if p is None:
+        p = _PLANS_LANDAU[key] = Ls2dBatch([(nx, ny)])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    p.set_landau((v1, v2, v3, g1, g2, g3, g4), cap, e_cap, strain_capping_tangent_ratio, strain_capping_smooth_power)
+    p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
+    # the iterate x (eps_bar-mean start as in the reference) and its image g
+    if eps_init is None:
+        x = t(np.broadcast_to(eps_bar, (nx, ny, 2, 2)))
+    else:
+        x = t(eps_init)
+        x += t(eps_bar) - x.mean(dim=(0, 1))
+    g = torch.empty_like(x)
+    sig = torch.empty_like(x)
+    n = x.numel()
+    lib = L.lib()
+    if m > 0:
+        hist = torch.empty((2 * m + 2) * n, dtype=torch.float64, device=dev)
+        work = torch.empty(int(lib.mgk_aa_work_bytes(n)), dtype=torch.uint8, device=dev)
+        dots = torch.zeros(16, dtype=torch.float64, device=dev)
+    A = np.zeros((max(m, 1), max(m, 1)))
+    k, slot_next, have_prev = 0, 0, False
+    S = L.stream_ptr(None)
+    info = None
+    for it in range(max_iter):
+        info = p.solve([0], [eps_bar], [g], [sig], eps_init=[x], max_iter=1, tol=tol)[0]
+        if info.status == L.NONFINITE or not np.isfinite(info.final_diff):
+            raise FloatingPointError("spectral_solver_landau_2d: non-finite strain update in LS loop (Landau energy "
+                                     "likely unstable at this strain; consider strain capping or smaller load steps).")
+        if verbose and it % 10 == 0:
+            print(f"  [landau-LS] iter {it:04d}: rel_diff = {info.final_diff:.3e}")
+        if info.final_diff < tol:
+            eps_np, sig_np = g.cpu().numpy(), sig.cpu().numpy()
+            return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
+        if m == 0:
+            x, g = g, x
+            continue
+        slot = slot_next if have_prev else 0
+        if have_prev:
+            slot_next = (slot_next + 1) % m
+            k = min(k + 1, m)
+        L.check(lib.mgk_aa_update(n, L.ptr(x), L.ptr(g), L.ptr(hist), m, slot, int(have_prev), k, L.ptr(dots),
+                                  L.ptr(work), S), "mgk_aa_update")
+        have_prev = True
+        if k == 0:
+            x, g = g, x
+            continue
+        d = dots.cpu().numpy()
+        A[slot, :k] = d[:k]
+        A[:k, slot] = d[:k]
+        gam = np.linalg.lstsq(A[:k, :k], d[8:8 + k], rcond=None)[0]
+        if not np.all(np.isfinite(gam)):
+            # ill-conditioned mix: the plain step, history restarted from the last pair
+            x, g = g, x
+            k, slot_next = 0, 0
+            continue
+        garr = (ctypes.c_double * k)(*gam)
+        L.check(lib.mgk_aa_mix(n, L.ptr(g), L.ptr(hist), m, k, ctypes.cast(garr, ctypes.c_void_p), L.ptr(x), S),
+                "mgk_aa_mix")
+    # not converged: the final stress of the last iterate (reference :1212-1228)
+    p.solve([0], [eps_bar], [g], [sig], eps_init=[x], max_iter=0, tol=tol)
+    eps_np, sig_np = g.cpu().numpy(), sig.cpu().numpy()
     return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
 
 

@@ -226,6 +226,127 @@ def spectral_solver_secant_3d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
     return out + (it_done, diff) if return_info else out
 
 
+def landau_stress_2d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1, cap_power=1.0):
+    """Landau small-strain stress, plane strain (mgkmc/elasticity.py:487-639,
+    e33 = 0): v = (v1, v2, v3, g1, g2, g3, g4).  With cap_type "piecewise" or
+    "smooth" the strain is capped at the equivalent strain E_cap (cap_limit, or
+    sqrt(0.2 mean(mu) / |g4|) when it is None or <= 0 and g4 < 0, else 999)
+    and a tangent 2 cap_ratio mu w (e - e_capped) is added."""
+    v1, v2, v3, g1, g2, g3, g4 = v
+    a11, a22, a12, a21 = e[..., 0, 0], e[..., 1, 1], e[..., 0, 1], e[..., 1, 0]
+    e33 = np.zeros_like(a11)
+    m3 = (a11 + a22 + e33) / 3.0
+    d11, d22, d33 = a11 - m3, a22 - m3, e33 - m3
+    if cap_type is not None:
+        mu_mean = np.mean(mu)
+        E_cap = cap_limit if cap_limit is not None and cap_limit > 0 else (
+            np.sqrt(0.2 * mu_mean / abs(g4)) if g4 < 0 else 999.0)
+        E_eq = np.sqrt(np.maximum(0.0, (2.0 / 3.0) * (d11 * d11 + d22 * d22 + d33 * d33 + 2.0 * a12 * a21)))
+        f = np.ones_like(E_eq)
+        nz = E_eq > 1e-12
+        if cap_type == "smooth":
+            rp = np.minimum(100.0, (E_eq[nz] / E_cap) ** cap_power)
+            f[nz] = (E_cap / E_eq[nz]) * np.tanh(rp) ** (1.0 / cap_power)
+            w = np.tanh(np.minimum(100.0, (E_eq / E_cap) ** cap_power)) ** 2
+        else:
+            capped = E_eq > E_cap
+            np.divide(E_cap, E_eq, out=f, where=capped)
+            w = capped.astype(float)
+        c11, c22, c12, c21, c33 = f * d11 + m3, f * d22 + m3, f * a12, f * a21, f * d33 + m3
+    else:
+        c11, c22, c12, c21, c33 = a11, a22, a12, a21, e33
+    I1 = c11 + c22 + c33
+    cross = c12 * c21
+    tr2 = c11 * c11 + c22 * c22 + 2.0 * cross
+    I2 = tr2 + c33 * c33
+    t_ip = c11 + c22
+    I3 = t_ip * (tr2 - (c11 * c22 - cross)) + c33 ** 3
+    cI = lam * I1 + 0.5 * v1 * I1 ** 2 + v2 * I2 + (1.0 / 6.0) * g1 * I1 ** 3 + g2 * I1 * I2 + (4.0 / 3.0) * g3 * I3
+    ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * I1 ** 2 + g4 * I2)
+    ce2 = 4.0 * (v3 + g3 * I1)
+    sig = np.empty(e.shape)
+    sig[..., 0, 0] = cI + ce * c11 + ce2 * (c11 * c11 + cross)
+    sig[..., 1, 1] = cI + ce * c22 + ce2 * (c22 * c22 + cross)
+    sig[..., 0, 1] = ce * c12 + ce2 * (c12 * t_ip)
+    sig[..., 1, 0] = ce * c21 + ce2 * (c21 * t_ip)
+    if cap_type is not None:
+        r = 2.0 * (cap_ratio * mu) * w
+        sig[..., 0, 0] += r * (a11 - c11)
+        sig[..., 1, 1] += r * (a22 - c22)
+        sig[..., 0, 1] += r * (a12 - c12)
+        sig[..., 1, 0] += r * (a21 - c21)
+    return sig
+
+
+def anderson_step(hist_g, hist_f, g, f, m):
+    """Type-II Anderson mixing of the last m + 1 fixed-point images and
+    residuals (mgkmc/linear_elastic_simulator.py:1185-1209): returns the next
+    iterate and the trimmed history; a non-finite mix gives the plain step
+    and restarts the history from the last pair."""
+    hist_g.append(g.reshape(-1))
+    hist_f.append(f.reshape(-1))
+    if len(hist_f) > m + 1:
+        hist_g.pop(0)
+        hist_f.pop(0)
+    if len(hist_f) < 2:
+        return g, hist_g, hist_f
+    dF = np.stack([hist_f[i + 1] - hist_f[i] for i in range(len(hist_f) - 1)], axis=1)
+    dG = np.stack([hist_g[i + 1] - hist_g[i] for i in range(len(hist_g) - 1)], axis=1)
+    try:
+        gam = np.linalg.lstsq(dF, hist_f[-1], rcond=None)[0]
+        x = hist_g[-1] - dG @ gam
+    except np.linalg.LinAlgError:
+        x = None
+    if x is not None and np.all(np.isfinite(x)):
+        return x.reshape(g.shape), hist_g, hist_f
+    return g, hist_g[-1:], hist_f[-1:]
+
+
+def spectral_solver_landau_2d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
+                              eps_init=None, anderson_m=5, cap_type=None, cap_limit=None, cap_ratio=0.1,
+                              cap_power=1.0, return_info=False):
+    """Landau small-strain LS fixed point, plane strain, the basic scheme
+    with Anderson mixing (mgkmc/linear_elastic_simulator.py:952-1228, solver
+    "dbfft"): medium (mean lam, mean mu) fixed; G(eps) = eps_bar + Gamma0 *
+    (sigma_L(eps - eps_p) - C0:eps) with zero-mean fluctuation; stop when
+    |G(eps) - eps| / |eps| < tol (eps = G(eps)); otherwise mix the history.
+    A non-finite update raises FloatingPointError."""
+    lam0, mu0 = float(np.mean(lam)), float(np.mean(mu))
+    shape = np.shape(lam)
+    axes = (0, 1)
+    G = green_operator(wave_vectors(shape, pixel), lam0, mu0)
+    if eps_init is not None:
+        eps = eps_init.copy()
+        eps += eps_bar - eps_init.mean(axis=axes)
+    else:
+        eps = np.broadcast_to(eps_bar, shape + (2, 2)).copy()
+    ep = eps_plastic
+    law = lambda x: landau_stress_2d(x - ep if ep is not None else x, lam, mu, v, cap_type, cap_limit, cap_ratio,
+                                     cap_power)
+    hg, hf = [], []
+    it_done, diff = 0, np.inf
+    for it in range(max_iter):
+        tau = law(eps) - hooke(eps, lam0, mu0, 2)
+        tau_hat = np.fft.fftn(tau, axes=axes, norm="ortho")
+        et = np.fft.ifftn(-np.einsum("xykhij,xyij->xykh", G, tau_hat), axes=axes, norm="ortho").real
+        et -= et.mean(axis=axes)
+        eps_new = eps_bar + et
+        diff = np.linalg.norm(eps_new - eps) / (np.linalg.norm(eps) + 1e-20)
+        it_done = it + 1
+        if not np.isfinite(diff):
+            raise FloatingPointError("spectral_solver_landau_2d: non-finite strain update in LS loop")
+        if diff < tol:
+            eps = eps_new
+            break
+        if anderson_m > 0:
+            eps, hg, hf = anderson_step(hg, hf, eps_new, eps_new - eps, anderson_m)
+        else:
+            eps = eps_new
+    sig_out = law(eps)
+    out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
+    return out + (it_done, diff) if return_info else out
+
+
 def rose_stress_2d(e, lam, mu, eta, floor_f=0.1, plane_mode="plane_strain"):
     """Rose secant-modulus stress (mgkmc/elasticity.py:868-944): G = max(mu
     exp(-eta eq), floor mu), K = lam + 2 mu / 3 kept; plane stress: eps_zz by

@@ -281,6 +281,45 @@ def ls3d_secant_fixtures():
     save("ls3d_secant_12x8x6", **out)
 
 
+LANDAU_V = (-199.7e9, -75.4e9, -23.1e9, 1432.0e9, 311.0e9, 145.0e9, -273.0e9)  # v1 v2 v3 g1 g2 g3 g4
+
+
+def ls2d_landau_fixtures():
+    """The reference's Landau stress law (stress_from_strain_landau_2d, plane
+    strain) without capping, with piecewise and with smooth capping, and its
+    LS solver (spectral_solver_landau_2d, basic scheme with Anderson mixing of
+    depth 5 and without) on a heterogeneous medium with eigenstrains."""
+    from mgkmc import elasticity as ELA
+    rng = np.random.default_rng(73)
+    nx, ny = 16, 12
+    E, nu = W.ls2d_material(nx, ny, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    v1, v2, v3, g1, g2, g3, g4 = LANDAU_V
+    kw = dict(v1=v1, v2=v2, v3=v3, g1=g1, g2=g2, g3=g3, g4=g4)
+    e = rng.normal(0, 0.02, (nx, ny, 2, 2))
+    out = dict(lam=lam, mu=mu, v=np.array(LANDAU_V), strain=e)
+    out["sig_plain"] = ELA.stress_from_strain_landau_2d(e, lam, mu, **kw)
+    out["sig_piecewise"] = ELA.stress_from_strain_landau_2d(e, lam, mu, **kw, strain_capping_enabled=True,
+                                                            strain_capping_limit=0.015)
+    out["sig_piecewise_auto"] = ELA.stress_from_strain_landau_2d(e, lam, mu, **kw, strain_capping_enabled=True)
+    out["sig_smooth"] = ELA.stress_from_strain_landau_2d(e, lam, mu, **kw, strain_capping_enabled=True,
+                                                         strain_capping_limit=0.015, strain_capping_type="smooth",
+                                                         strain_capping_smooth_power=2.0)
+    ep = W.pure_shear_eigenstrain_2d(nx, ny, rng, frac=0.1)
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    out.update(eps_plastic=ep, eps_bar=eb)
+    for tag, m in (("aa5", 5), ("aa0", 0)):
+        eps, sig, _, _ = LES.spectral_solver_landau_2d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, max_iter=400,
+                                                       tol=1e-12, anderson_m=m)
+        out.update({f"eps_{tag}": eps, f"sig_{tag}": sig})
+    eps, sig, _, _ = LES.spectral_solver_landau_2d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, max_iter=400,
+                                                   tol=1e-12, strain_capping_enabled=True,
+                                                   strain_capping_limit=0.01)
+    out.update(eps_cap=eps, sig_cap=sig)
+    save("ls2d_landau_16x12", **out)
+
+
 def ls2d_rose_fixtures():
     """The reference's Rose-law LS solver (spectral_solver_rose_2d), plane
     strain and plane stress, with the 3D Lame lambda as its KMC driver passes."""
@@ -338,3 +377,4 @@ if __name__ == "__main__":
     kmc2d_cascade_fixtures()
     kmc2d_patch_fixtures()
     ls3d_secant_fixtures()
+    ls2d_landau_fixtures()

@@ -197,3 +197,95 @@ def test_rose_refuses_asymmetric_strain(les):
     mu = E / (2 * (1 + nu))
     with pytest.raises(NotImplementedError):
         les.spectral_solver_rose_2d(lam, mu, 30.0, 0.1, np.array([[0.01, 0.002], [0.0, 0.0]]), ep)
+
+
+LANDAU_V = (-199.7e9, -75.4e9, -23.1e9, 1432.0e9, 311.0e9, 145.0e9, -273.0e9)
+
+
+def _landau_kw(v):
+    return dict(zip(("v1", "v2", "v3", "g1", "g2", "g3", "g4"), v))
+
+
+@pytest.mark.parametrize("tag", ["aa5", "aa0", "cap"])
+def test_golden_landau(les, golden, tag):
+    # Landau law, basic scheme with and without Anderson mixing, and with
+    # piecewise capping (CTA-wide kernels at 16 x 12) against the reference
+    g = golden("ls2d_landau_16x12")
+    kw = dict(anderson_m=0) if tag == "aa0" else dict(strain_capping_enabled=True,
+                                                      strain_capping_limit=0.01) if tag == "cap" else {}
+    eps, sig, _, sm = les.spectral_solver_landau_2d(g["lam"], g["mu"], **_landau_kw(g["v"]), eps_bar=g["eps_bar"],
+                                                    eps_plastic=g["eps_plastic"], max_iter=400, tol=1e-12, **kw)
+    assert rel(eps, g[f"eps_{tag}"]) < TOL
+    assert rel(sig, g[f"sig_{tag}"]) < TOL
+
+
+@pytest.mark.parametrize("nx,ny,m,cap", [(64, 64, 5, None), (256, 128, 5, "smooth"), (96, 192, 0, "piecewise"),
+                                         (128, 128, 8, None)])
+def test_landau_against_oracle(les, nx, ny, m, cap):
+    # warp-line kernels (sides 64..256) with the Landau law and device Anderson mixing, against the oracle
+    E, nu, ep, _ = W.ls2d_problem(nx, ny, seed=13)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    ckw = {} if cap is None else dict(strain_capping_enabled=True, strain_capping_limit=0.012,
+                                      strain_capping_type=cap, strain_capping_smooth_power=2.0)
+    eps, sig, _, _ = les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, eps_plastic=ep,
+                                                   max_iter=400, tol=1e-11, anderson_m=m, **ckw)
+    o = OL.spectral_solver_landau_2d(lam, mu, LANDAU_V, eb, ep, max_iter=400, tol=1e-11, anderson_m=m,
+                                     cap_type=cap, cap_limit=0.012, cap_power=2.0)
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
+def test_anderson_kernels():
+    # history update, inner products and mix of mgk_aa_* against numpy
+    import ctypes
+    import torch
+    from mgkmc_b200 import _lib as L
+    rng = np.random.default_rng(9)
+    n, m = 70001, 3
+    dev = torch.device("cuda")
+    hist = torch.zeros((2 * m + 2) * n, dtype=torch.float64, device=dev)
+    work = torch.empty(int(L.lib().mgk_aa_work_bytes(n)), dtype=torch.uint8, device=dev)
+    dots = torch.zeros(16, dtype=torch.float64, device=dev)
+    S = L.stream_ptr()
+    fs, gs = [], []
+    for it in range(5):
+        x, g = rng.normal(size=n), rng.normal(size=n)
+        tx, tg = torch.from_numpy(x).to(dev), torch.from_numpy(g).to(dev)
+        have = it > 0
+        slot = (it - 1) % m if have else 0
+        k = min(it, m)
+        L.check(L.lib().mgk_aa_update(n, L.ptr(tx), L.ptr(tg), L.ptr(hist), m, slot, int(have), k, L.ptr(dots),
+                                      L.ptr(work), S), "aa_update")
+        fs.append(g - x)
+        gs.append(g)
+        if not have:
+            continue
+        cols = {}
+        for j in range(1, it + 1):
+            cols[(j - 1) % m] = (fs[j] - fs[j - 1], gs[j] - gs[j - 1])
+        d = dots.cpu().numpy()
+        for j in range(k):
+            np.testing.assert_allclose(d[j], cols[j][0] @ cols[slot][0], rtol=1e-12)
+            np.testing.assert_allclose(d[8 + j], cols[j][0] @ fs[-1], rtol=1e-12)
+        gam = rng.normal(size=k)
+        out = torch.empty_like(tg)
+        arr = (ctypes.c_double * k)(*gam)
+        L.check(L.lib().mgk_aa_mix(n, L.ptr(tg), L.ptr(hist), m, k, ctypes.cast(arr, ctypes.c_void_p), L.ptr(out),
+                                   S), "aa_mix")
+        want = g - sum(gam[j] * cols[j][1] for j in range(k))
+        np.testing.assert_allclose(out.cpu().numpy(), want, rtol=0, atol=1e-12 * np.max(np.abs(want)))
+
+
+def test_landau_refusals(les):
+    E, nu, ep, _ = W.ls2d_problem(16, 16, seed=2)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.005, 0.0], [0.0, 0.0]])
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, plane_mode="plane_stress")
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=np.array([[0.0, 0.001], [0.0, 0.0]]))
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, solver="newton_cg")

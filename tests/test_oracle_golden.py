@@ -73,6 +73,27 @@ def test_ls3d_secant(golden, tag):
     assert rel(sig, g[f"sig_{tag}"]) < 1e-12
 
 
+@pytest.mark.parametrize("tag,cap,limit,power", [("plain", None, None, 1.0), ("piecewise", "piecewise", 0.015, 1.0),
+                                                   ("piecewise_auto", "piecewise", None, 1.0),
+                                                   ("smooth", "smooth", 0.015, 2.0)])
+def test_landau_law(golden, tag, cap, limit, power):
+    # the Landau stress restatement against the reference's stress_from_strain_landau_2d
+    g = golden("ls2d_landau_16x12")
+    sig = OL.landau_stress_2d(g["strain"], g["lam"], g["mu"], tuple(g["v"]), cap, limit, 0.1, power)
+    np.testing.assert_array_equal(sig, g[f"sig_{tag}"])
+
+
+@pytest.mark.parametrize("tag", ["aa5", "aa0", "cap"])
+def test_landau_solver(golden, tag):
+    # the Landau LS restatement (basic scheme, Anderson mixing) against the reference's solver
+    g = golden("ls2d_landau_16x12")
+    kw = dict(anderson_m=0) if tag == "aa0" else dict(cap_type="piecewise", cap_limit=0.01) if tag == "cap" else {}
+    eps, sig, _, _ = OL.spectral_solver_landau_2d(g["lam"], g["mu"], tuple(g["v"]), g["eps_bar"], g["eps_plastic"],
+                                                  max_iter=400, tol=1e-12, **kw)
+    assert rel(eps, g[f"eps_{tag}"]) < 1e-12
+    assert rel(sig, g[f"sig_{tag}"]) < 1e-12
+
+
 @pytest.mark.parametrize("tag,pm", [("ps", "plane_strain"), ("pst", "plane_stress")])
 def test_ls2d_rose(golden, tag, pm):
     # the Rose-law LS restatement against the reference's solver
