@@ -34,3 +34,34 @@ def test_bad_arguments_are_rejected_without_a_device():
     assert b"unsupported" in lib.mgk_last_error()
     assert lib.mgk_ls2d_create(64, 64, 7, 0, ctypes.byref(h)) == L.BAD_ARG
     assert lib.mgk_kmc_select(None, None, None, 0.5, None, None) == L.BAD_ARG
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_device():
+    # argument checks of the patch, Anderson and law entry points run before
+    # any device work
+    lib = L.lib()
+    assert lib.mgk_aa_work_bytes(1 << 20) == 296 * 16 * 8
+    assert lib.mgk_aa_update(0, None, None, None, 5, 0, 0, 0, None, None, None) == L.BAD_ARG
+    one = ctypes.c_void_p(16)  # never dereferenced: the size checks fail first
+    assert lib.mgk_aa_update(10, one, one, one, 9, 0, 0, 0, one, one, None) == L.BAD_ARG  # m > 8
+    assert lib.mgk_aa_mix(10, one, one, 3, 4, one, one, None) == L.BAD_ARG  # ncols > m
+    assert lib.mgk_kmc2d_patch(0, 4, 2, None, None, 0.0, None, None, 3, None, None, None, None) == L.BAD_ARG
+    assert lib.mgk_kmc2d_patch_setup(8, 8, 5000, one, one, one, one, None) == L.BAD_ARG  # R > 4096
+    assert lib.mgk_ls3d_set_secant(None, 0.5, 10.0) == L.BAD_ARG
+    assert lib.mgk_ls2d_set_landau(None, None, 0, 0.0, 0.1, 1.0) == L.BAD_ARG
+
+
+def test_landau_refusals_before_device_work():
+    import numpy as np
+    import pytest
+    from mgkmc_b200 import linear_elastic_simulator as les
+    lam = np.full((8, 8), 4e10)
+    mu = np.full((8, 8), 3e10)
+    v = dict(v1=0.0, v2=0.0, v3=0.0, g1=0.0, g2=0.0, g3=0.0, g4=0.0)
+    eb = np.zeros((2, 2))
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_landau_2d(lam, mu, **v, eps_bar=eb, plane_mode="plane_stress")
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_landau_2d(lam, mu, **v, eps_bar=eb, solver="newton_cg")
+    with pytest.raises(NotImplementedError):
+        les.spectral_solver_landau_2d(lam, mu, **v, eps_bar=eb, anderson_m=9)
