@@ -62,11 +62,20 @@ def parse():
                     help="comma list of forms to time (the headline is batched_mixed)")
     ap.add_argument("--fs-grid", type=int, default=128,
                     help="side of the finite-strain block (Neo-Hookean + F_p, 10 load steps); 0 skips it")
-    ap.add_argument("--ensemble", type=int, default=0,
+    ap.add_argument("--ensemble", type=int, default=96,
                     help="replicas of the batched KMC ensemble block (96 = the ensemble workload, ~1 min); 0 skips it")
-    ap.add_argument("--serve-window", type=float, default=0.1,
+    ap.add_argument("--kmc-events", type=int, default=2000,
+                    help="events of the 256^2 x 8 KMC/AQS block (2000 = the KMC workload); 0 skips it")
+    ap.add_argument("--serve-window", type=float, default=0.5,
                     help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
                          "0 skips it")
+    ap.add_argument("--serve-plain", type=int, default=12,
+                    help="requests of the serving window (seeded random subsample) that the plain FP64 form serves "
+                         "one at a time for the comparison on identical requests")
+    ap.add_argument("--cpu-kmc-seconds", type=float, default=12.0,
+                    help="seconds of the oracle's per-event KMC loop at 256^2 x 8 on one host core; 0 skips it")
+    ap.add_argument("--cpu-fs-grid", type=int, default=32,
+                    help="side of the oracle's finite-strain load step on one host core; 0 skips it")
     ap.add_argument("--profile-case", default="", choices=["", "ls3d", "fs3d", "kmc"],
                     help="run one kernel-profiling workload instead of the benchmark (for ncu captures): ls3d = "
                          "LS 3D solves at --profile-n^3 (tol 1e-8, three solves), fs3d = one finite-strain load "
@@ -85,55 +94,205 @@ def _rank():
 
 
 # ------------------------------------------------------------- CPU legs ----
-def _cpu_worker(args):
-    seed, deadline = args
+_THREAD_VARS = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS",
+                "VECLIB_MAXIMUM_THREADS")
+
+
+def _single_thread_env():
+    """One BLAS/OpenMP thread per process: spawned CPU workers inherit this
+    environment before numpy loads, so P processes use P cores, not P^2
+    threads."""
+    for k in _THREAD_VARS:
+        os.environ[k] = "1"
+
+
+def host_cpu():
+    """Host cores this process may use: the affinity mask, capped by a cgroup
+    CPU quota when one is set (a container can see many cores and be allowed
+    a fraction of them), and the CPU model."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        aff = len(os.sched_getaffinity(0))
+    except AttributeError:
+        aff = os.cpu_count() or 1
+    quota = None
+    for path in ("/sys/fs/cgroup/cpu.max",):
+        try:
+            q, p = open(path).read().split()[:2]
+            if q != "max":
+                quota = float(q) / float(p)
+        except (OSError, ValueError):
+            pass
+    if quota is None:
+        try:
+            q = float(open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us").read())
+            p = float(open("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read())
+            if q > 0:
+                quota = q / p
+        except (OSError, ValueError):
+            pass
+    usable = aff if quota is None else max(1, min(aff, int(quota + 1e-9)))
+    return {"model": model, "cpu_count": os.cpu_count(), "affinity": aff, "cgroup_quota_cores": quota,
+            "usable": usable}
+
+
+def _ls_worker(widx, share, warm_steps, steps, grid, tol, start, ready, results):
+    """Reference-arm worker: its share of every step's LS solves, after its
+    warm-up steps; reports when its timed steps end (perf_counter is the
+    system-wide monotonic clock on Linux, comparable across processes)."""
     from oracle import ls as OL
     from mgkmc_b200 import workloads as W
-    E, nu, ep, eb = W.ls2d_problem(NX, NY, seed)
+    E, nu, ep, eb = W.ls2d_problem(grid, grid, widx)
+    OL.spectral_solver(E, nu, eb, ep, max_iter=500, tol=tol)  # first call: imports, FFT plans
+    for _ in range(warm_steps * share):
+        OL.spectral_solver(E, nu, eb, ep, max_iter=500, tol=tol)
+    ready.put(widx)
+    start.wait()
     n = 0
-    t0 = time.perf_counter()
-    while True:
+    for _ in range(steps * share):
+        OL.spectral_solver(E, nu, eb, ep, max_iter=500, tol=tol)
+        n += 1
+    results.put((widx, time.perf_counter(), n))
+
+
+def cpu_ls_steps(procs, per_step, warm_steps, steps, grid, tol):
+    """Times `steps` steps of `per_step` oracle LS solves spread over `procs`
+    single-threaded spawn-started processes; the clock starts once every
+    worker has finished its warm-up.  Returns (solves/s, wall s, solves)."""
+    import multiprocessing as mp
+    _single_thread_env()
+    ctx = mp.get_context("spawn")
+    start, ready, results = ctx.Event(), ctx.Queue(), ctx.Queue()
+    shares = [per_step // procs + (1 if i < per_step % procs else 0) for i in range(procs)]
+    ws = [ctx.Process(target=_ls_worker, args=(i, shares[i], warm_steps, steps, grid, tol, start, ready, results))
+          for i in range(procs) if shares[i] > 0]
+    for w in ws:
+        w.start()
+    try:
+        for _ in ws:
+            ready.get(timeout=900)
+        t0 = time.perf_counter()
+        start.set()
+        ends = [results.get(timeout=1800) for _ in ws]
+    finally:
+        for w in ws:
+            w.join(timeout=60)
+    wall = max(e[1] for e in ends) - t0
+    solves = sum(e[2] for e in ends)
+    return solves / wall, wall, solves
+
+
+def cpu_ls_baseline(seconds):
+    """One host core, oracle LS solves of the headline problem for about
+    `seconds` (bounded sample); returns (solves/s, solves, wall s)."""
+    from oracle import ls as OL
+    from mgkmc_b200 import workloads as W
+    E, nu, ep, eb = W.ls2d_problem(NX, NY, 0)
+    OL.spectral_solver(E, nu, eb, ep, max_iter=500, tol=TOL)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
         OL.spectral_solver(E, nu, eb, ep, max_iter=500, tol=TOL)
         n += 1
-        if time.perf_counter() >= deadline:
-            break
-    return n, time.perf_counter() - t0
-
-
-def cpu_baseline(seconds, procs):
-    """Oracle restatement of the reference LS solve on host cores (bounded sample)."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    deadline = time.perf_counter() + seconds
-    t0 = time.perf_counter()
-    if procs == 1:
-        res = [_cpu_worker((0, deadline))]
-    else:
-        with ctx.Pool(procs) as pool:
-            # perf_counter is per-process monotonic; pass a relative deadline
-            res = pool.map(_cpu_worker_rel, [(s, seconds) for s in range(procs)])
     wall = time.perf_counter() - t0
-    solves = sum(r[0] for r in res)
-    return solves / wall, solves, wall
+    return n / wall, n, wall
 
 
-def _cpu_worker_rel(args):
-    seed, seconds = args
-    return _cpu_worker((seed, time.perf_counter() + seconds))
+def cpu_kmc_sample(seconds, n=256, M=8, strain=0.024):
+    """One host core, the oracle's per-event loop of the 256^2 x 8 KMC/AQS
+    workload (kmc_simulator.py:871-1101): barriers, rates with the sequential
+    total, selection, flip with redraws and a cold LS re-solve (tol 1e-6),
+    from a state pre-strained to `strain` (where the workload's events
+    happen), for about `seconds`.  Returns seconds per LS solve and per rate
+    step (barriers + rates), and events done."""
+    from oracle import kmc as OK
+    from oracle import ls as OL
+    from oracle.kmc_driver import pure_shear_modes
+    from mgkmc_b200 import workloads as W
+    rng = np.random.default_rng(1)
+    E, nu = W.ls2d_material(n, n, rng)
+    cat, Q0 = W.kmc2d_state(n, n, M, rng)
+    eps_p = np.zeros((n, n, 2, 2))
+    soft, t_last = np.zeros((n, n, 2)), np.full((n, n), -np.inf)
+    prev, Q = np.zeros((n, n, 2, 2)), np.zeros((n, n, M))
+    eb = np.zeros((2, 2))
+    eb[0, 0], eb[1, 1] = strain, -0.4 * strain
+    t_solve, t_rate, events = [], [], 0
+    t = time.perf_counter()
+    _, sig, _, _ = OL.spectral_solver(E, nu, eb, eps_p, max_iter=200, tol=1e-6)
+    t_solve.append(time.perf_counter() - t)
+    t_end = time.perf_counter() + seconds
+    tau = 1.0 / (1e13 * np.exp(-0.37 / (OK.KB * 300.0)))
+    while time.perf_counter() < t_end:
+        t = time.perf_counter()
+        OK.compute_barrier(Q, Q0, sig, cat, 1.0, soft, t_last, 0.0, prev, 2.0, 0, tau)
+        rates, idx, total = OK.compute_rates(Q, 1.0, 300.0, 1e13, cascade_mode=False)
+        k = OK.select_event(rates, total, rng.random())
+        t_rate.append(time.perf_counter() - t)
+        x, y, m = OK.decode_index_2d(int(idx[k]), n, M)
+        OK.apply_flip_2d(eps_p, soft, t_last, cat, x, y, m, 0.0, 0.0, 0.0, 2.0, 0.0)
+        prev[x, y] = cat[x, y, m]
+        cat[x, y] = pure_shear_modes(rng.uniform(0.0, np.pi, M), 0.1)
+        Q0[x, y] = np.clip(rng.normal(1.0, 0.15, M), 0.3, None)
+        t = time.perf_counter()
+        _, sig, _, _ = OL.spectral_solver(E, nu, eb, eps_p, max_iter=200, tol=1e-6)
+        t_solve.append(time.perf_counter() - t)
+        events += 1
+    return float(np.mean(t_solve)), float(np.mean(t_rate)), events, len(t_solve)
+
+
+def cpu_fs_sample(n=32):
+    """One host core, the oracle's first load step of the finite-strain
+    workload (Neo-Hookean + 2 % F_p, F_xx = 1.005, lateral stresses zero,
+    Newton 1e-8, CG 1e-6) at n^3.  Returns (seconds, Newton, Krylov)."""
+    from oracle import fs as OF
+    from mgkmc_b200 import workloads as W
+    E, nu, Fp = W.fs3d_material(n, n, n, np.random.default_rng(2))
+    Fp = OF.to_spatial(Fp)
+    F = np.broadcast_to(np.eye(3), (n, n, n, 3, 3)).copy()
+    Fb, _, Pt, Pm = OF.build_bc_3d((0, 0), 0.005, {(1, 1): 0.0, (2, 2): 0.0})
+    t0 = time.perf_counter()
+    OF.solver_step_3d(F, Fb, E, nu, Fp, (0, 0), Pt, Pm, tol_NW=1e-8, tol_CG=1e-6, model="neo_hookean",
+                      krylov="cg")
+    return time.perf_counter() - t0
+
+
+def headline_config(a, world=1):
+    """The workload description both arms print (identical dicts)."""
+    return {"workload": f"ls2d_{NX}_batched_mixed", "problems_per_step": a.batch, "grid": [NX, NY], "tol": TOL,
+            "material": "mu ~ mu0 (1 + 0.1 N(0,1)) clipped [0.7,1.3] mu0, K = 100 GPa, 5 % pure-shear "
+                        "eigenstrains gamma0 = 0.1, eps_xx = 0.01, plane strain",
+            "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
 
 
 def run_reference(a):
+    """The reference's CPU path (the oracle restatement of spectral_solver_2d:
+    the reference is Python and does not travel to the GPU host) on this
+    host's usable cores: one single-threaded process per core, each step a
+    bounded sample of the headline workload's solves."""
     rank, world, _ = _rank()
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
-    v, solves, wall = cpu_baseline(a.cpu_seconds, cores)
+    info = host_cpu()
+    P = info["usable"]
+    per_step = min(a.batch, 2 * P)
+    v, wall, solves = cpu_ls_steps(P, per_step, max(1, a.warmup), a.steps, NX, TOL)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * a.batch / v, "higher_is_better": True,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, survey config)",
-            "config": {"workload": f"ls2d_{NX}_batched_mixed", "batch": a.batch, "grid": [NX, NY], "tol": TOL},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": f"{solves} oracle solves in {wall:.1f} s, one process per core"},
+            "config": headline_config(a, world),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": P, "kind": "port",
+                             "sample": f"{a.steps} steps x {per_step} solves of the {NX}^2 problem (tol {TOL:g}), "
+                                       f"{P} single-threaded processes, clock started after every process had "
+                                       f"solved {max(1, a.warmup)} warm-up steps; {solves} solves in {wall:.2f} s",
+                             "host": info},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -184,29 +343,91 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- serving -----
-def run_serving(window):
+def run_serving(window, n_plain=12):
     """The serving stream's first `window` seconds of arrivals, served by the
-    continuous-batching server (mixed precision) and by the plain FP64 form one
-    request at a time; arrivals replayed in real time."""
+    continuous-batching server (mixed precision, arrivals replayed in real
+    time), and a seeded random subsample of `n_plain` of those requests served
+    by the plain FP64 form one request at a time (their own arrival times
+    replayed).  Latency ratios compare identical requests: each subsampled
+    request's latency inside the full served mix against its latency in the
+    plain form.  Solves/s: served = solves over the window's makespan; plain =
+    solves over its busy time (sum of service times), so its idle gaps between
+    sparse arrivals do not count against it."""
     from mgkmc_b200.serving import Server, request_stream, summarize
     reqs = [r for r in request_stream(rate=200.0, duration=60.0, seed=3) if r.t_arrival <= window]
+    rng = np.random.default_rng(4)
+    sub_ids = sorted(int(i) for i in rng.choice(len(reqs), size=min(n_plain, len(reqs)), replace=False))
+    sub = [reqs[i] for i in sub_ids]
     out = {"workload": (f"serving stream (Poisson 200 req/s, seed 3; 60 % equilibrium solves, 40 % 100-event KMC "
                         f"trajectories; 70 % 2D sides 64..1024, 30 % 3D finite-strain 64..128): the "
-                        f"{len(reqs)} arrivals of its first {window:g} s, replayed in real time"),
-           "requests": [[r.kind, r.dim, r.n] for r in reqs]}
-    for name, mode in (("served_mixed", "served"), ("plain_fp64_sequential", "sequential")):
-        srv = Server(mode=mode)
-        srv.prepare(reqs)
-        res = srv.run(reqs, realtime=True)
-        out[name] = summarize(res)
+                        f"{len(reqs)} arrivals of its first {window:g} s, replayed in real time; plain FP64 on a "
+                        f"seeded subsample of {len(sub)}"),
+           "requests": [[r.kind, r.dim, r.n] for r in reqs], "plain_subsample": [r.rid for r in sub]}
+    srv = Server(mode="served")
+    srv.prepare(reqs)
+    res = srv.run(reqs, realtime=True)
+    out["served_mixed"] = summarize(res)
+    by_id = {r.rid: r for r in res}
+    lat_sub = np.array([by_id[r.rid].latency for r in sub if not by_id[r.rid].error])
+    srv = Server(mode="sequential")
+    srv.prepare(sub)
+    res_p = srv.run(sub, realtime=True)
+    plain = summarize(res_p)
+    ok = [r for r in res_p if not r.error]
+    busy = sum(r.t_done - r.t_admit for r in ok)
+    plain["busy_s"] = busy
+    plain["solves_per_busy_s"] = sum(r.solves for r in ok) / max(busy, 1e-9)
+    out["plain_fp64_sequential"] = plain
     from mgkmc_b200 import serving as SV
     out["autotuned_ls_families"] = {f"{k[0]}^2 x{k[1]} {k[2]}": {"family": v[0], "ms_per_iteration": v[1]}
                                     for k, v in SV._TUNED.items()}
-    a, b = out["served_mixed"], out["plain_fp64_sequential"]
-    if a.get("completed") and b.get("completed"):
-        out["solves_per_s_ratio"] = a["solves_per_s"] / b["solves_per_s"]
-        out["p50_ratio"] = b["p50_s"] / a["p50_s"]
-        out["p99_ratio"] = b["p99_s"] / a["p99_s"]
+    a = out["served_mixed"]
+    if a.get("completed") and plain.get("completed") and lat_sub.size:
+        lat_p = np.array([r.latency for r in ok])
+        out["identical_requests"] = {"n": int(lat_sub.size),
+                                     "served_p50_s": float(np.percentile(lat_sub, 50)),
+                                     "served_p99_s": float(np.percentile(lat_sub, 99)),
+                                     "plain_p50_s": float(np.percentile(lat_p, 50)),
+                                     "plain_p99_s": float(np.percentile(lat_p, 99))}
+        out["solves_per_s_ratio"] = a["solves_per_s"] / plain["solves_per_busy_s"]
+        out["p50_ratio"] = out["identical_requests"]["plain_p50_s"] / out["identical_requests"]["served_p50_s"]
+        out["p99_ratio"] = out["identical_requests"]["plain_p99_s"] / out["identical_requests"]["served_p99_s"]
+    return out
+
+
+# ------------------------------------------------------------- KMC/AQS -----
+def run_kmc(n_events, n=256, M=8):
+    """The 256^2 x 8 KMC/AQS workload (heterogeneous medium, Q0 ~ N(1.0,
+    0.15) eV clipped at 0.3, T = 300 K, AQS steps of 1e-5 at a strain rate of
+    1e7/s, lateral mean stress driven to zero) for `n_events` events, in the
+    plain form (FP64 cold LS re-solves at tol 1e-6, the bit-exact sequential
+    rate total: the reference's arithmetic) and the served form (mixed
+    precision, warm starts, the fused rate pass).  Device-driven trajectory;
+    timed with CUDA events and the host clock."""
+    import torch
+    from mgkmc_b200.kmc import Kmc2D
+    from mgkmc_b200 import workloads as W
+    rng0 = np.random.default_rng(1)
+    E, nu = W.ls2d_material(n, n, rng0)
+    cat, Q0 = W.kmc2d_state(n, n, M, rng0)
+    out = {"workload": f"KMC/AQS {n}^2 x {M} modes, {n_events} events, seed 1"}
+    for name, kw in (("plain_fp64_exact", dict(selection="exact", ls_start="cold", precision="fp64")),
+                     ("served_mixed_fast", dict(selection="fast", ls_start="warm", precision="mixed"))):
+        k = Kmc2D(E, nu, cat, Q0, **kw)
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(st)
+        r = k.run(np.random.default_rng(1), 10 ** 9, max_events=n_events)
+        e1.record(st)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        out[name] = {"seconds": wall, "device_span_s": e0.elapsed_time(e1) / 1e3, "events": len(r["events"]),
+                     "aqs_steps": int(r["steps"]), "solves": int(r["solves"]),
+                     "events_per_s": len(r["events"]) / wall, "final_strain_xx": float(r["eps_macro"][0, 0]),
+                     "sim_time_s": float(r["time"])}
+        del k
     return out
 
 
@@ -438,6 +659,9 @@ def run_ours(a):
     finite_strain = None
     if world == 1 and a.fs_grid > 0:
         finite_strain = run_finite_strain(a.fs_grid, peak)
+    kmc = None
+    if world == 1 and a.kmc_events > 0:
+        kmc = run_kmc(a.kmc_events)
     ensemble = None
     if world == 1 and a.ensemble > 0:
         from mgkmc_b200.serving import ensemble_requests, run_ensemble
@@ -447,26 +671,55 @@ def run_ours(a):
                                 f"one batched solve launch per size per round")
     serving = None
     if world == 1 and a.serve_window > 0:
-        serving = run_serving(a.serve_window)
+        serving = run_serving(a.serve_window, a.serve_plain)
     cpu = None
-    if world == 1 and a.cpu_seconds > 0:
-        v, nsol, wall = cpu_baseline(a.cpu_seconds, 1)
-        cpu = {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
-               "sample": f"{nsol} oracle solves of the same {NX}^2 problem in {wall:.1f} s (numpy FFT, 1 thread)"}
+    cpu_other = None
+    if world == 1:
+        from threadpoolctl import threadpool_limits
+        host = host_cpu()
+        with threadpool_limits(1):
+            if a.cpu_seconds > 0:
+                v, nsol, wall = cpu_ls_baseline(a.cpu_seconds)
+                cpu = {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
+                       "sample": f"{nsol} oracle solves of the {NX}^2 problem (tol {TOL:g}) in {wall:.1f} s, "
+                                 f"numpy FFT, one thread", "host": host}
+            cpu_other = {}
+            if a.cpu_kmc_seconds > 0:
+                ts, tr, nev, nsol = cpu_kmc_sample(a.cpu_kmc_seconds)
+                d = {"kind": "port", "cores": 1, "s_per_ls_solve": ts, "s_per_rate_step": tr,
+                     "sample": f"{nev} events of the oracle's per-event loop at 256^2 x 8 (barriers, rates with the "
+                               f"sequential total, selection, flip with redraws, cold LS re-solve at tol 1e-6) "
+                               f"from a state pre-strained to 2.4 %, {nsol} LS solves"}
+                if kmc is not None:
+                    # the same trajectory's solve and rate-step counts at the CPU's per-unit costs
+                    pk = kmc["plain_fp64_exact"]
+                    cpu_s = pk["solves"] * ts + (pk["aqs_steps"] + pk["events"]) * tr
+                    d["events_per_s_estimate"] = pk["events"] / cpu_s
+                    d["estimate"] = (f"{pk['solves']} LS solves x {ts:.3f} s + {pk['aqs_steps'] + pk['events']} "
+                                     f"rate steps x {tr:.4f} s (the GPU trajectory's counts)")
+                cpu_other["kmc_256x256x8"] = d
+            if a.cpu_fs_grid > 0:
+                n = a.cpu_fs_grid
+                s = cpu_fs_sample(n)
+                scale = (128.0 / n) ** 3 * np.log(128.0 ** 3) / np.log(float(n) ** 3)
+                cpu_other["finite_strain_128"] = {
+                    "kind": "port", "cores": 1, "seconds_per_load_step_sample": s,
+                    "seconds_per_load_step_128_estimate": s * scale,
+                    "sample": f"the first load step (F_xx = 1.005) at {n}^3, Neo-Hookean + 2 % F_p, Newton 1e-8, "
+                              f"CG 1e-6; scaled to 128^3 by N log N ({scale:.1f}x)"}
     line = {"metric": METRIC, "value": rate[head], "unit": "solves/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms[head] / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, survey config)",
-            "config": {"workload": f"ls2d_{NX}_batched_mixed", "batch": B, "grid": [NX, NY], "tol": TOL,
-                       "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}",
-                       "forms_solves_per_s": rate,
-                       "speedup_vs_plain_fp64": rate[head] / rate["plain_fp64"] if "plain_fp64" in rate else None,
-                       "iters_mean": {k: float(np.mean(v)) for k, v in iters.items()},
-                       "mixed_field_err_vs_fp64": err_mixed, "mixed_residual": residual},
+            "vs_baseline": None, "dtype": "mixed fp32/fp64 (FP32 bulk iterations, FP64 finish, norms and sums)",
+            "data": "synthetic (seeded, survey config)", "config": headline_config(a, world),
+            "forms": {"solves_per_s": rate,
+                      "speedup_vs_plain_fp64": rate[head] / rate["plain_fp64"] if "plain_fp64" in rate else None,
+                      "iters_mean": {k: float(np.mean(v)) for k, v in iters.items()},
+                      "mixed_field_err_vs_fp64": err_mixed, "mixed_residual": residual},
             "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.Ls2dBatch",
                     "pipelining": "three plans on three streams, steps in turn", "host_result_err": e2e_err},
-            "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "finite_strain": finite_strain, "serving": serving, "ensemble": ensemble}
+            "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "cpu_baselines_other": cpu_other,
+            "clocks": clocks, "finite_strain": finite_strain, "kmc": kmc, "serving": serving, "ensemble": ensemble}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -302,6 +302,17 @@ MGK_API int mgk_fs3d_step(mgk_fs3d_t plan, const double* F_bar_in, int driving_i
 /* Copy out F and P (device, tensor-first) and compute the Cauchy stress
  * (cauchy_from_P_3d :1892-1904); any pointer may be NULL. */
 MGK_API int mgk_fs3d_get(mgk_fs3d_t plan, double* F_out, double* P_out, double* sig_out, mgk_stream_t stream);
+/* 2D plane-strain finite strain (mgkmc/finite_strain_simulator.py:2356-2572
+ * finite_strain_solver_step_2d, solver="newton_cg"; laws :591-1087 with
+ * plane_mode="plane_strain") on a plan created as (nx, 1, ny): the plane's
+ * axes are the plan's x and z, the out-of-plane axis is y (one voxel, no
+ * wave vector) with F_yy = 1, tensor index 1 of the 2D fields is index 2 of
+ * the plan's.  The 3D SVK and Neo-Hookean laws at F_yy = 1 are the
+ * reference's plane-strain laws, and the projection keeps every out-of-plane
+ * component of dF at zero, so the plan solves the 2D problem; on != 0 makes
+ * the Newton test use the 2D field's norm (||F|| without the N unit F_yy
+ * entries, :2521).  No counterpart in the reference as an entry point. */
+MGK_API int mgk_fs3d_set_plane_strain(mgk_fs3d_t plan, int on);
 /* Autotuner: times one Krylov iteration of each kernel family that can serve
  * the plan (warp-line passes, sides 64/96/128; CTA-wide passes) on the current
  * state and keeps the faster; *chosen 1 warp-line, 0 CTA-wide.  Call after a
@@ -446,6 +457,19 @@ MGK_API int mgk_kmc3d_flip(int nx, int ny, int nz, int M, double* eps_plastic, d
                            double* last_event_time, const double* catalog, int x, int y, int z, int m,
                            double current_time, double jp, double jt, double g_max, double jn_frac,
                            mgk_stream_t stream);
+
+/* One 3D KMC event on the device: mgkmc/aqs.py:889-892 (position *d_sel ->
+ * mode index via indices (NULL: identity, KMC mode) -> x, y, z, m by
+ * decode_index, stz/kmc.py:94-103), :996 apply_flip_soa, :997
+ * prev_strain_dir[x,y,z] = catalog[x,y,z,m], and :1006-1013 the redraw of
+ * the voxel's catalog (new_catalog, M x 3 x 3) and barriers (new_q0, M), both
+ * drawn by the host (NULL: keep).  Writes (x, y, z, m) to d_xyzm (device
+ * int64[4], may be NULL); a negative *d_sel leaves everything unchanged. */
+MGK_API int mgk_kmc3d_event(int nx, int ny, int nz, int M, const int64_t* d_sel, const int64_t* indices,
+                            double* eps_plastic, double* soft_prop, double* last_event_time, double* catalog,
+                            double* Q0, double* prev_strain_dir, const double* new_catalog, const double* new_q0,
+                            double current_time, double jp, double jt, double g_max, double jn_frac,
+                            int64_t* d_xyzm, mgk_stream_t stream);
 
 #ifdef __cplusplus
 }

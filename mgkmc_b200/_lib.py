@@ -92,6 +92,7 @@ _SIGS = {
     "mgk_fs3d_profile": (c_int, [_P, c_int, c_int, POINTER(ctypes.c_float), _P]),
     "mgk_fs3d_set_material": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_fs3d_set_F": (c_int, [_P, _P, _P]),
+    "mgk_fs3d_set_plane_strain": (c_int, [_P, c_int]),
     "mgk_fs3d_step": (c_int, [_P, POINTER(c_double), c_int, c_int, POINTER(c_double), POINTER(c_int), c_double,
                               c_double, c_double, c_double, c_int, c_double, c_int, POINTER(c_double),
                               POINTER(FsInfo), _P]),
@@ -121,6 +122,8 @@ _SIGS = {
                                 _P, _P, _P, _P, _P]),
     "mgk_kmc3d_flip": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, c_int, c_int, c_int, c_int, c_double,
                                c_double, c_double, c_double, c_double, _P]),
+    "mgk_kmc3d_event": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, c_double,
+                                c_double, c_double, c_double, c_double, _P, _P]),
 }
 
 _lib = None

@@ -1084,6 +1084,9 @@ struct mgk_fs3d_plan {
   cudaGraphExec_t cg_exec[2] = {nullptr, nullptr};
   int graph_mode = -1;  // -1 untried, 1 graphs, 0 host-driven loop
   int fast = 0;         // warp-line passes (every side has a compiled FFT)
+  // plane strain embedded as (nx, 1, ny): the out-of-plane F_yy = 1 adds N
+  // to ||F||^2, which the 2D solver's Newton norm does not contain
+  double ff_offset = 0.0;
 };
 
 static FsArgs fs_args(mgk_fs3d_t p) {
@@ -1552,7 +1555,7 @@ static int fs_newton(mgk_fs3d_t p, const double* F_bar, double tol_NW, double to
     if (!ok) { set_error("Newton-CG line search failed to find a valid step."); return MGK_NOT_CONVERGED; }
     if ((rc = fs_accept(p, s))) return rc;
     ++p->stat_newton;
-    const double res = sqrt(p->h_sc->xx) / (sqrt(p->h_sc->FF) + 1e-20);
+    const double res = sqrt(p->h_sc->xx) / (sqrt(std::max(0.0, p->h_sc->FF - p->ff_offset)) + 1e-20);
     if (res < tol_NW && it > 0) return MGK_OK;
   }
   set_error("Newton-CG inner solver did not converge within %d iterations.", max_NW);
@@ -1628,6 +1631,12 @@ extern "C" int mgk_fs3d_autotune(mgk_fs3d_t p, int reps, int* chosen, float* bes
   fs_drop_graphs(p);
   if (chosen) *chosen = best;
   if (best_ms) *best_ms = best_t;
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_set_plane_strain(mgk_fs3d_t p, int on) {
+  MGK_REQUIRE(p && (!on || p->ny == 1), "mgk_fs3d_set_plane_strain: the plan must be (nx, 1, ny)");
+  p->ff_offset = on ? (double)p->N : 0.0;
   return MGK_OK;
 }
 

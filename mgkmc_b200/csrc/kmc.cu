@@ -711,8 +711,10 @@ __global__ void flip2d_kernel(int nx, int ny, int M, double* ep, double* soft, d
 }
 
 // apply_flip_soa (mgkmc/stz/cascade.py:43-111), one thread.
-__global__ void flip3d_kernel(int nx, int ny, int nz, int M, double* ep, double* soft, double* tl, const double* cat,
-                              int x, int y, int z, int m, double t, double jp, double jt, double gmax, double jn) {
+// apply_flip_soa (stz/cascade.py:43-111) at voxel v = (x, y, z), mode m:
+// eps_p += C, softening from sum_sq, 26-neighbour fraction when jn > 0.
+__device__ void flip3d_body(int nx, int ny, int nz, int M, double* ep, double* soft, double* tl, const double* cat,
+                            int x, int y, int z, int m, double t, double jp, double jt, double gmax, double jn) {
   const long long v = ((long long)x * ny + y) * nz + z;
   const double* c = cat + ((v * M) + m) * 9;
   for (int q = 0; q < 9; ++q) ep[9 * v + q] = add(ep[9 * v + q], c[q]);
@@ -737,6 +739,45 @@ __global__ void flip3d_kernel(int nx, int ny, int nz, int M, double* ep, double*
           soft[4 * w + 1] = add(soft[4 * w + 1], mul(mul(jn, jt), s));
         }
   }
+}
+
+__global__ void flip3d_kernel(int nx, int ny, int nz, int M, double* ep, double* soft, double* tl, const double* cat,
+                              int x, int y, int z, int m, double t, double jp, double jt, double gmax, double jn) {
+  flip3d_body(nx, ny, nz, M, ep, soft, tl, cat, x, y, z, m, t, jp, jt, gmax, jn);
+}
+
+// One 3D KMC event on the device (aqs.py:889-892 selection and decode,
+// :996-997 apply_flip_soa and prev_strain_dir, :1006-1013 the redraw of the
+// voxel's catalog and barriers from values the host drew).  d_sel holds the
+// position in the rates array; `indices` maps it to the mode index (NULL:
+// identity, KMC mode).  Writes (x, y, z, m) to d_xyzm (may be NULL); a
+// negative selection changes nothing and writes -1s.
+__global__ void event3d_kernel(int nx, int ny, int nz, int M, const long long* d_sel, const long long* indices,
+                               double* ep, double* soft, double* tl, double* cat, double* Q0, double* prev,
+                               const double* new_cat, const double* new_q0, double t, double jp, double jt,
+                               double gmax, double jn, long long* d_xyzm) {
+  const long long k = *d_sel;
+  if (k < 0) {
+    if (d_xyzm) { d_xyzm[0] = -1; d_xyzm[1] = -1; d_xyzm[2] = -1; d_xyzm[3] = -1; }
+    return;
+  }
+  const long long idx = indices ? indices[k] : k;
+  const int m = (int)(idx % M);
+  long long tmp = idx / M;
+  const int z = (int)(tmp % nz);
+  tmp /= nz;
+  const int y = (int)(tmp % ny);
+  const int x = (int)(tmp / ny);
+  const long long v = ((long long)x * ny + y) * nz + z;
+  double C[9];
+  for (int q = 0; q < 9; ++q) C[q] = cat[(v * M + m) * 9 + q];
+  flip3d_body(nx, ny, nz, M, ep, soft, tl, cat, x, y, z, m, t, jp, jt, gmax, jn);
+  for (int q = 0; q < 9; ++q) prev[9 * v + q] = C[q];
+  if (new_cat)
+    for (int q = 0; q < 9 * M; ++q) cat[v * M * 9 + q] = new_cat[q];
+  if (new_q0)
+    for (int q = 0; q < M; ++q) Q0[v * M + q] = new_q0[q];
+  if (d_xyzm) { d_xyzm[0] = x; d_xyzm[1] = y; d_xyzm[2] = z; d_xyzm[3] = m; }
 }
 
 // One KMC event on the device (kmc_simulator.py:899-900, :1025-1042): decode
@@ -1085,6 +1126,22 @@ extern "C" int mgk_kmc3d_flip(int nx, int ny, int nz, int M, double* eps_plastic
   MGK_REQUIRE(eps_plastic && soft_prop && last_event_time && catalog, "mgk_kmc3d_flip: null argument");
   flip3d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, nz, M, eps_plastic, soft_prop, last_event_time, catalog,
                                                    x, y, z, m, current_time, jp, jt, g_max, jn_frac);
+  MGK_CUDA(cudaGetLastError());
+  return MGK_OK;
+}
+
+extern "C" int mgk_kmc3d_event(int nx, int ny, int nz, int M, const int64_t* d_sel, const int64_t* indices,
+                               double* eps_plastic, double* soft_prop, double* last_event_time, double* catalog,
+                               double* Q0, double* prev_strain_dir, const double* new_catalog,
+                               const double* new_q0, double current_time, double jp, double jt, double g_max,
+                               double jn_frac, int64_t* d_xyzm, mgk_stream_t stream) {
+  MGK_REQUIRE(nx > 0 && ny > 0 && nz > 0 && M > 0 && d_sel && eps_plastic && soft_prop && last_event_time &&
+                  catalog && Q0 && prev_strain_dir,
+              "mgk_kmc3d_event: bad argument");
+  event3d_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(nx, ny, nz, M, (const long long*)d_sel, (const long long*)indices,
+                                                    eps_plastic, soft_prop, last_event_time, catalog, Q0,
+                                                    prev_strain_dir, new_catalog, new_q0, current_time, jp, jt, g_max,
+                                                    jn_frac, (long long*)d_xyzm);
   MGK_CUDA(cudaGetLastError());
   return MGK_OK;
 }

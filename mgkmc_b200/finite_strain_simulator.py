@@ -192,3 +192,244 @@ def simulate_3d(E, nu, Fp, eps_target, n_steps, driving_component=(0, 0), mixed_
         out.append((Fb, dict(newton=info.newton_iterations, krylov=info.krylov_iterations,
                              macro=info.macro_iterations, sig_mean=np.array(info.sig_mean).reshape(3, 3))))
     return s, out
+
+
+_COMP = {(0, 0): "xx", (1, 1): "yy", (2, 2): "zz", (0, 1): "xy", (0, 2): "xz", (1, 2): "yz", (1, 0): "yx",
+         (2, 0): "zx", (2, 1): "zy"}
+
+
+def finite_strain_simulation_3d(E, nu, driving_component, eps_target, n_steps, mixed_targets=None, pixel=1.0,
+                                tol_NW=1e-5, tol_CG=1e-6, max_NW=20, tol_macro=1e6, max_iter_macro=20, store=True,
+                                log_path=None, global_log_path=None, enable_console=True,
+                                checkpoint_interval="none", checkpoint_path=None, vtk_interval="none", vtk_path=None,
+                                model_type="svk", A_m=0.0, B_m=0.0, C_m=0.0, solver="al", Fp=None, precision="fp64",
+                                **unused):
+    """Incremental 3D finite-strain load ramp (finite_strain_simulator.py:3175-3414)
+    on one device-resident plan: per load step s the boundary conditions of
+    build_finite_strain_bc_3d at eps_target * s / n_steps (seeded with the
+    previous step's F_bar), one Newton-Krylov load step from the previous
+    field.  Returns (F_macro, Sig_macro, P_macro, F list, Sig list) like the
+    reference.  ``Fp`` (tensor-first, optional) is an eigen-deformation field
+    the reference's driver does not take (it passes Fp=None, :3282); None
+    reproduces the reference.  Only solver="newton_cg" runs here."""
+    import time as _time
+    from datetime import datetime as _dt
+    if solver not in ("newton_cg", "newton"):
+        raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
+    if model_type not in _MODEL:
+        raise NotImplementedError(f"model_type={model_type!r}: SVK and Neo-Hookean run on the GPU")
+    if vtk_interval not in (None, "none"):
+        raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
+    torch = _torch()
+    mixed_targets = {} if mixed_targets is None else mixed_targets
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    shape = E.shape
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    s_ = Fs3dSolver(*shape, model=model_type, precision=precision)
+    s_.set_material(t(lam), t(mu), None if Fp is None else t(Fp))
+    F = torch.zeros((3, 3) + shape, dtype=torch.float64, device=dev)
+    for i in range(3):
+        F[i, i] = 1.0
+    s_.set_F(F)
+    P = torch.empty_like(F)
+    Sig = torch.empty_like(F)
+    lbl = _COMP.get(tuple(driving_component), "xx")
+    log_f = open(log_path, "w", buffering=1) if log_path else None
+    if log_f:
+        hdr = (f"{'Timestamp':<20} {'Elapsed(s)':<12} {'Step':<8} {'F_' + lbl:<14} {'Eng_strain_' + lbl:<20} "
+               f"{'Sig_' + lbl + '(GPa)':<18}\n")
+        log_f.write(hdr)
+        log_f.write("-" * len(hdr.rstrip()) + "\n")
+    glog_f = open(global_log_path, "w", buffering=1) if global_log_path else None
+    six = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    if glog_f:
+        ghdr = (f"{'Step':<8} " + " ".join(f"{'F_' + _COMP[c]:<12}" for c in six) + " " +
+                " ".join(f"{'EngStr_' + _COMP[c]:<14}" for c in six[:3]) + " " +
+                " ".join(f"{'P_' + _COMP[c] + '(GPa)':<14}" for c in six) + " " +
+                " ".join(f"{'Sig_' + _COMP[c] + '(GPa)':<16}" for c in six) + "\n")
+        glog_f.write(ghdr)
+        glog_f.write("-" * len(ghdr.rstrip()) + "\n")
+    t0 = _time.time()
+    F_macro, Sig_macro, P_macro, F_list, Sig_list = [], [], [], [], []
+    F_bar_init = None
+    E_avg, nu_avg = float(E.mean()), float(nu.mean())
+    for s, eps_s in enumerate(np.linspace(0.0, eps_target, n_steps + 1)):
+        F_bar, _, P_tgt, P_mask = build_finite_strain_bc_3d(driving_component, eps_s, mixed_targets,
+                                                            F_bar_initial=F_bar_init)
+        F_bar_init, info = s_.step(F_bar, driving_component, P_tgt, P_mask, E_avg, nu_avg, tol_NW, tol_CG, max_NW,
+                                   tol_macro, max_iter_macro)
+        if enable_console:
+            print(f"finite strain step: {info.macro_iterations} macro, {info.newton_iterations} Newton, "
+                  f"{info.krylov_iterations} CG iterations")
+        s_.get(F, P, Sig)
+        F_mac = F.mean(dim=(2, 3, 4)).cpu().numpy()
+        P_mac = P.mean(dim=(2, 3, 4)).cpu().numpy()
+        S_mac = Sig.mean(dim=(2, 3, 4)).cpu().numpy()
+        F_macro.append(F_mac)
+        Sig_macro.append(S_mac)
+        P_macro.append(P_mac)
+        if store:
+            F_list.append(F.cpu().numpy())
+            Sig_list.append(Sig.cpu().numpy())
+        i, j = driving_component
+        F_drv = F_mac[i, j]
+        eng = F_drv - (1.0 if i == j else 0.0)
+        if enable_console:
+            print(f"step {s}/{n_steps}: F_{lbl}={F_drv:.5f}, eng_strain={eng:.5f}, Sig_{lbl}={S_mac[i, j] / 1e9:.4f} GPa")
+        if log_f:
+            log_f.write(f"{_dt.now().strftime('%Y-%m-%d %H:%M:%S'):<20} {_time.time() - t0:<12.3f} {s:<8} "
+                        f"{F_drv:<14.6f} {eng:<20.6f} {S_mac[i, j] / 1e9:<18.6f}\n")
+        if glog_f:
+            glog_f.write(f"{s:<8} " + " ".join(f"{F_mac[c]:<12.6f}" for c in six) + " " +
+                         " ".join(f"{F_mac[c] - 1:<14.6f}" for c in six[:3]) + " " +
+                         " ".join(f"{P_mac[c] / 1e9:<14.6f}" for c in six) + " " +
+                         " ".join(f"{S_mac[c] / 1e9:<16.6f}" for c in six) + "\n")
+        if checkpoint_path is not None and checkpoint_interval not in (None, "none", "last"):
+            name = None
+            if checkpoint_interval == "current":
+                name = checkpoint_path
+            elif isinstance(checkpoint_interval, int) and s % checkpoint_interval == 0:
+                name = f"{checkpoint_path}_{s:06d}"
+            if name:
+                _checkpoint(name, s, E, nu, F, Sig, F_mac, S_mac, pixel)
+    if checkpoint_path is not None and (checkpoint_interval == "last" or (
+            isinstance(checkpoint_interval, int) and n_steps % checkpoint_interval != 0)):
+        _checkpoint(f"{checkpoint_path}_final", n_steps, E, nu, F, Sig, F_macro[-1], Sig_macro[-1], pixel)
+    total = _time.time() - t0
+    m_, sec = divmod(total, 60)
+    h_, m_ = divmod(m_, 60)
+    if log_f:
+        log_f.write(f"\nSimulation Finish Time: {_dt.now().strftime('%Y-%m-%d %H:%M:%S')}\nTotal Duration: "
+                    f"{total:.2f} seconds ({int(h_):d}h {int(m_):02d}m {int(sec):02d}s)\n")
+        log_f.close()
+    if glog_f:
+        glog_f.close()
+    return np.array(F_macro), np.array(Sig_macro), np.array(P_macro), F_list, Sig_list
+
+
+def _checkpoint(path, step, E, nu, F, Sig, F_mac, S_mac, pixel):
+    """The reference's checkpoint of a finite-strain step (:3351-3356): the
+    Green-Lagrange strain and the Cauchy stress, spatial-first."""
+    from . import checkpoint as C
+    torch = _torch()
+    E_GL = 0.5 * (torch.einsum("kixyz,kjxyz->ijxyz", F, F) - torch.eye(3, dtype=F.dtype, device=F.device)
+                  .reshape(3, 3, 1, 1, 1))
+    C.save_checkpoint_3d(path, step, E, nu, E_GL.permute(2, 3, 4, 0, 1).cpu().numpy(),
+                         Sig.permute(2, 3, 4, 0, 1).cpu().numpy(), F_mac, S_mac, pixel)
+
+
+# ------------------------------------------------ 2D plane strain ---
+_PLANE = (0, 2)  # 2D tensor index -> index in the embedded (nx, 1, ny) plan
+
+
+def _embed_2d(A2, fill, torch, dev):
+    """(2,2,nx,ny) -> tensor-first (3,3,nx,1,ny) device tensor; the out-of-plane
+    diagonal entry is ``fill``."""
+    A2 = torch.as_tensor(np.ascontiguousarray(A2, dtype=np.float64) if not hasattr(A2, "data_ptr") else A2,
+                         dtype=torch.float64, device=dev)
+    nx, ny = A2.shape[2:]
+    A3 = torch.zeros((3, 3, nx, 1, ny), dtype=torch.float64, device=dev)
+    for a, i in enumerate(_PLANE):
+        for b, j in enumerate(_PLANE):
+            A3[i, j, :, 0, :] = A2[a, b]
+    A3[1, 1] = fill
+    return A3
+
+
+def _extract_2d(A3):
+    return np.stack([np.stack([A3[i, j, :, 0, :] for j in _PLANE]) for i in _PLANE])
+
+
+def _embed_small(M2, fill, dtype=np.float64):
+    M3 = np.zeros((3, 3), dtype=dtype)
+    for a, i in enumerate(_PLANE):
+        for b, j in enumerate(_PLANE):
+            M3[i, j] = M2[a][b]
+    M3[1, 1] = fill
+    return M3
+
+
+class Fs2dSolver:
+    """2D plane-strain finite-strain solver: the 3D plan of an (nx, 1, ny) grid
+    with the out-of-plane axis y (F_yy = 1) and the 2D Newton norm
+    (``mgk_fs3d_set_plane_strain``).  Fields in and out are the reference's
+    tensor-first (2, 2, nx, ny)."""
+
+    def __init__(self, nx, ny, model="svk", precision="fp64", device=None):
+        self.nx, self.ny = int(nx), int(ny)
+        self.s = Fs3dSolver(self.nx, 1, self.ny, model=model, precision=precision, device=device)
+        L.check(L.lib().mgk_fs3d_set_plane_strain(self.s._h, 1), "mgk_fs3d_set_plane_strain")
+        self.device = self.s.device
+
+    def set_material(self, lam, mu, Fp=None, stream=None):
+        torch = _torch()
+        t = lambda a: torch.as_tensor(a, dtype=torch.float64, device=self.device).reshape(self.nx, 1, self.ny)
+        self._keep = (t(lam).contiguous(), t(mu).contiguous(),
+                      None if Fp is None else _embed_2d(Fp, 1.0, torch, self.device))
+        self.s.set_material(*self._keep, stream=stream)
+
+    def set_F(self, F, stream=None):
+        torch = _torch()
+        self._F = _embed_2d(F, 1.0, torch, self.device)
+        self.s.set_F(self._F, stream=stream)
+
+    def step(self, F_bar, driving_component=(0, 0), P_target=None, P_mask=None, E_avg=100e9, nu_avg=0.3,
+             tol_NW=1e-5, tol_CG=1e-6, max_NW=50, tol_macro=1e6, max_iter_macro=20, stream=None):
+        i, j = driving_component
+        Fb3, info = self.s.step(_embed_small(F_bar, 1.0), (_PLANE[i], _PLANE[j]),
+                                None if P_target is None else _embed_small(P_target, 0.0),
+                                None if P_mask is None else _embed_small(P_mask, False, bool), E_avg, nu_avg, tol_NW,
+                                tol_CG, max_NW, tol_macro, max_iter_macro, stream=stream)
+        return Fb3[np.ix_(_PLANE, _PLANE)].copy(), info
+
+    def get(self, stream=None):
+        """(F, P, Cauchy stress) as numpy (2, 2, nx, ny)."""
+        torch = _torch()
+        F3 = torch.empty((3, 3, self.nx, 1, self.ny), dtype=torch.float64, device=self.device)
+        P3, S3 = torch.empty_like(F3), torch.empty_like(F3)
+        self.s.get(F3, P3, S3, stream=stream)
+        return tuple(_extract_2d(t.cpu().numpy()) for t in (F3, P3, S3))
+
+
+_PLANS2 = {}
+
+
+def finite_strain_solver_step_2d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None, I4rt=None, Fp=None,
+                                 driving_component=(0, 0), P_target=None, P_mask=None, E_avg=100e9, nu_avg=0.3,
+                                 tol_NW=1e-5, tol_CG=1e-6, max_NW=50, tol_macro=1e6, max_iter_macro=20,
+                                 enable_console=True, model_type="svk", plane_mode="plane_strain", A_m=0.0, B_m=0.0,
+                                 C_m=0.0, solver="al", pixel=1.0, lam=None, mu=None, **unused):
+    """One mixed-BC 2D load step (mgkmc/finite_strain_simulator.py:2356-2572),
+    Newton-Krylov path, plane strain: returns (F, P, Sig, None, F_bar_current)
+    with (2, 2, nx, ny) fields.  The Lame fields come from ``C4`` (C4[0,0,1,1]
+    and C4[0,1,0,1], the reference's build_C4_2d) or ``lam``/``mu``."""
+    if solver not in ("newton_cg", "newton"):
+        raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
+    if model_type not in _MODEL:
+        raise NotImplementedError(f"model_type={model_type!r}: SVK and Neo-Hookean run on the GPU")
+    if plane_mode != "plane_strain":
+        raise NotImplementedError("plane_mode='plane_stress': only plane strain runs on the GPU")
+    torch = _torch()
+    F = np.ascontiguousarray(F, dtype=np.float64)
+    nx, ny = F.shape[2:]
+    if lam is None or mu is None:
+        lam = np.ascontiguousarray(C4[0, 0, 1, 1])
+        mu = np.ascontiguousarray(C4[0, 1, 0, 1])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (nx, ny, model_type, dev.index)
+    s = _PLANS2.get(key)
+    if s is None:
+        s = _PLANS2[key] = Fs2dSolver(nx, ny, model=model_type)
+    s.set_material(lam, mu, Fp)
+    s.set_F(F)
+    Fb, info = s.step(F_bar, driving_component, P_target, P_mask, E_avg, nu_avg, tol_NW, tol_CG, max_NW, tol_macro,
+                      max_iter_macro)
+    Fo, Po, So = s.get()
+    if enable_console:
+        print(f"finite strain 2D step: {info.macro_iterations} macro, {info.newton_iterations} Newton, "
+              f"{info.krylov_iterations} CG iterations")
+    return Fo, Po, So, None, Fb

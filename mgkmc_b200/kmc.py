@@ -38,6 +38,63 @@ def pure_shear_modes(theta, gamma0):
     return cat
 
 
+class GeneratorDraws:
+    """The driver's draws from an explicit numpy Generator, in a fixed order:
+    per attempt u_wait; per event u_sel, then M orientations theta ~ U[0, pi)
+    (pure-shear modes of amplitude gamma0/2) and M barriers N(q_mean, q_std)
+    clipped below at q_min."""
+
+    def __init__(self, rng, gamma0, q_mean, q_std, q_min):
+        self.rng, self.gamma0, self.q = rng, gamma0, (q_mean, q_std, q_min)
+
+    def u_wait(self):
+        return self.rng.random()
+
+    def u_sel(self):
+        return self.rng.random()
+
+    def catalog(self, M):
+        return pure_shear_modes(self.rng.uniform(0.0, np.pi, M), self.gamma0)
+
+    def q0(self, M):
+        return np.clip(self.rng.normal(self.q[0], self.q[1], M), self.q[2], None)
+
+
+class ReferenceDraws:
+    """The reference simulator's draws, call for call, from a numpy
+    RandomState standing for its global stream: t_wait = -ln(rand()) / total
+    (kmc_simulator.py:893); the selection threshold uniform(0, total)
+    (kmc_simulator_functions.py:62, taken here as u = U with r = u * total);
+    the redrawn catalog of stz_catalog_glass_2d (:78-98: per mode
+    gxx = 0.5 gamma0 N(0,1), then gxy, pure shear); the redrawn barriers of the
+    Gaussian generator (:222-229: normal(mean, std, size=M) clipped)."""
+
+    def __init__(self, rs, gamma0, mean, std, min_cutoff=None, max_cutoff=None):
+        self.rs, self.gamma0 = rs, gamma0
+        self.mean, self.std, self.lo, self.hi = mean, std, min_cutoff, max_cutoff
+
+    def u_wait(self):
+        return self.rs.rand()
+
+    def u_sel(self):
+        return self.rs.uniform(0.0, 1.0)
+
+    def catalog(self, M):
+        cat = np.zeros((M, 2, 2))
+        for i in range(M):
+            gxx = 0.5 * self.gamma0 * self.rs.normal()
+            gxy = 0.5 * self.gamma0 * self.rs.normal()
+            cat[i, 0, 0], cat[i, 1, 1] = gxx, -gxx
+            cat[i, 0, 1] = cat[i, 1, 0] = gxy
+        return cat
+
+    def q0(self, M):
+        b = self.rs.normal(loc=self.mean, scale=self.std, size=(M,))
+        if self.lo is not None or self.hi is not None:
+            b = np.clip(b, self.lo, self.hi)
+        return b
+
+
 class Kmc2D:
     def __init__(self, E, nu, catalog, Q0, gamma0=0.1, T=300.0, nu0=1e13, strain_rate=1e7, step_size=1e-5,
                  q_act_temp=0.37, jp=0.0, jt=0.0, cap=2.0, jn=0.0, stress_targets=None, mixed_tol=1e4,
@@ -122,6 +179,40 @@ class Kmc2D:
         self.time = 0.0
         self.events = []
         self.n_solves = 0
+        self.steps_done = 0
+        self._resume = False  # set by load_state_dict: the fields are the state, no initial solve
+
+    # ------------------------------------------------------- checkpoints ---
+    _FIELDS = ("E", "nu", "eps", "sig", "eps_p", "soft", "Q", "Q0", "catalog", "t_last", "prev")
+
+    def state_dict(self):
+        """Host copies of the trajectory state between AQS steps (the fields,
+        the clock, the macro strain, the event list and counters)."""
+        self.stream.synchronize()
+        st = {k: getattr(self, k).cpu().numpy() for k in self._FIELDS}
+        st.update(eps_macro=self.eps_macro.copy(), time=self.time, events=list(self.events),
+                  n_solves=self.n_solves, steps_done=self.steps_done, unit_ready=self.unit_ready,
+                  flips_since_sync=self.flips_since_sync)
+        return st
+
+    def load_state_dict(self, st):
+        """Restores a state from ``state_dict`` (same grid, modes and
+        material); the next ``trajectory`` continues from it without the
+        initial re-solve (the stored fields are that solve's result)."""
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            for k in self._FIELDS:
+                getattr(self, k).copy_(torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float64)).to(self.dev))
+        self.ls.set_eigenstrain(self.rep, self.eps_p, stream=self.stream)
+        self.eps_macro = np.array(st["eps_macro"], dtype=np.float64).reshape(2, 2)
+        self.time = float(st["time"])
+        self.events = [tuple(e) for e in st["events"]]
+        self.n_solves = int(st["n_solves"])
+        self.steps_done = int(st["steps_done"])
+        self.unit_ready = bool(st.get("unit_ready", False))
+        self.flips_since_sync = int(st.get("flips_since_sync", 0))
+        self._resume = True
+        self.stream.synchronize()
 
     def _setup_patches(self, precision):
         """LS responses to unit eigenstrains [[1,0],[0,-1]] and [[0,1],[1,0]] at
@@ -229,10 +320,13 @@ class Kmc2D:
         self.stream.synchronize()
         return float(self.total_h[0])
 
-    def event(self, u_sel, theta, q0, t_wait=0.0):
+    def event(self, u_sel, new_catalog, q0, t_wait=0.0):
+        """One KMC event on the device: selection with the draw u_sel, the flip
+        and its bookkeeping, the redraw of the voxel's catalog (new_catalog,
+        (M, 2, 2)) and barriers (q0, (M,))."""
         lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
         M = self.M
-        self.redraw_h[:4 * M] = self.torch.from_numpy(pure_shear_modes(theta, p["gamma0"]).reshape(-1))
+        self.redraw_h[:4 * M] = self.torch.from_numpy(np.ascontiguousarray(new_catalog, dtype=np.float64).reshape(-1))
         self.redraw_h[4 * M:] = self.torch.from_numpy(q0)
         self.redraw.copy_(self.redraw_h, non_blocking=True)
         total = self.total
@@ -291,7 +385,7 @@ class Kmc2D:
                 batch.append(int(f))
         return batch
 
-    def cascade_flips_batch(self, batch, rng):
+    def cascade_flips_batch(self, batch, draws):
         """Flips the batch's modes in order, each with the bookkeeping and
         redraws of a KMC event (kmc_simulator.py:728-760)."""
         lib, S, p = L.lib(), L.stream_ptr(self.stream), self.p
@@ -300,10 +394,8 @@ class Kmc2D:
         sel_h = torch.tensor(batch, dtype=torch.int64).pin_memory()
         red_h = torch.empty((k, 5 * M), dtype=torch.float64).pin_memory()
         for i in range(k):
-            theta = rng.uniform(0.0, np.pi, M)
-            q0 = np.clip(rng.normal(p["q_mean"], p["q_std"], M), p["q_min"], None)
-            red_h[i, :4 * M] = torch.from_numpy(pure_shear_modes(theta, p["gamma0"]).reshape(-1))
-            red_h[i, 4 * M:] = torch.from_numpy(q0)
+            red_h[i, :4 * M] = torch.from_numpy(np.ascontiguousarray(draws.catalog(M), dtype=np.float64).reshape(-1))
+            red_h[i, 4 * M:] = torch.from_numpy(np.ascontiguousarray(draws.q0(M), dtype=np.float64))
         with torch.cuda.stream(self.stream):
             sel_d = sel_h.to(self.dev, non_blocking=True)
             red_d = red_h.to(self.dev, non_blocking=True)
@@ -329,12 +421,18 @@ class Kmc2D:
         ``stream`` must complete; it returns the result dict.  A scheduler can
         advance many trajectories and batch their solves; ``run`` drives one."""
         p = self.p
-        self.after_solve((yield ("solve",)))
+        draws = rng if hasattr(rng, "u_wait") else GeneratorDraws(rng, p["gamma0"], p["q_mean"], p["q_std"],
+                                                                  p["q_min"])
+        if self._resume:
+            # restored between AQS steps: the stored fields are the last solve's
+            self._resume = False
+        else:
+            self.after_solve((yield ("solve",)))
         strain_unit = np.zeros((2, 2))
         strain_unit[0, 0] = 1.0
         dt_step = abs(p["step_size"]) / p["strain_rate"] if p["strain_rate"] > 0 else 1.0
         remaining = 0.0
-        steps_done = 0
+        steps_done = self.steps_done
         M = self.M
         cascade_count = 0
         n_batches = 0
@@ -349,7 +447,7 @@ class Kmc2D:
                         # _run_cascade: batches until no mode is unstable
                         local_step = flips = 0
                         while batch:
-                            self.cascade_flips_batch(batch, rng)
+                            self.cascade_flips_batch(batch, draws)
                             for f in batch:
                                 x, y, m = f // (self.ny * M), (f // M) % self.ny, f % M
                                 self.cascade_flips.append((x, y, m, self.time, n_batches))
@@ -376,16 +474,16 @@ class Kmc2D:
                 yield ("sync",)
                 total = float(self.total_h[0])
                 if total > 0:
-                    u = rng.random()
+                    u = draws.u_wait()
                     t_wait = -np.log(u) / total
                     if t_wait < remaining:
                         self.time += t_wait
                         self.eps_macro += strain_unit * (p["strain_rate"] * t_wait)
                         remaining -= t_wait
-                        u_sel = rng.random()
-                        theta = rng.uniform(0.0, np.pi, M)
-                        q0 = np.clip(rng.normal(p["q_mean"], p["q_std"], M), p["q_min"], None)
-                        self.event(u_sel, theta, q0, t_wait)
+                        u_sel = draws.u_sel()
+                        new_cat = draws.catalog(M)
+                        q0 = draws.q0(M)
+                        self.event(u_sel, new_cat, q0, t_wait)
                         if not self.fast:
                             self.after_solve((yield ("solve",)))
                         else:
@@ -431,6 +529,7 @@ class Kmc2D:
                     prev_s[idx] = sigM[idx]
                     self.eps_macro[idx] += step
             steps_done += 1
+            self.steps_done = steps_done
         return self.result(steps_done)
 
     def run(self, rng, n_steps, max_events=None):
@@ -450,6 +549,7 @@ class Kmc2D:
                 send = None
 
     def result(self, steps):
+        self.steps_done = steps
         return dict(events=list(self.events), eps_macro=self.eps_macro.copy(), sig=self.sig.cpu().numpy(),
                     eps_p=self.eps_p.cpu().numpy(), time=self.time, steps=steps, solves=self.n_solves,
                     cascade_flips=list(self.cascade_flips))

@@ -539,3 +539,155 @@ def update_stress_fft_full(eps_plastic_field, eps_macro, E, nu, pixel=1.0, max_i
     """mgkmc/stz/update_fft.py:4-22: the 3D solve with an eigenstrain field."""
     return spectral_solver_3d(E, nu, eps_macro, eps_plastic=eps_plastic_field, max_iter=max_iter, tol=tol,
                               verbose=verbose, pixel=pixel)
+
+
+# ------------------------------------------------ mixed-BC load ramps ---
+_COMP_LABELS = {(0, 0): "xx", (1, 1): "yy", (2, 2): "zz", (0, 1): "xy", (0, 2): "xz", (1, 2): "yz", (1, 0): "yx",
+                (2, 0): "zx", (2, 1): "zy"}
+
+
+def _ramp(dim, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls, max_iter_ls, tol_macro,
+          max_iter_macro, store, plane_mode, log_path, global_log_path, driving_component, enable_console, vtk_path,
+          vtk_interval, solver_kw):
+    """Mixed stress/strain load ramp of linear_elastic_simulation_2d/3d
+    (linear_elastic_simulator.py:90-272 / :378-566) on one device-resident LS
+    plan: targets ramped linearly over n_steps + 1 load steps; per load step
+    the macro loop (:176-197) solves with the prescribed strain components,
+    corrects the stress-controlled ones by the isotropic compliance
+    (:150-152) until their mean-stress error is below tol_macro; every solve
+    of a load step warm-starts from the previous load step's final field
+    (:199).  Fields stay on the device between solves; only the stored
+    fields and the per-step means come back."""
+    import time as _time
+    from datetime import datetime as _dt
+    torch = _torch()
+    if vtk_interval not in (None, "none"):
+        raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
+    chk_ival = solver_kw.pop("checkpoint_interval", None)
+    chk_path = solver_kw.pop("checkpoint_path", "checkpoint")
+    if chk_path and chk_ival not in (None, "none"):
+        import os
+        os.makedirs(os.path.dirname(chk_path) or ".", exist_ok=True)
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    shape = E.shape
+    mask = np.asarray(target_strain_mask, dtype=bool)
+    target_values = np.asarray(target_values, dtype=np.float64)
+    stress_mask = ~mask
+    dev = torch.device("cuda", torch.cuda.current_device())
+    plan = Ls2dBatch([shape], plane_mode=plane_mode) if dim == 2 else Ls3dBatch([shape])
+    t = lambda a: torch.from_numpy(a).to(dev)
+    plan.set_material(0, t(E), t(nu), None)
+    E_avg, nu_avg = E.mean(), nu.mean()
+    fshape = shape + (dim, dim)
+    eps = torch.empty(fshape, dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    warm = torch.empty_like(eps)
+    have_warm = False
+    lbl = _COMP_LABELS.get(tuple(driving_component), "xx")
+    log_f = open(log_path, "w", buffering=1) if log_path else None
+    if log_f:
+        hdr = f"{'Timestamp':<20} {'Elapsed(s)':<12} {'Step':<8} {'Eps_' + lbl:<14} {'Sig_' + lbl + '(GPa)':<16}\n"
+        log_f.write(hdr)
+        log_f.write("-" * len(hdr.rstrip()) + "\n")
+    glog_f = open(global_log_path, "w", buffering=1) if global_log_path else None
+    comps = [(0, 0), (1, 1), (0, 1)] if dim == 2 else [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    if glog_f:
+        ghdr = f"{'GlobalStep':<12} " + " ".join(f"{'Eps_' + _COMP_LABELS[c]:<14}" for c in comps) + " " + \
+               " ".join(f"{'Sig_' + _COMP_LABELS[c] + '(GPa)':<16}" for c in comps) + "\n"
+        glog_f.write(ghdr)
+        glog_f.write("-" * len(ghdr.rstrip()) + "\n")
+    t0 = _time.time()
+    eps_macro_list, sig_macro_list, eps_list, sig_list = [], [], [], []
+    cur = np.zeros((dim, dim))
+    axes = tuple(range(dim))
+    for s in range(n_steps + 1):
+        target_s = target_values * (s / n_steps)
+        max_err = 0.0
+        for _ in range(max_iter_macro):
+            cur[mask] = target_s[mask]
+            info = plan.solve([0], [cur], [eps], [sig], eps_init=[warm] if have_warm else None, max_iter=max_iter_ls,
+                              tol=tol_ls)[0]
+            sigM = np.array(info.sig_mean).reshape(dim, dim)
+            err = np.zeros((dim, dim))
+            err[stress_mask] = target_s[stress_mask] - sigM[stress_mask]
+            max_err = np.max(np.abs(err[stress_mask])) if np.any(stress_mask) else 0.0
+            if max_err < tol_macro:
+                break
+            d_eps = (err - nu_avg * np.trace(err) * np.eye(dim)) / E_avg
+            cur[stress_mask] += d_eps[stress_mask]
+        else:
+            print(f"Warning: Macro loop did not converge at step {s} (err={max_err:.2e})")
+        warm.copy_(eps)
+        have_warm = True
+        e_np, s_np = eps.cpu().numpy(), sig.cpu().numpy()
+        epsM, sigM = e_np.mean(axis=axes), s_np.mean(axis=axes)
+        eps_macro_list.append(epsM)
+        sig_macro_list.append(sigM)
+        if store:
+            eps_list.append(e_np)
+            sig_list.append(s_np)
+        i, j = driving_component
+        if enable_console:
+            print(f"step {s}/{n_steps}: eps_{lbl}={epsM[i, j]:.4f}, sig_{lbl}={sigM[i, j] / 1e9:.4f} GPa")
+        if log_f:
+            log_f.write(f"{_dt.now().strftime('%Y-%m-%d %H:%M:%S'):<20} {_time.time() - t0:<12.3f} {s:<8} "
+                        f"{epsM[i, j]:<14.6f} {sigM[i, j] / 1e9:<16.6f}\n")
+        if glog_f:
+            glog_f.write(f"{s:<12} " + " ".join(f"{epsM[c]:<14.6f}" for c in comps) + " " +
+                         " ".join(f"{sigM[c] / 1e9:<16.6f}" for c in comps) + "\n")
+        if chk_ival is not None and chk_ival not in ("none", "last"):
+            name = None
+            if chk_ival == "current":
+                name = f"{chk_path}.h5"
+            elif isinstance(chk_ival, int) and s % chk_ival == 0:
+                name = f"{chk_path}_{s:06d}.h5"
+            if name:
+                _save_chk(dim, name, s, E, nu, e_np, s_np, epsM, sigM, pixel)
+    if chk_ival == "last" or (isinstance(chk_ival, int) and n_steps % chk_ival != 0):
+        _save_chk(dim, f"{chk_path}_final.h5", n_steps, E, nu, e_np, s_np, epsM, sigM, pixel)
+    total = _time.time() - t0
+    m_, s_ = divmod(total, 60)
+    h_, m_ = divmod(m_, 60)
+    dur = (f"\nSimulation Finish Time: {_dt.now().strftime('%Y-%m-%d %H:%M:%S')}\nTotal Duration: {total:.2f} seconds "
+           f"({int(h_):d}h {int(m_):02d}m {int(s_):02d}s)\n")
+    if log_f:
+        log_f.write(dur)
+        log_f.close()
+    if glog_f:
+        glog_f.close()
+    if enable_console:
+        print(dur)
+    return np.array(eps_macro_list), np.array(sig_macro_list), eps_list, sig_list
+
+
+def _save_chk(dim, path, step, E, nu, eps, sig, epsM, sigM, pixel):
+    from . import checkpoint as C
+    if path.endswith(".h5") and not C._HAVE_H5PY:
+        path = path[:-3]  # the .npz container of the same layout
+    (C.save_checkpoint_2d if dim == 2 else C.save_checkpoint_3d)(path, step, E, nu, eps, sig, epsM, sigM, pixel)
+
+
+def linear_elastic_simulation_2d(E, nu, target_strain_mask, target_values, n_steps=20, pixel=1.0, tol_ls=1e-6,
+                                 max_iter_ls=200, tol_macro=1e-4, max_iter_macro=20, store=True,
+                                 plane_mode="plane_strain", log_path=None, global_log_path=None,
+                                 driving_component=(0, 0), enable_console=True, vtk_path=None, vtk_interval="none",
+                                 **solver_kw):
+    """Mixed stress/strain control in 2D (linear_elastic_simulator.py:90-272):
+    returns (eps_macro (n_steps+1,2,2), sig_macro (n_steps+1,2,2), eps list,
+    sig list).  Checkpoints (``checkpoint_interval``/``checkpoint_path``) use
+    the reference's layout (``mgkmc_b200.checkpoint``)."""
+    return _ramp(2, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls, max_iter_ls, tol_macro,
+                 max_iter_macro, store, plane_mode, log_path, global_log_path, driving_component, enable_console,
+                 vtk_path, vtk_interval, dict(solver_kw))
+
+
+def linear_elastic_simulation_3d(E, nu, target_strain_mask, target_values, n_steps=20, pixel=1.0, tol_ls=1e-6,
+                                 max_iter_ls=200, tol_macro=1e-4, max_iter_macro=20, store=True, log_path=None,
+                                 global_log_path=None, driving_component=(0, 0), enable_console=True, vtk_path=None,
+                                 vtk_interval="none", **solver_kw):
+    """Mixed stress/strain control in 3D (linear_elastic_simulator.py:378-566);
+    returns as linear_elastic_simulation_2d with (…,3,3) tensors."""
+    return _ramp(3, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls, max_iter_ls, tol_macro,
+                 max_iter_macro, store, "plane_strain", log_path, global_log_path, driving_component, enable_console,
+                 vtk_path, vtk_interval, dict(solver_kw))

@@ -244,3 +244,31 @@ def constitutive_2d_plane_strain_nh(F2, lam, mu):
     F3[..., 2, 2] = 1.0
     P, st = constitutive(F3, lam, mu, np.broadcast_to(np.eye(3), F3.shape), "neo_hookean", has_fp=False)
     return P[..., :2, :2], st
+
+
+# 2D plane strain as a 3D problem: the plane's axes (x, y) become the 3D axes
+# (x, z), the out-of-plane axis is the 3D y axis (one voxel thick) with
+# F_yy = 1.  Tensor indices map 0 -> 0, 1 -> 2.
+PLANE_AXES = (0, 2)
+
+
+def embed_plane_2d(A2, fill=1.0):
+    """Tensor-first (2,2,nx,ny) -> spatial-first (nx,1,ny,3,3); the
+    out-of-plane diagonal entry is ``fill`` (1 for F and F_p, 0 for P)."""
+    nx, ny = A2.shape[2:]
+    A3 = np.zeros((nx, 1, ny, 3, 3))
+    for a, i in enumerate(PLANE_AXES):
+        for b, j in enumerate(PLANE_AXES):
+            A3[:, 0, :, i, j] = A2[a, b]
+    A3[:, 0, :, 1, 1] = fill
+    return A3
+
+
+def extract_plane_2d(A3):
+    """Spatial-first (nx,1,ny,3,3) -> tensor-first (2,2,nx,ny)."""
+    nx, _, ny = A3.shape[:3]
+    A2 = np.zeros((2, 2, nx, ny))
+    for a, i in enumerate(PLANE_AXES):
+        for b, j in enumerate(PLANE_AXES):
+            A2[a, b] = A3[:, 0, :, i, j]
+    return A2

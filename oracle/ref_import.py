@@ -69,10 +69,12 @@ def install_stubs():
 
 
 def import_reference(path=None):
-    """Import the reference ``mgkmc`` package from ``path`` (default: env
-    ``MGKMC_REFERENCE`` or the reference checkout next to this repository)."""
+    """Import the reference ``mgkmc`` package from ``path`` (default: the
+    environment variable ``MGKMC_REFERENCE``; one of the two is required)."""
     install_stubs()
-    path = path or os.environ.get("MGKMC_REFERENCE", "/root/reference")
+    path = path or os.environ.get("MGKMC_REFERENCE")
+    if not path:
+        raise FileNotFoundError("reference checkout not given: pass a path or set MGKMC_REFERENCE")
     if not os.path.isdir(os.path.join(path, "mgkmc")):
         raise FileNotFoundError(f"reference package not found under {path}")
     if path not in sys.path:

@@ -26,7 +26,7 @@ sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
 from oracle.ref_import import import_reference  # noqa: E402
 from mgkmc_b200 import workloads as W  # noqa: E402
 
-import_reference()
+import_reference(os.environ.get("MGKMC_REFERENCE", "/root/reference"))
 from mgkmc import linear_elastic_simulator as LES  # noqa: E402
 from mgkmc import kmc_simulator_functions as KF  # noqa: E402
 from mgkmc import finite_strain_simulator as FS  # noqa: E402
@@ -366,15 +366,160 @@ def kmc2d_patch_fixtures():
     save("kmc2d_patch_16x12", **out)
 
 
+def kmc2d_trajectory_fixtures():
+    """A short trajectory of the reference's own KMC driver
+    (KmcSimulation2D.run_simulation, kmc_simulator.py:796-1157): small-strain
+    linear elasticity, KMC mode, softening off, every draw from numpy's global
+    stream (select_event_2d replaced by its pure-Python body, whose uniform
+    draw then comes from that stream instead of numba's).  Saves the initial
+    catalog and barriers, the RandomState state the run starts from, the
+    events (x, y, m, time) seen by the flip callback, the final macro strain,
+    stress and eigenstrain fields."""
+    import tempfile
+    from mgkmc import kmc_simulator as KS
+    nx, ny, M = 12, 8, 4
+    rng = np.random.default_rng(41)
+    E, nu = W.ls2d_material(nx, ny, rng)
+    KS.select_event_2d = KF.select_event_2d.py_func
+    np.random.seed(5)
+    with tempfile.TemporaryDirectory() as tmp:
+        sim = KS.KmcSimulation2D(nx, ny, M, 0.1, E, nu, barrier_generator="gaussian",
+                                 barrier_kwargs=dict(mean=0.6, std=0.15, min_cutoff=0.3), softening_cap=2.0,
+                                 jp=0.0, jt=0.0, temperature=300.0, strain_rate=1e7, output_dir=tmp)
+        cat0, Q00 = sim.catalog.copy(), sim.Q0.copy()
+        st = np.random.get_state()
+        events = []
+        sim.flip_callback = lambda s, x, y, m, *rest: events.append((x, y, m, s.time))
+        sim.run_simulation(60, 1e-4, component=(0, 0), stress_targets={(1, 1): 0.0}, mixed_tol=1e4,
+                           mixed_max_iter=50, enable_console_log=False, enable_summary_log=False,
+                           enable_global_log=False)
+    ev = np.array([e[:3] for e in events], dtype=np.int64).reshape(-1, 3)
+    times = np.array([e[3] for e in events], dtype=np.float64)
+    print(f"reference trajectory: {len(events)} events, final strain {sim.eps_macro[0, 0]:.5f}")
+    save("kmc2d_traj_12x8", E=E, nu=nu, catalog0=cat0, Q00=Q00, rs_keys=st[1], rs_pos=np.int64(st[2]),
+         rs_has_gauss=np.int64(st[3]), rs_gauss=np.float64(st[4]), n_steps=np.int64(60), step_size=1e-4,
+         events=ev, times=times, eps_macro=sim.eps_macro, sig=sim.sig_field, eps_plastic=sim.eps_plastic,
+         catalog=sim.catalog, Q0=sim.Q0)
+    KS.select_event_2d = KF.select_event_2d
+
+
+def driver_fixtures():
+    """The reference's 3D mixed-BC small-strain ramp and its 3D finite-strain
+    load ramp (Newton-CG, SVK), both run end to end."""
+    rng = np.random.default_rng(13)
+    shape = (8, 6, 4)
+    E, nu = W.ls3d_material(*shape, rng)
+    mask = np.ones((3, 3), bool)
+    mask[1, 1] = mask[2, 2] = False
+    target = np.zeros((3, 3))
+    target[0, 0] = 0.01
+    target[0, 1] = target[1, 0] = 0.002
+    epsM, sigM, eps_l, sig_l = LES.linear_elastic_simulation_3d(
+        E, nu, mask, target, n_steps=2, tol_ls=1e-10, max_iter_ls=300, tol_macro=1e3, max_iter_macro=30,
+        enable_console=False)
+    save("ls3d_macro_8x6x4", E=E, nu=nu, mask=mask, target=target, epsM=np.array(epsM), sigM=np.array(sigM),
+         eps_last=eps_l[-1], sig_last=sig_l[-1])
+
+    rng = np.random.default_rng(14)
+    shape = (6, 6, 6)
+    E, nu, _ = W.fs3d_material(*shape, rng)
+    Fm, Sm, Pm, F_l, S_l = FS.finite_strain_simulation_3d(
+        E, nu, (0, 0), 0.01, 2, mixed_targets={(1, 1): 0.0, (2, 2): 0.0}, tol_NW=1e-10, tol_CG=1e-11, max_NW=30,
+        tol_macro=1e3, max_iter_macro=30, enable_console=False, model_type="svk", solver="newton_cg")
+    save("fs3d_sim_6", E=E, nu=nu, F_macro=Fm, Sig_macro=Sm, P_macro=Pm, F_last=F_l[-1], Sig_last=S_l[-1])
+
+
+def kmc3d_trajectory_fixtures():
+    """A short trajectory of the reference's own 3D driver
+    (ThermalSimulation.run_simulation, aqs.py:682-1201): small strain, KMC
+    mode, softening off, draws from numpy's global stream (select_event
+    replaced by its pure-Python body).  apply_flip_soa is wrapped to record
+    each flip's (x, y, z, m, time)."""
+    import tempfile
+    from mgkmc import aqs as AQ
+    nx, ny, nz, M = 6, 6, 4, 4
+    rng = np.random.default_rng(42)
+    E, nu = W.ls3d_material(nx, ny, nz, rng)
+    flips = []
+    orig_flip = AQ.apply_flip_soa
+
+    def rec_flip(eps_p, _, soft, tl, cat, x, y, z, m, t, *rest):
+        flips.append((x, y, z, m, t))
+        return orig_flip(eps_p, _, soft, tl, cat, x, y, z, m, t, *rest)
+
+    AQ.select_event = SK.select_event.py_func
+    AQ.apply_flip_soa = rec_flip
+    np.random.seed(6)
+    with tempfile.TemporaryDirectory() as tmp:
+        sim = AQ.ThermalSimulation(nx, ny, nz, M, 0.1, E, nu, barrier_generator="gaussian",
+                                   barrier_kwargs=dict(mean=0.4, std=0.15, min_cutoff=0.2), softening_cap=2.0,
+                                   jp=0.0, jt=0.0, temperature=300.0, strain_rate=1e7, output_dir=tmp)
+        cat0, Q00 = sim.catalog.copy(), sim.Q0.copy()
+        st = np.random.get_state()
+        sim.run_simulation(60, 1e-4, component=(0, 0), stress_targets={(1, 1): 0.0, (2, 2): 0.0}, mixed_tol=1e4,
+                           mixed_max_iter=50, checkpoint_interval=None, enable_console_log=False,
+                           enable_summary_log=False, enable_global_log=False, enable_cascade_log=False,
+                           enable_kmc_log=False)
+    AQ.select_event = SK.select_event
+    AQ.apply_flip_soa = orig_flip
+    ev = np.array([f[:4] for f in flips], dtype=np.int64).reshape(-1, 4)
+    times = np.array([f[4] for f in flips], dtype=np.float64)
+    print(f"reference 3D trajectory: {len(flips)} events, final strain {sim.eps_macro[0, 0]:.5f}")
+    save("kmc3d_traj_6x6x4", E=E, nu=nu, catalog0=cat0, Q00=Q00, rs_keys=st[1], rs_pos=np.int64(st[2]),
+         rs_has_gauss=np.int64(st[3]), rs_gauss=np.float64(st[4]), n_steps=np.int64(60), step_size=1e-4,
+         events=ev, times=times, eps_macro=sim.eps_macro, sig=sim.sig_field, eps_plastic=sim.eps_plastic,
+         catalog=sim.catalog, Q0=sim.Q0)
+
+
+def fs2d_step_fixtures():
+    """The reference's 2D finite-strain path, plane strain:
+    * its Newton-CG load step (finite_strain_solver_step_2d, solver="newton_cg",
+      :2356-2572), SVK without F_p, F_bar fully prescribed (1.01, 0.996).  With
+      F_p, or with the Neo-Hookean law, or with a stress-controlled component,
+      its BiCGSTAB solves stall at small right-hand sides on this medium
+      (info 150) and the Newton loop diverges, so those converged states are
+      pinned through the law instead;
+    * its constitutive law (constitutive_hyperelastic_2d :591-1087) with a
+      plastic eigen-deformation field, SVK and Neo-Hookean: P and the Cauchy
+      stress at a perturbed F."""
+    rng = np.random.default_rng(71)
+    nx, ny = 12, 8
+    E, nu = W.ls2d_material(nx, ny, rng)
+    I2, I4, I4rt, I4s, II = FS._make_identity_tensors_2d(nx, ny)
+    Ghat4 = FS.build_ghat4_2d(nx, ny, float(nx), float(ny))
+    C4 = FS.build_C4_2d(E, nu, I4s, II, plane_mode="plane_strain")
+    Fp = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    sel = rng.random((nx, ny)) < 0.15
+    G = rng.standard_normal((2, 2, nx, ny))
+    S = 0.5 * (G + G.transpose(1, 0, 2, 3))
+    S -= 0.5 * (S[0, 0] + S[1, 1]) * np.eye(2)[:, :, None, None]
+    S /= np.sqrt(np.sum(S * S, axis=(0, 1)))
+    Fp += 0.05 * S * sel
+    F0 = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    Fb = np.diag([1.01, 0.996])
+    F, P, Sig, _, Fbo = FS.finite_strain_solver_step_2d(
+        F0, Fb, Ghat4, C4, I2, I4, I4rt, Fp=None, driving_component=(0, 0), E_avg=E.mean(), nu_avg=nu.mean(),
+        tol_NW=1e-9, tol_CG=1e-10, max_NW=30, enable_console=False, model_type="svk", plane_mode="plane_strain",
+        solver="newton_cg")
+    out = dict(E=E, nu=nu, Fp=Fp, F_bar=Fb, svk_F=F, svk_P=P, svk_Sig=Sig)
+    Fr = F0 + 0.02 * rng.standard_normal((2, 2, nx, ny))
+    out["F_law"] = Fr
+    for model in ("svk", "neo_hookean"):
+        Pl, _, F33 = FS.constitutive_hyperelastic_2d(Fr, C4, I2, I4, I4rt, Fp=Fp, model_type=model,
+                                                     plane_mode="plane_strain")
+        out[f"{model}_P_law"] = Pl
+        out[f"{model}_Sig_law"] = FS.cauchy_from_P(Pl, Fr, F33=F33)
+    save("fs2d_step_12x8", **out)
+
+
+ALL = ("ls2d_fixtures", "ls3d_fixtures", "kmc2d_fixtures", "kmc3d_fixtures", "fs3d_fixtures", "ls2d_secant_fixtures",
+       "ls2d_rose_fixtures", "kmc2d_cascade_fixtures", "kmc2d_patch_fixtures", "ls3d_secant_fixtures",
+       "ls2d_landau_fixtures", "kmc2d_trajectory_fixtures", "driver_fixtures",
+       "kmc3d_trajectory_fixtures", "fs2d_step_fixtures")
+
+
 if __name__ == "__main__":
-    ls2d_fixtures()
-    ls3d_fixtures()
-    kmc2d_fixtures()
-    kmc3d_fixtures()
-    fs3d_fixtures()
-    ls2d_secant_fixtures()
-    ls2d_rose_fixtures()
-    kmc2d_cascade_fixtures()
-    kmc2d_patch_fixtures()
-    ls3d_secant_fixtures()
-    ls2d_landau_fixtures()
+    # python make_golden.py [fixture function names]  (default: all)
+    for name in (sys.argv[1:] or ALL):
+        globals()[name]()
+

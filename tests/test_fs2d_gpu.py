@@ -1,0 +1,74 @@
+"""GPU parity of the 2D plane-strain finite-strain step
+(finite_strain_solver_step_2d, Newton-CG path) run on the embedded (nx, 1, ny)
+plan: against the reference's own Newton step (SVK, F_bar prescribed; golden)
+and against the oracle's step on the embedded problem (SVK and Neo-Hookean
+with plastic eigen-deformations, lateral Cauchy stress driven to zero), whose
+law tests/test_oracle_fs.py pins to the reference's 2D law.  Tolerance 1e-9
+relative."""
+import numpy as np
+import pytest
+
+from mgkmc_b200 import workloads as W
+from oracle import fs as OF
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_newton_step_matches_reference(golden):
+    from mgkmc_b200.finite_strain_simulator import finite_strain_solver_step_2d
+    g = golden("fs2d_step_12x8")
+    nx, ny = g["E"].shape
+    lam = g["E"] * g["nu"] / ((1 + g["nu"]) * (1 - 2 * g["nu"]))
+    mu = g["E"] / (2 * (1 + g["nu"]))
+    F0 = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    F, P, Sig, _, Fb = finite_strain_solver_step_2d(
+        F0, g["F_bar"], driving_component=(0, 0), E_avg=g["E"].mean(), nu_avg=g["nu"].mean(), tol_NW=1e-12,
+        tol_CG=1e-13, max_NW=30, enable_console=False, model_type="svk", solver="newton_cg", lam=lam, mu=mu)
+    assert np.max(np.abs(F - g["svk_F"])) < 1e-9
+    assert rel(P, g["svk_P"]) < 1e-9
+    assert rel(Sig, g["svk_Sig"]) < 1e-9
+
+
+def _fp2(nx, ny, rng, frac=0.15, amp=0.05):
+    Fp = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    sel = rng.random((nx, ny)) < frac
+    G = rng.standard_normal((2, 2, nx, ny))
+    S = 0.5 * (G + G.transpose(1, 0, 2, 3))
+    S -= 0.5 * (S[0, 0] + S[1, 1]) * np.eye(2)[:, :, None, None]
+    S /= np.sqrt(np.sum(S * S, axis=(0, 1)))
+    return Fp + amp * S * sel
+
+
+@pytest.mark.parametrize("model,shape", [("neo_hookean", (16, 12)), ("svk", (24, 16)), ("neo_hookean", (64, 48))])
+def test_mixed_bc_step_with_fp_matches_oracle(model, shape):
+    from mgkmc_b200.finite_strain_simulator import finite_strain_solver_step_2d
+    nx, ny = shape
+    rng = np.random.default_rng(nx + ny)
+    E, nu = W.ls2d_material(nx, ny, rng)
+    Fp = _fp2(nx, ny, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    # oracle: the 3D step on the embedded problem (plane axes x, z)
+    F0 = OF.embed_plane_2d(np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny))))
+    Fb3 = np.eye(3)
+    Fb3[0, 0] = 1.01
+    Pm3 = np.zeros((3, 3), bool)
+    Pm3[2, 2] = True
+    Fo, Po, So, Fbo = OF.solver_step_3d(F0, Fb3, E[:, None, :], nu[:, None, :], OF.embed_plane_2d(Fp), (0, 0),
+                                        np.zeros((3, 3)), Pm3, tol_NW=1e-12, tol_CG=1e-13, max_NW=40, tol_macro=1e2,
+                                        max_iter_macro=40, model=model, krylov="cg")
+    Fb2 = np.diag([1.01, 1.0])
+    Pm2 = np.array([[False, False], [False, True]])
+    F, P, Sig, _, Fb = finite_strain_solver_step_2d(
+        OF.extract_plane_2d(F0), Fb2, Fp=Fp, driving_component=(0, 0), P_target=np.zeros((2, 2)), P_mask=Pm2,
+        E_avg=E.mean(), nu_avg=nu.mean(), tol_NW=1e-12, tol_CG=1e-13, max_NW=40, tol_macro=1e2, max_iter_macro=40,
+        enable_console=False, model_type=model, solver="newton_cg", lam=lam, mu=mu)
+    assert rel(F, OF.extract_plane_2d(Fo)) < 1e-9
+    assert rel(P, OF.extract_plane_2d(Po)) < 1e-9
+    assert rel(Sig, OF.extract_plane_2d(So)) < 1e-9
+    assert abs(Fb[1, 1] - Fbo[2, 2]) < 1e-9
+    assert abs(Sig[1, 1].mean()) < 1e2

@@ -3,6 +3,7 @@ reference: constitutive P, the matrix-free tangent operator, the projection,
 one mixed-BC Newton-Krylov load step (golden fixture), and the 2D
 plane-strain Neo-Hookean law the 3D Neo-Hookean is restated from."""
 import numpy as np
+import pytest
 
 from oracle import fs as OF
 
@@ -69,3 +70,36 @@ def test_neo_hookean_close_to_svk_at_small_strain():
                                          max_NW=30, tol_macro=1.0, max_iter_macro=30, model=model, krylov="cg")
         out[model] = Sig.mean(axis=(0, 1, 2))
     assert abs(out["svk"][0, 0] - out["neo_hookean"][0, 0]) < 1e-3 * abs(out["svk"][0, 0])
+
+
+@pytest.mark.parametrize("model", ["svk", "neo_hookean"])
+def test_plane_strain_law_embedded_in_3d(golden, model):
+    # the reference's 2D plane-strain law (constitutive_hyperelastic_2d,
+    # :591-1087) with F_p equals the 3D law on the embedded problem (out-of-
+    # plane axis y, F_yy = 1): P and the Cauchy stress
+    g = golden("fs2d_step_12x8")
+    nx, ny = g["E"].shape
+    lam, mu = OF.lame_3d(g["E"][:, None, :], g["nu"][:, None, :])
+    F3 = OF.embed_plane_2d(g["F_law"])
+    Fpi = np.linalg.inv(OF.embed_plane_2d(g["Fp"]))
+    P3, _ = OF.constitutive(F3, lam, mu, Fpi, model, has_fp=True)
+    P2 = OF.extract_plane_2d(P3)
+    ref = g[f"{model}_P_law"]
+    assert np.max(np.abs(P2 - ref)) < 1e-12 * np.max(np.abs(ref))
+    S2 = OF.extract_plane_2d(OF.cauchy(P3, F3))
+    assert np.max(np.abs(S2 - g[f"{model}_Sig_law"])) < 1e-12 * np.max(np.abs(ref))
+
+
+def test_plane_strain_newton_step_embedded_in_3d(golden):
+    # the reference's 2D Newton-CG step (SVK, F_bar prescribed) equals the 3D
+    # oracle step on the embedded problem
+    g = golden("fs2d_step_12x8")
+    nx, ny = g["E"].shape
+    E3, nu3 = g["E"][:, None, :], g["nu"][:, None, :]
+    F0 = OF.embed_plane_2d(np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny))))
+    Fb = np.eye(3)
+    Fb[0, 0], Fb[2, 2] = g["F_bar"][0, 0], g["F_bar"][1, 1]
+    F, P, Sig, _ = OF.solver_step_3d(F0, Fb, E3, nu3, None, (0, 0), None, None, tol_NW=1e-12, tol_CG=1e-13,
+                                     max_NW=30, model="svk", krylov="cg")
+    assert np.max(np.abs(OF.extract_plane_2d(F) - g["svk_F"])) < 1e-9
+    assert np.max(np.abs(OF.extract_plane_2d(P) - g["svk_P"])) < 1e-9 * np.max(np.abs(g["svk_P"]))

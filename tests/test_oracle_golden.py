@@ -242,3 +242,49 @@ def test_kmc3d(golden):
     np.testing.assert_array_equal(ep, g["flip_out_eps_p"])
     np.testing.assert_array_equal(sp, g["flip_out_soft"])
     np.testing.assert_array_equal(tl, g["flip_out_tlast"])
+
+
+def _reference_draws(g, mod):
+    rs = np.random.RandomState()
+    rs.set_state(("MT19937", g["rs_keys"], int(g["rs_pos"]), int(g["rs_has_gauss"]), float(g["rs_gauss"])))
+    return mod.ReferenceDraws(rs, 0.1, 0.6, 0.15, 0.3)
+
+
+def test_kmc_driver_matches_reference_trajectory(golden):
+    # the reference's own KmcSimulation2D.run_simulation trajectory (174 events
+    # over 60 AQS steps), reproduced from the same initial catalog, barriers
+    # and RandomState draws
+    from oracle import kmc_driver as OD
+    g = golden("kmc2d_traj_12x8")
+    o = OD.run_kmc2d(g["E"], g["nu"], g["catalog0"], g["Q00"], _reference_draws(g, OD), n_steps=int(g["n_steps"]),
+                     step_size=float(g["step_size"]), strain_rate=1e7, T=300.0, jp=0.0, jt=0.0, cap=2.0,
+                     mixed_tol=1e4, mixed_max_iter=50, ls_tol=1e-6, ls_max_iter=200)
+    assert len(o["events"]) == len(g["events"])
+    np.testing.assert_array_equal(np.array([e[:3] for e in o["events"]]), g["events"])
+    t = np.array([e[3] for e in o["events"]])
+    assert np.max(np.abs(t - g["times"]) / np.abs(g["times"])) < 1e-12
+    assert np.max(np.abs(o["eps_macro"] - g["eps_macro"])) < 1e-15
+    assert rel(o["sig"], g["sig"]) < 1e-12
+    np.testing.assert_array_equal(o["eps_p"], g["eps_plastic"])
+    np.testing.assert_array_equal(o["catalog"], g["catalog"])
+    np.testing.assert_array_equal(o["Q0"], g["Q0"])
+
+
+def test_kmc3d_driver_matches_reference_trajectory(golden):
+    # the reference's own ThermalSimulation.run_simulation trajectory (small
+    # strain, 1348 events over 60 AQS steps on 6x6x4 x 4 modes)
+    from oracle import kmc_driver as OD
+    g = golden("kmc3d_traj_6x6x4")
+    rs = np.random.RandomState()
+    rs.set_state(("MT19937", g["rs_keys"], int(g["rs_pos"]), int(g["rs_has_gauss"]), float(g["rs_gauss"])))
+    o = OD.run_kmc3d(g["E"], g["nu"], g["catalog0"], g["Q00"], OD.ReferenceDraws3D(rs, 0.1, 0.4, 0.15, 0.2),
+                     n_steps=int(g["n_steps"]), step_size=float(g["step_size"]), T=300.0, jp=0.0, jt=0.0, cap=2.0,
+                     mixed_tol=1e4, mixed_max_iter=50)
+    np.testing.assert_array_equal(np.array([e[:4] for e in o["events"]]), g["events"])
+    t = np.array([e[4] for e in o["events"]])
+    assert np.max(np.abs(t - g["times"]) / np.abs(g["times"])) < 1e-12
+    assert np.max(np.abs(o["eps_macro"] - g["eps_macro"])) < 1e-15
+    assert rel(o["sig"], g["sig"]) < 1e-12
+    np.testing.assert_array_equal(o["eps_p"], g["eps_plastic"])
+    np.testing.assert_array_equal(o["catalog"], g["catalog"])
+    np.testing.assert_array_equal(o["Q0"], g["Q0"])
