@@ -66,12 +66,14 @@ def parse():
                     help="replicas of the batched KMC ensemble block (96 = the ensemble workload, ~1 min); 0 skips it")
     ap.add_argument("--kmc-events", type=int, default=2000,
                     help="events of the 256^2 x 8 KMC/AQS block (2000 = the KMC workload); 0 skips it")
-    ap.add_argument("--serve-window", type=float, default=0.5,
+    ap.add_argument("--serve-window", type=float, default=0.25,
                     help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
                          "0 skips it")
-    ap.add_argument("--serve-plain", type=int, default=12,
-                    help="requests of the serving window (seeded random subsample) that the plain FP64 form serves "
-                         "one at a time for the comparison on identical requests")
+    ap.add_argument("--serve-plain", type=int, default=0,
+                    help="0: the plain FP64 form's service time is measured for every request of the window; n > 0: "
+                         "for a seeded subsample of n (the others get a measured time of their class: an estimate)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving block (a long window: --serve-window 10 --serve-plain 150)")
     ap.add_argument("--cpu-kmc-seconds", type=float, default=12.0,
                     help="seconds of the oracle's per-event KMC loop at 256^2 x 8 on one host core; 0 skips it")
     ap.add_argument("--cpu-fs-grid", type=int, default=32,
@@ -343,55 +345,88 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- serving -----
-def run_serving(window, n_plain=12):
-    """The serving stream's first `window` seconds of arrivals, served by the
+def _fifo(arrivals, services):
+    """Latencies of a single sequential server taking requests in arrival
+    order: start = max(arrival, previous finish), finish = start + service."""
+    lat, finish = [], 0.0
+    for a, s in zip(arrivals, services):
+        finish = max(a, finish) + s
+        lat.append(finish - a)
+    return np.array(lat)
+
+
+def run_serving(window, n_plain=0):
+    """The serving stream's first `window` seconds of arrivals served by the
     continuous-batching server (mixed precision, arrivals replayed in real
-    time), and a seeded random subsample of `n_plain` of those requests served
-    by the plain FP64 form one request at a time (their own arrival times
-    replayed).  Latency ratios compare identical requests: each subsampled
-    request's latency inside the full served mix against its latency in the
-    plain form.  Solves/s: served = solves over the window's makespan; plain =
-    solves over its busy time (sum of service times), so its idle gaps between
-    sparse arrivals do not count against it."""
+    time, latency = completion - arrival on the host clock), against the plain
+    FP64 form served sequentially.  The sequential form runs one request at a
+    time, so a request's service time does not depend on the others: each is
+    measured running alone (back to back), and the sequential latencies of
+    the same arrivals follow exactly from the FIFO recursion.  n_plain = 0
+    measures every request's service time; n_plain > 0 measures a seeded
+    subsample and gives each other request the measured service time of a
+    subsampled request of its class (kind, dimension, side) -- an estimate,
+    labelled as such.  Solves/s: served = solves over the makespan; plain =
+    solves over the measured busy time."""
     from mgkmc_b200.serving import Server, request_stream, summarize
     reqs = [r for r in request_stream(rate=200.0, duration=60.0, seed=3) if r.t_arrival <= window]
-    rng = np.random.default_rng(4)
-    sub_ids = sorted(int(i) for i in rng.choice(len(reqs), size=min(n_plain, len(reqs)), replace=False))
-    sub = [reqs[i] for i in sub_ids]
     out = {"workload": (f"serving stream (Poisson 200 req/s, seed 3; 60 % equilibrium solves, 40 % 100-event KMC "
-                        f"trajectories; 70 % 2D sides 64..1024, 30 % 3D finite-strain 64..128): the "
-                        f"{len(reqs)} arrivals of its first {window:g} s, replayed in real time; plain FP64 on a "
-                        f"seeded subsample of {len(sub)}"),
-           "requests": [[r.kind, r.dim, r.n] for r in reqs], "plain_subsample": [r.rid for r in sub]}
+                        f"trajectories; 70 % 2D sides 64..1024, 30 % 3D sides 64..128): the {len(reqs)} arrivals of "
+                        f"its first {window:g} s"),
+           "classes": {}}
+    for r in reqs:
+        k = f"{r.dim}d_{r.kind}_{r.n}"
+        out["classes"][k] = out["classes"].get(k, 0) + 1
     srv = Server(mode="served")
     srv.prepare(reqs)
     res = srv.run(reqs, realtime=True)
     out["served_mixed"] = summarize(res)
-    by_id = {r.rid: r for r in res}
-    lat_sub = np.array([by_id[r.rid].latency for r in sub if not by_id[r.rid].error])
+    del srv
+    if n_plain and n_plain < len(reqs):
+        rng = np.random.default_rng(4)
+        sub = [reqs[i] for i in sorted(rng.choice(len(reqs), size=n_plain, replace=False))]
+    else:
+        sub = reqs
     srv = Server(mode="sequential")
     srv.prepare(sub)
-    res_p = srv.run(sub, realtime=True)
-    plain = summarize(res_p)
+    res_p = srv.run(sub, realtime=False)
     ok = [r for r in res_p if not r.error]
-    busy = sum(r.t_done - r.t_admit for r in ok)
-    plain["busy_s"] = busy
-    plain["solves_per_busy_s"] = sum(r.solves for r in ok) / max(busy, 1e-9)
+    svc = {r.rid: r.t_done - r.t_admit for r in ok}
+    solves = sum(r.solves for r in ok)
+    busy = sum(svc.values())
+    plain = {"measured_requests": len(ok), "errors": len(res_p) - len(ok), "solves": solves, "busy_s": busy,
+             "solves_per_busy_s": solves / max(busy, 1e-9),
+             "service_p50_s": float(np.percentile(list(svc.values()), 50)),
+             "service_p99_s": float(np.percentile(list(svc.values()), 99))}
+    cls = {}
+    for r in sub:
+        if r.rid in svc:
+            cls.setdefault((r.kind, r.dim, r.n), []).append(svc[r.rid])
+    services, estimated = [], 0
+    rng = np.random.default_rng(5)
+    for r in reqs:
+        if r.rid in svc:
+            services.append(svc[r.rid])
+        else:
+            pool = cls.get((r.kind, r.dim, r.n)) or [v for (k, d, _), vs in cls.items() if (k, d) == (r.kind, r.dim)
+                                                      for v in vs]
+            services.append(float(rng.choice(pool)))
+            estimated += 1
+    lat = _fifo([r.t_arrival for r in reqs], services)
+    plain.update(latency_p50_s=float(np.percentile(lat, 50)), latency_p99_s=float(np.percentile(lat, 99)),
+                 makespan_s=float(reqs[-1].t_arrival + lat[-1] - reqs[0].t_arrival) if len(lat) else 0.0,
+                 service_times="measured for every request" if estimated == 0 else
+                 f"measured for {len(reqs) - estimated}, drawn from the measured times of the same class for "
+                 f"{estimated} (estimate)")
     out["plain_fp64_sequential"] = plain
     from mgkmc_b200 import serving as SV
     out["autotuned_ls_families"] = {f"{k[0]}^2 x{k[1]} {k[2]}": {"family": v[0], "ms_per_iteration": v[1]}
                                     for k, v in SV._TUNED.items()}
     a = out["served_mixed"]
-    if a.get("completed") and plain.get("completed") and lat_sub.size:
-        lat_p = np.array([r.latency for r in ok])
-        out["identical_requests"] = {"n": int(lat_sub.size),
-                                     "served_p50_s": float(np.percentile(lat_sub, 50)),
-                                     "served_p99_s": float(np.percentile(lat_sub, 99)),
-                                     "plain_p50_s": float(np.percentile(lat_p, 50)),
-                                     "plain_p99_s": float(np.percentile(lat_p, 99))}
+    if a.get("completed"):
         out["solves_per_s_ratio"] = a["solves_per_s"] / plain["solves_per_busy_s"]
-        out["p50_ratio"] = out["identical_requests"]["plain_p50_s"] / out["identical_requests"]["served_p50_s"]
-        out["p99_ratio"] = out["identical_requests"]["plain_p99_s"] / out["identical_requests"]["served_p99_s"]
+        out["p50_ratio"] = plain["latency_p50_s"] / a["p50_s"]
+        out["p99_ratio"] = plain["latency_p99_s"] / a["p99_s"]
     return out
 
 
@@ -777,6 +812,16 @@ def main():
     a = parse()
     if a.profile_case:
         run_profile_case(a)
+        return
+    if a.serve_only:
+        # one serving-block line (no headline): for long windows of the stream
+        import torch
+        torch.cuda.set_device(0)
+        clk = ClockSampler(0)
+        clk.start()
+        out = run_serving(a.serve_window, a.serve_plain)
+        out["clocks"] = clk.stop()
+        print(json.dumps({"serving": out}), flush=True)
         return
     if a.impl == "reference":
         run_reference(a)
