@@ -200,7 +200,10 @@ MGK_API int mgk_ls2d_profile_batch(mgk_ls2d_t plan, int nsel, const int* sel, co
  *     call before any stream capture.
  *   - All calls on a device share the one array and each call resets what
  *     must start at zero; calls that overlap on the GPU (other streams, other
- *     host threads) race on it and must be serialised by the caller. */
+ *     host threads) race on it and must be serialised by the caller.
+ *   - The resolved address belongs to the device's primary context: after a
+ *     cudaDeviceReset (or any destruction of that context) the entry point
+ *     must not be called again in the same process. */
 #define MGK_NOALLOC_MAX_SIDE 256
 MGK_API int mgk_ls2d_solve_noalloc(int nx, int ny, int plane_mode, const double* E, const double* nu,
                                    const double* eps_plastic, const double* eps_bar, const double* eps_init,
@@ -246,6 +249,15 @@ MGK_API int mgk_ls3d_set_lame_rep(mgk_ls3d_t plan, int rep, const double* lam, c
  * eq the von Mises equivalent strain.  0 <= d <= 1, k >= 0; FP64 plans
  * only.  Takes effect at the next solve. */
 MGK_API int mgk_ls3d_set_secant(mgk_ls3d_t plan, double d, double k);
+/* The Landau small-strain law of spectral_solver_landau_3d
+ * (linear_elastic_simulator.py:1231-1350; elasticity.py:811-857 with the
+ * capping of :297-334) for every replica: v = (v1, v2, v3, g1, g2, g3, g4);
+ * capping 0 none, 1 piecewise, 2 smooth (tanh of power smooth_power) at the
+ * equivalent strain e_cap with tangent 2 tangent_ratio mu.  Medium (mean lam,
+ * mean mu): give the material with mgk_ls3d_set_lame_rep.  The basic scheme
+ * (no mixing, as the reference's 3D solver); symmetric strains; FP64 plans. */
+MGK_API int mgk_ls3d_set_landau(mgk_ls3d_t plan, const double* v, int capping, double e_cap, double tangent_ratio,
+                                double smooth_power);
 MGK_API int mgk_ls3d_solve_batch(mgk_ls3d_t plan, int nsel, const int* sel, const double* eps_bar,
                                  const double* const* eps_init, double* const* eps_out,
                                  double* const* sig_out, int max_iter, double tol, mgk_ls_info3* infos,

@@ -82,6 +82,7 @@ _SIGS = {
     "mgk_ls3d_set_material_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
     "mgk_ls3d_set_eigenstrain_rep": (c_int, [_P, c_int, _P, _P]),
     "mgk_ls3d_set_lame_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
+    "mgk_ls3d_set_landau": (c_int, [_P, _P, c_int, c_double, c_double, c_double]),
     "mgk_ls3d_set_secant": (c_int, [_P, c_double, c_double]),
     "mgk_ls3d_solve_batch": (c_int, [_P, c_int, POINTER(c_int), POINTER(c_double), POINTER(c_void_p),
                                      POINTER(c_void_p), POINTER(c_void_p), c_int, c_double, POINTER(LsInfo3), _P]),

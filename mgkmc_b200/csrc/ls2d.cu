@@ -1431,6 +1431,9 @@ struct mgk_ls2d_plan {
   size_t part_doubles = 0;
   int total_row_items = 0, total_col_items = 0;
   std::vector<void*> allocations;
+  // spectra of all replicas, one slab
+  void* spec_slab = nullptr;
+  size_t spec_bytes = 0;
   // loop graph for the current selection
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1572,6 +1575,7 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     p->fast = (env && env[0] == '0') ? 0 : p->fast_nat;
   }
   p->tc_gen.resize(nrep);
+  std::vector<size_t> spec_off(nrep, 0);
   int total_col_max = 0;
   size_t row_smem = 0, col_smem = 0, row_smem32 = 0, col_smem32 = 0;
   for (int r = 0; r < nrep; ++r) {
@@ -1621,8 +1625,9 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
     if (st) return fail(st);
     double* d = reinterpret_cast<double*>(f);
     R.mu = d; R.lam = d + R.N; R.eps = d + 2 * R.N; R.ep = d + 5 * R.N; R.epa = nullptr;
-    st = plan_alloc(p, &R.spec, 3 * (size_t)nx * R.ld * c64);
-    if (st) return fail(st);
+    // spectra of all replicas sit in one slab (assigned after the loop)
+    spec_off[r] = p->spec_bytes;
+    p->spec_bytes += (3 * (size_t)nx * R.ld * c64 + 255) / 256 * 256;
     if (mixed) {
       void* g = nullptr;
       st = plan_alloc(p, &g, sizeof(float) * R.N * 8);
@@ -1630,6 +1635,13 @@ extern "C" int mgk_ls2d_create_batch(int nrep, const int* nxs, const int* nys, i
       float* fl = reinterpret_cast<float*>(g);
       R.mu32 = fl; R.lam32 = fl + R.N; R.eps32 = fl + 2 * R.N; R.ep32 = fl + 5 * R.N;
     }
+  }
+  {
+    void* slab = nullptr;
+    int st = plan_alloc(p, &slab, p->spec_bytes);
+    if (st) return fail(st);
+    p->spec_slab = slab;
+    for (int r = 0; r < nrep; ++r) p->reps[r].spec = reinterpret_cast<char*>(slab) + spec_off[r];
   }
   p->row_smem = row_smem;
   p->col_smem = col_smem;

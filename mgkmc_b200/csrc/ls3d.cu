@@ -71,6 +71,9 @@ struct Ls3dRep {
   // degradation law with magnitude law_a and rate law_b (FP64 plans)
   int law;
   double law_a, law_b;
+  // law 3, Landau: v1, v2, v3, g1, g2, g3, g4, capping (0 none, 1 piecewise,
+  // 2 smooth), E_cap, tangent ratio, smooth power
+  double lp[11];
 };
 
 struct Ls3dState {
@@ -140,6 +143,67 @@ __device__ __forceinline__ void gamma3d_apply(const double2* t, double n0, doubl
 // the von Mises equivalent strain sqrt(2/3 e':e') of the elastic strain
 // (elasticity.py:665-700) given by its symmetric components; each pair of
 // shear entries sums to twice the symmetric one.
+// 3D Landau small-strain stress (elasticity.py:811-857) of the symmetric
+// elastic strain a = (xx, yy, zz, yz, xz, xy), with the strain capping of
+// elasticity.py:297-334: deviator scaled by f above the cap E_cap (piecewise)
+// or by the tanh profile (smooth), plus 2 (ratio mu) (a - capped) w.
+// sigma = (lam I1 + v1/2 I1^2 + v2 I2 + g1/6 I1^3 + g2 I1 I2 + 4/3 g3 I3) I
+//       + 2 (mu + v2 I1 + g2/2 I1^2 + g4 I2) e + 4 (v3 + g3 I1) e^2.
+__device__ __forceinline__ void landau_sigma3(double mu, double lam, const double* a, const double* __restrict__ lp,
+                                              double* sg) {
+  const double v1 = lp[0], v2 = lp[1], v3 = lp[2], g1 = lp[3], g2 = lp[4], g3 = lp[5], g4 = lp[6];
+  const int cap = (int)lp[7];
+  double c[6];
+  for (int q = 0; q < 6; ++q) c[q] = a[q];
+  double w = 0.0;
+  if (cap) {
+    const double I1a = a[0] + a[1] + a[2];
+    const double m3 = (1.0 / 3.0) * I1a;
+    const double d0 = a[0] - m3, d1 = a[1] - m3, d2 = a[2] - m3;
+    const double dd = d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * (a[3] * a[3] + a[4] * a[4] + a[5] * a[5]);
+    const double Eeq = sqrt(fmax(0.0, (2.0 / 3.0) * dd));
+    const double Ecap = lp[8];
+    double f = 1.0;
+    if (cap == 2) {
+      const double pw = lp[10];
+      if (Eeq > 1e-12) f = (Ecap / Eeq) * pow(tanh(fmin(100.0, pow(Eeq / Ecap, pw))), 1.0 / pw);
+      const double t = tanh(fmin(100.0, pow(Eeq / Ecap, pw)));
+      w = t * t;
+    } else if (Eeq > Ecap) {
+      f = Ecap / Eeq;
+      w = 1.0;
+    }
+    c[0] = d0 * f + m3;
+    c[1] = d1 * f + m3;
+    c[2] = d2 * f + m3;
+    c[3] = a[3] * f;
+    c[4] = a[4] * f;
+    c[5] = a[5] * f;
+  }
+  // e^2 of the symmetric tensor [[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]]
+  const double xx = c[0], yy = c[1], zz = c[2], yz = c[3], xz = c[4], xy = c[5];
+  double e2[6];
+  e2[0] = xx * xx + xy * xy + xz * xz;
+  e2[1] = xy * xy + yy * yy + yz * yz;
+  e2[2] = xz * xz + yz * yz + zz * zz;
+  e2[3] = xy * xz + yy * yz + yz * zz;
+  e2[4] = xx * xz + xy * yz + xz * zz;
+  e2[5] = xx * xy + xy * yy + xz * yz;
+  const double I1 = xx + yy + zz;
+  const double I2 = e2[0] + e2[1] + e2[2];
+  const double I3 = (e2[0] * xx + e2[5] * xy + e2[4] * xz) + (e2[5] * xy + e2[1] * yy + e2[3] * yz) +
+                    (e2[4] * xz + e2[3] * yz + e2[2] * zz);
+  const double cI = lam * I1 + 0.5 * v1 * (I1 * I1) + v2 * I2 + (1.0 / 6.0) * g1 * (I1 * I1 * I1) + g2 * I1 * I2 +
+                    (4.0 / 3.0) * g3 * I3;
+  const double ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * (I1 * I1) + g4 * I2);
+  const double ce2 = 4.0 * (v3 + g3 * I1);
+  for (int q = 0; q < 6; ++q) sg[q] = (q < 3 ? cI : 0.0) + ce * c[q] + ce2 * e2[q];
+  if (cap) {
+    const double r = 2.0 * (lp[9] * mu) * w;
+    for (int q = 0; q < 6; ++q) sg[q] += r * (a[q] - c[q]);
+  }
+}
+
 __device__ __forceinline__ double secant_mu3(double m, double xx, double yy, double zz, double yz, double xz,
                                              double xy, double d, double k) {
   const double tr3 = (xx + yy + zz) / 3.0;
@@ -443,10 +507,19 @@ __global__ void __launch_bounds__(256) ls3d_zline_kernel(const Ls3dRep* __restri
       for (int c = 0; c < 6; ++c) d[c] = e[c] - R.ep[c * N + i];
       if (R.law == 1) m = secant_mu3(m, d[0], d[1], d[2], d[3], d[4], d[5], R.law_a, R.law_b);
       const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
+      if (R.law == 3) {
+        double sg[6];
+        landau_sigma3(m, l, d, R.lp, sg);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) tr[h][c] = (2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre);
+        for (int c = 0; c < 3; ++c) tr[h][c] = sg[c] - (2 * mu0 * e[c] + lam0 * tre);
 #pragma unroll
-      for (int c = 3; c < 6; ++c) tr[h][c] = 2 * m * d[c] - 2 * mu0 * e[c];
+        for (int c = 3; c < 6; ++c) tr[h][c] = sg[c] - 2 * mu0 * e[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tr[h][c] = (2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre);
+#pragma unroll
+        for (int c = 3; c < 6; ++c) tr[h][c] = 2 * m * d[c] - 2 * mu0 * e[c];
+      }
     }
 #pragma unroll
     for (int c = 0; c < 6; ++c) out[c * nz + z] = make_double2(tr[0][c], tr[1][c]);
@@ -694,10 +767,19 @@ __device__ __forceinline__ void ls3_zline_body(const Ls3dRep& R, Ls3dState& S, i
       for (int c = 0; c < 6; ++c) d[c] = e[c] - (double)stg[(16 + 2 * c) * NZ + j];
       if constexpr (LAW == 1) m = secant_mu3(m, d[0], d[1], d[2], d[3], d[4], d[5], R.law_a, R.law_b);
       const double trd = d[0] + d[1] + d[2], tre = e[0] + e[1] + e[2];
+      if constexpr (LAW == 3) {
+        double sg[6];
+        landau_sigma3(m, l, d, R.lp, sg);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) tr[h][c] = (T)((2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre));
+        for (int c = 0; c < 3; ++c) tr[h][c] = (T)(sg[c] - (2 * mu0 * e[c] + lam0 * tre));
 #pragma unroll
-      for (int c = 3; c < 6; ++c) tr[h][c] = (T)(2 * m * d[c] - 2 * mu0 * e[c]);
+        for (int c = 3; c < 6; ++c) tr[h][c] = (T)(sg[c] - 2 * mu0 * e[c]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tr[h][c] = (T)((2 * m * d[c] + l * trd) - (2 * mu0 * e[c] + lam0 * tre));
+#pragma unroll
+        for (int c = 3; c < 6; ++c) tr[h][c] = (T)(2 * m * d[c] - 2 * mu0 * e[c]);
+      }
     }
 #pragma unroll
     for (int c = 0; c < 6; ++c) lines[c * PL + pz] = mk<C>(tr[0][c], tr[1][c]);
@@ -765,7 +847,7 @@ __global__ void __launch_bounds__(96, 8) ls3d_zline_fast_kernel(const Ls3dRep* _
                                                             int guard_cap) {
   ls3d_zline_fast_entry<T, IN_SPEC, FINAL>(reps, st, map, loc, partials, rep_counter, ctl, cond, use_cond, guard_cap);
 }
-template <bool IN_SPEC, bool FINAL, int LAW = 0>  // LAW 1: the secant law
+template <bool IN_SPEC, bool FINAL, int LAW = 0>  // LAW 1: the secant law, 3: the Landau law
 __global__ void __launch_bounds__(96, 5) ls3d_zline_fast64_kernel(const Ls3dRep* __restrict__ reps, Ls3dState* st,
                                                                 const int* __restrict__ map, const int* __restrict__ loc,
                                                                 double* partials, unsigned int* rep_counter,
@@ -911,7 +993,7 @@ __global__ void ls3d_phase2_kernel(Ls3dState* st, const int* sel, int nsel, Ls3d
 }
 
 // outputs (nx,ny,nz,3,3) and partial sums for the means; grid (G, nsel)
-template <int LAW = 0>  // 1: the secant law
+template <int LAW = 0>  // 1: the secant law, 3: the Landau law
 __global__ void ls3d_output_kernel(const Ls3dRep* reps, const Ls3dState* st, const int* sel, double* partials) {
   __shared__ double red[32];
   const int r = sel[blockIdx.y];
@@ -949,7 +1031,18 @@ __global__ void ls3d_output_kernel(const Ls3dRep* reps, const Ls3dState* st, con
                       R.law_a, R.law_b);
     const double tr = d[0] + d[4] + d[8];
     double sg[9];
-    for (int q = 0; q < 9; ++q) sg[q] = 2 * mu * d[q] + ((q % 4) == 0 ? lam * tr : 0.0);
+    if constexpr (LAW == 3) {
+      // symmetric strains (the Landau solver takes symmetric tensors)
+      const double a6[6] = {d[0], d[4], d[8], d[5], d[2], d[1]};
+      double s6[6];
+      landau_sigma3(mu, lam, a6, R.lp, s6);
+      sg[0] = s6[0]; sg[4] = s6[1]; sg[8] = s6[2];
+      sg[5] = sg[7] = s6[3];
+      sg[2] = sg[6] = s6[4];
+      sg[1] = sg[3] = s6[5];
+    } else {
+      for (int q = 0; q < 9; ++q) sg[q] = 2 * mu * d[q] + ((q % 4) == 0 ? lam * tr : 0.0);
+    }
     for (int q = 0; q < 9; ++q) {
       if (R.out_eps) R.out_eps[9 * i + q] = e[q];
       if (R.out_sig) R.out_sig[9 * i + q] = sg[q];
@@ -1132,6 +1225,8 @@ extern "C" int mgk_ls3d_create_batch(int nrep, const int* nxs, const int* nys, c
        raise_smem((const void*)ls3d_zline_fast64_kernel<false, true>, (int)p->zl_smem) ||
        raise_smem((const void*)ls3d_zline_fast64_kernel<true, true, 1>, (int)p->zl_smem) ||
        raise_smem((const void*)ls3d_zline_fast64_kernel<false, true, 1>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast64_kernel<true, true, 3>, (int)p->zl_smem) ||
+       raise_smem((const void*)ls3d_zline_fast64_kernel<false, true, 3>, (int)p->zl_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, -1>, (int)p->ax_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 1, 1>, (int)p->ax_smem) ||
        raise_smem((const void*)ls3d_axis_fast_kernel<double, 0, 0>, (int)p->ax_smem) ||
@@ -1248,6 +1343,31 @@ extern "C" int mgk_ls3d_set_secant(mgk_ls3d_t p, double d, double k) {
   return MGK_OK;
 }
 
+// every replica to the Landau law (spectral_solver_landau_3d); cached loop
+// graphs hold the previous law's z-line kernel and are dropped
+extern "C" int mgk_ls3d_set_landau(mgk_ls3d_t p, const double* v, int capping, double e_cap, double tangent_ratio,
+                                   double smooth_power) {
+  MGK_REQUIRE(p && v, "mgk_ls3d_set_landau: null argument");
+  MGK_REQUIRE(p->prec == MGK_FP64, "mgk_ls3d_set_landau: the Landau law runs in FP64 plans only");
+  MGK_REQUIRE(capping >= 0 && capping <= 2, "mgk_ls3d_set_landau: capping must be 0, 1 or 2");
+  MGK_REQUIRE(capping == 0 || (e_cap > 0.0 && (capping != 2 || smooth_power > 0.0)),
+              "mgk_ls3d_set_landau: need e_cap > 0 (and smooth_power > 0 for smooth capping)");
+  for (int q = 0; q < 7; ++q) MGK_REQUIRE(isfinite(v[q]), "mgk_ls3d_set_landau: non-finite coefficient");
+  for (auto& R : p->reps) {
+    R.law = 3;
+    for (int q = 0; q < 7; ++q) R.lp[q] = v[q];
+    R.lp[7] = capping;
+    R.lp[8] = e_cap;
+    R.lp[9] = tangent_ratio;
+    R.lp[10] = smooth_power;
+  }
+  if (p->law != 3) {
+    if (p->graph_mode == 1) p->graph_mode = -1;
+    p->law = 3;
+  }
+  return MGK_OK;
+}
+
 extern "C" int mgk_ls3d_set_eigenstrain_rep(mgk_ls3d_t p, int rep, const double* epsp, mgk_stream_t stream) {
   MGK_REQUIRE(p && rep >= 0 && rep < p->nrep && p->has_material[rep], "mgk_ls3d_set_eigenstrain: no material");
   return set3(p, rep, nullptr, nullptr, epsp, 0, (cudaStream_t)stream);
@@ -1276,6 +1396,8 @@ struct Loop3 {
 static void* zline_fn(int fast, bool in_spec, bool f32 = false, int law = 0) {
   if (fast && !f32 && law == 1)
     return in_spec ? (void*)ls3d_zline_fast64_kernel<true, true, 1> : (void*)ls3d_zline_fast64_kernel<false, true, 1>;
+  if (fast && !f32 && law == 3)
+    return in_spec ? (void*)ls3d_zline_fast64_kernel<true, true, 3> : (void*)ls3d_zline_fast64_kernel<false, true, 3>;
   if (fast && f32)
     return in_spec ? (void*)ls3d_zline_fast_kernel<float, true, false> : (void*)ls3d_zline_fast_kernel<float, false, false>;
   if (fast)
@@ -1510,6 +1632,8 @@ extern "C" int mgk_ls3d_solve_batch(mgk_ls3d_t p, int nsel, const int* sel, cons
   }
   if (p->law == 1)
     ls3d_output_kernel<1><<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
+  else if (p->law == 3)
+    ls3d_output_kernel<3><<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   else
     ls3d_output_kernel<0><<<dim3(G, nsel), kT3, 0, s>>>(p->d_reps, p->d_st, d_sel, p->d_part);
   MGK_CUDA(cudaGetLastError());

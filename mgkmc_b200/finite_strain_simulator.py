@@ -433,3 +433,104 @@ def finite_strain_solver_step_2d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None
         print(f"finite strain 2D step: {info.macro_iterations} macro, {info.newton_iterations} Newton, "
               f"{info.krylov_iterations} CG iterations")
     return Fo, Po, So, None, Fb
+
+
+def build_finite_strain_bc(driving_component, eps_target_step, mixed_targets, plane_mode="plane_strain", ndim=2,
+                           F_bar_initial=None):
+    """2D boundary conditions of a load step (finite_strain_simulator.py:1912-1979):
+    the same rule as build_finite_strain_bc_3d with ndim = 2 (``plane_mode``
+    does not change it)."""
+    return build_finite_strain_bc_3d(driving_component, eps_target_step, mixed_targets, ndim=ndim,
+                                     F_bar_initial=F_bar_initial)
+
+
+def finite_strain_simulation_2d(E, nu, driving_component, eps_target, n_steps, mixed_targets=None,
+                                plane_mode="plane_strain", pixel=1.0, tol_NW=1e-5, tol_CG=1e-6, max_NW=20,
+                                tol_macro=1e6, max_iter_macro=20, store=True, log_path=None, global_log_path=None,
+                                enable_console=True, checkpoint_interval="none", checkpoint_path=None,
+                                vtk_interval="none", vtk_path=None, model_type="svk", A_m=0.0, B_m=0.0, C_m=0.0,
+                                solver="al", Fp=None, precision="fp64", **unused):
+    """Incremental 2D plane-strain finite-strain ramp
+    (finite_strain_simulator.py:2580-2851) on one device-resident embedded
+    plan (``Fs2dSolver``): per load step the boundary conditions of
+    build_finite_strain_bc at eps_target * s / n_steps (seeded with the
+    previous F_bar), one Newton-Krylov load step from the previous field.
+    Returns (F_macro, Sig_macro, P_macro, F list, Sig list) with (2, 2, nx, ny)
+    fields.  ``Fp`` is an optional eigen-deformation field (the reference's
+    driver passes none)."""
+    import time as _time
+    from datetime import datetime as _dt
+    if solver not in ("newton_cg", "newton"):
+        raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
+    if plane_mode != "plane_strain":
+        raise NotImplementedError("plane_mode='plane_stress': only plane strain runs on the GPU")
+    if vtk_interval not in (None, "none"):
+        raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
+    mixed_targets = {} if mixed_targets is None else mixed_targets
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    nu = np.ascontiguousarray(nu, dtype=np.float64)
+    nx, ny = E.shape
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    s_ = Fs2dSolver(nx, ny, model=model_type, precision=precision)
+    s_.set_material(lam, mu, Fp)
+    s_.set_F(np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny))))
+    lbl = _COMP.get(tuple(driving_component), "xx")
+    log_f = open(log_path, "w", buffering=1) if log_path else None
+    if log_f:
+        hdr = (f"{'Timestamp':<20} {'Elapsed(s)':<12} {'Step':<8} {'F_' + lbl:<14} {'Eng_strain_' + lbl:<20} "
+               f"{'Sig_' + lbl + '(GPa)':<18}\n")
+        log_f.write(hdr)
+        log_f.write("-" * len(hdr.rstrip()) + "\n")
+    glog_f = open(global_log_path, "w", buffering=1) if global_log_path else None
+    t0 = _time.time()
+    F_macro, Sig_macro, P_macro, F_list, Sig_list = [], [], [], [], []
+    F_bar_init = None
+    E_avg, nu_avg = float(E.mean()), float(nu.mean())
+    for s, eps_s in enumerate(np.linspace(0.0, eps_target, n_steps + 1)):
+        F_bar, _, P_tgt, P_mask = build_finite_strain_bc(driving_component, eps_s, mixed_targets, plane_mode,
+                                                         F_bar_initial=F_bar_init)
+        F_bar_init, info = s_.step(F_bar, driving_component, P_tgt, P_mask, E_avg, nu_avg, tol_NW, tol_CG, max_NW,
+                                   tol_macro, max_iter_macro)
+        F, P, Sig = s_.get()
+        F_mac, P_mac, S_mac = F.mean(axis=(2, 3)), P.mean(axis=(2, 3)), Sig.mean(axis=(2, 3))
+        F_macro.append(F_mac)
+        P_macro.append(P_mac)
+        Sig_macro.append(S_mac)
+        if store:
+            F_list.append(F)
+            Sig_list.append(Sig)
+        i, j = driving_component
+        F_drv = F_mac[i, j]
+        eng = F_drv - (1.0 if i == j else 0.0)
+        if enable_console:
+            print(f"step {s}/{n_steps}: F_{lbl}={F_drv:.5f}, eng_strain={eng:.5f}, Sig_{lbl}={S_mac[i, j] / 1e9:.4f} GPa")
+        if log_f:
+            log_f.write(f"{_dt.now().strftime('%Y-%m-%d %H:%M:%S'):<20} {_time.time() - t0:<12.3f} {s:<8} "
+                        f"{F_drv:<14.6f} {eng:<20.6f} {S_mac[i, j] / 1e9:<18.6f}\n")
+        if glog_f:
+            glog_f.write(f"{s:<8} {F_mac[0, 0]:<12.6f} {F_mac[1, 1]:<12.6f} {F_mac[0, 1]:<12.6f} "
+                         f"{F_mac[0, 0] - 1:<14.6f} {F_mac[1, 1] - 1:<14.6f} {P_mac[0, 0] / 1e9:<14.6f} "
+                         f"{P_mac[1, 1] / 1e9:<14.6f} {P_mac[0, 1] / 1e9:<14.6f} {S_mac[0, 0] / 1e9:<16.6f} "
+                         f"{S_mac[1, 1] / 1e9:<16.6f} {S_mac[0, 1] / 1e9:<16.6f}\n")
+        if checkpoint_path is not None and (checkpoint_interval == "current" or (
+                isinstance(checkpoint_interval, int) and s % checkpoint_interval == 0)):
+            _checkpoint_2d(checkpoint_path if checkpoint_interval == "current" else f"{checkpoint_path}_{s:06d}", s,
+                           E, nu, F, Sig, F_mac, S_mac, pixel)
+    if checkpoint_path is not None and (checkpoint_interval == "last" or (
+            isinstance(checkpoint_interval, int) and n_steps % checkpoint_interval != 0)):
+        _checkpoint_2d(f"{checkpoint_path}_final", n_steps, E, nu, F, Sig, F_macro[-1], Sig_macro[-1], pixel)
+    if log_f:
+        log_f.close()
+    if glog_f:
+        glog_f.close()
+    return np.array(F_macro), np.array(Sig_macro), np.array(P_macro), F_list, Sig_list
+
+
+def _checkpoint_2d(path, step, E, nu, F, Sig, F_mac, S_mac, pixel):
+    """The reference's checkpoint of a 2D finite-strain step: Green-Lagrange
+    strain and Cauchy stress, spatial-first (nx, ny, 2, 2)."""
+    from . import checkpoint as C
+    E_GL = 0.5 * (np.einsum("kixy,kjxy->ijxy", F, F) - np.eye(2)[:, :, None, None])
+    C.save_checkpoint_2d(path, step, E, nu, np.moveaxis(E_GL, (0, 1), (2, 3)), np.moveaxis(Sig, (0, 1), (2, 3)),
+                         F_mac, S_mac, pixel)

@@ -134,6 +134,7 @@ class Kmc3D:
         self.events = []
         self.n_solves = 0
         self.steps_done = 0
+        self.host_result = True
 
     @property
     def E_avg(self):
@@ -267,7 +268,12 @@ class Kmc3D:
                 send = None
 
     def result(self, steps):
+        """The trajectory's result; with ``host_result`` False the fields stay
+        on the device (the caller reads what it needs)."""
         self.steps_done = steps
-        return dict(events=list(self.events), eps_macro=self.eps_macro.copy(), sig=self.sig.cpu().numpy(),
-                    eps_p=self.eps_p.cpu().numpy(), time=self.time, steps=steps, solves=self.n_solves,
-                    catalog=self.catalog.cpu().numpy(), Q0=self.Q0.cpu().numpy())
+        out = dict(events=list(self.events), eps_macro=self.eps_macro.copy(), time=self.time, steps=steps,
+                   solves=self.n_solves)
+        if self.host_result:
+            out.update(sig=self.sig.cpu().numpy(), eps_p=self.eps_p.cpu().numpy(), catalog=self.catalog.cpu().numpy(),
+                       Q0=self.Q0.cpu().numpy())
+        return out

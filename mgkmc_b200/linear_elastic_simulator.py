@@ -453,6 +453,13 @@ class Ls3dBatch:
         """Secant degradation law for every replica (0 < d <= 1; d = 0 linear)."""
         L.check(L.lib().mgk_ls3d_set_secant(self._h, float(d), float(k)), "mgk_ls3d_set_secant")
 
+    def set_landau(self, v, capping=0, e_cap=0.0, tangent_ratio=0.1, smooth_power=1.0):
+        """Landau law for every replica: v = (v1, v2, v3, g1, g2, g3, g4);
+        capping 0 none, 1 piecewise, 2 smooth at e_cap; FP64 plans."""
+        arr = (ctypes.c_double * 7)(*[float(a) for a in v])
+        L.check(L.lib().mgk_ls3d_set_landau(self._h, ctypes.cast(arr, ctypes.c_void_p), int(capping), float(e_cap),
+                                            float(tangent_ratio), float(smooth_power)), "mgk_ls3d_set_landau")
+
     def set_eigenstrain(self, rep, eps_plastic, stream=None):
         self._keep[("e", rep)] = eps_plastic
         L.check(L.lib().mgk_ls3d_set_eigenstrain_rep(self._h, int(rep), L.ptr(eps_plastic), L.stream_ptr(stream)),
@@ -531,6 +538,56 @@ def spectral_solver_secant_3d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
     info = p.solve([0], [eps_bar], [eps], [sig], None if eps_init is None else [t(eps_init)], max_iter, tol)[0]
     if verbose:
         print(f"secant LS 3D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
+    e, s_ = eps.cpu().numpy(), sig.cpu().numpy()
+    return e, s_, e.mean(axis=(0, 1, 2)), s_.mean(axis=(0, 1, 2))
+
+
+_PLANS3_LANDAU = {}
+
+
+def spectral_solver_landau_3d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6,
+                              verbose=False, pixel=1.0, Gamma=None, eps_init=None, strain_capping_enabled=False,
+                              strain_capping_limit=None, strain_capping_tangent_ratio=0.1,
+                              strain_capping_type="piecewise", strain_capping_smooth_power=1.0, solver="dbfft"):
+    """Nonlinear 3D Lippmann-Schwinger solve with the Landau small-strain law
+    (linear_elastic_simulator.py:1231-1350): the basic scheme with the (mean
+    lam, mean mu) medium, the whole loop on the device (the law compiled into
+    the z-line and output kernels).  Returns (eps, sig, eps.mean(axis=(0,1,2)),
+    sig.mean(axis=(0,1,2))); a non-finite update raises FloatingPointError as
+    the reference does.  Symmetric strain tensors only."""
+    if solver == "newton_cg":
+        raise NotImplementedError("Newton-CG solver is not yet implemented for 3D small-strain")
+    torch = _torch()
+    lam = np.array(np.broadcast_to(np.asarray(lam, dtype=np.float64), np.shape(mu) or np.shape(lam)))
+    mu = np.array(np.broadcast_to(np.asarray(mu, dtype=np.float64), lam.shape))
+    eps_bar = np.asarray(eps_bar, dtype=np.float64)
+    for a in (eps_bar, eps_plastic, eps_init):
+        if a is not None and not np.array_equal(np.asarray(a), np.swapaxes(np.asarray(a), -1, -2)):
+            raise NotImplementedError("spectral_solver_landau_3d: asymmetric strain tensors are not supported")
+    cap, e_cap = 0, 0.0
+    if strain_capping_enabled:
+        cap = 2 if strain_capping_type == "smooth" else 1
+        if strain_capping_limit is None or strain_capping_limit <= 0:
+            e_cap = float(np.sqrt(0.2 * mu.mean() / abs(g4))) if g4 < 0 else 999.0
+        else:
+            e_cap = float(strain_capping_limit)
+    shape = lam.shape
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (shape, dev.index)
+    p = _PLANS3_LANDAU.get(key)
+    if p is None:
+        p = _PLANS3_LANDAU[key] = Ls3dBatch([shape])
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
+    p.set_landau((v1, v2, v3, g1, g2, g3, g4), cap, e_cap, strain_capping_tangent_ratio, strain_capping_smooth_power)
+    eps = torch.empty(shape + (3, 3), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    info = p.solve([0], [eps_bar], [eps], [sig], None if eps_init is None else [t(eps_init)], max_iter, tol)[0]
+    if info.status == L.NONFINITE or not np.isfinite(info.final_diff):
+        raise FloatingPointError("spectral_solver_landau_3d: non-finite strain update in LS loop (Landau energy "
+                                 "likely unstable at this strain; consider strain capping or smaller load steps).")
+    if verbose:
+        print(f"landau LS 3D: {info.iterations} iterations, diff = {info.final_diff:.3e}")
     e, s_ = eps.cpu().numpy(), sig.cpu().numpy()
     return e, s_, e.mean(axis=(0, 1, 2)), s_.mean(axis=(0, 1, 2))
 

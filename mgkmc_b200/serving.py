@@ -11,8 +11,14 @@ A request is one of
     model of the 256^2 KMC workload;
   * a 3D finite-strain load step (the Newton-Krylov step of
     mgkmc/finite_strain_simulator.py:2967-3168, Neo-Hookean with eigen-
-    deformations, F_xx = 1 + ``fs_strain`` prescribed, lateral stresses zero).
-    3D requests of the trajectory kind are served as this load step too.
+    deformations, F_xx = 1 + ``fs_strain`` prescribed, lateral stresses zero);
+  * a 3D KMC/AQS trajectory of ``n_events`` events (the small-strain path of
+    ThermalSimulation.run_simulation, mgkmc/aqs.py:682-1201, as run by
+    ``Kmc3D``): the 2D trajectory's medium, catalog and barrier model in 3D.
+    A finite-strain trajectory would need thousands of Newton load steps per
+    request (one per AQS step, aqs.py:1097, plus the sub-stepped flips), so
+    3D trajectories use the small-strain solver, the reference's default
+    strain assumption.
 
 Each request's inputs are generated on the GPU from its seed.
 
@@ -26,8 +32,11 @@ call (one launch per stage, loop on the device) and records an event; a
 size's next round starts as soon as its event completes, independently of the
 other sizes, so the work of different sizes overlaps on the device.  Solves
 use the mixed-precision form and warm starts from the device-resident fields
-(the previous macro iterate, or the trajectory's previous field).  3D steps
-run on a worker thread with their own stream and overlap with the 2D work.
+(the previous macro iterate, or the trajectory's previous field).  3D
+finite-strain steps run on a worker thread with their own stream; 3D
+trajectories on a second worker thread that advances them in rounds over
+per-size batched 3D LS plans (one solve launch per stage for every admitted
+trajectory of a size); both overlap with the 2D work.
 
 Sequential form (``mode="sequential"``): the plain FP64 form of the same
 requests one at a time in arrival order, cold LS starts and the exact
@@ -104,6 +113,8 @@ class Result:
 def footprint_bytes(req, n_modes=8):
     """Device bytes a request holds while admitted (its own tensors; the
     per-size plan slots are allocated once)."""
+    if req.dim == 3 and req.kind == "trajectory":
+        return req.n ** 3 * 8 * (2 + 9 * n_modes + 4 * n_modes + 9 + 4 + 1 + 9 + 27)
     if req.dim == 3:
         return req.n ** 3 * 8 * (83 + 9 + 2 + 27)
     N = req.n * req.n
@@ -137,6 +148,18 @@ class _Bucket:
         self.event = torch.cuda.Event()
 
 
+class _Bucket3:
+    """One 3D grid size of trajectories: a batched 3D LS plan and a stream."""
+
+    def __init__(self, torch, n, slots, precision):
+        from .linear_elastic_simulator import Ls3dBatch
+        self.n = n
+        self.stream = torch.cuda.Stream()
+        self.plan = Ls3dBatch([(n, n, n)] * slots, precision=precision)
+        self.free = list(range(slots))[::-1]
+        self.tasks = []
+
+
 class Server:
     def __init__(self, mode="served", hbm_budget=None, slots=None, ls_tol=1e-8, ls_max_iter=500,
                  macro_tol=1e4, macro_max_iter=20, n_events=100, n_modes=8, q_mean=1.0, kmc_T=300.0,
@@ -160,7 +183,9 @@ class Server:
             hbm_budget = int(0.5 * free)
         self.hbm_budget = hbm_budget
         self.slots = dict(slots) if slots else {64: 32, 128: 32, 256: 32, 512: 16, 768: 8, 1024: 8}
+        self.slots3 = {64: 8, 96: 4, 128: 2}
         self.buckets = {}
+        self.buckets3 = {}
         self.fs_plans = {}
         self.used = 0
         self.lock = threading.Lock()
@@ -248,6 +273,118 @@ class Server:
             else:
                 yield ("sync",)
                 send = None
+
+    # ----------------------------------------------------- 3D trajectories ---
+    def _bucket3(self, n):
+        b = self.buckets3.get(n)
+        if b is None:
+            k = self.slots3.get(n, 1) if self.served else 1
+            b = self.buckets3[n] = _Bucket3(self.torch, n, k, self.precision)
+        return b
+
+    def _traj3_task(self, b, slot, req, res):
+        """A 3D KMC/AQS trajectory of n_events events (generator, as _traj_task)."""
+        from .kmc3d import Kmc3D
+        n, M = req.n, self.n_modes
+        E, nu = W.ls3d_material_dev(n, n, n, req.seed, self.dev)
+        cat, Q0 = W.kmc3d_state_dev(n, n, n, M, req.seed, self.dev, q_mean=self.q_mean)
+        k = Kmc3D(E, nu, cat, Q0, T=self.kmc_T if req.T is None else req.T, q_mean=self.q_mean, ls_tol=self.ls_tol,
+                  ls_max_iter=self.ls_max_iter, selection=self.selection, ls_start=self.ls_start,
+                  precision=self.precision, ls=b.plan, rep=slot, stream=b.stream)
+        k.host_result = False
+        del E, nu, cat, Q0
+        gen = k.trajectory(np.random.default_rng(req.seed), 10 ** 9,
+                           max_events=self.n_events if req.n_events is None else req.n_events)
+        send = None
+        while True:
+            try:
+                need = gen.send(send)
+            except StopIteration as stop:
+                out = stop.value
+                res.solves = k.n_solves
+                return dict(events=out["events"], eps_macro=out["eps_macro"], eps=k.eps, sig=k.sig,
+                            eps_p=k.eps_p, time=out["time"], steps=out["steps"])
+            if need[0] == "solve":
+                _, _, eb, eo, so, init = k.solve_args()
+                info = yield ("solve", eb, eo, so, init)
+                res.ls_iterations += info.iterations
+                send = info
+            else:
+                yield ("sync",)
+                send = None
+
+    def _round3(self, b):
+        """One round of a 3D bucket: resume every trajectory until it needs a
+        device result, then one batched solve of all of them."""
+        torch = self.torch
+        solving, syncing, alive = [], [], []
+        with torch.cuda.stream(b.stream):
+            for t in b.tasks:
+                try:
+                    t.need = t.gen.send(t.send)
+                except StopIteration as stop:
+                    self._finish(t.res, stop.value)
+                    b.free.append(t.slot)
+                    continue
+                except ValueError as e:
+                    self._finish(t.res, error=str(e))
+                    b.free.append(t.slot)
+                    continue
+                alive.append(t)
+                (solving if t.need[0] == "solve" else syncing).append(t)
+        b.tasks = alive
+        if solving:
+            infos = b.plan.solve([t.slot for t in solving], [t.need[1] for t in solving],
+                                 [t.need[2] for t in solving], [t.need[3] for t in solving],
+                                 eps_init=[t.need[4] for t in solving], max_iter=self.ls_max_iter, tol=self.ls_tol,
+                                 sync=True, stream=b.stream)
+            for t, info in zip(solving, infos):
+                t.send = info
+        if syncing:
+            b.stream.synchronize()
+            for t in syncing:
+                t.send = None
+
+    def _traj3_worker(self, q):
+        """Admits 3D trajectories into free slots of their size and advances
+        the admitted ones in rounds until the queue is closed and all are done."""
+        waiting = collections.deque()
+        closed = False
+        while True:
+            try:
+                while True:
+                    r = q.get_nowait()
+                    if r is None:
+                        closed = True
+                    else:
+                        waiting.append(r)
+            except queue.Empty:
+                pass
+            still = collections.deque()
+            for r in waiting:
+                b = self._bucket3(r.n)
+                if b.free:
+                    res = self.results[r.rid]
+                    res.t_admit = self._now()
+                    slot = b.free.pop()
+                    with self.torch.cuda.stream(b.stream):
+                        gen = self._traj3_task(b, slot, r, res)
+                    b.tasks.append(_Task(r, res, gen, slot, 0))
+                else:
+                    still.append(r)
+            waiting = still
+            active = [b for b in self.buckets3.values() if b.tasks]
+            if not active:
+                if closed and not waiting:
+                    return
+                r = q.get()
+                if r is None:
+                    closed = True
+                else:
+                    waiting.append(r)
+                continue
+            for b in active:
+                self._round3(b)
 
     def _admit(self, b, req):
         res = self.results[req.rid]
@@ -373,8 +510,21 @@ class Server:
                 for k in range(1, min(4, len(b.free)) + 1):
                     b.plan.solve(list(range(k)), [eb] * k, [eps] * k, [None] * k, max_iter=self.ls_max_iter,
                                  tol=self.ls_tol, sync=True, stream=b.stream)
-        for n in sorted({r.n for r in requests if r.dim == 3}):
+        for n in sorted({r.n for r in requests if r.dim == 3 and r.kind == "solve"}):
             self._fs_plan(n)
+        for n in sorted({r.n for r in requests if r.dim == 3 and r.kind == "trajectory"}):
+            b = self._bucket3(n)
+            with torch.cuda.stream(b.stream):
+                E, nu = W.ls3d_material_dev(n, n, n, 0, self.dev)
+                eps = torch.empty((n, n, n, 3, 3), dtype=torch.float64, device=self.dev)
+                eb = np.zeros((3, 3))
+                eb[0, 0] = 0.01
+                k = min(2, len(b.free))
+                for r in range(k):
+                    b.plan.set_material(r, E, nu, None, stream=b.stream)
+                for r in range(1, k + 1):
+                    b.plan.solve(list(range(r)), [eb] * r, [eps] * r, [None] * r, max_iter=self.ls_max_iter,
+                                 tol=self.ls_tol, sync=True, stream=b.stream)
         torch.cuda.synchronize()
 
     def run(self, requests, realtime=True, keep_outputs=False):
@@ -396,11 +546,14 @@ class Server:
         torch = self.torch
         pending = collections.deque(order)
         fs_q = queue.Queue()
+        t3_q = queue.Queue()
         fs_stream = torch.cuda.Stream()
         worker = threading.Thread(target=self._fs_worker, args=(fs_q, fs_stream), daemon=True)
+        worker3 = threading.Thread(target=self._traj3_worker, args=(t3_q,), daemon=True)
         n3d = sum(1 for r in order if r.dim == 3)
         self._t0 = time.perf_counter()
         worker.start()
+        worker3.start()
         done3d = lambda: sum(1 for r in self.results.values() if r.dim == 3 and r.t_done > 0)
         try:
             while True:
@@ -410,7 +563,7 @@ class Server:
                     if not realtime:
                         self.results[r.rid].t_arrival = now
                     if r.dim == 3:
-                        fs_q.put(r)
+                        (t3_q if r.kind == "trajectory" else fs_q).put(r)
                     else:
                         self._bucket(r.n).waiting.append(r)
                 progressed = False
@@ -434,7 +587,9 @@ class Server:
                         time.sleep(2e-5)
         finally:
             fs_q.put(None)
+            t3_q.put(None)
             worker.join()
+            worker3.join()
 
     def _run_sequential(self, order, realtime):
         torch = self.torch
@@ -449,12 +604,16 @@ class Server:
                 res.t_arrival = self._now()
             res.t_admit = self._now()
             try:
-                if r.dim == 3:
+                if r.dim == 3 and r.kind == "solve":
                     out = self._fs_run(r, stream)
                     res.solves = 1
                 else:
-                    b = self._bucket(r.n)
-                    gen = (self._solve_task if r.kind == "solve" else self._traj_task)(b, 0, r, res)
+                    b = self._bucket(r.n) if r.dim == 2 else self._bucket3(r.n)
+                    if r.dim == 3:
+                        task = self._traj3_task
+                    else:
+                        task = self._solve_task if r.kind == "solve" else self._traj_task
+                    gen = task(b, 0, r, res)
                     send = None
                     while True:
                         try:

@@ -201,3 +201,33 @@ def fs3d_material_dev(nx, ny, nz, seed, device, mu_mean=MU0, cv=0.1, K=K_BULK, f
     Fp[sel] += fp_amp * S
     Fp = Fp.reshape(nx, ny, nz, 3, 3).permute(3, 4, 0, 1, 2).contiguous()
     return lam.contiguous(), mu2.contiguous(), Fp
+
+
+def ls3d_material_dev(nx, ny, nz, seed, device, mu0=MU0, K=K_BULK, cv=0.1):
+    """3D (E, nu) (nx, ny, nz) on ``device``: the 2D workloads' medium in 3D."""
+    import torch
+    g = _gen(seed, device)
+    f64 = torch.float64
+    mu = mu0 * (1.0 + cv * torch.randn((nx, ny, nz), generator=g, device=device, dtype=f64))
+    mu = mu.clamp(0.7 * mu0, 1.3 * mu0)
+    E = 9.0 * K * mu / (3.0 * K + mu)
+    nu = (3.0 * K - 2.0 * mu) / (2.0 * (3.0 * K + mu))
+    return E.contiguous(), nu.contiguous()
+
+
+def kmc3d_state_dev(nx, ny, nz, M, seed, device, gamma0=0.1, q_mean=1.0, q_std=0.15, q_min=0.3):
+    """In-plane pure-shear STZ catalog (nx, ny, nz, M, 3, 3) and barriers Q0
+    (nx, ny, nz, M) on ``device`` (the 2D catalog's distribution, glass modes
+    of mgkmc/stz/catalog.py:7-29 with fixed amplitude gamma0/2)."""
+    import torch
+    g = _gen(seed + 7919, device)
+    f64 = torch.float64
+    theta = torch.rand((nx, ny, nz, M), generator=g, device=device, dtype=f64) * np.pi
+    c, s = torch.cos(2 * theta), torch.sin(2 * theta)
+    cat = torch.zeros((nx, ny, nz, M, 3, 3), dtype=f64, device=device)
+    cat[..., 0, 0] = 0.5 * gamma0 * c
+    cat[..., 1, 1] = -0.5 * gamma0 * c
+    cat[..., 0, 1] = 0.5 * gamma0 * s
+    cat[..., 1, 0] = 0.5 * gamma0 * s
+    Q0 = (q_mean + q_std * torch.randn((nx, ny, nz, M), generator=g, device=device, dtype=f64)).clamp_min(q_min)
+    return cat, Q0

@@ -347,6 +347,87 @@ def spectral_solver_landau_2d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=40
     return out + (it_done, diff) if return_info else out
 
 
+def landau_stress_3d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1, cap_power=1.0):
+    """Landau small-strain stress in 3D (mgkmc/elasticity.py:811-857) with the
+    strain capping of :297-334: sigma = cI I + ce e + ce2 e^2 from the
+    invariants I1 = tr e, I2 = tr e^2, I3 = tr e^3 of the (capped) strain,
+    cI = lam I1 + v1/2 I1^2 + v2 I2 + g1/6 I1^3 + g2 I1 I2 + 4/3 g3 I3,
+    ce = 2 (mu + v2 I1 + g2/2 I1^2 + g4 I2), ce2 = 4 (v3 + g3 I1); capping as
+    in landau_stress_2d with the 3D deviator."""
+    v1, v2, v3, g1, g2, g3, g4 = v
+    eye = np.eye(3)
+    w = None
+    if cap_type is not None:
+        I1a = np.trace(e, axis1=-2, axis2=-1)
+        dev = e - (1.0 / 3.0) * I1a[..., None, None] * eye
+        E_eq = np.sqrt(np.maximum(0.0, (2.0 / 3.0) * np.einsum("...ij,...ji->...", dev, dev)))
+        mu_mean = np.mean(mu)
+        E_cap = cap_limit if cap_limit is not None and cap_limit > 0 else (
+            np.sqrt(0.2 * mu_mean / abs(g4)) if g4 < 0 else 999.0)
+        f = np.ones_like(E_eq)
+        nz = E_eq > 1e-12
+        if cap_type == "smooth":
+            rp = np.minimum(100.0, (E_eq[nz] / E_cap) ** cap_power)
+            f[nz] = (E_cap / E_eq[nz]) * np.tanh(rp) ** (1.0 / cap_power)
+            w = np.tanh(np.minimum(100.0, (E_eq / E_cap) ** cap_power)) ** 2
+        else:
+            capped = E_eq > E_cap
+            np.divide(E_cap, E_eq, out=f, where=capped)
+            w = capped.astype(float)
+        c = dev * f[..., None, None] + (1.0 / 3.0) * I1a[..., None, None] * eye
+    else:
+        c = e
+    I1 = np.trace(c, axis1=-2, axis2=-1)
+    c2 = np.einsum("...ij,...jk->...ik", c, c)
+    I2 = np.trace(c2, axis1=-2, axis2=-1)
+    I3 = np.trace(np.einsum("...ij,...jk->...ik", c2, c), axis1=-2, axis2=-1)
+    cI = lam * I1 + 0.5 * v1 * I1 ** 2 + v2 * I2 + (1.0 / 6.0) * g1 * I1 ** 3 + g2 * I1 * I2 + (4.0 / 3.0) * g3 * I3
+    ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * I1 ** 2 + g4 * I2)
+    ce2 = 4.0 * (v3 + g3 * I1)
+    sig = cI[..., None, None] * eye + ce[..., None, None] * c + ce2[..., None, None] * c2
+    if cap_type is not None:
+        sig += 2.0 * (cap_ratio * np.asarray(mu))[..., None, None] * (e - c) * w[..., None, None]
+    return sig
+
+
+def spectral_solver_landau_3d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
+                              eps_init=None, cap_type=None, cap_limit=None, cap_ratio=0.1, cap_power=1.0,
+                              return_info=False):
+    """3D Landau small-strain LS fixed point (mgkmc/linear_elastic_simulator.py:
+    1231-1350): medium (mean lam, mean mu); eps <- eps_bar + zero-mean
+    Gamma0 * (sigma_L(eps - eps_p) - C0:eps); stop when the relative update
+    is below tol (the basic scheme, no mixing)."""
+    lam0, mu0 = float(np.mean(lam)), float(np.mean(mu))
+    shape = np.shape(lam)
+    axes = (0, 1, 2)
+    G = green_operator(wave_vectors(shape, pixel), lam0, mu0)
+    if eps_init is not None:
+        eps = eps_init.copy()
+        eps += eps_bar - eps_init.mean(axis=axes)
+    else:
+        eps = np.broadcast_to(eps_bar, shape + (3, 3)).copy()
+    ep = eps_plastic
+    law = lambda x: landau_stress_3d(x - ep if ep is not None else x, lam, mu, v, cap_type, cap_limit, cap_ratio,
+                                     cap_power)
+    it_done, diff = 0, np.inf
+    for it in range(max_iter):
+        tau = law(eps) - hooke(eps, lam0, mu0, 3)
+        tau_hat = np.fft.fftn(tau, axes=axes, norm="ortho")
+        et = np.fft.ifftn(-np.einsum("xyzkhij,xyzij->xyzkh", G, tau_hat), axes=axes, norm="ortho").real
+        et -= et.mean(axis=axes)
+        eps_new = eps_bar + et
+        diff = np.linalg.norm(eps_new - eps) / (np.linalg.norm(eps) + 1e-20)
+        eps = eps_new
+        it_done = it + 1
+        if not np.isfinite(diff):
+            raise FloatingPointError("spectral_solver_landau_3d: non-finite strain update in LS loop")
+        if diff < tol:
+            break
+    sig_out = law(eps)
+    out = (eps, sig_out, eps.mean(axis=axes), sig_out.mean(axis=axes))
+    return out + (it_done, diff) if return_info else out
+
+
 def rose_stress_2d(e, lam, mu, eta, floor_f=0.1, plane_mode="plane_strain"):
     """Rose secant-modulus stress (mgkmc/elasticity.py:868-944): G = max(mu
     exp(-eta eq), floor mu), K = lam + 2 mu / 3 kept; plane stress: eps_zz by

@@ -512,10 +512,64 @@ def fs2d_step_fixtures():
     save("fs2d_step_12x8", **out)
 
 
+def fs2d_sim_fixtures():
+    """The reference's 2D finite-strain load ramp (finite_strain_simulation_2d,
+    :2580-2851), SVK, Newton-CG, F_xx driven to 1.01 in 2 steps with F_yy held
+    at 1 (no stress-controlled component: see fs2d_step_fixtures).  Newton
+    tolerance 1e-7: each load step converges in three Newton iterations, the
+    last step of size ~3e-10; a fourth iteration, which a tighter tolerance
+    asks for, meets the stalled BiCGSTAB solve and its line search fails."""
+    rng = np.random.default_rng(72)
+    E, nu = W.ls2d_material(12, 8, rng)
+    Fm, Sm, Pm, F_l, S_l = FS.finite_strain_simulation_2d(
+        E, nu, (0, 0), 0.01, 2, mixed_targets={}, tol_NW=1e-7, tol_CG=1e-8, max_NW=30, enable_console=False,
+        model_type="svk", solver="newton_cg")
+    save("fs2d_sim_12x8", E=E, nu=nu, F_macro=Fm, Sig_macro=Sm, P_macro=Pm, F_last=F_l[-1], Sig_last=S_l[-1])
+
+
+def ls3d_landau_fixtures():
+    """The reference's 3D Landau law (stress_from_strain_landau_3d) without
+    capping, with piecewise and with smooth capping, and its LS solver
+    (spectral_solver_landau_3d, the basic scheme) on a heterogeneous medium
+    with eigenstrains, with and without capping, and at fixed iteration
+    counts."""
+    from mgkmc import elasticity as ELA
+    rng = np.random.default_rng(74)
+    shape = (12, 8, 6)
+    E, nu = W.ls3d_material(*shape, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    v1, v2, v3, g1, g2, g3, g4 = LANDAU_V
+    kw = dict(v1=v1, v2=v2, v3=v3, g1=g1, g2=g2, g3=g3, g4=g4)
+    e = rng.normal(0, 0.02, shape + (3, 3))
+    e = 0.5 * (e + np.swapaxes(e, -1, -2))
+    out = dict(lam=lam, mu=mu, v=np.array(LANDAU_V), strain=e)
+    out["sig_plain"] = ELA.stress_from_strain_landau_3d(e, lam, mu, **kw)
+    out["sig_piecewise"] = ELA.stress_from_strain_landau_3d(e, lam, mu, **kw, strain_capping_enabled=True,
+                                                            strain_capping_limit=0.015)
+    out["sig_smooth"] = ELA.stress_from_strain_landau_3d(e, lam, mu, **kw, strain_capping_enabled=True,
+                                                         strain_capping_limit=0.015, strain_capping_type="smooth",
+                                                         strain_capping_smooth_power=2.0)
+    ep = W.pure_shear_eigenstrain_3d(*shape, rng, frac=0.1)
+    eb = np.array([[0.008, 0.002, 0.0], [0.002, -0.003, 0.001], [0.0, 0.001, -0.002]])
+    out.update(eps_plastic=ep, eps_bar=eb)
+    for k in (1, 3):
+        eps, sig, _, _ = LES.spectral_solver_landau_3d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, max_iter=k, tol=0.0)
+        out.update({f"eps_it{k}": eps, f"sig_it{k}": sig})
+    eps, sig, _, _ = LES.spectral_solver_landau_3d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, max_iter=400, tol=1e-12)
+    out.update(eps_conv=eps, sig_conv=sig)
+    eps, sig, _, _ = LES.spectral_solver_landau_3d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, max_iter=400, tol=1e-12,
+                                                   strain_capping_enabled=True, strain_capping_limit=0.01,
+                                                   strain_capping_type="smooth", strain_capping_smooth_power=2.0)
+    out.update(eps_cap=eps, sig_cap=sig)
+    save("ls3d_landau_12x8x6", **out)
+
+
 ALL = ("ls2d_fixtures", "ls3d_fixtures", "kmc2d_fixtures", "kmc3d_fixtures", "fs3d_fixtures", "ls2d_secant_fixtures",
        "ls2d_rose_fixtures", "kmc2d_cascade_fixtures", "kmc2d_patch_fixtures", "ls3d_secant_fixtures",
        "ls2d_landau_fixtures", "kmc2d_trajectory_fixtures", "driver_fixtures",
-       "kmc3d_trajectory_fixtures", "fs2d_step_fixtures")
+       "kmc3d_trajectory_fixtures", "fs2d_step_fixtures",
+       "fs2d_sim_fixtures", "ls3d_landau_fixtures")
 
 
 if __name__ == "__main__":

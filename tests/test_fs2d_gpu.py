@@ -72,3 +72,16 @@ def test_mixed_bc_step_with_fp_matches_oracle(model, shape):
     assert rel(Sig, OF.extract_plane_2d(So)) < 1e-9
     assert abs(Fb[1, 1] - Fbo[2, 2]) < 1e-9
     assert abs(Sig[1, 1].mean()) < 1e2
+
+
+def test_simulation_2d_matches_reference(golden):
+    from mgkmc_b200.finite_strain_simulator import finite_strain_simulation_2d
+    g = golden("fs2d_sim_12x8")
+    Fm, Sm, Pm, F_l, S_l = finite_strain_simulation_2d(
+        g["E"], g["nu"], (0, 0), 0.01, 2, mixed_targets={}, tol_NW=1e-12, tol_CG=1e-13, max_NW=30,
+        enable_console=False, model_type="svk", solver="newton_cg")
+    assert np.max(np.abs(Fm - g["F_macro"])) < 1e-9
+    assert np.max(np.abs(Pm - g["P_macro"])) < 1e-9 * np.max(np.abs(g["P_macro"]))
+    assert np.max(np.abs(Sm - g["Sig_macro"])) < 1e-9 * np.max(np.abs(g["Sig_macro"]))
+    assert rel(F_l[-1], g["F_last"]) < 1e-9
+    assert rel(S_l[-1], g["Sig_last"]) < 1e-9

@@ -288,3 +288,23 @@ def test_kmc3d_driver_matches_reference_trajectory(golden):
     np.testing.assert_array_equal(o["eps_p"], g["eps_plastic"])
     np.testing.assert_array_equal(o["catalog"], g["catalog"])
     np.testing.assert_array_equal(o["Q0"], g["Q0"])
+
+
+def test_landau_3d_law_and_solver(golden):
+    # the reference's 3D Landau law (plain, piecewise and smooth capping) and
+    # its basic-scheme LS solver at fixed iteration counts and converged
+    g = golden("ls3d_landau_12x8x6")
+    v = tuple(g["v"])
+    e = g["strain"]
+    assert rel(OL.landau_stress_3d(e, g["lam"], g["mu"], v), g["sig_plain"]) < 1e-13
+    assert rel(OL.landau_stress_3d(e, g["lam"], g["mu"], v, "piecewise", 0.015), g["sig_piecewise"]) < 1e-13
+    assert rel(OL.landau_stress_3d(e, g["lam"], g["mu"], v, "smooth", 0.015, cap_power=2.0), g["sig_smooth"]) < 1e-13
+    kw = dict(eps_plastic=g["eps_plastic"])
+    for k in (1, 3):
+        eps, sig, _, _ = OL.spectral_solver_landau_3d(g["lam"], g["mu"], v, g["eps_bar"], max_iter=k, tol=0.0, **kw)
+        assert rel(eps, g[f"eps_it{k}"]) < 1e-12 and rel(sig, g[f"sig_it{k}"]) < 1e-12
+    eps, sig, _, _ = OL.spectral_solver_landau_3d(g["lam"], g["mu"], v, g["eps_bar"], max_iter=400, tol=1e-12, **kw)
+    assert rel(eps, g["eps_conv"]) < 1e-12 and rel(sig, g["sig_conv"]) < 1e-12
+    eps, sig, _, _ = OL.spectral_solver_landau_3d(g["lam"], g["mu"], v, g["eps_bar"], max_iter=400, tol=1e-12,
+                                                  cap_type="smooth", cap_limit=0.01, cap_power=2.0, **kw)
+    assert rel(eps, g["eps_cap"]) < 1e-12 and rel(sig, g["sig_cap"]) < 1e-12

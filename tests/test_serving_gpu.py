@@ -1,7 +1,7 @@
 """Served form: each request's result is the same alone and in the mix.
 
-A small stream of 2D solves, 2D KMC trajectories and 3D finite-strain steps
-runs through the continuous-batching server; then every request runs again
+A small stream of 2D solves, 2D KMC trajectories, 3D finite-strain steps and
+a 3D KMC trajectory runs through the continuous-batching server; then every request runs again
 alone on a fresh server.  Batching changes which replicas share a launch,
 never a replica's arithmetic, so fields, event lists and macro strains must
 agree to 1e-12 relative (they agree bit for bit in practice)."""
@@ -21,7 +21,7 @@ def _mix():
     from mgkmc_b200.serving import Request
     reqs = []
     spec = [("solve", 2, 64), ("trajectory", 2, 64), ("solve", 2, 128), ("solve", 2, 64), ("trajectory", 2, 64),
-            ("solve", 3, 32), ("solve", 2, 128), ("trajectory", 2, 128), ("solve", 3, 32)]
+            ("solve", 3, 32), ("solve", 2, 128), ("trajectory", 2, 128), ("solve", 3, 32), ("trajectory", 3, 64)]
     for i, (kind, dim, n) in enumerate(spec):
         reqs.append(Request(i, 0.002 * i, kind, dim, n, 1000 + 17 * i))
     return reqs
@@ -39,7 +39,11 @@ def test_served_results_match_alone():
     for req, rm in zip(reqs, mixed):
         alone = _server().run([req], realtime=False, keep_outputs=True)[0]
         assert not alone.error
-        if req.dim == 3:
+        if req.dim == 3 and req.kind == "trajectory":
+            assert len(rm.out["events"]) == 6 and rm.out["events"] == alone.out["events"]
+            assert np.allclose(rm.out["eps_macro"], alone.out["eps_macro"], rtol=1e-12, atol=0)
+            assert _rel(rm.out["sig"], alone.out["sig"]) < 1e-12
+        elif req.dim == 3:
             assert _rel(rm.out["F"], alone.out["F"]) < 1e-12
             assert _rel(rm.out["P"], alone.out["P"]) < 1e-12
         elif req.kind == "solve":
