@@ -66,6 +66,7 @@ def parse():
                     help="replicas of the batched KMC ensemble block (96 = the ensemble workload, ~1 min); 0 skips it")
     ap.add_argument("--kmc-events", type=int, default=2000,
                     help="events of the 256^2 x 8 KMC/AQS block (2000 = the KMC workload); 0 skips it")
+    ap.add_argument("--landau", type=int, default=1, help="1: the Landau 2D block (256^2, Anderson depth 5); 0 skips it")
     ap.add_argument("--serve-window", type=float, default=0.25,
                     help="seconds of the serving stream (Poisson 200 req/s, seed 3) replayed in the serving block; "
                          "0 skips it")
@@ -466,6 +467,56 @@ def run_kmc(n_events, n=256, M=8):
     return out
 
 
+# the Landau coefficients (v1, v2, v3, g1, g2, g3, g4) in Pa of the
+# reference's Landau tests
+LANDAU_COEFF = (-199.7e9, -75.4e9, -23.1e9, 1432.0e9, 311.0e9, 145.0e9, -273.0e9)
+
+
+def run_landau(n=256, m=5, reps=5):
+    """The Landau 2D LS solve (plane strain, Anderson depth m) at n^2 on the
+    benchmark material and eigenstrains with a sheared macro strain, tol 1e-8:
+    the numpy-in, numpy-out drop-in (host clock) and the device-resident
+    solve (CUDA events), with the per-iteration device time from a capped
+    solve of 2 iterations."""
+    import torch
+    from mgkmc_b200 import linear_elastic_simulator as les
+    from mgkmc_b200 import workloads as W
+    E, nu, ep, _ = W.ls2d_problem(n, n, seed=13)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    kw = dict(zip(("v1", "v2", "v3", "g1", "g2", "g3", "g4"), LANDAU_COEFF))
+    les.spectral_solver_landau_2d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, tol=1e-8, anderson_m=m)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        les.spectral_solver_landau_2d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, tol=1e-8, anderson_m=m)
+    dropin_ms = (time.perf_counter() - t0) / reps * 1e3
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    p = les.Ls2dBatch([(n, n)])
+    p.set_landau(LANDAU_COEFF)
+    p.set_anderson(m)
+    p.set_lame(0, t(lam), t(mu), t(ep))
+    eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    ms, its = {}, {}
+    for cap in (2, 400):
+        its[cap] = p.solve([0], [eb], [eps], [sig], max_iter=cap, tol=1e-8)[0].iterations
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            p.solve([0], [eb], [eps], [sig], max_iter=cap, tol=1e-8, sync=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms[cap] = e0.elapsed_time(e1) / reps
+    return {"workload": f"Landau LS 2D {n}^2 plane strain, Anderson depth {m}, tol 1e-8, benchmark material "
+                        f"and eigenstrains, eps_bar = [[0.008, 0.002], [0.002, -0.003]]",
+            "dropin_ms": dropin_ms, "device_solve_ms": ms[400], "iterations": int(its[400]),
+            "device_us_per_iteration": (ms[400] - ms[2]) / max(1, its[400] - 2) * 1e3}
+
+
 # ------------------------------------------------------- finite strain -----
 def run_finite_strain(n, peak):
     """3D finite-strain ramp (Neo-Hookean, 2 % F_p, F_xx to 1.05 in 10 load
@@ -697,6 +748,7 @@ def run_ours(a):
     kmc = None
     if world == 1 and a.kmc_events > 0:
         kmc = run_kmc(a.kmc_events)
+    landau = run_landau() if world == 1 and a.landau else None
     ensemble = None
     if world == 1 and a.ensemble > 0:
         from mgkmc_b200.serving import ensemble_requests, run_ensemble
@@ -754,7 +806,8 @@ def run_ours(a):
                     "d2h_bytes_per_step": int(d2h), "api": "mgkmc_b200.linear_elastic_simulator.Ls2dBatch",
                     "pipelining": "three plans on three streams, steps in turn", "host_result_err": e2e_err},
             "gpu_launches": gpu_launches, "roofline": roof, "cpu_baseline": cpu, "cpu_baselines_other": cpu_other,
-            "clocks": clocks, "finite_strain": finite_strain, "kmc": kmc, "serving": serving, "ensemble": ensemble}
+            "clocks": clocks, "finite_strain": finite_strain, "kmc": kmc, "landau": landau, "serving": serving,
+            "ensemble": ensemble}
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

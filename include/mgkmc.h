@@ -111,10 +111,24 @@ MGK_API int mgk_ls2d_set_rose(mgk_ls2d_t plan, double eta, double floor_fraction
  * 1 piecewise, 2 smooth (tanh of power smooth_power) at the equivalent
  * strain e_cap with tangent 2 tangent_ratio mu.  Medium (mean lam, mean mu):
  * give the material with mgk_ls2d_set_lame_rep.  Symmetric strains; FP64
- * plans only.  A solve runs the basic scheme; Anderson mixing of its iterates
- * is mgk_aa_update / mgk_aa_mix between one-iteration solves. */
+ * plans only.  A solve runs the basic scheme; mgk_ls2d_set_anderson adds the
+ * reference's Anderson mixing of the iterates inside the device loop. */
 MGK_API int mgk_ls2d_set_landau(mgk_ls2d_t plan, const double* v, int capping, double e_cap, double tangent_ratio,
                                 double smooth_power);
+/* Type-II Anderson mixing of depth m (0 <= m <= 8; 0 turns it off) inside
+ * the device loop of every later solve of this FP64 plan, as
+ * spectral_solver_landau_2d mixes its iterates
+ * (linear_elastic_simulator.py:1185-1209): after each iteration that neither
+ * converged nor went non-finite, x = g - dG gamma with gamma the
+ * least-squares fit of the last residual by the last m residual differences
+ * (strain inner products over the four tensor entries; eigenvalues of the
+ * Gram matrix below 1e-14 of the largest are dropped); a mix with
+ * non-finite coefficients takes the plain step and restarts the history
+ * from the last pair.  When the iteration cap ends the loop the outputs are
+ * those of the last mixed iterate; when it converges, of the image g.  A
+ * solve with m > 0 selects one replica.  Allocates a ring of (3 + 2m) strain
+ * fields (3 N doubles each) at the first call that needs it. */
+MGK_API int mgk_ls2d_set_anderson(mgk_ls2d_t plan, int m);
 /* Type-II Anderson mixing (linear_elastic_simulator.py:1185-1209) of
  * fixed-point iterates x -> g = G(x), fields of n doubles, history depth
  * 1 <= m <= 8.  hist: (2m + 2) n doubles (dF columns, dG columns, f_prev,

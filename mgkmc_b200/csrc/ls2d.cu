@@ -1374,6 +1374,226 @@ __global__ void aa_mix_kernel(long long n, const double* __restrict__ g, const d
   }
 }
 
+
+// ------------------------------------- Anderson mixing inside the LS loop ---
+// Type-II Anderson mixing of one replica's fixed-point iterates, run in the
+// loop body between the row kernel that forms the image g = G(x) (with the
+// update norm and the convergence decision) and the first row pass of the
+// next iterate (linear_elastic_simulator.py:1185-1209): residual f = g - x;
+// differences dF, dG of consecutive (f, g) pairs, at most m of them;
+// gamma = argmin |dF gamma - f|; x = g - dG gamma.  When the coefficients are
+// not finite the step is the plain one (x = g) and the history restarts from
+// the last pair, as the reference's fallback does.  Fields are the replica's
+// symmetric strain planes (xx, yy, xy); inner products weight the xy plane
+// by 2, as the reference's sums over the four tensor entries do.  The
+// differences sit in a ring of m slots; the least-squares solution does not
+// depend on the order of the columns.
+struct Ls2dAA {
+  int k;          // valid difference columns, in slots 0 .. k-1
+  int slot_next;  // ring slot of the next column
+  int have_prev;  // a previous (f, g) pair exists
+  int nmix;       // columns of the current mix (0: the plain step)
+  double A[kAaMax][kAaMax];  // Gram matrix <dF_i, dF_j>
+  double gamma[kAaMax];
+};
+
+// Mixing follows every iteration except the converged or non-finite one:
+// the reference leaves its loop with the image g there, and with the last
+// mixed iterate when the iteration cap ends the loop.
+__device__ __forceinline__ bool aa_skip(const Ls2dState& S) {
+  return S.done != 0 && S.status != MGK_NOT_CONVERGED;
+}
+
+// Ring buffer of one plan (n3 = 3 N doubles each): x, f_prev, g_prev, then
+// dF slots 0 .. m-1 and dG slots 0 .. m-1.
+__global__ void ls2d_aa_init_kernel(const Ls2dRep* reps, const int* sel, double* buf, Ls2dAA* aa) {
+  const Ls2dRep& R = reps[sel[0]];
+  const long long n3 = 3 * R.N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    buf[i] = R.eps[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    aa->k = 0;
+    aa->slot_next = 0;
+    aa->have_prev = 0;
+    aa->nmix = 0;
+  }
+}
+
+// f = g - x; with a previous pair, the new column dF = f - f_prev and
+// dG = g - g_prev goes to slot slot_next; (f, g) become the previous pair.
+// Per-block partial sums of <dF_j, dF_new> and <dF_j, f> over the columns
+// valid after this update.
+__global__ void __launch_bounds__(256) ls2d_aa_update_kernel(const Ls2dRep* reps, const Ls2dState* st,
+                                                             const int* sel, double* buf, const Ls2dAA* aa, int m,
+                                                             double* part) {
+  __shared__ double red[32];
+  const int r = sel[0];
+  const Ls2dRep& R = reps[r];
+  if (aa_skip(st[r])) return;
+  const long long N = R.N, n3 = 3 * N;
+  const int have_prev = aa->have_prev;
+  const int slot = have_prev ? aa->slot_next : -1;
+  const int ncols = have_prev ? min(aa->k + 1, m) : aa->k;
+  const double* x = buf;
+  double* fp = buf + n3;
+  double* gp = buf + 2 * n3;
+  double* dF = buf + 3 * n3;
+  double* dG = dF + (size_t)m * n3;
+  double an[kAaMax], ar[kAaMax];
+#pragma unroll
+  for (int j = 0; j < kAaMax; ++j) { an[j] = 0.0; ar[j] = 0.0; }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
+    const double w = i >= 2 * N ? 2.0 : 1.0;
+    const double gi = R.eps[i], fi = gi - x[i];
+    double df = 0.0;
+    if (have_prev) {
+      df = fi - fp[i];
+      dF[(size_t)slot * n3 + i] = df;
+      dG[(size_t)slot * n3 + i] = gi - gp[i];
+    }
+    fp[i] = fi;
+    gp[i] = gi;
+#pragma unroll
+    for (int j = 0; j < kAaMax; ++j)
+      if (j < ncols) {
+        const double c = w * (j == slot ? df : dF[(size_t)j * n3 + i]);
+        an[j] += c * df;
+        ar[j] += c * fi;
+      }
+  }
+  for (int j = 0; j < ncols; ++j) {
+    const double a = block_sum(an[j], red);
+    const double b = block_sum(ar[j], red);
+    if (threadIdx.x == 0) {
+      part[(size_t)blockIdx.x * 2 * kAaMax + j] = a;
+      part[(size_t)blockIdx.x * 2 * kAaMax + kAaMax + j] = b;
+    }
+  }
+}
+
+// Sums the partials, updates the Gram matrix and solves the k x k
+// least-squares problem through the eigen-decomposition of the Gram matrix
+// (cyclic Jacobi rotations, Golub & Van Loan, Matrix Computations, 8.5):
+// gamma = sum over eigenpairs (lambda_i, v_i) with lambda_i above
+// 1e-14 lambda_max of (v_i . b / lambda_i) v_i, the minimum-norm solution
+// with small singular values of dF cut off.  One block.
+__global__ void __launch_bounds__(256) ls2d_aa_solve_kernel(const Ls2dState* st, const int* sel, Ls2dAA* aa,
+                                                            int m, const double* part, int nb) {
+  __shared__ double red[32];
+  __shared__ double sums[2 * kAaMax];
+  if (aa_skip(st[sel[0]])) return;
+  const int have_prev = aa->have_prev;
+  const int ncols = have_prev ? min(aa->k + 1, m) : aa->k;
+  for (int q = 0; q < 2 * kAaMax; ++q) {
+    if (q % kAaMax >= ncols) continue;
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) a += part[(size_t)b * 2 * kAaMax + q];
+    a = block_sum(a, red);
+    if (threadIdx.x == 0) sums[q] = a;
+  }
+  if (threadIdx.x != 0) return;
+  if (have_prev) {
+    const int slot = aa->slot_next;
+    for (int j = 0; j < ncols; ++j) {
+      aa->A[slot][j] = sums[j];
+      aa->A[j][slot] = sums[j];
+    }
+    aa->k = ncols;
+    aa->slot_next = (slot + 1) % m;
+  }
+  aa->have_prev = 1;
+  const int k = aa->k;
+  aa->nmix = 0;
+  if (k == 0) return;
+  double a[kAaMax][kAaMax], v[kAaMax][kAaMax];
+  double fro = 0.0;
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j < k; ++j) {
+      a[i][j] = aa->A[i][j];
+      v[i][j] = i == j ? 1.0 : 0.0;
+      fro += a[i][j] * a[i][j];
+    }
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < k; ++i)
+      for (int j = i + 1; j < k; ++j) off += a[i][j] * a[i][j];
+    if (!(off > 1e-30 * fro)) break;  // also leaves on NaN
+    for (int p = 0; p < k; ++p)
+      for (int q = p + 1; q < k; ++q) {
+        const double apq = a[p][q];
+        if (fabs(apq) <= 1e-18 * sqrt(fabs(a[p][p] * a[q][q]))) {  // negligible: no rotation
+          a[p][q] = 0.0;
+          a[q][p] = 0.0;
+          continue;
+        }
+        const double th = (a[q][q] - a[p][p]) / (2.0 * apq);
+        const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        for (int i = 0; i < k; ++i) {
+          const double aip = a[i][p], aiq = a[i][q];
+          a[i][p] = c * aip - s * aiq;
+          a[i][q] = s * aip + c * aiq;
+        }
+        for (int i = 0; i < k; ++i) {
+          const double api = a[p][i], aqi = a[q][i];
+          a[p][i] = c * api - s * aqi;
+          a[q][i] = s * api + c * aqi;
+          const double vip = v[i][p], viq = v[i][q];
+          v[i][p] = c * vip - s * viq;
+          v[i][q] = s * vip + c * viq;
+        }
+      }
+  }
+  double lmax = 0.0;
+  for (int i = 0; i < k; ++i) lmax = fmax(lmax, a[i][i]);
+  double g[kAaMax];
+  bool ok = isfinite(lmax);
+  for (int j = 0; j < k; ++j) g[j] = 0.0;
+  if (ok && lmax > 0.0) {
+    for (int i = 0; i < k; ++i) {
+      const double li = a[i][i];
+      if (!(li > 1e-14 * lmax)) continue;
+      double vb = 0.0;
+      for (int j = 0; j < k; ++j) vb += v[j][i] * sums[kAaMax + j];
+      const double cf = vb / li;
+      for (int j = 0; j < k; ++j) g[j] += cf * v[j][i];
+    }
+  }
+  for (int j = 0; j < k; ++j) ok = ok && isfinite(g[j]);
+  if (!ok) {  // the plain step; the history restarts from the last pair
+    aa->k = 0;
+    aa->slot_next = 0;
+    return;
+  }
+  for (int j = 0; j < k; ++j) aa->gamma[j] = g[j];
+  aa->nmix = k;
+}
+
+// x = g - dG gamma (x = g for the plain step), into the plan's strain planes
+// (the next tau) and the ring's x.
+__global__ void __launch_bounds__(256) ls2d_aa_mix_kernel(const Ls2dRep* reps, const Ls2dState* st, const int* sel,
+                                                          double* buf, const Ls2dAA* aa, int m) {
+  const int r = sel[0];
+  const Ls2dRep& R = reps[r];
+  if (aa_skip(st[r])) return;
+  const long long n3 = 3 * R.N;
+  const int nmix = aa->nmix;
+  double gam[kAaMax];
+#pragma unroll
+  for (int j = 0; j < kAaMax; ++j) gam[j] = j < nmix ? aa->gamma[j] : 0.0;
+  double* x = buf;
+  const double* dG = buf + (3 + (size_t)m) * n3;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < kAaMax; ++j)
+      if (j < nmix) s += gam[j] * dG[(size_t)j * n3 + i];
+    const double xv = R.eps[i] - s;
+    R.eps[i] = xv;
+    x[i] = xv;
+  }
+}
+
 }  // namespace mgk
 
 // ================================================================== plan ===
@@ -1439,10 +1659,11 @@ struct mgk_ls2d_plan {
   cudaGraphExec_t exec = nullptr;
   int graph_mode = -1;  // -1 untried, 1 while-node graph, 0 host loop
   int graph_cap = 0;
+  int graph_aa = 0;     // Anderson depth of the current graph
   // instantiated loop graphs by selection shape (a serving loop selects
   // varying numbers of replicas; each shape is built once)
   struct GraphEntry {
-    int rows, cols, nsel, cap;
+    int rows, cols, nsel, cap, aa;
     cudaGraph_t g;
     cudaGraphExec_t x;
   };
@@ -1455,6 +1676,14 @@ struct mgk_ls2d_plan {
   int stage64 = 0, stage32 = 0;
   size_t tma_smem64 = 0, tma_smem32 = 0;
   int occ64 = 0, occ32 = 0, num_sms = 0;
+  // Anderson mixing inside the loop (one replica per solve): depth, ring
+  // buffer of (3 + 2 m) strain fields, state and per-block partial sums
+  int aa_m = 0;
+  double* aa_buf = nullptr;
+  size_t aa_doubles = 0;
+  Ls2dAA* d_aa = nullptr;
+  double* aa_part = nullptr;
+  int aa_nb = 0;
 };
 
 static int plan_alloc(mgk_ls2d_t p, void** ptr, size_t bytes) {
@@ -1528,6 +1757,9 @@ extern "C" int mgk_ls2d_destroy(mgk_ls2d_t p) {
   }
   if (p->staged) cudaEventDestroy(p->staged);
   for (void* a : p->allocations) cudaFree(a);
+  if (p->aa_buf) cudaFree(p->aa_buf);
+  if (p->d_aa) cudaFree(p->d_aa);
+  if (p->aa_part) cudaFree(p->aa_part);
   if (p->h_reps) cudaFreeHost(p->h_reps);
   if (p->h_maps) cudaFreeHost(p->h_maps);
   if (p->h_ctl) cudaFreeHost(p->h_ctl);
@@ -1836,6 +2068,56 @@ extern "C" int mgk_ls2d_set_landau(mgk_ls2d_t p, const double* v, int capping, d
   return ls2d_set_law(p, 3, 0.0, 0.0, 0, lp);
 }
 
+extern "C" int mgk_ls2d_set_anderson(mgk_ls2d_t p, int m) {
+  MGK_REQUIRE(p, "mgk_ls2d_set_anderson: null plan");
+  MGK_REQUIRE(m >= 0 && m <= kAaMax, "mgk_ls2d_set_anderson: depth must be 0..%d", kAaMax);
+  MGK_REQUIRE(m == 0 || p->prec == MGK_FP64, "mgk_ls2d_set_anderson: Anderson mixing runs in FP64 plans only");
+  if (m == p->aa_m) return MGK_OK;
+  int rc = staging_wait(p);
+  if (rc) return rc;
+  // loop graphs hold the ring's address: rebuild them
+  for (auto& e : p->gcache) {
+    cudaGraphExecDestroy(e.x);
+    cudaGraphDestroy(e.g);
+  }
+  p->gcache.clear();
+  p->graph = nullptr;
+  p->exec = nullptr;
+  p->sel_rows = p->sel_cols = p->nsel = 0;
+  if (p->graph_mode == 1) p->graph_mode = -1;
+  if (m > 0) {
+    const size_t need = (size_t)(3 + 2 * m) * 3 * (size_t)p->maxN;
+    if (need > p->aa_doubles) {
+      MGK_CUDA(cudaDeviceSynchronize());  // the old ring may be in use by queued work
+      if (p->aa_buf) cudaFree(p->aa_buf);
+      p->aa_buf = nullptr;
+      p->aa_doubles = 0;
+      if (cudaMalloc((void**)&p->aa_buf, need * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        p->aa_buf = nullptr;
+        p->aa_m = 0;
+        set_error("mgk_ls2d_set_anderson: cudaMalloc of %zu bytes failed", need * sizeof(double));
+        return MGK_OOM;
+      }
+      p->aa_doubles = need;
+    }
+    if (!p->d_aa) {
+      int dev = 0, sms = 148;
+      if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      p->aa_nb = std::max(1, std::min(2 * sms, ceil_div(3 * p->maxN, kThreads)));
+      if (cudaMalloc((void**)&p->d_aa, sizeof(Ls2dAA)) != cudaSuccess ||
+          cudaMalloc((void**)&p->aa_part, sizeof(double) * 2 * kAaMax * p->aa_nb) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("mgk_ls2d_set_anderson: cudaMalloc failed");
+        p->aa_m = 0;
+        return MGK_OOM;
+      }
+    }
+  }
+  p->aa_m = m;
+  return MGK_OK;
+}
+
 extern "C" int mgk_ls2d_set_eigenstrain_rep(mgk_ls2d_t p, int rep, const double* epsp, mgk_stream_t stream) {
   MGK_REQUIRE(p && rep >= 0 && rep < p->nrep && p->has_material[rep],
               "mgk_ls2d_set_eigenstrain: replica has no material");
@@ -1865,7 +2147,14 @@ struct LoopArgs {
   int stage_bytes;
   size_t tma_smem;
   int fast;           // warp-line iteration kernels
-  int law = 0;        // constitutive law of the warp-line row kernel (1: secant, 2: Rose)
+  int law = 0;        // constitutive law of the warp-line row kernel (1: secant, 2: Rose, 3: Landau)
+  // Anderson mixing (FP64 loop of a one-replica selection; aa_m = 0: none)
+  int aa_m = 0;
+  int aa_nb = 0;
+  double* aa_buf = nullptr;
+  Ls2dAA* aa = nullptr;
+  double* aa_part = nullptr;
+  const int* sel = nullptr;
 };
 
 template <typename TS, bool IN_SPEC, bool FINAL>
@@ -1904,6 +2193,13 @@ static int launch_body(const LoopArgs& a, cudaStream_t s) {
   else
     launch_row<TS, true, FINAL>(a, s);
   MGK_CUDA(cudaGetLastError());
+  if (sizeof(TS) == 8 && a.aa_m > 0) {
+    ls2d_aa_update_kernel<<<a.aa_nb, kThreads, 0, s>>>(a.reps, a.st, a.sel, a.aa_buf, a.aa, a.aa_m, a.aa_part);
+    ls2d_aa_solve_kernel<<<1, kThreads, 0, s>>>(a.st, a.sel, a.aa, a.aa_m, a.aa_part, a.aa_nb);
+    ls2d_aa_mix_kernel<<<a.aa_nb, kThreads, 0, s>>>(a.reps, a.st, a.sel, a.aa_buf, a.aa, a.aa_m);
+    launch_row<TS, false, FINAL>(a, s);  // tau of the mixed iterate
+    MGK_CUDA(cudaGetLastError());
+  }
   return MGK_OK;
 }
 
@@ -1952,6 +2248,42 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
     k2.blockDim = dim3(a.fast ? row_threads(a.fast) : kThreads);
   }
   MGK_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2));
+  if (sizeof(TS) == 8 && a.aa_m > 0) {
+    // Anderson mixing of the image, then tau of the mixed iterate
+    cudaGraphNode_t n3, n4, n5, n6;
+    cudaKernelNodeParams k3, k4, k5, k6;
+    memset(&k3, 0, sizeof(k3));
+    memset(&k4, 0, sizeof(k4));
+    memset(&k5, 0, sizeof(k5));
+    memset(&k6, 0, sizeof(k6));
+    void* a3[] = {&a.reps, &a.st, &a.sel, &a.aa_buf, &a.aa, &a.aa_m, &a.aa_part};
+    k3.func = (void*)ls2d_aa_update_kernel;
+    k3.gridDim = dim3(a.aa_nb);
+    k3.blockDim = dim3(kThreads);
+    k3.kernelParams = a3;
+    MGK_CUDA(cudaGraphAddKernelNode(&n3, body, &n2, 1, &k3));
+    void* a4[] = {&a.st, &a.sel, &a.aa, &a.aa_m, &a.aa_part, &a.aa_nb};
+    k4.func = (void*)ls2d_aa_solve_kernel;
+    k4.gridDim = dim3(1);
+    k4.blockDim = dim3(kThreads);
+    k4.kernelParams = a4;
+    MGK_CUDA(cudaGraphAddKernelNode(&n4, body, &n3, 1, &k4));
+    void* a5[] = {&a.reps, &a.st, &a.sel, &a.aa_buf, &a.aa, &a.aa_m};
+    k5.func = (void*)ls2d_aa_mix_kernel;
+    k5.gridDim = dim3(a.aa_nb);
+    k5.blockDim = dim3(kThreads);
+    k5.kernelParams = a5;
+    MGK_CUDA(cudaGraphAddKernelNode(&n5, body, &n4, 1, &k5));
+    cudaGraphConditionalHandle h0 = 0;
+    int zero = 0;
+    void* a6[] = {&a.reps, &a.st, &a.row_map, &a.row_local, &a.part, &a.repctr, &a.ctl, &h0, &zero, &zero};
+    k6.func = a.fast ? row_fast_fn<TS, false, FINAL>(a.fast, a.law) : (void*)ls2d_row_kernel<TS, TS, false, FINAL>;
+    k6.gridDim = dim3(a.rows);
+    k6.blockDim = dim3(a.fast ? row_threads(a.fast) : kThreads);
+    k6.sharedMemBytes = (unsigned)a.row_smem;
+    k6.kernelParams = a6;
+    MGK_CUDA(cudaGraphAddKernelNode(&n6, body, &n5, 1, &k6));
+  }
   return MGK_OK;
 }
 
@@ -2020,7 +2352,7 @@ static int build_graph(mgk_ls2d_t p, LoopArgs& a64, LoopArgs& a32, const int* d_
     cudaGraphDestroy(p->gcache.front().g);
     p->gcache.erase(p->gcache.begin());
   }
-  p->gcache.push_back({a64.rows, a64.cols, nsel, guard_cap, g, x});
+  p->gcache.push_back({a64.rows, a64.cols, nsel, guard_cap, a64.aa_m, g, x});
   p->graph = g;
   p->exec = x;
   return MGK_OK;
@@ -2148,6 +2480,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
                                     int max_iter, double tol, mgk_ls_info* infos, mgk_stream_t stream) {
   MGK_REQUIRE(p && eps_bar && nsel >= 1 && nsel <= p->nrep, "mgk_ls2d_solve_batch: bad argument");
   MGK_REQUIRE(max_iter >= 0 && max_iter <= 1000000, "mgk_ls2d_solve: max_iter out of range");
+  MGK_REQUIRE(p->aa_m == 0 || nsel == 1, "mgk_ls2d_solve_batch: Anderson mixing solves one replica per call");
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<int> selv(nsel);
   std::vector<char> seen(p->nrep, 0);
@@ -2168,7 +2501,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   // per-call fields and compact work maps
   int rows = 0, cols = 0;
   for (int q = 0; q < nsel; ++q) { rows += p->reps[selv[q]].row_items; cols += p->reps[selv[q]].col_items; }
-  const bool changed = rows != p->sel_rows || cols != p->sel_cols || nsel != p->nsel;
+  const bool changed = rows != p->sel_rows || cols != p->sel_cols || nsel != p->nsel || p->aa_m != p->graph_aa;
   int* row_map = p->h_maps;
   int* row_local = row_map + rows;
   int* col_map = row_local + rows;
@@ -2238,6 +2571,16 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     a64.law = p->law;
     LoopArgs a32 = a64;
     a32.law = 0;
+    if (p->aa_m > 0) {
+      a64.aa_m = p->aa_m;
+      a64.aa_nb = p->aa_nb;
+      a64.aa_buf = p->aa_buf;
+      a64.aa = p->d_aa;
+      a64.aa_part = p->aa_part;
+      a64.sel = d_sel;
+      ls2d_aa_init_kernel<<<p->aa_nb, kThreads, 0, s>>>(p->d_reps, d_sel, p->aa_buf, p->d_aa);
+      MGK_CUDA(cudaGetLastError());
+    }
     a32.row_smem = p->row_smem32;
     a32.col_smem = p->col_smem32;
     a32.stage_bytes = p->stage32;
@@ -2250,10 +2593,11 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     if (p->graph_mode == 1 && (changed || guard_cap > p->graph_cap)) {
       bool hit = false;
       for (auto& e : p->gcache)
-        if (e.rows == rows && e.cols == cols && e.nsel == nsel && e.cap >= guard_cap) {
+        if (e.rows == rows && e.cols == cols && e.nsel == nsel && e.cap >= guard_cap && e.aa == p->aa_m) {
           p->graph = e.g;
           p->exec = e.x;
           p->graph_cap = e.cap;
+          p->graph_aa = e.aa;
           hit = true;
           break;
         }
@@ -2265,6 +2609,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
       else {
         p->graph_mode = build_graph(p, a64, a32, d_sel, nsel, G, guard_cap) == MGK_OK ? 1 : 0;
         p->graph_cap = guard_cap;
+        p->graph_aa = p->aa_m;
       }
     }
     if (p->graph_mode == 1) {

@@ -12,6 +12,7 @@ the reference builds it whenever it is not passed (:25-29) and how its own
 drivers build it when they pass it (:142-145).
 """
 import ctypes
+import threading
 
 import numpy as np
 
@@ -95,6 +96,11 @@ class Ls2dBatch:
         arr = (ctypes.c_double * 7)(*[float(a) for a in v])
         L.check(L.lib().mgk_ls2d_set_landau(self._h, ctypes.cast(arr, ctypes.c_void_p), int(capping), float(e_cap),
                                             float(tangent_ratio), float(smooth_power)), "mgk_ls2d_set_landau")
+
+    def set_anderson(self, m):
+        """Type-II Anderson mixing of depth m (0: off) inside the device loop of
+        later solves; FP64 plans, one replica per solve."""
+        L.check(L.lib().mgk_ls2d_set_anderson(self._h, int(m)), "mgk_ls2d_set_anderson")
 
     def solve(self, reps, eps_bars, eps_out, sig_out, eps_init=None, max_iter=200, tol=1e-6, sync=True,
               stream=None):
@@ -300,6 +306,7 @@ def spectral_solver_rose_2d(lam, mu, eta, mu_floor_fraction=0.1, eps_bar=None, e
 
 
 _PLANS_LANDAU = {}
+_PLANS_LANDAU_LOCK = threading.Lock()
 
 
 def spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6,
@@ -309,13 +316,13 @@ def spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_
                               strain_capping_smooth_power=1.0, solver="dbfft", e33_state=None, anderson_m=5):
     """Nonlinear 2D Lippmann-Schwinger solve with the Landau small-strain law
     (linear_elastic_simulator.py:952-1228, solver "dbfft"), plane strain: the
-    basic scheme with the (mean lam, mean mu) medium, each iteration one
-    device solve step, and type-II Anderson mixing of the last anderson_m
-    iterates on the device (the small least-squares problem on the host).
-    Returns (eps, sig, eps.mean(axis=(0,1)), sig.mean(axis=(0,1))); a
-    non-finite update raises FloatingPointError as the reference does.
-    Plane stress, the Newton-CG branch and asymmetric strains are not built
-    (NotImplementedError); anderson_m is limited to 8."""
+    basic scheme with the (mean lam, mean mu) medium and type-II Anderson
+    mixing of the last anderson_m iterates, the whole loop (update norm,
+    convergence decision, least-squares fit and mix) on the device in one
+    graph launch.  Returns (eps, sig, eps.mean(axis=(0,1)),
+    sig.mean(axis=(0,1))); a non-finite update raises FloatingPointError as
+    the reference does.  Plane stress, the Newton-CG branch and asymmetric
+    strains are not built (NotImplementedError); anderson_m is limited to 8."""
     if plane_mode != "plane_strain":
         raise NotImplementedError("spectral_solver_landau_2d: plane stress is not built (plane strain only)")
     if solver != "dbfft":
@@ -339,69 +346,26 @@ def spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_
             e_cap = float(strain_capping_limit)
     nx, ny = lam.shape
     dev = torch.device("cuda", torch.cuda.current_device())
-    key = (nx, ny, dev.index)
-    p = _PLANS_LANDAU.get(key)
-    if p is None:
-        p = _PLANS_LANDAU[key] = Ls2dBatch([(nx, ny)])
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
-    p.set_landau((v1, v2, v3, g1, g2, g3, g4), cap, e_cap, strain_capping_tangent_ratio, strain_capping_smooth_power)
-    p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
-    # the iterate x (eps_bar-mean start as in the reference) and its image g
-    if eps_init is None:
-        x = t(np.broadcast_to(eps_bar, (nx, ny, 2, 2)))
-    else:
-        x = t(eps_init)
-        x += t(eps_bar) - x.mean(dim=(0, 1))
-    g = torch.empty_like(x)
-    sig = torch.empty_like(x)
-    n = x.numel()
-    lib = L.lib()
-    if m > 0:
-        hist = torch.empty((2 * m + 2) * n, dtype=torch.float64, device=dev)
-        work = torch.empty(int(lib.mgk_aa_work_bytes(n)), dtype=torch.uint8, device=dev)
-        dots = torch.zeros(16, dtype=torch.float64, device=dev)
-    A = np.zeros((max(m, 1), max(m, 1)))
-    k, slot_next, have_prev = 0, 0, False
-    S = L.stream_ptr(None)
-    info = None
-    for it in range(max_iter):
-        info = p.solve([0], [eps_bar], [g], [sig], eps_init=[x], max_iter=1, tol=tol)[0]
-        if info.status == L.NONFINITE or not np.isfinite(info.final_diff):
-            raise FloatingPointError("spectral_solver_landau_2d: non-finite strain update in LS loop (Landau energy "
-                                     "likely unstable at this strain; consider strain capping or smaller load steps).")
-        if verbose and it % 10 == 0:
-            print(f"  [landau-LS] iter {it:04d}: rel_diff = {info.final_diff:.3e}")
-        if info.final_diff < tol:
-            eps_np, sig_np = g.cpu().numpy(), sig.cpu().numpy()
-            return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
-        if m == 0:
-            x, g = g, x
-            continue
-        slot = slot_next if have_prev else 0
-        if have_prev:
-            slot_next = (slot_next + 1) % m
-            k = min(k + 1, m)
-        L.check(lib.mgk_aa_update(n, L.ptr(x), L.ptr(g), L.ptr(hist), m, slot, int(have_prev), k, L.ptr(dots),
-                                  L.ptr(work), S), "mgk_aa_update")
-        have_prev = True
-        if k == 0:
-            x, g = g, x
-            continue
-        d = dots.cpu().numpy()
-        A[slot, :k] = d[:k]
-        A[:k, slot] = d[:k]
-        gam = np.linalg.lstsq(A[:k, :k], d[8:8 + k], rcond=None)[0]
-        if not np.all(np.isfinite(gam)):
-            # ill-conditioned mix: the plain step, history restarted from the last pair
-            x, g = g, x
-            k, slot_next = 0, 0
-            continue
-        garr = (ctypes.c_double * k)(*gam)
-        L.check(lib.mgk_aa_mix(n, L.ptr(g), L.ptr(hist), m, k, ctypes.cast(garr, ctypes.c_void_p), L.ptr(x), S),
-                "mgk_aa_mix")
-    # not converged: the final stress of the last iterate (reference :1212-1228)
-    p.solve([0], [eps_bar], [g], [sig], eps_init=[x], max_iter=0, tol=tol)
-    eps_np, sig_np = g.cpu().numpy(), sig.cpu().numpy()
+    with _PLANS_LANDAU_LOCK:
+        key = (nx, ny, dev.index)
+        p = _PLANS_LANDAU.get(key)
+        if p is None:
+            p = _PLANS_LANDAU[key] = Ls2dBatch([(nx, ny)])
+        p.set_landau((v1, v2, v3, g1, g2, g3, g4), cap, e_cap, strain_capping_tangent_ratio,
+                     strain_capping_smooth_power)
+        p.set_anderson(m)
+        p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
+        eps = torch.empty((nx, ny, 2, 2), dtype=torch.float64, device=dev)
+        sig = torch.empty_like(eps)
+        init = None if eps_init is None else [t(eps_init)]
+        info = p.solve([0], [eps_bar], [eps], [sig], eps_init=init, max_iter=max_iter, tol=tol)[0]
+        eps_np, sig_np = eps.cpu().numpy(), sig.cpu().numpy()
+    if info.status == L.NONFINITE or not np.isfinite(info.final_diff):
+        raise FloatingPointError("spectral_solver_landau_2d: non-finite strain update in LS loop (Landau energy "
+                                 "likely unstable at this strain; consider strain capping or smaller load steps).")
+    if verbose:
+        print(f"  [landau-LS] {info.iterations} iterations: rel_diff = {info.final_diff:.3e}")
     return eps_np, sig_np, eps_np.mean(axis=(0, 1)), sig_np.mean(axis=(0, 1))
 
 

@@ -237,6 +237,56 @@ def test_landau_against_oracle(les, nx, ny, m, cap):
     assert rel(sig, o[1]) < TOL
 
 
+@pytest.mark.parametrize("it", [1, 2, 7])
+def test_landau_capped_iterations_return_the_mixed_iterate(les, it):
+    # when the iteration cap ends the loop, the reference returns the last
+    # mixed iterate and its stress (linear_elastic_simulator.py:1211-1228):
+    # the device loop mixes after the capped iteration too
+    E, nu, ep, _ = W.ls2d_problem(64, 64, seed=21)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    eps, sig, _, _ = les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, eps_plastic=ep,
+                                                   max_iter=it, tol=1e-14, anderson_m=3)
+    o = OL.spectral_solver_landau_2d(lam, mu, LANDAU_V, eb, ep, max_iter=it, tol=1e-14, anderson_m=3)
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
+def test_landau_device_loop_iteration_cost(les):
+    # the Anderson-mixed Landau loop runs in one graph launch: per-iteration
+    # device time at 256^2 (row, column, history update, least squares, mix,
+    # tau of the mixed iterate)
+    import torch
+    E, nu, ep, _ = W.ls2d_problem(256, 256, seed=13)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    p = les.Ls2dBatch([(256, 256)])
+    p.set_landau(LANDAU_V)
+    p.set_anderson(5)
+    p.set_lame(0, t(lam), t(mu), t(ep))
+    eps = torch.empty((256, 256, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    ms, its = {}, {}
+    for n in (2, 400):
+        its[n] = p.solve([0], [eb], [eps], [sig], max_iter=n, tol=1e-12)[0].iterations  # graph built
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(5):
+            p.solve([0], [eb], [eps], [sig], max_iter=n, tol=1e-12, sync=False)
+        b.record()
+        torch.cuda.synchronize()
+        ms[n] = a.elapsed_time(b) / 5
+    assert its[2] == 2 and its[400] > 6
+    per_it_us = (ms[400] - ms[2]) / (its[400] - 2) * 1e3
+    print(f"landau+AA device loop: {per_it_us:.1f} us per iteration at 256^2")
+    assert per_it_us < 60.0
+
+
 def test_anderson_kernels():
     # history update, inner products and mix of mgk_aa_* against numpy
     import ctypes
