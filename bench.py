@@ -356,7 +356,7 @@ def _fifo(arrivals, services):
     return np.array(lat)
 
 
-def run_serving(window, n_plain=0):
+def run_serving(window, n_plain=0, progress=None):
     """The serving stream's first `window` seconds of arrivals served by the
     continuous-batching server (mixed precision, arrivals replayed in real
     time, latency = completion - arrival on the host clock), against the plain
@@ -368,7 +368,9 @@ def run_serving(window, n_plain=0):
     subsample and gives each other request the measured service time of a
     subsampled request of its class (kind, dimension, side) -- an estimate,
     labelled as such.  Solves/s: served = solves over the makespan; plain =
-    solves over the measured busy time."""
+    solves over the measured busy time.  progress: seconds between progress
+    lines on stderr, and the served summary printed there as soon as it is
+    known (None: quiet)."""
     from mgkmc_b200.serving import Server, request_stream, summarize
     reqs = [r for r in request_stream(rate=200.0, duration=60.0, seed=3) if r.t_arrival <= window]
     out = {"workload": (f"serving stream (Poisson 200 req/s, seed 3; 60 % equilibrium solves, 40 % 100-event KMC "
@@ -379,9 +381,12 @@ def run_serving(window, n_plain=0):
         k = f"{r.dim}d_{r.kind}_{r.n}"
         out["classes"][k] = out["classes"].get(k, 0) + 1
     srv = Server(mode="served")
+    srv.progress = progress
     srv.prepare(reqs)
     res = srv.run(reqs, realtime=True)
     out["served_mixed"] = summarize(res)
+    if progress is not None:
+        print(json.dumps({"served_mixed": out["served_mixed"]}), file=sys.stderr, flush=True)
     del srv
     if n_plain and n_plain < len(reqs):
         rng = np.random.default_rng(4)
@@ -389,6 +394,7 @@ def run_serving(window, n_plain=0):
     else:
         sub = reqs
     srv = Server(mode="sequential")
+    srv.progress = progress
     srv.prepare(sub)
     res_p = srv.run(sub, realtime=False)
     ok = [r for r in res_p if not r.error]
@@ -872,7 +878,7 @@ def main():
         torch.cuda.set_device(0)
         clk = ClockSampler(0)
         clk.start()
-        out = run_serving(a.serve_window, a.serve_plain)
+        out = run_serving(a.serve_window, a.serve_plain, progress=30.0)
         out["clocks"] = clk.stop()
         print(json.dumps({"serving": out}), flush=True)
         return

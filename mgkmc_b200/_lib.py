@@ -95,6 +95,7 @@ _SIGS = {
     "mgk_fs3d_set_material": (c_int, [_P, _P, _P, _P, _P]),
     "mgk_fs3d_set_F": (c_int, [_P, _P, _P]),
     "mgk_fs3d_set_plane_strain": (c_int, [_P, c_int]),
+    "mgk_fs3d_set_plane_stress": (c_int, [_P, c_int]),
     "mgk_fs3d_step": (c_int, [_P, POINTER(c_double), c_int, c_int, POINTER(c_double), POINTER(c_int), c_double,
                               c_double, c_double, c_double, c_int, c_double, c_int, POINTER(c_double),
                               POINTER(FsInfo), _P]),

@@ -50,6 +50,7 @@ struct FsArgs {
   int nx, ny, nz, nzh, ld, tc;
   long long N;
   int has_fp, model;  // model 0 SVK, 1 Neo-Hookean
+  int plane_stress;   // (nx, 1, ny) plan of a 2D plane-stress SVK solve: Cauchy J carries F33
   FftLen fx, fy, fz;
   const double* F;
   const double* Fpi;
@@ -590,6 +591,28 @@ __global__ void fs_scalar_kernel(FsArgs a, int nb, cudaGraphConditionalHandle co
   }
 }
 
+// Out-of-plane stretch of a plane-stress SVK voxel on the (nx, 1, ny) plan
+// (finite_strain_simulator.py:1042-1049): with the in-plane Green-Lagrange
+// strain of Fe = F Fp^-1 (plane axes x and z), E33 = -(lam / (2 mu)) tr E,
+// F33 = sqrt(max(1e-12, 1 + 2 E33)); lam is the plane-stress lambda the
+// caller gives as the material.  1 for every other plan.
+__device__ __forceinline__ double fs_f33(const FsArgs& a, long long i, const double* Fv) {
+  if (!a.plane_stress) return 1.0;
+  double Fe[9];
+  if (a.has_fp) {
+    double Fpi[9];
+    for (int q = 0; q < 9; ++q) Fpi[q] = a.Fpi[q * a.N + i];
+    mm(Fv, Fpi, Fe);
+  } else {
+    for (int q = 0; q < 9; ++q) Fe[q] = Fv[q];
+  }
+  const double cxx = Fe[0] * Fe[0] + Fe[3] * Fe[3] + Fe[6] * Fe[6];
+  const double czz = Fe[2] * Fe[2] + Fe[5] * Fe[5] + Fe[8] * Fe[8];
+  const double trE = 0.5 * (cxx - 1.0) + 0.5 * (czz - 1.0);
+  const double e33 = -(a.lam[i] / (2.0 * a.mu[i])) * trE;
+  return sqrt(fmax(1e-12, 1.0 + 2.0 * e33));
+}
+
 // Constitutive evaluation at F + alpha (x + dbar) (or at F when dx is 0):
 // writes Fout, Pout; per-CTA partials: min Je, NaN count, sum F^2, sum x^2,
 // and the Cauchy stress sums (cauchy_from_P_3d).  16 values per CTA.
@@ -614,6 +637,7 @@ __global__ void fs_constitutive_kernel(FsArgs a, double alpha, const double* __r
     if (!(law.Je == law.Je)) nan += 1;
     mnJ = fmin(mnJ, law.Je);
     double J = det3(Ft);
+    if (a.plane_stress) J *= fs_f33(a, i, Ft);
     if (fabs(J) < 1e-14) J = 1e-14;
     double PF[9];
     mmt(P, Ft, PF);
@@ -694,12 +718,15 @@ __global__ void fs_meanF_finalize(FsArgs a, int nb) {
   }
 }
 
-// Cauchy stress field (cauchy_from_P_3d), tensor-first
-__global__ void fs_cauchy_kernel(const double* __restrict__ P, const double* __restrict__ F, long long N, double* sig) {
+// Cauchy stress field (cauchy_from_P_3d; cauchy_from_P with F33 for plane
+// stress), tensor-first
+__global__ void fs_cauchy_kernel(FsArgs a, double* sig) {
+  const long long N = a.N;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
     double Pv[9], Fv[9], PF[9];
-    for (int q = 0; q < 9; ++q) { Pv[q] = P[q * N + i]; Fv[q] = F[q * N + i]; }
+    for (int q = 0; q < 9; ++q) { Pv[q] = a.P[q * N + i]; Fv[q] = a.F[q * N + i]; }
     double J = det3(Fv);
+    if (a.plane_stress) J *= fs_f33(a, i, Fv);
     if (fabs(J) < 1e-14) J = 1e-14;
     mmt(Pv, Fv, PF);
     for (int q = 0; q < 9; ++q) sig[q * N + i] = PF[q] / J;
@@ -1087,13 +1114,14 @@ struct mgk_fs3d_plan {
   // plane strain embedded as (nx, 1, ny): the out-of-plane F_yy = 1 adds N
   // to ||F||^2, which the 2D solver's Newton norm does not contain
   double ff_offset = 0.0;
+  int plane_stress = 0;  // 2D plane-stress SVK on the (nx, 1, ny) plan
 };
 
 static FsArgs fs_args(mgk_fs3d_t p) {
   FsArgs a;
   memset(&a, 0, sizeof(a));
   a.nx = p->nx; a.ny = p->ny; a.nz = p->nz; a.nzh = p->nzh; a.ld = p->ld; a.tc = p->tc;
-  a.N = p->N; a.has_fp = p->has_fp; a.model = p->model;
+  a.N = p->N; a.has_fp = p->has_fp; a.model = p->model; a.plane_stress = p->plane_stress;
   a.fx = p->fx; a.fy = p->fy; a.fz = p->fz;
   a.F = p->F; a.Fpi = p->Fpi; a.mu = p->mu; a.lam = p->lam; a.P = p->P;
   a.x = p->x; a.r = p->r; a.p = p->p; a.q = p->q; a.Fout = p->Ftr; a.Pout = p->Ptr;
@@ -1301,7 +1329,7 @@ extern "C" int mgk_fs3d_get(mgk_fs3d_t p, double* F_out, double* P_out, double* 
   if (F_out) MGK_CUDA(cudaMemcpyAsync(F_out, p->F, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
   if (P_out) MGK_CUDA(cudaMemcpyAsync(P_out, p->P, sizeof(double) * 9 * p->N, cudaMemcpyDeviceToDevice, s));
   if (sig_out) {
-    fs_cauchy_kernel<<<p->nblk, 256, 0, s>>>(p->P, p->F, p->N, sig_out);
+    fs_cauchy_kernel<<<p->nblk, 256, 0, s>>>(fs_args(p), sig_out);
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
@@ -1636,6 +1664,14 @@ extern "C" int mgk_fs3d_autotune(mgk_fs3d_t p, int reps, int* chosen, float* bes
 
 extern "C" int mgk_fs3d_set_plane_strain(mgk_fs3d_t p, int on) {
   MGK_REQUIRE(p && (!on || p->ny == 1), "mgk_fs3d_set_plane_strain: the plan must be (nx, 1, ny)");
+  p->ff_offset = on ? (double)p->N : 0.0;
+  return MGK_OK;
+}
+
+extern "C" int mgk_fs3d_set_plane_stress(mgk_fs3d_t p, int on) {
+  MGK_REQUIRE(p && (!on || (p->ny == 1 && p->model == 0)),
+              "mgk_fs3d_set_plane_stress: the plan must be (nx, 1, ny) with the SVK model");
+  p->plane_stress = on ? 1 : 0;
   p->ff_offset = on ? (double)p->N : 0.0;
   return MGK_OK;
 }

@@ -322,7 +322,7 @@ def _checkpoint(path, step, E, nu, F, Sig, F_mac, S_mac, pixel):
                          Sig.permute(2, 3, 4, 0, 1).cpu().numpy(), F_mac, S_mac, pixel)
 
 
-# ------------------------------------------------ 2D plane strain ---
+# ------------------------------------- 2D plane strain and plane stress ---
 _PLANE = (0, 2)  # 2D tensor index -> index in the embedded (nx, 1, ny) plan
 
 
@@ -354,15 +354,27 @@ def _embed_small(M2, fill, dtype=np.float64):
 
 
 class Fs2dSolver:
-    """2D plane-strain finite-strain solver: the 3D plan of an (nx, 1, ny) grid
-    with the out-of-plane axis y (F_yy = 1) and the 2D Newton norm
-    (``mgk_fs3d_set_plane_strain``).  Fields in and out are the reference's
+    """2D finite-strain solver: the 3D plan of an (nx, 1, ny) grid with the
+    out-of-plane axis y (F_yy = 1) and the 2D Newton norm.  plane_mode
+    "plane_strain" (``mgk_fs3d_set_plane_strain``) or, for the SVK model,
+    "plane_stress" (``mgk_fs3d_set_plane_stress``: the material's lam is the
+    plane-stress lambda E nu / (1 - nu^2), and the Cauchy stress carries the
+    out-of-plane stretch F33).  Fields in and out are the reference's
     tensor-first (2, 2, nx, ny)."""
 
-    def __init__(self, nx, ny, model="svk", precision="fp64", device=None):
+    def __init__(self, nx, ny, model="svk", precision="fp64", device=None, plane_mode="plane_strain"):
+        if plane_mode not in ("plane_strain", "plane_stress"):
+            raise ValueError(f"plane_mode={plane_mode!r}")
+        if plane_mode == "plane_stress" and model != "svk":
+            raise NotImplementedError("plane stress runs with the SVK model (the Neo-Hookean out-of-plane Newton "
+                                      "solve is not built)")
         self.nx, self.ny = int(nx), int(ny)
+        self.plane_mode = plane_mode
         self.s = Fs3dSolver(self.nx, 1, self.ny, model=model, precision=precision, device=device)
-        L.check(L.lib().mgk_fs3d_set_plane_strain(self.s._h, 1), "mgk_fs3d_set_plane_strain")
+        if plane_mode == "plane_stress":
+            L.check(L.lib().mgk_fs3d_set_plane_stress(self.s._h, 1), "mgk_fs3d_set_plane_stress")
+        else:
+            L.check(L.lib().mgk_fs3d_set_plane_strain(self.s._h, 1), "mgk_fs3d_set_plane_strain")
         self.device = self.s.device
 
     def set_material(self, lam, mu, Fp=None, stream=None):
@@ -404,15 +416,18 @@ def finite_strain_solver_step_2d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None
                                  enable_console=True, model_type="svk", plane_mode="plane_strain", A_m=0.0, B_m=0.0,
                                  C_m=0.0, solver="al", pixel=1.0, lam=None, mu=None, **unused):
     """One mixed-BC 2D load step (mgkmc/finite_strain_simulator.py:2356-2572),
-    Newton-Krylov path, plane strain: returns (F, P, Sig, None, F_bar_current)
-    with (2, 2, nx, ny) fields.  The Lame fields come from ``C4`` (C4[0,0,1,1]
-    and C4[0,1,0,1], the reference's build_C4_2d) or ``lam``/``mu``."""
+    Newton-Krylov path, plane strain (SVK, Neo-Hookean) or plane stress (SVK):
+    returns (F, P, Sig, None, F_bar_current) with (2, 2, nx, ny) fields.  The
+    Lame fields come from ``C4`` (C4[0,0,1,1] and C4[0,1,0,1], the reference's
+    build_C4_2d, whose lambda is the plane-stress one in plane stress) or
+    ``lam``/``mu``."""
     if solver not in ("newton_cg", "newton"):
         raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
     if model_type not in _MODEL:
         raise NotImplementedError(f"model_type={model_type!r}: SVK and Neo-Hookean run on the GPU")
-    if plane_mode != "plane_strain":
-        raise NotImplementedError("plane_mode='plane_stress': only plane strain runs on the GPU")
+    if plane_mode == "plane_stress" and model_type != "svk":
+        raise NotImplementedError("plane stress runs with the SVK model on the GPU (the Neo-Hookean out-of-plane "
+                                  "Newton solve is not built)")
     torch = _torch()
     F = np.ascontiguousarray(F, dtype=np.float64)
     nx, ny = F.shape[2:]
@@ -420,10 +435,10 @@ def finite_strain_solver_step_2d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None
         lam = np.ascontiguousarray(C4[0, 0, 1, 1])
         mu = np.ascontiguousarray(C4[0, 1, 0, 1])
     dev = torch.device("cuda", torch.cuda.current_device())
-    key = (nx, ny, model_type, dev.index)
+    key = (nx, ny, model_type, plane_mode, dev.index)
     s = _PLANS2.get(key)
     if s is None:
-        s = _PLANS2[key] = Fs2dSolver(nx, ny, model=model_type)
+        s = _PLANS2[key] = Fs2dSolver(nx, ny, model=model_type, plane_mode=plane_mode)
     s.set_material(lam, mu, Fp)
     s.set_F(F)
     Fb, info = s.step(F_bar, driving_component, P_target, P_mask, E_avg, nu_avg, tol_NW, tol_CG, max_NW, tol_macro,
@@ -450,9 +465,10 @@ def finite_strain_simulation_2d(E, nu, driving_component, eps_target, n_steps, m
                                 enable_console=True, checkpoint_interval="none", checkpoint_path=None,
                                 vtk_interval="none", vtk_path=None, model_type="svk", A_m=0.0, B_m=0.0, C_m=0.0,
                                 solver="al", Fp=None, precision="fp64", **unused):
-    """Incremental 2D plane-strain finite-strain ramp
-    (finite_strain_simulator.py:2580-2851) on one device-resident embedded
-    plan (``Fs2dSolver``): per load step the boundary conditions of
+    """Incremental 2D finite-strain ramp (finite_strain_simulator.py:2580-2851),
+    plane strain or (SVK) plane stress with the plane-stress lambda
+    E nu / (1 - nu^2) of build_C4_2d, on one device-resident embedded plan
+    (``Fs2dSolver``): per load step the boundary conditions of
     build_finite_strain_bc at eps_target * s / n_steps (seeded with the
     previous F_bar), one Newton-Krylov load step from the previous field.
     Returns (F_macro, Sig_macro, P_macro, F list, Sig list) with (2, 2, nx, ny)
@@ -462,17 +478,18 @@ def finite_strain_simulation_2d(E, nu, driving_component, eps_target, n_steps, m
     from datetime import datetime as _dt
     if solver not in ("newton_cg", "newton"):
         raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
-    if plane_mode != "plane_strain":
-        raise NotImplementedError("plane_mode='plane_stress': only plane strain runs on the GPU")
     if vtk_interval not in (None, "none"):
         raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
     mixed_targets = {} if mixed_targets is None else mixed_targets
     E = np.ascontiguousarray(E, dtype=np.float64)
     nu = np.ascontiguousarray(nu, dtype=np.float64)
     nx, ny = E.shape
-    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    if plane_mode == "plane_stress":
+        lam = E * nu / (1.0 - nu ** 2)
+    else:
+        lam = E * nu / ((1 + nu) * (1 - 2 * nu))
     mu = E / (2 * (1 + nu))
-    s_ = Fs2dSolver(nx, ny, model=model_type, precision=precision)
+    s_ = Fs2dSolver(nx, ny, model=model_type, precision=precision, plane_mode=plane_mode)
     s_.set_material(lam, mu, Fp)
     s_.set_F(np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny))))
     lbl = _COMP.get(tuple(driving_component), "xx")

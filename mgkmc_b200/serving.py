@@ -48,6 +48,7 @@ is busy waits, and that wait is part of its latency.
 """
 import collections
 import queue
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -160,10 +161,18 @@ class _Bucket3:
         self.tasks = []
 
 
+def _by_tol(tasks):
+    """[(tol, tasks solved at tol)] in first-seen order."""
+    groups = {}
+    for t in tasks:
+        groups.setdefault(t.need[5], []).append(t)
+    return list(groups.items())
+
+
 class Server:
     def __init__(self, mode="served", hbm_budget=None, slots=None, ls_tol=1e-8, ls_max_iter=500,
                  macro_tol=1e4, macro_max_iter=20, n_events=100, n_modes=8, q_mean=1.0, kmc_T=300.0,
-                 fs_strain=0.005, fs_tol_nw=1e-8, fs_tol_cg=1e-6, selection=None, device=None):
+                 fs_strain=0.005, fs_tol_nw=1e-8, fs_tol_cg=1e-6, selection=None, device=None, traj_ls_tol=1e-6):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("mgkmc_b200 needs a CUDA device (no CPU fallback)")
@@ -174,7 +183,10 @@ class Server:
         self.precision = "mixed" if self.served else "fp64"
         self.ls_start = "warm" if self.served else "cold"
         self.selection = selection or ("fast" if self.served else "exact")
-        self.ls_tol, self.ls_max_iter = ls_tol, ls_max_iter
+        # single solves at ls_tol; a trajectory's re-solves at the KMC driver's
+        # spectral_solver_2d default tolerance (kmc_simulator.py:134, :517 pass
+        # no tol; linear_elastic_simulator.py:13)
+        self.ls_tol, self.ls_max_iter, self.traj_ls_tol = ls_tol, ls_max_iter, traj_ls_tol
         self.macro_tol, self.macro_max_iter = macro_tol, macro_max_iter
         self.n_events, self.n_modes, self.q_mean, self.kmc_T = n_events, n_modes, q_mean, kmc_T
         self.fs_strain, self.fs_tol_nw, self.fs_tol_cg = fs_strain, fs_tol_nw, fs_tol_cg
@@ -189,6 +201,18 @@ class Server:
         self.fs_plans = {}
         self.used = 0
         self.lock = threading.Lock()
+        self.progress = None  # seconds between progress lines on stderr (None: quiet)
+        self._last_report = 0.0
+
+    def _report(self, tag):
+        if self.progress is None:
+            return
+        now = self._now()
+        if now - self._last_report < self.progress:
+            return
+        self._last_report = now
+        done = sum(1 for r in self.results.values() if r.t_done > 0)
+        print(f"[{tag}] t = {now:.0f} s: {done} / {len(self.results)} requests done", file=sys.stderr, flush=True)
 
     # ------------------------------------------------------------ helpers ---
     def _now(self):
@@ -230,7 +254,7 @@ class Server:
         sigM = None
         for _ in range(self.macro_max_iter):
             eps_bar[strain_mask] = target[strain_mask]
-            info = yield ("solve", eps_bar.copy(), eps, sig, eps if warm else None)
+            info = yield ("solve", eps_bar.copy(), eps, sig, eps if warm else None, self.ls_tol)
             warm = self.ls_start == "warm"
             res.solves += 1
             res.ls_iterations += info.iterations
@@ -251,7 +275,7 @@ class Server:
         n, M = req.n, self.n_modes
         E, nu, _, _ = W.ls2d_problem_dev(n, n, req.seed, self.dev)
         cat, Q0 = W.kmc2d_state_dev(n, n, M, req.seed, self.dev, q_mean=self.q_mean)
-        k = Kmc2D(E, nu, cat, Q0, T=self.kmc_T if req.T is None else req.T, q_mean=self.q_mean, ls_tol=self.ls_tol,
+        k = Kmc2D(E, nu, cat, Q0, T=self.kmc_T if req.T is None else req.T, q_mean=self.q_mean, ls_tol=self.traj_ls_tol,
                   ls_max_iter=self.ls_max_iter, selection=self.selection, ls_start=self.ls_start,
                   precision=self.precision, ls=b.plan, rep=slot, stream=b.stream)
         rng = np.random.default_rng(req.seed)
@@ -267,7 +291,7 @@ class Server:
                             eps_p=k.eps_p, time=out["time"], steps=out["steps"])
             if need[0] == "solve":
                 _, _, eb, eo, so, init = k.solve_args()
-                info = yield ("solve", eb, eo, so, init)
+                info = yield ("solve", eb, eo, so, init, self.traj_ls_tol)
                 res.ls_iterations += info.iterations
                 send = info
             else:
@@ -288,7 +312,8 @@ class Server:
         n, M = req.n, self.n_modes
         E, nu = W.ls3d_material_dev(n, n, n, req.seed, self.dev)
         cat, Q0 = W.kmc3d_state_dev(n, n, n, M, req.seed, self.dev, q_mean=self.q_mean)
-        k = Kmc3D(E, nu, cat, Q0, T=self.kmc_T if req.T is None else req.T, q_mean=self.q_mean, ls_tol=self.ls_tol,
+        k = Kmc3D(E, nu, cat, Q0, T=self.kmc_T if req.T is None else req.T, q_mean=self.q_mean,
+                  ls_tol=self.traj_ls_tol,
                   ls_max_iter=self.ls_max_iter, selection=self.selection, ls_start=self.ls_start,
                   precision=self.precision, ls=b.plan, rep=slot, stream=b.stream)
         k.host_result = False
@@ -306,7 +331,7 @@ class Server:
                             eps_p=k.eps_p, time=out["time"], steps=out["steps"])
             if need[0] == "solve":
                 _, _, eb, eo, so, init = k.solve_args()
-                info = yield ("solve", eb, eo, so, init)
+                info = yield ("solve", eb, eo, so, init, self.traj_ls_tol)
                 res.ls_iterations += info.iterations
                 send = info
             else:
@@ -333,12 +358,12 @@ class Server:
                 alive.append(t)
                 (solving if t.need[0] == "solve" else syncing).append(t)
         b.tasks = alive
-        if solving:
-            infos = b.plan.solve([t.slot for t in solving], [t.need[1] for t in solving],
-                                 [t.need[2] for t in solving], [t.need[3] for t in solving],
-                                 eps_init=[t.need[4] for t in solving], max_iter=self.ls_max_iter, tol=self.ls_tol,
+        for tol, group in _by_tol(solving):
+            infos = b.plan.solve([t.slot for t in group], [t.need[1] for t in group],
+                                 [t.need[2] for t in group], [t.need[3] for t in group],
+                                 eps_init=[t.need[4] for t in group], max_iter=self.ls_max_iter, tol=tol,
                                  sync=True, stream=b.stream)
-            for t, info in zip(solving, infos):
+            for t, info in zip(group, infos):
                 t.send = info
         if syncing:
             b.stream.synchronize()
@@ -419,11 +444,10 @@ class Server:
                 if t.need[0] == "solve":
                     solving.append(t)
         b.tasks = alive
-        if solving:
-            reps = [t.slot for t in solving]
-            b.plan.solve(reps, [t.need[1] for t in solving], [t.need[2] for t in solving],
-                         [t.need[3] for t in solving], eps_init=[t.need[4] for t in solving],
-                         max_iter=self.ls_max_iter, tol=self.ls_tol, sync=False, stream=b.stream)
+        for tol, group in _by_tol(solving):  # one launch per tolerance in use
+            b.plan.solve([t.slot for t in group], [t.need[1] for t in group], [t.need[2] for t in group],
+                         [t.need[3] for t in group], eps_init=[t.need[4] for t in group],
+                         max_iter=self.ls_max_iter, tol=tol, sync=False, stream=b.stream)
         b.solving = solving
         b.inflight = list(alive)  # tasks admitted during the round join the next one
         b.event.record(b.stream)
@@ -577,6 +601,7 @@ class Server:
                     if b.inflight is None and b.tasks:
                         self._start_round(b)
                         progressed = True
+                self._report("served")
                 busy = any(b.tasks or b.waiting or b.inflight for b in self.buckets.values())
                 if not pending and not busy and done3d() == n3d:
                     break
@@ -600,6 +625,7 @@ class Server:
             if realtime and r.t_arrival > now:
                 time.sleep(r.t_arrival - now)
             res = self.results[r.rid]
+            self._report("sequential")
             if not realtime:
                 res.t_arrival = self._now()
             res.t_admit = self._now()
@@ -625,7 +651,7 @@ class Server:
                             break
                         if need[0] == "solve":
                             send = b.plan.solve([0], [need[1]], [need[2]], [need[3]],
-                                                eps_init=[need[4]], max_iter=self.ls_max_iter, tol=self.ls_tol,
+                                                eps_init=[need[4]], max_iter=self.ls_max_iter, tol=need[5],
                                                 sync=True, stream=b.stream)[0]
                         else:
                             b.stream.synchronize()

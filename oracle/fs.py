@@ -113,10 +113,25 @@ def project(A):
     return np.fft.ifftn(R, axes=(0, 1, 2)).real
 
 
-def cauchy(P, F):
+def cauchy(P, F, F33=None):
+    """cauchy_from_P_3d (:1892-1904); with F33, the 2D cauchy_from_P's
+    J = det(F) F33 (:1094-1115)."""
     J = det3(F)
+    if F33 is not None:
+        J = J * F33
     J = np.where(np.abs(J) < 1e-14, 1e-14, J)
     return P @ _tr(F) / J[..., None, None]
+
+
+def plane_stress_f33(F, lam, mu, Fpi):
+    """Out-of-plane stretch of the 2D plane-stress SVK law (:1042-1049) on the
+    embedded problem (plane axes x, z): E the in-plane Green-Lagrange strain
+    of Fe = F Fp^-1, E33 = -(lam / (2 mu)) tr E, F33 = sqrt(max(1e-12,
+    1 + 2 E33)); lam is the plane-stress lambda."""
+    Fe = F @ Fpi
+    C = _tr(Fe) @ Fe
+    trE = 0.5 * (C[..., 0, 0] - 1.0) + 0.5 * (C[..., 2, 2] - 1.0)
+    return np.sqrt(np.maximum(1e-12, 1.0 + 2.0 * (-(lam / (2.0 * mu)) * trE)))
 
 
 def build_bc_3d(driving_component, eps, mixed_targets, F_bar_initial=None):
@@ -189,10 +204,12 @@ def newton(F_start, F_bar, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model="svk", kr
 
 def solver_step_3d(F, F_bar, E, nu, Fp, driving_component=(0, 0), P_target=None, P_mask=None, E_avg=None,
                    nu_avg=None, tol_NW=1e-5, tol_CG=1e-6, max_NW=50, tol_macro=1e6, max_iter_macro=20,
-                   model="svk", krylov="bicgstab"):
+                   model="svk", krylov="bicgstab", lame=None, plane_stress=False):
     """finite_strain_solver_step_3d (:2967-3168), Newton branch, spatial-first fields.
-    Returns (F, P, Sig, F_bar_current)."""
-    lam, mu = lame_3d(E, nu)
+    Returns (F, P, Sig, F_bar_current).  ``lame`` = (lam, mu) fields replace
+    the ones from (E, nu); ``plane_stress``: the embedded 2D plane-stress SVK
+    problem (lam the plane-stress lambda), whose Cauchy stress carries F33."""
+    lam, mu = lame_3d(E, nu) if lame is None else lame
     Fpi = np.linalg.inv(Fp) if Fp is not None else np.broadcast_to(np.eye(3), F.shape)
     E_avg = E.mean() if E_avg is None else E_avg
     nu_avg = nu.mean() if nu_avg is None else nu_avg
@@ -210,7 +227,7 @@ def solver_step_3d(F, F_bar, E, nu, Fp, driving_component=(0, 0), P_target=None,
     for it in range(max_iter_macro):
         F_curr, P = newton(F_start, F_bar_cur, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model, krylov,
                            has_fp=Fp is not None)
-        Sig = cauchy(P, F_curr)
+        Sig = cauchy(P, F_curr, plane_stress_f33(F_curr, lam, mu, Fpi) if plane_stress else None)
         Sm = Sig.mean(axis=(0, 1, 2))
         if not np.any(P_mask):
             return F_curr, P, Sig, F_bar_cur

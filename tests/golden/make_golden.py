@@ -527,6 +527,39 @@ def fs2d_sim_fixtures():
     save("fs2d_sim_12x8", E=E, nu=nu, F_macro=Fm, Sig_macro=Sm, P_macro=Pm, F_last=F_l[-1], Sig_last=S_l[-1])
 
 
+def fs2d_pstress_fixtures():
+    """The reference's 2D plane-stress Newton-CG load step
+    (finite_strain_solver_step_2d, plane_mode="plane_stress", :2356-2572;
+    SVK law :1038-1049 with the plane-stress lambda of build_C4_2d and the
+    Cauchy stress with F33, :1094-1115), F_bar prescribed (1.01, 0.997), SVK,
+    without F_p ("nofp") and with F_p of amplitude 0.02 on 15 % of voxels
+    ("fp").  Newton tolerance 1e-7: a tighter one reaches the stalled
+    BiCGSTAB solve (see fs2d_sim_fixtures) and its line search fails."""
+    rng = np.random.default_rng(73)
+    nx, ny = 12, 8
+    E, nu = W.ls2d_material(nx, ny, rng)
+    I2, I4, I4rt, I4s, II = FS._make_identity_tensors_2d(nx, ny)
+    Ghat4 = FS.build_ghat4_2d(nx, ny, float(nx), float(ny))
+    C4 = FS.build_C4_2d(E, nu, I4s, II, plane_mode="plane_stress")
+    Fp = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    sel = rng.random((nx, ny)) < 0.15
+    G = rng.standard_normal((2, 2, nx, ny))
+    S = 0.5 * (G + G.transpose(1, 0, 2, 3))
+    S -= 0.5 * (S[0, 0] + S[1, 1]) * np.eye(2)[:, :, None, None]
+    S /= np.sqrt(np.sum(S * S, axis=(0, 1)))
+    Fp += 0.02 * S * sel
+    F0 = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    Fb = np.diag([1.01, 0.997])
+    out = dict(E=E, nu=nu, Fp=Fp, F_bar=Fb)
+    for tag, fp in (("nofp", None), ("fp", Fp)):
+        F, P, Sig, _, _ = FS.finite_strain_solver_step_2d(
+            F0, Fb, Ghat4, C4, I2, I4, I4rt, Fp=fp, driving_component=(0, 0), E_avg=E.mean(), nu_avg=nu.mean(),
+            tol_NW=1e-7, tol_CG=1e-8, max_NW=30, enable_console=False, model_type="svk", plane_mode="plane_stress",
+            solver="newton_cg")
+        out.update({f"{tag}_F": F, f"{tag}_P": P, f"{tag}_Sig": Sig})
+    save("fs2d_pstress_12x8", **out)
+
+
 def ls3d_landau_fixtures():
     """The reference's 3D Landau law (stress_from_strain_landau_3d) without
     capping, with piecewise and with smooth capping, and its LS solver
@@ -569,7 +602,7 @@ ALL = ("ls2d_fixtures", "ls3d_fixtures", "kmc2d_fixtures", "kmc3d_fixtures", "fs
        "ls2d_rose_fixtures", "kmc2d_cascade_fixtures", "kmc2d_patch_fixtures", "ls3d_secant_fixtures",
        "ls2d_landau_fixtures", "kmc2d_trajectory_fixtures", "driver_fixtures",
        "kmc3d_trajectory_fixtures", "fs2d_step_fixtures",
-       "fs2d_sim_fixtures", "ls3d_landau_fixtures")
+       "fs2d_sim_fixtures", "ls3d_landau_fixtures", "fs2d_pstress_fixtures")
 
 
 if __name__ == "__main__":
