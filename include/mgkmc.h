@@ -126,8 +126,10 @@ MGK_API int mgk_ls2d_set_landau(mgk_ls2d_t plan, const double* v, int capping, d
  * non-finite coefficients takes the plain step and restarts the history
  * from the last pair.  When the iteration cap ends the loop the outputs are
  * those of the last mixed iterate; when it converges, of the image g.  A
- * solve with m > 0 selects one replica.  Allocates a ring of (3 + 2m) strain
- * fields (3 N doubles each) at the first call that needs it. */
+ * solve with m > 0 selects one replica and needs a nonlinear law
+ * (mgk_ls2d_set_secant, _set_rose or _set_landau).  Allocates a ring of
+ * (3 + 2m) strain fields (3 N doubles each) at the first call that needs
+ * it. */
 MGK_API int mgk_ls2d_set_anderson(mgk_ls2d_t plan, int m);
 /* Type-II Anderson mixing (linear_elastic_simulator.py:1185-1209) of
  * fixed-point iterates x -> g = G(x), fields of n doubles, history depth

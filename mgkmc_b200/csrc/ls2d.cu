@@ -62,6 +62,9 @@ namespace mgk {
 
 const void* twiddles(int n, int prec);
 
+constexpr int kAaMax = 8;  // deepest Anderson history
+struct Ls2dAA;
+
 struct Ls2dRep {
   int nx, ny, nyh, ld, tc;
   int row_items, col_items;
@@ -93,6 +96,12 @@ struct Ls2dRep {
   double tol;
   int max_iter;
   int row_first, col_first;  // first work item of this replica in the call's maps
+  // Anderson mixing of this call (null: none): state, the ring's dG slots
+  // and its x (the mix is applied by the first row pass of each iterate and,
+  // when the iteration cap ends the loop, by the output kernel)
+  const Ls2dAA* aa;
+  const double* aa_dG;
+  double* aa_x;
 };
 
 struct Ls2dState {
@@ -118,6 +127,40 @@ struct Ls2dCtl {
   int any;
   int error;              // a bounded wait gave up (MGK_TIMEOUT)
 };
+
+struct Ls2dAA {
+  int k;          // valid difference columns, in slots 0 .. k-1
+  int slot_next;  // ring slot of the next column
+  int have_prev;  // a previous (f, g) pair exists
+  int nmix;       // columns of the current mix (0: the plain step)
+  unsigned int ctr;  // blocks of the update kernel done (self-resetting)
+  int pad;
+  double A[kAaMax][kAaMax];  // Gram matrix <dF_i, dF_j>
+  double gamma[kAaMax];
+};
+
+// The Anderson mix x = g - dG gamma of voxel i's three strain planes (g in
+// e), written to the plan's strain planes and the ring's x.
+__device__ __forceinline__ void aa_mix_voxel(const Ls2dRep& R, long long i, int nmix, const double* gam, double* e) {
+  const long long N = R.N, n3 = 3 * N;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double sm = 0.0;
+#pragma unroll
+    for (int j = 0; j < kAaMax; ++j)
+      if (j < nmix) sm += gam[j] * R.aa_dG[(size_t)j * n3 + c * N + i];
+    e[c] -= sm;
+    R.eps[c * N + i] = e[c];
+    R.aa_x[c * N + i] = e[c];
+  }
+}
+
+__device__ __forceinline__ int aa_load(const Ls2dRep& R, double* gam) {
+  const int nmix = R.aa->nmix;
+#pragma unroll
+  for (int j = 0; j < kAaMax; ++j) gam[j] = j < nmix ? R.aa->gamma[j] : 0.0;
+  return nmix;
+}
 
 constexpr double kMixedPhase1Tol = 2e-6;
 constexpr int kMixedPhase1Cap = 64;
@@ -579,6 +622,10 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
     cur = fft_any<+1>(bufA, bufB, 3, ny, fy);
   }
   C* out = (IN_SPEC && cur == bufA) ? bufB : bufA;
+  double gam[kAaMax];
+  const int nmix = (!IN_SPEC && sizeof(TS) == 8 && R.aa) ? aa_load(R, gam) : 0;
+  // with Anderson mixing the image's tau is never used (see row_fast_body)
+  const bool img_only = IN_SPEC && sizeof(TS) == 8 && law != 0 && R.aa != nullptr;
   for (int y = threadIdx.x; y < ny; y += blockDim.x) {
     TC tr[2][3];
 #pragma unroll
@@ -601,7 +648,9 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
         eps[2 * N + i] = (TS)e[2];
       } else {
         e[0] = o0; e[1] = o1; e[2] = o2;
+        if (!IN_SPEC && sizeof(TS) == 8 && R.aa) aa_mix_voxel(R, i, nmix, gam, e);  // the mixed iterate
       }
+      if (img_only) continue;
       const double dxx = e[0] - p0, dyy = e[1] - p1, dxy = e[2] - p2;
       const double tre = e[0] + e[1];
       double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
@@ -613,19 +662,22 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
       tr[h][1] = (TC)(s1 - (2 * mu0 * e[1] + lam0 * tre));
       tr[h][2] = (TC)(s2 - 2 * mu0 * e[2]);
     }
+    if (img_only) continue;
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c * ny + y] = mk<C>(tr[0][c], tr[1][c]);
   }
-  __syncthreads();
-  C* scratch = (out == bufA) ? bufB : bufA;
-  C* Z = fft_any<-1>(out, scratch, 3, ny, fy);
-  for (int e = threadIdx.x; e < 3 * nyh; e += blockDim.x) {
-    const int c = e / nyh, k = e - c * nyh;
-    const C z = Z[c * ny + k];
-    const C w = Z[c * ny + (k == 0 ? 0 : ny - k)];
-    C* ra = spec + ((size_t)c * nx + x0) * ld;
-    ra[k] = mk<C>(TC(0.5) * (z.x + w.x), TC(0.5) * (z.y - w.y));
-    ra[ld + k] = mk<C>(TC(0.5) * (z.y + w.y), TC(-0.5) * (z.x - w.x));
+  if (!img_only) {
+    __syncthreads();
+    C* scratch = (out == bufA) ? bufB : bufA;
+    C* Z = fft_any<-1>(out, scratch, 3, ny, fy);
+    for (int e = threadIdx.x; e < 3 * nyh; e += blockDim.x) {
+      const int c = e / nyh, k = e - c * nyh;
+      const C z = Z[c * ny + k];
+      const C w = Z[c * ny + (k == 0 ? 0 : ny - k)];
+      C* ra = spec + ((size_t)c * nx + x0) * ld;
+      ra[k] = mk<C>(TC(0.5) * (z.x + w.x), TC(0.5) * (z.y - w.y));
+      ra[ld + k] = mk<C>(TC(0.5) * (z.y + w.y), TC(-0.5) * (z.x - w.x));
+    }
   }
   if (!IN_SPEC) return;
   // partial sums -> fixed slot; the replica's last CTA reduces and decides
@@ -1015,6 +1067,11 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
   const int law = R.law, law_ps = R.law_ps;
   const double law_a = R.law_a, law_b = R.law_b;
   const double eb0 = S.ebar[0], eb1 = S.ebar[1], eb2 = S.ebar[2];
+  double gam[kAaMax];
+  const int nmix = (!IN_SPEC && sizeof(T) == 8 && R.aa) ? aa_load(R, gam) : 0;
+  // with Anderson mixing the image's tau is never used (the next tau is the
+  // mixed iterate's): the pass stops at the image and its update norm
+  const bool img_only = IN_SPEC && LAW != 0 && sizeof(T) == 8 && R.aa != nullptr;
   double d2 = 0, n2 = 0;
   for (int y = threadIdx.x; y < NY; y += NT) {
     T tr[2][3];
@@ -1044,7 +1101,13 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
         eps[2 * N + i] = (T)e2;
       } else {
         e0 = o0; e1 = o1; e2 = o2;
+        if (!IN_SPEC && sizeof(T) == 8 && R.aa) {  // the mixed iterate
+          double e[3] = {o0, o1, o2};
+          aa_mix_voxel(R, i, nmix, gam, e);
+          e0 = e[0]; e1 = e[1]; e2 = e[2];
+        }
       }
+      if (img_only) continue;
       const double dxx = e0 - p0, dyy = e1 - p1, dxy = e2 - p2;
       const double tre = e0 + e1;
       double s0, s1, s2;  // LAW 0 linear; 1 secant, 2 Rose, 3 Landau (FP64 plans)
@@ -1053,16 +1116,19 @@ __device__ __forceinline__ void row_fast_body(const Ls2dRep& R, Ls2dState& S, in
       tr[h][1] = (T)(s1 - (2 * mu0 * e1 + lam0 * tre));
       tr[h][2] = (T)(s2 - 2 * mu0 * e2);
     }
+    if (img_only) continue;
 #pragma unroll
     for (int c = 0; c < 3; ++c) lines[c * PL + py] = mk<C>(tr[0][c], tr[1][c]);
   }
-  __syncthreads();
-  warp_fft<NY, -1, 1, G>(line, PL, tw, lane, bid);
-  for (int k = lane; k < NYH; k += G) {
-    const C zz = line[pidx<C>(k)];
-    const C w = line[pidx<C>(k == 0 ? 0 : NY - k)];
-    ra[k] = mk<C>(T(0.5) * (zz.x + w.x), T(0.5) * (zz.y - w.y));
-    rbp[k] = mk<C>(T(0.5) * (zz.y + w.y), T(-0.5) * (zz.x - w.x));
+  if (!img_only) {
+    __syncthreads();
+    warp_fft<NY, -1, 1, G>(line, PL, tw, lane, bid);
+    for (int k = lane; k < NYH; k += G) {
+      const C zz = line[pidx<C>(k)];
+      const C w = line[pidx<C>(k == 0 ? 0 : NY - k)];
+      ra[k] = mk<C>(T(0.5) * (zz.x + w.x), T(0.5) * (zz.y - w.y));
+      rbp[k] = mk<C>(T(0.5) * (zz.y + w.y), T(-0.5) * (zz.x - w.x));
+    }
   }
   if (!IN_SPEC) return;
   d2 = block_sum(d2, red);
@@ -1257,11 +1323,16 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
   double* sig_out = R.out_sig;
   const int law_ps = R.law_ps;
   const double law_a = R.law_a, law_b = R.law_b;
+  const bool capped_mix = R.aa && S.done == 2 && S.status == MGK_NOT_CONVERGED;
+  double gam[kAaMax];
+  const int nmix = capped_mix ? aa_load(R, gam) : 0;
   double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
        i += (long long)gridDim.x * blockDim.x) {
-    const double sxy = R.eps[2 * N + i];
-    const double exx = R.eps[i], eyy = R.eps[N + i];
+    double ev[3] = {R.eps[i], R.eps[N + i], R.eps[2 * N + i]};
+    if (capped_mix) aa_mix_voxel(R, i, nmix, gam, ev);  // the loop ended at the cap: the last mixed iterate
+    const double sxy = ev[2];
+    const double exx = ev[0], eyy = ev[1];
     const double exy = abar == 0 ? sxy : sxy + abar;
     const double eyx = abar == 0 ? sxy : sxy - abar;
     double pxx = R.ep[i], pyy = R.ep[N + i], pxy, pyx;
@@ -1302,7 +1373,6 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
 // forms f = g - x, writes column `slot` (dF = f - f_prev, dG = g - g_prev)
 // when a previous pair exists, stores f and g as the previous pair, and
 // accumulates <dF_j, dF_slot> and <dF_j, f> for the ncols valid columns.
-constexpr int kAaMax = 8;
 constexpr int kAaBlocks = 296;
 
 __global__ void __launch_bounds__(256) aa_update_kernel(long long n, const double* __restrict__ x,
@@ -1388,14 +1458,6 @@ __global__ void aa_mix_kernel(long long n, const double* __restrict__ g, const d
 // by 2, as the reference's sums over the four tensor entries do.  The
 // differences sit in a ring of m slots; the least-squares solution does not
 // depend on the order of the columns.
-struct Ls2dAA {
-  int k;          // valid difference columns, in slots 0 .. k-1
-  int slot_next;  // ring slot of the next column
-  int have_prev;  // a previous (f, g) pair exists
-  int nmix;       // columns of the current mix (0: the plain step)
-  double A[kAaMax][kAaMax];  // Gram matrix <dF_i, dF_j>
-  double gamma[kAaMax];
-};
 
 // Mixing follows every iteration except the converged or non-finite one:
 // the reference leaves its loop with the image g there, and with the last
@@ -1416,17 +1478,171 @@ __global__ void ls2d_aa_init_kernel(const Ls2dRep* reps, const int* sel, double*
     aa->slot_next = 0;
     aa->have_prev = 0;
     aa->nmix = 0;
+    aa->ctr = 0;
   }
+}
+
+// Sum over the warp, the same value in every lane (reduced to lane 0, then
+// broadcast: a butterfly would round differently per lane).
+__device__ __forceinline__ double warp_allsum(double v) {
+  return __shfl_sync(0xffffffffu, warp_sum(v), 0);
+}
+
+// Least squares of the mix, one warp (lanes = matrix rows): gamma = sum
+// over eigenpairs (lambda_i, v_i) of the k x k Gram matrix with lambda_i
+// above 1e-14 lambda_max of (v_i . b / lambda_i) v_i, the minimum-norm
+// solution with the small singular values of dF cut off.  Eigenpairs by
+// cyclic Jacobi rotations (Golub & Van Loan, Matrix Computations, 8.5), each
+// rotation's row and column updates spread over the lanes.  sa, sv: k x k
+// shared scratch; b in sb.  Writes gamma and nmix (0 for the plain step,
+// and the history restarts from the last pair when the coefficients are
+// not finite).
+// Fast path of the same least squares (one thread): when the Gram matrix
+// is comfortably conditioned no eigenvalue falls under the cut-off, so the
+// truncated eigen solution is A^-1 b, solved here by Cholesky.  The test:
+// lambda_min >= 1 / tr(A^-1) = 1 / ||L^-1||_F^2 and lambda_max <= tr(A);
+// when 1 / ||L^-1||_F^2 > 1e-12 tr(A) every eigenvalue is above
+// 1e-14 lambda_max with margin for the rounding of the estimate.  Returns
+// false (nothing written) when the factorisation fails or the test does not
+// hold: the eigen path decides then.
+__device__ bool aa_lstsq_cholesky(Ls2dAA* aa, int k, const double* sb) {
+  double Lm[kAaMax][kAaMax];
+  double tr = 0.0;
+  for (int i = 0; i < k; ++i) tr += aa->A[i][i];
+  for (int j = 0; j < k; ++j) {
+    double d = aa->A[j][j];
+    for (int q = 0; q < j; ++q) d -= Lm[j][q] * Lm[j][q];
+    if (!(d > 0.0)) return false;
+    const double ljj = sqrt(d);
+    Lm[j][j] = ljj;
+    for (int i = j + 1; i < k; ++i) {
+      double v = aa->A[i][j];
+      for (int q = 0; q < j; ++q) v -= Lm[i][q] * Lm[j][q];
+      Lm[i][j] = v / ljj;
+    }
+  }
+  // ||L^-1||_F^2, column by column of L^-1 (forward substitution on e_c)
+  double fro = 0.0;
+  for (int c = 0; c < k; ++c) {
+    double z[kAaMax];
+    for (int i = 0; i < k; ++i) {
+      double v = i == c ? 1.0 : 0.0;
+      for (int q = c; q < i; ++q) v -= Lm[i][q] * z[q];
+      z[i] = i < c ? 0.0 : v / Lm[i][i];
+      if (i >= c) fro += z[i] * z[i];
+    }
+  }
+  if (!(isfinite(fro) && 1.0 / fro > 1e-12 * tr)) return false;
+  double y[kAaMax], g[kAaMax];
+  for (int i = 0; i < k; ++i) {
+    double v = sb[i];
+    for (int q = 0; q < i; ++q) v -= Lm[i][q] * y[q];
+    y[i] = v / Lm[i][i];
+  }
+  for (int i = k - 1; i >= 0; --i) {
+    double v = y[i];
+    for (int q = i + 1; q < k; ++q) v -= Lm[q][i] * g[q];
+    g[i] = v / Lm[i][i];
+  }
+  for (int i = 0; i < k; ++i)
+    if (!isfinite(g[i])) return false;
+  for (int i = 0; i < k; ++i) aa->gamma[i] = g[i];
+  aa->nmix = k;
+  return true;
+}
+
+__device__ void aa_lstsq_warp(Ls2dAA* aa, int k, double (*sa)[kAaMax], double (*sv)[kAaMax], const double* sb) {
+  const int l = threadIdx.x;  // lane, < 32
+  for (int e = l; e < k * k; e += 32) {
+    const int i = e / k, j = e - (e / k) * k;
+    sa[i][j] = aa->A[i][j];
+    sv[i][j] = i == j ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  double fro = 0.0;
+  for (int e = l; e < k * k; e += 32) {
+    const int i = e / k, j = e - (e / k) * k;
+    fro += sa[i][j] * sa[i][j];
+  }
+  fro = warp_allsum(fro);
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0;
+    for (int e = l; e < k * k; e += 32) {
+      const int i = e / k, j = e - (e / k) * k;
+      if (j > i) off += sa[i][j] * sa[i][j];
+    }
+    off = warp_allsum(off);
+    if (!(off > 1e-30 * fro)) break;  // also leaves on NaN (uniform: every lane has the same sums)
+    for (int p = 0; p < k; ++p)
+      for (int q = p + 1; q < k; ++q) {
+        const double apq = sa[p][q], app = sa[p][p], aqq = sa[q][q];
+        __syncwarp();
+        if (fabs(apq) <= 1e-18 * sqrt(fabs(app * aqq))) {  // negligible: no rotation
+          if (l == 0) { sa[p][q] = 0.0; sa[q][p] = 0.0; }
+          __syncwarp();
+          continue;
+        }
+        const double th = (aqq - app) / (2.0 * apq);
+        const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+        double x0 = 0.0, x1 = 0.0;
+        if (l < k) { x0 = sa[l][p]; x1 = sa[l][q]; }
+        __syncwarp();
+        if (l < k) { sa[l][p] = c * x0 - sn * x1; sa[l][q] = sn * x0 + c * x1; }
+        __syncwarp();
+        if (l < k) { x0 = sa[p][l]; x1 = sa[q][l]; }
+        __syncwarp();
+        if (l < k) {
+          sa[p][l] = c * x0 - sn * x1;
+          sa[q][l] = sn * x0 + c * x1;
+          const double v0 = sv[l][p], v1 = sv[l][q];
+          sv[l][p] = c * v0 - sn * v1;
+          sv[l][q] = sn * v0 + c * v1;
+        }
+        __syncwarp();
+      }
+  }
+  double lmax = 0.0;
+  for (int i = 0; i < k; ++i) lmax = fmax(lmax, sa[i][i]);
+  // gamma_j (lane j) = sum_i [lambda_i kept] v_ji (v_i . b) / lambda_i
+  double g = 0.0;
+  bool ok = isfinite(lmax);
+  if (ok && lmax > 0.0 && l < k) {
+    for (int i = 0; i < k; ++i) {
+      const double li = sa[i][i];
+      if (!(li > 1e-14 * lmax)) continue;
+      double vb = 0.0;
+      for (int j = 0; j < k; ++j) vb += sv[j][i] * sb[j];
+      g += sv[l][i] * (vb / li);
+    }
+  }
+  ok = __all_sync(0xffffffffu, ok && (l >= k || isfinite(g)));
+  if (!ok) {  // the plain step; the history restarts from the last pair
+    if (l == 0) {
+      aa->k = 0;
+      aa->slot_next = 0;
+      aa->nmix = 0;
+    }
+    return;
+  }
+  if (l < k) aa->gamma[l] = g;
+  if (l == 0) aa->nmix = k;
 }
 
 // f = g - x; with a previous pair, the new column dF = f - f_prev and
 // dG = g - g_prev goes to slot slot_next; (f, g) become the previous pair.
 // Per-block partial sums of <dF_j, dF_new> and <dF_j, f> over the columns
-// valid after this update.
-__global__ void __launch_bounds__(256) ls2d_aa_update_kernel(const Ls2dRep* reps, const Ls2dState* st,
-                                                             const int* sel, double* buf, const Ls2dAA* aa, int m,
-                                                             double* part) {
-  __shared__ double red[32];
+// valid after this update; the last block to finish sums them, updates the
+// Gram matrix and solves the least-squares problem of the mix.
+constexpr int kAaThreads = 256, kAaWarps = kAaThreads / 32;
+__global__ void __launch_bounds__(kAaThreads) ls2d_aa_update_kernel(const Ls2dRep* reps, const Ls2dState* st,
+                                                                    const int* sel, double* buf, Ls2dAA* aa, int m,
+                                                                    double* part) {
+  __shared__ double wred[kAaWarps][2 * kAaMax];
+  __shared__ double lred[kAaThreads / (2 * kAaMax)][2 * kAaMax];
+  __shared__ double sums[2 * kAaMax];
+  __shared__ double sa[kAaMax][kAaMax], sv[kAaMax][kAaMax];
+  __shared__ int s_last;
   const int r = sel[0];
   const Ls2dRep& R = reps[r];
   if (aa_skip(st[r])) return;
@@ -1461,138 +1677,68 @@ __global__ void __launch_bounds__(256) ls2d_aa_update_kernel(const Ls2dRep* reps
         ar[j] += c * fi;
       }
   }
-  for (int j = 0; j < ncols; ++j) {
-    const double a = block_sum(an[j], red);
-    const double b = block_sum(ar[j], red);
-    if (threadIdx.x == 0) {
-      part[(size_t)blockIdx.x * 2 * kAaMax + j] = a;
-      part[(size_t)blockIdx.x * 2 * kAaMax + kAaMax + j] = b;
+  // block partials in a fixed order: warp trees, then the warps in order
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kAaMax; ++j)
+    if (j < ncols) {
+      const double a = warp_sum(an[j]), b = warp_sum(ar[j]);
+      if (lane == 0) { wred[wid][j] = a; wred[wid][kAaMax + j] = b; }
     }
+  __syncthreads();
+  constexpr int Q = 2 * kAaMax;
+  if (threadIdx.x < Q && threadIdx.x % kAaMax < ncols) {
+    double t = 0.0;
+    for (int w = 0; w < kAaWarps; ++w) t += wred[w][threadIdx.x];
+    part[(size_t)blockIdx.x * Q + threadIdx.x] = t;
+    __threadfence();
   }
-}
-
-// Sums the partials, updates the Gram matrix and solves the k x k
-// least-squares problem through the eigen-decomposition of the Gram matrix
-// (cyclic Jacobi rotations, Golub & Van Loan, Matrix Computations, 8.5):
-// gamma = sum over eigenpairs (lambda_i, v_i) with lambda_i above
-// 1e-14 lambda_max of (v_i . b / lambda_i) v_i, the minimum-norm solution
-// with small singular values of dF cut off.  One block.
-__global__ void __launch_bounds__(256) ls2d_aa_solve_kernel(const Ls2dState* st, const int* sel, Ls2dAA* aa,
-                                                            int m, const double* part, int nb) {
-  __shared__ double red[32];
-  __shared__ double sums[2 * kAaMax];
-  if (aa_skip(st[sel[0]])) return;
-  const int have_prev = aa->have_prev;
-  const int ncols = have_prev ? min(aa->k + 1, m) : aa->k;
-  for (int q = 0; q < 2 * kAaMax; ++q) {
-    if (q % kAaMax >= ncols) continue;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int t = atomicInc(&aa->ctr, gridDim.x - 1);  // self-resetting
+    s_last = t == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // the last block: sums over the blocks (value q = thread % Q, blocks in
+  // strides of the thread's group, then the groups in order)
+  const int nb = gridDim.x;
+  {
+    const int q = threadIdx.x % Q, g0 = threadIdx.x / Q;
     double a = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) a += part[(size_t)b * 2 * kAaMax + q];
-    a = block_sum(a, red);
-    if (threadIdx.x == 0) sums[q] = a;
+    if (q % kAaMax < ncols)
+      for (int b = g0; b < nb; b += kAaThreads / Q) a += __ldcg(&part[(size_t)b * Q + q]);
+    lred[g0][q] = a;
   }
-  if (threadIdx.x != 0) return;
-  if (have_prev) {
-    const int slot = aa->slot_next;
-    for (int j = 0; j < ncols; ++j) {
-      aa->A[slot][j] = sums[j];
-      aa->A[j][slot] = sums[j];
-    }
-    aa->k = ncols;
-    aa->slot_next = (slot + 1) % m;
+  __syncthreads();
+  if (threadIdx.x < Q) {
+    double t = 0.0;
+    for (int g = 0; g < kAaThreads / Q; ++g) t += lred[g][threadIdx.x];
+    sums[threadIdx.x] = t;
   }
-  aa->have_prev = 1;
-  const int k = aa->k;
-  aa->nmix = 0;
-  if (k == 0) return;
-  double a[kAaMax][kAaMax], v[kAaMax][kAaMax];
-  double fro = 0.0;
-  for (int i = 0; i < k; ++i)
-    for (int j = 0; j < k; ++j) {
-      a[i][j] = aa->A[i][j];
-      v[i][j] = i == j ? 1.0 : 0.0;
-      fro += a[i][j] * a[i][j];
-    }
-  for (int sweep = 0; sweep < 40; ++sweep) {
-    double off = 0.0;
-    for (int i = 0; i < k; ++i)
-      for (int j = i + 1; j < k; ++j) off += a[i][j] * a[i][j];
-    if (!(off > 1e-30 * fro)) break;  // also leaves on NaN
-    for (int p = 0; p < k; ++p)
-      for (int q = p + 1; q < k; ++q) {
-        const double apq = a[p][q];
-        if (fabs(apq) <= 1e-18 * sqrt(fabs(a[p][p] * a[q][q]))) {  // negligible: no rotation
-          a[p][q] = 0.0;
-          a[q][p] = 0.0;
-          continue;
-        }
-        const double th = (a[q][q] - a[p][p]) / (2.0 * apq);
-        const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-        for (int i = 0; i < k; ++i) {
-          const double aip = a[i][p], aiq = a[i][q];
-          a[i][p] = c * aip - s * aiq;
-          a[i][q] = s * aip + c * aiq;
-        }
-        for (int i = 0; i < k; ++i) {
-          const double api = a[p][i], aqi = a[q][i];
-          a[p][i] = c * api - s * aqi;
-          a[q][i] = s * api + c * aqi;
-          const double vip = v[i][p], viq = v[i][q];
-          v[i][p] = c * vip - s * viq;
-          v[i][q] = s * vip + c * viq;
-        }
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  if (threadIdx.x == 0) {
+    if (have_prev) {
+      for (int j = 0; j < ncols; ++j) {
+        aa->A[slot][j] = sums[j];
+        aa->A[j][slot] = sums[j];
       }
-  }
-  double lmax = 0.0;
-  for (int i = 0; i < k; ++i) lmax = fmax(lmax, a[i][i]);
-  double g[kAaMax];
-  bool ok = isfinite(lmax);
-  for (int j = 0; j < k; ++j) g[j] = 0.0;
-  if (ok && lmax > 0.0) {
-    for (int i = 0; i < k; ++i) {
-      const double li = a[i][i];
-      if (!(li > 1e-14 * lmax)) continue;
-      double vb = 0.0;
-      for (int j = 0; j < k; ++j) vb += v[j][i] * sums[kAaMax + j];
-      const double cf = vb / li;
-      for (int j = 0; j < k; ++j) g[j] += cf * v[j][i];
+      aa->k = ncols;
+      aa->slot_next = (slot + 1) % m;
     }
+    aa->have_prev = 1;
+    aa->nmix = 0;
   }
-  for (int j = 0; j < k; ++j) ok = ok && isfinite(g[j]);
-  if (!ok) {  // the plain step; the history restarts from the last pair
-    aa->k = 0;
-    aa->slot_next = 0;
-    return;
-  }
-  for (int j = 0; j < k; ++j) aa->gamma[j] = g[j];
-  aa->nmix = k;
+  __syncwarp();
+  if (ncols == 0) return;
+  int fast = 0;
+  if (threadIdx.x == 0) fast = aa_lstsq_cholesky(aa, ncols, sums + kAaMax) ? 1 : 0;
+  if (__shfl_sync(0xffffffffu, fast, 0)) return;
+  aa_lstsq_warp(aa, ncols, sa, sv, sums + kAaMax);
 }
 
-// x = g - dG gamma (x = g for the plain step), into the plan's strain planes
-// (the next tau) and the ring's x.
-__global__ void __launch_bounds__(256) ls2d_aa_mix_kernel(const Ls2dRep* reps, const Ls2dState* st, const int* sel,
-                                                          double* buf, const Ls2dAA* aa, int m) {
-  const int r = sel[0];
-  const Ls2dRep& R = reps[r];
-  if (aa_skip(st[r])) return;
-  const long long n3 = 3 * R.N;
-  const int nmix = aa->nmix;
-  double gam[kAaMax];
-#pragma unroll
-  for (int j = 0; j < kAaMax; ++j) gam[j] = j < nmix ? aa->gamma[j] : 0.0;
-  double* x = buf;
-  const double* dG = buf + (3 + (size_t)m) * n3;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
-    double s = 0.0;
-#pragma unroll
-    for (int j = 0; j < kAaMax; ++j)
-      if (j < nmix) s += gam[j] * dG[(size_t)j * n3 + i];
-    const double xv = R.eps[i] - s;
-    R.eps[i] = xv;
-    x[i] = xv;
-  }
-}
 
 }  // namespace mgk
 
@@ -2104,7 +2250,7 @@ extern "C" int mgk_ls2d_set_anderson(mgk_ls2d_t p, int m) {
     if (!p->d_aa) {
       int dev = 0, sms = 148;
       if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      p->aa_nb = std::max(1, std::min(2 * sms, ceil_div(3 * p->maxN, kThreads)));
+      p->aa_nb = std::max(1, std::min(8 * sms, ceil_div(3 * p->maxN, kAaThreads)));
       if (cudaMalloc((void**)&p->d_aa, sizeof(Ls2dAA)) != cudaSuccess ||
           cudaMalloc((void**)&p->aa_part, sizeof(double) * 2 * kAaMax * p->aa_nb) != cudaSuccess) {
         cudaGetLastError();
@@ -2194,10 +2340,8 @@ static int launch_body(const LoopArgs& a, cudaStream_t s) {
     launch_row<TS, true, FINAL>(a, s);
   MGK_CUDA(cudaGetLastError());
   if (sizeof(TS) == 8 && a.aa_m > 0) {
-    ls2d_aa_update_kernel<<<a.aa_nb, kThreads, 0, s>>>(a.reps, a.st, a.sel, a.aa_buf, a.aa, a.aa_m, a.aa_part);
-    ls2d_aa_solve_kernel<<<1, kThreads, 0, s>>>(a.st, a.sel, a.aa, a.aa_m, a.aa_part, a.aa_nb);
-    ls2d_aa_mix_kernel<<<a.aa_nb, kThreads, 0, s>>>(a.reps, a.st, a.sel, a.aa_buf, a.aa, a.aa_m);
-    launch_row<TS, false, FINAL>(a, s);  // tau of the mixed iterate
+    ls2d_aa_update_kernel<<<a.aa_nb, kAaThreads, 0, s>>>(a.reps, a.st, a.sel, a.aa_buf, a.aa, a.aa_m, a.aa_part);
+    launch_row<TS, false, FINAL>(a, s);  // the mix and tau of the mixed iterate
     MGK_CUDA(cudaGetLastError());
   }
   return MGK_OK;
@@ -2249,31 +2393,18 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
   }
   MGK_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &k2));
   if (sizeof(TS) == 8 && a.aa_m > 0) {
-    // Anderson mixing of the image, then tau of the mixed iterate
-    cudaGraphNode_t n3, n4, n5, n6;
-    cudaKernelNodeParams k3, k4, k5, k6;
+    // Anderson history and least squares, then the mix and tau of the mixed
+    // iterate in the first row pass
+    cudaGraphNode_t n3, n6;
+    cudaKernelNodeParams k3, k6;
     memset(&k3, 0, sizeof(k3));
-    memset(&k4, 0, sizeof(k4));
-    memset(&k5, 0, sizeof(k5));
     memset(&k6, 0, sizeof(k6));
     void* a3[] = {&a.reps, &a.st, &a.sel, &a.aa_buf, &a.aa, &a.aa_m, &a.aa_part};
     k3.func = (void*)ls2d_aa_update_kernel;
     k3.gridDim = dim3(a.aa_nb);
-    k3.blockDim = dim3(kThreads);
+    k3.blockDim = dim3(kAaThreads);
     k3.kernelParams = a3;
     MGK_CUDA(cudaGraphAddKernelNode(&n3, body, &n2, 1, &k3));
-    void* a4[] = {&a.st, &a.sel, &a.aa, &a.aa_m, &a.aa_part, &a.aa_nb};
-    k4.func = (void*)ls2d_aa_solve_kernel;
-    k4.gridDim = dim3(1);
-    k4.blockDim = dim3(kThreads);
-    k4.kernelParams = a4;
-    MGK_CUDA(cudaGraphAddKernelNode(&n4, body, &n3, 1, &k4));
-    void* a5[] = {&a.reps, &a.st, &a.sel, &a.aa_buf, &a.aa, &a.aa_m};
-    k5.func = (void*)ls2d_aa_mix_kernel;
-    k5.gridDim = dim3(a.aa_nb);
-    k5.blockDim = dim3(kThreads);
-    k5.kernelParams = a5;
-    MGK_CUDA(cudaGraphAddKernelNode(&n5, body, &n4, 1, &k5));
     cudaGraphConditionalHandle h0 = 0;
     int zero = 0;
     void* a6[] = {&a.reps, &a.st, &a.row_map, &a.row_local, &a.part, &a.repctr, &a.ctl, &h0, &zero, &zero};
@@ -2282,7 +2413,7 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
     k6.blockDim = dim3(a.fast ? row_threads(a.fast) : kThreads);
     k6.sharedMemBytes = (unsigned)a.row_smem;
     k6.kernelParams = a6;
-    MGK_CUDA(cudaGraphAddKernelNode(&n6, body, &n5, 1, &k6));
+    MGK_CUDA(cudaGraphAddKernelNode(&n6, body, &n3, 1, &k6));
   }
   return MGK_OK;
 }
@@ -2481,6 +2612,7 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
   MGK_REQUIRE(p && eps_bar && nsel >= 1 && nsel <= p->nrep, "mgk_ls2d_solve_batch: bad argument");
   MGK_REQUIRE(max_iter >= 0 && max_iter <= 1000000, "mgk_ls2d_solve: max_iter out of range");
   MGK_REQUIRE(p->aa_m == 0 || nsel == 1, "mgk_ls2d_solve_batch: Anderson mixing solves one replica per call");
+  MGK_REQUIRE(p->aa_m == 0 || p->law != 0, "mgk_ls2d_solve_batch: Anderson mixing runs with a nonlinear law");
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<int> selv(nsel);
   std::vector<char> seen(p->nrep, 0);
@@ -2518,6 +2650,9 @@ extern "C" int mgk_ls2d_solve_batch(mgk_ls2d_t p, int nsel, const int* sel, cons
     for (int k = 0; k < 4; ++k) H.eb[k] = eps_bar[4 * q + k];
     H.tol = tol;
     H.max_iter = max_iter;
+    H.aa = p->aa_m > 0 ? p->d_aa : nullptr;
+    H.aa_x = p->aa_m > 0 ? p->aa_buf : nullptr;
+    H.aa_dG = p->aa_m > 0 ? p->aa_buf + (size_t)(3 + p->aa_m) * 3 * (size_t)H.N : nullptr;
     H.row_first = ri;
     H.col_first = ci;
     for (int i = 0; i < H.row_items; ++i) { row_map[ri] = r; row_local[ri] = i; ++ri; }
