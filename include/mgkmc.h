@@ -341,15 +341,17 @@ MGK_API int mgk_fs3d_get(mgk_fs3d_t plan, double* F_out, double* P_out, double* 
  * the Newton test use the 2D field's norm (||F|| without the N unit F_yy
  * entries, :2521).  No counterpart in the reference as an entry point. */
 MGK_API int mgk_fs3d_set_plane_strain(mgk_fs3d_t plan, int on);
-/* 2D plane-stress finite strain, SVK model (finite_strain_simulator.py:
- * 1042-1049 and cauchy_from_P :1094-1115 with F33) on an (nx, 1, ny) plan:
- * the plane-strain embedding and Newton norm of mgk_fs3d_set_plane_strain,
- * the material's lam being the plane-stress lambda E nu / (1 - nu^2) of
- * build_C4_2d (:233-259), so the in-plane SVK stress and tangent are the
- * reference's; the Cauchy stress divides by J = det(F) F33 with
- * F33 = sqrt(max(1e-12, 1 - (lam / mu) tr E)), E the in-plane Green-Lagrange
- * strain of F Fp^-1.  The Neo-Hookean plane-stress law (an out-of-plane
- * Newton solve per voxel) is not built: refused for model 1. */
+/* 2D plane-stress finite strain (finite_strain_simulator.py:631-684
+ * Neo-Hookean, :1038-1049 SVK, cauchy_from_P :1094-1115 with F33) on an
+ * (nx, 1, ny) plan: the plane-strain embedding and Newton norm of
+ * mgk_fs3d_set_plane_strain, the material's lam being the plane-stress
+ * lambda E nu / (1 - nu^2) of build_C4_2d (:233-259).  SVK: the in-plane
+ * stress and tangent are the reference's, F33 = sqrt(max(1e-12,
+ * 1 - (lam / mu) tr E)), E the in-plane Green-Lagrange strain of F Fp^-1.
+ * Neo-Hookean: per voxel x = F33^2 from the reference's Newton solve of
+ * mu x + lam_3d/2 ln x = mu - lam_3d ln Je, S = mu I - mu x C^-1 and the
+ * condensed tangent (lam*, mu x).  The Cauchy stress divides by
+ * J = det(F) F33. */
 MGK_API int mgk_fs3d_set_plane_stress(mgk_fs3d_t plan, int on);
 /* Autotuner: times one Krylov iteration of each kernel family that can serve
  * the plan (warp-line passes, sides 64/96/128; CTA-wide passes) on the current

@@ -50,7 +50,7 @@ struct FsArgs {
   int nx, ny, nz, nzh, ld, tc;
   long long N;
   int has_fp, model;  // model 0 SVK, 1 Neo-Hookean
-  int plane_stress;   // (nx, 1, ny) plan of a 2D plane-stress SVK solve: Cauchy J carries F33
+  int plane_stress;   // (nx, 1, ny) plan of a 2D plane-stress solve (lam the plane-stress lambda)
   FftLen fx, fy, fz;
   const double* F;
   const double* Fpi;
@@ -162,6 +162,7 @@ template <typename T>
 struct VoxelLaw {
   T Fe[9], Fpi[9], Sref[9], S[9], Ci[9];
   T lam, mu, c, Je;
+  T f33;  // out-of-plane stretch of a plane-stress plan (1 otherwise)
   int model, has_fp;
 
   __device__ void init(const FsArgs& a, long long i, const T* F, T alpha, const T* dX) {
@@ -181,11 +182,37 @@ struct VoxelLaw {
     T C[9];
     mtm(Fe, Fe, C);
     Je = det3(Fe);
+    f33 = T(1);
     if (model == 0) {
       T Eg[9];
       for (int q = 0; q < 9; ++q) Eg[q] = T(0.5) * (C[q] - ((q % 4 == 0) ? T(1) : T(0)));
       const T tr = Eg[0] + Eg[4] + Eg[8];
       for (int q = 0; q < 9; ++q) S[q] = 2 * mu * Eg[q] + ((q % 4 == 0) ? lam * tr : T(0));
+      if (a.plane_stress) {
+        // :1042-1049: E33 = -(lam / (2 mu)) tr E of the in-plane strain (x, z)
+        const T e33 = -(lam / (T(2) * mu)) * (Eg[0] + Eg[8]);
+        f33 = sqrt(fmax(T(1e-12), T(1) + T(2) * e33));
+      }
+    } else if (a.plane_stress) {
+      // plane-stress Neo-Hookean (:631-684): lam is the plane-stress lambda,
+      // lam_3d = 2 mu lam / (2 mu - lam); x = F33^2 from the Newton solve of
+      // mu x + lam_3d/2 ln x = mu - lam_3d ln Je (Je of the in-plane Fe, at
+      // most 10 steps, until the step is below 1e-12); S = mu I - mu x C^-1;
+      // the tangent's lam* = 2 lam_3d mu x / (lam_3d + 2 mu x), c = mu x
+      const T lam3 = (T(2) * mu * lam) / fmax(T(1e-14), T(2) * mu - lam);
+      const T target = mu - lam3 * log(fmax(T(1e-14), Je));
+      T x = T(1);
+      for (int it = 0; it < 10; ++it) {
+        const T fx = mu * x + T(0.5) * lam3 * log(x) - target;
+        const T dx = -fx / (mu + T(0.5) * lam3 / x);
+        x = fmax(T(1e-10), x + dx);
+        if (fabs(dx) < T(1e-12)) break;
+      }
+      f33 = sqrt(fmax(T(1e-12), x));
+      inv3(C, Ci);
+      c = mu * x;
+      for (int q = 0; q < 9; ++q) S[q] = -c * Ci[q] + ((q % 4 == 0) ? mu : T(0));
+      lam = (T(2) * lam3 * c) / fmax(T(1e-14), lam3 + T(2) * c);
     } else {
       const T lnJ = log(fmax(T(1e-14), Je));
       inv3(C, Ci);
@@ -591,28 +618,6 @@ __global__ void fs_scalar_kernel(FsArgs a, int nb, cudaGraphConditionalHandle co
   }
 }
 
-// Out-of-plane stretch of a plane-stress SVK voxel on the (nx, 1, ny) plan
-// (finite_strain_simulator.py:1042-1049): with the in-plane Green-Lagrange
-// strain of Fe = F Fp^-1 (plane axes x and z), E33 = -(lam / (2 mu)) tr E,
-// F33 = sqrt(max(1e-12, 1 + 2 E33)); lam is the plane-stress lambda the
-// caller gives as the material.  1 for every other plan.
-__device__ __forceinline__ double fs_f33(const FsArgs& a, long long i, const double* Fv) {
-  if (!a.plane_stress) return 1.0;
-  double Fe[9];
-  if (a.has_fp) {
-    double Fpi[9];
-    for (int q = 0; q < 9; ++q) Fpi[q] = a.Fpi[q * a.N + i];
-    mm(Fv, Fpi, Fe);
-  } else {
-    for (int q = 0; q < 9; ++q) Fe[q] = Fv[q];
-  }
-  const double cxx = Fe[0] * Fe[0] + Fe[3] * Fe[3] + Fe[6] * Fe[6];
-  const double czz = Fe[2] * Fe[2] + Fe[5] * Fe[5] + Fe[8] * Fe[8];
-  const double trE = 0.5 * (cxx - 1.0) + 0.5 * (czz - 1.0);
-  const double e33 = -(a.lam[i] / (2.0 * a.mu[i])) * trE;
-  return sqrt(fmax(1e-12, 1.0 + 2.0 * e33));
-}
-
 // Constitutive evaluation at F + alpha (x + dbar) (or at F when dx is 0):
 // writes Fout, Pout; per-CTA partials: min Je, NaN count, sum F^2, sum x^2,
 // and the Cauchy stress sums (cauchy_from_P_3d).  16 values per CTA.
@@ -637,7 +642,7 @@ __global__ void fs_constitutive_kernel(FsArgs a, double alpha, const double* __r
     if (!(law.Je == law.Je)) nan += 1;
     mnJ = fmin(mnJ, law.Je);
     double J = det3(Ft);
-    if (a.plane_stress) J *= fs_f33(a, i, Ft);
+    if (a.plane_stress) J *= law.f33;
     if (fabs(J) < 1e-14) J = 1e-14;
     double PF[9];
     mmt(P, Ft, PF);
@@ -726,7 +731,11 @@ __global__ void fs_cauchy_kernel(FsArgs a, double* sig) {
     double Pv[9], Fv[9], PF[9];
     for (int q = 0; q < 9; ++q) { Pv[q] = a.P[q * N + i]; Fv[q] = a.F[q * N + i]; }
     double J = det3(Fv);
-    if (a.plane_stress) J *= fs_f33(a, i, Fv);
+    if (a.plane_stress) {
+      VoxelLaw<double> law;
+      law.init(a, i, Fv, 0.0, nullptr);
+      J *= law.f33;
+    }
     if (fabs(J) < 1e-14) J = 1e-14;
     mmt(Pv, Fv, PF);
     for (int q = 0; q < 9; ++q) sig[q * N + i] = PF[q] / J;
@@ -1114,7 +1123,7 @@ struct mgk_fs3d_plan {
   // plane strain embedded as (nx, 1, ny): the out-of-plane F_yy = 1 adds N
   // to ||F||^2, which the 2D solver's Newton norm does not contain
   double ff_offset = 0.0;
-  int plane_stress = 0;  // 2D plane-stress SVK on the (nx, 1, ny) plan
+  int plane_stress = 0;  // 2D plane stress on the (nx, 1, ny) plan
 };
 
 static FsArgs fs_args(mgk_fs3d_t p) {
@@ -1669,8 +1678,7 @@ extern "C" int mgk_fs3d_set_plane_strain(mgk_fs3d_t p, int on) {
 }
 
 extern "C" int mgk_fs3d_set_plane_stress(mgk_fs3d_t p, int on) {
-  MGK_REQUIRE(p && (!on || (p->ny == 1 && p->model == 0)),
-              "mgk_fs3d_set_plane_stress: the plan must be (nx, 1, ny) with the SVK model");
+  MGK_REQUIRE(p && (!on || p->ny == 1), "mgk_fs3d_set_plane_stress: the plan must be (nx, 1, ny)");
   p->plane_stress = on ? 1 : 0;
   p->ff_offset = on ? (double)p->N : 0.0;
   return MGK_OK;

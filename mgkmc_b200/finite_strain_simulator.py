@@ -356,18 +356,16 @@ def _embed_small(M2, fill, dtype=np.float64):
 class Fs2dSolver:
     """2D finite-strain solver: the 3D plan of an (nx, 1, ny) grid with the
     out-of-plane axis y (F_yy = 1) and the 2D Newton norm.  plane_mode
-    "plane_strain" (``mgk_fs3d_set_plane_strain``) or, for the SVK model,
-    "plane_stress" (``mgk_fs3d_set_plane_stress``: the material's lam is the
-    plane-stress lambda E nu / (1 - nu^2), and the Cauchy stress carries the
-    out-of-plane stretch F33).  Fields in and out are the reference's
-    tensor-first (2, 2, nx, ny)."""
+    "plane_strain" (``mgk_fs3d_set_plane_strain``) or "plane_stress"
+    (``mgk_fs3d_set_plane_stress``: the material's lam is the plane-stress
+    lambda E nu / (1 - nu^2); the laws are the reference's plane-stress ones,
+    the Neo-Hookean with its per-voxel out-of-plane Newton solve, and the
+    Cauchy stress carries the out-of-plane stretch F33).  Fields in and out
+    are the reference's tensor-first (2, 2, nx, ny)."""
 
     def __init__(self, nx, ny, model="svk", precision="fp64", device=None, plane_mode="plane_strain"):
         if plane_mode not in ("plane_strain", "plane_stress"):
             raise ValueError(f"plane_mode={plane_mode!r}")
-        if plane_mode == "plane_stress" and model != "svk":
-            raise NotImplementedError("plane stress runs with the SVK model (the Neo-Hookean out-of-plane Newton "
-                                      "solve is not built)")
         self.nx, self.ny = int(nx), int(ny)
         self.plane_mode = plane_mode
         self.s = Fs3dSolver(self.nx, 1, self.ny, model=model, precision=precision, device=device)
@@ -416,7 +414,7 @@ def finite_strain_solver_step_2d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None
                                  enable_console=True, model_type="svk", plane_mode="plane_strain", A_m=0.0, B_m=0.0,
                                  C_m=0.0, solver="al", pixel=1.0, lam=None, mu=None, **unused):
     """One mixed-BC 2D load step (mgkmc/finite_strain_simulator.py:2356-2572),
-    Newton-Krylov path, plane strain (SVK, Neo-Hookean) or plane stress (SVK):
+    Newton-Krylov path, plane strain or plane stress (SVK, Neo-Hookean):
     returns (F, P, Sig, None, F_bar_current) with (2, 2, nx, ny) fields.  The
     Lame fields come from ``C4`` (C4[0,0,1,1] and C4[0,1,0,1], the reference's
     build_C4_2d, whose lambda is the plane-stress one in plane stress) or
@@ -425,9 +423,8 @@ def finite_strain_solver_step_2d(F, F_bar, Ghat4=None, C4=None, I2=None, I4=None
         raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
     if model_type not in _MODEL:
         raise NotImplementedError(f"model_type={model_type!r}: SVK and Neo-Hookean run on the GPU")
-    if plane_mode == "plane_stress" and model_type != "svk":
-        raise NotImplementedError("plane stress runs with the SVK model on the GPU (the Neo-Hookean out-of-plane "
-                                  "Newton solve is not built)")
+    if plane_mode not in ("plane_strain", "plane_stress"):
+        raise ValueError(f"plane_mode={plane_mode!r}")
     torch = _torch()
     F = np.ascontiguousarray(F, dtype=np.float64)
     nx, ny = F.shape[2:]
@@ -466,7 +463,7 @@ def finite_strain_simulation_2d(E, nu, driving_component, eps_target, n_steps, m
                                 vtk_interval="none", vtk_path=None, model_type="svk", A_m=0.0, B_m=0.0, C_m=0.0,
                                 solver="al", Fp=None, precision="fp64", **unused):
     """Incremental 2D finite-strain ramp (finite_strain_simulator.py:2580-2851),
-    plane strain or (SVK) plane stress with the plane-stress lambda
+    plane strain or plane stress with the plane-stress lambda
     E nu / (1 - nu^2) of build_C4_2d, on one device-resident embedded plan
     (``Fs2dSolver``): per load step the boundary conditions of
     build_finite_strain_bc at eps_target * s / n_steps (seeded with the

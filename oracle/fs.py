@@ -56,13 +56,46 @@ def det3(A):
             + A[..., 0, 2] * (A[..., 1, 0] * A[..., 2, 1] - A[..., 1, 1] * A[..., 2, 0]))
 
 
-def constitutive(F, lam, mu, Fpi, model="svk", has_fp=True):
-    """(P, state) with state holding what the tangent needs."""
+def plane_stress_nh_x(Fe, lam2, mu):
+    """x = F33^2 of the plane-stress Neo-Hookean law (:631-684) on the
+    embedded problem: lam_3d = 2 mu lam2 / (2 mu - lam2) from the
+    plane-stress lambda, Je the in-plane det(Fe), Newton on
+    mu x + lam_3d/2 ln x = mu - lam_3d ln Je from x = 1, at most 10 steps,
+    until every voxel's step is below 1e-12 (the reference's loop)."""
+    lam3 = (2.0 * mu * lam2) / np.maximum(1e-14, 2.0 * mu - lam2)
+    Je = np.maximum(1e-14, det3(Fe))
+    x = np.ones_like(Je)
+    target = mu - lam3 * np.log(Je)
+    for _ in range(10):
+        f = mu * x + 0.5 * lam3 * np.log(x) - target
+        dx = -f / (mu + 0.5 * lam3 / x)
+        x = np.maximum(1e-10, x + dx)
+        if np.max(np.abs(dx)) < 1e-12:
+            break
+    return x, lam3
+
+
+def constitutive(F, lam, mu, Fpi, model="svk", has_fp=True, plane_stress=False):
+    """(P, state) with state holding what the tangent needs.  plane_stress:
+    the embedded 2D plane-stress laws (lam the plane-stress lambda); the
+    state then also holds F33."""
     I = np.eye(3)
     Fe = F @ Fpi
     C = _tr(Fe) @ Fe
     l = lam[..., None, None]
     m = mu[..., None, None]
+    if model == "neo_hookean" and plane_stress:
+        # :631-684: S = mu I - mu x C^-1; tangent lam* C^-1 (x) C^-1 + mu x (C^-1 . C^-1)
+        x, lam3 = plane_stress_nh_x(Fe, lam, mu)
+        Ci = np.linalg.inv(C)
+        S = m * I + (-mu * x)[..., None, None] * Ci
+        c = mu * x
+        lam_t = (2.0 * lam3 * c) / np.maximum(1e-14, lam3 + 2.0 * c)
+        st = dict(Fe=Fe, Fpi=Fpi, model=model, Ci=Ci, c=c, F33=np.sqrt(np.maximum(1e-12, x)))
+        st["Sref"] = Fpi @ S @ _tr(Fpi)
+        st["lam"], st["mu"] = lam_t, mu
+        st["has_fp"] = has_fp
+        return Fe @ S @ _tr(Fpi), st
     if model == "svk":
         Eg = 0.5 * (C - I)
         S = l * np.trace(Eg, axis1=-2, axis2=-1)[..., None, None] * I + 2 * m * Eg
@@ -78,6 +111,8 @@ def constitutive(F, lam, mu, Fpi, model="svk", has_fp=True):
     st["Sref"] = Fpi @ S @ _tr(Fpi)
     st["lam"], st["mu"] = lam, mu
     st["has_fp"] = has_fp
+    if plane_stress:
+        st["F33"] = plane_stress_f33(F, lam, mu, Fpi)
     P = Fe @ S @ _tr(Fpi)
     return P, st
 
@@ -161,11 +196,11 @@ def build_bc_3d(driving_component, eps, mixed_targets, F_bar_initial=None):
 
 
 def newton(F_start, F_bar, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model="svk", krylov="bicgstab",
-           return_stats=False, has_fp=True):
+           return_stats=False, has_fp=True, plane_stress=False):
     """Newton branch of finite_strain_solver_step_3d (:3046-3119)."""
     shape = F_start.shape
     DbarF = np.broadcast_to(F_bar - F_start.mean(axis=(0, 1, 2)), shape)
-    P, st = constitutive(F_start, lam, mu, Fpi, model, has_fp)
+    P, st = constitutive(F_start, lam, mu, Fpi, model, has_fp, plane_stress)
     cur = dict(st=st)
     A = spla.LinearOperator((F_start.size, F_start.size),
                             matvec=lambda v: project(kdf(v.reshape(shape), cur["st"])).ravel(), dtype=float)
@@ -186,7 +221,7 @@ def newton(F_start, F_bar, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model="svk", kr
             if np.any(Je <= 1e-4) or np.any(np.isnan(Je)):
                 alpha *= 0.5
                 continue
-            Pt, stt = constitutive(Ft, lam, mu, Fpi, model, has_fp)
+            Pt, stt = constitutive(Ft, lam, mu, Fpi, model, has_fp, plane_stress)
             if np.any(np.isnan(Pt)):
                 alpha *= 0.5
                 continue
@@ -197,7 +232,7 @@ def newton(F_start, F_bar, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model="svk", kr
             raise ValueError("Newton-CG line search failed to find a valid step.")
         if np.linalg.norm(dFm) / (np.linalg.norm(F_curr) + 1e-20) < tol_NW and i > 0:
             if return_stats:
-                return F_curr, P, dict(newton=i + 1, krylov=nmv)
+                return F_curr, P, dict(newton=i + 1, krylov=nmv, F33=cur["st"].get("F33"))
             return F_curr, P
     raise ValueError(f"Newton-CG inner solver did not converge within {max_NW} iterations.")
 
@@ -207,8 +242,9 @@ def solver_step_3d(F, F_bar, E, nu, Fp, driving_component=(0, 0), P_target=None,
                    model="svk", krylov="bicgstab", lame=None, plane_stress=False):
     """finite_strain_solver_step_3d (:2967-3168), Newton branch, spatial-first fields.
     Returns (F, P, Sig, F_bar_current).  ``lame`` = (lam, mu) fields replace
-    the ones from (E, nu); ``plane_stress``: the embedded 2D plane-stress SVK
-    problem (lam the plane-stress lambda), whose Cauchy stress carries F33."""
+    the ones from (E, nu); ``plane_stress``: the embedded 2D plane-stress
+    problem (SVK or Neo-Hookean; lam the plane-stress lambda), whose Cauchy
+    stress carries F33."""
     lam, mu = lame_3d(E, nu) if lame is None else lame
     Fpi = np.linalg.inv(Fp) if Fp is not None else np.broadcast_to(np.eye(3), F.shape)
     E_avg = E.mean() if E_avg is None else E_avg
@@ -225,9 +261,9 @@ def solver_step_3d(F, F_bar, E, nu, Fp, driving_component=(0, 0), P_target=None,
     prev_F = prev_s = None
     max_err = 0.0
     for it in range(max_iter_macro):
-        F_curr, P = newton(F_start, F_bar_cur, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model, krylov,
-                           has_fp=Fp is not None)
-        Sig = cauchy(P, F_curr, plane_stress_f33(F_curr, lam, mu, Fpi) if plane_stress else None)
+        F_curr, P, stats = newton(F_start, F_bar_cur, lam, mu, Fpi, tol_NW, tol_CG, max_NW, model, krylov,
+                                  return_stats=True, has_fp=Fp is not None, plane_stress=plane_stress)
+        Sig = cauchy(P, F_curr, stats["F33"] if plane_stress else None)
         Sm = Sig.mean(axis=(0, 1, 2))
         if not np.any(P_mask):
             return F_curr, P, Sig, F_bar_cur

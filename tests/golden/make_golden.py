@@ -557,6 +557,23 @@ def fs2d_pstress_fixtures():
             tol_NW=1e-7, tol_CG=1e-8, max_NW=30, enable_console=False, model_type="svk", plane_mode="plane_stress",
             solver="newton_cg")
         out.update({f"{tag}_F": F, f"{tag}_P": P, f"{tag}_Sig": Sig})
+    # the plane-stress laws (:591-1087) with F_p at a perturbed F: P and the
+    # Cauchy stress with the law's F33, SVK and Neo-Hookean (its out-of-plane
+    # stretch from the per-voxel Newton solve)
+    Fr = F0 + 0.02 * rng.standard_normal((2, 2, nx, ny))
+    out["F_law"] = Fr
+    for model in ("svk", "neo_hookean"):
+        Pl, _, F33 = FS.constitutive_hyperelastic_2d(Fr, C4, I2, I4, I4rt, Fp=Fp, model_type=model,
+                                                     plane_mode="plane_stress")
+        out[f"{model}_P_law"] = Pl
+        out[f"{model}_F33_law"] = F33
+        out[f"{model}_Sig_law"] = FS.cauchy_from_P(Pl, Fr, F33=F33)
+    # the Neo-Hookean plane-stress Newton-CG step, F_bar prescribed, no F_p
+    F, P, Sig, _, _ = FS.finite_strain_solver_step_2d(
+        F0, Fb, Ghat4, C4, I2, I4, I4rt, Fp=None, driving_component=(0, 0), E_avg=E.mean(), nu_avg=nu.mean(),
+        tol_NW=1e-7, tol_CG=1e-8, max_NW=30, enable_console=False, model_type="neo_hookean",
+        plane_mode="plane_stress", solver="newton_cg")
+    out.update(nh_F=F, nh_P=P, nh_Sig=Sig)
     save("fs2d_pstress_12x8", **out)
 
 

@@ -141,9 +141,48 @@ def test_plane_stress_mixed_bc_with_fp_matches_oracle():
     assert abs(Sig[1, 1].mean()) < 1e2
 
 
-def test_plane_stress_refuses_neo_hookean():
+def test_plane_stress_neo_hookean_step_matches_reference(golden):
+    # the reference's plane-stress Neo-Hookean Newton-CG step (per-voxel
+    # out-of-plane Newton solve for F33, condensed tangent), F_bar prescribed
     from mgkmc_b200.finite_strain_simulator import finite_strain_solver_step_2d
-    F0 = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((8, 8)))
-    with pytest.raises(NotImplementedError):
-        finite_strain_solver_step_2d(F0, np.eye(2), model_type="neo_hookean", plane_mode="plane_stress",
-                                     solver="newton_cg", lam=np.ones((8, 8)), mu=np.ones((8, 8)))
+    g = golden("fs2d_pstress_12x8")
+    E, nu = g["E"], g["nu"]
+    nx, ny = E.shape
+    lam, mu = E * nu / (1.0 - nu ** 2), E / (2 * (1 + nu))
+    F0 = np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny)))
+    F, P, Sig, _, _ = finite_strain_solver_step_2d(
+        F0, g["F_bar"], driving_component=(0, 0), E_avg=E.mean(), nu_avg=nu.mean(), tol_NW=1e-12, tol_CG=1e-13,
+        max_NW=40, enable_console=False, model_type="neo_hookean", plane_mode="plane_stress", solver="newton_cg",
+        lam=lam, mu=mu)
+    assert np.max(np.abs(F - g["nh_F"])) < 1e-9
+    assert rel(P, g["nh_P"]) < 1e-9
+    assert rel(Sig, g["nh_Sig"]) < 1e-9
+
+
+def test_plane_stress_neo_hookean_mixed_bc_with_fp_matches_oracle():
+    # plane-stress Neo-Hookean with F_p, the lateral mean Cauchy stress driven
+    # to zero: against the oracle's step on the embedded problem
+    from mgkmc_b200.finite_strain_simulator import finite_strain_solver_step_2d
+    nx, ny = 24, 32
+    rng = np.random.default_rng(78)
+    E, nu = W.ls2d_material(nx, ny, rng)
+    Fp = _fp2(nx, ny, rng, amp=0.03)
+    lam, mu = E * nu / (1.0 - nu ** 2), E / (2 * (1 + nu))
+    F0 = OF.embed_plane_2d(np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny))))
+    Fb3 = np.eye(3)
+    Fb3[0, 0] = 1.01
+    Pm3 = np.zeros((3, 3), bool)
+    Pm3[2, 2] = True
+    Fo, Po, So, Fbo = OF.solver_step_3d(F0, Fb3, E[:, None, :], nu[:, None, :], OF.embed_plane_2d(Fp), (0, 0),
+                                        np.zeros((3, 3)), Pm3, tol_NW=1e-12, tol_CG=1e-13, max_NW=40, tol_macro=1e2,
+                                        max_iter_macro=40, model="neo_hookean", krylov="cg",
+                                        lame=(lam[:, None, :], mu[:, None, :]), plane_stress=True)
+    F, P, Sig, _, Fb = finite_strain_solver_step_2d(
+        OF.extract_plane_2d(F0), np.diag([1.01, 1.0]), Fp=Fp, driving_component=(0, 0), P_target=np.zeros((2, 2)),
+        P_mask=np.array([[False, False], [False, True]]), E_avg=E.mean(), nu_avg=nu.mean(), tol_NW=1e-12,
+        tol_CG=1e-13, max_NW=40, tol_macro=1e2, max_iter_macro=40, enable_console=False, model_type="neo_hookean",
+        plane_mode="plane_stress", solver="newton_cg", lam=lam, mu=mu)
+    assert rel(F, OF.extract_plane_2d(Fo)) < 1e-9
+    assert rel(P, OF.extract_plane_2d(Po)) < 1e-9
+    assert rel(Sig, OF.extract_plane_2d(So)) < 1e-9
+    assert abs(Fb[1, 1] - Fbo[2, 2]) < 1e-9

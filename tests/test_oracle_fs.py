@@ -142,3 +142,39 @@ def test_plane_stress_newton_step_with_fp_embedded_in_3d(golden):
     assert np.max(np.abs(OF.extract_plane_2d(F) - g["fp_F"])) < 1e-8
     for a, b in ((P, g["fp_P"]), (Sig, g["fp_Sig"])):
         assert np.max(np.abs(OF.extract_plane_2d(a) - b)) < 2e-7 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("model", ["svk", "neo_hookean"])
+def test_plane_stress_law_embedded_in_3d(golden, model):
+    # the reference's 2D plane-stress laws with F_p (:591-1087; Neo-Hookean
+    # with its out-of-plane Newton solve) equal the oracle's on the embedded
+    # problem with the plane-stress lambda: P, F33 and the Cauchy stress
+    g = golden("fs2d_pstress_12x8")
+    E, nu = g["E"], g["nu"]
+    lam, mu = (E * nu / (1.0 - nu ** 2))[:, None, :], (E / (2 * (1 + nu)))[:, None, :]
+    F3 = OF.embed_plane_2d(g["F_law"])
+    Fpi = np.linalg.inv(OF.embed_plane_2d(g["Fp"]))
+    P3, st = OF.constitutive(F3, lam, mu, Fpi, model, has_fp=True, plane_stress=True)
+    ref = g[f"{model}_P_law"]
+    assert np.max(np.abs(OF.extract_plane_2d(P3) - ref)) < 1e-12 * np.max(np.abs(ref))
+    assert np.max(np.abs(st["F33"][:, 0, :] - g[f"{model}_F33_law"])) < 1e-14
+    S2 = OF.extract_plane_2d(OF.cauchy(P3, F3, st["F33"]))
+    assert np.max(np.abs(S2 - g[f"{model}_Sig_law"])) < 1e-12 * np.max(np.abs(ref))
+
+
+def test_plane_stress_neo_hookean_step_embedded_in_3d(golden):
+    # the reference's plane-stress Neo-Hookean Newton-CG step (F_bar
+    # prescribed, no F_p) equals the oracle's step on the embedded problem
+    g = golden("fs2d_pstress_12x8")
+    E, nu = g["E"], g["nu"]
+    nx, ny = E.shape
+    lam, mu = E * nu / (1.0 - nu ** 2), E / (2 * (1 + nu))
+    F0 = OF.embed_plane_2d(np.einsum("ij,xy->ijxy", np.eye(2), np.ones((nx, ny))))
+    Fb = np.eye(3)
+    Fb[0, 0], Fb[2, 2] = g["F_bar"][0, 0], g["F_bar"][1, 1]
+    F, P, Sig, _ = OF.solver_step_3d(F0, Fb, E[:, None, :], nu[:, None, :], None, (0, 0), None, None, tol_NW=1e-12,
+                                     tol_CG=1e-13, max_NW=40, model="neo_hookean", krylov="cg",
+                                     lame=(lam[:, None, :], mu[:, None, :]), plane_stress=True)
+    assert np.max(np.abs(OF.extract_plane_2d(F) - g["nh_F"])) < 1e-9
+    for a, b in ((P, g["nh_P"]), (Sig, g["nh_Sig"])):
+        assert np.max(np.abs(OF.extract_plane_2d(a) - b)) < 1e-9 * np.max(np.abs(b))
