@@ -478,12 +478,45 @@ def run_kmc(n_events, n=256, M=8):
 LANDAU_COEFF = (-199.7e9, -75.4e9, -23.1e9, 1432.0e9, 311.0e9, 145.0e9, -273.0e9)
 
 
+def _landau_device(n, m, reps=5, tol=1e-8):
+    """Device time of one Landau LS solve at n^2 with Anderson depth m (CUDA
+    events, device-resident fields), its iterations, and the per-iteration
+    time from the difference with a solve capped at 2 iterations."""
+    import torch
+    from mgkmc_b200 import linear_elastic_simulator as les
+    from mgkmc_b200 import workloads as W
+    E, nu, ep, _ = W.ls2d_problem(n, n, seed=13)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    p = les.Ls2dBatch([(n, n)])
+    p.set_landau(LANDAU_COEFF)
+    p.set_anderson(m)
+    p.set_lame(0, t(lam), t(mu), t(ep))
+    eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=dev)
+    sig = torch.empty_like(eps)
+    ms, its = {}, {}
+    for cap in (2, 400):
+        its[cap] = p.solve([0], [eb], [eps], [sig], max_iter=cap, tol=tol)[0].iterations
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            p.solve([0], [eb], [eps], [sig], max_iter=cap, tol=tol, sync=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms[cap] = e0.elapsed_time(e1) / reps
+    return ms[400], int(its[400]), (ms[400] - ms[2]) / max(1, its[400] - 2) * 1e3
+
+
 def run_landau(n=256, m=5, reps=5):
     """The Landau 2D LS solve (plane strain, Anderson depth m) at n^2 on the
     benchmark material and eigenstrains with a sheared macro strain, tol 1e-8:
     the numpy-in, numpy-out drop-in (host clock) and the device-resident
-    solve (CUDA events), with the per-iteration device time from a capped
-    solve of 2 iterations."""
+    solve (CUDA events); per-iteration device times (tol 1e-12, so that the
+    loops run long enough) at depths 0, 1 and m, at n^2 and 1024^2."""
     import torch
     from mgkmc_b200 import linear_elastic_simulator as les
     from mgkmc_b200 import workloads as W
@@ -498,29 +531,15 @@ def run_landau(n=256, m=5, reps=5):
     for _ in range(reps):
         les.spectral_solver_landau_2d(lam, mu, **kw, eps_bar=eb, eps_plastic=ep, tol=1e-8, anderson_m=m)
     dropin_ms = (time.perf_counter() - t0) / reps * 1e3
-    dev = torch.device("cuda", torch.cuda.current_device())
-    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-    p = les.Ls2dBatch([(n, n)])
-    p.set_landau(LANDAU_COEFF)
-    p.set_anderson(m)
-    p.set_lame(0, t(lam), t(mu), t(ep))
-    eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=dev)
-    sig = torch.empty_like(eps)
-    ms, its = {}, {}
-    for cap in (2, 400):
-        its[cap] = p.solve([0], [eb], [eps], [sig], max_iter=cap, tol=1e-8)[0].iterations
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(reps):
-            p.solve([0], [eb], [eps], [sig], max_iter=cap, tol=1e-8, sync=False)
-        e1.record()
-        torch.cuda.synchronize()
-        ms[cap] = e0.elapsed_time(e1) / reps
+    solve_ms, iters, _ = _landau_device(n, m, reps)
+    per_it = {}
+    for side in (n, 1024):
+        for depth in (0, 1, m):
+            per_it[f"{side}^2 depth {depth}"] = _landau_device(side, depth, reps, tol=1e-12)[2]
     return {"workload": f"Landau LS 2D {n}^2 plane strain, Anderson depth {m}, tol 1e-8, benchmark material "
                         f"and eigenstrains, eps_bar = [[0.008, 0.002], [0.002, -0.003]]",
-            "dropin_ms": dropin_ms, "device_solve_ms": ms[400], "iterations": int(its[400]),
-            "device_us_per_iteration": (ms[400] - ms[2]) / max(1, its[400] - 2) * 1e3}
+            "dropin_ms": dropin_ms, "device_solve_ms": solve_ms, "iterations": iters,
+            "device_us_per_iteration": per_it}
 
 
 # ------------------------------------------------------- finite strain -----

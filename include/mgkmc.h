@@ -105,16 +105,24 @@ MGK_API int mgk_ls2d_set_secant(mgk_ls2d_t plan, double d, double k);
  * (mean mu + floor_fraction mean mu) / 2): call before mgk_ls2d_set_lame_rep.
  * Macro strain, eigenstrain and warm start must be symmetric; FP64 plans. */
 MGK_API int mgk_ls2d_set_rose(mgk_ls2d_t plan, double eta, double floor_fraction, int plane_stress);
-/* The Landau small-strain law of spectral_solver_landau_2d, plane strain
- * (linear_elastic_simulator.py:952-1228; elasticity.py:487-639 with e33 = 0)
- * for every replica: v = (v1, v2, v3, g1, g2, g3, g4); capping 0 none,
- * 1 piecewise, 2 smooth (tanh of power smooth_power) at the equivalent
- * strain e_cap with tangent 2 tangent_ratio mu.  Medium (mean lam, mean mu):
+/* The Landau small-strain law of spectral_solver_landau_2d
+ * (linear_elastic_simulator.py:952-1228; elasticity.py:487-639) for every
+ * replica: v = (v1, v2, v3, g1, g2, g3, g4); capping 0 none, 1 piecewise,
+ * 2 smooth (tanh of power smooth_power) at the equivalent strain e_cap with
+ * tangent 2 tangent_ratio mu.  plane_stress = 0: e33 = 0; != 0: e33 per voxel
+ * from Newton steps on sigma33 = 0 (elasticity.py:571-616) until the step is
+ * below 1e-9, the stress evaluated at the stepped e33 (the reference evaluates
+ * before the last step and carries a warm start between calls; both fixed
+ * points solve sigma33 = 0).  Medium (mean lam, mean mu), lam the 3D lambda:
  * give the material with mgk_ls2d_set_lame_rep.  Symmetric strains; FP64
  * plans only.  A solve runs the basic scheme; mgk_ls2d_set_anderson adds the
  * reference's Anderson mixing of the iterates inside the device loop. */
 MGK_API int mgk_ls2d_set_landau(mgk_ls2d_t plan, const double* v, int capping, double e_cap, double tangent_ratio,
-                                double smooth_power);
+                                double smooth_power, int plane_stress);
+/* Where the output pass of later solves writes replica rep's out-of-plane
+ * strain e33 under the plane-stress Landau law (device, N doubles; NULL: not
+ * written), the field the reference returns in its e33_state. */
+MGK_API int mgk_ls2d_set_e33_out(mgk_ls2d_t plan, int rep, double* e33);
 /* Type-II Anderson mixing of depth m (0 <= m <= 8; 0 turns it off) inside
  * the device loop of every later solve of this FP64 plan, as
  * spectral_solver_landau_2d mixes its iterates

@@ -58,7 +58,8 @@ _SIGS = {
     "mgk_ls2d_set_lame_rep": (c_int, [_P, c_int, _P, _P, _P, _P]),
     "mgk_ls2d_set_secant": (c_int, [_P, c_double, c_double]),
     "mgk_ls2d_set_rose": (c_int, [_P, c_double, c_double, c_int]),
-    "mgk_ls2d_set_landau": (c_int, [_P, _P, c_int, c_double, c_double, c_double]),
+    "mgk_ls2d_set_landau": (c_int, [_P, _P, c_int, c_double, c_double, c_double, c_int]),
+    "mgk_ls2d_set_e33_out": (c_int, [_P, c_int, _P]),
     "mgk_ls2d_set_anderson": (c_int, [_P, c_int]),
     "mgk_aa_work_bytes": (c_int64, [c_int64]),
     "mgk_aa_update": (c_int, [c_int64, _P, _P, _P, c_int, c_int, c_int, c_int, _P, _P, _P]),

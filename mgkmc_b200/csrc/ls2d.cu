@@ -71,7 +71,7 @@ struct Ls2dRep {
   long long N;
   // constitutive law: 0 linear (elasticity.py:12-18); 1 secant degradation
   // (law_a = d, law_b = k); 2 Rose (law_a = eta, law_b = floor fraction,
-  // law_ps = 1 for plane stress); 3 Landau, plane strain (lp: v1, v2, v3,
+  // law_ps = 1 for plane stress); 3 Landau, law_ps = 1 for plane stress (lp: v1, v2, v3,
   // g1, g2, g3, g4, capping 0 none / 1 piecewise / 2 smooth, E_cap, tangent
   // ratio, smooth power)
   int law, law_ps;
@@ -92,6 +92,7 @@ struct Ls2dRep {
   const double* init;
   double* out_eps;
   double* out_sig;
+  double* out_e33;  // Landau plane stress: the out-of-plane strain per voxel (set_e33_out; may be null)
   double eb[4];
   double tol;
   int max_iter;
@@ -245,15 +246,22 @@ __device__ __forceinline__ double rose_moduli(double l, double m, double dxx, do
 // e33 = 0), parameters lp as in Ls2dRep; a12, a21 the two shear entries of
 // the elastic strain.  With capping on, every voxel's strain goes through the
 // capped form f (a - m) + m, as in the reference.
-__device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, double a22, double a12, double a21,
-                                             const double* __restrict__ lp, double& s11, double& s22, double& s12,
-                                             double& s21) {
+// Capped components, invariants and coefficients of the Landau law at the
+// block-diagonal strain (in-plane a, out-of-plane e33)
+// (elasticity.py:527-569).
+struct LandauScal {
+  double c11, c22, c12, c21, c33, w, I1, I2, cI, ce, ce2;
+};
+
+__device__ __forceinline__ LandauScal landau_scal(double mu, double lam, double a11, double a22, double a12,
+                                                  double a21, double e33, const double* __restrict__ lp) {
   const double v1 = lp[0], v2 = lp[1], v3 = lp[2], g1 = lp[3], g2 = lp[4], g3 = lp[5], g4 = lp[6];
   const int cap = (int)lp[7];
-  double c11 = a11, c22 = a22, c12 = a12, c21 = a21, c33 = 0.0, w = 0.0;
+  LandauScal s;
+  s.c11 = a11; s.c22 = a22; s.c12 = a12; s.c21 = a21; s.c33 = e33; s.w = 0.0;
   if (cap) {
-    const double m3 = (a11 + a22 + 0.0) / 3.0;
-    const double d11 = a11 - m3, d22 = a22 - m3, d33 = 0.0 - m3;
+    const double m3 = (a11 + a22 + e33) / 3.0;
+    const double d11 = a11 - m3, d22 = a22 - m3, d33 = e33 - m3;
     const double Ecap = lp[8];
     const double Eeq = sqrt(fmax(0.0, (2.0 / 3.0) * (d11 * d11 + d22 * d22 + d33 * d33 + 2.0 * a12 * a21)));
     double f = 1.0;
@@ -261,37 +269,81 @@ __device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, 
       const double pw = lp[10];
       if (Eeq > 1e-12) f = (Ecap / Eeq) * pow(tanh(fmin(100.0, pow(Eeq / Ecap, pw))), 1.0 / pw);
       const double t = tanh(fmin(100.0, pow(Eeq / Ecap, pw)));
-      w = t * t;
+      s.w = t * t;
     } else if (Eeq > Ecap) {
       f = Ecap / Eeq;
-      w = 1.0;
+      s.w = 1.0;
     }
-    c11 = f * d11 + m3;
-    c22 = f * d22 + m3;
-    c12 = f * a12;
-    c21 = f * a21;
-    c33 = f * d33 + m3;
+    s.c11 = f * d11 + m3;
+    s.c22 = f * d22 + m3;
+    s.c12 = f * a12;
+    s.c21 = f * a21;
+    s.c33 = f * d33 + m3;
   }
+  const double c11 = s.c11, c22 = s.c22, c33 = s.c33;
   const double I1 = c11 + c22 + c33;
-  const double cross = c12 * c21;
+  const double cross = s.c12 * s.c21;
   const double tr2 = c11 * c11 + c22 * c22 + 2.0 * cross;
   const double I2 = tr2 + c33 * c33;
   const double t_ip = c11 + c22;
   const double I3 = t_ip * (tr2 - (c11 * c22 - cross)) + c33 * c33 * c33;
-  const double cI = lam * I1 + 0.5 * v1 * (I1 * I1) + v2 * I2 + (1.0 / 6.0) * g1 * (I1 * I1 * I1) + g2 * I1 * I2 +
-                    (4.0 / 3.0) * g3 * I3;
-  const double ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * (I1 * I1) + g4 * I2);
-  const double ce2 = 4.0 * (v3 + g3 * I1);
-  s11 = cI + ce * c11 + ce2 * (c11 * c11 + cross);
-  s22 = cI + ce * c22 + ce2 * (c22 * c22 + cross);
-  s12 = ce * c12 + ce2 * (c12 * t_ip);
-  s21 = ce * c21 + ce2 * (c21 * t_ip);
-  if (cap) {
-    const double r = 2.0 * (lp[9] * mu) * w;
-    s11 += r * (a11 - c11);
-    s22 += r * (a22 - c22);
-    s12 += r * (a12 - c12);
-    s21 += r * (a21 - c21);
+  s.I1 = I1;
+  s.I2 = I2;
+  s.cI = lam * I1 + 0.5 * v1 * (I1 * I1) + v2 * I2 + (1.0 / 6.0) * g1 * (I1 * I1 * I1) + g2 * I1 * I2 +
+         (4.0 / 3.0) * g3 * I3;
+  s.ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * (I1 * I1) + g4 * I2);
+  s.ce2 = 4.0 * (v3 + g3 * I1);
+  return s;
+}
+
+// The Landau small-strain stress of a 2D voxel (elasticity.py:487-639).
+// Plane strain: e33 = 0.  Plane stress (ps): e33 from Newton steps on
+// sigma33 = 0 (:571-616) from the linear guess -lam/(lam + 2 mu) tr a, at
+// most 20, until the voxel's step is below 1e-9; the stress is evaluated at
+// the stepped e33.  The reference runs the steps of all voxels together
+// until every step is below 1e-9, evaluates each voxel before its last step
+// and warm-starts the next call from the stepped field; its solver's fixed
+// point is the one where e33 solves sigma33 = 0, as here.  e33_out (may be
+// null) receives e33.
+__device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, double a22, double a12, double a21,
+                                             const double* __restrict__ lp, int ps, double& s11, double& s22,
+                                             double& s12, double& s21, double* e33_out = nullptr) {
+  double e33 = 0.0;
+  if (ps) {
+    const double v1 = lp[0], v2 = lp[1], g1 = lp[3], g2 = lp[4], g3 = lp[5], g4 = lp[6];
+    const double Gt = lp[9] * mu;
+    e33 = -lam / (lam + 2.0 * mu) * (a11 + a22);
+    for (int it = 0; it < 20; ++it) {
+      const LandauScal t = landau_scal(mu, lam, a11, a22, a12, a21, e33, lp);
+      const double c33 = t.c33, I1 = t.I1, I2 = t.I2;
+      double s33 = t.cI + t.ce * c33 + t.ce2 * (c33 * c33);
+      const double dcI = lam + v1 * I1 + 0.5 * g1 * (I1 * I1) + g2 * I2 + 2.0 * (v2 + g2 * I1) * c33 +
+                         4.0 * g3 * (c33 * c33);
+      const double dce = 2.0 * (v2 + g2 * I1) + 4.0 * g4 * c33;
+      double ds33 = dcI + dce * c33 + t.ce + 4.0 * g3 * (c33 * c33) + 2.0 * t.ce2 * c33;
+      if ((int)lp[7]) {
+        s33 = s33 + 2.0 * Gt * (e33 - c33) * t.w;
+        ds33 = ds33 + 2.0 * Gt * t.w;
+      }
+      const double delta = -s33 / (ds33 + 1e-12);
+      e33 = e33 + delta;
+      if (!(fabs(delta) >= 1e-9)) break;  // also leaves on NaN, which the stress then carries
+    }
+    if (e33_out) *e33_out = e33;
+  }
+  const LandauScal t = landau_scal(mu, lam, a11, a22, a12, a21, e33, lp);
+  const double cross = t.c12 * t.c21;
+  const double t_ip = t.c11 + t.c22;
+  s11 = t.cI + t.ce * t.c11 + t.ce2 * (t.c11 * t.c11 + cross);
+  s22 = t.cI + t.ce * t.c22 + t.ce2 * (t.c22 * t.c22 + cross);
+  s12 = t.ce * t.c12 + t.ce2 * (t.c12 * t_ip);
+  s21 = t.ce * t.c21 + t.ce2 * (t.c21 * t_ip);
+  if ((int)lp[7]) {
+    const double r = 2.0 * (lp[9] * mu) * t.w;
+    s11 += r * (a11 - t.c11);
+    s22 += r * (a22 - t.c22);
+    s12 += r * (a12 - t.c12);
+    s21 += r * (a21 - t.c21);
   }
 }
 
@@ -303,7 +355,7 @@ __device__ __forceinline__ void law_sigma(double m, double l, double dxx, double
                                           const double* __restrict__ lp = nullptr) {
   if constexpr (LAW == 3) {
     double syx;
-    landau_sigma(m, l, dxx, dyy, dxy, dxy, lp, sxx, syy, sxy, syx);
+    landau_sigma(m, l, dxx, dyy, dxy, dxy, lp, ps, sxx, syy, sxy, syx);
   } else if constexpr (LAW == 2) {
     double G, le;
     const double tr = rose_moduli(l, m, dxx, dyy, dxy, a, b, ps, G, le);
@@ -656,7 +708,7 @@ __global__ void __launch_bounds__(256) ls2d_row_kernel(const Ls2dRep* __restrict
       double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
       if (sizeof(TS) == 8 && law == 1) law_sigma<1>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
       else if (sizeof(TS) == 8 && law == 2) law_sigma<2>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
-      else if (sizeof(TS) == 8 && law == 3) law_sigma<3>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2, R.lp);
+      else if (sizeof(TS) == 8 && law == 3) law_sigma<3>(m, l, dxx, dyy, dxy, 0.0, 0.0, law_ps, s0, s1, s2, R.lp);
       else law_sigma<0>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2);
       tr[h][0] = (TC)(s0 - (2 * mu0 * e[0] + lam0 * tre));
       tr[h][1] = (TC)(s1 - (2 * mu0 * e[1] + lam0 * tre));
@@ -839,7 +891,7 @@ __global__ void __launch_bounds__(256, 1) ls2d_row_tma_kernel(const Ls2dRep* __r
           double s0, s1, s2;  // nonlinear laws only in FP64 kernels (their plans are FP64)
           if (sizeof(TS) == 8 && law == 1) law_sigma<1>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
           else if (sizeof(TS) == 8 && law == 2) law_sigma<2>(m, l, dxx, dyy, dxy, law_a, law_b, law_ps, s0, s1, s2);
-          else if (sizeof(TS) == 8 && law == 3) law_sigma<3>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2, R.lp);
+          else if (sizeof(TS) == 8 && law == 3) law_sigma<3>(m, l, dxx, dyy, dxy, 0.0, 0.0, law_ps, s0, s1, s2, R.lp);
           else law_sigma<0>(m, l, dxx, dyy, dxy, 0.0, 0.0, 0, s0, s1, s2);
           tr[h][0] = (TC)(s0 - (2 * mu0 * e0 + lam0 * tre));
           tr[h][1] = (TC)(s1 - (2 * mu0 * e1 + lam0 * tre));
@@ -1343,7 +1395,7 @@ __global__ void ls2d_output_kernel(const Ls2dRep* reps, const Ls2dState* st, con
     double mu = R.mu[i];
     double sxx, syy, sxy2, syx2;
     if constexpr (LAW == 3) {
-      landau_sigma(mu, lam, dxx, dyy, dxy, dyx, R.lp, sxx, syy, sxy2, syx2);
+      landau_sigma(mu, lam, dxx, dyy, dxy, dyx, R.lp, law_ps, sxx, syy, sxy2, syx2, R.out_e33 ? R.out_e33 + i : nullptr);
     } else if constexpr (LAW == 2) {
       // Rose: sigma_yx is a copy of sigma_xy, from the [0,1] strain entry
       law_sigma<2>(mu, lam, dxx, dyy, dxy, law_a, law_b, law_ps, sxx, syy, sxy2);
@@ -2198,7 +2250,7 @@ extern "C" int mgk_ls2d_set_rose(mgk_ls2d_t p, double eta, double floor_fraction
 }
 
 extern "C" int mgk_ls2d_set_landau(mgk_ls2d_t p, const double* v, int capping, double e_cap, double tangent_ratio,
-                                   double smooth_power) {
+                                   double smooth_power, int plane_stress) {
   MGK_REQUIRE(p && v, "mgk_ls2d_set_landau: null argument");
   MGK_REQUIRE(p->prec == MGK_FP64, "mgk_ls2d_set_landau: the Landau law runs in FP64 plans only");
   MGK_REQUIRE(capping >= 0 && capping <= 2, "mgk_ls2d_set_landau: capping must be 0, 1 or 2");
@@ -2211,7 +2263,13 @@ extern "C" int mgk_ls2d_set_landau(mgk_ls2d_t p, const double* v, int capping, d
     lp[q] = v[q];
   }
   lp[7] = capping; lp[8] = e_cap; lp[9] = tangent_ratio; lp[10] = smooth_power;
-  return ls2d_set_law(p, 3, 0.0, 0.0, 0, lp);
+  return ls2d_set_law(p, 3, 0.0, 0.0, plane_stress ? 1 : 0, lp);
+}
+
+extern "C" int mgk_ls2d_set_e33_out(mgk_ls2d_t p, int rep, double* e33) {
+  MGK_REQUIRE(p && rep >= 0 && rep < p->nrep, "mgk_ls2d_set_e33_out: bad argument");
+  p->reps[rep].out_e33 = e33;
+  return MGK_OK;
 }
 
 extern "C" int mgk_ls2d_set_anderson(mgk_ls2d_t p, int m) {

@@ -16,6 +16,7 @@ import ctypes
 import numpy as np
 
 from . import _lib as L
+from .linear_elastic_simulator import _vtk_final, _vtk_step
 
 _MODEL = {"svk": 0, "neo_hookean": 1}
 
@@ -218,8 +219,6 @@ def finite_strain_simulation_3d(E, nu, driving_component, eps_target, n_steps, m
         raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
     if model_type not in _MODEL:
         raise NotImplementedError(f"model_type={model_type!r}: SVK and Neo-Hookean run on the GPU")
-    if vtk_interval not in (None, "none"):
-        raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
     torch = _torch()
     mixed_targets = {} if mixed_targets is None else mixed_targets
     E = np.ascontiguousarray(E, dtype=np.float64)
@@ -296,9 +295,13 @@ def finite_strain_simulation_3d(E, nu, driving_component, eps_target, n_steps, m
                 name = f"{checkpoint_path}_{s:06d}"
             if name:
                 _checkpoint(name, s, E, nu, F, Sig, F_mac, S_mac, pixel)
+        if vtk_path is not None:
+            _vtk_step(vtk_interval, vtk_path, s, *_vtk_fields_3d(F, Sig), E, nu, pixel)
     if checkpoint_path is not None and (checkpoint_interval == "last" or (
             isinstance(checkpoint_interval, int) and n_steps % checkpoint_interval != 0)):
         _checkpoint(f"{checkpoint_path}_final", n_steps, E, nu, F, Sig, F_macro[-1], Sig_macro[-1], pixel)
+    if vtk_path is not None:
+        _vtk_final(vtk_interval, vtk_path, n_steps, *_vtk_fields_3d(F, Sig), E, nu, pixel)
     total = _time.time() - t0
     m_, sec = divmod(total, 60)
     h_, m_ = divmod(m_, 60)
@@ -309,6 +312,15 @@ def finite_strain_simulation_3d(E, nu, driving_component, eps_target, n_steps, m
     if glog_f:
         glog_f.close()
     return np.array(F_macro), np.array(Sig_macro), np.array(P_macro), F_list, Sig_list
+
+
+def _vtk_fields_3d(F, Sig):
+    """The fields the reference's ramp writes to VTK (:3367-3370): the
+    Green-Lagrange strain and the Cauchy stress, spatial-first numpy."""
+    torch = _torch()
+    E_GL = 0.5 * (torch.einsum("kixyz,kjxyz->ijxyz", F, F) - torch.eye(3, dtype=F.dtype, device=F.device)
+                  .reshape(3, 3, 1, 1, 1))
+    return E_GL.permute(2, 3, 4, 0, 1).cpu().numpy(), Sig.permute(2, 3, 4, 0, 1).cpu().numpy()
 
 
 def _checkpoint(path, step, E, nu, F, Sig, F_mac, S_mac, pixel):
@@ -475,8 +487,6 @@ def finite_strain_simulation_2d(E, nu, driving_component, eps_target, n_steps, m
     from datetime import datetime as _dt
     if solver not in ("newton_cg", "newton"):
         raise NotImplementedError(f"solver={solver!r}: only the Newton-Krylov path runs on the GPU")
-    if vtk_interval not in (None, "none"):
-        raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
     mixed_targets = {} if mixed_targets is None else mixed_targets
     E = np.ascontiguousarray(E, dtype=np.float64)
     nu = np.ascontiguousarray(nu, dtype=np.float64)
@@ -531,14 +541,24 @@ def finite_strain_simulation_2d(E, nu, driving_component, eps_target, n_steps, m
                 isinstance(checkpoint_interval, int) and s % checkpoint_interval == 0)):
             _checkpoint_2d(checkpoint_path if checkpoint_interval == "current" else f"{checkpoint_path}_{s:06d}", s,
                            E, nu, F, Sig, F_mac, S_mac, pixel)
+        if vtk_path is not None:
+            _vtk_step(vtk_interval, vtk_path, s, *_vtk_fields_2d(F, Sig), E, nu, pixel)
     if checkpoint_path is not None and (checkpoint_interval == "last" or (
             isinstance(checkpoint_interval, int) and n_steps % checkpoint_interval != 0)):
         _checkpoint_2d(f"{checkpoint_path}_final", n_steps, E, nu, F, Sig, F_macro[-1], Sig_macro[-1], pixel)
+    if vtk_path is not None:
+        _vtk_final(vtk_interval, vtk_path, n_steps, *_vtk_fields_2d(F, Sig), E, nu, pixel)
     if log_f:
         log_f.close()
     if glog_f:
         glog_f.close()
     return np.array(F_macro), np.array(Sig_macro), np.array(P_macro), F_list, Sig_list
+
+
+def _vtk_fields_2d(F, Sig):
+    """Green-Lagrange strain and Cauchy stress, spatial-first (:2797-2800)."""
+    E_GL = 0.5 * (np.einsum("kixy,kjxy->ijxy", F, F) - np.eye(2)[:, :, None, None])
+    return np.moveaxis(E_GL, (0, 1), (2, 3)), np.moveaxis(Sig, (0, 1), (2, 3))
 
 
 def _checkpoint_2d(path, step, E, nu, F, Sig, F_mac, S_mac, pixel):

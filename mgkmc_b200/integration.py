@@ -18,6 +18,7 @@ from . import finite_strain_simulator as _fss
 from . import kmc_simulator_functions as _kf
 from . import linear_elastic_simulator as _les
 from . import stz as _stz
+from . import vtk as _vtk
 
 # (reference module, attribute) -> replacement
 _TABLE = [
@@ -51,6 +52,11 @@ _TABLE = [
     ("finite_strain_simulator", "finite_strain_simulation_3d", _fss.finite_strain_simulation_3d),     # run.py:783
     ("finite_strain_simulator", "finite_strain_simulation_2d", _fss.finite_strain_simulation_2d),     # run.py:483
     ("stz.update_fft", "update_stress_fft_full", _les.update_stress_fft_full),
+    # the VTK writer the drivers bind at import time (meshio-free)
+    ("kmc_simulator", "export_to_vtk", _vtk.export_to_vtk),                        # kmc_simulator.py:11
+    ("linear_elastic_simulator", "export_to_vtk", _vtk.export_to_vtk),             # :9
+    ("finite_strain_simulator", "export_to_vtk", _vtk.export_to_vtk),              # :28
+    ("analysis.vtk", "export_to_vtk", _vtk.export_to_vtk),
 ]
 
 _SAVED = {}

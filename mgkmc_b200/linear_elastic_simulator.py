@@ -90,12 +90,20 @@ class Ls2dBatch:
         L.check(L.lib().mgk_ls2d_set_rose(self._h, float(eta), float(mu_floor_fraction),
                                           1 if plane_mode == "plane_stress" else 0), "mgk_ls2d_set_rose")
 
-    def set_landau(self, v, capping=0, e_cap=0.0, tangent_ratio=0.1, smooth_power=1.0):
-        """Landau law (plane strain) for every replica: v = (v1, v2, v3, g1, g2,
-        g3, g4); capping 0 none, 1 piecewise, 2 smooth at e_cap; FP64 plans."""
+    def set_landau(self, v, capping=0, e_cap=0.0, tangent_ratio=0.1, smooth_power=1.0, plane_stress=False):
+        """Landau law for every replica: v = (v1, v2, v3, g1, g2, g3, g4);
+        capping 0 none, 1 piecewise, 2 smooth at e_cap; plane_stress solves
+        e33 per voxel (sigma33 = 0); FP64 plans."""
         arr = (ctypes.c_double * 7)(*[float(a) for a in v])
         L.check(L.lib().mgk_ls2d_set_landau(self._h, ctypes.cast(arr, ctypes.c_void_p), int(capping), float(e_cap),
-                                            float(tangent_ratio), float(smooth_power)), "mgk_ls2d_set_landau")
+                                            float(tangent_ratio), float(smooth_power), 1 if plane_stress else 0),
+                "mgk_ls2d_set_landau")
+
+    def set_e33_out(self, rep, e33):
+        """Device buffer (N doubles) for replica rep's plane-stress Landau e33
+        in later solves (None: not written)."""
+        self._keep[("e33", rep)] = e33
+        L.check(L.lib().mgk_ls2d_set_e33_out(self._h, int(rep), L.ptr(e33)), "mgk_ls2d_set_e33_out")
 
     def set_anderson(self, m):
         """Type-II Anderson mixing of depth m (0: off) inside the device loop of
@@ -315,16 +323,19 @@ def spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_
                               strain_capping_tangent_ratio=0.1, strain_capping_type="piecewise",
                               strain_capping_smooth_power=1.0, solver="dbfft", e33_state=None, anderson_m=5):
     """Nonlinear 2D Lippmann-Schwinger solve with the Landau small-strain law
-    (linear_elastic_simulator.py:952-1228, solver "dbfft"), plane strain: the
-    basic scheme with the (mean lam, mean mu) medium and type-II Anderson
-    mixing of the last anderson_m iterates, the whole loop (update norm,
-    convergence decision, least-squares fit and mix) on the device in one
-    graph launch.  Returns (eps, sig, eps.mean(axis=(0,1)),
+    (linear_elastic_simulator.py:952-1228, solver "dbfft"), plane strain or
+    plane stress (e33 per voxel from the law's Newton solve of sigma33 = 0;
+    ``e33_state``, when given, receives the final e33 field as the
+    reference's does; its warm start is not needed, each evaluation solving
+    e33 to convergence): the basic scheme with the (mean lam, mean mu) medium
+    and type-II Anderson mixing of the last anderson_m iterates, the whole
+    loop (update norm, convergence decision, least-squares fit and mix) on
+    the device in one graph launch.  Returns (eps, sig, eps.mean(axis=(0,1)),
     sig.mean(axis=(0,1))); a non-finite update raises FloatingPointError as
-    the reference does.  Plane stress, the Newton-CG branch and asymmetric
-    strains are not built (NotImplementedError); anderson_m is limited to 8."""
-    if plane_mode != "plane_strain":
-        raise NotImplementedError("spectral_solver_landau_2d: plane stress is not built (plane strain only)")
+    the reference does.  The Newton-CG branch and asymmetric strains are not
+    built (NotImplementedError); anderson_m is limited to 8."""
+    if plane_mode not in ("plane_strain", "plane_stress"):
+        raise ValueError(f"spectral_solver_landau_2d: plane_mode={plane_mode!r}")
     if solver != "dbfft":
         raise NotImplementedError("spectral_solver_landau_2d: only the basic scheme (solver='dbfft') is built")
     m = int(anderson_m)
@@ -352,15 +363,23 @@ def spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eps_bar, eps_
         p = _PLANS_LANDAU.get(key)
         if p is None:
             p = _PLANS_LANDAU[key] = Ls2dBatch([(nx, ny)])
+        ps = plane_mode == "plane_stress"
         p.set_landau((v1, v2, v3, g1, g2, g3, g4), cap, e_cap, strain_capping_tangent_ratio,
-                     strain_capping_smooth_power)
+                     strain_capping_smooth_power, plane_stress=ps)
         p.set_anderson(m)
         p.set_lame(0, t(lam), t(mu), None if eps_plastic is None else t(eps_plastic))
         eps = torch.empty((nx, ny, 2, 2), dtype=torch.float64, device=dev)
         sig = torch.empty_like(eps)
+        e33 = torch.empty((nx, ny), dtype=torch.float64, device=dev) if ps and e33_state is not None else None
+        p.set_e33_out(0, e33)
         init = None if eps_init is None else [t(eps_init)]
-        info = p.solve([0], [eps_bar], [eps], [sig], eps_init=init, max_iter=max_iter, tol=tol)[0]
+        try:
+            info = p.solve([0], [eps_bar], [eps], [sig], eps_init=init, max_iter=max_iter, tol=tol)[0]
+        finally:
+            p.set_e33_out(0, None)
         eps_np, sig_np = eps.cpu().numpy(), sig.cpu().numpy()
+        if e33 is not None:
+            e33_state["e33"] = e33.cpu().numpy()
     if info.status == L.NONFINITE or not np.isfinite(info.final_diff):
         raise FloatingPointError("spectral_solver_landau_2d: non-finite strain update in LS loop (Landau energy "
                                  "likely unstable at this strain; consider strain capping or smaller load steps).")
@@ -567,6 +586,27 @@ _COMP_LABELS = {(0, 0): "xx", (1, 1): "yy", (2, 2): "zz", (0, 1): "xy", (0, 2): 
                 (2, 0): "zx", (2, 1): "zy"}
 
 
+def _vtk_step(ival, path, s, eps, sig, E, nu, pixel):
+    """The ramps' per-step VTK file (linear_elastic_simulator.py:237-246):
+    ival "current" rewrites <path>.vtu, an integer writes <path>_<step>.vtu
+    every ival steps; "none", "last" and None write nothing here."""
+    if ival is None or ival in ("none", "last"):
+        return
+    from .vtk import export_to_vtk
+    if ival == "current":
+        export_to_vtk(f"{path}.vtu", eps, sig, E, nu, pixel, match_matplotlib_orientation=True)
+    elif isinstance(ival, int) and s % ival == 0:
+        export_to_vtk(f"{path}_{s:06d}.vtu", eps, sig, E, nu, pixel, match_matplotlib_orientation=True)
+
+
+def _vtk_final(ival, path, n_steps, eps, sig, E, nu, pixel):
+    """The ramps' final VTK file (:253-256): <path>_final.vtu for "last", or
+    for an integer interval that did not end on the last step."""
+    if ival == "last" or (isinstance(ival, int) and n_steps % ival != 0):
+        from .vtk import export_to_vtk
+        export_to_vtk(f"{path}_final.vtu", eps, sig, E, nu, pixel, match_matplotlib_orientation=True)
+
+
 def _ramp(dim, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls, max_iter_ls, tol_macro,
           max_iter_macro, store, plane_mode, log_path, global_log_path, driving_component, enable_console, vtk_path,
           vtk_interval, solver_kw):
@@ -582,8 +622,6 @@ def _ramp(dim, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls,
     import time as _time
     from datetime import datetime as _dt
     torch = _torch()
-    if vtk_interval not in (None, "none"):
-        raise NotImplementedError("VTK output is not part of the GPU path (write the returned fields instead)")
     chk_ival = solver_kw.pop("checkpoint_interval", None)
     chk_path = solver_kw.pop("checkpoint_path", "checkpoint")
     if chk_path and chk_ival not in (None, "none"):
@@ -665,8 +703,10 @@ def _ramp(dim, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls,
                 name = f"{chk_path}_{s:06d}.h5"
             if name:
                 _save_chk(dim, name, s, E, nu, e_np, s_np, epsM, sigM, pixel)
+        _vtk_step(vtk_interval, vtk_path, s, e_np, s_np, E, nu, pixel)
     if chk_ival == "last" or (isinstance(chk_ival, int) and n_steps % chk_ival != 0):
         _save_chk(dim, f"{chk_path}_final.h5", n_steps, E, nu, e_np, s_np, epsM, sigM, pixel)
+    _vtk_final(vtk_interval, vtk_path, n_steps, e_np, s_np, E, nu, pixel)
     total = _time.time() - t0
     m_, s_ = divmod(total, 60)
     h_, m_ = divmod(m_, 60)

@@ -226,21 +226,15 @@ def spectral_solver_secant_3d(lam, mu, d, k, eps_bar, eps_plastic=None, max_iter
     return out + (it_done, diff) if return_info else out
 
 
-def landau_stress_2d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1, cap_power=1.0):
-    """Landau small-strain stress, plane strain (mgkmc/elasticity.py:487-639,
-    e33 = 0): v = (v1, v2, v3, g1, g2, g3, g4).  With cap_type "piecewise" or
-    "smooth" the strain is capped at the equivalent strain E_cap (cap_limit, or
-    sqrt(0.2 mean(mu) / |g4|) when it is None or <= 0 and g4 < 0, else 999)
-    and a tangent 2 cap_ratio mu w (e - e_capped) is added."""
+def _landau_scalars_2d(a11, a22, a12, a21, e33, lam, mu, v, cap):
+    """Capped components, invariants and Landau coefficients of the
+    block-diagonal strain (in-plane a, out-of-plane e33)
+    (mgkmc/elasticity.py:527-569).  cap: None or (type, E_cap, power)."""
     v1, v2, v3, g1, g2, g3, g4 = v
-    a11, a22, a12, a21 = e[..., 0, 0], e[..., 1, 1], e[..., 0, 1], e[..., 1, 0]
-    e33 = np.zeros_like(a11)
     m3 = (a11 + a22 + e33) / 3.0
     d11, d22, d33 = a11 - m3, a22 - m3, e33 - m3
-    if cap_type is not None:
-        mu_mean = np.mean(mu)
-        E_cap = cap_limit if cap_limit is not None and cap_limit > 0 else (
-            np.sqrt(0.2 * mu_mean / abs(g4)) if g4 < 0 else 999.0)
+    if cap is not None:
+        cap_type, E_cap, cap_power = cap
         E_eq = np.sqrt(np.maximum(0.0, (2.0 / 3.0) * (d11 * d11 + d22 * d22 + d33 * d33 + 2.0 * a12 * a21)))
         f = np.ones_like(E_eq)
         nz = E_eq > 1e-12
@@ -254,6 +248,7 @@ def landau_stress_2d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1
             w = capped.astype(float)
         c11, c22, c12, c21, c33 = f * d11 + m3, f * d22 + m3, f * a12, f * a21, f * d33 + m3
     else:
+        w = None
         c11, c22, c12, c21, c33 = a11, a22, a12, a21, e33
     I1 = c11 + c22 + c33
     cross = c12 * c21
@@ -264,13 +259,66 @@ def landau_stress_2d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1
     cI = lam * I1 + 0.5 * v1 * I1 ** 2 + v2 * I2 + (1.0 / 6.0) * g1 * I1 ** 3 + g2 * I1 * I2 + (4.0 / 3.0) * g3 * I3
     ce = 2.0 * (mu + v2 * I1 + 0.5 * g2 * I1 ** 2 + g4 * I2)
     ce2 = 4.0 * (v3 + g3 * I1)
+    return I1, I2, c11, c22, c12, c21, c33, w, cI, ce, ce2
+
+
+def landau_stress_2d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1, cap_power=1.0,
+                     plane_stress=False, e33_state=None):
+    """Landau small-strain stress (mgkmc/elasticity.py:487-639): v = (v1, v2,
+    v3, g1, g2, g3, g4).  With cap_type "piecewise" or "smooth" the strain is
+    capped at the equivalent strain E_cap (cap_limit, or sqrt(0.2 mean(mu) /
+    |g4|) when it is None or <= 0 and g4 < 0, else 999) and a tangent
+    2 cap_ratio mu w (e - e_capped) is added.  Plane strain: e33 = 0.  Plane
+    stress (:571-616): e33 from Newton steps on sigma33 = 0 from the warm
+    state (e33_state["e33"]) or the linear guess -lam/(lam + 2 mu) tr e, at
+    most 20, until every voxel's step is below 1e-9; the stress is that of
+    the last state evaluated before the final step; e33_state receives the
+    stepped e33."""
+    v1, v2, v3, g1, g2, g3, g4 = v
+    a11, a22, a12, a21 = e[..., 0, 0], e[..., 1, 1], e[..., 0, 1], e[..., 1, 0]
+    cap = None
+    if cap_type is not None:
+        mu_mean = np.mean(mu)
+        E_cap = cap_limit if cap_limit is not None and cap_limit > 0 else (
+            np.sqrt(0.2 * mu_mean / abs(g4)) if g4 < 0 else 999.0)
+        cap = (cap_type, E_cap, cap_power)
+        Gt = cap_ratio * mu
+    if plane_stress:
+        warm = None if e33_state is None else e33_state.get("e33")
+        if warm is not None and warm.shape == a11.shape:
+            e33 = warm.copy()
+        else:
+            e33 = -lam / (lam + 2.0 * mu) * (a11 + a22)
+        for _ in range(20):
+            I1, I2, c11, c22, c12, c21, c33, w, cI, ce, ce2 = _landau_scalars_2d(a11, a22, a12, a21, e33, lam, mu,
+                                                                                   v, cap)
+            s33 = cI + ce * c33 + ce2 * c33 ** 2
+            dcI = lam + v1 * I1 + 0.5 * g1 * I1 ** 2 + g2 * I2 + 2.0 * (v2 + g2 * I1) * c33 + 4.0 * g3 * c33 ** 2
+            dce = 2.0 * (v2 + g2 * I1) + 4.0 * g4 * c33
+            ds33 = dcI + dce * c33 + ce + 4.0 * g3 * c33 ** 2 + 2.0 * ce2 * c33
+            if cap is not None:
+                s33 = s33 + 2.0 * Gt * (e33 - c33) * w
+                ds33 = ds33 + 2.0 * Gt * w
+            delta = -s33 / (ds33 + 1e-12)
+            if not np.all(np.isfinite(delta)):
+                raise FloatingPointError("landau_stress_2d: non-finite e33 Newton update")
+            e33 = e33 + delta
+            if np.all(np.abs(delta) < 1e-9):
+                break
+        if e33_state is not None:
+            e33_state["e33"] = e33
+    else:
+        e33 = np.zeros_like(a11)
+        I1, I2, c11, c22, c12, c21, c33, w, cI, ce, ce2 = _landau_scalars_2d(a11, a22, a12, a21, e33, lam, mu, v, cap)
+    cross = c12 * c21
+    t_ip = c11 + c22
     sig = np.empty(e.shape)
     sig[..., 0, 0] = cI + ce * c11 + ce2 * (c11 * c11 + cross)
     sig[..., 1, 1] = cI + ce * c22 + ce2 * (c22 * c22 + cross)
     sig[..., 0, 1] = ce * c12 + ce2 * (c12 * t_ip)
     sig[..., 1, 0] = ce * c21 + ce2 * (c21 * t_ip)
-    if cap_type is not None:
-        r = 2.0 * (cap_ratio * mu) * w
+    if cap is not None:
+        r = 2.0 * Gt * w
         sig[..., 0, 0] += r * (a11 - c11)
         sig[..., 1, 1] += r * (a22 - c22)
         sig[..., 0, 1] += r * (a12 - c12)
@@ -304,8 +352,9 @@ def anderson_step(hist_g, hist_f, g, f, m):
 
 def spectral_solver_landau_2d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
                               eps_init=None, anderson_m=5, cap_type=None, cap_limit=None, cap_ratio=0.1,
-                              cap_power=1.0, return_info=False):
-    """Landau small-strain LS fixed point, plane strain, the basic scheme
+                              cap_power=1.0, return_info=False, plane_stress=False, e33_state=None):
+    """Landau small-strain LS fixed point (plane strain, or plane stress with
+    the e33 Newton solve and its warm state e33_state), the basic scheme
     with Anderson mixing (mgkmc/linear_elastic_simulator.py:952-1228, solver
     "dbfft"): medium (mean lam, mean mu) fixed; G(eps) = eps_bar + Gamma0 *
     (sigma_L(eps - eps_p) - C0:eps) with zero-mean fluctuation; stop when
@@ -322,7 +371,7 @@ def spectral_solver_landau_2d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=40
         eps = np.broadcast_to(eps_bar, shape + (2, 2)).copy()
     ep = eps_plastic
     law = lambda x: landau_stress_2d(x - ep if ep is not None else x, lam, mu, v, cap_type, cap_limit, cap_ratio,
-                                     cap_power)
+                                     cap_power, plane_stress, e33_state)
     hg, hf = [], []
     it_done, diff = 0, np.inf
     for it in range(max_iter):

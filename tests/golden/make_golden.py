@@ -320,6 +320,56 @@ def ls2d_landau_fixtures():
     save("ls2d_landau_16x12", **out)
 
 
+def ls2d_landau_pstress_fixtures():
+    """The reference's Landau law in plane stress (stress_from_strain_landau_2d
+    with its e33 Newton solve, elasticity.py:571-616) without capping, with
+    piecewise and with smooth capping, cold and from a warm e33 state; its LS
+    solver in plane stress (spectral_solver_landau_2d, basic scheme, Anderson
+    depth 5, an e33 state carried across the iterations) without and with
+    capping."""
+    from mgkmc import elasticity as ELA
+    rng = np.random.default_rng(74)
+    nx, ny = 16, 12
+    E, nu = W.ls2d_material(nx, ny, rng)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    v1, v2, v3, g1, g2, g3, g4 = LANDAU_V
+    kw = dict(v1=v1, v2=v2, v3=v3, g1=g1, g2=g2, g3=g3, g4=g4, plane_mode="plane_stress")
+    e = rng.normal(0, 0.02, (nx, ny, 2, 2))
+    e[..., 1, 0] = e[..., 0, 1]
+    out = dict(lam=lam, mu=mu, v=np.array(LANDAU_V), strain=e)
+    caps = {"plain": {}, "piecewise": dict(strain_capping_enabled=True, strain_capping_limit=0.015),
+            "smooth": dict(strain_capping_enabled=True, strain_capping_limit=0.015, strain_capping_type="smooth",
+                           strain_capping_smooth_power=2.0)}
+    for tag, ck in caps.items():
+        st = {}
+        out[f"sig_{tag}"] = ELA.stress_from_strain_landau_2d(e, lam, mu, **kw, **ck, e33_state=st)
+        out[f"e33_{tag}"] = st["e33"]
+        warm = {"e33": st["e33"] + 1e-4 * rng.standard_normal(st["e33"].shape)}
+        out[f"warm_in_{tag}"] = warm["e33"].copy()
+        out[f"sig_warm_{tag}"] = ELA.stress_from_strain_landau_2d(e, lam, mu, **kw, **ck, e33_state=warm)
+    ep = W.pure_shear_eigenstrain_2d(nx, ny, rng, frac=0.1)
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    out.update(eps_plastic=ep, eps_bar=eb)
+    for tag, ck in (("solve", {}), ("solve_cap", dict(strain_capping_enabled=True, strain_capping_limit=0.01))):
+        st = {}
+        eps, sig, _, _ = LES.spectral_solver_landau_2d(lam, mu, **kw, **ck, eps_bar=eb, eps_plastic=ep, max_iter=400,
+                                                       tol=1e-12, anderson_m=5, e33_state=st)
+        out.update({f"eps_{tag}": eps, f"sig_{tag}": sig, f"e33_{tag}": st["e33"]})
+    save("ls2d_landau_pstress_16x12", **out)
+
+
+def vtk_fixtures():
+    """The reference's node-displacement reconstruction of its VTK writer
+    (analysis/vtk.py:4-116) for a 2D and a 3D random strain field."""
+    from mgkmc.analysis import vtk as RV
+    rng = np.random.default_rng(75)
+    e2 = rng.normal(0, 0.01, (6, 5, 2, 2))
+    e3 = rng.normal(0, 0.01, (4, 3, 5, 3, 3))
+    save("vtk_displacement", eps2=e2, u2=RV.reconstruct_displacement_element_centered(e2, pixel=1.5),
+         eps3=e3, u3=RV.reconstruct_displacement_element_centered(e3, pixel=0.5))
+
+
 def ls2d_rose_fixtures():
     """The reference's Rose-law LS solver (spectral_solver_rose_2d), plane
     strain and plane stress, with the 3D Lame lambda as its KMC driver passes."""
@@ -619,7 +669,8 @@ ALL = ("ls2d_fixtures", "ls3d_fixtures", "kmc2d_fixtures", "kmc3d_fixtures", "fs
        "ls2d_rose_fixtures", "kmc2d_cascade_fixtures", "kmc2d_patch_fixtures", "ls3d_secant_fixtures",
        "ls2d_landau_fixtures", "kmc2d_trajectory_fixtures", "driver_fixtures",
        "kmc3d_trajectory_fixtures", "fs2d_step_fixtures",
-       "fs2d_sim_fixtures", "ls3d_landau_fixtures", "fs2d_pstress_fixtures")
+       "fs2d_sim_fixtures", "ls3d_landau_fixtures", "fs2d_pstress_fixtures",
+       "ls2d_landau_pstress_fixtures", "vtk_fixtures")
 
 
 if __name__ == "__main__":

@@ -290,6 +290,40 @@ def test_landau_device_loop_iteration_cost(les):
     assert per_it_us < 80.0
 
 
+@pytest.mark.parametrize("tag", ["solve", "solve_cap"])
+def test_golden_landau_plane_stress(les, golden, tag):
+    # plane-stress Landau solve (per-voxel e33 Newton, Anderson depth 5,
+    # CTA-wide kernels at 16 x 12) against the reference's run with an e33
+    # state; e33_state receives the out-of-plane strain
+    g = golden("ls2d_landau_pstress_16x12")
+    kw = dict(strain_capping_enabled=True, strain_capping_limit=0.01) if tag == "solve_cap" else {}
+    st = {}
+    eps, sig, _, _ = les.spectral_solver_landau_2d(g["lam"], g["mu"], **_landau_kw(g["v"]), eps_bar=g["eps_bar"],
+                                                   eps_plastic=g["eps_plastic"], max_iter=400, tol=1e-12,
+                                                   plane_mode="plane_stress", e33_state=st, **kw)
+    assert rel(eps, g[f"eps_{tag}"]) < TOL
+    assert rel(sig, g[f"sig_{tag}"]) < TOL
+    assert np.max(np.abs(st["e33"] - g[f"e33_{tag}"])) < 1e-11
+
+
+@pytest.mark.parametrize("nx,ny,cap", [(64, 64, None), (256, 128, "smooth"), (128, 96, "piecewise")])
+def test_landau_plane_stress_against_oracle(les, nx, ny, cap):
+    # warp-line kernels with the plane-stress Landau law against the oracle
+    # (the reference's global e33 Newton with its warm state)
+    E, nu, ep, _ = W.ls2d_problem(nx, ny, seed=17)
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    eb = np.array([[0.008, 0.002], [0.002, -0.003]])
+    ckw = {} if cap is None else dict(strain_capping_enabled=True, strain_capping_limit=0.012,
+                                      strain_capping_type=cap, strain_capping_smooth_power=2.0)
+    eps, sig, _, _ = les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, eps_plastic=ep,
+                                                   max_iter=400, tol=1e-11, plane_mode="plane_stress", **ckw)
+    o = OL.spectral_solver_landau_2d(lam, mu, LANDAU_V, eb, ep, max_iter=400, tol=1e-11, cap_type=cap,
+                                     cap_limit=0.012, cap_power=2.0, plane_stress=True, e33_state={})
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
 def test_anderson_kernels():
     # history update, inner products and mix of mgk_aa_* against numpy
     import ctypes
@@ -336,8 +370,6 @@ def test_landau_refusals(les):
     lam = E * nu / ((1 + nu) * (1 - 2 * nu))
     mu = E / (2 * (1 + nu))
     eb = np.array([[0.005, 0.0], [0.0, 0.0]])
-    with pytest.raises(NotImplementedError):
-        les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, plane_mode="plane_stress")
     with pytest.raises(NotImplementedError):
         les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=np.array([[0.0, 0.001], [0.0, 0.0]]))
     with pytest.raises(NotImplementedError):

@@ -308,3 +308,26 @@ def test_landau_3d_law_and_solver(golden):
     eps, sig, _, _ = OL.spectral_solver_landau_3d(g["lam"], g["mu"], v, g["eps_bar"], max_iter=400, tol=1e-12,
                                                   cap_type="smooth", cap_limit=0.01, cap_power=2.0, **kw)
     assert rel(eps, g["eps_cap"]) < 1e-12 and rel(sig, g["sig_cap"]) < 1e-12
+
+
+def test_landau_plane_stress_law_and_solver(golden):
+    # the oracle's plane-stress Landau law (global e33 Newton, warm state) and
+    # solver against the reference's
+    from oracle import ls as OL
+    g = golden("ls2d_landau_pstress_16x12")
+    v = tuple(g["v"])
+    caps = {"plain": (None, None, 1.0), "piecewise": ("piecewise", 0.015, 1.0), "smooth": ("smooth", 0.015, 2.0)}
+    for tag, (ct, cl, cp) in caps.items():
+        st = {}
+        sig = OL.landau_stress_2d(g["strain"], g["lam"], g["mu"], v, ct, cl, 0.1, cp, True, st)
+        assert np.max(np.abs(sig - g[f"sig_{tag}"])) <= 1e-12 * np.max(np.abs(g[f"sig_{tag}"]))
+        assert np.max(np.abs(st["e33"] - g[f"e33_{tag}"])) <= 1e-15
+        warm = {"e33": g[f"warm_in_{tag}"].copy()}
+        sig = OL.landau_stress_2d(g["strain"], g["lam"], g["mu"], v, ct, cl, 0.1, cp, True, warm)
+        assert np.max(np.abs(sig - g[f"sig_warm_{tag}"])) <= 1e-12 * np.max(np.abs(g[f"sig_warm_{tag}"]))
+    for tag, (ct, cl) in (("solve", (None, None)), ("solve_cap", ("piecewise", 0.01))):
+        st = {}
+        o = OL.spectral_solver_landau_2d(g["lam"], g["mu"], v, g["eps_bar"], g["eps_plastic"], max_iter=400, tol=1e-12,
+                                         anderson_m=5, cap_type=ct, cap_limit=cl, plane_stress=True, e33_state=st)
+        assert np.max(np.abs(o[0] - g[f"eps_{tag}"])) < 1e-9 * np.max(np.abs(g[f"eps_{tag}"]))
+        assert np.max(np.abs(o[1] - g[f"sig_{tag}"])) < 1e-9 * np.max(np.abs(g[f"sig_{tag}"]))
