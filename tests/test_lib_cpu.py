@@ -48,7 +48,8 @@ def test_new_entry_points_reject_bad_arguments_without_a_device():
     assert lib.mgk_kmc2d_patch(0, 4, 2, None, None, 0.0, None, None, 3, None, None, None, None) == L.BAD_ARG
     assert lib.mgk_kmc2d_patch_setup(8, 8, 5000, one, one, one, one, None) == L.BAD_ARG  # R > 4096
     assert lib.mgk_ls3d_set_secant(None, 0.5, 10.0) == L.BAD_ARG
-    assert lib.mgk_ls2d_set_landau(None, None, 0, 0.0, 0.1, 1.0) == L.BAD_ARG
+    assert lib.mgk_ls2d_set_landau(None, None, 0, 0.0, 0.1, 1.0, 0) == L.BAD_ARG
+    assert lib.mgk_ls2d_set_e33_out(None, 0, None) == L.BAD_ARG
 
 
 def test_landau_refusals_before_device_work():
@@ -59,8 +60,8 @@ def test_landau_refusals_before_device_work():
     mu = np.full((8, 8), 3e10)
     v = dict(v1=0.0, v2=0.0, v3=0.0, g1=0.0, g2=0.0, g3=0.0, g4=0.0)
     eb = np.zeros((2, 2))
-    with pytest.raises(NotImplementedError):
-        les.spectral_solver_landau_2d(lam, mu, **v, eps_bar=eb, plane_mode="plane_stress")
+    with pytest.raises(ValueError):
+        les.spectral_solver_landau_2d(lam, mu, **v, eps_bar=eb, plane_mode="plane_strian")
     with pytest.raises(NotImplementedError):
         les.spectral_solver_landau_2d(lam, mu, **v, eps_bar=eb, solver="newton_cg")
     with pytest.raises(NotImplementedError):
