@@ -64,6 +64,8 @@ def parse():
                     help="side of the finite-strain block (Neo-Hookean + F_p, 10 load steps); 0 skips it")
     ap.add_argument("--ensemble", type=int, default=96,
                     help="replicas of the batched KMC ensemble block (96 = the ensemble workload, ~1 min); 0 skips it")
+    ap.add_argument("--ensemble-ragged", type=int, default=1,
+                    help="1: also run the ensemble with every replica in one ragged plan; 0 skips it")
     ap.add_argument("--kmc-events", type=int, default=2000,
                     help="events of the 256^2 x 8 KMC/AQS block (2000 = the KMC workload); 0 skips it")
     ap.add_argument("--landau", type=int, default=1, help="1: the Landau 2D block (256^2, Anderson depth 5); 0 skips it")
@@ -777,10 +779,15 @@ def run_ours(a):
     ensemble = None
     if world == 1 and a.ensemble > 0:
         from mgkmc_b200.serving import ensemble_requests, run_ensemble
-        _, ensemble = run_ensemble(ensemble_requests(n_replicas=a.ensemble, n_events=500))
+        reqs = ensemble_requests(n_replicas=a.ensemble, n_events=500)
+        _, ensemble = run_ensemble(reqs)
         ensemble["workload"] = (f"{a.ensemble} 2D KMC/AQS replicas, sides uniform in {{128,192,256,384,512}}, "
                                 f"T uniform in [200, 400] K, seeds 0..{a.ensemble - 1}, 500 events each, mixed form, "
-                                f"one batched solve launch per size per round")
+                                f"one batched solve launch per size per round, the sizes on their own streams")
+        if a.ensemble_ragged:
+            _, rag = run_ensemble(reqs, ragged=True)
+            rag["workload"] = "the same replicas in one ragged plan: one launch per solver stage for all replicas"
+            ensemble["ragged"] = rag
     serving = None
     if world == 1 and a.serve_window > 0:
         serving = run_serving(a.serve_window, a.serve_plain)

@@ -134,19 +134,36 @@ class _Task:
 
 
 class _Bucket:
-    """One 2D grid size: a batched LS plan with ``slots`` replicas and a stream."""
+    """A batched 2D LS plan with a stream: ``slots`` replicas of side n, or
+    one replica per entry of ``sizes`` (a ragged bucket: replicas of several
+    sides advance in one launch per solver stage)."""
 
-    def __init__(self, torch, n, slots, precision):
+    def __init__(self, torch, n, slots, precision, sizes=None):
         from .linear_elastic_simulator import Ls2dBatch
         self.n = n
+        self.sizes = list(sizes) if sizes is not None else [n] * slots
         self.stream = torch.cuda.Stream()
-        self.plan = Ls2dBatch([(n, n)] * slots, precision=precision)
-        self.free = list(range(slots))[::-1]
+        self.plan = Ls2dBatch([(m, m) for m in self.sizes], precision=precision)
+        self.free_by = {}
+        for idx in range(len(self.sizes) - 1, -1, -1):
+            self.free_by.setdefault(self.sizes[idx], []).append(idx)
         self.tasks = []        # admitted tasks
         self.waiting = collections.deque()
         self.inflight = None   # tasks of the running round
         self.solving = []
         self.event = torch.cuda.Event()
+
+    def has_free(self, n):
+        return bool(self.free_by.get(n))
+
+    def take(self, n):
+        return self.free_by[n].pop()
+
+    def give(self, slot):
+        self.free_by[self.sizes[slot]].append(slot)
+
+    def nfree(self, n):
+        return len(self.free_by.get(n, ()))
 
 
 class _Bucket3:
@@ -172,7 +189,8 @@ def _by_tol(tasks):
 class Server:
     def __init__(self, mode="served", hbm_budget=None, slots=None, ls_tol=1e-8, ls_max_iter=500,
                  macro_tol=1e4, macro_max_iter=20, n_events=100, n_modes=8, q_mean=1.0, kmc_T=300.0,
-                 fs_strain=0.005, fs_tol_nw=1e-8, fs_tol_cg=1e-6, selection=None, device=None, traj_ls_tol=1e-6):
+                 fs_strain=0.005, fs_tol_nw=1e-8, fs_tol_cg=1e-6, selection=None, device=None, traj_ls_tol=1e-6,
+                 ragged=None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("mgkmc_b200 needs a CUDA device (no CPU fallback)")
@@ -196,6 +214,9 @@ class Server:
         self.hbm_budget = hbm_budget
         self.slots = dict(slots) if slots else {64: 32, 128: 32, 256: 32, 512: 16, 768: 8, 1024: 8}
         self.slots3 = {64: 8, 96: 4, 128: 2}
+        # ragged: sides of the slots of one bucket shared by every 2D request
+        # (None: one bucket per side)
+        self.ragged = list(ragged) if ragged is not None else None
         self.buckets = {}
         self.buckets3 = {}
         self.fs_plans = {}
@@ -218,7 +239,34 @@ class Server:
     def _now(self):
         return time.perf_counter() - self._t0
 
+    def _prepare_ragged(self):
+        """The ragged bucket: the kernel family picked by timing one replica
+        of each side, then one solve of those (graph set-up)."""
+        torch = self.torch
+        b = self._bucket(None)
+        with torch.cuda.stream(b.stream):
+            reps, ebs, outs = [], [], []
+            for n in sorted(set(b.sizes)):
+                r = b.sizes.index(n)
+                E, nu, ep, eb = W.ls2d_problem_dev(n, n, 0, self.dev)
+                b.plan.set_material(r, E, nu, ep, stream=b.stream)
+                reps.append(r)
+                ebs.append(eb)
+                outs.append(torch.empty((n, n, 2, 2), dtype=torch.float64, device=self.dev))
+            key = ("ragged", tuple(b.sizes), self.precision)
+            if key not in _TUNED:
+                _TUNED[key] = b.plan.autotune(reps, ebs, stream=b.stream)
+            else:
+                b.plan.set_family(_TUNED[key][0])
+            b.plan.solve(reps, ebs, outs, [None] * len(reps), max_iter=self.ls_max_iter, tol=self.ls_tol,
+                         sync=True, stream=b.stream)
+
     def _bucket(self, n):
+        if self.ragged is not None:  # one bucket for every 2D request
+            b = self.buckets.get("ragged")
+            if b is None:
+                b = self.buckets["ragged"] = _Bucket(self.torch, 0, 0, self.precision, sizes=self.ragged)
+            return b
         b = self.buckets.get(n)
         if b is None:
             k = self.slots.get(n, 4) if self.served else 1
@@ -414,7 +462,7 @@ class Server:
     def _admit(self, b, req):
         res = self.results[req.rid]
         nbytes = footprint_bytes(req, self.n_modes)
-        slot = b.free.pop()
+        slot = b.take(req.n)
         self.used += nbytes
         res.t_admit = self._now()
         with self.torch.cuda.stream(b.stream):
@@ -422,7 +470,7 @@ class Server:
         b.tasks.append(_Task(req, res, gen, slot, nbytes))
 
     def _release(self, b, t):
-        b.free.append(t.slot)
+        b.give(t.slot)
         self.used -= t.bytes
 
     def _start_round(self, b):
@@ -516,22 +564,25 @@ class Server:
         so that plan set-up and graph instantiation happen before the first
         arrival (a server is started before its traffic)."""
         torch = self.torch
-        for n in sorted({r.n for r in requests if r.dim == 2}):
+        if self.ragged is not None:
+            self._prepare_ragged()
+        for n in sorted({r.n for r in requests if r.dim == 2} if self.ragged is None else ()):
             b = self._bucket(n)
             with torch.cuda.stream(b.stream):
                 E, nu, ep, eb = W.ls2d_problem_dev(n, n, 0, self.dev)
                 eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=self.dev)
-                for k in range(min(4, len(b.free))):
+                nf = b.nfree(n)
+                for k in range(min(4, nf)):
                     b.plan.set_material(k, E, nu, ep, stream=b.stream)
-                k = min(4, len(b.free))
+                k = min(4, nf)
                 if self.served:
                     # kernel family picked by measurement, once per (side, slots, precision)
-                    key = (n, len(b.free), self.precision)
+                    key = (n, nf, self.precision)
                     if key not in _TUNED:
                         _TUNED[key] = b.plan.autotune(list(range(k)), [eb] * k, stream=b.stream)
                     else:
                         b.plan.set_family(_TUNED[key][0])
-                for k in range(1, min(4, len(b.free)) + 1):
+                for k in range(1, min(4, nf) + 1):
                     b.plan.solve(list(range(k)), [eb] * k, [eps] * k, [None] * k, max_iter=self.ls_max_iter,
                                  tol=self.ls_tol, sync=True, stream=b.stream)
         for n in sorted({r.n for r in requests if r.dim == 3 and r.kind == "solve"}):
@@ -592,7 +643,7 @@ class Server:
                         self._bucket(r.n).waiting.append(r)
                 progressed = False
                 for b in self.buckets.values():
-                    while b.waiting and b.free and (self.used + footprint_bytes(b.waiting[0], self.n_modes)
+                    while b.waiting and b.has_free(b.waiting[0].n) and (self.used + footprint_bytes(b.waiting[0], self.n_modes)
                                                     <= self.hbm_budget or not b.tasks):
                         self._admit(b, b.waiting.popleft())
                     if b.inflight is not None and b.event.query():
@@ -674,12 +725,17 @@ def ensemble_requests(n_replicas=96, sizes=(128, 192, 256, 384, 512), T_range=(2
     return out
 
 
-def run_ensemble(requests, slots=None, **server_kw):
+def run_ensemble(requests, slots=None, ragged=False, **server_kw):
     """Runs an ensemble through the served form (every replica admitted at
-    once when slots allow; one batched solve launch per size per round) and
-    returns (results, summary with events/s)."""
+    once when slots allow) and returns (results, summary with events/s).
+    ragged=False: one bucket per side, one batched solve launch per side per
+    round, the sides' buckets on their own streams; True: one ragged bucket
+    with a slot per replica, one launch per solver stage for all replicas of
+    a round."""
     from collections import Counter
     cnt = Counter(r.n for r in requests)
+    if ragged:
+        server_kw["ragged"] = sorted(r.n for r in requests)
     srv = Server(mode="served", slots=slots or {n: c for n, c in cnt.items()}, **server_kw)
     srv.prepare(requests)
     t0 = time.perf_counter()

@@ -89,3 +89,17 @@ def test_ensemble_runs_every_replica_to_its_event_count():
     assert all(len(r.out["events"]) == 4 for r in res)
     alone = Server(mode="served", n_events=4, q_mean=0.6, slots={64: 1, 96: 1}).run([reqs[2]], realtime=False)[0]
     assert alone.out["events"] == res[2].out["events"]
+
+
+def test_ragged_ensemble_matches_per_size_buckets():
+    # one ragged plan (every replica's solve in one launch per stage) gives
+    # each replica the trajectory it has in the per-size buckets
+    import numpy as np
+    from mgkmc_b200.serving import ensemble_requests, run_ensemble
+    reqs = ensemble_requests(n_replicas=6, sizes=(64, 96, 128), T_range=(300.0, 400.0), n_events=4)
+    per, _ = run_ensemble(reqs, q_mean=0.6)
+    rag, summ = run_ensemble(reqs, ragged=True, q_mean=0.6)
+    assert summ["completed"] == 6 and summ["events"] == 24
+    for a, b in zip(per, rag):
+        assert a.out["events"] == b.out["events"]
+        assert np.array_equal(a.out["eps_macro"], b.out["eps_macro"])
