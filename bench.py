@@ -81,11 +81,12 @@ def parse():
                     help="seconds of the oracle's per-event KMC loop at 256^2 x 8 on one host core; 0 skips it")
     ap.add_argument("--cpu-fs-grid", type=int, default=32,
                     help="side of the oracle's finite-strain load step on one host core; 0 skips it")
-    ap.add_argument("--profile-case", default="", choices=["", "ls3d", "fs3d", "kmc"],
+    ap.add_argument("--profile-case", default="", choices=["", "ls3d", "fs3d", "kmc", "landau"],
                     help="run one kernel-profiling workload instead of the benchmark (for ncu captures): ls3d = "
                          "LS 3D solves at --profile-n^3 (tol 1e-8, three solves), fs3d = one finite-strain load "
                          "step at --profile-n^3 (Neo-Hookean + 2 %% F_p, F_xx = 1.005), kmc = three rounds of "
-                         "barrier, exact rates/total and selection at --profile-n^2 x 8 modes")
+                         "barrier, exact rates/total and selection at --profile-n^2 x 8 modes, landau = three Landau "
+                         "LS 2D solves at --profile-n^2 (Anderson depth 5, tol 1e-8)")
     ap.add_argument("--profile-n", type=int, default=128)
     ap.add_argument("--profile-precision", default="fp64", choices=["fp64", "mixed"])
     a = ap.parse_args()
@@ -851,7 +852,11 @@ def run_profile_case(a):
     from mgkmc_b200 import workloads as W
     n, prec = a.profile_n, a.profile_precision
     dev = torch.device("cuda", 0)
-    if a.profile_case == "ls3d":
+    if a.profile_case == "landau":
+        for _ in range(3):
+            solve_ms, iters, _ = _landau_device(n, 5, reps=1)
+        print(f"landau {n}^2 depth 5: {iters} iterations, {solve_ms:.3f} ms", flush=True)
+    elif a.profile_case == "ls3d":
         from mgkmc_b200.linear_elastic_simulator import Ls3dBatch
         rng = np.random.default_rng(21)
         E, nu = W.ls3d_material(n, n, n, rng)
