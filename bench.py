@@ -423,7 +423,16 @@ def run_serving(window, n_plain=0, progress=None):
             services.append(float(rng.choice(pool)))
             estimated += 1
     lat = _fifo([r.t_arrival for r in reqs], services)
-    plain.update(latency_p50_s=float(np.percentile(lat, 50)), latency_p99_s=float(np.percentile(lat, 99)),
+    # the whole window's plain busy time and solves: measured where measured;
+    # elsewhere the class's service time and the served run's solve count of
+    # the request (both forms run the same macro-loop solves)
+    plain_solves = {r.rid: r.solves for r in ok}
+    served_solves = {r.rid: r.solves for r in res}
+    win_solves = sum(plain_solves.get(r.rid, served_solves.get(r.rid, 0)) for r in reqs)
+    win_busy = float(np.sum(services))
+    plain.update(window_solves=int(win_solves), window_busy_s=win_busy,
+                 window_solves_per_busy_s=win_solves / max(win_busy, 1e-9),
+                 latency_p50_s=float(np.percentile(lat, 50)), latency_p99_s=float(np.percentile(lat, 99)),
                  makespan_s=float(reqs[-1].t_arrival + lat[-1] - reqs[0].t_arrival) if len(lat) else 0.0,
                  service_times="measured for every request" if estimated == 0 else
                  f"measured for {len(reqs) - estimated}, drawn from the measured times of the same class for "
@@ -435,6 +444,7 @@ def run_serving(window, n_plain=0, progress=None):
     a = out["served_mixed"]
     if a.get("completed"):
         out["solves_per_s_ratio"] = a["solves_per_s"] / plain["solves_per_busy_s"]
+        out["solves_per_s_ratio_window"] = a["solves_per_s"] / plain["window_solves_per_busy_s"]
         out["p50_ratio"] = plain["latency_p50_s"] / a["p50_s"]
         out["p99_ratio"] = plain["latency_p99_s"] / a["p99_s"]
     return out

@@ -419,9 +419,12 @@ class Server:
                 t.send = None
 
     def _traj3_worker(self, q):
-        """Admits 3D trajectories into free slots of their size and advances
-        the admitted ones in rounds until the queue is closed and all are done."""
+        """Admits the 3D trajectories of its queue into free slots of their
+        size and advances the admitted ones in rounds until the queue is
+        closed and all are done.  A worker advances only the buckets its own
+        requests went to."""
         waiting = collections.deque()
+        mine = []
         closed = False
         while True:
             try:
@@ -436,6 +439,8 @@ class Server:
             still = collections.deque()
             for r in waiting:
                 b = self._bucket3(r.n)
+                if b not in mine:
+                    mine.append(b)
                 if b.free:
                     res = self.results[r.rid]
                     res.t_admit = self._now()
@@ -446,7 +451,7 @@ class Server:
                 else:
                     still.append(r)
             waiting = still
-            active = [b for b in self.buckets3.values() if b.tasks]
+            active = [b for b in mine if b.tasks]
             if not active:
                 if closed and not waiting:
                     return
@@ -621,14 +626,17 @@ class Server:
         torch = self.torch
         pending = collections.deque(order)
         fs_q = queue.Queue()
-        t3_q = queue.Queue()
         fs_stream = torch.cuda.Stream()
         worker = threading.Thread(target=self._fs_worker, args=(fs_q, fs_stream), daemon=True)
-        worker3 = threading.Thread(target=self._traj3_worker, args=(t3_q,), daemon=True)
+        # one 3D-trajectory worker per side: a side's rounds (synchronous
+        # batched solves) do not wait behind another side's
+        t3_qs = {n: queue.Queue() for n in sorted({r.n for r in order if r.dim == 3 and r.kind == "trajectory"})}
+        workers3 = [threading.Thread(target=self._traj3_worker, args=(q,), daemon=True) for q in t3_qs.values()]
         n3d = sum(1 for r in order if r.dim == 3)
         self._t0 = time.perf_counter()
         worker.start()
-        worker3.start()
+        for w in workers3:
+            w.start()
         done3d = lambda: sum(1 for r in self.results.values() if r.dim == 3 and r.t_done > 0)
         try:
             while True:
@@ -638,7 +646,7 @@ class Server:
                     if not realtime:
                         self.results[r.rid].t_arrival = now
                     if r.dim == 3:
-                        (t3_q if r.kind == "trajectory" else fs_q).put(r)
+                        (t3_qs[r.n] if r.kind == "trajectory" else fs_q).put(r)
                     else:
                         self._bucket(r.n).waiting.append(r)
                 progressed = False
@@ -663,9 +671,11 @@ class Server:
                         time.sleep(2e-5)
         finally:
             fs_q.put(None)
-            t3_q.put(None)
+            for q in t3_qs.values():
+                q.put(None)
             worker.join()
-            worker3.join()
+            for w in workers3:
+                w.join()
 
     def _run_sequential(self, order, realtime):
         torch = self.torch
