@@ -297,14 +297,18 @@ __device__ __forceinline__ LandauScal landau_scal(double mu, double lam, double 
 }
 
 // The Landau small-strain stress of a 2D voxel (elasticity.py:487-639).
-// Plane strain: e33 = 0.  Plane stress (ps): e33 from Newton steps on
-// sigma33 = 0 (:571-616) from the linear guess -lam/(lam + 2 mu) tr a, at
-// most 20, until the voxel's step is below 1e-9; the stress is evaluated at
-// the stepped e33.  The reference runs the steps of all voxels together
-// until every step is below 1e-9, evaluates each voxel before its last step
-// and warm-starts the next call from the stepped field; its solver's fixed
-// point is the one where e33 solves sigma33 = 0, as here.  e33_out (may be
-// null) receives e33.
+// Plane strain: e33 = 0.  Plane stress (ps): e33 from the reference's Newton
+// steps on sigma33 = 0 (:571-616) from the linear guess
+// -lam/(lam + 2 mu) tr a, here until the voxel's step is below 1e-14 (at
+// most 64 steps); the stress is evaluated at the stepped e33.  The
+// reference runs the steps of all voxels together until every step is below
+// 1e-9, evaluates each voxel before its last step and warm-starts the next
+// call from the stepped field, so across its solver's iterations e33
+// converges to the root of sigma33 = 0, which the kernel solves for at
+// every evaluation.  With capping the step's derivative leaves out the
+// capping factor's dependence on e33 and the steps converge linearly, so a
+// single cold solve stopped at 1e-9 would leave ~1e-10 in e33.  e33_out
+// (may be null) receives e33.
 __device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, double a22, double a12, double a21,
                                              const double* __restrict__ lp, int ps, double& s11, double& s22,
                                              double& s12, double& s21, double* e33_out = nullptr) {
@@ -313,7 +317,7 @@ __device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, 
     const double v1 = lp[0], v2 = lp[1], g1 = lp[3], g2 = lp[4], g3 = lp[5], g4 = lp[6];
     const double Gt = lp[9] * mu;
     e33 = -lam / (lam + 2.0 * mu) * (a11 + a22);
-    for (int it = 0; it < 20; ++it) {
+    for (int it = 0; it < 64; ++it) {
       const LandauScal t = landau_scal(mu, lam, a11, a22, a12, a21, e33, lp);
       const double c33 = t.c33, I1 = t.I1, I2 = t.I2;
       double s33 = t.cI + t.ce * c33 + t.ce2 * (c33 * c33);
@@ -327,7 +331,7 @@ __device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, 
       }
       const double delta = -s33 / (ds33 + 1e-12);
       e33 = e33 + delta;
-      if (!(fabs(delta) >= 1e-9)) break;  // also leaves on NaN, which the stress then carries
+      if (!(fabs(delta) >= 1e-14)) break;  // also leaves on NaN, which the stress then carries
     }
     if (e33_out) *e33_out = e33;
   }
