@@ -326,6 +326,26 @@ def landau_stress_2d(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1
     return sig
 
 
+def landau_stress_2d_root(e, lam, mu, v, cap_type=None, cap_limit=None, cap_ratio=0.1, cap_power=1.0):
+    """The plane-stress Landau stress at the root of sigma33 = 0: the
+    reference's Newton steps (landau_stress_2d) repeated from the stepped e33
+    until no voxel's e33 moves by 1e-15, from the linear guess; the stress of
+    the last evaluation.  The reference reaches this state only over its
+    solver's iterations (its e33 lags by its last step); the GPU kernels
+    solve for it at every evaluation."""
+    a11, a22 = e[..., 0, 0], e[..., 1, 1]
+    e33 = -lam / (lam + 2.0 * mu) * (a11 + a22)
+    sig = None
+    for _ in range(200):
+        st = {"e33": e33}
+        sig = landau_stress_2d(e, lam, mu, v, cap_type, cap_limit, cap_ratio, cap_power, True, st)
+        moved = np.max(np.abs(st["e33"] - e33))
+        e33 = st["e33"]
+        if moved < 1e-15:
+            break
+    return sig
+
+
 def anderson_step(hist_g, hist_f, g, f, m):
     """Type-II Anderson mixing of the last m + 1 fixed-point images and
     residuals (mgkmc/linear_elastic_simulator.py:1185-1209): returns the next
@@ -352,9 +372,11 @@ def anderson_step(hist_g, hist_f, g, f, m):
 
 def spectral_solver_landau_2d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=400, tol=1e-6, pixel=1.0,
                               eps_init=None, anderson_m=5, cap_type=None, cap_limit=None, cap_ratio=0.1,
-                              cap_power=1.0, return_info=False, plane_stress=False, e33_state=None):
+                              cap_power=1.0, return_info=False, plane_stress=False, e33_state=None,
+                              e33_root=False):
     """Landau small-strain LS fixed point (plane strain, or plane stress with
-    the e33 Newton solve and its warm state e33_state), the basic scheme
+    the e33 Newton solve and its warm state e33_state; e33_root: e33 solved
+    to its root at every evaluation instead), the basic scheme
     with Anderson mixing (mgkmc/linear_elastic_simulator.py:952-1228, solver
     "dbfft"): medium (mean lam, mean mu) fixed; G(eps) = eps_bar + Gamma0 *
     (sigma_L(eps - eps_p) - C0:eps) with zero-mean fluctuation; stop when
@@ -370,8 +392,12 @@ def spectral_solver_landau_2d(lam, mu, v, eps_bar, eps_plastic=None, max_iter=40
     else:
         eps = np.broadcast_to(eps_bar, shape + (2, 2)).copy()
     ep = eps_plastic
-    law = lambda x: landau_stress_2d(x - ep if ep is not None else x, lam, mu, v, cap_type, cap_limit, cap_ratio,
-                                     cap_power, plane_stress, e33_state)
+    if plane_stress and e33_root:  # e33 at the root at every evaluation
+        law = lambda x: landau_stress_2d_root(x - ep if ep is not None else x, lam, mu, v, cap_type, cap_limit,
+                                              cap_ratio, cap_power)
+    else:
+        law = lambda x: landau_stress_2d(x - ep if ep is not None else x, lam, mu, v, cap_type, cap_limit, cap_ratio,
+                                         cap_power, plane_stress, e33_state)
     hg, hf = [], []
     it_done, diff = 0, np.inf
     for it in range(max_iter):

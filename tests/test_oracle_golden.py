@@ -331,3 +331,16 @@ def test_landau_plane_stress_law_and_solver(golden):
                                          anderson_m=5, cap_type=ct, cap_limit=cl, plane_stress=True, e33_state=st)
         assert np.max(np.abs(o[0] - g[f"eps_{tag}"])) < 1e-9 * np.max(np.abs(g[f"eps_{tag}"]))
         assert np.max(np.abs(o[1] - g[f"sig_{tag}"])) < 1e-9 * np.max(np.abs(g[f"sig_{tag}"]))
+
+
+def test_landau_plane_stress_root_fixed_point_matches_reference(golden):
+    # e33 solved to its root at every evaluation (as the GPU kernels do)
+    # reaches the reference's fixed point within 1e-9 on its own fixtures
+    from oracle import ls as OL
+    g = golden("ls2d_landau_pstress_16x12")
+    v = tuple(g["v"])
+    for tag, (ct, cl) in (("solve", (None, None)), ("solve_cap", ("piecewise", 0.01))):
+        o = OL.spectral_solver_landau_2d(g["lam"], g["mu"], v, g["eps_bar"], g["eps_plastic"], max_iter=400, tol=1e-12,
+                                         anderson_m=5, cap_type=ct, cap_limit=cl, plane_stress=True, e33_root=True)
+        assert np.max(np.abs(o[0] - g[f"eps_{tag}"])) < 1e-9 * np.max(np.abs(g[f"eps_{tag}"]))
+        assert np.max(np.abs(o[1] - g[f"sig_{tag}"])) < 1e-9 * np.max(np.abs(g[f"sig_{tag}"]))
