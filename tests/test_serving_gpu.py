@@ -93,7 +93,9 @@ def test_ensemble_runs_every_replica_to_its_event_count():
 
 def test_ragged_ensemble_matches_per_size_buckets():
     # one ragged plan (every replica's solve in one launch per stage) gives
-    # each replica the trajectory it has in the per-size buckets
+    # each replica the trajectory it has in the per-size buckets (the
+    # autotuner may pick another kernel family for the ragged plan, so the
+    # fields agree to rounding, the events exactly)
     import numpy as np
     from mgkmc_b200.serving import ensemble_requests, run_ensemble
     reqs = ensemble_requests(n_replicas=6, sizes=(64, 96, 128), T_range=(300.0, 400.0), n_events=4)
@@ -102,4 +104,4 @@ def test_ragged_ensemble_matches_per_size_buckets():
     assert summ["completed"] == 6 and summ["events"] == 24
     for a, b in zip(per, rag):
         assert a.out["events"] == b.out["events"]
-        assert np.array_equal(a.out["eps_macro"], b.out["eps_macro"])
+        assert np.allclose(a.out["eps_macro"], b.out["eps_macro"], rtol=1e-9, atol=0)
