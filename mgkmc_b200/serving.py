@@ -625,17 +625,18 @@ class Server:
     def _run_served(self, order, realtime):
         torch = self.torch
         pending = collections.deque(order)
-        fs_q = queue.Queue()
-        fs_stream = torch.cuda.Stream()
-        worker = threading.Thread(target=self._fs_worker, args=(fs_q, fs_stream), daemon=True)
+        # one finite-strain worker per side, each with its plan and stream:
+        # load steps of different sides overlap on the device
+        fs_qs = {n: queue.Queue() for n in sorted({r.n for r in order if r.dim == 3 and r.kind == "solve"})}
+        workers_fs = [threading.Thread(target=self._fs_worker, args=(q, torch.cuda.Stream()), daemon=True)
+                      for q in fs_qs.values()]
         # one 3D-trajectory worker per side: a side's rounds (synchronous
         # batched solves) do not wait behind another side's
         t3_qs = {n: queue.Queue() for n in sorted({r.n for r in order if r.dim == 3 and r.kind == "trajectory"})}
         workers3 = [threading.Thread(target=self._traj3_worker, args=(q,), daemon=True) for q in t3_qs.values()]
         n3d = sum(1 for r in order if r.dim == 3)
         self._t0 = time.perf_counter()
-        worker.start()
-        for w in workers3:
+        for w in workers_fs + workers3:
             w.start()
         done3d = lambda: sum(1 for r in self.results.values() if r.dim == 3 and r.t_done > 0)
         try:
@@ -646,7 +647,7 @@ class Server:
                     if not realtime:
                         self.results[r.rid].t_arrival = now
                     if r.dim == 3:
-                        (t3_qs[r.n] if r.kind == "trajectory" else fs_q).put(r)
+                        (t3_qs if r.kind == "trajectory" else fs_qs)[r.n].put(r)
                     else:
                         self._bucket(r.n).waiting.append(r)
                 progressed = False
@@ -670,11 +671,9 @@ class Server:
                     else:
                         time.sleep(2e-5)
         finally:
-            fs_q.put(None)
-            for q in t3_qs.values():
+            for q in list(fs_qs.values()) + list(t3_qs.values()):
                 q.put(None)
-            worker.join()
-            for w in workers3:
+            for w in workers_fs + workers3:
                 w.join()
 
     def _run_sequential(self, order, realtime):
