@@ -132,38 +132,46 @@ def _rng_from_json(s):
 
 
 def save_trajectory(path, sim, rng, step=None, fmt=None, pixel=1.0):
-    """Checkpoint of a device-resident 2D KMC/AQS trajectory (``Kmc2D``)
-    between AQS steps, in the layout of mgkmc/aqs.py:1207-1267 plus the
-    ``resume`` group.  ``rng`` is the Generator the trajectory draws from."""
+    """Checkpoint of a device-resident KMC/AQS trajectory (``Kmc2D``, or
+    ``Kmc3D``: the reference's own 3D layout) between AQS steps, in the
+    layout of mgkmc/aqs.py:1207-1267 plus the ``resume`` group.  ``rng`` is
+    the Generator the trajectory draws from."""
     st = sim.state_dict()
     p = sim.p
-    nx, ny, M = sim.nx, sim.ny, sim.M
+    three_d = hasattr(sim, "nz")
+    shape = (sim.nx, sim.ny, sim.nz) if three_d else (sim.nx, sim.ny)
+    M = sim.M
     groups = {"fields/eps_field": st["eps"], "fields/sig_field": st["sig"], "fields/E_field": st["E"],
-              "fields/nu_field": st["nu"], "fields/Tlocal": np.full((nx, ny), float(p["T"])),
+              "fields/nu_field": st["nu"], "fields/Tlocal": np.full(shape, float(p["T"])),
               "grid/eps_plastic": st["eps_p"], "grid/soft_prop": st["soft"], "grid/Q": st["Q"],
               "grid/Q0": st["Q0"], "grid/catalog": st["catalog"], "grid/last_event_time": st["t_last"],
               "state/eps_macro": st["eps_macro"], "resume/prev_strain_dir": st["prev"]}
-    ev = np.array([(x, y, m) for x, y, m, _ in st["events"]], dtype=np.int32).reshape(-1, 3)
+    nsite = 4 if three_d else 3  # (x, y, [z,] m) per flip
+    ev = np.array([e[:nsite] for e in st["events"]], dtype=np.int32).reshape(-1, nsite)
     groups["history/flips"] = ev
-    groups["resume/event_times"] = np.array([t for *_, t in st["events"]], dtype=np.float64)
-    meta = {"nx": nx, "ny": ny, "nz": 1, "M": M, "gamma0": p["gamma0"], "pixel": pixel,
-            "timestamp": datetime.datetime.now().isoformat(), "step": int(st["steps_done"] if step is None else step),
-            "sim_time": st["time"], "nu0": p["nu0"], "temperature": p["T"], "strain_rate": p["strain_rate"],
-            "stability_threshold": sim.stability_threshold, "jp": p["jp"], "jt": p["jt"],
+    groups["resume/event_times"] = np.array([e[nsite] for e in st["events"]], dtype=np.float64)
+    meta = {"nx": sim.nx, "ny": sim.ny, "nz": sim.nz if three_d else 1, "M": M, "gamma0": p["gamma0"],
+            "pixel": pixel, "timestamp": datetime.datetime.now().isoformat(),
+            "step": int(st["steps_done"] if step is None else step), "sim_time": st["time"], "nu0": p["nu0"],
+            "temperature": p["T"], "strain_rate": p["strain_rate"], "jp": p["jp"], "jt": p["jt"],
             "neighbor_softening_fraction": p["jn"], "softening_cap": p["cap"], "softening_scheme": 0,
             "scale_rate_by_volume": True, "enable_thermal": False}
+    if hasattr(sim, "stability_threshold"):
+        meta["stability_threshold"] = sim.stability_threshold
     resume = {"steps_done": int(st["steps_done"]), "n_solves": int(st["n_solves"]),
               "rng_state": _rng_state_json(rng), "selection": sim.selection, "ls_start": sim.ls_start,
-              "precision": getattr(sim.ls, "precision", "fp64"), "unit_ready": int(st["unit_ready"]),
-              "flips_since_sync": int(st["flips_since_sync"])}
+              "precision": getattr(sim.ls, "precision", "fp64"), "unit_ready": int(st.get("unit_ready", 0)),
+              "flips_since_sync": int(st.get("flips_since_sync", 0))}
     return write(path, groups, {"metadata": meta, "resume": resume}, fmt)
 
 
 def load_trajectory(path):
-    """(state dict for ``Kmc2D.load_state_dict``, numpy Generator, metadata)."""
+    """(state dict for ``Kmc2D.load_state_dict`` or ``Kmc3D.load_state_dict``,
+    numpy Generator, metadata)."""
     data, attrs = load(path)
     meta, res = attrs.get("metadata", {}), attrs.get("resume", {})
-    ev = data["history/flips"].reshape(-1, 3)
+    ev = data["history/flips"]
+    nsite = ev.shape[1] if ev.ndim == 2 else 3
     times = data["resume/event_times"]
     st = {"eps": data["fields/eps_field"], "sig": data["fields/sig_field"], "E": data["fields/E_field"],
           "nu": data["fields/nu_field"], "eps_p": data["grid/eps_plastic"], "soft": data["grid/soft_prop"],
@@ -172,6 +180,6 @@ def load_trajectory(path):
           "eps_macro": data["state/eps_macro"], "time": float(meta["sim_time"]),
           "steps_done": int(res["steps_done"]), "n_solves": int(res["n_solves"]),
           "unit_ready": bool(res.get("unit_ready", 0)), "flips_since_sync": int(res.get("flips_since_sync", 0)),
-          "events": [(int(a), int(b), int(c), float(t)) for (a, b, c), t in zip(ev, times)]}
+          "events": [tuple(int(v) for v in e) + (float(t),) for e, t in zip(ev.reshape(-1, nsite), times)]}
     rng = _rng_from_json(str(res["rng_state"]))
     return st, rng, meta

@@ -135,6 +135,35 @@ class Kmc3D:
         self.n_solves = 0
         self.steps_done = 0
         self.host_result = True
+        self._resume = False
+
+    _FIELDS = ("E", "nu", "eps", "sig", "eps_p", "soft", "Q", "Q0", "catalog", "t_last", "prev")
+
+    def state_dict(self):
+        """Host copies of the trajectory state between AQS steps (the fields,
+        the clock, the macro strain, the event list and counters)."""
+        self.stream.synchronize()
+        st = {k: getattr(self, k).cpu().numpy() for k in self._FIELDS}
+        st.update(eps_macro=self.eps_macro.copy(), time=self.time, events=list(self.events),
+                  n_solves=self.n_solves, steps_done=self.steps_done)
+        return st
+
+    def load_state_dict(self, st):
+        """Restores a state from ``state_dict`` (same grid, modes and
+        material); the next ``trajectory`` continues from it without the
+        initial re-solve (the stored fields are that solve's result)."""
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            for k in self._FIELDS:
+                getattr(self, k).copy_(torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float64)).to(self.dev))
+        self.ls.set_eigenstrain(self.rep, self.eps_p, stream=self.stream)
+        self.eps_macro = np.array(st["eps_macro"], dtype=np.float64).reshape(3, 3)
+        self.time = float(st["time"])
+        self.events = [tuple(e) for e in st["events"]]
+        self.n_solves = int(st["n_solves"])
+        self.steps_done = int(st["steps_done"])
+        self._resume = True
+        self.stream.synchronize()
 
     @property
     def E_avg(self):
@@ -208,7 +237,10 @@ class Kmc3D:
                                                                     p["q_min"])
         unit = np.zeros((3, 3))
         unit[self.component] = 1.0
-        self.after_solve((yield ("solve",)))
+        if self._resume:  # the restored fields are the last solve's result
+            self._resume = False
+        else:
+            self.after_solve((yield ("solve",)))
         dt_step = abs(p["step_size"]) / p["strain_rate"] if p["strain_rate"] > 0 else 1.0
         remaining = 0.0
         steps_done = self.steps_done

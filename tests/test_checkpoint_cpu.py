@@ -37,3 +37,40 @@ def test_rng_state_roundtrip():
     h = C._rng_from_json(C._rng_state_json(g))
     np.testing.assert_array_equal(g.random(5), h.random(5))
     np.testing.assert_array_equal(g.normal(size=3), h.normal(size=3))
+
+
+class _Fake3D:
+    """A stand-in for Kmc3D's checkpoint surface (no device needed)."""
+
+    def __init__(self, rng):
+        self.nx, self.ny, self.nz, self.M = 4, 3, 2, 2
+        sh = (4, 3, 2)
+        self.p = dict(T=300.0, gamma0=0.1, nu0=1e13, strain_rate=1e7, jp=0.0, jt=0.0, jn=0.0, cap=2.0)
+        self.selection, self.ls_start = "fast", "warm"
+        self.ls = type("P", (), {"precision": "mixed"})()
+        self._st = {"E": rng.random(sh), "nu": rng.random(sh), "eps": rng.random(sh + (3, 3)),
+                    "sig": rng.random(sh + (3, 3)), "eps_p": rng.random(sh + (3, 3)), "soft": rng.random(sh + (4,)),
+                    "Q": rng.random(sh + (2,)), "Q0": rng.random(sh + (2,)), "catalog": rng.random(sh + (2, 3, 3)),
+                    "t_last": rng.random(sh), "prev": rng.random(sh + (3, 3)), "eps_macro": rng.random((3, 3)),
+                    "time": 1.25e-9, "events": [(1, 2, 0, 1, 3.0e-10), (3, 0, 1, 0, 9.5e-10)], "n_solves": 17,
+                    "steps_done": 5}
+
+    def state_dict(self):
+        return dict(self._st)
+
+
+def test_trajectory_roundtrip_3d(tmp_path):
+    # the 3D trajectory checkpoint: the reference's aqs.py layout (flips as
+    # (x, y, z, m)) plus the resume group, read back into a state dict
+    rng = np.random.default_rng(2)
+    sim = _Fake3D(rng)
+    g = np.random.default_rng(99)
+    g.random(3)
+    path = C.save_trajectory(str(tmp_path / "t3"), sim, g, fmt="npz")
+    data, attrs = C.load(path)
+    assert data["history/flips"].shape == (2, 4) and attrs["metadata"]["nz"] == 2
+    st, rng2, meta = C.load_trajectory(path)
+    for k in ("eps", "sig", "eps_p", "soft", "Q", "Q0", "catalog", "t_last", "prev", "eps_macro", "E", "nu"):
+        np.testing.assert_array_equal(st[k], sim._st[k])
+    assert st["events"] == sim._st["events"] and st["steps_done"] == 5 and st["n_solves"] == 17
+    np.testing.assert_array_equal(rng2.random(4), g.random(4))

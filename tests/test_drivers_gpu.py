@@ -172,6 +172,36 @@ def test_checkpoint_resume_is_bit_exact(tmp_path, selection, ls_start, precision
     assert res["time"] == full["time"] and res["solves"] == full["solves"]
 
 
+@pytest.mark.parametrize("selection,ls_start,precision", [("exact", "cold", "fp64"), ("fast", "warm", "mixed")])
+def test_kmc3d_checkpoint_resume_is_bit_exact(tmp_path, selection, ls_start, precision):
+    # a 3D trajectory checkpointed after 20 AQS steps (the reference's 3D
+    # layout plus the resume group) and resumed equals the uninterrupted run
+    from mgkmc_b200 import checkpoint as C
+    from mgkmc_b200.kmc3d import Kmc3D, in_plane_modes
+    n, M = 32, 8
+    rng0 = np.random.default_rng(4)
+    E, nu = W.ls3d_material(n, n, n, rng0)
+    cat = in_plane_modes(rng0.uniform(0.0, np.pi, (n, n, n, M)), 0.1)
+    Q0 = np.clip(rng0.normal(0.5, 0.15, (n, n, n, M)), 0.3, None)
+    kw = dict(step_size=1e-4, q_mean=0.5, selection=selection, ls_start=ls_start, precision=precision)
+    full = Kmc3D(E, nu, cat, Q0, **kw).run(np.random.default_rng(9), 40)
+    a = Kmc3D(E, nu, cat, Q0, **kw)
+    rng = np.random.default_rng(9)
+    a.run(rng, 20)
+    path = C.save_trajectory(str(tmp_path / "traj3"), a, rng)
+    st, rng2, meta = C.load_trajectory(path)
+    assert meta["step"] == 20 and meta["nz"] == n
+    b = Kmc3D(st["E"], st["nu"], st["catalog"], st["Q0"], **kw)
+    b.load_state_dict(st)
+    res = b.run(rng2, 40)
+    assert len(full["events"]) > 0
+    assert res["events"] == full["events"]
+    np.testing.assert_array_equal(res["sig"], full["sig"])
+    np.testing.assert_array_equal(res["eps_p"], full["eps_p"])
+    np.testing.assert_array_equal(res["eps_macro"], full["eps_macro"])
+    assert res["time"] == full["time"] and res["solves"] == full["solves"]
+
+
 def test_kmc3d_driver_matches_reference_trajectory(golden):
     # the reference's own 3D trajectory (ThermalSimulation.run_simulation,
     # small strain): 1348 events, identical modes, times to 1e-9
