@@ -1691,6 +1691,9 @@ __device__ void aa_lstsq_warp(Ls2dAA* aa, int k, double (*sa)[kAaMax], double (*
 // valid after this update; the last block to finish sums them, updates the
 // Gram matrix and solves the least-squares problem of the mix.
 constexpr int kAaThreads = 256, kAaWarps = kAaThreads / 32;
+// K: the history depth m, compile-time so that only m accumulator pairs
+// live in registers
+template <int K>
 __global__ void __launch_bounds__(kAaThreads) ls2d_aa_update_kernel(const Ls2dRep* reps, const Ls2dState* st,
                                                                     const int* sel, double* buf, Ls2dAA* aa, int m,
                                                                     double* part) {
@@ -1711,9 +1714,9 @@ __global__ void __launch_bounds__(kAaThreads) ls2d_aa_update_kernel(const Ls2dRe
   double* gp = buf + 2 * n3;
   double* dF = buf + 3 * n3;
   double* dG = dF + (size_t)m * n3;
-  double an[kAaMax], ar[kAaMax];
+  double an[K], ar[K];
 #pragma unroll
-  for (int j = 0; j < kAaMax; ++j) { an[j] = 0.0; ar[j] = 0.0; }
+  for (int j = 0; j < K; ++j) { an[j] = 0.0; ar[j] = 0.0; }
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
     const double w = i >= 2 * N ? 2.0 : 1.0;
     const double gi = R.eps[i], fi = gi - x[i];
@@ -1726,7 +1729,7 @@ __global__ void __launch_bounds__(kAaThreads) ls2d_aa_update_kernel(const Ls2dRe
     fp[i] = fi;
     gp[i] = gi;
 #pragma unroll
-    for (int j = 0; j < kAaMax; ++j)
+    for (int j = 0; j < K; ++j)
       if (j < ncols) {
         const double c = w * (j == slot ? df : dF[(size_t)j * n3 + i]);
         an[j] += c * df;
@@ -1736,7 +1739,7 @@ __global__ void __launch_bounds__(kAaThreads) ls2d_aa_update_kernel(const Ls2dRe
   // block partials in a fixed order: warp trees, then the warps in order
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int j = 0; j < kAaMax; ++j)
+  for (int j = 0; j < K; ++j)
     if (j < ncols) {
       const double a = warp_sum(an[j]), b = warp_sum(ar[j]);
       if (lane == 0) { wred[wid][j] = a; wred[wid][kAaMax + j] = b; }
@@ -2391,6 +2394,20 @@ static void launch_col(const LoopArgs& a, cudaStream_t s) {
   }
 }
 
+// the history kernel of depth m (1..kAaMax)
+static void* aa_update_fn(int m) {
+  switch (m) {
+    case 1: return (void*)ls2d_aa_update_kernel<1>;
+    case 2: return (void*)ls2d_aa_update_kernel<2>;
+    case 3: return (void*)ls2d_aa_update_kernel<3>;
+    case 4: return (void*)ls2d_aa_update_kernel<4>;
+    case 5: return (void*)ls2d_aa_update_kernel<5>;
+    case 6: return (void*)ls2d_aa_update_kernel<6>;
+    case 7: return (void*)ls2d_aa_update_kernel<7>;
+    default: return (void*)ls2d_aa_update_kernel<8>;
+  }
+}
+
 template <typename TS, bool FINAL>
 static int launch_body(const LoopArgs& a, cudaStream_t s) {
   launch_col<TS>(a, s);
@@ -2402,7 +2419,9 @@ static int launch_body(const LoopArgs& a, cudaStream_t s) {
     launch_row<TS, true, FINAL>(a, s);
   MGK_CUDA(cudaGetLastError());
   if (sizeof(TS) == 8 && a.aa_m > 0) {
-    ls2d_aa_update_kernel<<<a.aa_nb, kAaThreads, 0, s>>>(a.reps, a.st, a.sel, a.aa_buf, a.aa, a.aa_m, a.aa_part);
+    void* args[] = {(void*)&a.reps, (void*)&a.st, (void*)&a.sel, (void*)&a.aa_buf, (void*)&a.aa, (void*)&a.aa_m,
+                    (void*)&a.aa_part};
+    cudaLaunchKernel(aa_update_fn(a.aa_m), dim3(a.aa_nb), dim3(kAaThreads), args, 0, s);
     launch_row<TS, false, FINAL>(a, s);  // the mix and tau of the mixed iterate
     MGK_CUDA(cudaGetLastError());
   }
@@ -2462,7 +2481,7 @@ static int add_while(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t
     memset(&k3, 0, sizeof(k3));
     memset(&k6, 0, sizeof(k6));
     void* a3[] = {&a.reps, &a.st, &a.sel, &a.aa_buf, &a.aa, &a.aa_m, &a.aa_part};
-    k3.func = (void*)ls2d_aa_update_kernel;
+    k3.func = aa_update_fn(a.aa_m);
     k3.gridDim = dim3(a.aa_nb);
     k3.blockDim = dim3(kAaThreads);
     k3.kernelParams = a3;
