@@ -138,11 +138,11 @@ class _Bucket:
     one replica per entry of ``sizes`` (a ragged bucket: replicas of several
     sides advance in one launch per solver stage)."""
 
-    def __init__(self, torch, n, slots, precision, sizes=None):
+    def __init__(self, torch, n, slots, precision, sizes=None, priority=0):
         from .linear_elastic_simulator import Ls2dBatch
         self.n = n
         self.sizes = list(sizes) if sizes is not None else [n] * slots
-        self.stream = torch.cuda.Stream()
+        self.stream = torch.cuda.Stream(priority=priority)
         self.plan = Ls2dBatch([(m, m) for m in self.sizes], precision=precision)
         self.free_by = {}
         for idx in range(len(self.sizes) - 1, -1, -1):
@@ -261,16 +261,23 @@ class Server:
             b.plan.solve(reps, ebs, outs, [None] * len(reps), max_iter=self.ls_max_iter, tol=self.ls_tol,
                          sync=True, stream=b.stream)
 
-    def _bucket(self, n):
+    def _bucket(self, n, kind="trajectory"):
+        """The 2D bucket of side n: in the served form single solves and
+        trajectories have separate buckets, the solves' on a high-priority
+        stream (a solve's few kernels are scheduled ahead of the long
+        trajectory and 3D work at kernel boundaries); one bucket per side in
+        the sequential form."""
         if self.ragged is not None:  # one bucket for every 2D request
             b = self.buckets.get("ragged")
             if b is None:
                 b = self.buckets["ragged"] = _Bucket(self.torch, 0, 0, self.precision, sizes=self.ragged)
             return b
-        b = self.buckets.get(n)
+        key = (n, kind) if self.served else n
+        b = self.buckets.get(key)
         if b is None:
             k = self.slots.get(n, 4) if self.served else 1
-            b = self.buckets[n] = _Bucket(self.torch, n, k, self.precision)
+            prio = -1 if self.served and kind == "solve" else 0
+            b = self.buckets[key] = _Bucket(self.torch, n, k, self.precision, priority=prio)
         return b
 
     def _finish(self, res, out=None, error=""):
@@ -571,8 +578,8 @@ class Server:
         torch = self.torch
         if self.ragged is not None:
             self._prepare_ragged()
-        for n in sorted({r.n for r in requests if r.dim == 2} if self.ragged is None else ()):
-            b = self._bucket(n)
+        for n, kind in sorted({(r.n, r.kind) for r in requests if r.dim == 2} if self.ragged is None else ()):
+            b = self._bucket(n, kind)
             with torch.cuda.stream(b.stream):
                 E, nu, ep, eb = W.ls2d_problem_dev(n, n, 0, self.dev)
                 eps = torch.empty((n, n, 2, 2), dtype=torch.float64, device=self.dev)
@@ -628,7 +635,7 @@ class Server:
         # one finite-strain worker per side, each with its plan and stream:
         # load steps of different sides overlap on the device
         fs_qs = {n: queue.Queue() for n in sorted({r.n for r in order if r.dim == 3 and r.kind == "solve"})}
-        workers_fs = [threading.Thread(target=self._fs_worker, args=(q, torch.cuda.Stream()), daemon=True)
+        workers_fs = [threading.Thread(target=self._fs_worker, args=(q, torch.cuda.Stream(priority=-1)), daemon=True)
                       for q in fs_qs.values()]
         # one 3D-trajectory worker per side: a side's rounds (synchronous
         # batched solves) do not wait behind another side's
@@ -649,7 +656,7 @@ class Server:
                     if r.dim == 3:
                         (t3_qs if r.kind == "trajectory" else fs_qs)[r.n].put(r)
                     else:
-                        self._bucket(r.n).waiting.append(r)
+                        self._bucket(r.n, r.kind).waiting.append(r)
                 progressed = False
                 for b in self.buckets.values():
                     while b.waiting and b.has_free(b.waiting[0].n) and (self.used + footprint_bytes(b.waiting[0], self.n_modes)
