@@ -172,13 +172,15 @@ def test_checkpoint_resume_is_bit_exact(tmp_path, selection, ls_start, precision
     assert res["time"] == full["time"] and res["solves"] == full["solves"]
 
 
-@pytest.mark.parametrize("selection,ls_start,precision", [("exact", "cold", "fp64"), ("fast", "warm", "mixed")])
-def test_kmc3d_checkpoint_resume_is_bit_exact(tmp_path, selection, ls_start, precision):
+@pytest.mark.parametrize("n,selection,ls_start,precision", [(32, "exact", "cold", "fp64"),
+                                                           (64, "fast", "warm", "mixed")])
+def test_kmc3d_checkpoint_resume_is_bit_exact(tmp_path, n, selection, ls_start, precision):
     # a 3D trajectory checkpointed after 20 AQS steps (the reference's 3D
     # layout plus the resume group) and resumed equals the uninterrupted run
+    # (the mixed 3D form runs sides 64, 96 and 128)
     from mgkmc_b200 import checkpoint as C
     from mgkmc_b200.kmc3d import Kmc3D, in_plane_modes
-    n, M = 32, 8
+    M = 8
     rng0 = np.random.default_rng(4)
     E, nu = W.ls3d_material(n, n, n, rng0)
     cat = in_plane_modes(rng0.uniform(0.0, np.pi, (n, n, n, M)), 0.1)
