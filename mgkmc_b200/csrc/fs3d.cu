@@ -202,6 +202,7 @@ struct VoxelLaw {
       const T lam3 = (T(2) * mu * lam) / fmax(T(1e-14), T(2) * mu - lam);
       const T target = mu - lam3 * log(fmax(T(1e-14), Je));
       T x = T(1);
+#pragma unroll 1
       for (int it = 0; it < 10; ++it) {
         const T fx = mu * x + T(0.5) * lam3 * log(x) - target;
         const T dx = -fx / (mu + T(0.5) * lam3 / x);

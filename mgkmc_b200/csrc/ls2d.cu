@@ -317,6 +317,7 @@ __device__ __forceinline__ void landau_sigma(double mu, double lam, double a11, 
     const double v1 = lp[0], v2 = lp[1], g1 = lp[3], g2 = lp[4], g3 = lp[5], g4 = lp[6];
     const double Gt = lp[9] * mu;
     e33 = -lam / (lam + 2.0 * mu) * (a11 + a22);
+#pragma unroll 1
     for (int it = 0; it < 64; ++it) {
       const LandauScal t = landau_scal(mu, lam, a11, a22, a12, a21, e33, lp);
       const double c33 = t.c33, I1 = t.I1, I2 = t.I2;
