@@ -253,6 +253,25 @@ def test_landau_capped_iterations_return_the_mixed_iterate(les, it):
     assert rel(sig, o[1]) < TOL
 
 
+def test_landau_anderson_nearly_degenerate_history(les):
+    # a nearly homogeneous medium: the residual contracts along almost one
+    # direction, the history's difference columns become nearly parallel
+    # and the Gram matrix nearly singular (the least squares leaves the
+    # Cholesky path); the fixed point still equals the oracle's (numpy
+    # lstsq, as the reference) to 1e-9 at a tolerance near round-off
+    rng = np.random.default_rng(31)
+    n = 64
+    lam = np.full((n, n), 5.8e10) * (1 + 1e-4 * rng.standard_normal((n, n)))
+    mu = np.full((n, n), 3.3e10) * (1 + 1e-4 * rng.standard_normal((n, n)))
+    eb = np.array([[0.006, 0.001], [0.001, -0.002]])
+    eps, sig, _, _ = les.spectral_solver_landau_2d(lam, mu, **_landau_kw(LANDAU_V), eps_bar=eb, max_iter=400,
+                                                   tol=1e-13, anderson_m=5)
+    o = OL.spectral_solver_landau_2d(lam, mu, LANDAU_V, eb, None, max_iter=400, tol=1e-13, anderson_m=5)
+    assert np.all(np.isfinite(eps)) and np.all(np.isfinite(sig))
+    assert rel(eps, o[0]) < TOL
+    assert rel(sig, o[1]) < TOL
+
+
 def test_landau_device_loop_iteration_cost(les):
     # the Anderson-mixed Landau loop runs in one graph launch: per-iteration
     # device time at 256^2 (row, column, history update, least squares, mix,
