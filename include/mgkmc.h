@@ -122,7 +122,7 @@ MGK_API int mgk_ls2d_set_landau(mgk_ls2d_t plan, const double* v, int capping, d
 /* Where the output pass of later solves writes replica rep's out-of-plane
  * strain e33 under the plane-stress Landau law (device, N doubles; NULL: not
  * written), the field the reference returns in its e33_state
- * (elasticity.py:613-614). */
+ * (elasticity.py:614-615). */
 MGK_API int mgk_ls2d_set_e33_out(mgk_ls2d_t plan, int rep, double* e33);
 /* Type-II Anderson mixing of depth m (0 <= m <= 8; 0 turns it off) inside
  * the device loop of every later solve of this FP64 plan, as
