@@ -440,7 +440,7 @@ def run_serving(window, n_plain=0, progress=None):
     out["plain_fp64_sequential"] = plain
     from mgkmc_b200 import serving as SV
     out["autotuned_ls_families"] = {f"{k[0]}^2 x{k[1]} {k[2]}": {"family": v[0], "ms_per_iteration": v[1]}
-                                    for k, v in SV._TUNED.items()}
+                                    for k, v in SV._TUNED.items() if isinstance(k[0], int)}
     a = out["served_mixed"]
     if a.get("completed"):
         out["solves_per_s_ratio"] = a["solves_per_s"] / plain["solves_per_busy_s"]

@@ -32,11 +32,14 @@ call (one launch per stage, loop on the device) and records an event; a
 size's next round starts as soon as its event completes, independently of the
 other sizes, so the work of different sizes overlaps on the device.  Solves
 use the mixed-precision form and warm starts from the device-resident fields
-(the previous macro iterate, or the trajectory's previous field).  3D
-finite-strain steps run on a worker thread with their own stream; 3D
-trajectories on a second worker thread that advances them in rounds over
-per-size batched 3D LS plans (one solve launch per stage for every admitted
-trajectory of a size); both overlap with the 2D work.
+(the previous macro iterate, or the trajectory's previous field).  Single
+solves and trajectories of a size have separate plans, the solves' on
+high-priority streams, so that a solve's kernels are scheduled ahead of the
+long trajectory work at kernel boundaries.  3D finite-strain steps run on one
+worker thread per size with its own high-priority stream; 3D trajectories on
+one worker thread per size that advances them in rounds over a batched 3D LS
+plan (one solve launch per stage for every admitted trajectory of the size);
+all of it overlaps with the 2D work.
 
 Sequential form (``mode="sequential"``): the plain FP64 form of the same
 requests one at a time in arrival order, cold LS starts and the exact
