@@ -39,6 +39,34 @@ def test_linear_elastic_simulation_2d_matches_reference(golden):
     assert rel(sig_l[-1], g["sig_last"]) < 1e-9
 
 
+def test_ramps_write_vtk_on_the_reference_schedule(golden, tmp_path):
+    # vtk_interval 2 over 3 load steps: files at steps 0 and 2 and the final
+    # one (3 % 2 != 0), holding the step's fields (linear_elastic_simulator.py
+    # :237-256); the finite-strain ramp with "last" writes only the final one
+    from mgkmc_b200 import vtk as V
+    from mgkmc_b200.finite_strain_simulator import finite_strain_simulation_2d
+    from mgkmc_b200.linear_elastic_simulator import linear_elastic_simulation_2d
+    g = golden("ls2d_macro_16")
+    path = str(tmp_path / "ls")
+    epsM, sigM, eps_l, sig_l = linear_elastic_simulation_2d(
+        g["E"], g["nu"], g["mask"], g["target"], n_steps=3, tol_ls=1e-10, max_iter_ls=300, tol_macro=1e3,
+        max_iter_macro=30, enable_console=False, vtk_path=path, vtk_interval=2)
+    import os
+    assert sorted(f for f in os.listdir(tmp_path) if f.endswith(".vtu")) == \
+        ["ls_000000.vtu", "ls_000002.vtu", "ls_final.vtu"]
+    _, _, _, cd = V.read_vtu(path + "_final.vtu")
+    np.testing.assert_array_equal(cd["sig_xx"], sig_l[-1][..., 0, 0].ravel())
+    np.testing.assert_array_equal(cd["eps_xy"], eps_l[-1][..., 0, 1].ravel())
+    fpath = str(tmp_path / "fs")
+    F_m, S_m, P_m, F_l, S_l = finite_strain_simulation_2d(
+        g["E"], g["nu"], (0, 0), 0.004, 2, mixed_targets={}, tol_NW=1e-10, tol_CG=1e-11, max_NW=30,
+        enable_console=False, model_type="svk", solver="newton_cg", vtk_path=fpath, vtk_interval="last")
+    _, _, _, cd = V.read_vtu(fpath + "_final.vtu")
+    np.testing.assert_array_equal(cd["sig_yy"], S_l[-1][1, 1].ravel())
+    E_GL = 0.5 * (np.einsum("kixy,kjxy->ijxy", F_l[-1], F_l[-1]) - np.eye(2)[:, :, None, None])
+    np.testing.assert_allclose(cd["eps_xx"], E_GL[0, 0].ravel(), rtol=0, atol=1e-15)
+
+
 def test_linear_elastic_simulation_3d_matches_reference(golden):
     from mgkmc_b200.linear_elastic_simulator import linear_elastic_simulation_3d
     g = golden("ls3d_macro_8x6x4")
