@@ -99,6 +99,24 @@ def _rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def _max_over_ranks(values, device=None):
+    """Element-wise maximum of per-rank values over the job's ranks (a job's
+    time is its slowest rank's); the values themselves on one process."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def _job_rates(ms, per_rank_items, steps, world):
+    """Whole-job throughput: every rank's items over the slowest rank's time
+    (ms: {form: max-over-ranks milliseconds for `steps` steps})."""
+    return {k: per_rank_items * steps * world / (v / 1e3) for k, v in ms.items()}
+
+
 # ------------------------------------------------------------- CPU legs ----
 _THREAD_VARS = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMEXPR_NUM_THREADS",
                 "VECLIB_MAXIMUM_THREADS")
@@ -691,11 +709,8 @@ def run_ours(a):
     clk.start()
     ms = {name: _time_steps(fn, a.steps, flush, stream) for name, fn in forms.items()}
     clocks = clk.stop()
-    if world > 1:
-        t = torch.tensor([ms[k] for k in forms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = {k: float(v) for k, v in zip(forms, t.tolist())}
-    rate = {k: B * a.steps * world / (ms[k] / 1e3) for k in forms}
+    ms = dict(zip(forms, _max_over_ranks([ms[k] for k in forms], dev)))
+    rate = _job_rates(ms, B, a.steps, world)
     head = "batched_mixed" if "batched_mixed" in forms else list(forms)[-1]
 
     # per-kernel timing (CUDA events on the launching stream) over the batch
