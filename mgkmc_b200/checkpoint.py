@@ -54,6 +54,8 @@ def write(path, groups, attrs, fmt=None):
         import h5py
         if not path.endswith(".h5"):
             path += ".h5"
+        # file locking off for the process, as the reference's writers set it
+        # (linear_elastic_simulator.py:573, aqs.py:1209)
         os.environ["HDF5_USE_FILE_LOCKING"] = "FALSE"
         with h5py.File(path, "w") as f:
             for g, d in attrs.items():
@@ -62,7 +64,9 @@ def write(path, groups, attrs, fmt=None):
                     grp.attrs[k] = v
             for k, v in groups.items():
                 v = _to_np(v)
-                f.create_dataset(k, data=v, compression="gzip" if v.ndim >= 2 else None)
+                # chunked (compressed) storage needs a non-empty array: an
+                # empty event list is stored contiguous
+                f.create_dataset(k, data=v, compression="gzip" if v.ndim >= 2 and v.size > 0 else None)
         return path
     if fmt != "npz":
         raise ValueError(f"unknown checkpoint format {fmt!r}")

@@ -74,3 +74,15 @@ def test_trajectory_roundtrip_3d(tmp_path):
         np.testing.assert_array_equal(st[k], sim._st[k])
     assert st["events"] == sim._st["events"] and st["steps_done"] == 5 and st["n_solves"] == 17
     np.testing.assert_array_equal(rng2.random(4), g.random(4))
+
+
+def test_trajectory_without_events(tmp_path):
+    # a checkpoint taken before the first event: an empty flip history that
+    # still reads back as (0, 4) and an empty event list
+    sim = _Fake3D(np.random.default_rng(4))
+    sim._st["events"] = []
+    path = C.save_trajectory(str(tmp_path / "t0"), sim, np.random.default_rng(1), fmt="npz")
+    data, _ = C.load(path)
+    assert data["history/flips"].shape == (0, 4)
+    st, _, _ = C.load_trajectory(path)
+    assert st["events"] == []
