@@ -310,7 +310,7 @@ def run_reference(a):
     v, wall, solves = cpu_ls_steps(P, per_step, max(1, a.warmup), a.steps, NX, TOL)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, survey config)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; the benchmark material and sizes, no dataset)",
             "config": headline_config(a, world),
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": P, "kind": "port",
                              "sample": f"{a.steps} steps x {per_step} solves of the {NX}^2 problem (tol {TOL:g}), "
@@ -855,7 +855,7 @@ def run_ours(a):
     line = {"metric": METRIC, "value": rate[head], "unit": "solves/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms[head] / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "mixed fp32/fp64 (FP32 bulk iterations, FP64 finish, norms and sums)",
-            "data": "synthetic (seeded, survey config)", "config": headline_config(a, world),
+            "data": "synthetic (seeded; the benchmark material and sizes, no dataset)", "config": headline_config(a, world),
             "forms": {"solves_per_s": rate,
                       "speedup_vs_plain_fp64": rate[head] / rate["plain_fp64"] if "plain_fp64" in rate else None,
                       "iters_mean": {k: float(np.mean(v)) for k, v in iters.items()},
