@@ -47,6 +47,11 @@ _TABLE = [
     ("linear_elastic_simulator", "spectral_solver_landau_3d", _les.spectral_solver_landau_3d),  # aqs.py:331
     ("linear_elastic_simulator", "linear_elastic_simulation_2d", _les.linear_elastic_simulation_2d),  # run.py:729
     ("linear_elastic_simulator", "linear_elastic_simulation_3d", _les.linear_elastic_simulation_3d),  # run.py:934
+    ("linear_elastic_simulator", "secant_elastic_simulation_2d", _les.secant_elastic_simulation_2d),  # run.py:544
+    ("linear_elastic_simulator", "rose_elastic_simulation_2d", _les.rose_elastic_simulation_2d),      # run.py:608
+    ("linear_elastic_simulator", "landau_elastic_simulation_2d", _les.landau_elastic_simulation_2d),  # run.py:666
+    ("linear_elastic_simulator", "secant_elastic_simulation_3d", _les.secant_elastic_simulation_3d),  # run.py:830
+    ("linear_elastic_simulator", "landau_elastic_simulation_3d", _les.landau_elastic_simulation_3d),  # run.py:879
     ("finite_strain_simulator", "finite_strain_solver_step_2d", _fss.finite_strain_solver_step_2d),   # ks:403-418
     ("finite_strain_simulator", "finite_strain_solver_step_3d", _fss.finite_strain_solver_step_3d),   # aqs.py:289
     ("finite_strain_simulator", "finite_strain_simulation_3d", _fss.finite_strain_simulation_3d),     # run.py:783

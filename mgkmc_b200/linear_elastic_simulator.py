@@ -752,3 +752,322 @@ def linear_elastic_simulation_3d(E, nu, target_strain_mask, target_values, n_ste
     return _ramp(3, E, nu, target_strain_mask, target_values, n_steps, pixel, tol_ls, max_iter_ls, tol_macro,
                  max_iter_macro, store, "plane_strain", log_path, global_log_path, driving_component, enable_console,
                  vtk_path, vtk_interval, dict(solver_kw))
+
+
+# ------------------------------------ nonlinear mixed-BC load ramps ---
+# The load-step drivers of the secant, Rose and Landau solvers
+# (linear_elastic_simulator.py:1353-2517).  Each load step runs the same
+# macro loop as the linear ramps, calling the nonlinear device solver (the
+# drop-ins above) once per macro iteration, warm-started from the previous
+# load step's final field.  The stress-controlled components are corrected
+# by the compliance of the solver's reference medium; the Landau ramps
+# replace that slope per component by the secant slope of the last two macro
+# iterates once it is trustworthy (:2186-2204).
+
+def _vm_eq_2d(eps):
+    """Von Mises equivalent strain of a 2D field with eps_33 = 0
+    (elasticity.py:641-663): the in-plane trace removed, the out-of-plane
+    deviator -(e11 + e22)/3, the shear as the mean of e12 and e21."""
+    e11, e22 = eps[..., 0, 0], eps[..., 1, 1]
+    t3 = (e11 + e22) / 3.0
+    g = 0.5 * (eps[..., 0, 1] + eps[..., 1, 0])
+    return np.sqrt((2.0 / 3.0) * ((e11 - t3) ** 2 + (e22 - t3) ** 2 + t3 ** 2 + 2.0 * g ** 2))
+
+
+def _vm_eq_3d(eps):
+    """Von Mises equivalent strain of a 3D field (elasticity.py:665-700)."""
+    t3 = np.trace(eps, axis1=-2, axis2=-1) / 3.0
+    dev = sum((eps[..., i, i] - t3) ** 2 for i in range(3))
+    shear = sum((eps[..., i, j] + eps[..., j, i]) ** 2 for i, j in ((0, 1), (0, 2), (1, 2)))
+    return np.sqrt((2.0 / 3.0) * (dev + 0.5 * shear))
+
+
+def _e_nu(lam, mu):
+    """(E, nu) of Lame moduli, guarded as the ramps' VTK output guards them."""
+    return mu * (3.0 * lam + 2.0 * mu) / (lam + mu + 1e-30), lam / (2.0 * (lam + mu) + 1e-30)
+
+
+def _rose_mu_sec_2d(eps, lam, mu, eta, floor_f, plane_mode):
+    """The Rose secant shear modulus of a 2D field for the ramp's VTK output
+    (linear_elastic_simulator.py:1766-1800): plane strain at e33 = 0; plane
+    stress with e33 from five fixed-point steps of the isotropic relation
+    e33 = -(3K - 2G)/(3K + 4G) (e11 + e22) from the linear guess, G taken
+    before the last step."""
+    exx, eyy, exy = eps[..., 0, 0], eps[..., 1, 1], eps[..., 0, 1]
+
+    def g_of(ezz):
+        t3 = (exx + eyy + ezz) / 3.0
+        eq = np.sqrt((2.0 / 3.0) * ((exx - t3) ** 2 + (eyy - t3) ** 2 + (ezz - t3) ** 2 + 2.0 * exy ** 2))
+        return np.maximum(mu * np.exp(-eta * eq), floor_f * mu)
+
+    if plane_mode != "plane_stress":
+        return g_of(0.0)
+    K = lam + (2.0 / 3.0) * mu
+    ezz = -lam / (lam + 2.0 * mu) * (exx + eyy)
+    for _ in range(5):
+        G = g_of(ezz)
+        ezz = -(3.0 * K - 2.0 * G) / (3.0 * K + 4.0 * G) * (exx + eyy)
+    return G
+
+
+class _RampLog:
+    """The ramps' per-step log (timestamp, elapsed time, step, driven strain
+    and stress) and global log (every independent component), in the
+    reference's column layout."""
+
+    def __init__(self, dim, log_path, global_log_path, driving_component):
+        import time as _time
+        self.lbl = _COMP_LABELS.get(tuple(driving_component), "xx")
+        self.ij = tuple(driving_component)
+        self.comps = [(0, 0), (1, 1), (0, 1)] if dim == 2 else [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+        self.f = open(log_path, "w", buffering=1) if log_path else None
+        if self.f:
+            hdr = (f"{'Timestamp':<20} {'Elapsed(s)':<12} {'Step':<8} {'Eps_' + self.lbl:<14} "
+                   f"{'Sig_' + self.lbl + '(GPa)':<16}\n")
+            self.f.write(hdr)
+            self.f.write("-" * len(hdr.rstrip()) + "\n")
+        self.g = open(global_log_path, "w", buffering=1) if global_log_path else None
+        if self.g:
+            ghdr = f"{'GlobalStep':<12} " + " ".join(f"{'Eps_' + _COMP_LABELS[c]:<14}" for c in self.comps) + " " + \
+                   " ".join(f"{'Sig_' + _COMP_LABELS[c] + '(GPa)':<16}" for c in self.comps) + "\n"
+            self.g.write(ghdr)
+            self.g.write("-" * len(ghdr.rstrip()) + "\n")
+        self.t0 = _time.time()
+
+    def step(self, s, n_steps, epsM, sigM, console):
+        import time as _time
+        from datetime import datetime as _dt
+        e, g = epsM[self.ij], sigM[self.ij]
+        if console:
+            print(f"step {s}/{n_steps}: eps_{self.lbl}={e:.4f}, sig_{self.lbl}={g / 1e9:.4f} GPa")
+        if self.f:
+            self.f.write(f"{_dt.now().strftime('%Y-%m-%d %H:%M:%S'):<20} {_time.time() - self.t0:<12.3f} {s:<8} "
+                         f"{e:<14.6f} {g / 1e9:<16.6f}\n")
+        if self.g:
+            self.g.write(f"{s:<12} " + " ".join(f"{epsM[c]:<14.6f}" for c in self.comps) + " " +
+                         " ".join(f"{sigM[c] / 1e9:<16.6f}" for c in self.comps) + "\n")
+
+    def close(self, console):
+        import time as _time
+        from datetime import datetime as _dt
+        total = _time.time() - self.t0
+        m_, s_ = divmod(total, 60)
+        h_, m_ = divmod(m_, 60)
+        dur = (f"\nSimulation Finish Time: {_dt.now().strftime('%Y-%m-%d %H:%M:%S')}\nTotal Duration: {total:.2f} "
+               f"seconds ({int(h_):d}h {int(m_):02d}m {int(s_):02d}s)\n")
+        if self.f:
+            self.f.write(dur)
+            self.f.close()
+        if self.g:
+            self.g.close()
+        if console:
+            print(dur)
+
+
+def _nl_ramp(dim, solve, lam, mu, mu_ref, target_strain_mask, target_values, n_steps, tol_macro, max_iter_macro,
+             store, pixel, log_path, global_log_path, driving_component, enable_console, vtk_path, vtk_interval,
+             solver_kw, vtk_moduli, secant_slopes=False):
+    """Load ramp of the nonlinear drivers.  ``solve(eps_bar, eps_init)``
+    returns (eps, sig, eps_mean, sig_mean) of one device solve; ``mu_ref`` is
+    the shear modulus of the solver's reference medium (lambda is the mean
+    lambda), whose isotropic compliance corrects the stress-controlled
+    components; ``vtk_moduli(eps)`` gives the (E, nu) fields written with
+    the VTK output.  Checkpoints carry the linear (E, nu) of (lambda, mu): the
+    reference passes None there, which its writer cannot store."""
+    chk_ival = solver_kw.pop("checkpoint_interval", None)
+    chk_path = solver_kw.pop("checkpoint_path", "checkpoint")
+    if chk_path and chk_ival not in (None, "none"):
+        import os
+        os.makedirs(os.path.dirname(chk_path) or ".", exist_ok=True)
+    mask = np.asarray(target_strain_mask, dtype=bool)
+    stress_mask = ~mask
+    target_values = np.asarray(target_values, dtype=np.float64)
+    lam_avg = float(np.mean(lam))
+    E_ref = mu_ref * (3.0 * lam_avg + 2.0 * mu_ref) / (lam_avg + mu_ref)
+    nu_ref = lam_avg / (2.0 * (lam_avg + mu_ref))
+    log = _RampLog(dim, log_path, global_log_path, driving_component)
+    cur = np.zeros((dim, dim))
+    warm = None
+    eps_macro_list, sig_macro_list, eps_list, sig_list = [], [], [], []
+    for s in range(n_steps + 1):
+        target_s = target_values * (s / n_steps)
+        max_err = 0.0
+        prev_e = prev_s = None  # secant history of the stress-controlled components, per load step
+        for _ in range(max_iter_macro):
+            cur[mask] = target_s[mask]
+            eps, sig, epsM, sigM = solve(cur.copy(), warm)
+            err = np.zeros((dim, dim))
+            err[stress_mask] = target_s[stress_mask] - sigM[stress_mask]
+            max_err = np.max(np.abs(err[stress_mask])) if np.any(stress_mask) else 0.0
+            if max_err < tol_macro:
+                break
+            d = ((err - nu_ref * np.trace(err) * np.eye(dim)) / E_ref)[stress_mask]
+            if secant_slopes:
+                e_sc, s_sc = cur[stress_mask].copy(), np.asarray(sigM)[stress_mask].copy()
+                if prev_e is not None:
+                    de, ds = e_sc - prev_e, s_sc - prev_s
+                    with np.errstate(divide="ignore", invalid="ignore"):
+                        slope = ds / de
+                    ok = np.isfinite(slope) & (np.abs(de) > 1e-14) & (slope > 0.01 * E_ref)
+                    d[ok] = err[stress_mask][ok] / slope[ok]
+                prev_e, prev_s = e_sc, s_sc
+            cur[stress_mask] += d
+        else:
+            print(f"Warning: Macro loop did not converge at step {s} (err={max_err:.2e})")
+        warm = eps
+        eps_macro_list.append(epsM)
+        sig_macro_list.append(sigM)
+        if store:
+            eps_list.append(eps)
+            sig_list.append(sig)
+        log.step(s, n_steps, epsM, sigM, enable_console)
+        if chk_ival is not None and chk_ival not in ("none", "last"):
+            name = None
+            if chk_ival == "current":
+                name = f"{chk_path}.h5"
+            elif isinstance(chk_ival, int) and s % chk_ival == 0:
+                name = f"{chk_path}_{s:06d}.h5"
+            if name:
+                _save_chk(dim, name, s, *_e_nu(lam, mu), eps, sig, epsM, sigM, pixel)
+        if vtk_interval is not None and vtk_interval not in ("none", "last"):
+            _vtk_step(vtk_interval, vtk_path, s, eps, sig, *vtk_moduli(eps), pixel)
+    if chk_ival == "last":
+        _save_chk(dim, f"{chk_path}_final.h5", n_steps, *_e_nu(lam, mu), eps, sig, epsM, sigM, pixel)
+    if vtk_interval == "last" and vtk_path:
+        from .vtk import export_to_vtk
+        export_to_vtk(f"{vtk_path}_final.vtu", eps, sig, *vtk_moduli(eps), pixel, match_matplotlib_orientation=True)
+    log.close(enable_console)
+    return np.array(eps_macro_list), np.array(sig_macro_list), eps_list, sig_list
+
+
+def _pop_landau_kw(solver_kw):
+    """The Landau ramps' solver options (linear_elastic_simulator.py:2121-2127)."""
+    return dict(solver=solver_kw.pop("solver", "dbfft"),
+                strain_capping_enabled=solver_kw.pop("strain_capping_enabled", False),
+                strain_capping_limit=solver_kw.pop("strain_capping_limit", None),
+                strain_capping_tangent_ratio=solver_kw.pop("strain_capping_tangent_ratio", 0.1),
+                strain_capping_type=solver_kw.pop("strain_capping_type", "piecewise"),
+                strain_capping_smooth_power=solver_kw.pop("strain_capping_smooth_power", 1.0))
+
+
+def secant_elastic_simulation_2d(lam, mu, d, k, target_strain_mask, target_values, n_steps=20, pixel=1.0, tol_ls=1e-6,
+                                 max_iter_ls=400, tol_macro=1e-4, max_iter_macro=20, store=True,
+                                 plane_mode="plane_strain", log_path=None, global_log_path=None,
+                                 driving_component=(0, 0), enable_console=True, vtk_path=None, vtk_interval="none",
+                                 **solver_kw):
+    """Mixed stress/strain ramp with the secant-degradation law in 2D
+    (linear_elastic_simulator.py:1353-1600); returns as
+    linear_elastic_simulation_2d.  VTK moduli from the secant shear modulus
+    of the final strain (:1567-1571)."""
+    lam = np.asarray(lam, dtype=np.float64)
+    mu = np.asarray(mu, dtype=np.float64)
+
+    def solve(eb, init):
+        return spectral_solver_secant_2d(lam, mu, d, k, eb, max_iter=max_iter_ls, tol=tol_ls, pixel=pixel,
+                                         plane_mode=plane_mode, eps_init=init)
+
+    def moduli(eps):
+        return _e_nu(lam, mu * (1.0 - d * (1.0 - np.exp(-k * _vm_eq_2d(eps)))))
+
+    return _nl_ramp(2, solve, lam, mu, float(mu.mean()), target_strain_mask, target_values, n_steps, tol_macro,
+                    max_iter_macro, store, pixel, log_path, global_log_path, driving_component, enable_console,
+                    vtk_path, vtk_interval, dict(solver_kw), moduli)
+
+
+def rose_elastic_simulation_2d(lam, mu, eta, mu_floor_fraction=0.1, target_strain_mask=None, target_values=None,
+                               n_steps=20, pixel=1.0, tol_ls=1e-6, max_iter_ls=400, tol_macro=1e-4, max_iter_macro=20,
+                               store=True, plane_mode="plane_strain", log_path=None, global_log_path=None,
+                               driving_component=(0, 0), enable_console=True, vtk_path=None, vtk_interval="none",
+                               **solver_kw):
+    """Mixed stress/strain ramp with the Rose law in 2D
+    (linear_elastic_simulator.py:1603-1856): the compliance of the solver's
+    reference medium (mean lambda, (1 + floor) mean mu / 2) corrects the
+    stress-controlled components (:1640-1652); returns as
+    linear_elastic_simulation_2d."""
+    lam = np.asarray(lam, dtype=np.float64)
+    mu = np.asarray(mu, dtype=np.float64)
+
+    def solve(eb, init):
+        return spectral_solver_rose_2d(lam, mu, eta, mu_floor_fraction, eps_bar=eb, max_iter=max_iter_ls, tol=tol_ls,
+                                       pixel=pixel, plane_mode=plane_mode, eps_init=init)
+
+    def moduli(eps):
+        return _e_nu(lam, _rose_mu_sec_2d(eps, lam, mu, eta, mu_floor_fraction, plane_mode))
+
+    mu_ref = 0.5 * (1.0 + mu_floor_fraction) * float(mu.mean())
+    return _nl_ramp(2, solve, lam, mu, mu_ref, target_strain_mask, target_values, n_steps, tol_macro, max_iter_macro,
+                    store, pixel, log_path, global_log_path, driving_component, enable_console, vtk_path,
+                    vtk_interval, dict(solver_kw), moduli)
+
+
+def secant_elastic_simulation_3d(lam, mu, d, k, target_strain_mask, target_values, n_steps=20, pixel=1.0, tol_ls=1e-6,
+                                 max_iter_ls=400, tol_macro=1e-4, max_iter_macro=20, store=True, log_path=None,
+                                 global_log_path=None, driving_component=(0, 0), enable_console=True, vtk_path=None,
+                                 vtk_interval="none", **solver_kw):
+    """Mixed stress/strain ramp with the secant-degradation law in 3D
+    (linear_elastic_simulator.py:1857-2054); returns as
+    linear_elastic_simulation_3d."""
+    lam = np.asarray(lam, dtype=np.float64)
+    mu = np.asarray(mu, dtype=np.float64)
+
+    def solve(eb, init):
+        return spectral_solver_secant_3d(lam, mu, d, k, eb, max_iter=max_iter_ls, tol=tol_ls, pixel=pixel,
+                                         eps_init=init)
+
+    def moduli(eps):
+        return _e_nu(lam, mu * (1.0 - d * (1.0 - np.exp(-k * _vm_eq_3d(eps)))))
+
+    return _nl_ramp(3, solve, lam, mu, float(mu.mean()), target_strain_mask, target_values, n_steps, tol_macro,
+                    max_iter_macro, store, pixel, log_path, global_log_path, driving_component, enable_console,
+                    vtk_path, vtk_interval, dict(solver_kw), moduli)
+
+
+def landau_elastic_simulation_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, target_strain_mask, target_values, n_steps=20,
+                                 pixel=1.0, tol_ls=1e-6, max_iter_ls=400, tol_macro=1e-4, max_iter_macro=20,
+                                 store=True, plane_mode="plane_strain", log_path=None, global_log_path=None,
+                                 driving_component=(0, 0), enable_console=True, vtk_path=None, vtk_interval="none",
+                                 **solver_kw):
+    """Mixed stress/strain ramp with the Landau law in 2D
+    (linear_elastic_simulator.py:2055-2284): the stress-controlled
+    components take the secant slope of the last two macro iterates where it
+    is finite and above 1 % of the reference Young's modulus (:2186-2204),
+    else the compliance step; plane stress passes one e33 state through
+    every solve (:2146).  Solver options (``solver``, strain capping) come in
+    ``solver_kw``; returns as linear_elastic_simulation_2d."""
+    lam = np.asarray(lam, dtype=np.float64)
+    mu = np.asarray(mu, dtype=np.float64)
+    skw = dict(solver_kw)
+    lkw = _pop_landau_kw(skw)
+    e33_state = {} if plane_mode == "plane_stress" else None
+
+    def solve(eb, init):
+        return spectral_solver_landau_2d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eb, max_iter=max_iter_ls, tol=tol_ls,
+                                         pixel=pixel, plane_mode=plane_mode, eps_init=init, e33_state=e33_state,
+                                         **lkw)
+
+    return _nl_ramp(2, solve, lam, mu, float(mu.mean()), target_strain_mask, target_values, n_steps, tol_macro,
+                    max_iter_macro, store, pixel, log_path, global_log_path, driving_component, enable_console,
+                    vtk_path, vtk_interval, skw, lambda eps: _e_nu(lam, mu), secant_slopes=True)
+
+
+def landau_elastic_simulation_3d(lam, mu, v1, v2, v3, g1, g2, g3, g4, target_strain_mask, target_values, n_steps=20,
+                                 pixel=1.0, tol_ls=1e-6, max_iter_ls=400, tol_macro=1e-4, max_iter_macro=20,
+                                 store=True, log_path=None, global_log_path=None, driving_component=(0, 0),
+                                 enable_console=True, vtk_path=None, vtk_interval="none", **solver_kw):
+    """Mixed stress/strain ramp with the Landau law in 3D
+    (linear_elastic_simulator.py:2287-2517), the 2D ramp's macro loop with
+    3x3 tensors.  The global log carries all six independent components
+    under the reference's six-column header (the reference writes xx, yy and
+    xz there only, :2463-2467)."""
+    lam = np.asarray(lam, dtype=np.float64)
+    mu = np.asarray(mu, dtype=np.float64)
+    skw = dict(solver_kw)
+    lkw = _pop_landau_kw(skw)
+
+    def solve(eb, init):
+        return spectral_solver_landau_3d(lam, mu, v1, v2, v3, g1, g2, g3, g4, eb, max_iter=max_iter_ls, tol=tol_ls,
+                                         pixel=pixel, eps_init=init, **lkw)
+
+    return _nl_ramp(3, solve, lam, mu, float(mu.mean()), target_strain_mask, target_values, n_steps, tol_macro,
+                    max_iter_macro, store, pixel, log_path, global_log_path, driving_component, enable_console,
+                    vtk_path, vtk_interval, skw, lambda eps: _e_nu(lam, mu), secant_slopes=True)

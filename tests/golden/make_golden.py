@@ -665,12 +665,52 @@ def ls3d_landau_fixtures():
     save("ls3d_landau_12x8x6", **out)
 
 
+def nl_ramp_fixtures():
+    """The reference's nonlinear small-strain load ramps
+    (linear_elastic_simulator.py:1353-2517: secant_elastic_simulation_2d/3d,
+    rose_elastic_simulation_2d, landau_elastic_simulation_2d/3d) on
+    heterogeneous media: three load steps of a driven xx strain with every
+    other component stress-free, so each load step's macro loop iterates
+    (the Landau ramps with their secant-slope correction)."""
+    rng = np.random.default_rng(81)
+
+    def lame(E, nu):
+        return E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))
+
+    lam2, mu2 = lame(*W.ls2d_material(16, 12, rng))
+    lam3, mu3 = lame(*W.ls3d_material(12, 8, 6, rng))
+    m2 = np.zeros((2, 2), dtype=bool)
+    m2[0, 0] = True
+    m3 = np.zeros((3, 3), dtype=bool)
+    m3[0, 0] = True
+    t2, t3 = np.zeros((2, 2)), np.zeros((3, 3))
+    common = dict(n_steps=3, tol_ls=1e-11, max_iter_ls=600, tol_macro=1e3, max_iter_macro=30, store=True,
+                  enable_console=False)
+    out = dict(lam2=lam2, mu2=mu2, lam3=lam3, mu3=mu3, mask2=m2, mask3=m3, v=np.array(LANDAU_V))
+    runs = (
+        ("secant2d", 0.02, lambda t: LES.secant_elastic_simulation_2d(lam2, mu2, 0.3, 50.0, m2, t, **common)),
+        ("rose2d", 0.02, lambda t: LES.rose_elastic_simulation_2d(lam2, mu2, 30.0, 0.1, m2, t, **common)),
+        ("rose2d_pst", 0.02, lambda t: LES.rose_elastic_simulation_2d(lam2, mu2, 30.0, 0.1, m2, t, **common,
+                                                                      plane_mode="plane_stress")),
+        ("secant3d", 0.02, lambda t: LES.secant_elastic_simulation_3d(lam3, mu3, 0.3, 50.0, m3, t, **common)),
+        ("landau2d", 0.01, lambda t: LES.landau_elastic_simulation_2d(lam2, mu2, *LANDAU_V, m2, t, **common)),
+        ("landau3d", 0.01, lambda t: LES.landau_elastic_simulation_3d(lam3, mu3, *LANDAU_V, m3, t, **common)),
+    )
+    for tag, exx, run in runs:
+        t = (t2 if "2d" in tag else t3).copy()
+        t[0, 0] = exx
+        em, sm, el, sl = run(t)
+        out.update({f"{tag}_target": t, f"{tag}_eps_mac": em, f"{tag}_sig_mac": sm, f"{tag}_eps": el[-1],
+                    f"{tag}_sig": sl[-1]})
+    save("nl_ramps", **out)
+
+
 ALL = ("ls2d_fixtures", "ls3d_fixtures", "kmc2d_fixtures", "kmc3d_fixtures", "fs3d_fixtures", "ls2d_secant_fixtures",
        "ls2d_rose_fixtures", "kmc2d_cascade_fixtures", "kmc2d_patch_fixtures", "ls3d_secant_fixtures",
        "ls2d_landau_fixtures", "kmc2d_trajectory_fixtures", "driver_fixtures",
        "kmc3d_trajectory_fixtures", "fs2d_step_fixtures",
        "fs2d_sim_fixtures", "ls3d_landau_fixtures", "fs2d_pstress_fixtures",
-       "ls2d_landau_pstress_fixtures", "vtk_fixtures")
+       "ls2d_landau_pstress_fixtures", "vtk_fixtures", "nl_ramp_fixtures")
 
 
 if __name__ == "__main__":

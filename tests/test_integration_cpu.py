@@ -46,6 +46,7 @@ def test_patch_real_reference():
         import mgkmc.linear_elastic_simulator as les
         assert ks.select_event_2d is I._kf.select_event_2d
         assert les.linear_elastic_simulation_3d is I._les.linear_elastic_simulation_3d
+        assert les.landau_elastic_simulation_3d is I._les.landau_elastic_simulation_3d
         assert "aqs.apply_flip_soa" in done
     finally:
         I.unpatch_reference()
