@@ -696,12 +696,22 @@ def nl_ramp_fixtures():
         ("landau2d", 0.01, lambda t: LES.landau_elastic_simulation_2d(lam2, mu2, *LANDAU_V, m2, t, **common)),
         ("landau3d", 0.01, lambda t: LES.landau_elastic_simulation_3d(lam3, mu3, *LANDAU_V, m3, t, **common)),
     )
+    # the (E, nu) fields each ramp hands to its VTK writer on the "last"
+    # schedule, recorded from the reference's own call
+    seen = {}
+
+    def record(fname, eps, sig, E, nu, pixel=1.0, **kw):
+        seen["E"], seen["nu"] = np.array(E), np.array(nu)
+
+    LES.export_to_vtk = record
+    common.update(vtk_path=os.path.join(HERE, "_unused"), vtk_interval="last")
     for tag, exx, run in runs:
         t = (t2 if "2d" in tag else t3).copy()
         t[0, 0] = exx
+        seen.clear()
         em, sm, el, sl = run(t)
         out.update({f"{tag}_target": t, f"{tag}_eps_mac": em, f"{tag}_sig_mac": sm, f"{tag}_eps": el[-1],
-                    f"{tag}_sig": sl[-1]})
+                    f"{tag}_sig": sl[-1], f"{tag}_vtk_E": seen["E"], f"{tag}_vtk_nu": seen["nu"]})
     save("nl_ramps", **out)
 
 

@@ -144,3 +144,22 @@ def test_vm_equivalent_strains():
     s3 = 0.5 * (e3 + np.swapaxes(e3, -1, -2))
     d3 = s3 - np.trace(s3, axis1=-2, axis2=-1)[..., None, None] * np.eye(3) / 3
     np.testing.assert_allclose(les._vm_eq_3d(e3), np.sqrt(2 / 3 * np.sum(d3 ** 2, axis=(-2, -1))), rtol=1e-13)
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_ramp_vtk_moduli_match_reference(golden, oracle_solvers, monkeypatch, tmp_path, tag):
+    # the (E, nu) fields written with the final VTK file: the secant and Rose
+    # ramps' secant moduli of the final strain (Rose plane stress with its
+    # e33 fixed point), the Landau ramps' linear moduli
+    from mgkmc_b200 import vtk
+    seen = {}
+
+    def record(fname, eps, sig, E, nu, pixel=1.0, **kw):
+        seen["name"], seen["E"], seen["nu"] = fname, np.array(E), np.array(nu)
+
+    monkeypatch.setattr(vtk, "export_to_vtk", record)
+    g = golden("nl_ramps")
+    run_ramp(g, tag, vtk_path=str(tmp_path / "r"), vtk_interval="last", store=False)
+    assert seen["name"] == str(tmp_path / "r") + "_final.vtu"
+    np.testing.assert_allclose(seen["E"], g[f"{tag}_vtk_E"], rtol=1e-12)
+    np.testing.assert_allclose(seen["nu"], g[f"{tag}_vtk_nu"], rtol=1e-12)
