@@ -86,3 +86,45 @@ def test_trajectory_without_events(tmp_path):
     assert data["history/flips"].shape == (0, 4)
     st, _, _ = C.load_trajectory(path)
     assert st["events"] == []
+
+
+class _Fake2D:
+    """A stand-in for Kmc2D's checkpoint surface (no device needed)."""
+
+    def __init__(self, rng):
+        self.nx, self.ny, self.M = 6, 4, 3
+        sh = (6, 4)
+        self.p = dict(T=250.0, gamma0=0.1, nu0=1e13, strain_rate=1e7, jp=0.1, jt=0.2, jn=0.3, cap=2.0)
+        self.selection, self.ls_start = "exact", "cold"
+        self.ls = type("P", (), {"precision": "fp64"})()
+        self.stability_threshold = -0.05
+        self._st = {"E": rng.random(sh), "nu": rng.random(sh), "eps": rng.random(sh + (2, 2)),
+                    "sig": rng.random(sh + (2, 2)), "eps_p": rng.random(sh + (2, 2)), "soft": rng.random(sh + (2,)),
+                    "Q": rng.random(sh + (3,)), "Q0": rng.random(sh + (3,)), "catalog": rng.random(sh + (3, 2, 2)),
+                    "t_last": rng.random(sh), "prev": rng.random(sh + (2, 2)), "eps_macro": rng.random((2, 2)),
+                    "time": 3.5e-9, "events": [(5, 1, 2, 1.0e-9), (0, 3, 0, 2.5e-9), (2, 2, 1, 3.0e-9)],
+                    "n_solves": 9, "steps_done": 4, "unit_ready": True, "flips_since_sync": 2}
+
+    def state_dict(self):
+        return dict(self._st)
+
+
+def test_trajectory_roundtrip_2d(tmp_path):
+    # the 2D trajectory checkpoint: flips as (x, y, m), nz = 1 in the
+    # metadata, the fast-patching counters and the cascade threshold kept
+    sim = _Fake2D(np.random.default_rng(6))
+    g = np.random.default_rng(7)
+    g.normal(size=5)
+    path = C.save_trajectory(str(tmp_path / "t2"), sim, g, fmt="npz")
+    data, attrs = C.load(path)
+    assert data["history/flips"].shape == (3, 3) and data["history/flips"].dtype == np.int32
+    meta = attrs["metadata"]
+    assert meta["nz"] == 1 and meta["M"] == 3 and meta["stability_threshold"] == -0.05
+    assert meta["temperature"] == 250.0 and meta["neighbor_softening_fraction"] == 0.3
+    np.testing.assert_array_equal(data["fields/Tlocal"], np.full((6, 4), 250.0))
+    st, g2, _ = C.load_trajectory(path)
+    for k in ("eps", "sig", "eps_p", "soft", "Q", "Q0", "catalog", "t_last", "prev", "eps_macro", "E", "nu"):
+        np.testing.assert_array_equal(st[k], sim._st[k])
+    assert st["events"] == sim._st["events"] and st["unit_ready"] is True and st["flips_since_sync"] == 2
+    assert st["time"] == 3.5e-9 and st["steps_done"] == 4 and st["n_solves"] == 9
+    np.testing.assert_array_equal(g2.normal(size=4), g.normal(size=4))
